@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Time-to-gap benchmark of the SDPX interior-point hot path on B200.
+
+Workload: the bootstrap-shaped Float64 SDP -- 32 PSD blocks of order U{10..60} with Chebyshev
+bases, m = 2000 constraints of four rank-one terms each, seed 0 -- solved to the reference's
+default gap 1e-8 with the condensed KKT form.  One "step" is one complete solve to the gap.
+
+  value     time-to-gap (s) with the problem already resident in HBM (sdpx_solve), max over ranks
+  e2e       the same metric through the C ABI with host buffers: sdpx_prepare (copy, Ruiz
+            equilibration, H2D upload) + sdpx_solve + sdpx_result_f64 (D2H) + sdpx_destroy
+  roofline  the dominant device phase, timed with CUDA events on the library's stream
+  cpu_baseline  the oracle (reference-algorithm CPU restatement, numpy/OpenBLAS, all host cores)
+            on a bounded sample of the same solve (the first iterations), projected to the gap
+
+``--impl reference`` times the reference's CPU path (the oracle port; the Rust reference cannot be
+built on this image) on rank 0 and prints the same metric.  Multi-GPU runs are independent
+replicas (the solve does not shard): each rank solves the same instance on its own GPU.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "sdpx.rs_b200"))
+
+METRIC = "time-to-gap 1e-8 (Float64, plain GPU form)"
+WORKLOAD = {"workload": "rank1_sdp: 32 PSD blocks n_j~U{10..60}, Chebyshev bases s_j=2n_j, "
+                        "m=2000 constraints x 4 rank-one terms, seed 0, gap 1e-8, kkt_form condensed",
+            "blocks": 32, "m": 2000, "seed": 0, "precision_bits": 53,
+            "l2": "inputs resident; the Schur complement (32 MB) and its factor are rewritten every "
+                  "iteration, per-solve working set ~0.2 GB > 126 MB L2"}
+CPU_SAMPLE_ITERS = 5
+
+
+def make_problem():
+    from sdpx_b200 import problems
+    return problems.rank1_sdp(32, 2000, seed=0)
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def fp64_gemm_peak():
+    """cuBLAS DGEMM throughput on this GPU (TFLOP/s): the FP64 roofline denominator."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(4):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def schur_model(prob):
+    """Algorithmic work of one iteration's phases (Measurement)."""
+    import numpy as np
+    n = prob.n
+    orders = [d for _, d in prob.cones]
+    A = prob.A.tocsc()
+    k = []
+    r0 = 0
+    for d in orders:
+        t = d * (d + 1) // 2
+        sub = A[r0:r0 + t, :]
+        k.append(int(np.count_nonzero(sub.getnnz(axis=0))))
+        r0 += t
+    assemble = sum(4.0 * kj * d ** 3 + 2.0 * kj * kj * d * (d + 1) / 2 for kj, d in zip(k, orders))
+    return {"n": n, "factor_flops": n ** 3 / 3.0, "trisolve_bytes": 8.0 * n * n,
+            "symv_bytes": 8.0 * n * n, "assemble_flops": assemble,
+            "scale_flops": sum(20.0 * d ** 3 for d in orders)}
+
+
+def traffic_from_profile(phase):
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        v = d.get(phase)
+        if isinstance(v, dict):
+            return v.get("bytes_per_launch")
+    return None
+
+
+def cpu_baseline(prob, gpu_iters):
+    """Oracle on a bounded sample: the first CPU_SAMPLE_ITERS iterations (plus the start)."""
+    from oracle import ipm
+    t0 = time.perf_counter()
+    r = ipm.Solver(prob, ipm.Settings(max_iter=CPU_SAMPLE_ITERS)).solve()
+    dt = time.perf_counter() - t0
+    per_iter = dt / max(r.iterations, 1)
+    return {"value": per_iter * gpu_iters, "unit": "s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"oracle (numpy + OpenBLAS) start + first {r.iterations} IPM iterations "
+                      f"took {dt:.2f} s; projected to the {gpu_iters} iterations the solve needs",
+            "seconds_per_iteration": per_iter}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    prob = make_problem()
+    gpu_iters = 15  # iterations to the gap of this instance (oracle and GPU agree, see tests)
+    for _ in range(args.warmup):
+        cpu_baseline(prob, gpu_iters)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(prob, gpu_iters))
+    wall = time.perf_counter() - t0
+    v = statistics.mean(x["value"] for x in vals)
+    cb = dict(vals[-1])
+    cb["value"] = v
+    line = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": WORKLOAD, "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    os.environ["SDPX_B200_DEVICE"] = str(local)
+    torch.cuda.set_device(local)
+    from sdpx_b200.solver import DefaultSettings, DefaultSolver
+
+    prob = make_problem()
+    settings = DefaultSettings(kkt_form="condensed")
+    solver = DefaultSolver(prob.P, prob.q, prob.A, prob.b, prob.cones, settings)
+    for _ in range(args.warmup):
+        solver.solve()
+    iters = solver.solution.iterations
+    status = solver.solution.status
+    solver.set_kernel_timing(True)
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    from sdpx_b200 import _lib
+    launches0 = _lib.load().sdpx_b200_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        solver.solve()
+    ev1.record()
+    torch.cuda.synchronize()
+    launches = _lib.load().sdpx_b200_launch_count() - launches0
+    wall = (time.perf_counter() - t0) / args.steps
+    barrier(world)
+    clk = clocks.stop()
+    dev_s = ev0.elapsed_time(ev1) / 1e3 / args.steps
+    value = max_over_ranks(world, dev_s)
+    ktimes = solver.kernel_times()
+    solver.set_kernel_timing(False)
+    gpu_launches = int(launches)
+
+    # ---- end-to-end through the C ABI with host buffers ----
+    e2e_times = []
+    h2d = d2h = 0
+    for i in range(args.warmup + args.steps):
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s2 = DefaultSolver(prob.P, prob.q, prob.A, prob.b, prob.cones, settings)
+        s2.solve()
+        del s2
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            e2e_times.append(time.perf_counter() - t0)
+    e2e = max_over_ranks(world, statistics.mean(e2e_times))
+    # bytes crossing per step: the uploaded problem (dense per-block columns of A, index maps,
+    # q, b) and the result vector
+    model = schur_model(prob)
+    nnz_dense = sum(d * (d + 1) // 2 for _, d in prob.cones)
+    A = prob.A.tocsc()
+    h2d = int(8 * A.nnz + 4 * 3 * A.nnz // max(nnz_dense, 1) + 8 * (prob.n + prob.m))
+    dense_cols = 0
+    r0 = 0
+    for _, d in prob.cones:
+        t = d * (d + 1) // 2
+        dense_cols += t * int(np.count_nonzero(A[r0:r0 + t, :].getnnz(axis=0)))
+        r0 += t
+    h2d = int(8 * dense_cols + 8 * (prob.n + prob.m) + 16 * prob.n * 4)
+    d2h = int(8 * (prob.n + 2 * prob.m + 6))
+
+    # ---- roofline of the dominant device phase ----
+    hbm, hbm_kind = measured_peaks()
+    dom = max(ktimes, key=lambda k: ktimes[k][0])
+    ms, cnt = ktimes[dom]
+    per = ms / 1e3 / max(cnt, 1)
+    fp64 = None
+    if dom in ("factor", "assemble", "scale", "cone", "step"):
+        fp64 = fp64_gemm_peak()
+        flops = {"factor": model["factor_flops"], "assemble": model["assemble_flops"],
+                 "scale": model["scale_flops"]}.get(dom)
+        if flops is None:
+            flops = sum(4.0 * d ** 3 for _, d in prob.cones)
+        achieved = flops / per / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
+                "frac": achieved / fp64, "traffic": traffic_from_profile(dom),
+                "kernel": dom, "launch_ms": per * 1e3,
+                "note": "FP64 pipe; peak = cuBLAS DGEMM 8192^3 measured in this run (FP64 is not "
+                        "in MEASURED_PEAKS.json)"}
+    else:
+        nbytes = model["trisolve_bytes"] if dom == "trisolve" else model["symv_bytes"]
+        achieved = nbytes / per / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": traffic_from_profile(dom), "kernel": dom,
+                "launch_ms": per * 1e3, "note": f"peak {hbm_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+    phases = {k: {"ms_total": v[0], "launches": v[1]} for k, v in ktimes.items()}
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cb = cpu_baseline(prob, iters)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": dict(WORKLOAD, parallelism=f"replicas{world}"),
+                "status": status, "iterations": iters, "wall_s_per_step": wall,
+                "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h},
+                "roofline": roof, "phases": phases, "gpu_launches": gpu_launches,
+                "clocks": clk, "cpu_baseline": cb}
+        print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            rc = run_reference(args, world, rank)
+        else:
+            rc = run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

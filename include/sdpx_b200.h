@@ -1,0 +1,182 @@
+/* sdpx_b200: B200 (sm_100a) implementation of the SDPX interior-point hot path.
+ *
+ * Two C-ABI levels, both exported by libsdpx_b200.so:
+ *
+ *  1. The solver ABI of the reference (yongjunx23-del/SDPX.rs, include/sdpx.h, ABI 4): the same
+ *     entry points, struct layouts, return codes and status codes, so a C caller of libsdpx
+ *     relinks against this library unchanged.  Each declaration cites the reference line it
+ *     replaces.  The hot path (NT scaling, Schur assembly, dense Cholesky, solves, refinement,
+ *     step lengths) runs on the GPU; setup (copying, Ruiz equilibration) runs on the host.
+ *
+ *  2. Kernel-level entry points (sdpxg_*) for a host that keeps its own interior-point driver
+ *     (the Rust solver's KKTSolver / DirectLDLSolver / Cone seams).  They take host pointers,
+ *     run one hot-path operation on the context's stream and return when it is complete.
+ *
+ * Conventions shared with the reference (include/sdpx.h:8-17): inputs are copied; indices are
+ * zero based, sorted and unique within each CSC column; P is upper triangular; PSD entries use
+ * the upper triangle in column order with off-diagonal entries scaled by sqrt(2).
+ * Return codes: 0 OK, 1 invalid input, 2 unsupported, 3 busy, 4 poisoned, 5 internal error
+ * (the reference's "panic": an exception caught at the boundary), 6 insufficient output
+ * capacity, 7 no solved result.  The last error message is thread-local.
+ *
+ * Supported subset: precision_bits 53 (binary64), PSD triangle cones of order <= 64,
+ * kkt_form 0 (auto) or 2 (condensed).  Other inputs return 2 (unsupported) with a message.
+ */
+#ifndef SDPX_B200_H
+#define SDPX_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SDPX_ABI_VERSION 4u
+#define SDPX_PREPROCESS_RUIZ 1u
+#define SDPX_PREPROCESS_PRESOLVE 2u
+#define SDPX_PREPROCESS_CHORDAL 4u
+#define SDPX_PREPROCESS_ALL 7u
+
+/* ---- solver ABI: layouts identical to the reference (include/sdpx.h:25-81) ---- */
+typedef struct sdpx_handle sdpx_handle;
+/* include/sdpx.h:26 -- kind 0 = f64 array, 1 = decimal strings */
+typedef struct {
+  uint32_t kind;
+  uint32_t reserved;
+  uint64_t count;
+  const double *f64;
+  const char *const *decimal;
+} sdpx_scalars;
+/* include/sdpx.h:27 */
+typedef struct {
+  uint64_t rows, cols, nnz;
+  const uint64_t *colptr, *rowval;
+  sdpx_scalars values;
+} sdpx_csc;
+/* include/sdpx.h:39 -- kind 3 = PSD triangle (dim = matrix order) */
+typedef struct {
+  uint32_t kind, reserved;
+  uint64_t dim;
+  sdpx_scalars alpha;
+} sdpx_cone;
+/* include/sdpx.h:47-50 */
+typedef struct {
+  uint64_t row_start, column_start, dim, basis_rows, basis_cols;
+  sdpx_scalars basis, weights;
+} sdpx_sampled_block;
+/* include/sdpx.h:51-66 (88 bytes on 64-bit) */
+typedef struct {
+  uint32_t abi_version, struct_size, precision_bits, max_iter;
+  uint32_t verbose, preprocessing_flags, max_threads, kkt_form;
+  uint32_t reserved_0;
+  double time_limit;
+  const char *tol_gap_abs, *tol_gap_rel, *tol_feas, *tol_infeas_abs, *tol_infeas_rel;
+} sdpx_settings;
+/* include/sdpx.h:67-75 (112 bytes on 64-bit) */
+typedef struct {
+  uint32_t abi_version, struct_size, status, iterations;
+  uint32_t working_bits, backend_threads, cone_threads, kkt_form;
+  uint32_t reserved_0;
+  uint64_t n, m;
+  double solve_time, objective, dual_objective, primal_residual, dual_residual, gap_abs, gap_rel;
+} sdpx_info;
+
+/* include/sdpx.h:84 (ffi/src/lib.rs:586-593) */
+int32_t sdpx_default_settings_v4(sdpx_settings *out);
+#define sdpx_default_settings sdpx_default_settings_v4
+/* include/sdpx.h:88 (ffi/src/lib.rs:720-723): always 1, one GPU per handle */
+int32_t sdpx_mpi_world_size(void);
+/* include/sdpx.h:89 (ffi/src/lib.rs:594-607) */
+int32_t sdpx_prepare(const sdpx_csc *P, const sdpx_scalars *q, const sdpx_csc *A,
+                     const sdpx_scalars *b, const sdpx_cone *cones, uint64_t cone_count,
+                     const sdpx_settings *settings, sdpx_handle **out);
+/* include/sdpx.h:92 (ffi/src/lib.rs:608-621): factor blocks are not supported here (2) */
+int32_t sdpx_prepare_sampled(const sdpx_csc *P, const sdpx_scalars *q, const sdpx_csc *A_linear,
+                             const sdpx_scalars *b, const sdpx_cone *cones, uint64_t cone_count,
+                             const sdpx_settings *settings, const sdpx_sampled_block *blocks,
+                             uint64_t block_count, sdpx_handle **out);
+/* include/sdpx.h:93 (ffi/src/lib.rs:660-663) */
+int32_t sdpx_solve(sdpx_handle *handle);
+/* include/sdpx.h:100 (ffi/src/lib.rs:664-670) */
+int32_t sdpx_update(sdpx_handle *handle, const sdpx_scalars *q, const sdpx_scalars *b);
+/* include/sdpx.h:101 (ffi/src/lib.rs:671-680) */
+int32_t sdpx_get_info(sdpx_handle *handle, sdpx_info *out);
+/* include/sdpx.h:106 (ffi/src/lib.rs:689-703) */
+int32_t sdpx_get_solver_name(sdpx_handle *handle, char *out, uint64_t capacity,
+                             uint64_t *required);
+/* include/sdpx.h:113 (ffi/src/lib.rs:722-735): x[n], z[m], s[m], 6 summary scalars */
+int32_t sdpx_result_f64(sdpx_handle *handle, double *out, uint64_t capacity, uint64_t *required);
+/* include/sdpx.h:114 (ffi/src/lib.rs:736-752) */
+int32_t sdpx_result_decimal(sdpx_handle *handle, char *out, uint64_t capacity,
+                            uint64_t *required);
+/* include/sdpx.h:117 (ffi/src/lib.rs:753-768) */
+uint64_t sdpx_last_error(char *out, uint64_t capacity);
+/* include/sdpx.h:118 (ffi/src/lib.rs:769-786) */
+int32_t sdpx_destroy(sdpx_handle *handle);
+
+/* ---- B200 extensions of the solver ABI ---- */
+/* Per-phase wall times (seconds) of the last solve, in the order scale, assemble, factor,
+ * kkt_solve, step, residual, other; and counters (factorizations, kkt solves, outer and inner
+ * refinement steps).  Counterpart of the reference's SDPX_PROFILE phase receipt
+ * (src/receipt.rs:104-160).  times needs 7 doubles, counts 4 uint64. */
+int32_t sdpx_b200_phase_times(sdpx_handle *handle, double *times, uint64_t *counts);
+/* Enable (on != 0) or disable CUDA-event timing of the device phases of later solves and reset
+ * the totals.  Events are recorded on the handle's stream around each phase: NT scaling,
+ * Schur assembly, factorisation, triangular solves, cone congruences, step lengths and the
+ * Schur matvec, in that order (no counterpart in the reference, which has no device). */
+int32_t sdpx_b200_set_kernel_timing(sdpx_handle *handle, int32_t on);
+/* Totals since the last reset: ms[7] milliseconds and counts[7] timed regions per phase. */
+int32_t sdpx_b200_kernel_times(sdpx_handle *handle, double *ms, uint64_t *counts);
+/* Number of CUDA kernels this library has launched in this process (all handles). */
+uint64_t sdpx_b200_launch_count(void);
+
+/* ---- kernel-level ABI (sdpxg_*): one hot-path operation per call ---- */
+typedef struct sdpxg_ctx sdpxg_ctx;
+/* Create a context on CUDA device `device` (flags must be 0). */
+int32_t sdpxg_ctx_create(int32_t device, uint32_t flags, sdpxg_ctx **out);
+int32_t sdpxg_ctx_destroy(sdpxg_ctx *ctx);
+/* Upload an already equilibrated problem: P (n x n upper CSC, may be NULL), A (m x n CSC) whose
+ * rows stack the svec rows of `block_count` PSD blocks of the given orders.  Replaces the data
+ * that CondensedKKTSolver::new reads (kkt/condensed/mod.rs:1279-1347). */
+int32_t sdpxg_problem_upload(sdpxg_ctx *ctx, const sdpx_csc *P, const sdpx_csc *A,
+                             const uint64_t *psd_orders, uint64_t block_count);
+/* NT scaling of every PSD block at (s, z) (m-length svec vectors).  Writes lambda (sum of
+ * orders) when out_lambda is not NULL.  *status: 0 ok, else SDPXG_ST bits.
+ * Replaces PSDTriangleCone::update_scaling (cones/psdtrianglecone.rs:311-439). */
+int32_t sdpxg_nt_scale(sdpxg_ctx *ctx, const double *s, const double *z, double *out_lambda,
+                       uint32_t *status);
+/* Identity scaling of every block (core/solver.rs:1212 reset_scaling). */
+int32_t sdpxg_identity_scaling(sdpxg_ctx *ctx);
+/* Assemble the condensed Schur complement P + A' Hs^-1 A of the current scaling.  Optional
+ * out_schur receives the dense n x n matrix (column-major).  Replaces
+ * CondensedKKTSolver::assemble (kkt/condensed/mod.rs:1962-2147). */
+int32_t sdpxg_schur_assemble(sdpxg_ctx *ctx, double *out_schur);
+/* Factor Schur + shift*I with the dynamic pivot rule (dynamic != 0: pivots <= eps become
+ * delta).  *status != 0 on a failed pivot.  Replaces DenseBlockSolver::refactor /
+ * factor_with_shift (kkt/ldl/dense_block.rs:95-365, kkt/direct/solver.rs:758-877). */
+int32_t sdpxg_factor(sdpxg_ctx *ctx, double shift, uint32_t dynamic, double eps, double delta,
+                     uint32_t *status);
+/* Solve the factored reduced system for ncols right-hand sides (n-length columns), refined
+ * against the unshifted Schur complement.  Replaces DirectLDLSolver::solve
+ * (kkt/ldl/dense_block.rs:795-850 with kkt/direct/solver.rs:1046-1125). */
+int32_t sdpxg_solve_many(sdpxg_ctx *ctx, const double *rhs, double *out, uint32_t ncols);
+/* Full condensed KKT solve [P A'; A -Hs][x; z] = [bx; bz] with the outer refinement on the
+ * original operator.  Replaces CondensedKKTSolver::solve (kkt/condensed/kkt.rs:275-318). */
+int32_t sdpxg_kkt_solve(sdpxg_ctx *ctx, const double *bx, const double *bz, double *x, double *z);
+/* e = b - [P A'; A -Hs][x; z]; returns ||e||_inf in *norm.  Replaces residual_inner
+ * (kkt/condensed/mod.rs:2631-2871). */
+int32_t sdpxg_residual(sdpxg_ctx *ctx, const double *bx, const double *bz, const double *x,
+                       const double *z, double *ex, double *ez, double *norm);
+/* Largest alpha <= amax keeping z + alpha dz and s + alpha ds in the PSD cones, from the current
+ * NT scaling; mode 1 only tests whether amax is admissible (out = amax or 0).  Replaces
+ * PSDTriangleCone::step_length (cones/psdtrianglecone.rs:475-576, 1168-1231). */
+int32_t sdpxg_step_length(sdpxg_ctx *ctx, const double *dz, const double *ds, double amax,
+                          uint32_t mode, double *out_alpha, uint32_t *status);
+/* y = op(x) per PSD block: op 0 W, 1 W', 2 W^-1, 3 W^-T, 4 Hs = W'W, 5 Hs^-1.
+ * Replaces mul_W / mul_Winv / PsdBlock::apply (cones/psdtrianglecone.rs:860-917,
+ * kkt/condensed/psd.rs:1968-2027). */
+int32_t sdpxg_cone_apply(sdpxg_ctx *ctx, uint32_t op, const double *x, double *y);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SDPX_B200_H */

@@ -1,0 +1,149 @@
+// Shared definitions for the sm_100a SDPX hot-path kernels.
+//
+// Layout conventions (all device buffers in HBM, float64):
+//  * PSD vectors use the reference's triangle convention: upper triangle, column order,
+//    off-diagonal entries scaled by sqrt(2); entry (i, j), i <= j, sits at j(j+1)/2 + i
+//    (include/sdpx.h:32-33 of the reference).
+//  * Per-block n x n matrices (R, Rinv, Ginv, ...) are column-major with leading dimension n,
+//    packed one after another at BlockDesc::mat_off.
+//  * The Schur complement and its factor are dense column-major m x m.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define SDPXG_NMAX 64               // largest PSD block order handled by the CTA kernels
+#define SDPXG_LD (SDPXG_NMAX + 1)   // shared-memory leading dimension (odd: fewer bank conflicts)
+#define SDPXG_THREADS 256
+#define SDPXG_RSQRT2 0.70710678118654752440
+#define SDPXG_SQRT2 1.41421356237309504880
+
+// Device status bits reported by the kernels (read back by the host after each phase).
+enum SdpxgStatus : uint32_t {
+  SDPXG_ST_OK = 0,
+  SDPXG_ST_CHOL_FAIL = 1u,        // Cholesky of s or z failed (not interior)
+  SDPXG_ST_SVD_UNCONVERGED = 2u,  // Jacobi sweeps hit their bound
+  SDPXG_ST_NONFINITE = 4u,        // a non-finite value was produced
+  SDPXG_ST_PIVOT_FAIL = 8u,       // clearly negative or non-finite Schur pivot
+  SDPXG_ST_EIG_FAIL = 16u,        // eigenvalue bisection did not converge
+};
+
+struct BlockDesc {
+  int n;         // block order
+  int svec_off;  // first row of the block in the stacked cone vector
+  int mat_off;   // offset of the block's n*n matrices
+  int vec_off;   // offset of the block's length-n vectors (lambda, Lambda^-1/2)
+};
+
+__device__ __forceinline__ int tri_idx(int i, int j) {  // i <= j
+  return j * (j + 1) / 2 + i;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// ------------------------------------------------------------------------------------
+// CTA-level helpers on n x n shared-memory matrices with leading dimension SDPXG_LD.
+// Callers place __syncthreads() between dependent calls.
+// ------------------------------------------------------------------------------------
+#define SM(A, i, j) (A)[(i) + (j) * SDPXG_LD]
+
+// M = smat(v): symmetric matrix from an svec.
+__device__ __forceinline__ void cta_load_smat(double* M, const double* __restrict__ v, int n) {
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    int i = e % n, j = e / n;
+    int a = min(i, j), b = max(i, j);
+    double x = v[tri_idx(a, b)];
+    SM(M, i, j) = (i == j) ? x : x * SDPXG_RSQRT2;
+  }
+}
+
+// v = svec(sym(M)): off-diagonal (M_ij + M_ji) / sqrt(2).
+__device__ __forceinline__ void cta_store_svec(double* __restrict__ v, const double* M, int n) {
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    int i = e % n, j = e / n;
+    if (i > j) continue;
+    v[tri_idx(i, j)] = (i == j) ? SM(M, i, j) : (SM(M, i, j) + SM(M, j, i)) * SDPXG_RSQRT2;
+  }
+}
+
+__device__ __forceinline__ void cta_load_mat(double* M, const double* __restrict__ g, int n) {
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) SM(M, e % n, e / n) = g[e];
+}
+
+__device__ __forceinline__ void cta_store_mat(double* __restrict__ g, const double* M, int n) {
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) g[e] = SM(M, e % n, e / n);
+}
+
+// C = op(A) * op(B); ta/tb select the transpose.  C must not alias A or B.
+__device__ __forceinline__ void cta_gemm(double* C, const double* A, bool ta, const double* B,
+                                         bool tb, int n) {
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    int i = e % n, j = e / n;
+    double acc = 0.0;
+    for (int k = 0; k < n; ++k) {
+      double a = ta ? SM(A, k, i) : SM(A, i, k);
+      double b = tb ? SM(B, j, k) : SM(B, k, j);
+      acc = fma(a, b, acc);
+    }
+    SM(C, i, j) = acc;
+  }
+}
+
+// In-place lower Cholesky A = L L' (lower triangle of A used).  The update is lagged so
+// one barrier per column suffices: the trailing matrix is updated with the unscaled
+// column divided by the pivot, and columns are scaled at the end.  Returns false (CTA
+// uniform) when a pivot is not positive and finite.  `piv` is n doubles of shared memory.
+__device__ inline bool cta_cholesky_lower(double* A, int n, double* piv) {
+  for (int k = 0; k < n; ++k) {
+    __syncthreads();
+    double d = SM(A, k, k);
+    if (!(d > 0.0) || !isfinite(d)) {
+      __syncthreads();
+      return false;
+    }
+    if (threadIdx.x == 0) piv[k] = d;
+    int rem = n - k - 1;
+    double dinv = 1.0 / d;
+    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
+      int i = k + 1 + e % rem, j = k + 1 + e / rem;
+      if (i < j) continue;
+      SM(A, i, j) -= SM(A, i, k) * SM(A, j, k) * dinv;
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    int i = e % n, j = e / n;
+    double r = sqrt(piv[j]);
+    if (i > j) SM(A, i, j) /= r;
+    else if (i == j) SM(A, i, j) = r;
+    else SM(A, i, j) = 0.0;
+  }
+  __syncthreads();
+  return true;
+}
+
+// Solve L' X = B in place of B (L lower, n x n), one column per thread.
+__device__ __forceinline__ void cta_trsm_lower_t(const double* L, double* B, int n) {
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    for (int i = n - 1; i >= 0; --i) {
+      double acc = SM(B, i, j);
+      for (int k = i + 1; k < n; ++k) acc = fma(-SM(L, k, i), SM(B, k, j), acc);
+      SM(B, i, j) = acc / SM(L, i, i);
+    }
+  }
+}

@@ -1,0 +1,149 @@
+// Host-side helpers: device buffers, kernel launch wrappers and the batched scalar reducer.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace sdpxg {
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+
+inline void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t count) { alloc(count); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void upload(const T* h, size_t count, cudaStream_t st) {
+    if (count) check(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, st), "H2D");
+  }
+  void upload(const std::vector<T>& h, cudaStream_t st) {
+    if (h.size() > n) alloc(h.size());
+    upload(h.data(), h.size(), st);
+  }
+  operator T*() const { return p; }
+};
+
+// Kernel declarations (defined in the *_kernels.cu translation units of this library).
+extern "C" {
+__global__ void k_nt_scale(const BlockDesc*, const double*, const double*, double*, double*,
+                           double*, double*, double*, uint32_t*);
+__global__ void k_identity_scaling(const BlockDesc*, double*, double*, double*, double*, double*);
+__global__ void k_congruence(const BlockDesc*, int, const double*, const double*, const double*,
+                             double*, long);
+__global__ void k_circ_op(const BlockDesc*, const double*, const double*, double*);
+__global__ void k_lam_inv_circ(const BlockDesc*, const double*, const double*, double*);
+__global__ void k_affine_ds(const BlockDesc*, const double*, double*);
+__global__ void k_shift_unit(const BlockDesc*, double*, double);
+__global__ void k_step_length(const BlockDesc*, const double*, const double*, const double*,
+                              const double*, const double*, double, int, double*, uint32_t*);
+__global__ void k_margins(const BlockDesc*, const double*, long, double*, uint32_t*);
+__global__ void k_schur_transform(const BlockDesc*, const int*, const int*, const long*,
+                                  const double*, const double*, double*);
+__global__ void k_schur_block_gemm(const BlockDesc*, const int*, const int*, const long*,
+                                   const long*, const double*, const double*, double*);
+__global__ void k_schur_gather(int, const int*, const int*, const int*, const int*, const long*,
+                               const double*, double*);
+__global__ void k_add_upper_csc(int, const int*, const int*, const double*, double*);
+__global__ void k_op_forward(const BlockDesc*, const int*, const int*, const int*, const long*,
+                             const double*, const double*, long, double, double, double*, long);
+__global__ void k_op_adjoint_partial(const BlockDesc*, const int*, const int*, const int*,
+                                     const long*, const double*, const double*, long, double*,
+                                     long, int);
+__global__ void k_op_adjoint_gather(int, const int*, const int*, const int*, const int*,
+                                    const double*, long, double, double, double*, long);
+__global__ void k_potrf_diag(double*, int, int, double, double, int, const double*, double*,
+                             uint32_t*);
+__global__ void k_trsm_panel(double*, int, int, const double*);
+__global__ void k_syrk_update(double*, int, int);
+__global__ void k_trsv_fwd(const double*, int, int, const double*, double*, double*, long, int);
+__global__ void k_trsv_bwd(const double*, int, int, const double*, double*, double*, long, int);
+__global__ void k_shifted_copy(const double*, double*, int, double, double*);
+__global__ void k_symv_partial(const double*, int, const double*, long, double*, long);
+__global__ void k_symv_finish(int, const double*, long, const double*, long, double*, long);
+__global__ void k_lincomb(long, double, const double*, double, const double*, double,
+                          const double*, double*);
+__global__ void k_reduce_partial(int, long, const double*, const double*, double*);
+__global__ void k_reduce_final(int, int, const double*, double*);
+__global__ void k_diag_absmax(const double*, int, double*);
+__global__ void k_csr_spmv(int, const int*, const int*, const double*, const double*, double,
+                           double, double*);
+}
+
+// Kernel launches issued by this library in this process (every launch site increments it).
+inline uint64_t g_launches = 0;
+
+enum RedOp { RED_DOT = 0, RED_SUMSQ = 1, RED_MAXABS = 2, RED_FINITE = 3 };
+
+// Queues reductions into device scalar slots; fetch() copies them back in one transfer.
+class Reducer {
+ public:
+  static constexpr int kBlocks = 148;
+  static constexpr int kSlots = 64;
+  void init() {
+    partial_.alloc((size_t)kBlocks * kSlots);
+    slots_.alloc(kSlots);
+    host_.resize(kSlots);
+  }
+  int add(cudaStream_t st, int op, long n, const double* x, const double* y) {
+    if (count_ >= kSlots) throw CudaError("reducer slots exhausted");
+    if (n > 0 && !x) throw std::invalid_argument("null device buffer: reduction input");
+    int s = count_++;
+    if (n > 0) {
+      ++g_launches, k_reduce_partial<<<kBlocks, 256, 0, st>>>(op, n, x, y, partial_.p + (size_t)s * kBlocks);
+      ++g_launches, k_reduce_final<<<1, 32, 0, st>>>(op, kBlocks, partial_.p + (size_t)s * kBlocks, slots_.p + s);
+    } else {
+      double id = (op == RED_FINITE) ? 1.0 : 0.0;
+      check(cudaMemcpyAsync(slots_.p + s, &id_[op], sizeof(double), cudaMemcpyHostToDevice, st),
+            "reducer identity");
+      (void)id;
+    }
+    return s;
+  }
+  const std::vector<double>& fetch(cudaStream_t st) {
+    if (count_) {
+      check(cudaMemcpyAsync(host_.data(), slots_.p, count_ * sizeof(double),
+                            cudaMemcpyDeviceToHost, st), "reducer D2H");
+    }
+    check(cudaStreamSynchronize(st), "reducer sync");
+    count_ = 0;
+    return host_;
+  }
+
+ private:
+  DevBuf<double> partial_, slots_;
+  std::vector<double> host_;
+  int count_ = 0;
+  const double id_[4] = {0.0, 0.0, 0.0, 1.0};
+};
+
+}  // namespace sdpxg

@@ -1,0 +1,197 @@
+// CTA-level dense eigen / singular-value routines for PSD blocks of order <= SDPXG_NMAX.
+//
+//  * cta_jacobi_svd: one-sided (Hestenes) Jacobi with the parallel round-robin ordering.
+//    It orthogonalises the columns of M in place and accumulates the right singular
+//    vectors V.  Relative accuracy of the small singular values is what the NT scaling
+//    needs (the reference takes the SVD of L2'L1 directly instead of an eigensolve of the
+//    squared matrix, cones/psdtrianglecone.rs:378-386).
+//  * cta_tridiagonalize: Householder reduction of a symmetric matrix to tridiagonal form.
+//  * sturm_count / bisect_kth: eigenvalues of the tridiagonal by Sturm-sequence bisection
+//    (the same method the reference uses for its binary64 lambda_min bound,
+//    cones/psdtrianglecone.rs:1250-1290), every loop bounded.
+#pragma once
+#include "common.cuh"
+
+#define SDPXG_JACOBI_MAX_SWEEPS 60
+#define SDPXG_JACOBI_TOL 1e-15
+#define SDPXG_BISECT_MAX 256
+
+// Returns the number of sweeps used, or -1 when the sweep bound was hit.
+// `flag` is one int of shared memory.
+__device__ inline int cta_jacobi_svd(double* M, double* V, int n, int* flag) {
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    int i = e % n, j = e / n;
+    SM(V, i, j) = (i == j) ? 1.0 : 0.0;
+  }
+  const int N = n + (n & 1);
+  const int nwarps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (n < 2) {
+    __syncthreads();
+    return 0;
+  }
+  for (int sweep = 0; sweep < SDPXG_JACOBI_MAX_SWEEPS; ++sweep) {
+    if (threadIdx.x == 0) *flag = 0;
+    __syncthreads();
+    for (int r = 0; r < N - 1; ++r) {
+      for (int pi = warp; pi < N / 2; pi += nwarps) {
+        int p, q;
+        if (pi == 0) {
+          p = N - 1;
+          q = r;
+        } else {
+          p = (r + pi) % (N - 1);
+          q = (r - pi + N - 1) % (N - 1);
+        }
+        if (p >= n || q >= n) continue;
+        double a = 0.0, b = 0.0, g = 0.0;
+        for (int k = lane; k < n; k += 32) {
+          double x = SM(M, k, p), y = SM(M, k, q);
+          a = fma(x, x, a);
+          b = fma(y, y, b);
+          g = fma(x, y, g);
+        }
+        a = warp_sum(a);
+        b = warp_sum(b);
+        g = warp_sum(g);
+        if (fabs(g) > SDPXG_JACOBI_TOL * sqrt(a * b)) {
+          double zeta = (b - a) / (2.0 * g);
+          double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
+          double c = rsqrt(fma(t, t, 1.0));
+          double s = c * t;
+          for (int k = lane; k < n; k += 32) {
+            double x = SM(M, k, p), y = SM(M, k, q);
+            SM(M, k, p) = c * x - s * y;
+            SM(M, k, q) = s * x + c * y;
+            x = SM(V, k, p);
+            y = SM(V, k, q);
+            SM(V, k, p) = c * x - s * y;
+            SM(V, k, q) = s * x + c * y;
+          }
+          if (lane == 0) *flag = 1;
+        }
+      }
+      __syncthreads();
+    }
+    int more = *flag;
+    __syncthreads();
+    if (!more) return sweep + 1;
+  }
+  return -1;
+}
+
+// Householder tridiagonalisation of the symmetric A (destroyed).  d[0..n), e[0..n-1).
+// `work` is 2*n doubles of shared memory, `red` 32 doubles.
+__device__ inline void cta_tridiagonalize(double* A, int n, double* d, double* e, double* work,
+                                   double* red) {
+  double* v = work;
+  double* p = work + n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int k = 0; k + 2 < n; ++k) {
+    const int m = n - k - 1;  // length of the column below the diagonal
+    // ||x||^2 of x = A[k+1:n, k]
+    double part = 0.0;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+      double x = SM(A, k + 1 + i, k);
+      part = fma(x, x, part);
+    }
+    part = warp_sum(part);
+    if (lane == 0) red[warp] = part;
+    __syncthreads();
+    double nrm2 = 0.0;
+    for (int w = 0; w < nwarps; ++w) nrm2 += red[w];
+    double x0 = SM(A, k + 1, k);
+    double alpha = -copysign(sqrt(nrm2), x0);
+    double vnorm2 = nrm2 - x0 * x0 + (x0 - alpha) * (x0 - alpha);
+    if (threadIdx.x == 0) {
+      d[k] = SM(A, k, k);
+      e[k] = (nrm2 == 0.0) ? 0.0 : alpha;
+    }
+    __syncthreads();
+    if (nrm2 == 0.0 || vnorm2 == 0.0) continue;  // column already reduced (uniform)
+    double vs = rsqrt(vnorm2);
+    for (int i = threadIdx.x; i < m; i += blockDim.x)
+      v[i] = (i == 0 ? (x0 - alpha) : SM(A, k + 1 + i, k)) * vs;
+    __syncthreads();
+    // p = A_sub v
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+      double acc = 0.0;
+      for (int j = 0; j < m; ++j) acc = fma(SM(A, k + 1 + i, k + 1 + j), v[j], acc);
+      p[i] = acc;
+    }
+    __syncthreads();
+    part = 0.0;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) part = fma(v[i], p[i], part);
+    part = warp_sum(part);
+    if (lane == 0) red[warp] = part;
+    __syncthreads();
+    double K = 0.0;
+    for (int w = 0; w < nwarps; ++w) K += red[w];
+    __syncthreads();
+    for (int i = threadIdx.x; i < m; i += blockDim.x) p[i] = p[i] - K * v[i];  // q
+    __syncthreads();
+    for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+      int i = t % m, j = t / m;
+      SM(A, k + 1 + i, k + 1 + j) -= 2.0 * (v[i] * p[j] + p[i] * v[j]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (n >= 2) {
+      d[n - 2] = SM(A, n - 2, n - 2);
+      d[n - 1] = SM(A, n - 1, n - 1);
+      e[n - 2] = SM(A, n - 1, n - 2);
+    } else if (n == 1) {
+      d[0] = SM(A, 0, 0);
+    }
+  }
+  __syncthreads();
+}
+
+// Number of eigenvalues of the tridiagonal (d, e) strictly below x.
+__device__ __forceinline__ int sturm_count(const double* d, const double* e, int n, double x,
+                                           double pivmin) {
+  int cnt = 0;
+  double q = d[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  cnt += (q < 0.0);
+  for (int i = 1; i < n; ++i) {
+    q = (d[i] - x) - e[i - 1] * e[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    cnt += (q < 0.0);
+  }
+  return cnt;
+}
+
+__device__ __forceinline__ void gershgorin(const double* d, const double* e, int n, double* lo,
+                                           double* hi, double* pivmin) {
+  double l = 1e300, h = -1e300, emax = 0.0;
+  for (int i = 0; i < n; ++i) {
+    double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < n ? fabs(e[i]) : 0.0);
+    l = fmin(l, d[i] - r);
+    h = fmax(h, d[i] + r);
+    if (i + 1 < n) emax = fmax(emax, e[i] * e[i]);
+  }
+  double span = fmax(fabs(l), fabs(h));
+  *lo = l - 2.0 * 2.220446049250313e-16 * span - 1e-300;
+  *hi = h + 2.0 * 2.220446049250313e-16 * span + 1e-300;
+  *pivmin = 2.2250738585072014e-308 * fmax(1.0, emax);
+}
+
+// k-th smallest eigenvalue (k = 0 is the minimum) by bisection; one thread.
+// Sets *ok = false when the bound on steps was hit before convergence.
+__device__ inline double bisect_kth(const double* d, const double* e, int n, int k, bool* ok) {
+  double lo, hi, pivmin;
+  gershgorin(d, e, n, &lo, &hi, &pivmin);
+  for (int it = 0; it < SDPXG_BISECT_MAX; ++it) {
+    double mid = 0.5 * (lo + hi);
+    if (!(mid > lo && mid < hi) ||
+        hi - lo <= 2.0 * 2.220446049250313e-16 * fmax(fabs(lo), fabs(hi)) + pivmin) {
+      *ok = true;
+      return mid;
+    }
+    if (sturm_count(d, e, n, mid, pivmin) > k) hi = mid;
+    else lo = mid;
+  }
+  *ok = false;
+  return 0.5 * (lo + hi);
+}

@@ -1,0 +1,518 @@
+// Device engine: problem upload and the per-iteration hot-path operations on one GPU.
+//
+// Everything an iteration touches stays resident in HBM; the host receives scalars only
+// (reductions, status words, per-block step bounds).  The operations map onto the
+// reference's KKTSolver / DirectLDLSolver / Cone seams:
+//   nt_scale          Cone::update_scaling            (cones/psdtrianglecone.rs:311)
+//   assemble          CondensedKKTSolver::assemble    (kkt/condensed/mod.rs:1962)
+//   factor            DirectLDLKKTSolver::factor_with_shift + DenseBlockSolver
+//                     (kkt/direct/solver.rs:758, kkt/ldl/dense_block.rs:95)
+//   trisolve / symv   DenseBlockSolver::solve / residual (dense_block.rs:604-719)
+//   apply_cone        PsdBlock::apply and the W products (kkt/condensed/psd.rs:1968)
+//   step_bounds       Cone::step_length (cones/psdtrianglecone.rs:475)
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "device.cuh"
+
+namespace sdpxg {
+
+constexpr int kMatD = SDPXG_LD * SDPXG_NMAX;
+constexpr size_t kSmemNt = (5 * kMatD + 3 * SDPXG_NMAX) * sizeof(double) + (SDPXG_NMAX + 1) * sizeof(int);
+constexpr size_t kSmemCong = 4 * kMatD * sizeof(double);
+constexpr size_t kSmemCirc = 2 * kMatD * sizeof(double);
+constexpr size_t kSmemStep = (4 * kMatD + 5 * SDPXG_NMAX + 32) * sizeof(double);
+constexpr size_t kSmemMarg = (kMatD + 5 * SDPXG_NMAX + 32) * sizeof(double);
+constexpr size_t kSmemTrans = 3 * kMatD * sizeof(double);
+constexpr size_t kSmemTrsm = 2 * 64 * 65 * sizeof(double);
+constexpr size_t kSmemSyrk = 2 * 64 * 66 * sizeof(double);
+constexpr int kNB = 64;
+
+// Equilibrated problem in host memory (CSC, int64 indices as in the reference ABI).
+struct HostProblem {
+  int n = 0, m = 0;
+  std::vector<int64_t> Pcolptr, Prow;
+  std::vector<double> Pval;
+  std::vector<int64_t> Acolptr, Arow;
+  std::vector<double> Aval;
+  std::vector<double> q, b;
+  std::vector<int> psd;  // PSD block orders in cone order
+};
+
+// Cone operator modes of k_congruence.
+enum ConeMode { CM_W = 0, CM_WT = 1, CM_WINV = 2, CM_WINVT = 3, CM_HS = 4, CM_HINV = 5 };
+
+// Every wrapper checks its device pointers on the host before launching: a missing buffer is
+// reported as an error instead of reaching a kernel.
+inline void need(const void* p, const char* what) {
+  if (!p) throw std::invalid_argument(std::string("null device buffer: ") + what);
+}
+
+// Kernel-phase timers: CUDA events recorded on the engine's stream around each phase.
+enum KernelPhase { KT_SCALE = 0, KT_ASSEMBLE, KT_FACTOR, KT_TRISOLVE, KT_CONE, KT_STEP, KT_SYMV, KT_N };
+
+class Engine {
+ public:
+  cudaStream_t st = nullptr;
+  bool timing = false;
+  double kt_ms[KT_N] = {0};
+  uint64_t kt_count[KT_N] = {0};
+  void reset_timers() {
+    for (int k = 0; k < KT_N; ++k) { kt_ms[k] = 0; kt_count[k] = 0; }
+  }
+  int n = 0, m = 0, nblk = 0;
+  int nchol = 0;  // Schur tiles per side
+  std::vector<BlockDesc> hblocks;
+  std::vector<int> hk;  // columns per block
+  Reducer red;
+
+  Engine() = default;
+  ~Engine() {
+    for (auto& e : ev_) if (e) cudaEventDestroy(e);
+    if (st) cudaStreamDestroy(st);
+  }
+  void tbegin(int k) {
+    if (timing) check(cudaEventRecord(ev_[2 * k], st), "event");
+  }
+  void tend(int k) {
+    if (!timing) return;
+    check(cudaEventRecord(ev_[2 * k + 1], st), "event");
+    check(cudaEventSynchronize(ev_[2 * k + 1]), "event sync");
+    float ms = 0.f;
+    check(cudaEventElapsedTime(&ms, ev_[2 * k], ev_[2 * k + 1]), "event time");
+    kt_ms[k] += ms;
+    kt_count[k]++;
+  }
+
+  void init(int device) {
+    check(cudaSetDevice(device), "cudaSetDevice");
+    check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+    set_smem(reinterpret_cast<const void*>(k_nt_scale), kSmemNt);
+    set_smem(reinterpret_cast<const void*>(k_congruence), kSmemCong);
+    set_smem(reinterpret_cast<const void*>(k_circ_op), kSmemCirc);
+    set_smem(reinterpret_cast<const void*>(k_step_length), kSmemStep);
+    set_smem(reinterpret_cast<const void*>(k_margins), kSmemMarg);
+    set_smem(reinterpret_cast<const void*>(k_schur_transform), kSmemTrans);
+    set_smem(reinterpret_cast<const void*>(k_trsm_panel), kSmemTrsm);
+    set_smem(reinterpret_cast<const void*>(k_syrk_update), kSmemSyrk);
+    red.init();
+    status_.alloc(1);
+    for (auto& e : ev_) check(cudaEventCreate(&e), "event create");
+  }
+
+  void upload(const HostProblem& p) {
+    n = p.n;
+    m = p.m;
+    nblk = (int)p.psd.size();
+    hblocks.clear();
+    int row = 0, mat = 0, vec = 0;
+    for (int d : p.psd) {
+      if (d > SDPXG_NMAX) throw std::invalid_argument("PSD block order above 64 is not supported");
+      hblocks.push_back({d, row, mat, vec});
+      row += d * (d + 1) / 2;
+      mat += d * d;
+      vec += d;
+    }
+    if (row != m) throw std::invalid_argument("cone rows do not match A");
+    matlen_ = mat;
+    veclen_ = vec;
+    // per-block dense column storage of A
+    hk.assign(nblk, 0);
+    std::vector<std::vector<int>> bcols(nblk);
+    std::vector<std::vector<std::pair<int, int>>> c2b(n);  // (block, local)
+    for (int c = 0; c < n; ++c) {
+      int64_t p0 = p.Acolptr[c], p1 = p.Acolptr[c + 1];
+      int64_t q0 = p0;
+      for (int j = 0; j < nblk && q0 < p1; ++j) {
+        int r0 = hblocks[j].svec_off, r1 = r0 + hblocks[j].n * (hblocks[j].n + 1) / 2;
+        while (q0 < p1 && p.Arow[q0] < r0) ++q0;
+        int64_t q1 = q0;
+        while (q1 < p1 && p.Arow[q1] < r1) ++q1;
+        if (q1 > q0) {
+          c2b[c].push_back({j, hk[j]});
+          bcols[j].push_back(c);
+          hk[j]++;
+        }
+        q0 = q1;
+      }
+    }
+    std::vector<long> acol_off(nblk), s_off(nblk);
+    std::vector<int> col_ptr(nblk + 1, 0), col_idx;
+    long aoff = 0, soff = 0;
+    for (int j = 0; j < nblk; ++j) {
+      int tn = hblocks[j].n * (hblocks[j].n + 1) / 2;
+      acol_off[j] = aoff;
+      aoff += (long)tn * hk[j];
+      s_off[j] = soff;
+      soff += (long)hk[j] * hk[j];
+      col_ptr[j + 1] = col_ptr[j] + hk[j];
+      col_idx.insert(col_idx.end(), bcols[j].begin(), bcols[j].end());
+    }
+    std::vector<double> acol(aoff, 0.0);
+    for (int j = 0; j < nblk; ++j) {
+      int r0 = hblocks[j].svec_off, tn = hblocks[j].n * (hblocks[j].n + 1) / 2;
+      for (int t = 0; t < hk[j]; ++t) {
+        int c = bcols[j][t];
+        for (int64_t q = p.Acolptr[c]; q < p.Acolptr[c + 1]; ++q) {
+          int64_t r = p.Arow[q];
+          if (r >= r0 && r < r0 + tn) acol[acol_off[j] + (long)t * tn + (r - r0)] = p.Aval[q];
+        }
+      }
+    }
+    std::vector<int> c2b_ptr(n + 1, 0), c2b_blk, c2b_loc;
+    for (int c = 0; c < n; ++c) {
+      for (auto& e : c2b[c]) {
+        c2b_blk.push_back(e.first);
+        c2b_loc.push_back(e.second);
+      }
+      c2b_ptr[c + 1] = (int)c2b_blk.size();
+    }
+    std::vector<int> wblk, wloc, tiles;
+    for (int j = 0; j < nblk; ++j) {
+      for (int t = 0; t < hk[j]; ++t) {
+        wblk.push_back(j);
+        wloc.push_back(t);
+      }
+      int nt = (hk[j] + 31) / 32;
+      for (int tj = 0; tj < nt; ++tj)
+        for (int ti = 0; ti < nt; ++ti) {
+          tiles.push_back(j);
+          tiles.push_back(ti);
+          tiles.push_back(tj);
+        }
+    }
+    nwork_ = (int)wblk.size();
+    ntiles_ = (int)tiles.size() / 3;
+    // symmetric P in CSR (both triangles) for the x-row products
+    std::vector<std::vector<std::pair<int, double>>> prow(n);
+    for (int c = 0; c < n; ++c)
+      for (int64_t q = p.Pcolptr[c]; q < p.Pcolptr[c + 1]; ++q) {
+        int r = (int)p.Prow[q];
+        if (r > c) continue;
+        prow[r].push_back({c, p.Pval[q]});
+        if (r != c) prow[c].push_back({r, p.Pval[q]});
+      }
+    std::vector<int> prp(n + 1, 0), pci;
+    std::vector<double> pv;
+    for (int r = 0; r < n; ++r) {
+      std::sort(prow[r].begin(), prow[r].end());
+      for (auto& e : prow[r]) {
+        pci.push_back(e.first);
+        pv.push_back(e.second);
+      }
+      prp[r + 1] = (int)pci.size();
+    }
+    p_nnz_ = (int)pci.size();
+    std::vector<int> pup_ptr(n + 1, 0), pup_row;
+    std::vector<double> pup_val;
+    for (int c = 0; c < n; ++c) {
+      for (int64_t q = p.Pcolptr[c]; q < p.Pcolptr[c + 1]; ++q)
+        if (p.Prow[q] <= c) {
+          pup_row.push_back((int)p.Prow[q]);
+          pup_val.push_back(p.Pval[q]);
+        }
+      pup_ptr[c + 1] = (int)pup_row.size();
+    }
+
+    blocks_.alloc(nblk);
+    blocks_.upload(hblocks.data(), nblk, st);
+    R_.alloc(matlen_); Rinv_.alloc(matlen_); Ginv_.alloc(matlen_);
+    lam_.alloc(veclen_); lisqrt_.alloc(veclen_);
+    acol_.alloc(aoff); acol_.upload(acol.data(), aoff, st);
+    tcol_.alloc(aoff);
+    S_.alloc(std::max<long>(soff, 1));
+    acol_off_.alloc(nblk); acol_off_.upload(acol_off.data(), nblk, st);
+    s_off_.alloc(nblk); s_off_.upload(s_off.data(), nblk, st);
+    kcount_.alloc(nblk); kcount_.upload(hk.data(), nblk, st);
+    col_ptr_.alloc(nblk + 1); col_ptr_.upload(col_ptr.data(), nblk + 1, st);
+    col_idx_.alloc(std::max<size_t>(col_idx.size(), 1)); col_idx_.upload(col_idx.data(), col_idx.size(), st);
+    c2b_ptr_.alloc(n + 1); c2b_ptr_.upload(c2b_ptr.data(), n + 1, st);
+    c2b_blk_.alloc(std::max<size_t>(c2b_blk.size(), 1)); c2b_blk_.upload(c2b_blk.data(), c2b_blk.size(), st);
+    c2b_loc_.alloc(std::max<size_t>(c2b_loc.size(), 1)); c2b_loc_.upload(c2b_loc.data(), c2b_loc.size(), st);
+    wblk_.alloc(std::max(nwork_, 1)); wblk_.upload(wblk.data(), wblk.size(), st);
+    wloc_.alloc(std::max(nwork_, 1)); wloc_.upload(wloc.data(), wloc.size(), st);
+    tiles_.alloc(std::max<size_t>(tiles.size(), 1)); tiles_.upload(tiles.data(), tiles.size(), st);
+    prp_.alloc(n + 1); prp_.upload(prp.data(), n + 1, st);
+    pci_.alloc(std::max(p_nnz_, 1)); pci_.upload(pci.data(), pci.size(), st);
+    pv_.alloc(std::max(p_nnz_, 1)); pv_.upload(pv.data(), pv.size(), st);
+    pup_ptr_.alloc(n + 1); pup_ptr_.upload(pup_ptr.data(), n + 1, st);
+    pup_row_.alloc(std::max<size_t>(pup_row.size(), 1)); pup_row_.upload(pup_row.data(), pup_row.size(), st);
+    pup_val_.alloc(std::max<size_t>(pup_val.size(), 1)); pup_val_.upload(pup_val.data(), pup_val.size(), st);
+    pup_nnz_ = (int)pup_row.size();
+    adj_part_.alloc(std::max<size_t>((size_t)nwork_ * 2, 1));
+    nchol = (n + kNB - 1) / kNB;
+    Hsave_.alloc((size_t)n * n);
+    F_.alloc((size_t)n * n);
+    Dinv_.alloc((size_t)std::max(nchol, 1) * kNB * kNB);
+    diag0_.alloc(std::max(n, 1));
+    symv_part_.alloc((size_t)16 * std::max(n, 1));
+    tri_b_.alloc(std::max(n, 1));
+    tri_y_.alloc(std::max(n, 1));
+    step_out_.alloc(2 * std::max(nblk, 1));
+    marg_out_.alloc(2 * std::max(nblk, 1));
+    scal_.alloc(4);
+    check(cudaStreamSynchronize(st), "upload sync");
+  }
+
+  // ---- status word ----
+  void clear_status() { check(cudaMemsetAsync(status_.p, 0, sizeof(uint32_t), st), "memset"); }
+  uint32_t read_status() {
+    uint32_t s = 0;
+    check(cudaMemcpyAsync(&s, status_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "status");
+    check(cudaStreamSynchronize(st), "status sync");
+    return s;
+  }
+
+  // ---- cone scaling ----
+  void identity_scaling() {
+    if (nblk) ++g_launches, k_identity_scaling<<<nblk, 256, 0, st>>>(blocks_, R_, Rinv_, Ginv_, lam_, lisqrt_);
+  }
+  bool nt_scale(const double* s, const double* z) {
+    need(s, "nt_scale s");
+    need(z, "nt_scale z");
+    clear_status();
+    tbegin(KT_SCALE);
+    if (nblk)
+      ++g_launches, k_nt_scale<<<nblk, SDPXG_THREADS, kSmemNt, st>>>(blocks_, s, z, R_, Rinv_, Ginv_, lam_,
+                                                      lisqrt_, status_);
+    launched("k_nt_scale");
+    tend(KT_SCALE);
+    return read_status() == 0;
+  }
+
+  // y = op(x) for cone operator `mode`, ncols columns with stride ld.
+  void cone_apply(int mode, const double* x, double* y, int ncols = 1, long ld = 0) {
+    need(x, "cone_apply x");
+    need(y, "cone_apply y");
+    if (!nblk) return;
+    tbegin(KT_CONE);
+    ++g_launches, k_congruence<<<dim3(nblk, ncols), SDPXG_THREADS, kSmemCong, st>>>(blocks_, mode, R_, Rinv_, x,
+                                                                      y, ld ? ld : m);
+    launched("k_congruence");
+    tend(KT_CONE);
+  }
+  void circ_op(const double* y, const double* z, double* x) {
+    need(y, "circ y");
+    need(z, "circ z");
+    need(x, "circ x");
+    if (nblk) ++g_launches, k_circ_op<<<nblk, SDPXG_THREADS, kSmemCirc, st>>>(blocks_, y, z, x);
+    launched("k_circ_op");
+  }
+  void lam_inv_circ(const double* z, double* x) {
+    need(z, "lam_inv z");
+    need(x, "lam_inv x");
+    if (nblk) ++g_launches, k_lam_inv_circ<<<nblk, 256, 0, st>>>(blocks_, lam_, z, x);
+  }
+  void affine_ds(double* ds) {
+    need(ds, "affine_ds");
+    if (nblk) ++g_launches, k_affine_ds<<<nblk, 256, 0, st>>>(blocks_, lam_, ds);
+  }
+  void shift_unit(double* v, double a) {
+    need(v, "shift_unit");
+    if (nblk) ++g_launches, k_shift_unit<<<nblk, 64, 0, st>>>(blocks_, v, a);
+  }
+  // per-block (dual, primal) bounds; returns false on an eigen failure
+  bool step_bounds(const double* dz, const double* ds, double amax, int mode, double* az,
+                   double* as) {
+    need(dz, "step dz");
+    need(ds, "step ds");
+    *az = amax;
+    *as = amax;
+    if (!nblk) return true;
+    clear_status();
+    tbegin(KT_STEP);
+    ++g_launches, k_step_length<<<dim3(nblk, 2), SDPXG_THREADS, kSmemStep, st>>>(blocks_, R_, Rinv_, lisqrt_, dz,
+                                                                   ds, amax, mode, step_out_,
+                                                                   status_);
+    launched("k_step_length");
+    tend(KT_STEP);
+    std::vector<double> h(2 * nblk);
+    check(cudaMemcpyAsync(h.data(), step_out_.p, 2 * nblk * sizeof(double),
+                          cudaMemcpyDeviceToHost, st), "step D2H");
+    uint32_t s = read_status();
+    for (int j = 0; j < nblk; ++j) {
+      *az = std::min(*az, h[2 * j]);
+      *as = std::min(*as, h[2 * j + 1]);
+    }
+    return s == 0;
+  }
+  // (lambda_min, sum of positive eigenvalues) per block of v
+  bool margins(const double* v, std::vector<double>& out) {
+    need(v, "margins v");
+    out.assign(2 * nblk, 0.0);
+    if (!nblk) return true;
+    clear_status();
+    ++g_launches, k_margins<<<dim3(nblk, 1), SDPXG_THREADS, kSmemMarg, st>>>(blocks_, v, m, marg_out_, status_);
+    launched("k_margins");
+    check(cudaMemcpyAsync(out.data(), marg_out_.p, 2 * nblk * sizeof(double),
+                          cudaMemcpyDeviceToHost, st), "margins D2H");
+    return read_status() == 0;
+  }
+
+  // ---- constraint operator ----
+  // y = alpha * A x + beta * y   (rows m)
+  void A_forward(const double* x, double alpha, double beta, double* y) {
+    need(x, "A_forward x");
+    need(y, "A_forward y");
+    if (!nblk) return;
+    ++g_launches, k_op_forward<<<dim3(nblk, 1), 256, 0, st>>>(blocks_, kcount_, col_ptr_, col_idx_, acol_off_,
+                                                acol_, x, n, alpha, beta, y, m);
+    launched("k_op_forward");
+  }
+  // y = alpha * A' z + beta * y   (length n)
+  void A_adjoint(const double* z, double alpha, double beta, double* y) {
+    need(z, "A_adjoint z");
+    need(y, "A_adjoint y");
+    if (nwork_) {
+      int wpb = 8;
+      ++g_launches, k_op_adjoint_partial<<<dim3((nwork_ + wpb - 1) / wpb, 1), 256, 0, st>>>(
+          blocks_, wblk_, wloc_, col_ptr_, acol_off_, acol_, z, m, adj_part_, nwork_, nwork_);
+      launched("k_op_adjoint_partial");
+    }
+    if (n) {
+      ++g_launches, k_op_adjoint_gather<<<dim3((n + 255) / 256, 1), 256, 0, st>>>(
+          n, c2b_ptr_, c2b_blk_, c2b_loc_, col_ptr_, adj_part_, nwork_, alpha, beta, y, n);
+      launched("k_op_adjoint_gather");
+    }
+  }
+  // y = alpha * P x + beta * y  (P symmetric)
+  void P_mult(const double* x, double alpha, double beta, double* y) {
+    need(x, "P_mult x");
+    need(y, "P_mult y");
+    if (!n) return;
+    if (p_nnz_ == 0) {
+      lincomb(n, 0.0, nullptr, beta, beta == 0.0 ? nullptr : y, 0.0, nullptr, y);
+      return;
+    }
+    ++g_launches, k_csr_spmv<<<(n + 255) / 256, 256, 0, st>>>(n, prp_, pci_, pv_, x, alpha, beta, y);
+    launched("k_csr_spmv");
+  }
+  bool has_P() const { return p_nnz_ > 0; }
+
+  // ---- Schur complement ----
+  bool assemble() {
+    tbegin(KT_ASSEMBLE);
+    if (nwork_) {
+      ++g_launches, k_schur_transform<<<nwork_, SDPXG_THREADS, kSmemTrans, st>>>(blocks_, wblk_, wloc_, acol_off_,
+                                                                   Ginv_, acol_, tcol_);
+      launched("k_schur_transform");
+      ++g_launches, k_schur_block_gemm<<<ntiles_, 256, 0, st>>>(blocks_, tiles_, kcount_, acol_off_, s_off_, acol_,
+                                                  tcol_, S_);
+      launched("k_schur_block_gemm");
+    }
+    long tot = (long)n * n;
+    if (tot) {
+      ++g_launches, k_schur_gather<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, c2b_ptr_, c2b_blk_, c2b_loc_,
+                                                                  kcount_, s_off_, S_, Hsave_);
+      launched("k_schur_gather");
+    }
+    if (pup_nnz_) {
+      ++g_launches, k_add_upper_csc<<<(n + 255) / 256, 256, 0, st>>>(n, pup_ptr_, pup_row_, pup_val_, Hsave_);
+    }
+    tend(KT_ASSEMBLE);
+    int s = red.add(st, RED_FINITE, tot, Hsave_, nullptr);
+    return red.fetch(st)[s] == 1.0;
+  }
+  double schur_diag_absmax() {
+    if (!n) return 0.0;
+    ++g_launches, k_diag_absmax<<<1, 1024, 0, st>>>(Hsave_, n, scal_);
+    double v = 0.0;
+    check(cudaMemcpyAsync(&v, scal_.p, sizeof(double), cudaMemcpyDeviceToHost, st), "diag D2H");
+    check(cudaStreamSynchronize(st), "diag sync");
+    return v;
+  }
+  // F = chol(Hsave + eps I) with the dynamic pivot rule
+  bool factor(double eps, bool dynamic, double dyn_eps, double dyn_delta) {
+    if (!n) return true;
+    clear_status();
+    tbegin(KT_FACTOR);
+    ++g_launches, k_shifted_copy<<<1184, 256, 0, st>>>(Hsave_, F_, n, eps, diag0_);
+    for (int kb = 0; kb < nchol; ++kb) {
+      ++g_launches, k_potrf_diag<<<1, SDPXG_THREADS, 0, st>>>(F_, n, kb, dyn_eps, dyn_delta, dynamic ? 1 : 0,
+                                                diag0_, Dinv_, status_);
+      int rest = nchol - kb - 1;
+      if (rest > 0) {
+        ++g_launches, k_trsm_panel<<<rest, SDPXG_THREADS, kSmemTrsm, st>>>(F_, n, kb, Dinv_);
+        ++g_launches, k_syrk_update<<<rest * (rest + 1) / 2, SDPXG_THREADS, kSmemSyrk, st>>>(F_, n, kb);
+      }
+    }
+    launched("factor");
+    tend(KT_FACTOR);
+    uint32_t s = read_status();
+    factor_ok_ = (s == 0);
+    return factor_ok_;
+  }
+  // x = F^-1 r (no refinement); x may alias nothing.
+  void trisolve(const double* r, double* x) {
+    need(r, "trisolve r");
+    need(x, "trisolve x");
+    tbegin(KT_TRISOLVE);
+    check(cudaMemcpyAsync(tri_b_.p, r, n * sizeof(double), cudaMemcpyDeviceToDevice, st), "trisolve copy");
+    for (int kb = 0; kb < nchol; ++kb)
+      ++g_launches, k_trsv_fwd<<<nchol - kb, SDPXG_THREADS, 0, st>>>(F_, n, kb, Dinv_, tri_b_, tri_y_, n, 1);
+    for (int kb = nchol - 1; kb >= 0; --kb)
+      ++g_launches, k_trsv_bwd<<<kb + 1, SDPXG_THREADS, 0, st>>>(F_, n, kb, Dinv_, tri_y_, x, n, 1);
+    launched("trisolve");
+    tend(KT_TRISOLVE);
+  }
+  // e = r - Hsave x
+  void schur_residual(const double* r, const double* x, double* e) {
+    need(r, "schur_residual r");
+    need(x, "schur_residual x");
+    need(e, "schur_residual e");
+    if (!n) return;
+    tbegin(KT_SYMV);
+    ++g_launches, k_symv_partial<<<dim3((n + 127) / 128, 16, 1), 128, 0, st>>>(Hsave_, n, x, n, symv_part_,
+                                                                 (long)16 * n);
+    ++g_launches, k_symv_finish<<<dim3((n + 255) / 256, 1), 256, 0, st>>>(n, symv_part_, (long)16 * n, r, n, e, n);
+    launched("schur_residual");
+    tend(KT_SYMV);
+  }
+
+  void lincomb(long len, double a, const double* x, double b, const double* y, double c,
+               const double* w, double* out) {
+    if (len <= 0) return;
+    need(out, "lincomb out");
+    int grid = (int)std::min<long>((len + 255) / 256, 1184);
+    ++g_launches, k_lincomb<<<grid, 256, 0, st>>>(len, a, x, b, y, c, w, out);
+  }
+  void copy(double* dst, const double* src, long len) {
+    if (len > 0) {
+      need(dst, "copy dst");
+      need(src, "copy src");
+    }
+    if (len > 0)
+      check(cudaMemcpyAsync(dst, src, len * sizeof(double), cudaMemcpyDeviceToDevice, st), "d2d");
+  }
+
+  double* Hsave() { return Hsave_.p; }
+  double* F() { return F_.p; }
+  const BlockDesc* blocks() const { return blocks_.p; }
+
+ private:
+  static void set_smem(const void* fn, size_t bytes) {
+    check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+          "cudaFuncSetAttribute");
+  }
+  void launched(const char* what) { check(cudaGetLastError(), what); }
+
+  int matlen_ = 0, veclen_ = 0, nwork_ = 0, ntiles_ = 0, p_nnz_ = 0, pup_nnz_ = 0;
+  bool factor_ok_ = false;
+  DevBuf<BlockDesc> blocks_;
+  DevBuf<double> R_, Rinv_, Ginv_, lam_, lisqrt_;
+  DevBuf<double> acol_, tcol_, S_;
+  DevBuf<long> acol_off_, s_off_;
+  DevBuf<int> kcount_, col_ptr_, col_idx_, c2b_ptr_, c2b_blk_, c2b_loc_, wblk_, wloc_, tiles_;
+  DevBuf<int> prp_, pci_, pup_ptr_, pup_row_;
+  DevBuf<double> pv_, pup_val_;
+  DevBuf<double> adj_part_;
+  DevBuf<double> Hsave_, F_, Dinv_, diag0_, symv_part_, tri_b_, tri_y_;
+  DevBuf<double> step_out_, marg_out_, scal_;
+  DevBuf<uint32_t> status_;
+  cudaEvent_t ev_[2 * KT_N] = {};
+};
+
+}  // namespace sdpxg

@@ -1,0 +1,775 @@
+// Host driver of the homogeneous self-dual interior-point iteration over the device engine.
+//
+// A restatement of the reference's binary64 predictor/corrector
+// (crates/solver/src/solver/core/solver.rs:285-1472, default/variables.rs:148-788,
+// default/kktsystem.rs:186-655, default/residuals.rs:340-490, default/info.rs:89-537) with
+// the condensed KKT system of kkt/condensed/* and the refinement of kkt/refinement.rs.
+// Vectors live on the device; the host keeps tau, kappa and the scalar summaries.
+#pragma once
+#include <chrono>
+#include <cmath>
+#include <limits>
+
+#include "engine.cuh"
+
+namespace sdpxg {
+
+constexpr double kEps = 2.220446049250313e-16;
+
+// Solver status codes of the reference C ABI (include/sdpx.h:76-80).
+enum Status {
+  ST_UNSOLVED = 0, ST_SOLVED = 1, ST_PRIMAL_INFEASIBLE = 2, ST_DUAL_INFEASIBLE = 3,
+  ST_ALMOST_SOLVED = 4, ST_ALMOST_PRIMAL_INFEASIBLE = 5, ST_ALMOST_DUAL_INFEASIBLE = 6,
+  ST_MAX_ITERATIONS = 7, ST_MAX_TIME = 8, ST_NUMERICAL_ERROR = 9, ST_INSUFFICIENT_PROGRESS = 10,
+};
+
+// Binary64 defaults of default/settings.rs:17-314.
+struct Settings {
+  int max_iter = 200;
+  double time_limit = std::numeric_limits<double>::infinity();
+  double max_step_fraction = 0.99;
+  double tol_gap_abs = 1e-8, tol_gap_rel = 1e-8, tol_feas = 1e-8;
+  double tol_infeas_abs = 1e-8, tol_infeas_rel = 1e-8, tol_ktratio = 1e-6;
+  double reduced_tol_gap_abs = 5e-5, reduced_tol_gap_rel = 5e-5, reduced_tol_feas = 1e-4;
+  double reduced_tol_infeas_abs = 5e-12, reduced_tol_infeas_rel = 5e-5, reduced_tol_ktratio = 1e-4;
+  double tol_original = 1e-6;  // <= 0 disables the original-coordinate test
+  bool equilibrate_enable = true;
+  int equilibrate_max_iter = 10;
+  double equilibrate_min_scaling = 1e-4, equilibrate_max_scaling = 1e4;
+  bool static_reg_enable = true;
+  double static_reg_constant = 1e-8, static_reg_proportional = kEps * kEps;
+  bool dynamic_reg_enable = true;
+  double dynamic_reg_eps = 1e-13, dynamic_reg_delta = 2e-7;
+  bool ir_enable = true;
+  double ir_reltol = 1e-13, ir_abstol = 1e-12;
+  int ir_max_iter = 10;
+  double ir_stop_ratio = 5.0;
+};
+
+struct Equilibration {
+  std::vector<double> d, dinv, e, einv;
+  double c = 1.0;
+};
+
+struct Info {
+  int status = ST_UNSOLVED;
+  int iterations = 0;
+  double cost_primal = 0, cost_dual = 0, res_primal = 0, res_dual = 0;
+  double res_primal_inf = 0, res_dual_inf = 0, gap_abs = 0, gap_rel = 0, ktratio = 0;
+  double solve_time = 0;
+  double rz_ns = 0, rx_ns = 0;
+};
+
+struct PhaseTimes {
+  double residual = 0, scale = 0, assemble = 0, factor = 0, solve = 0, step = 0, other = 0;
+  int factorizations = 0, kkt_solves = 0, outer_refinements = 0, inner_refinements = 0;
+};
+
+class HsdSolver {
+ public:
+  HsdSolver(Engine& eng, const HostProblem& p, const Equilibration& eq, const Settings& st)
+      : E(eng), eq_(eq), st_(st), n_(p.n), m_(p.m) {
+    const int n = n_, m = m_;
+    auto vn = [&](DevBuf<double>& b) { b.alloc(std::max(n, 1)); };
+    auto vm = [&](DevBuf<double>& b) { b.alloc(std::max(m, 1)); };
+    for (auto* b : {&x_, &px_, &bx_, &rx_, &rxinf_, &Px_, &x2_, &dx_, &ax_, &tx_, &prevx_, &bestx_,
+                    &rhsx_, &x1_, &xhat_, &en_, &dxn_, &candn_, &e2n_, &ex_, &cx_, &candx_, &ex2_,
+                    &negq_, &q_, &d_, &dinv_, &wn_})
+      vn(*b);
+    for (auto* b : {&s_, &z_, &ps_, &pz_, &rz_, &rzinf_, &z2_, &ds_, &dz_, &as_, &az_, &ts_, &tz_,
+                    &prevs_, &prevz_, &bests_, &bestz_, &rhsz_, &rhss_, &cvec_, &workz_, &z1_,
+                    &tm_, &ez_, &cz_, &candz_, &ez2_, &wm1_, &wm2_, &wm3_, &b_, &e_, &einv_})
+      vm(*b);
+    q_.upload(p.q.data(), n, E.st);
+    b_.upload(p.b.data(), m, E.st);
+    std::vector<double> nq(p.q);
+    for (auto& v : nq) v = -v;
+    negq_.upload(nq.data(), n, E.st);
+    d_.upload(eq.d.data(), n, E.st);
+    dinv_.upload(eq.dinv.data(), n, E.st);
+    e_.upload(eq.e.data(), m, E.st);
+    einv_.upload(eq.einv.data(), m, E.st);
+    degree_ = 0;
+    for (int d : p.psd) degree_ += d;
+    // scaled norms of the data (default/problemdata.rs:444-465)
+    normq_ = 0;
+    for (int i = 0; i < n; ++i) normq_ = std::max(normq_, std::fabs(p.q[i] * eq.dinv[i]));
+    normq_ /= eq.c;
+    normb_ = 0;
+    for (int i = 0; i < m; ++i) normb_ = std::max(normb_, std::fabs(p.b[i] * eq.einv[i]));
+    data_scale_ = 1.0;
+    for (double v : p.b) data_scale_ = std::max(data_scale_, std::fabs(v));
+    for (double v : p.q) data_scale_ = std::max(data_scale_, std::fabs(v));
+    for (double v : p.Aval) data_scale_ = std::max(data_scale_, std::fabs(v));
+    dmax_ = 1.0;
+    for (double v : eq.d) dmax_ = std::max(dmax_, v);
+  }
+
+  Info info;
+  PhaseTimes times;
+  std::vector<double> hx, hs, hz;  // unscaled solution
+
+  void solve();
+
+  // ---------------- KKT system (also driven directly by the kernel-level ABI) ----------------
+  bool kkt_update();
+  bool reduced_solve(const double* r, double* x);
+  bool solve_raw(const double* bx, const double* bz, double* x, double* z);
+  bool kkt_solve(const double* bx, const double* bz, double* x, double* z);
+  void residual_full(const double* bx, const double* bz, const double* x, const double* z,
+                     double* ex, double* ez);
+
+ private:
+  using clock = std::chrono::steady_clock;
+  static double secs(clock::time_point a) {
+    return std::chrono::duration<double>(clock::now() - a).count();
+  }
+  cudaStream_t st() const { return E.st; }
+  // ---------------- HSD pieces ----------------
+  struct Resid { double qx, bz, sz, xPx, rtau; double norms[8]; };
+  Resid residuals();
+  void update_info(const Resid& r);
+  bool is_solved(double ga, double gr, double feas) const;
+  void check_convergence(const Resid& r, bool full);
+  bool check_termination(const Resid& r, int iter);
+  double original_ratio(bool reduced);
+  bool hsd_direction(const double* rhs_x, const double* workz, double rhs_tau, double rhs_kappa,
+                     const double* rhs_z, const double* x1, const double* z1, double* dtau,
+                     double* dkappa);
+  double step_bounds(const double* dz, const double* ds, double dtau, double dkappa, int mode,
+                     double amax_cap);
+  bool default_start();
+  double tolerance_multiple(const Info& in) const {
+    double gap = std::min(in.gap_abs / st_.tol_gap_abs, in.gap_rel / st_.tol_gap_rel);
+    return std::max(std::max(in.res_primal, in.res_dual) / st_.tol_feas, gap);
+  }
+
+  Engine& E;
+  Equilibration eq_;
+  Settings st_;
+  int n_, m_, degree_ = 0;
+  double normq_ = 0, normb_ = 0, data_scale_ = 1, dmax_ = 1;
+  double tau_ = 1, kappa_ = 1;
+  double best_tau_ = 1, best_kappa_ = 1;
+  int reg_boost_ = 0;
+  Info prev_;
+  bool have_prev_ = false;
+  // device vectors (n-length then m-length groups)
+  DevBuf<double> x_, px_, bx_, rx_, rxinf_, Px_, x2_, dx_, ax_, tx_, prevx_, bestx_, rhsx_, x1_,
+      xhat_, en_, dxn_, candn_, e2n_, ex_, cx_, candx_, ex2_, negq_, q_, d_, dinv_, wn_;
+  DevBuf<double> s_, z_, ps_, pz_, rz_, rzinf_, z2_, ds_, dz_, as_, az_, ts_, tz_, prevs_, prevz_,
+      bests_, bestz_, rhsz_, rhss_, cvec_, workz_, z1_, tm_, ez_, cz_, candz_, ez2_, wm1_, wm2_, wm3_,
+      b_, e_, einv_;
+};
+
+// ------------------------------------------------------------------------------------------
+// KKT: assemble + factor with the static shift and its escalation (kkt/direct/solver.rs:758-877,
+// 511-520, 1473-1485)
+// ------------------------------------------------------------------------------------------
+inline bool HsdSolver::kkt_update() {
+  auto t0 = clock::now();
+  bool ok = E.assemble();
+  times.assemble += secs(t0);
+  if (!ok) return false;
+  auto t1 = clock::now();
+  double diag = E.schur_diag_absmax();
+  for (;;) {
+    double eps = 0.0;
+    if (st_.static_reg_enable) {
+      eps = st_.static_reg_constant + st_.static_reg_proportional * diag;
+      if (reg_boost_ > 0) eps *= std::pow(100.0, reg_boost_);
+    }
+    times.factorizations++;
+    ok = E.factor(eps, st_.dynamic_reg_enable, st_.dynamic_reg_eps, st_.dynamic_reg_delta);
+    if (ok || !st_.static_reg_enable || reg_boost_ >= 3) break;
+    reg_boost_++;
+  }
+  times.factor += secs(t1);
+  return ok;
+}
+
+// Stationary refinement of the reduced system against the unshifted Schur complement.
+inline bool HsdSolver::reduced_solve(const double* r, double* x) {
+  const int n = n_;
+  E.trisolve(r, x);
+  if (!st_.ir_enable) return true;
+  E.schur_residual(r, x, en_);
+  int s0 = E.red.add(st(), RED_MAXABS, n, r, nullptr);
+  int s1 = E.red.add(st(), RED_MAXABS, n, en_, nullptr);
+  int s2 = E.red.add(st(), RED_FINITE, n, x, nullptr);
+  auto& h = E.red.fetch(st());
+  double normb = h[s0], norme = h[s1];
+  if (h[s2] != 1.0 || !std::isfinite(norme)) return false;
+  const double tol = st_.ir_abstol + st_.ir_reltol * normb;
+  bool converged = norme <= tol;
+  for (int it = 0; it < st_.ir_max_iter && !converged; ++it) {
+    double previous = norme;
+    times.inner_refinements++;
+    E.trisolve(en_, dxn_);
+    E.lincomb(n, 1.0, x, 1.0, dxn_, 0.0, nullptr, candn_);
+    E.schur_residual(r, candn_, e2n_);
+    int a = E.red.add(st(), RED_MAXABS, n, e2n_, nullptr);
+    norme = E.red.fetch(st())[a];
+    if (!std::isfinite(norme)) return false;
+    double ratio = previous / norme;
+    if (ratio < st_.ir_stop_ratio) {
+      if (ratio > 1.0) E.copy(x, candn_, n);
+      break;
+    }
+    E.copy(x, candn_, n);
+    E.copy(en_, e2n_, n);
+    converged = norme <= tol;
+  }
+  return true;
+}
+
+// Condense, reduced solve, recover (kkt/condensed/mod.rs:2416-2622).
+inline bool HsdSolver::solve_raw(const double* bx, const double* bz, double* x, double* z) {
+  E.cone_apply(CM_HINV, bz, tm_);             // Hs^-1 bz
+  E.copy(xhat_, bx, n_);
+  E.A_adjoint(tm_, 1.0, 1.0, xhat_);          // bx + A' Hs^-1 bz
+  if (!reduced_solve(xhat_, x)) return false;
+  E.lincomb(m_, -1.0, bz, 0.0, nullptr, 0.0, nullptr, tm_);
+  E.A_forward(x, 1.0, 1.0, tm_);              // A x - bz
+  E.cone_apply(CM_HINV, tm_, z);              // z = Hs^-1 (A x - bz)
+  return true;
+}
+
+// e = b - [P A'; A -Hs] [x; z] against the unshifted original operator.
+inline void HsdSolver::residual_full(const double* bx, const double* bz, const double* x,
+                                     const double* z, double* ex, double* ez) {
+  E.P_mult(x, -1.0, 0.0, wn_);
+  E.lincomb(n_, 1.0, bx, 1.0, wn_, 0.0, nullptr, ex);
+  E.A_adjoint(z, -1.0, 1.0, ex);
+  E.cone_apply(CM_HS, z, wm3_);
+  E.lincomb(m_, 1.0, bz, 1.0, wm3_, 0.0, nullptr, ez);
+  E.A_forward(x, -1.0, 1.0, ez);
+}
+
+// Solve with outer refinement on the original operator (kkt/condensed/kkt.rs:275-318,
+// kkt/refinement.rs:118-191).
+inline bool HsdSolver::kkt_solve(const double* bx, const double* bz, double* x, double* z) {
+  auto t0 = clock::now();
+  times.kkt_solves++;
+  const int n = n_, m = m_;
+  {
+    int a = E.red.add(st(), RED_FINITE, n, bx, nullptr);
+    int b = E.red.add(st(), RED_FINITE, m, bz, nullptr);
+    auto& h = E.red.fetch(st());
+    if (h[a] != 1.0 || h[b] != 1.0) return false;
+  }
+  if (!solve_raw(bx, bz, x, z)) return false;
+  bool ok = true;
+  if (st_.ir_enable) {
+    residual_full(bx, bz, x, z, ex_, ez_);
+    int s0 = E.red.add(st(), RED_MAXABS, n, bx, nullptr);
+    int s1 = E.red.add(st(), RED_MAXABS, m, bz, nullptr);
+    int s2 = E.red.add(st(), RED_MAXABS, n, ex_, nullptr);
+    int s3 = E.red.add(st(), RED_MAXABS, m, ez_, nullptr);
+    auto& h = E.red.fetch(st());
+    double normb = std::max(h[s0], h[s1]);
+    double norme = std::max(h[s2], h[s3]);
+    if (!std::isfinite(norme)) {
+      ok = false;
+    } else {
+      const double tol = st_.ir_abstol + st_.ir_reltol * normb;
+      bool converged = norme <= tol;
+      for (int it = 0; it < st_.ir_max_iter && !converged; ++it) {
+        double previous = norme;
+        times.outer_refinements++;
+        if (!solve_raw(ex_, ez_, cx_, cz_)) { ok = false; break; }
+        E.lincomb(n, 1.0, x, 1.0, cx_, 0.0, nullptr, candx_);
+        E.lincomb(m, 1.0, z, 1.0, cz_, 0.0, nullptr, candz_);
+        residual_full(bx, bz, candx_, candz_, ex2_, ez2_);
+        int a = E.red.add(st(), RED_MAXABS, n, ex2_, nullptr);
+        int b = E.red.add(st(), RED_MAXABS, m, ez2_, nullptr);
+        auto& hh = E.red.fetch(st());
+        norme = std::max(hh[a], hh[b]);
+        if (!std::isfinite(norme)) { ok = false; break; }
+        double ratio = previous / norme;
+        if (ratio < st_.ir_stop_ratio) {
+          if (ratio > 1.0) {
+            E.copy(x, candx_, n);
+            E.copy(z, candz_, m);
+          }
+          break;
+        }
+        E.copy(x, candx_, n);
+        E.copy(z, candz_, m);
+        E.copy(ex_, ex2_, n);
+        E.copy(ez_, ez2_, m);
+        converged = norme <= tol;
+      }
+    }
+  }
+  times.solve += secs(t0);
+  return ok;
+}
+
+// ------------------------------------------------------------------------------------------
+// Residuals and info (default/residuals.rs:340-490, default/info.rs:89-192)
+// ------------------------------------------------------------------------------------------
+inline HsdSolver::Resid HsdSolver::residuals() {
+  auto t0 = clock::now();
+  const int n = n_, m = m_;
+  E.P_mult(x_, 1.0, 0.0, Px_);
+  E.A_adjoint(z_, -1.0, 0.0, rxinf_);
+  E.copy(rzinf_, s_, m);
+  E.A_forward(x_, 1.0, 1.0, rzinf_);
+  E.lincomb(n, -1.0, Px_, -tau_, q_, 1.0, rxinf_, rx_);
+  E.lincomb(m, 1.0, rzinf_, -tau_, b_, 0.0, nullptr, rz_);
+  int sq = E.red.add(st(), RED_DOT, n, q_, x_);
+  int sb = E.red.add(st(), RED_DOT, m, b_, z_);
+  int ss = E.red.add(st(), RED_DOT, m, s_, z_);
+  int sp = E.red.add(st(), RED_DOT, n, x_, Px_);
+  int nr[8];
+  nr[0] = E.red.add(st(), RED_SUMSQ, n, x_, d_);
+  nr[1] = E.red.add(st(), RED_SUMSQ, m, z_, e_);
+  nr[2] = E.red.add(st(), RED_SUMSQ, m, s_, einv_);
+  nr[3] = E.red.add(st(), RED_SUMSQ, n, rxinf_, dinv_);
+  nr[4] = E.red.add(st(), RED_SUMSQ, n, Px_, dinv_);
+  nr[5] = E.red.add(st(), RED_SUMSQ, m, rzinf_, einv_);
+  nr[6] = E.red.add(st(), RED_SUMSQ, m, rz_, einv_);
+  nr[7] = E.red.add(st(), RED_SUMSQ, n, rx_, dinv_);
+  auto& h = E.red.fetch(st());
+  Resid r;
+  r.qx = h[sq];
+  r.bz = h[sb];
+  r.sz = h[ss];
+  r.xPx = h[sp];
+  for (int k = 0; k < 8; ++k) r.norms[k] = std::sqrt(h[nr[k]]);
+  r.rtau = r.qx + r.bz + kappa_ + r.xPx / tau_;
+  times.residual += secs(t0);
+  return r;
+}
+
+inline void HsdSolver::update_info(const Resid& r) {
+  const double tinv = 1.0 / tau_, cinv = 1.0 / eq_.c;
+  const double xpx = r.xPx * tinv * tinv / 2.0;
+  Info& in = info;
+  in.cost_primal = (r.qx * tinv + xpx) * cinv;
+  in.cost_dual = (-r.bz * tinv - xpx) * cinv;
+  double normx = r.norms[0], normz = r.norms[1] * cinv, norms = r.norms[2];
+  in.res_primal_inf = (r.norms[3] * cinv) / std::max(1.0, normz);
+  in.res_dual_inf = std::max(r.norms[4] / std::max(1.0, normx), r.norms[5] / std::max(1.0, normx + norms));
+  normx *= tinv;
+  normz *= tinv;
+  norms *= tinv;
+  in.rz_ns = r.norms[6];
+  in.rx_ns = r.norms[7];
+  in.res_primal = r.norms[6] * tinv / std::max(1.0, normb_ + normx + norms);
+  in.res_dual = r.norms[7] * tinv * cinv / std::max(1.0, normq_ + normx + normz);
+  in.gap_abs = std::fabs(in.cost_primal - in.cost_dual);
+  in.gap_rel = in.gap_abs / std::max(1.0, std::min(std::fabs(in.cost_primal), std::fabs(in.cost_dual)));
+  in.ktratio = kappa_ * tinv;
+}
+
+inline bool HsdSolver::is_solved(double ga, double gr, double feas) const {
+  return (info.gap_abs < ga || info.gap_rel < gr) && info.res_primal < feas && info.res_dual < feas;
+}
+
+inline void HsdSolver::check_convergence(const Resid& r, bool full) {
+  double ga, gr, fe, ia, ir, kt;
+  int c0, c1, c2;
+  if (full) {
+    ga = st_.tol_gap_abs; gr = st_.tol_gap_rel; fe = st_.tol_feas;
+    ia = st_.tol_infeas_abs; ir = st_.tol_infeas_rel; kt = st_.tol_ktratio;
+    c0 = ST_SOLVED; c1 = ST_PRIMAL_INFEASIBLE; c2 = ST_DUAL_INFEASIBLE;
+  } else {
+    ga = st_.reduced_tol_gap_abs; gr = st_.reduced_tol_gap_rel; fe = st_.reduced_tol_feas;
+    ia = st_.reduced_tol_infeas_abs; ir = st_.reduced_tol_infeas_rel; kt = st_.reduced_tol_ktratio;
+    c0 = ST_ALMOST_SOLVED; c1 = ST_ALMOST_PRIMAL_INFEASIBLE; c2 = ST_ALMOST_DUAL_INFEASIBLE;
+  }
+  if (info.ktratio <= 1.0 && is_solved(ga, gr, fe)) {
+    info.status = c0;
+  } else if (info.ktratio > (1.0 / kt) * 1000.0) {
+    if (r.bz < -ia && info.res_primal_inf < -ir * r.bz) info.status = c1;
+    else if (r.qx < -ia && info.res_dual_inf < -ir * r.qx) info.status = c2;
+  }
+}
+
+// default/info.rs:263-327
+inline bool HsdSolver::check_termination(const Resid& r, int iter) {
+  check_convergence(r, true);
+  if (info.status == ST_UNSOLVED && iter > 1 && have_prev_ &&
+      (info.res_dual > prev_.res_dual || info.res_primal > prev_.res_primal)) {
+    if (info.ktratio < kEps * 100.0 &&
+        (prev_.gap_abs < st_.tol_gap_abs || prev_.gap_rel < st_.tol_gap_rel))
+      info.status = ST_INSUFFICIENT_PROGRESS;
+    if (info.ktratio < 1.0) {
+      if ((info.res_dual > st_.tol_feas * 100.0 && info.res_dual > prev_.res_dual * 100.0) ||
+          (info.res_primal > st_.tol_feas * 100.0 && info.res_primal > prev_.res_primal * 100.0))
+        info.status = ST_INSUFFICIENT_PROGRESS;
+    }
+  }
+  if (info.status == ST_UNSOLVED) {
+    if (st_.max_iter == iter) info.status = ST_MAX_ITERATIONS;
+    else if (info.solve_time > st_.time_limit) info.status = ST_MAX_TIME;
+  }
+  return info.status != ST_UNSOLVED;
+}
+
+// Original-coordinate acceptance (default/original_check.rs, default/solution.rs:169-193).
+// PSD equilibration is one scalar per cone, so the cone distances scale exactly.
+inline double HsdSolver::original_ratio(bool reduced) {
+  if (!(st_.tol_original > 0)) return -1.0;
+  const int n = n_, m = m_;
+  const double tinv = 1.0 / tau_, cinv = 1.0 / eq_.c;
+  int a = E.red.add(st(), RED_MAXABS, m, rz_, einv_);
+  int b = E.red.add(st(), RED_MAXABS, n, rx_, dinv_);
+  auto& h = E.red.fetch(st());
+  double prim = h[a] * tinv, dual = h[b] * tinv * cinv;
+  E.lincomb(m, tau_, b_, 0.0, nullptr, 0.0, nullptr, wm1_);
+  E.A_forward(x_, -1.0, 1.0, wm1_);  // b tau - A x
+  std::vector<double> mr, ms, mz;
+  E.margins(wm1_, mr);
+  E.margins(s_, ms);
+  E.margins(z_, mz);
+  for (int j = 0; j < E.nblk; ++j) {
+    double ej = eq_.e[E.hblocks[j].svec_off];
+    prim = std::max(prim, std::max(0.0, -mr[2 * j]) * tinv / ej);
+    prim = std::max(prim, std::max(0.0, -ms[2 * j]) * tinv / ej);
+    dual = std::max(dual, std::max(0.0, -mz[2 * j]) * tinv * cinv * ej);
+  }
+  prim /= (1.0 + normb_);
+  dual /= (1.0 + normq_);
+  double gap_abs = std::fabs(info.cost_primal - info.cost_dual);
+  double gap_rel = gap_abs / (1.0 + std::fabs(info.cost_primal));
+  double tf = st_.tol_original, ta = st_.tol_original, tr = st_.tol_original;
+  if (reduced) {
+    tf = std::max(tf, st_.reduced_tol_feas);
+    ta = std::max(ta, st_.reduced_tol_gap_abs);
+    tr = std::max(tr, st_.reduced_tol_gap_rel);
+  }
+  double gap = std::min(gap_abs / ta, gap_rel / tr);
+  double r = std::max(std::max(prim / tf, dual / tf), gap);
+  return std::isnan(r) ? std::numeric_limits<double>::infinity() : r;
+}
+
+// Homogeneous direction from a solved column (x1, z1) and the constant column (x2, z2):
+// dtau (default/kktsystem.rs:550-655), dx, dz, ds from the linear row (403-418), dkappa.
+inline bool HsdSolver::hsd_direction(const double* rhs_x, const double* workz, double rhs_tau,
+                                     double rhs_kappa, const double* rhs_z, const double* x1,
+                                     const double* z1, double* dtau, double* dkappa) {
+  (void)rhs_x; (void)workz;
+  const int n = n_, m = m_;
+  int a = E.red.add(st(), RED_DOT, n, q_, x1);
+  int b = E.red.add(st(), RED_DOT, m, b_, z1);
+  int c = E.red.add(st(), RED_DOT, n, q_, x2_);
+  int d = E.red.add(st(), RED_DOT, m, b_, z2_);
+  int f1 = -1, f2 = -1, f3 = -1;
+  if (E.has_P()) {
+    // xi = x / tau; quad1 = xi' P x1; delta = (xi - x2)' P (xi - x2); quad2 = x2' P x2
+    E.P_mult(x1, 1.0, 0.0, wn_);
+    E.lincomb(n, 1.0 / tau_, x_, 0.0, nullptr, 0.0, nullptr, tx_);
+    f1 = E.red.add(st(), RED_DOT, n, tx_, wn_);
+    E.lincomb(n, 1.0 / tau_, x_, -1.0, x2_, 0.0, nullptr, tx_);
+    E.P_mult(tx_, 1.0, 0.0, candn_);
+    f2 = E.red.add(st(), RED_DOT, n, tx_, candn_);
+    E.P_mult(x2_, 1.0, 0.0, e2n_);
+    f3 = E.red.add(st(), RED_DOT, n, x2_, e2n_);
+  }
+  auto& h = E.red.fetch(st());
+  double q1 = h[a], b1 = h[b], q2 = h[c], b2 = h[d];
+  double quad1 = f1 >= 0 ? h[f1] : 0.0, delta = f2 >= 0 ? h[f2] : 0.0, quad2 = f3 >= 0 ? h[f3] : 0.0;
+  double num = rhs_tau - rhs_kappa / tau_ + q1 + b1 + 2.0 * quad1;
+  double den = kappa_ / tau_ - q2 - b2;
+  den += delta - quad2;
+  double dt = num / den;
+  if (!std::isfinite(dt)) return false;
+  E.lincomb(n, 1.0, x1, dt, x2_, 0.0, nullptr, dx_);
+  E.lincomb(m, 1.0, z1, dt, z2_, 0.0, nullptr, dz_);
+  E.lincomb(m, -1.0, rhs_z, dt, b_, 0.0, nullptr, ds_);
+  E.A_forward(dx_, -1.0, 1.0, ds_);
+  *dtau = dt;
+  *dkappa = -(rhs_kappa + kappa_ * dt) / tau_;
+  return true;
+}
+
+// min(alpha_tau, alpha_kappa, cap, cone bounds) (default/variables.rs:697-750)
+inline double HsdSolver::step_bounds(const double* dz, const double* ds, double dtau, double dkappa,
+                                     int mode, double cap) {
+  auto t0 = clock::now();
+  double at = dtau < 0 ? -tau_ / dtau : std::numeric_limits<double>::max();
+  double ak = dkappa < 0 ? -kappa_ / dkappa : std::numeric_limits<double>::max();
+  double a = std::min(std::min(at, ak), cap);
+  double az, as;
+  bool ok = E.step_bounds(dz, ds, a, mode, &az, &as);
+  times.step += secs(t0);
+  if (!ok) return 0.0;
+  return std::min(az, as);
+}
+
+// core/solver.rs:1209-1322 and default/kktsystem.rs:462-527, variables.rs:577-620
+inline bool HsdSolver::default_start() {
+  const int n = n_, m = m_;
+  E.identity_scaling();
+  reg_boost_ = 0;
+  bool ok = kkt_update();
+  E.lincomb(n, 0.0, nullptr, 0.0, nullptr, 0.0, nullptr, x_);
+  if (ok) {
+    if (!E.has_P()) {
+      E.lincomb(n, 0.0, nullptr, 0.0, nullptr, 0.0, nullptr, wn_);
+      ok = kkt_solve(wn_, b_, x_, wm2_);
+      if (ok) {
+        E.lincomb(m, -1.0, wm2_, 0.0, nullptr, 0.0, nullptr, s_);
+        E.lincomb(m, 0.0, nullptr, 0.0, nullptr, 0.0, nullptr, wm1_);
+        ok = kkt_solve(negq_, wm1_, wn_, z_);
+      }
+    } else {
+      ok = kkt_solve(negq_, b_, x_, z_);
+      if (ok) E.lincomb(m, -1.0, z_, 0.0, nullptr, 0.0, nullptr, s_);
+    }
+  }
+  if (ok) {
+    int a = E.red.add(st(), RED_MAXABS, n, x_, nullptr);
+    int b = E.red.add(st(), RED_MAXABS, m, z_, nullptr);
+    auto& h = E.red.fetch(st());
+    double bound = 1e12 * data_scale_;
+    if (!(h[a] <= bound && h[b] <= bound)) ok = false;
+  }
+  if (ok) {
+    for (double* v : {s_.p, z_.p}) {
+      std::vector<double> mg;
+      if (!E.margins(v, mg)) return false;
+      double mn = std::numeric_limits<double>::max(), pos = 0.0;
+      for (int j = 0; j < E.nblk; ++j) {
+        mn = std::min(mn, mg[2 * j]);
+        pos += mg[2 * j + 1];
+      }
+      double target = std::max(1.0, (pos * 0.1) / std::max(degree_, 1));
+      if (mn <= 0) {
+        E.shift_unit(v, -mn);
+        E.shift_unit(v, target);
+      } else if (mn < target) {
+        E.shift_unit(v, target - mn);
+      }
+    }
+    tau_ = 1.0;
+    kappa_ = 1.0;
+  } else {
+    // unit start (core/solver.rs:1259-1290)
+    E.lincomb(n, 0.0, nullptr, 0.0, nullptr, 0.0, nullptr, x_);
+    E.lincomb(m, 0.0, nullptr, 0.0, nullptr, 0.0, nullptr, s_);
+    E.shift_unit(s_, 1.0);
+    E.copy(z_, s_, m);
+    double t0 = std::min(1.0, 1.0 / dmax_);
+    tau_ = t0;
+    kappa_ = 1.0 / t0;
+  }
+  return true;
+}
+
+// ------------------------------------------------------------------------------------------
+// The iteration (core/solver.rs:285-505, 831-1012)
+// ------------------------------------------------------------------------------------------
+inline void HsdSolver::solve() {
+  auto tstart = clock::now();
+  const int n = n_, m = m_;
+  info = Info();
+  have_prev_ = false;
+  default_start();
+  int it = 0;
+  double mu = 0.0, sigma = 1.0, alpha = 0.0;
+  bool have_best = false;
+  double best_tm = 0.0;
+  double prev_tau = tau_, prev_kappa = kappa_;
+  E.copy(prevx_, x_, n);
+  E.copy(prevs_, s_, m);
+  E.copy(prevz_, z_, m);
+  double orig_best = -1.0;
+  int orig_stale = 0;
+  Resid r{};
+  for (;;) {
+    r = residuals();
+    mu = (r.sz + tau_ * kappa_) / (degree_ + 1);
+    update_info(r);
+    info.iterations = it;
+    info.solve_time = secs(tstart);
+    bool stop = check_termination(r, it);
+    if (stop && info.status == ST_SOLVED) {
+      double ratio = original_ratio(false);
+      if (ratio >= 0 && !(ratio <= 1.0)) {
+        if (orig_best < 0 || ratio < orig_best * 0.5) {
+          orig_best = ratio;
+          orig_stale = 0;
+        } else {
+          orig_stale++;
+        }
+        if (orig_stale >= 3) info.status = ST_INSUFFICIENT_PROGRESS;
+        else if (it >= st_.max_iter) info.status = ST_MAX_ITERATIONS;
+        else {
+          info.status = ST_UNSOLVED;
+          stop = false;
+        }
+      }
+    }
+    if (stop) {
+      if (info.status == ST_INSUFFICIENT_PROGRESS) {
+        E.copy(x_, prevx_, n);
+        E.copy(s_, prevs_, m);
+        E.copy(z_, prevz_, m);
+        tau_ = prev_tau;
+        kappa_ = prev_kappa;
+      }
+      break;
+    }
+    // scale
+    auto t0 = clock::now();
+    bool sok = E.nt_scale(s_, z_);
+    times.scale += secs(t0);
+    if (!sok) {
+      info.status = ST_NUMERICAL_ERROR;
+      break;
+    }
+    ++it;
+    // ---------------- predictor ----------------
+    bool ok = kkt_update();
+    if (ok) {
+      ok = kkt_solve(negq_, b_, x2_, z2_);
+      while (!ok && st_.static_reg_enable && reg_boost_ < 3) {
+        reg_boost_++;
+        ok = kkt_update() && kkt_solve(negq_, b_, x2_, z2_);
+      }
+    }
+    double dtau = 0, dkappa = 0;
+    if (ok) {
+      E.lincomb(m, 1.0, s_, -1.0, rz_, 0.0, nullptr, workz_);
+      ok = kkt_solve(rx_, workz_, x1_, z1_) &&
+           hsd_direction(rx_, workz_, r.rtau, tau_ * kappa_, rz_, x1_, z1_, &dtau, &dkappa);
+    }
+    if (!ok) {
+      info.status = ST_NUMERICAL_ERROR;
+      alpha = 0.0;
+      break;
+    }
+    // keep the raw affine direction for the curve search
+    E.copy(ax_, dx_, n);
+    E.copy(as_, ds_, m);
+    E.copy(az_, dz_, m);
+    double adtau = dtau, adkappa = dkappa;
+    alpha = step_bounds(dz_, ds_, dtau, dkappa, 0, 1.0);
+    sigma = std::max(std::pow(1.0 - alpha, 3), 0.0);
+    const double mfac = (it == 1) ? alpha : 1.0;
+    // ---------------- combined rhs ----------------
+    auto tc = clock::now();
+    E.lincomb(n, 1.0 - sigma, rx_, 0.0, nullptr, 0.0, nullptr, rhsx_);
+    double rhs_tau = (1.0 - sigma) * r.rtau;
+    double rhs_kappa = -sigma * mu + mfac * dtau * dkappa + tau_ * kappa_;
+    E.lincomb(m, mfac, dz_, 0.0, nullptr, 0.0, nullptr, wm1_);
+    E.cone_apply(CM_W, wm1_, wm2_);       // W dz
+    E.cone_apply(CM_WINVT, ds_, wm3_);    // W^-T ds
+    E.circ_op(wm3_, wm2_, wm1_);
+    E.shift_unit(wm1_, -sigma * mu);
+    E.affine_ds(rhss_);
+    E.lincomb(m, 1.0, rhss_, 1.0, wm1_, 0.0, nullptr, rhss_);
+    E.lincomb(m, 1.0 - sigma, rz_, 0.0, nullptr, 0.0, nullptr, rhsz_);
+    E.lam_inv_circ(rhss_, wm2_);
+    E.cone_apply(CM_WT, wm2_, cvec_);     // W'(lambda \ ds)
+    E.lincomb(m, 1.0, cvec_, -1.0, rhsz_, 0.0, nullptr, workz_);
+    times.other += secs(tc);
+    ok = kkt_solve(rhsx_, workz_, x1_, z1_) &&
+         hsd_direction(rhsx_, workz_, rhs_tau, rhs_kappa, rhsz_, x1_, z1_, &dtau, &dkappa);
+    if (!ok) {
+      info.status = ST_NUMERICAL_ERROR;
+      alpha = 0.0;
+      break;
+    }
+    // ---------------- step length and curve search ----------------
+    alpha = step_bounds(dz_, ds_, dtau, dkappa, 0, 1.0) * st_.max_step_fraction;
+    if (alpha > 0.0 && alpha < 0.9) {
+      for (double frac : {0.5, 0.25}) {
+        double t = alpha + (1.0 - alpha) * frac;
+        if (t * (1.0 - sigma * t) <= 1.01 * alpha * (1.0 - sigma)) continue;
+        E.lincomb(n, 1.0 - t, ax_, t, dx_, 0.0, nullptr, tx_);
+        E.lincomb(m, 1.0 - t, as_, t, ds_, 0.0, nullptr, ts_);
+        E.lincomb(m, 1.0 - t, az_, t, dz_, 0.0, nullptr, tz_);
+        double ttau = (1.0 - t) * adtau + t * dtau, tkap = (1.0 - t) * adkappa + t * dkappa;
+        double a = t / st_.max_step_fraction;
+        bool admitted = a <= 1.0 && tau_ + a * ttau >= 0 && kappa_ + a * tkap >= 0;
+        if (admitted) {
+          double az, as;
+          auto t1 = clock::now();
+          bool eok = E.step_bounds(tz_, ts_, a, 1, &az, &as);
+          times.step += secs(t1);
+          admitted = eok && az >= a && as >= a;
+        }
+        if (admitted) {
+          E.copy(dx_, tx_, n);
+          E.copy(ds_, ts_, m);
+          E.copy(dz_, tz_, m);
+          dtau = ttau;
+          dkappa = tkap;
+          alpha = t;
+          break;
+        }
+      }
+    }
+    if (alpha <= 0.0) {
+      info.status = ST_INSUFFICIENT_PROGRESS;
+      break;
+    }
+    prev_ = info;
+    have_prev_ = true;
+    double tm = tolerance_multiple(info);
+    if (!have_best || tm < best_tm) {
+      have_best = true;
+      best_tm = tm;
+      E.copy(bestx_, x_, n);
+      E.copy(bests_, s_, m);
+      E.copy(bestz_, z_, m);
+      best_tau_ = tau_;
+      best_kappa_ = kappa_;
+    }
+    E.copy(prevx_, x_, n);
+    E.copy(prevs_, s_, m);
+    E.copy(prevz_, z_, m);
+    prev_tau = tau_;
+    prev_kappa = kappa_;
+    E.lincomb(n, 1.0, x_, alpha, dx_, 0.0, nullptr, x_);
+    E.lincomb(m, 1.0, s_, alpha, ds_, 0.0, nullptr, s_);
+    E.lincomb(m, 1.0, z_, alpha, dz_, 0.0, nullptr, z_);
+    tau_ += alpha * dtau;
+    kappa_ += alpha * dkappa;
+  }
+  // finish (core/solver.rs:1128-1207)
+  const int before = info.status;
+  if (before == ST_NUMERICAL_ERROR || before == ST_INSUFFICIENT_PROGRESS ||
+      before == ST_MAX_ITERATIONS || before == ST_MAX_TIME) {
+    r = residuals();
+    update_info(r);
+    if (have_best && best_tm < tolerance_multiple(info)) {
+      E.copy(x_, bestx_, n);
+      E.copy(s_, bests_, m);
+      E.copy(z_, bestz_, m);
+      tau_ = best_tau_;
+      kappa_ = best_kappa_;
+      r = residuals();
+      update_info(r);
+    }
+    info.status = before;
+    check_convergence(r, false);
+    if (info.status == ST_ALMOST_SOLVED && before != ST_ALMOST_SOLVED) {
+      double ratio = original_ratio(true);
+      if (ratio >= 0 && !(ratio <= 1.0)) info.status = before;
+    }
+  }
+  info.iterations = it;
+  // unscale (default/variables.rs:640-665)
+  hx.resize(n);
+  hs.resize(m);
+  hz.resize(m);
+  check(cudaMemcpyAsync(hx.data(), x_.p, n * sizeof(double), cudaMemcpyDeviceToHost, st()), "x D2H");
+  check(cudaMemcpyAsync(hs.data(), s_.p, m * sizeof(double), cudaMemcpyDeviceToHost, st()), "s D2H");
+  check(cudaMemcpyAsync(hz.data(), z_.p, m * sizeof(double), cudaMemcpyDeviceToHost, st()), "z D2H");
+  check(cudaStreamSynchronize(st()), "result sync");
+  const double tinv = 1.0 / tau_;
+  for (int i = 0; i < n; ++i) hx[i] = hx[i] * eq_.d[i] * tinv;
+  for (int i = 0; i < m; ++i) {
+    hs[i] = hs[i] * eq_.einv[i] * tinv;
+    hz[i] = hz[i] * eq_.e[i] * tinv / eq_.c;
+  }
+  info.solve_time = secs(tstart);
+}
+
+}  // namespace sdpxg

@@ -1,0 +1,264 @@
+// Kernel-level C ABI (sdpxg_*): one hot-path operation per call, host pointers in and out.
+// These are the entry points a host that keeps its own interior-point driver binds in place
+// of its CPU kernels; each copies its inputs to the device, runs on the context's stream and
+// copies the outputs back before returning.
+#include <memory>
+#include <string>
+
+#include "../../include/sdpx_b200.h"
+#include "hsd.cuh"
+
+using namespace sdpxg;
+
+namespace sdpxg {
+extern thread_local std::string g_last_error;
+}
+
+namespace {
+
+template <typename F>
+int32_t guard(F&& f) {
+  try {
+    return f();
+  } catch (const std::invalid_argument& e) {
+    sdpxg::g_last_error = e.what();
+    return 1;
+  } catch (const std::exception& e) {
+    sdpxg::g_last_error = std::string("internal error: ") + e.what();
+    return 5;
+  } catch (...) {
+    sdpxg::g_last_error = "internal error";
+    return 5;
+  }
+}
+}  // namespace
+
+struct sdpxg_ctx {
+  int device = 0;
+  std::unique_ptr<Engine> eng;
+  HostProblem prob;
+  Equilibration eq;
+  std::unique_ptr<HsdSolver> kkt;  // owns the refinement scratch
+  DevBuf<double> a, b, c, d, e, f;
+  bool uploaded = false;
+};
+
+namespace {
+void need(sdpxg_ctx* c) {
+  if (!c) throw std::invalid_argument("null context");
+  if (!c->uploaded) throw std::invalid_argument("no problem uploaded");
+}
+void to_dev(DevBuf<double>& buf, const double* h, size_t n, cudaStream_t st) {
+  if (buf.n < std::max<size_t>(n, 1)) buf.alloc(std::max<size_t>(n, 1));
+  if (n) {
+    if (!h) throw std::invalid_argument("null pointer");
+    buf.upload(h, n, st);
+  }
+}
+void to_host(double* h, const DevBuf<double>& buf, size_t n, cudaStream_t st) {
+  if (!n) return;
+  if (!h) throw std::invalid_argument("null pointer");
+  check(cudaMemcpyAsync(h, buf.p, n * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+  check(cudaStreamSynchronize(st), "sync");
+}
+void csc_into(const sdpx_csc* m, std::vector<int64_t>& cp, std::vector<int64_t>& rv,
+              std::vector<double>& v, uint64_t cols) {
+  cp.assign(cols + 1, 0);
+  rv.clear();
+  v.clear();
+  if (!m) return;
+  if (m->cols != cols || m->values.kind != 0 || !m->colptr) throw std::invalid_argument("bad CSC");
+  for (uint64_t j = 0; j <= cols; ++j) cp[j] = (int64_t)m->colptr[j];
+  for (uint64_t p = 0; p < m->nnz; ++p) {
+    rv.push_back((int64_t)m->rowval[p]);
+    v.push_back(m->values.f64[p]);
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int32_t sdpxg_ctx_create(int32_t device, uint32_t flags, sdpxg_ctx** out) {
+  return guard([&] {
+    if (!out) throw std::invalid_argument("null pointer");
+    *out = nullptr;
+    if (flags != 0) throw std::invalid_argument("flags must be 0");
+    auto c = std::make_unique<sdpxg_ctx>();
+    c->device = device;
+    c->eng = std::make_unique<Engine>();
+    c->eng->init(device);
+    *out = c.release();
+    return 0;
+  });
+}
+
+int32_t sdpxg_ctx_destroy(sdpxg_ctx* ctx) {
+  return guard([&] {
+    delete ctx;
+    return 0;
+  });
+}
+
+int32_t sdpxg_problem_upload(sdpxg_ctx* ctx, const sdpx_csc* P, const sdpx_csc* A,
+                             const uint64_t* psd_orders, uint64_t block_count) {
+  return guard([&] {
+    if (!ctx || !A) throw std::invalid_argument("null pointer");
+    if (block_count && !psd_orders) throw std::invalid_argument("null pointer");
+    HostProblem& p = ctx->prob;
+    p = HostProblem();
+    p.n = (int)A->cols;
+    p.m = (int)A->rows;
+    csc_into(A, p.Acolptr, p.Arow, p.Aval, A->cols);
+    csc_into(P, p.Pcolptr, p.Prow, p.Pval, A->cols);
+    for (uint64_t j = 0; j < block_count; ++j) p.psd.push_back((int)psd_orders[j]);
+    p.q.assign(p.n, 0.0);
+    p.b.assign(p.m, 0.0);
+    ctx->eq.d.assign(p.n, 1.0);
+    ctx->eq.dinv.assign(p.n, 1.0);
+    ctx->eq.e.assign(p.m, 1.0);
+    ctx->eq.einv.assign(p.m, 1.0);
+    ctx->eq.c = 1.0;
+    ctx->eng->upload(p);
+    ctx->kkt = std::make_unique<HsdSolver>(*ctx->eng, p, ctx->eq, Settings());
+    ctx->uploaded = true;
+    return 0;
+  });
+}
+
+int32_t sdpxg_identity_scaling(sdpxg_ctx* ctx) {
+  return guard([&] {
+    need(ctx);
+    ctx->eng->identity_scaling();
+    check(cudaStreamSynchronize(ctx->eng->st), "sync");
+    return 0;
+  });
+}
+
+int32_t sdpxg_nt_scale(sdpxg_ctx* ctx, const double* s, const double* z, double* out_lambda,
+                       uint32_t* status) {
+  return guard([&] {
+    need(ctx);
+    Engine& E = *ctx->eng;
+    to_dev(ctx->a, s, E.m, E.st);
+    to_dev(ctx->b, z, E.m, E.st);
+    bool ok = E.nt_scale(ctx->a, ctx->b);
+    if (status) *status = ok ? 0u : 1u;
+    if (out_lambda && ok) {
+      // lambda is the diagonal of W^-T s = svec(diag(lambda)) per block
+      to_dev(ctx->c, nullptr, E.m, E.st);
+      E.cone_apply(CM_WINVT, ctx->a, ctx->c);
+      std::vector<double> h(E.m);
+      to_host(h.data(), ctx->c, E.m, E.st);
+      size_t k = 0;
+      for (const BlockDesc& bd : E.hblocks)
+        for (int i = 0; i < bd.n; ++i) out_lambda[k++] = h[bd.svec_off + i * (i + 1) / 2 + i];
+    }
+    return 0;
+  });
+}
+
+int32_t sdpxg_schur_assemble(sdpxg_ctx* ctx, double* out_schur) {
+  return guard([&] {
+    need(ctx);
+    Engine& E = *ctx->eng;
+    if (!E.assemble()) throw std::runtime_error("non-finite Schur complement");
+    if (out_schur) {
+      check(cudaMemcpyAsync(out_schur, E.Hsave(), (size_t)E.n * E.n * sizeof(double),
+                            cudaMemcpyDeviceToHost, E.st), "schur D2H");
+      check(cudaStreamSynchronize(E.st), "sync");
+    }
+    return 0;
+  });
+}
+
+int32_t sdpxg_factor(sdpxg_ctx* ctx, double shift, uint32_t dynamic, double eps, double delta,
+                     uint32_t* status) {
+  return guard([&] {
+    need(ctx);
+    bool ok = ctx->eng->factor(shift, dynamic != 0, eps, delta);
+    if (status) *status = ok ? 0u : (uint32_t)SDPXG_ST_PIVOT_FAIL;
+    return 0;
+  });
+}
+
+int32_t sdpxg_solve_many(sdpxg_ctx* ctx, const double* rhs, double* out, uint32_t ncols) {
+  return guard([&] {
+    need(ctx);
+    Engine& E = *ctx->eng;
+    for (uint32_t c = 0; c < ncols; ++c) {
+      to_dev(ctx->a, rhs + (size_t)c * E.n, E.n, E.st);
+      to_dev(ctx->b, nullptr, E.n, E.st);
+      if (!ctx->kkt->reduced_solve(ctx->a, ctx->b)) throw std::runtime_error("reduced solve failed");
+      to_host(out + (size_t)c * E.n, ctx->b, E.n, E.st);
+    }
+    return 0;
+  });
+}
+
+int32_t sdpxg_kkt_solve(sdpxg_ctx* ctx, const double* bx, const double* bz, double* x, double* z) {
+  return guard([&] {
+    need(ctx);
+    Engine& E = *ctx->eng;
+    to_dev(ctx->a, bx, E.n, E.st);
+    to_dev(ctx->b, bz, E.m, E.st);
+    to_dev(ctx->c, nullptr, E.n, E.st);
+    to_dev(ctx->d, nullptr, E.m, E.st);
+    if (!ctx->kkt->kkt_solve(ctx->a, ctx->b, ctx->c, ctx->d)) throw std::runtime_error("KKT solve failed");
+    to_host(x, ctx->c, E.n, E.st);
+    to_host(z, ctx->d, E.m, E.st);
+    return 0;
+  });
+}
+
+int32_t sdpxg_residual(sdpxg_ctx* ctx, const double* bx, const double* bz, const double* x,
+                       const double* z, double* ex, double* ez, double* norm) {
+  return guard([&] {
+    need(ctx);
+    Engine& E = *ctx->eng;
+    to_dev(ctx->a, bx, E.n, E.st);
+    to_dev(ctx->b, bz, E.m, E.st);
+    to_dev(ctx->c, x, E.n, E.st);
+    to_dev(ctx->d, z, E.m, E.st);
+    to_dev(ctx->e, nullptr, E.n, E.st);
+    to_dev(ctx->f, nullptr, E.m, E.st);
+    ctx->kkt->residual_full(ctx->a, ctx->b, ctx->c, ctx->d, ctx->e, ctx->f);
+    int s0 = E.red.add(E.st, RED_MAXABS, E.n, ctx->e, nullptr);
+    int s1 = E.red.add(E.st, RED_MAXABS, E.m, ctx->f, nullptr);
+    auto& h = E.red.fetch(E.st);
+    if (norm) *norm = std::max(h[s0], h[s1]);
+    if (ex) to_host(ex, ctx->e, E.n, E.st);
+    if (ez) to_host(ez, ctx->f, E.m, E.st);
+    return 0;
+  });
+}
+
+int32_t sdpxg_step_length(sdpxg_ctx* ctx, const double* dz, const double* ds, double amax,
+                          uint32_t mode, double* out_alpha, uint32_t* status) {
+  return guard([&] {
+    need(ctx);
+    if (!out_alpha) throw std::invalid_argument("null pointer");
+    Engine& E = *ctx->eng;
+    to_dev(ctx->a, dz, E.m, E.st);
+    to_dev(ctx->b, ds, E.m, E.st);
+    double az, as;
+    bool ok = E.step_bounds(ctx->a, ctx->b, amax, mode ? 1 : 0, &az, &as);
+    *out_alpha = std::min(az, as);
+    if (status) *status = ok ? 0u : (uint32_t)SDPXG_ST_EIG_FAIL;
+    return 0;
+  });
+}
+
+int32_t sdpxg_cone_apply(sdpxg_ctx* ctx, uint32_t op, const double* x, double* y) {
+  return guard([&] {
+    need(ctx);
+    if (op > 5) throw std::invalid_argument("unknown cone operator");
+    Engine& E = *ctx->eng;
+    to_dev(ctx->a, x, E.m, E.st);
+    to_dev(ctx->b, nullptr, E.m, E.st);
+    E.cone_apply((int)op, ctx->a, ctx->b);
+    to_host(y, ctx->b, E.m, E.st);
+    return 0;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,206 @@
+// Condensed Schur complement of the PSD rows and the constraint-operator products.
+//
+// Data layout (uploaded once per problem):
+//   For PSD block j the columns of A that touch it are stored densely, column-major,
+//   as Acol[acol_off[j] + t * tri(n_j) + r], t < k_j, with their global indices
+//   col_idx[col_ptr[j] + t].  The transpose map lists, per constraint i, its (block, t)
+//   pairs in cone order: c2b_ptr[i] .. c2b_ptr[i+1] into c2b_blk / c2b_loc.
+//
+// Schur entry (kkt/condensed/psd.rs:1120-1570, scaling.rs:7-81):
+//   H_ab = sum_j < A_aj , Ginv_j A_bj Ginv_j >  (+ P_ab)
+// computed as T = svec(Ginv A Ginv) per column (k_schur_transform), one grouped GEMM
+// S_j = Acol_j' T_j per block (k_schur_block_gemm), and a deterministic cone-order gather
+// into the dense m x m matrix (k_schur_gather).
+#include "common.cuh"
+
+namespace {
+constexpr int kMat = SDPXG_LD * SDPXG_NMAX;
+}
+
+// One CTA per (block, column) work item: item w -> block wblk[w], local column wloc[w].
+extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
+k_schur_transform(const BlockDesc* __restrict__ blocks, const int* __restrict__ wblk,
+                  const int* __restrict__ wloc, const long* __restrict__ acol_off,
+                  const double* __restrict__ Ginv, const double* __restrict__ Acol,
+                  double* __restrict__ Tcol) {
+  extern __shared__ double smem[];
+  const int j = wblk[blockIdx.x], t = wloc[blockIdx.x];
+  const BlockDesc bd = blocks[j];
+  const int n = bd.n;
+  const int tn = n * (n + 1) / 2;
+  double* G = smem;
+  double* X = G + kMat;
+  double* Y = X + kMat;
+  cta_load_mat(G, Ginv + bd.mat_off, n);
+  const long off = acol_off[j] + (long)t * tn;
+  cta_load_smat(X, Acol + off, n);
+  __syncthreads();
+  cta_gemm(Y, G, false, X, false, n);  // Y = Ginv A
+  __syncthreads();
+  cta_gemm(X, Y, false, G, false, n);  // X = Ginv A Ginv
+  __syncthreads();
+  cta_store_svec(Tcol + off, X, n);
+}
+
+// Grouped GEMM S_j = Acol_j' * Tcol_j (k_j x k_j, inner tri(n_j)).  Tile list entries
+// (block, tile row, tile col) of 32 x 32 output tiles.
+#define SCHUR_TILE 32
+#define SCHUR_KC 32
+extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
+k_schur_block_gemm(const BlockDesc* __restrict__ blocks, const int* __restrict__ tiles,
+                   const int* __restrict__ kcount, const long* __restrict__ acol_off,
+                   const long* __restrict__ s_off, const double* __restrict__ Acol,
+                   const double* __restrict__ Tcol, double* __restrict__ S) {
+  __shared__ double As[SCHUR_KC][SCHUR_TILE + 1];
+  __shared__ double Ts[SCHUR_KC][SCHUR_TILE + 1];
+  const int j = tiles[3 * blockIdx.x], ti = tiles[3 * blockIdx.x + 1],
+            tj = tiles[3 * blockIdx.x + 2];
+  const int n = blocks[j].n;
+  const int tn = n * (n + 1) / 2;
+  const int k = kcount[j];
+  const double* A = Acol + acol_off[j];
+  const double* T = Tcol + acol_off[j];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const int a0 = ti * SCHUR_TILE + 2 * tx, b0 = tj * SCHUR_TILE + 2 * ty;
+  double c00 = 0, c01 = 0, c10 = 0, c11 = 0;
+  for (int r0 = 0; r0 < tn; r0 += SCHUR_KC) {
+    for (int e = threadIdx.x; e < SCHUR_KC * SCHUR_TILE; e += blockDim.x) {
+      int rr = e % SCHUR_KC, cc = e / SCHUR_KC;
+      int r = r0 + rr;
+      int ca = ti * SCHUR_TILE + cc, cb = tj * SCHUR_TILE + cc;
+      As[rr][cc] = (r < tn && ca < k) ? A[(long)ca * tn + r] : 0.0;
+      Ts[rr][cc] = (r < tn && cb < k) ? T[(long)cb * tn + r] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int rr = 0; rr < SCHUR_KC; ++rr) {
+      double x0 = As[rr][2 * tx], x1 = As[rr][2 * tx + 1];
+      double y0 = Ts[rr][2 * ty], y1 = Ts[rr][2 * ty + 1];
+      c00 = fma(x0, y0, c00);
+      c01 = fma(x0, y1, c01);
+      c10 = fma(x1, y0, c10);
+      c11 = fma(x1, y1, c11);
+    }
+    __syncthreads();
+  }
+  double* out = S + s_off[j];
+  if (a0 < k && b0 < k) out[a0 + (long)b0 * k] = c00;
+  if (a0 < k && b0 + 1 < k) out[a0 + (long)(b0 + 1) * k] = c01;
+  if (a0 + 1 < k && b0 < k) out[a0 + 1 + (long)b0 * k] = c10;
+  if (a0 + 1 < k && b0 + 1 < k) out[a0 + 1 + (long)(b0 + 1) * k] = c11;
+}
+
+// H (m x m, full, column-major) = sum over shared blocks of S_j[la, lb], in cone order.
+// One thread per (a, b) with a <= b; both triangles written (symmetrised by construction).
+extern "C" __global__ void k_schur_gather(int m, const int* __restrict__ c2b_ptr,
+                                          const int* __restrict__ c2b_blk,
+                                          const int* __restrict__ c2b_loc,
+                                          const int* __restrict__ kcount,
+                                          const long* __restrict__ s_off,
+                                          const double* __restrict__ S, double* __restrict__ H) {
+  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long total = (long)m * m;
+  if (idx >= total) return;
+  int a = (int)(idx % m), b = (int)(idx / m);
+  if (a > b) return;
+  int pa = c2b_ptr[a], ea = c2b_ptr[a + 1], pb = c2b_ptr[b], eb = c2b_ptr[b + 1];
+  double acc = 0.0;
+  while (pa < ea && pb < eb) {
+    int ja = c2b_blk[pa], jb = c2b_blk[pb];
+    if (ja < jb) {
+      ++pa;
+    } else if (jb < ja) {
+      ++pb;
+    } else {
+      const int k = kcount[ja];
+      const double* Sj = S + s_off[ja];
+      int la = c2b_loc[pa], lb = c2b_loc[pb];
+      // symmetric in exact arithmetic: average the two computed halves
+      acc += 0.5 * (Sj[la + (long)lb * k] + Sj[lb + (long)la * k]);
+      ++pa;
+      ++pb;
+    }
+  }
+  H[a + (long)b * m] = acc;
+  H[b + (long)a * m] = acc;
+}
+
+// H += sym(P) for P given as an upper-triangular CSC (n x n).
+extern "C" __global__ void k_add_upper_csc(int n, const int* __restrict__ colptr,
+                                           const int* __restrict__ rowval,
+                                           const double* __restrict__ val, double* __restrict__ H) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  for (int p = colptr[j]; p < colptr[j + 1]; ++p) {
+    int i = rowval[p];
+    if (i > j) continue;
+    H[i + (long)j * n] += val[p];
+    if (i != j) H[j + (long)i * n] += val[p];
+  }
+}
+
+// y[rows of block j] = alpha * Acol_j x[cols_j] + beta * y   (one CTA per block, thread/row)
+extern "C" __global__ void k_op_forward(const BlockDesc* __restrict__ blocks,
+                                        const int* __restrict__ kcount,
+                                        const int* __restrict__ col_ptr,
+                                        const int* __restrict__ col_idx,
+                                        const long* __restrict__ acol_off,
+                                        const double* __restrict__ Acol,
+                                        const double* __restrict__ x, long ldx, double alpha,
+                                        double beta, double* __restrict__ y, long ldy) {
+  const int j = blockIdx.x;
+  const BlockDesc bd = blocks[j];
+  const int tn = bd.n * (bd.n + 1) / 2;
+  const int k = kcount[j];
+  const double* A = Acol + acol_off[j];
+  const int* cols = col_idx + col_ptr[j];
+  const double* xc = x + (long)blockIdx.y * ldx;
+  double* yc = y + (long)blockIdx.y * ldy;
+  for (int r = threadIdx.x; r < tn; r += blockDim.x) {
+    double acc = 0.0;
+    for (int t = 0; t < k; ++t) acc = fma(A[(long)t * tn + r], xc[cols[t]], acc);
+    double prev = (beta == 0.0) ? 0.0 : beta * yc[bd.svec_off + r];
+    yc[bd.svec_off + r] = alpha * acc + prev;
+  }
+}
+
+// Per-block partial adjoint p[acol column] = Acol_j[:, t] . z_j  (one warp per column)
+extern "C" __global__ void k_op_adjoint_partial(const BlockDesc* __restrict__ blocks,
+                                                const int* __restrict__ wblk,
+                                                const int* __restrict__ wloc,
+                                                const int* __restrict__ col_ptr,
+                                                const long* __restrict__ acol_off,
+                                                const double* __restrict__ Acol,
+                                                const double* __restrict__ z, long ldz,
+                                                double* __restrict__ p, long ldp, int nwork) {
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= nwork) return;
+  const int j = wblk[w], t = wloc[w];
+  const BlockDesc bd = blocks[j];
+  const int tn = bd.n * (bd.n + 1) / 2;
+  const double* A = Acol + acol_off[j] + (long)t * tn;
+  const double* zc = z + (long)blockIdx.y * ldz + bd.svec_off;
+  double acc = 0.0;
+  for (int r = lane; r < tn; r += 32) acc = fma(A[r], zc[r], acc);
+  acc = warp_sum(acc);
+  if (lane == 0) p[(long)blockIdx.y * ldp + col_ptr[j] + t] = acc;
+}
+
+// y[i] = alpha * sum over (block, t) of constraint i of p[...] + beta * y[i]  (cone order)
+extern "C" __global__ void k_op_adjoint_gather(int n, const int* __restrict__ c2b_ptr,
+                                               const int* __restrict__ c2b_blk,
+                                               const int* __restrict__ c2b_loc,
+                                               const int* __restrict__ col_ptr,
+                                               const double* __restrict__ p, long ldp,
+                                               double alpha, double beta, double* __restrict__ y,
+                                               long ldy) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* pc = p + (long)blockIdx.y * ldp;
+  double acc = 0.0;
+  for (int q = c2b_ptr[i]; q < c2b_ptr[i + 1]; ++q) acc += pc[col_ptr[c2b_blk[q]] + c2b_loc[q]];
+  double* yc = y + (long)blockIdx.y * ldy;
+  double prev = (beta == 0.0) ? 0.0 : beta * yc[i];
+  yc[i] = alpha * acc + prev;
+}

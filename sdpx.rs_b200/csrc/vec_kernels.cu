@@ -1,0 +1,95 @@
+// Vector kernels of the interior-point iteration: linear combinations and deterministic
+// reductions (fixed grid, fixed order: repeated runs give bitwise identical scalars).
+#include "common.cuh"
+
+#define RED_BLOCKS 148
+#define RED_THREADS 256
+
+// out = a*x + b*y + c*w  (null pointers contribute zero; out may alias any input)
+extern "C" __global__ void k_lincomb(long n, double a, const double* x, double b, const double* y,
+                                     double c, const double* w, double* out) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    if (x) v = a * x[i];
+    if (y) v = fma(b, y[i], v);
+    if (w) v = fma(c, w[i], v);
+    out[i] = v;
+  }
+}
+
+// op 0: sum x*y;  op 1: sum (x*y)^2 (scaled 2-norm squared, y = scales or null);
+// op 2: max |x*y|;  op 3: all finite (1.0 / 0.0) of x
+__device__ __forceinline__ double red_elem(int op, const double* x, const double* y, long i) {
+  double xv = x[i];
+  double yv = y ? y[i] : 1.0;
+  switch (op) {
+    case 0: return xv * yv;
+    case 1: { double t = xv * yv; return t * t; }
+    case 2: return fabs(xv * yv);
+    default: return isfinite(xv) ? 1.0 : 0.0;
+  }
+}
+
+__device__ __forceinline__ double red_combine(int op, double a, double b) {
+  if (op == 2) return fmax(a, b);
+  if (op == 3) return fmin(a, b);
+  return a + b;
+}
+
+__device__ __forceinline__ double red_identity(int op) { return op == 3 ? 1.0 : 0.0; }
+
+extern "C" __global__ void __launch_bounds__(RED_THREADS)
+k_reduce_partial(int op, long n, const double* __restrict__ x, const double* __restrict__ y,
+                 double* __restrict__ partial) {
+  __shared__ double red[RED_THREADS / 32];
+  double acc = red_identity(op);
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    acc = red_combine(op, acc, red_elem(op, x, y, i));
+  for (int o = 16; o > 0; o >>= 1) acc = red_combine(op, acc, __shfl_xor_sync(0xffffffffu, acc, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = red_identity(op);
+    for (int w = 0; w < RED_THREADS / 32; ++w) v = red_combine(op, v, red[w]);
+    partial[blockIdx.x] = v;
+  }
+}
+
+extern "C" __global__ void k_reduce_final(int op, int nparts, const double* __restrict__ partial,
+                                          double* __restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double v = red_identity(op);
+    for (int p = 0; p < nparts; ++p) v = red_combine(op, v, partial[p]);
+    *out = v;
+  }
+}
+
+// Diagonal max |H_ii| of a dense m x m matrix (for the proportional static shift).
+extern "C" __global__ void k_diag_absmax(const double* __restrict__ H, int m,
+                                         double* __restrict__ out) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) acc = fmax(acc, fabs(H[i + (long)i * m]));
+  acc = warp_max(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v = fmax(v, red[w]);
+    *out = v;
+  }
+}
+
+// y = alpha * P x + beta * y for P in CSR (both triangles), one thread per row.
+extern "C" __global__ void k_csr_spmv(int n, const int* __restrict__ rowptr,
+                                      const int* __restrict__ colidx,
+                                      const double* __restrict__ val, const double* __restrict__ x,
+                                      double alpha, double beta, double* __restrict__ y) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double acc = 0.0;
+  for (int p = rowptr[r]; p < rowptr[r + 1]; ++p) acc = fma(val[p], x[colidx[p]], acc);
+  y[r] = alpha * acc + (beta == 0.0 ? 0.0 : beta * y[r]);
+}

@@ -1,0 +1,312 @@
+"""Host-side mirror of the reference solver API over the CUDA library.
+
+Mirrors ``DefaultSolver::new(&P, &q, &A, &b, &cones, settings)`` /
+``solver.solve()`` / ``solver.solution`` / ``solver.info`` of the reference
+(crates/solver/src/solver/default/solver.rs:260, solution.rs, info.rs) with the same
+argument meaning, status names and error behaviour (invalid input raises, like the
+reference's ``Result`` error), calling the reference-compatible C ABI ``sdpx_*`` of
+libsdpx_b200.so.  ``KernelContext`` wraps the kernel-level ``sdpxg_*`` entry points.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib
+from ._lib import dptr
+
+STATUS_NAMES = {
+    0: "Unsolved", 1: "Solved", 2: "PrimalInfeasible", 3: "DualInfeasible", 4: "AlmostSolved",
+    5: "AlmostPrimalInfeasible", 6: "AlmostDualInfeasible", 7: "MaxIterations", 8: "MaxTime",
+    9: "NumericalError", 10: "InsufficientProgress", 11: "CallbackTerminated", 12: "DualFeasible",
+}
+CONE_KINDS = {"zero": 0, "nonneg": 1, "soc": 2, "psd": 3}
+
+
+def PSDTriangleConeT(n: int) -> Tuple[str, int]:
+    return ("psd", int(n))
+
+
+@dataclass
+class DefaultSettings:
+    """Subset of DefaultSettings (default/settings.rs:17-314) carried by the C ABI."""
+    max_iter: int = 200
+    time_limit: float = float("inf")
+    verbose: bool = False
+    tol_gap_abs: Optional[float] = None
+    tol_gap_rel: Optional[float] = None
+    tol_feas: Optional[float] = None
+    tol_infeas_abs: Optional[float] = None
+    tol_infeas_rel: Optional[float] = None
+    equilibrate_enable: bool = True
+    presolve_enable: bool = True
+    chordal_decomposition_enable: bool = True
+    kkt_form: str = "auto"
+    precision_bits: int = 53
+
+    def to_c(self) -> Tuple[_lib.Settings, list]:
+        s = _lib.Settings()
+        _lib.call("sdpx_default_settings_v4", C.byref(s))
+        s.max_iter = self.max_iter
+        s.time_limit = self.time_limit
+        s.verbose = int(bool(self.verbose))
+        s.precision_bits = self.precision_bits
+        s.kkt_form = {"auto": 0, "augmented": 1, "condensed": 2}[self.kkt_form]
+        s.preprocessing_flags = (int(self.equilibrate_enable) | 2 * int(self.presolve_enable)
+                                 | 4 * int(self.chordal_decomposition_enable))
+        keep = []
+        for name in ("tol_gap_abs", "tol_gap_rel", "tol_feas", "tol_infeas_abs", "tol_infeas_rel"):
+            v = getattr(self, name)
+            if v is not None:
+                b = repr(float(v)).encode()
+                keep.append(b)
+                setattr(s, name, b)
+        return s, keep
+
+
+@dataclass
+class Solution:
+    x: np.ndarray
+    z: np.ndarray
+    s: np.ndarray
+    status: str
+    status_code: int
+    obj_val: float
+    obj_val_dual: float
+    r_prim: float
+    r_dual: float
+    iterations: int
+    solve_time: float
+
+
+@dataclass
+class SolveInfo:
+    status: str
+    iterations: int
+    cost_primal: float
+    cost_dual: float
+    res_primal: float
+    res_dual: float
+    gap_abs: float
+    gap_rel: float
+    solve_time: float
+    phase_times: dict = field(default_factory=dict)
+    counts: dict = field(default_factory=dict)
+
+
+def _scalars(a: np.ndarray) -> _lib.Scalars:
+    s = _lib.Scalars()
+    s.kind = 0
+    s.reserved = 0
+    s.count = a.size
+    s.f64 = dptr(a)
+    s.decimal = None
+    return s
+
+
+class _CscHold:
+    """Keeps the numpy buffers of a C CSC view alive."""
+
+    def __init__(self, M: sp.spmatrix):
+        M = sp.csc_matrix(M, dtype=np.float64)
+        M.sort_indices()
+        self.colptr = np.ascontiguousarray(M.indptr, dtype=np.uint64)
+        self.rowval = np.ascontiguousarray(M.indices, dtype=np.uint64)
+        self.values = np.ascontiguousarray(M.data, dtype=np.float64)
+        c = _lib.Csc()
+        c.rows, c.cols, c.nnz = M.shape[0], M.shape[1], M.nnz
+        c.colptr = self.colptr.ctypes.data_as(_lib.PU64)
+        c.rowval = self.rowval.ctypes.data_as(_lib.PU64)
+        c.values = _scalars(self.values)
+        self.c = c
+
+
+class DefaultSolver:
+    """GPU solve through the reference-compatible C ABI (sdpx_prepare / sdpx_solve)."""
+
+    def __init__(self, P, q, A, b, cones: Sequence[Tuple[str, int]],
+                 settings: Optional[DefaultSettings] = None):
+        settings = settings or DefaultSettings()
+        A = sp.csc_matrix(A, dtype=np.float64)
+        n = A.shape[1]
+        P = sp.csc_matrix((n, n)) if P is None else sp.triu(sp.csc_matrix(P, dtype=np.float64)).tocsc()
+        self._q = np.ascontiguousarray(q, dtype=np.float64)
+        self._b = np.ascontiguousarray(b, dtype=np.float64)
+        self._P, self._A = _CscHold(P), _CscHold(A)
+        cone_arr = (_lib.Cone * max(len(cones), 1))()
+        for i, (kind, d) in enumerate(cones):
+            cone_arr[i].kind = CONE_KINDS[kind]
+            cone_arr[i].reserved = 0
+            cone_arr[i].dim = int(d)
+            cone_arr[i].alpha = _scalars(np.zeros(0))
+        cs, keep = settings.to_c()
+        h = C.c_void_p()
+        _lib.call("sdpx_prepare", C.byref(self._P.c), C.byref(_scalars(self._q)), C.byref(self._A.c),
+                  C.byref(_scalars(self._b)), cone_arr, len(cones), C.byref(cs), C.byref(h))
+        self._h = h
+        self.n, self.m = n, A.shape[0]
+        self.solution: Optional[Solution] = None
+        self.info: Optional[SolveInfo] = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.load().sdpx_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def solve(self) -> Solution:
+        _lib.call("sdpx_solve", self._h)
+        info = _lib.Info()
+        _lib.call("sdpx_get_info", self._h, C.byref(info))
+        need = C.c_uint64()
+        _lib.call("sdpx_result_f64", self._h, None, 0, C.byref(need))
+        out = np.empty(need.value)
+        _lib.call("sdpx_result_f64", self._h, dptr(out), need.value, C.byref(need))
+        n, m = self.n, self.m
+        times = np.zeros(7)
+        counts = np.zeros(4, dtype=np.uint64)
+        _lib.call("sdpx_b200_phase_times", self._h, dptr(times), counts.ctypes.data_as(_lib.PU64))
+        status = STATUS_NAMES.get(info.status, str(info.status))
+        self.solution = Solution(x=out[:n].copy(), z=out[n:n + m].copy(), s=out[n + m:n + 2 * m].copy(),
+                                 status=status, status_code=info.status, obj_val=out[-6],
+                                 obj_val_dual=out[-5], r_prim=out[-4], r_dual=out[-3],
+                                 iterations=info.iterations, solve_time=info.solve_time)
+        names = ["scale", "assemble", "factor", "kkt_solve", "step", "residual", "other"]
+        self.info = SolveInfo(status=status, iterations=info.iterations, cost_primal=info.objective,
+                              cost_dual=info.dual_objective, res_primal=info.primal_residual,
+                              res_dual=info.dual_residual, gap_abs=info.gap_abs,
+                              gap_rel=info.gap_rel, solve_time=info.solve_time,
+                              phase_times=dict(zip(names, times.tolist())),
+                              counts=dict(zip(["factorizations", "kkt_solves", "outer_refinements",
+                                               "inner_refinements"], counts.tolist())))
+        return self.solution
+
+    KERNEL_PHASES = ["scale", "assemble", "factor", "trisolve", "cone", "step", "symv"]
+
+    def set_kernel_timing(self, on: bool):
+        _lib.call("sdpx_b200_set_kernel_timing", self._h, int(bool(on)))
+
+    def kernel_times(self) -> dict:
+        ms = np.zeros(7)
+        cnt = np.zeros(7, dtype=np.uint64)
+        _lib.call("sdpx_b200_kernel_times", self._h, dptr(ms), cnt.ctypes.data_as(_lib.PU64))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.KERNEL_PHASES)}
+
+    def update(self, q, b):
+        self._q = np.ascontiguousarray(q, dtype=np.float64)
+        self._b = np.ascontiguousarray(b, dtype=np.float64)
+        _lib.call("sdpx_update", self._h, C.byref(_scalars(self._q)), C.byref(_scalars(self._b)))
+
+    def solver_name(self) -> str:
+        need = C.c_uint64()
+        _lib.call("sdpx_get_solver_name", self._h, None, 0, C.byref(need))
+        buf = C.create_string_buffer(need.value)
+        _lib.call("sdpx_get_solver_name", self._h, buf, need.value, C.byref(need))
+        return buf.value.decode()
+
+    def result_decimal(self) -> List[str]:
+        need = C.c_uint64()
+        _lib.call("sdpx_result_decimal", self._h, None, 0, C.byref(need))
+        buf = C.create_string_buffer(need.value)
+        _lib.call("sdpx_result_decimal", self._h, buf, need.value, C.byref(need))
+        return [s.decode() for s in buf.raw[:need.value].split(b"\0")[:-1]]
+
+
+def solve_problem(prob, settings: Optional[DefaultSettings] = None) -> DefaultSolver:
+    """Prepare and solve a ``problems.ConicProblem``."""
+    s = DefaultSolver(prob.P, prob.q, prob.A, prob.b, prob.cones, settings)
+    s.solve()
+    return s
+
+
+class KernelContext:
+    """The kernel-level ABI (sdpxg_*): one hot-path operation per call on host arrays."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _lib.call("sdpxg_ctx_create", device, 0, C.byref(h))
+        self._h = h
+        self.n = self.m = 0
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.load().sdpxg_ctx_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def upload(self, A, psd_orders: Sequence[int], P=None):
+        A = sp.csc_matrix(A, dtype=np.float64)
+        self._A = _CscHold(A)
+        self._P = _CscHold(sp.triu(sp.csc_matrix(P)).tocsc()) if P is not None else None
+        orders = np.ascontiguousarray(psd_orders, dtype=np.uint64)
+        _lib.call("sdpxg_problem_upload", self._h, C.byref(self._P.c) if self._P else None,
+                  C.byref(self._A.c), orders.ctypes.data_as(_lib.PU64), orders.size)
+        self.m, self.n = A.shape
+        self.nlam = int(orders.sum())
+
+    def nt_scale(self, s, z):
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        lam = np.empty(self.nlam)
+        st = C.c_uint32()
+        _lib.call("sdpxg_nt_scale", self._h, dptr(s), dptr(z), dptr(lam), C.byref(st))
+        return lam, st.value
+
+    def identity_scaling(self):
+        _lib.call("sdpxg_identity_scaling", self._h)
+
+    def schur(self):
+        H = np.empty((self.n, self.n), order="F")
+        _lib.call("sdpxg_schur_assemble", self._h, H.ctypes.data_as(_lib.PD))
+        return H
+
+    def factor(self, shift, dynamic=True, eps=1e-13, delta=2e-7):
+        st = C.c_uint32()
+        _lib.call("sdpxg_factor", self._h, float(shift), int(dynamic), eps, delta, C.byref(st))
+        return st.value
+
+    def solve_many(self, rhs):
+        rhs = np.asfortranarray(np.atleast_2d(np.asarray(rhs, dtype=np.float64).T).T)
+        out = np.empty_like(rhs, order="F")
+        _lib.call("sdpxg_solve_many", self._h, rhs.ctypes.data_as(_lib.PD),
+                  out.ctypes.data_as(_lib.PD), rhs.shape[1])
+        return out
+
+    def kkt_solve(self, bx, bz):
+        bx = np.ascontiguousarray(bx, dtype=np.float64)
+        bz = np.ascontiguousarray(bz, dtype=np.float64)
+        x, z = np.empty(self.n), np.empty(self.m)
+        _lib.call("sdpxg_kkt_solve", self._h, dptr(bx), dptr(bz), dptr(x), dptr(z))
+        return x, z
+
+    def residual(self, bx, bz, x, z):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (bx, bz, x, z)]
+        ex, ez = np.empty(self.n), np.empty(self.m)
+        nrm = C.c_double()
+        _lib.call("sdpxg_residual", self._h, *[dptr(a) for a in arrs], dptr(ex), dptr(ez), C.byref(nrm))
+        return ex, ez, nrm.value
+
+    def step_length(self, dz, ds, amax, mode=0):
+        dz = np.ascontiguousarray(dz, dtype=np.float64)
+        ds = np.ascontiguousarray(ds, dtype=np.float64)
+        a = C.c_double()
+        st = C.c_uint32()
+        _lib.call("sdpxg_step_length", self._h, dptr(dz), dptr(ds), float(amax), int(mode),
+                  C.byref(a), C.byref(st))
+        return a.value, st.value
+
+    def cone_apply(self, op, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.m)
+        _lib.call("sdpxg_cone_apply", self._h, int(op), dptr(x), dptr(y))
+        return y
