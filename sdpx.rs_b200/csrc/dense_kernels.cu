@@ -1,0 +1,314 @@
+// Dense Cholesky of the Schur complement with the reference's dynamic pivot rule, the explicit
+// inverse of its factor, and the GEMVs that apply it.
+//
+// Factorisation H + eps I = U'U (upper), right-looking over 64 x 64 tiles
+// (kkt/ldl/dense_block.rs:334-365 potrf_dynamic, 370-388 potrf_tile, 515-594 tiled_potrf):
+//   k_potrf_diag   factor the diagonal tile with the dynamic pivot rule; store Dinv = U_kk^-1
+//   k_trsm_panel   U[k, j] = U_kk^-T H[k, j] for the tiles right of the diagonal
+//   k_syrk_update  H[i, j] -= U[k, i]' U[k, j] on the upper trailing tiles
+// Inverse X = U^-1, recursive over tile groups: with U = [U11 U12; 0 U22],
+//   X12 = -X11 (U12 X22), level by level (k_trinv_level, two batched GEMM phases per level),
+// so every level is one wide batched GEMM instead of a serial chain of tiles.
+// Solves of an iteration then read X twice: y = X' b (upper, by columns) and x = X y (through
+// the stored transpose, by columns) -- coalesced GEMVs (the reference substitutes tile by tile,
+// dense_block.rs:604-669; refinement against the unshifted matrix makes the two equivalent).
+#include "common.cuh"
+
+#define CH_NB 64
+#define CH_LD (CH_NB + 1)
+
+// F = Hsave + eps I (copy), diag0 = diag(F).
+extern "C" __global__ void k_shifted_copy(const double* __restrict__ Hs, double* __restrict__ F,
+                                          int m, double eps, double* __restrict__ diag0) {
+  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long total = (long)m * m;
+  for (; idx < total; idx += (long)gridDim.x * blockDim.x) {
+    int i = (int)(idx % m), j = (int)(idx / m);
+    double v = Hs[idx];
+    if (i == j) {
+      v += eps;
+      diag0[i] = v;
+    }
+    F[idx] = v;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Diagonal tile: lagged upper Cholesky with the dynamic pivot rule, then Dinv = U^-1.
+// Dynamic shared memory: two CH_NB x CH_LD tiles.
+extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
+k_potrf_diag(double* __restrict__ H, int m, int kb, double eps, double delta, int dynamic,
+             const double* __restrict__ diag0, double* __restrict__ Dinv,
+             uint32_t* __restrict__ status) {
+  extern __shared__ double pd_sm[];
+  double* A = pd_sm;
+  double* X = A + CH_NB * CH_LD;
+  __shared__ double dmod[CH_NB];
+  const int k0 = kb * CH_NB;
+  const int nb = min(CH_NB, m - k0);
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    int i = e % nb, j = e / nb;
+    if (i <= j) A[i + j * CH_LD] = H[(k0 + i) + (long)(k0 + j) * m];
+  }
+  for (int k = 0; k < nb; ++k) {
+    __syncthreads();
+    double d = A[k + k * CH_LD];
+    bool fail = !isfinite(d);
+    if (!fail && dynamic && d <= eps) {
+      // a pivot within rounding of zero becomes delta; a clearly negative one fails
+      if (d < -64.0 * 2.220446049250313e-16 * nb * fabs(diag0[k0 + k])) fail = true;
+      else d = delta;
+    }
+    if (!fail && !(d > 0.0)) fail = true;
+    if (fail) {
+      if (threadIdx.x == 0) atomicOr(status, SDPXG_ST_PIVOT_FAIL);
+      return;  // uniform: every thread read the same pivot
+    }
+    if (threadIdx.x == 0) dmod[k] = d;
+    const int rem = nb - k - 1;
+    const double dinv = 1.0 / d;
+    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
+      int i = k + 1 + e % rem, j = k + 1 + e / rem;
+      if (i > j) continue;
+      A[i + j * CH_LD] -= A[k + i * CH_LD] * A[k + j * CH_LD] * dinv;
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    int i = e % nb, j = e / nb;
+    if (i > j) continue;
+    double r = sqrt(dmod[i]);
+    double u = (i == j) ? r : A[i + j * CH_LD] / r;
+    A[i + j * CH_LD] = u;
+    H[(k0 + i) + (long)(k0 + j) * m] = u;
+  }
+  __syncthreads();
+  // Dinv = U^-1 (upper): column j by back substitution in shared memory.
+  for (int j = threadIdx.x; j < CH_NB; j += blockDim.x) {
+    for (int i = CH_NB - 1; i > j; --i) X[i + j * CH_LD] = 0.0;
+    if (j < nb) {
+      X[j + j * CH_LD] = 1.0 / A[j + j * CH_LD];
+      for (int i = j - 1; i >= 0; --i) {
+        double acc = 0.0;
+        for (int l = i + 1; l <= j; ++l) acc = fma(A[i + l * CH_LD], X[l + j * CH_LD], acc);
+        X[i + j * CH_LD] = -acc / A[i + i * CH_LD];
+      }
+    } else {
+      for (int i = 0; i <= j; ++i) X[i + j * CH_LD] = 0.0;
+    }
+  }
+  __syncthreads();
+  double* D = Dinv + (long)kb * CH_NB * CH_NB;
+  for (int e = threadIdx.x; e < CH_NB * CH_NB; e += blockDim.x)
+    D[e] = X[(e % CH_NB) + (e / CH_NB) * CH_LD];
+}
+
+// ------------------------------------------------------------------------------------
+extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
+k_trsm_panel(double* __restrict__ H, int m, int kb, const double* __restrict__ Dinv) {
+  extern __shared__ double sm[];
+  double* D = sm;                 // CH_NB x CH_LD
+  double* P = D + CH_NB * CH_LD;  // CH_NB x CH_LD
+  const int k0 = kb * CH_NB, nb = min(CH_NB, m - k0);
+  const int cb = kb + 1 + blockIdx.x;
+  const int c0 = cb * CH_NB, nc = min(CH_NB, m - c0);
+  const double* Dg = Dinv + (long)kb * CH_NB * CH_NB;
+  for (int e = threadIdx.x; e < CH_NB * CH_NB; e += blockDim.x)
+    D[(e % CH_NB) + (e / CH_NB) * CH_LD] = Dg[e];
+  for (int e = threadIdx.x; e < nb * nc; e += blockDim.x) {
+    int i = e % nb, c = e / nb;
+    P[i + c * CH_LD] = H[(k0 + i) + (long)(c0 + c) * m];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nb * nc; e += blockDim.x) {
+    int i = e % nb, c = e / nb;
+    double acc = 0.0;
+    for (int l = 0; l <= i; ++l) acc = fma(D[l + i * CH_LD], P[l + c * CH_LD], acc);
+    H[(k0 + i) + (long)(c0 + c) * m] = acc;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Trailing update on upper tiles; blockIdx.x enumerates (ib <= jb) over the T x T trailing
+// tile grid in column order.
+extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
+k_syrk_update(double* __restrict__ H, int m, int kb) {
+  extern __shared__ double syrk_sm[];
+  double (*Ui)[CH_NB + 2] = reinterpret_cast<double (*)[CH_NB + 2]>(syrk_sm);
+  double (*Uj)[CH_NB + 2] = reinterpret_cast<double (*)[CH_NB + 2]>(syrk_sm + CH_NB * (CH_NB + 2));
+  const int t = blockIdx.x;
+  int jb = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while (jb * (jb + 1) / 2 > t) --jb;
+  while ((jb + 1) * (jb + 2) / 2 <= t) ++jb;
+  int ib = t - jb * (jb + 1) / 2;
+  ib += kb + 1;
+  jb += kb + 1;
+  const int k0 = kb * CH_NB, nb = min(CH_NB, m - k0);
+  const int i0 = ib * CH_NB, ni = min(CH_NB, m - i0);
+  const int j0 = jb * CH_NB, nj = min(CH_NB, m - j0);
+  for (int e = threadIdx.x; e < CH_NB * CH_NB; e += blockDim.x) {
+    int l = e % CH_NB, c = e / CH_NB;
+    Ui[l][c] = (l < nb && c < ni) ? H[(k0 + l) + (long)(i0 + c) * m] : 0.0;
+    Uj[l][c] = (l < nb && c < nj) ? H[(k0 + l) + (long)(j0 + c) * m] : 0.0;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int l = 0; l < nb; ++l) {
+    double x[4], y[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) x[a] = Ui[l][tx + 16 * a];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) y[b] = Uj[l][ty + 16 * b];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = fma(x[a], y[b], acc[a][b]);
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      int r = tx + 16 * a, c = ty + 16 * b;
+      if (r < ni && c < nj && (ib < jb || r <= c)) H[(i0 + r) + (long)(j0 + c) * m] -= acc[a][b];
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Inverse of the factor.  Diagonal tiles: X_ii = Dinv_i (stored in Uinv and, transposed, UinvT).
+extern "C" __global__ void k_trtri_diag(int m, const double* __restrict__ Dinv,
+                                        double* __restrict__ Uinv, double* __restrict__ UinvT) {
+  const int ib = blockIdx.x;
+  const int i0 = ib * CH_NB, ni = min(CH_NB, m - i0);
+  const double* D = Dinv + (long)ib * CH_NB * CH_NB;
+  for (int e = threadIdx.x; e < ni * ni; e += blockDim.x) {
+    int r = e % ni, c = e / ni;
+    double v = D[r + c * CH_NB];  // zero below the diagonal
+    Uinv[(i0 + r) + (long)(i0 + c) * m] = v;
+    UinvT[(i0 + c) + (long)(i0 + r) * m] = v;
+  }
+}
+
+// Level `level` >= 1 of the recursive inverse: groups of 2^level tiles, left half L (2^(level-1)
+// full tiles), right half R (possibly ragged).  phase 0: T = U[L,R] X[R,R] into Tmp[L,R];
+// phase 1: X[L,R] = -X[L,L] T.  X's strictly lower part is never stored: loads mask it to zero.
+// grid = (row tiles of L, column tiles of R, groups).  Dynamic shared memory: two tiles.
+extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
+k_trinv_level(const double* __restrict__ F, double* __restrict__ Uinv, double* __restrict__ UinvT,
+              double* __restrict__ Tmp, int n, int level, int phase) {
+  extern __shared__ double tl_sm[];
+  double* As = tl_sm;               // [r + k * CH_LD]
+  double* Bs = As + CH_NB * CH_LD;  // [k + c * CH_LD]
+  const int g = 1 << level, h = g >> 1;
+  const int L0 = blockIdx.z * g * CH_NB;
+  const int R0 = L0 + h * CH_NB;
+  if (R0 >= n) return;
+  const int Ln = h * CH_NB;
+  const int Rn = min(R0 + h * CH_NB, n) - R0;
+  const int tm = blockIdx.x, tn = blockIdx.y;
+  if (tm * CH_NB >= Ln || tn * CH_NB >= Rn) return;
+  const double* A;
+  const double* B;
+  int ar, ac, br, bc, K;
+  if (phase == 0) {
+    A = F; ar = L0; ac = R0; B = Uinv; br = R0; bc = R0; K = Rn;
+  } else {
+    A = Uinv; ar = L0; ac = L0; B = Tmp; br = L0; bc = R0; K = Ln;
+  }
+  // triangular operands: skip the K chunks that are structurally zero
+  int kbeg = 0, kend = K;
+  if (phase == 0) kend = min(K, (tn + 1) * CH_NB);
+  else kbeg = tm * CH_NB;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int k0 = kbeg; k0 < kend; k0 += CH_NB) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < CH_NB * CH_NB; e += blockDim.x) {
+      int r = e % CH_NB, k = e / CH_NB;
+      int gr = ar + tm * CH_NB + r, gc = ac + k0 + k;
+      bool in = (tm * CH_NB + r < Ln) && (k0 + k < K) && !(phase == 1 && gr > gc);
+      As[r + k * CH_LD] = in ? A[gr + (long)gc * n] : 0.0;
+      int hr = br + k0 + r, hc = bc + tn * CH_NB + k;
+      bool inb = (k0 + r < K) && (tn * CH_NB + k < Rn) && !(phase == 0 && hr > hc);
+      Bs[r + k * CH_LD] = inb ? B[hr + (long)hc * n] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < CH_NB; ++k) {
+      double x[4], y[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) x[a] = As[(tx + 16 * a) + k * CH_LD];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) y[b] = Bs[k + (ty + 16 * b) * CH_LD];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(x[a], y[b], acc[a][b]);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      int r = tm * CH_NB + tx + 16 * a, c = tn * CH_NB + ty + 16 * b;
+      if (r >= Ln || c >= Rn) continue;
+      long gr = L0 + r, gc = R0 + c;
+      if (phase == 0) {
+        Tmp[gr + gc * n] = acc[a][b];
+      } else {
+        Uinv[gr + gc * n] = -acc[a][b];
+        UinvT[gc + gr * n] = -acc[a][b];
+      }
+    }
+}
+
+// out[c] = sum over the stored triangle of column c of A (n x n): rows 0..c (upper) or c..n-1
+// (lower), times v.  One warp per column: coalesced column reads.
+extern "C" __global__ void k_tri_colgemv(const double* __restrict__ A, int n, int lower,
+                                         const double* __restrict__ v, double* __restrict__ out) {
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (c >= n) return;
+  const int r0 = lower ? c : 0, r1 = lower ? n : c + 1;
+  const double* col = A + (long)c * n;
+  double acc = 0.0;
+  for (int r = r0 + lane; r < r1; r += 32) acc = fma(col[r], v[r], acc);
+  acc = warp_sum(acc);
+  if (lane == 0) out[c] = acc;
+}
+
+// Partial sums of e = r - H x over column chunks: part[s][i] for chunk s.
+#define SYMV_SPLIT 16
+extern "C" __global__ void k_symv_partial(const double* __restrict__ Hs, int m,
+                                          const double* __restrict__ x, long ldx,
+                                          double* __restrict__ part, long ldp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  const int c = blockIdx.z;
+  if (i >= m) return;
+  const int chunk = (m + SYMV_SPLIT - 1) / SYMV_SPLIT;
+  const int k0 = s * chunk, k1 = min(m, k0 + chunk);
+  const double* xc = x + c * ldx;
+  double acc = 0.0;
+  for (int k = k0; k < k1; ++k) acc = fma(Hs[i + (long)k * m], xc[k], acc);
+  part[(long)c * ldp + (long)s * m + i] = acc;
+}
+
+extern "C" __global__ void k_symv_finish(int m, const double* __restrict__ part, long ldp,
+                                         const double* __restrict__ r, long ldr,
+                                         double* __restrict__ e, long lde) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (i >= m) return;
+  double acc = 0.0;
+  for (int s = 0; s < SYMV_SPLIT; ++s) acc += part[(long)c * ldp + (long)s * m + i];
+  e[c * lde + i] = r[c * ldr + i] - acc;
+}

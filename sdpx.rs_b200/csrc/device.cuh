@@ -85,8 +85,9 @@ __global__ void k_potrf_diag(double*, int, int, double, double, int, const doubl
                              uint32_t*);
 __global__ void k_trsm_panel(double*, int, int, const double*);
 __global__ void k_syrk_update(double*, int, int);
-__global__ void k_trsv_fwd(const double*, int, int, const double*, double*, double*, long, int);
-__global__ void k_trsv_bwd(const double*, int, int, const double*, double*, double*, long, int);
+__global__ void k_trtri_diag(int, const double*, double*, double*);
+__global__ void k_trinv_level(const double*, double*, double*, double*, int, int, int);
+__global__ void k_tri_colgemv(const double*, int, int, const double*, double*);
 __global__ void k_shifted_copy(const double*, double*, int, double, double*);
 __global__ void k_symv_partial(const double*, int, const double*, long, double*, long);
 __global__ void k_symv_finish(int, const double*, long, const double*, long, double*, long);

@@ -29,6 +29,7 @@ constexpr size_t kSmemMarg = (kMatD + 5 * SDPXG_NMAX + 32) * sizeof(double);
 constexpr size_t kSmemTrans = 3 * kMatD * sizeof(double);
 constexpr size_t kSmemTrsm = 2 * 64 * 65 * sizeof(double);
 constexpr size_t kSmemSyrk = 2 * 64 * 66 * sizeof(double);
+constexpr size_t kSmemTrtri = 2 * 64 * 65 * sizeof(double);
 constexpr int kNB = 64;
 
 // Equilibrated problem in host memory (CSC, int64 indices as in the reference ABI).
@@ -98,6 +99,8 @@ class Engine {
     set_smem(reinterpret_cast<const void*>(k_schur_transform), kSmemTrans);
     set_smem(reinterpret_cast<const void*>(k_trsm_panel), kSmemTrsm);
     set_smem(reinterpret_cast<const void*>(k_syrk_update), kSmemSyrk);
+    set_smem(reinterpret_cast<const void*>(k_trinv_level), kSmemTrtri);
+    set_smem(reinterpret_cast<const void*>(k_potrf_diag), kSmemTrtri);
     red.init();
     status_.alloc(1);
     for (auto& e : ev_) check(cudaEventCreate(&e), "event create");
@@ -249,8 +252,10 @@ class Engine {
     Dinv_.alloc((size_t)std::max(nchol, 1) * kNB * kNB);
     diag0_.alloc(std::max(n, 1));
     symv_part_.alloc((size_t)16 * std::max(n, 1));
-    tri_b_.alloc(std::max(n, 1));
     tri_y_.alloc(std::max(n, 1));
+    Uinv_.alloc((size_t)n * n);
+    UinvT_.alloc((size_t)n * n);
+    Tmp_.alloc((size_t)n * n);
     step_out_.alloc(2 * std::max(nblk, 1));
     marg_out_.alloc(2 * std::max(nblk, 1));
     scal_.alloc(4);
@@ -431,7 +436,7 @@ class Engine {
     tbegin(KT_FACTOR);
     ++g_launches, k_shifted_copy<<<1184, 256, 0, st>>>(Hsave_, F_, n, eps, diag0_);
     for (int kb = 0; kb < nchol; ++kb) {
-      ++g_launches, k_potrf_diag<<<1, SDPXG_THREADS, 0, st>>>(F_, n, kb, dyn_eps, dyn_delta, dynamic ? 1 : 0,
+      ++g_launches, k_potrf_diag<<<1, SDPXG_THREADS, kSmemTrtri, st>>>(F_, n, kb, dyn_eps, dyn_delta, dynamic ? 1 : 0,
                                                 diag0_, Dinv_, status_);
       int rest = nchol - kb - 1;
       if (rest > 0) {
@@ -440,21 +445,31 @@ class Engine {
       }
     }
     launched("factor");
-    tend(KT_FACTOR);
     uint32_t s = read_status();
     factor_ok_ = (s == 0);
+    if (factor_ok_) {
+      // explicit inverse of the factor: diagonal tiles, then one batched GEMM pair per level
+      ++g_launches, k_trtri_diag<<<nchol, SDPXG_THREADS, 0, st>>>(n, Dinv_, Uinv_, UinvT_);
+      for (int level = 1; (1 << (level - 1)) < nchol; ++level) {
+        const int g = 1 << level, h = g >> 1;
+        dim3 grid(h, h, (nchol + g - 1) / g);
+        for (int phase = 0; phase < 2; ++phase)
+          ++g_launches, k_trinv_level<<<grid, SDPXG_THREADS, kSmemTrtri, st>>>(
+              F_, Uinv_, UinvT_, Tmp_, n, level, phase);
+      }
+      launched("trinv");
+    }
+    tend(KT_FACTOR);
     return factor_ok_;
   }
-  // x = F^-1 r (no refinement); x may alias nothing.
+  // x = F^-1 r = U^-1 (U^-T r) through the explicit inverse: two coalesced GEMVs.
   void trisolve(const double* r, double* x) {
     need(r, "trisolve r");
     need(x, "trisolve x");
     tbegin(KT_TRISOLVE);
-    check(cudaMemcpyAsync(tri_b_.p, r, n * sizeof(double), cudaMemcpyDeviceToDevice, st), "trisolve copy");
-    for (int kb = 0; kb < nchol; ++kb)
-      ++g_launches, k_trsv_fwd<<<nchol - kb, SDPXG_THREADS, 0, st>>>(F_, n, kb, Dinv_, tri_b_, tri_y_, n, 1);
-    for (int kb = nchol - 1; kb >= 0; --kb)
-      ++g_launches, k_trsv_bwd<<<kb + 1, SDPXG_THREADS, 0, st>>>(F_, n, kb, Dinv_, tri_y_, x, n, 1);
+    const int grid = (n + 7) / 8;
+    ++g_launches, k_tri_colgemv<<<grid, 256, 0, st>>>(Uinv_, n, 0, r, tri_y_);
+    ++g_launches, k_tri_colgemv<<<grid, 256, 0, st>>>(UinvT_, n, 1, tri_y_, x);
     launched("trisolve");
     tend(KT_TRISOLVE);
   }
@@ -509,7 +524,7 @@ class Engine {
   DevBuf<int> prp_, pci_, pup_ptr_, pup_row_;
   DevBuf<double> pv_, pup_val_;
   DevBuf<double> adj_part_;
-  DevBuf<double> Hsave_, F_, Dinv_, diag0_, symv_part_, tri_b_, tri_y_;
+  DevBuf<double> Hsave_, F_, Dinv_, diag0_, symv_part_, tri_y_, Uinv_, UinvT_, Tmp_;
   DevBuf<double> step_out_, marg_out_, scal_;
   DevBuf<uint32_t> status_;
   cudaEvent_t ev_[2 * KT_N] = {};

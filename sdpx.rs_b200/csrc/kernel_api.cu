@@ -48,12 +48,14 @@ void need(sdpxg_ctx* c) {
   if (!c) throw std::invalid_argument("null context");
   if (!c->uploaded) throw std::invalid_argument("no problem uploaded");
 }
+// Ensure buf holds n doubles; copy h into it when h is given (h == nullptr: allocate only).
 void to_dev(DevBuf<double>& buf, const double* h, size_t n, cudaStream_t st) {
   if (buf.n < std::max<size_t>(n, 1)) buf.alloc(std::max<size_t>(n, 1));
-  if (n) {
-    if (!h) throw std::invalid_argument("null pointer");
-    buf.upload(h, n, st);
-  }
+  if (n && h) buf.upload(h, n, st);
+}
+void in_dev(DevBuf<double>& buf, const double* h, size_t n, cudaStream_t st) {
+  if (n && !h) throw std::invalid_argument("null pointer");
+  to_dev(buf, h, n, st);
 }
 void to_host(double* h, const DevBuf<double>& buf, size_t n, cudaStream_t st) {
   if (!n) return;
@@ -139,8 +141,8 @@ int32_t sdpxg_nt_scale(sdpxg_ctx* ctx, const double* s, const double* z, double*
   return guard([&] {
     need(ctx);
     Engine& E = *ctx->eng;
-    to_dev(ctx->a, s, E.m, E.st);
-    to_dev(ctx->b, z, E.m, E.st);
+    in_dev(ctx->a, s, E.m, E.st);
+    in_dev(ctx->b, z, E.m, E.st);
     bool ok = E.nt_scale(ctx->a, ctx->b);
     if (status) *status = ok ? 0u : 1u;
     if (out_lambda && ok) {
@@ -186,7 +188,7 @@ int32_t sdpxg_solve_many(sdpxg_ctx* ctx, const double* rhs, double* out, uint32_
     need(ctx);
     Engine& E = *ctx->eng;
     for (uint32_t c = 0; c < ncols; ++c) {
-      to_dev(ctx->a, rhs + (size_t)c * E.n, E.n, E.st);
+      in_dev(ctx->a, rhs + (size_t)c * E.n, E.n, E.st);
       to_dev(ctx->b, nullptr, E.n, E.st);
       if (!ctx->kkt->reduced_solve(ctx->a, ctx->b)) throw std::runtime_error("reduced solve failed");
       to_host(out + (size_t)c * E.n, ctx->b, E.n, E.st);
@@ -199,8 +201,8 @@ int32_t sdpxg_kkt_solve(sdpxg_ctx* ctx, const double* bx, const double* bz, doub
   return guard([&] {
     need(ctx);
     Engine& E = *ctx->eng;
-    to_dev(ctx->a, bx, E.n, E.st);
-    to_dev(ctx->b, bz, E.m, E.st);
+    in_dev(ctx->a, bx, E.n, E.st);
+    in_dev(ctx->b, bz, E.m, E.st);
     to_dev(ctx->c, nullptr, E.n, E.st);
     to_dev(ctx->d, nullptr, E.m, E.st);
     if (!ctx->kkt->kkt_solve(ctx->a, ctx->b, ctx->c, ctx->d)) throw std::runtime_error("KKT solve failed");
@@ -215,10 +217,10 @@ int32_t sdpxg_residual(sdpxg_ctx* ctx, const double* bx, const double* bz, const
   return guard([&] {
     need(ctx);
     Engine& E = *ctx->eng;
-    to_dev(ctx->a, bx, E.n, E.st);
-    to_dev(ctx->b, bz, E.m, E.st);
-    to_dev(ctx->c, x, E.n, E.st);
-    to_dev(ctx->d, z, E.m, E.st);
+    in_dev(ctx->a, bx, E.n, E.st);
+    in_dev(ctx->b, bz, E.m, E.st);
+    in_dev(ctx->c, x, E.n, E.st);
+    in_dev(ctx->d, z, E.m, E.st);
     to_dev(ctx->e, nullptr, E.n, E.st);
     to_dev(ctx->f, nullptr, E.m, E.st);
     ctx->kkt->residual_full(ctx->a, ctx->b, ctx->c, ctx->d, ctx->e, ctx->f);
@@ -238,8 +240,8 @@ int32_t sdpxg_step_length(sdpxg_ctx* ctx, const double* dz, const double* ds, do
     need(ctx);
     if (!out_alpha) throw std::invalid_argument("null pointer");
     Engine& E = *ctx->eng;
-    to_dev(ctx->a, dz, E.m, E.st);
-    to_dev(ctx->b, ds, E.m, E.st);
+    in_dev(ctx->a, dz, E.m, E.st);
+    in_dev(ctx->b, ds, E.m, E.st);
     double az, as;
     bool ok = E.step_bounds(ctx->a, ctx->b, amax, mode ? 1 : 0, &az, &as);
     *out_alpha = std::min(az, as);
@@ -253,7 +255,7 @@ int32_t sdpxg_cone_apply(sdpxg_ctx* ctx, uint32_t op, const double* x, double* y
     need(ctx);
     if (op > 5) throw std::invalid_argument("unknown cone operator");
     Engine& E = *ctx->eng;
-    to_dev(ctx->a, x, E.m, E.st);
+    in_dev(ctx->a, x, E.m, E.st);
     to_dev(ctx->b, nullptr, E.m, E.st);
     E.cone_apply((int)op, ctx->a, ctx->b);
     to_host(y, ctx->b, E.m, E.st);
