@@ -159,6 +159,15 @@ int32_t sdpxg_factor(sdpxg_ctx *ctx, double shift, uint32_t dynamic, double eps,
  * against the unshifted Schur complement.  Replaces DirectLDLSolver::solve
  * (kkt/ldl/dense_block.rs:795-850 with kkt/direct/solver.rs:1046-1125). */
 int32_t sdpxg_solve_many(sdpxg_ctx *ctx, const double *rhs, double *out, uint32_t ncols);
+/* No counterpart in the reference (it has no device memory to manage).  The refined reduced
+ * solve of sdpxg_solve_many for callers that cannot allocate device memory at call time (a
+ * host that owns all device memory through its own pool, or a latency-bound loop where a
+ * cudaMalloc could synchronise the device): d_rhs and d_out are DEVICE pointers to n x ncols
+ * column-major arrays, and all per-call scratch sits in one static device array of the library
+ * (about 0.7 MB on every GPU that loads it).  It calls no cudaMalloc or cudaFree.  n above 4096
+ * returns 2.  The first call on a device looks up the array's address: make it before any
+ * stream capture.  Calls that overlap on the GPU share the array and race. */
+int32_t sdpxg_solve_noalloc(sdpxg_ctx *ctx, const double *d_rhs, double *d_out, uint32_t ncols);
 /* Full condensed KKT solve [P A'; A -Hs][x; z] = [bx; bz] with the outer refinement on the
  * original operator.  Replaces CondensedKKTSolver::solve (kkt/condensed/kkt.rs:275-318). */
 int32_t sdpxg_kkt_solve(sdpxg_ctx *ctx, const double *bx, const double *bz, double *x, double *z);

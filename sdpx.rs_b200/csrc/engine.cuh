@@ -88,7 +88,10 @@ class Engine {
     kt_count[k]++;
   }
 
-  void init(int device) {
+  int device = 0;
+
+  void init(int dev) {
+    device = dev;
     check(cudaSetDevice(device), "cudaSetDevice");
     check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
     set_smem(reinterpret_cast<const void*>(k_nt_scale), kSmemNt);
@@ -504,6 +507,9 @@ class Engine {
   }
 
   double* Hsave() { return Hsave_.p; }
+  const double* uinv() const { return Uinv_.p; }
+  const double* uinvT() const { return UinvT_.p; }
+  bool factored() const { return factor_ok_; }
   double* F() { return F_.p; }
   const BlockDesc* blocks() const { return blocks_.p; }
 

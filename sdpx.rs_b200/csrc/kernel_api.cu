@@ -43,6 +43,11 @@ struct sdpxg_ctx {
   bool uploaded = false;
 };
 
+namespace sdpxg {
+// The engine of a context with an uploaded problem (nullptr otherwise).
+Engine* ctx_engine(sdpxg_ctx* c) { return (c && c->uploaded) ? c->eng.get() : nullptr; }
+}  // namespace sdpxg
+
 namespace {
 void need(sdpxg_ctx* c) {
   if (!c) throw std::invalid_argument("null context");

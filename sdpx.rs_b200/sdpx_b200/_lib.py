@@ -83,6 +83,7 @@ SIGNATURES = {
     "sdpxg_schur_assemble": (i32, [C.c_void_p, PD]),
     "sdpxg_factor": (i32, [C.c_void_p, f64, u32, f64, f64, PU32]),
     "sdpxg_solve_many": (i32, [C.c_void_p, PD, PD, u32]),
+    "sdpxg_solve_noalloc": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u32]),
     "sdpxg_kkt_solve": (i32, [C.c_void_p, PD, PD, PD, PD]),
     "sdpxg_residual": (i32, [C.c_void_p, PD, PD, PD, PD, PD, PD, PD]),
     "sdpxg_step_length": (i32, [C.c_void_p, PD, PD, f64, u32, PD, PU32]),
