@@ -311,6 +311,8 @@ def run_ours(args, world, rank, local):
                 "frac": achieved / hbm, "traffic": traffic_from_profile(dom), "kernel": dom,
                 "launch_ms": per * 1e3, "note": f"peak {hbm_kind} (MEASURED_PEAKS.json hbm_gbs)"}
     phases = {k: {"ms_total": v[0], "launches": v[1]} for k, v in ktimes.items()}
+    host_phases = {k: round(v, 5) for k, v in solver.info.phase_times.items()}
+    host_phases["counts"] = solver.info.counts
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -324,7 +326,8 @@ def run_ours(args, world, rank, local):
                 "status": status, "iterations": iters, "wall_s_per_step": wall,
                 "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
-                "roofline": roof, "phases": phases, "gpu_launches": gpu_launches,
+                "roofline": roof, "phases": phases, "host_phase_s_last_solve": host_phases,
+                "gpu_launches": gpu_launches,
                 "clocks": clk, "cpu_baseline": cb}
         print(json.dumps(line))
     return 0

@@ -13,7 +13,8 @@
 
 #define SDPXG_NMAX 64               // largest PSD block order handled by the CTA kernels
 #define SDPXG_LD (SDPXG_NMAX + 1)   // shared-memory leading dimension (odd: fewer bank conflicts)
-#define SDPXG_THREADS 256
+#define SDPXG_THREADS 256         // dense tile kernels (their thread maps assume 256)
+#define SDPXG_CONE_THREADS 1024   // one CTA per PSD block: one warp per Jacobi rotation pair
 #define SDPXG_RSQRT2 0.70710678118654752440
 #define SDPXG_SQRT2 1.41421356237309504880
 
@@ -62,13 +63,24 @@ __device__ __forceinline__ double warp_min(double v) {
 // ------------------------------------------------------------------------------------
 #define SM(A, i, j) (A)[(i) + (j) * SDPXG_LD]
 
-// M = smat(v): symmetric matrix from an svec.
+// Shared matrices are 64 x 64 (leading dimension SDPXG_LD) whatever the block order n; the
+// entries outside n x n are kept at zero so the tensor-core products below can run on whole
+// 8 x 8 x 4 fragments.  Loads write the zero padding; products of padded inputs keep it.
+__device__ __forceinline__ void cta_zero_mat(double* M) {
+  for (int e = threadIdx.x; e < SDPXG_LD * SDPXG_NMAX; e += blockDim.x) M[e] = 0.0;
+}
+
+// M = smat(v): symmetric matrix from an svec (zero padded to 64 x 64).
 __device__ __forceinline__ void cta_load_smat(double* M, const double* __restrict__ v, int n) {
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-    int i = e % n, j = e / n;
-    int a = min(i, j), b = max(i, j);
-    double x = v[tri_idx(a, b)];
-    SM(M, i, j) = (i == j) ? x : x * SDPXG_RSQRT2;
+  for (int e = threadIdx.x; e < SDPXG_NMAX * SDPXG_NMAX; e += blockDim.x) {
+    int i = e % SDPXG_NMAX, j = e / SDPXG_NMAX;
+    double x = 0.0;
+    if (i < n && j < n) {
+      int a = min(i, j), b = max(i, j);
+      x = v[tri_idx(a, b)];
+      if (i != j) x *= SDPXG_RSQRT2;
+    }
+    SM(M, i, j) = x;
   }
 }
 
@@ -82,25 +94,54 @@ __device__ __forceinline__ void cta_store_svec(double* __restrict__ v, const dou
 }
 
 __device__ __forceinline__ void cta_load_mat(double* M, const double* __restrict__ g, int n) {
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) SM(M, e % n, e / n) = g[e];
+  for (int e = threadIdx.x; e < SDPXG_NMAX * SDPXG_NMAX; e += blockDim.x) {
+    int i = e % SDPXG_NMAX, j = e / SDPXG_NMAX;
+    SM(M, i, j) = (i < n && j < n) ? g[i + j * n] : 0.0;
+  }
 }
 
 __device__ __forceinline__ void cta_store_mat(double* __restrict__ g, const double* M, int n) {
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) g[e] = SM(M, e % n, e / n);
 }
 
+// One FP64 tensor-core MMA: D(8x8) = A(8x4) B(4x8) + C.  Fragments (PTX mma.m8n8k4 .f64):
+// lane l holds A[l/4][l%4], B[l%4][l/4] and C/D[l/4][2(l%4) + {0,1}].
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// C = op(A) op(B) on zero-padded shared matrices, one 8 x 8 output tile per warp at a time,
+// K in steps of 4 up to n rounded up.  C must not alias A or B.
+template <bool TA, bool TB>
+__device__ __forceinline__ void cta_gemm_mma(double* C, const double* A, const double* B, int n) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int tiles = (n + 7) >> 3, ksteps = (n + 3) >> 2;
+  const int r = lane >> 2, q = lane & 3;
+  for (int t = warp; t < tiles * tiles; t += nwarps) {
+    const int ti = (t % tiles) << 3, tj = (t / tiles) << 3;
+    double d0 = 0.0, d1 = 0.0;
+    for (int ks = 0; ks < ksteps; ++ks) {
+      const int k = (ks << 2) + q;
+      const double a = TA ? SM(A, k, ti + r) : SM(A, ti + r, k);
+      const double b = TB ? SM(B, tj + r, k) : SM(B, k, tj + r);
+      dmma_m8n8k4(d0, d1, a, b);
+    }
+    SM(C, ti + r, tj + 2 * q) = d0;
+    SM(C, ti + r, tj + 2 * q + 1) = d1;
+  }
+}
+
 // C = op(A) * op(B); ta/tb select the transpose.  C must not alias A or B.
 __device__ __forceinline__ void cta_gemm(double* C, const double* A, bool ta, const double* B,
                                          bool tb, int n) {
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-    int i = e % n, j = e / n;
-    double acc = 0.0;
-    for (int k = 0; k < n; ++k) {
-      double a = ta ? SM(A, k, i) : SM(A, i, k);
-      double b = tb ? SM(B, j, k) : SM(B, k, j);
-      acc = fma(a, b, acc);
-    }
-    SM(C, i, j) = acc;
+  if (ta) {
+    if (tb) cta_gemm_mma<true, true>(C, A, B, n);
+    else cta_gemm_mma<true, false>(C, A, B, n);
+  } else {
+    if (tb) cta_gemm_mma<false, true>(C, A, B, n);
+    else cta_gemm_mma<false, false>(C, A, B, n);
   }
 }
 

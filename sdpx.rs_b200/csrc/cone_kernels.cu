@@ -20,7 +20,7 @@ constexpr int kMat = SDPXG_LD * SDPXG_NMAX;  // doubles per shared matrix
 // R = L1 V lam^-1/2, Rinv = lam^1/2 V' L1^-1, Ginv = Rinv' Rinv.
 // Shared memory: 5 matrices + 3n doubles + n ints + 1 int.
 // ---------------------------------------------------------------------------------------
-extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
+extern "C" __global__ void __launch_bounds__(SDPXG_CONE_THREADS)
 k_nt_scale(const BlockDesc* __restrict__ blocks, const double* __restrict__ s,
            const double* __restrict__ z, double* __restrict__ R, double* __restrict__ Rinv,
            double* __restrict__ Ginv, double* __restrict__ lam, double* __restrict__ lisqrt,
@@ -39,6 +39,8 @@ k_nt_scale(const BlockDesc* __restrict__ blocks, const double* __restrict__ s,
   int* rank = reinterpret_cast<int*>(lsort + SDPXG_NMAX);
   int* flag = rank + SDPXG_NMAX;
 
+  cta_zero_mat(V);  // V and X are written n x n only: keep their padding zero for the MMAs
+  cta_zero_mat(X);
   cta_load_smat(L1, s + bd.svec_off, n);
   cta_load_smat(L2, z + bd.svec_off, n);
   bool ok1 = cta_cholesky_lower(L1, n, piv);
@@ -152,7 +154,7 @@ __device__ void cta_congruence(double* Y, double* T, const double* X, const doub
   __syncthreads();
 }
 
-extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
+extern "C" __global__ void __launch_bounds__(SDPXG_CONE_THREADS)
 k_congruence(const BlockDesc* __restrict__ blocks, int mode, const double* __restrict__ R,
              const double* __restrict__ Rinv, const double* __restrict__ x, double* __restrict__ y,
              long ld) {
@@ -184,7 +186,7 @@ k_congruence(const BlockDesc* __restrict__ blocks, int mode, const double* __res
 }
 
 // x = svec((Y Z + Z Y) / 2) per block.
-extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
+extern "C" __global__ void __launch_bounds__(SDPXG_CONE_THREADS)
 k_circ_op(const BlockDesc* __restrict__ blocks, const double* __restrict__ yv,
           const double* __restrict__ zv, double* __restrict__ xv) {
   extern __shared__ double smem[];
@@ -249,7 +251,7 @@ extern "C" __global__ void k_shift_unit(const BlockDesc* __restrict__ blocks, do
 // mode 1: admission only (out = amax if admitted else 0).
 // out[2*block + side].
 // ---------------------------------------------------------------------------------------
-extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
+extern "C" __global__ void __launch_bounds__(SDPXG_CONE_THREADS)
 k_step_length(const BlockDesc* __restrict__ blocks, const double* __restrict__ R,
               const double* __restrict__ Rinv, const double* __restrict__ lisqrt,
               const double* __restrict__ dz, const double* __restrict__ ds, double amax, int mode,
@@ -293,15 +295,13 @@ k_step_length(const BlockDesc* __restrict__ blocks, const double* __restrict__ R
   }
   if (!admitted) {
     cta_tridiagonalize(X, n, dd, ee, work, red);
-    if (threadIdx.x == 0) {
-      bool ok = true;
-      double g = bisect_kth(dd, ee, n, 0, &ok);
-      if (!ok || !isfinite(g)) {
-        atomicOr(status, SDPXG_ST_EIG_FAIL);
-        res = 0.0;
-      } else {
-        res = (g < 0.0) ? fmin(-1.0 / g, amax) : amax;
-      }
+    bool ok = true;
+    double g = cta_eig_min(dd, ee, n, reinterpret_cast<int*>(red), &ok);
+    if (!ok || !isfinite(g)) {
+      if (threadIdx.x == 0) atomicOr(status, SDPXG_ST_EIG_FAIL);
+      res = 0.0;
+    } else {
+      res = (g < 0.0) ? fmin(-1.0 / g, amax) : amax;
     }
   }
   if (threadIdx.x == 0) out[2 * b + side] = res;
@@ -310,7 +310,7 @@ k_step_length(const BlockDesc* __restrict__ blocks, const double* __restrict__ R
 // Eigenvalue summary of smat(v) per block: out[2b] = lambda_min, out[2b+1] = sum of positive
 // eigenvalues.  (margins, psdtrianglecone.rs; also the cone distance of the original-
 // coordinate acceptance test, default/original_check.rs:306-340.)
-extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
+extern "C" __global__ void __launch_bounds__(SDPXG_CONE_THREADS)
 k_margins(const BlockDesc* __restrict__ blocks, const double* __restrict__ v, long ld,
           double* __restrict__ out, uint32_t* __restrict__ status) {
   extern __shared__ double smem[];

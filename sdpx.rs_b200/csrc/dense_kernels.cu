@@ -36,23 +36,36 @@ extern "C" __global__ void k_shifted_copy(const double* __restrict__ Hs, double*
 // ------------------------------------------------------------------------------------
 // Diagonal tile: lagged upper Cholesky with the dynamic pivot rule, then Dinv = U^-1.
 // Dynamic shared memory: two CH_NB x CH_LD tiles.
-extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
+extern "C" __global__ void __launch_bounds__(1024)
 k_potrf_diag(double* __restrict__ H, int m, int kb, double eps, double delta, int dynamic,
              const double* __restrict__ diag0, double* __restrict__ Dinv,
              uint32_t* __restrict__ status) {
   extern __shared__ double pd_sm[];
   double* A = pd_sm;
-  double* X = A + CH_NB * CH_LD;
+  __shared__ double rowbuf[2][CH_NB];   // row k of the partially eliminated tile
+  __shared__ double mrowbuf[2][CH_NB];  // row k of M = L^-1 (unit lower)
   __shared__ double dmod[CH_NB];
   const int k0 = kb * CH_NB;
   const int nb = min(CH_NB, m - k0);
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    int i = e % nb, j = e / nb;
-    if (i <= j) A[i + j * CH_LD] = H[(k0 + i) + (long)(k0 + j) * m];
-  }
+  // thread (tx, ty) owns rows tx + 32p and columns ty + 32q (p, q < 2) of the tile, in
+  // registers: a = upper triangle being eliminated (H = L D L'), mm = lower triangle of
+  // M = L^-1, updated with the same elimination multipliers (Gauss elimination applied to I).
+  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
+  double a[2][2], mm[2][2];
+#pragma unroll
+  for (int p = 0; p < 2; ++p)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      int i = tx + 32 * p, j = ty + 32 * q;
+      a[p][q] = (i <= j && j < nb) ? H[(k0 + i) + (long)(k0 + j) * m] : 0.0;
+      mm[p][q] = (i == j) ? 1.0 : 0.0;
+      if (i == 0 && j < nb) rowbuf[0][j] = a[p][q];
+      if (i == 0) mrowbuf[0][j] = (j == 0) ? 1.0 : 0.0;
+    }
   for (int k = 0; k < nb; ++k) {
     __syncthreads();
-    double d = A[k + k * CH_LD];
+    const double* row = rowbuf[k & 1];
+    double d = row[k];
     bool fail = !isfinite(d);
     if (!fail && dynamic && d <= eps) {
       // a pivot within rounding of zero becomes delta; a clearly negative one fails
@@ -64,43 +77,45 @@ k_potrf_diag(double* __restrict__ H, int m, int kb, double eps, double delta, in
       if (threadIdx.x == 0) atomicOr(status, SDPXG_ST_PIVOT_FAIL);
       return;  // uniform: every thread read the same pivot
     }
+    const double dinv = 1.0 / d, r = sqrt(d);
     if (threadIdx.x == 0) dmod[k] = d;
-    const int rem = nb - k - 1;
-    const double dinv = 1.0 / d;
-    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
-      int i = k + 1 + e % rem, j = k + 1 + e / rem;
-      if (i > j) continue;
-      A[i + j * CH_LD] -= A[k + i * CH_LD] * A[k + j * CH_LD] * dinv;
-    }
+    const double* mrow = mrowbuf[k & 1];
+    double* next = rowbuf[(k + 1) & 1];
+    double* mnext = mrowbuf[(k + 1) & 1];
+#pragma unroll
+    for (int p = 0; p < 2; ++p)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int i = tx + 32 * p, j = ty + 32 * q;
+        if (i >= nb || j >= nb) continue;
+        if (i <= j) {
+          if (i == k) A[k + j * CH_LD] = (j == k) ? r : a[p][q] / r;  // final row k of U
+          if (i > k) {
+            a[p][q] -= row[i] * row[j] * dinv;
+            if (i == k + 1) next[j] = a[p][q];
+          }
+        }
+        if (i >= j) {  // M entry (i, c = j): row i -= l_ik * row k, for c <= k
+          if (i > k && j <= k) mm[p][q] -= (row[i] * dinv) * mrow[j];
+          if (i == k + 1 && j <= k + 1) mnext[j] = mm[p][q];
+        }
+      }
   }
   __syncthreads();
   for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
     int i = e % nb, j = e / nb;
-    if (i > j) continue;
-    double r = sqrt(dmod[i]);
-    double u = (i == j) ? r : A[i + j * CH_LD] / r;
-    A[i + j * CH_LD] = u;
-    H[(k0 + i) + (long)(k0 + j) * m] = u;
+    if (i <= j) H[(k0 + i) + (long)(k0 + j) * m] = A[i + j * CH_LD];
   }
-  __syncthreads();
-  // Dinv = U^-1 (upper): column j by back substitution in shared memory.
-  for (int j = threadIdx.x; j < CH_NB; j += blockDim.x) {
-    for (int i = CH_NB - 1; i > j; --i) X[i + j * CH_LD] = 0.0;
-    if (j < nb) {
-      X[j + j * CH_LD] = 1.0 / A[j + j * CH_LD];
-      for (int i = j - 1; i >= 0; --i) {
-        double acc = 0.0;
-        for (int l = i + 1; l <= j; ++l) acc = fma(A[i + l * CH_LD], X[l + j * CH_LD], acc);
-        X[i + j * CH_LD] = -acc / A[i + i * CH_LD];
-      }
-    } else {
-      for (int i = 0; i <= j; ++i) X[i + j * CH_LD] = 0.0;
-    }
-  }
-  __syncthreads();
+  // Dinv = U^-1 = L^-T D^-1/2: Dinv[c][i] = M[i][c] / sqrt(d_i) (upper, zero elsewhere)
   double* D = Dinv + (long)kb * CH_NB * CH_NB;
-  for (int e = threadIdx.x; e < CH_NB * CH_NB; e += blockDim.x)
-    D[e] = X[(e % CH_NB) + (e / CH_NB) * CH_LD];
+#pragma unroll
+  for (int p = 0; p < 2; ++p)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int i = tx + 32 * p, c = ty + 32 * q;
+      const bool live = (i >= c && i < nb);
+      D[c + i * CH_NB] = live ? mm[p][q] / sqrt(dmod[i]) : 0.0;
+    }
 }
 
 // ------------------------------------------------------------------------------------
@@ -119,13 +134,36 @@ k_trsm_panel(double* __restrict__ H, int m, int kb, const double* __restrict__ D
     int i = e % nb, c = e / nb;
     P[i + c * CH_LD] = H[(k0 + i) + (long)(c0 + c) * m];
   }
-  __syncthreads();
-  for (int e = threadIdx.x; e < nb * nc; e += blockDim.x) {
-    int i = e % nb, c = e / nb;
-    double acc = 0.0;
-    for (int l = 0; l <= i; ++l) acc = fma(D[l + i * CH_LD], P[l + c * CH_LD], acc);
-    H[(k0 + i) + (long)(c0 + c) * m] = acc;
+  for (int e = threadIdx.x; e < CH_NB * CH_NB; e += blockDim.x) {  // zero the ragged edge
+    int i = e % CH_NB, c = e / CH_NB;
+    if (i >= nb || c >= nc) P[i + c * CH_LD] = 0.0;
   }
+  __syncthreads();
+  // out = D' P with 4 x 4 register tiles (D is upper with zeros below the diagonal)
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int l = 0; l < nb; ++l) {
+    double x[4], y[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) x[a] = D[l + (tx + 16 * a) * CH_LD];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) y[b] = P[l + (ty + 16 * b) * CH_LD];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = fma(x[a], y[b], acc[a][b]);
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      int i = tx + 16 * a, c = ty + 16 * b;
+      if (i < nb && c < nc) H[(k0 + i) + (long)(c0 + c) * m] = acc[a][b];
+    }
 }
 
 // ------------------------------------------------------------------------------------

@@ -75,7 +75,8 @@ __global__ void k_schur_gather(int, const int*, const int*, const int*, const in
                                const double*, double*);
 __global__ void k_add_upper_csc(int, const int*, const int*, const double*, double*);
 __global__ void k_op_forward(const BlockDesc*, const int*, const int*, const int*, const long*,
-                             const double*, const double*, long, double, double, double*, long);
+                             const double*, const int*, const int*, const double*, long, double,
+                             double, double*, long);
 __global__ void k_op_adjoint_partial(const BlockDesc*, const int*, const int*, const int*,
                                      const long*, const double*, const double*, long, double*,
                                      long, int);

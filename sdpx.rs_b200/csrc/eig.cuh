@@ -177,6 +177,36 @@ __device__ __forceinline__ void gershgorin(const double* d, const double* e, int
   *pivmin = 2.2250738585072014e-308 * fmax(1.0, emax);
 }
 
+// Smallest eigenvalue of the tridiagonal (d, e) by CTA-wide multisection: each round every
+// thread evaluates one Sturm count on an even grid over the current bracket and the bracket
+// shrinks to the first grid cell holding an eigenvalue (about blockDim-fold per round).
+// Uniform result; `best` is one int of shared memory.  *ok = false if the round bound is hit.
+__device__ inline double cta_eig_min(const double* d, const double* e, int n, int* best, bool* ok) {
+  double lo, hi, pivmin;
+  gershgorin(d, e, n, &lo, &hi, &pivmin);
+  const int T = blockDim.x;
+  for (int round = 0; round < 16; ++round) {
+    if (!(hi - lo > 2.0 * 2.220446049250313e-16 * fmax(fabs(lo), fabs(hi)) + pivmin)) {
+      *ok = true;
+      return 0.5 * (lo + hi);
+    }
+    const double step = (hi - lo) / (T + 1);
+    if (threadIdx.x == 0) *best = T;
+    __syncthreads();
+    const double x = lo + step * (threadIdx.x + 1);
+    if (x > lo && x < hi && sturm_count(d, e, n, x, pivmin) >= 1) atomicMin(best, (int)threadIdx.x);
+    __syncthreads();
+    const int t = *best;
+    __syncthreads();
+    const double nlo = (t == 0) ? lo : lo + step * t;
+    const double nhi = (t == T) ? hi : lo + step * (t + 1);
+    lo = nlo;
+    hi = nhi;
+  }
+  *ok = false;
+  return 0.5 * (lo + hi);
+}
+
 // k-th smallest eigenvalue (k = 0 is the minimum) by bisection; one thread.
 // Sets *ok = false when the bound on steps was hit before convergence.
 __device__ inline double bisect_kth(const double* d, const double* e, int n, int k, bool* ok) {

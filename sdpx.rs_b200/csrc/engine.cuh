@@ -240,6 +240,19 @@ class Engine {
     c2b_loc_.alloc(std::max<size_t>(c2b_loc.size(), 1)); c2b_loc_.upload(c2b_loc.data(), c2b_loc.size(), st);
     wblk_.alloc(std::max(nwork_, 1)); wblk_.upload(wblk.data(), wblk.size(), st);
     wloc_.alloc(std::max(nwork_, 1)); wloc_.upload(wloc.data(), wloc.size(), st);
+    {  // 64-row tiles of every block for the forward product
+      std::vector<int> fb, fr;
+      for (int j = 0; j < nblk; ++j) {
+        int tn = hblocks[j].n * (hblocks[j].n + 1) / 2;
+        for (int r0 = 0; r0 < tn; r0 += 64) {
+          fb.push_back(j);
+          fr.push_back(r0);
+        }
+      }
+      nftile_ = (int)fb.size();
+      ftile_blk_.alloc(std::max(nftile_, 1)); ftile_blk_.upload(fb.data(), fb.size(), st);
+      ftile_r0_.alloc(std::max(nftile_, 1)); ftile_r0_.upload(fr.data(), fr.size(), st);
+    }
     tiles_.alloc(std::max<size_t>(tiles.size(), 1)); tiles_.upload(tiles.data(), tiles.size(), st);
     prp_.alloc(n + 1); prp_.upload(prp.data(), n + 1, st);
     pci_.alloc(std::max(p_nnz_, 1)); pci_.upload(pci.data(), pci.size(), st);
@@ -284,7 +297,7 @@ class Engine {
     clear_status();
     tbegin(KT_SCALE);
     if (nblk)
-      ++g_launches, k_nt_scale<<<nblk, SDPXG_THREADS, kSmemNt, st>>>(blocks_, s, z, R_, Rinv_, Ginv_, lam_,
+      ++g_launches, k_nt_scale<<<nblk, SDPXG_CONE_THREADS, kSmemNt, st>>>(blocks_, s, z, R_, Rinv_, Ginv_, lam_,
                                                       lisqrt_, status_);
     launched("k_nt_scale");
     tend(KT_SCALE);
@@ -297,7 +310,7 @@ class Engine {
     need(y, "cone_apply y");
     if (!nblk) return;
     tbegin(KT_CONE);
-    ++g_launches, k_congruence<<<dim3(nblk, ncols), SDPXG_THREADS, kSmemCong, st>>>(blocks_, mode, R_, Rinv_, x,
+    ++g_launches, k_congruence<<<dim3(nblk, ncols), SDPXG_CONE_THREADS, kSmemCong, st>>>(blocks_, mode, R_, Rinv_, x,
                                                                       y, ld ? ld : m);
     launched("k_congruence");
     tend(KT_CONE);
@@ -306,7 +319,7 @@ class Engine {
     need(y, "circ y");
     need(z, "circ z");
     need(x, "circ x");
-    if (nblk) ++g_launches, k_circ_op<<<nblk, SDPXG_THREADS, kSmemCirc, st>>>(blocks_, y, z, x);
+    if (nblk) ++g_launches, k_circ_op<<<nblk, SDPXG_CONE_THREADS, kSmemCirc, st>>>(blocks_, y, z, x);
     launched("k_circ_op");
   }
   void lam_inv_circ(const double* z, double* x) {
@@ -332,7 +345,7 @@ class Engine {
     if (!nblk) return true;
     clear_status();
     tbegin(KT_STEP);
-    ++g_launches, k_step_length<<<dim3(nblk, 2), SDPXG_THREADS, kSmemStep, st>>>(blocks_, R_, Rinv_, lisqrt_, dz,
+    ++g_launches, k_step_length<<<dim3(nblk, 2), SDPXG_CONE_THREADS, kSmemStep, st>>>(blocks_, R_, Rinv_, lisqrt_, dz,
                                                                    ds, amax, mode, step_out_,
                                                                    status_);
     launched("k_step_length");
@@ -353,7 +366,7 @@ class Engine {
     out.assign(2 * nblk, 0.0);
     if (!nblk) return true;
     clear_status();
-    ++g_launches, k_margins<<<dim3(nblk, 1), SDPXG_THREADS, kSmemMarg, st>>>(blocks_, v, m, marg_out_, status_);
+    ++g_launches, k_margins<<<dim3(nblk, 1), SDPXG_CONE_THREADS, kSmemMarg, st>>>(blocks_, v, m, marg_out_, status_);
     launched("k_margins");
     check(cudaMemcpyAsync(out.data(), marg_out_.p, 2 * nblk * sizeof(double),
                           cudaMemcpyDeviceToHost, st), "margins D2H");
@@ -366,8 +379,9 @@ class Engine {
     need(x, "A_forward x");
     need(y, "A_forward y");
     if (!nblk) return;
-    ++g_launches, k_op_forward<<<dim3(nblk, 1), 256, 0, st>>>(blocks_, kcount_, col_ptr_, col_idx_, acol_off_,
-                                                acol_, x, n, alpha, beta, y, m);
+    ++g_launches, k_op_forward<<<dim3(nftile_, 1), 256, 0, st>>>(blocks_, kcount_, col_ptr_, col_idx_,
+                                                              acol_off_, acol_, ftile_blk_, ftile_r0_,
+                                                              x, n, alpha, beta, y, m);
     launched("k_op_forward");
   }
   // y = alpha * A' z + beta * y   (length n)
@@ -404,7 +418,7 @@ class Engine {
   bool assemble() {
     tbegin(KT_ASSEMBLE);
     if (nwork_) {
-      ++g_launches, k_schur_transform<<<nwork_, SDPXG_THREADS, kSmemTrans, st>>>(blocks_, wblk_, wloc_, acol_off_,
+      ++g_launches, k_schur_transform<<<nwork_, SDPXG_CONE_THREADS, kSmemTrans, st>>>(blocks_, wblk_, wloc_, acol_off_,
                                                                    Ginv_, acol_, tcol_);
       launched("k_schur_transform");
       ++g_launches, k_schur_block_gemm<<<ntiles_, 256, 0, st>>>(blocks_, tiles_, kcount_, acol_off_, s_off_, acol_,
@@ -439,7 +453,7 @@ class Engine {
     tbegin(KT_FACTOR);
     ++g_launches, k_shifted_copy<<<1184, 256, 0, st>>>(Hsave_, F_, n, eps, diag0_);
     for (int kb = 0; kb < nchol; ++kb) {
-      ++g_launches, k_potrf_diag<<<1, SDPXG_THREADS, kSmemTrtri, st>>>(F_, n, kb, dyn_eps, dyn_delta, dynamic ? 1 : 0,
+      ++g_launches, k_potrf_diag<<<1, 1024, kSmemTrtri, st>>>(F_, n, kb, dyn_eps, dyn_delta, dynamic ? 1 : 0,
                                                 diag0_, Dinv_, status_);
       int rest = nchol - kb - 1;
       if (rest > 0) {
@@ -527,6 +541,8 @@ class Engine {
   DevBuf<double> acol_, tcol_, S_;
   DevBuf<long> acol_off_, s_off_;
   DevBuf<int> kcount_, col_ptr_, col_idx_, c2b_ptr_, c2b_blk_, c2b_loc_, wblk_, wloc_, tiles_;
+  DevBuf<int> ftile_blk_, ftile_r0_;
+  int nftile_ = 0;
   DevBuf<int> prp_, pci_, pup_ptr_, pup_row_;
   DevBuf<double> pv_, pup_val_;
   DevBuf<double> adj_part_;

@@ -18,7 +18,7 @@ constexpr int kMat = SDPXG_LD * SDPXG_NMAX;
 }
 
 // One CTA per (block, column) work item: item w -> block wblk[w], local column wloc[w].
-extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
+extern "C" __global__ void __launch_bounds__(SDPXG_CONE_THREADS)
 k_schur_transform(const BlockDesc* __restrict__ blocks, const int* __restrict__ wblk,
                   const int* __restrict__ wloc, const long* __restrict__ acol_off,
                   const double* __restrict__ Ginv, const double* __restrict__ Acol,
@@ -140,15 +140,17 @@ extern "C" __global__ void k_add_upper_csc(int n, const int* __restrict__ colptr
 }
 
 // y[rows of block j] = alpha * Acol_j x[cols_j] + beta * y   (one CTA per block, thread/row)
-extern "C" __global__ void k_op_forward(const BlockDesc* __restrict__ blocks,
-                                        const int* __restrict__ kcount,
-                                        const int* __restrict__ col_ptr,
-                                        const int* __restrict__ col_idx,
-                                        const long* __restrict__ acol_off,
-                                        const double* __restrict__ Acol,
-                                        const double* __restrict__ x, long ldx, double alpha,
-                                        double beta, double* __restrict__ y, long ldy) {
-  const int j = blockIdx.x;
+// One CTA per 64-row tile of a block (tile list ftile_blk / ftile_r0): 64 rows x 4 column
+// groups; the four partial sums are combined in a fixed order (deterministic).
+extern "C" __global__ void __launch_bounds__(256)
+k_op_forward(const BlockDesc* __restrict__ blocks, const int* __restrict__ kcount,
+             const int* __restrict__ col_ptr, const int* __restrict__ col_idx,
+             const long* __restrict__ acol_off, const double* __restrict__ Acol,
+             const int* __restrict__ ftile_blk, const int* __restrict__ ftile_r0,
+             const double* __restrict__ x, long ldx, double alpha, double beta,
+             double* __restrict__ y, long ldy) {
+  __shared__ double part[4][64];
+  const int j = ftile_blk[blockIdx.x], r0 = ftile_r0[blockIdx.x];
   const BlockDesc bd = blocks[j];
   const int tn = bd.n * (bd.n + 1) / 2;
   const int k = kcount[j];
@@ -156,11 +158,17 @@ extern "C" __global__ void k_op_forward(const BlockDesc* __restrict__ blocks,
   const int* cols = col_idx + col_ptr[j];
   const double* xc = x + (long)blockIdx.y * ldx;
   double* yc = y + (long)blockIdx.y * ldy;
-  for (int r = threadIdx.x; r < tn; r += blockDim.x) {
-    double acc = 0.0;
-    for (int t = 0; t < k; ++t) acc = fma(A[(long)t * tn + r], xc[cols[t]], acc);
+  const int rr = threadIdx.x & 63, g = threadIdx.x >> 6;
+  const int r = r0 + rr;
+  double acc = 0.0;
+  if (r < tn)
+    for (int t = g; t < k; t += 4) acc = fma(A[(long)t * tn + r], xc[cols[t]], acc);
+  part[g][rr] = acc;
+  __syncthreads();
+  if (g == 0 && r < tn) {
+    double s = ((part[0][rr] + part[1][rr]) + part[2][rr]) + part[3][rr];
     double prev = (beta == 0.0) ? 0.0 : beta * yc[bd.svec_off + r];
-    yc[bd.svec_off + r] = alpha * acc + prev;
+    yc[bd.svec_off + r] = alpha * s + prev;
   }
 }
 

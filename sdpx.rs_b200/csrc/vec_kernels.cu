@@ -57,13 +57,14 @@ k_reduce_partial(int op, long n, const double* __restrict__ x, const double* __r
   }
 }
 
+// One warp: lane l folds partials l, l+32, ... in order, then a fixed shuffle tree.
 extern "C" __global__ void k_reduce_final(int op, int nparts, const double* __restrict__ partial,
                                           double* __restrict__ out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    double v = red_identity(op);
-    for (int p = 0; p < nparts; ++p) v = red_combine(op, v, partial[p]);
-    *out = v;
-  }
+  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+  double v = red_identity(op);
+  for (int p = threadIdx.x; p < nparts; p += 32) v = red_combine(op, v, partial[p]);
+  for (int o = 16; o > 0; o >>= 1) v = red_combine(op, v, __shfl_xor_sync(0xffffffffu, v, o));
+  if (threadIdx.x == 0) *out = v;
 }
 
 // Diagonal max |H_ii| of a dense m x m matrix (for the proportional static shift).
