@@ -180,6 +180,18 @@ int32_t sdpxg_residual(sdpxg_ctx *ctx, const double *bx, const double *bz, const
  * PSDTriangleCone::step_length (cones/psdtrianglecone.rs:475-576, 1168-1231). */
 int32_t sdpxg_step_length(sdpxg_ctx *ctx, const double *dz, const double *ds, double amax,
                           uint32_t mode, double *out_alpha, uint32_t *status);
+/* Exact product C = op(A) op(B) of MpFloat<limbs> matrices (the reference's in-memory layout:
+ * limbs u64 least significant first, i32 kind = sign * MPFR kind (2 zero, 3 regular), i32
+ * exponent; 8 * limbs + 8 bytes per element), column-major with leading dimensions lda / ldb;
+ * C is m x n column-major (ldc = m).  Every entry is the exact dot product rounded once to
+ * 64 * limbs bits, ties to even -- bitwise MpFloat::dot_fma.  ta, tb are 'N' or 'T'; upper_only
+ * computes the entries i <= j and writes zeros below.  limbs 1..16.  Non-finite operands
+ * return 2 with *status = SDPXG_ST_NONFINITE.  Replaces rns_blas::gemm
+ * (crates/solver/src/algebra/dense/blas/rns_blas.rs:2134-2417) with residue products modulo
+ * primes below 2^21 on the GPU. */
+int32_t sdpxg_rns_gemm(sdpxg_ctx *ctx, uint32_t limbs, char ta, char tb, uint64_t m, uint64_t n,
+                       uint64_t k, const void *A, uint64_t lda, const void *B, uint64_t ldb,
+                       uint32_t upper_only, void *C, uint32_t *status);
 /* y = op(x) per PSD block: op 0 W, 1 W', 2 W^-1, 3 W^-T, 4 Hs = W'W, 5 Hs^-1.
  * Replaces mul_W / mul_Winv / PsdBlock::apply (cones/psdtrianglecone.rs:860-917,
  * kkt/condensed/psd.rs:1968-2027). */

@@ -1,0 +1,179 @@
+"""Exact-rounding restatement of the MPFR contract used by the RNS BLAS -- TEST ORACLE.
+
+Test infrastructure only (see ``oracle/__init__``).  Restates, in Python integers:
+
+* ``MpFloat<N>`` (crates/arithmetic/src/lib.rs:333-349): N x 64-bit mantissa limbs, least
+  significant first, an i32 MPFR kind whose sign is the value's sign (2 = zero, 3 = regular)
+  and an i32 exponent; a regular value is M * 2^(exponent - 64N) with 2^(64N-1) <= M < 2^(64N);
+* ``from_scaled_integer`` (crates/arithmetic/src/exactdot.rs:1316-1392): round an exact integer
+  times a power of two to 64N bits, ties to even;
+* ``dot_fma`` (crates/arithmetic/src/lib.rs:535-545, exactdot.rs:53-70): the exact dot product
+  rounded once -- the value every RNS product must reproduce bitwise
+  (crates/solver/src/algebra/dense/blas/rns_blas_tests.rs:30-144);
+* the reference's RNS test-input generator (rns_blas_tests.rs:4-28): a 64-bit LCG, values
+  (2u - 1) / (u + 1/2) rounded at the working precision, 5% zeros, and a power-of-two spread.
+
+Correct rounding is a definition, so this oracle is pinned by it; ``tests/test_oracle_pins.py``
+cross-checks the rounding against mpmath.
+"""
+from __future__ import annotations
+
+import struct
+from fractions import Fraction
+from typing import List, Sequence, Tuple
+
+ZERO_KIND = 2
+REGULAR_KIND = 3
+MASK64 = (1 << 64) - 1
+
+
+class Mp:
+    """A finite MpFloat<N> value: (negative, mantissa M, exponent e) or zero."""
+
+    __slots__ = ("n", "neg", "mant", "exp")
+
+    def __init__(self, n: int, neg: bool = False, mant: int = 0, exp: int = 0):
+        self.n, self.neg, self.mant, self.exp = n, neg, mant, exp
+
+    @property
+    def p(self) -> int:
+        return 64 * self.n
+
+    def is_zero(self) -> bool:
+        return self.mant == 0
+
+    def fraction(self) -> Fraction:
+        if self.mant == 0:
+            return Fraction(0)
+        v = Fraction(self.mant) * Fraction(2) ** (self.exp - self.p)
+        return -v if self.neg else v
+
+    def pack(self) -> bytes:
+        limbs = [(self.mant >> (64 * q)) & MASK64 for q in range(self.n)]
+        if self.mant == 0:
+            return struct.pack(f"<{self.n}Qii", *([0] * self.n), ZERO_KIND, 0)
+        kind = -REGULAR_KIND if self.neg else REGULAR_KIND
+        return struct.pack(f"<{self.n}Qii", *limbs, kind, self.exp)
+
+    @staticmethod
+    def unpack(n: int, raw: bytes) -> "Mp":
+        vals = struct.unpack(f"<{n}Qii", raw)
+        limbs, kind, exp = vals[:n], vals[n], vals[n + 1]
+        if abs(kind) == ZERO_KIND:
+            return Mp(n)
+        if abs(kind) != REGULAR_KIND:
+            raise ValueError(f"non-finite kind {kind}")
+        mant = sum(int(l) << (64 * q) for q, l in enumerate(limbs))
+        return Mp(n, kind < 0, mant, exp)
+
+    def __eq__(self, other) -> bool:
+        if self.is_zero() or other.is_zero():
+            return self.is_zero() and other.is_zero()
+        return (self.neg, self.mant, self.exp) == (other.neg, other.mant, other.exp)
+
+    def __repr__(self) -> str:
+        return f"Mp({'-' if self.neg else '+'}{self.mant:#x}*2^({self.exp}-{self.p}))"
+
+
+def from_scaled_integer(n: int, negative: bool, mag: int, scale: int) -> Mp:
+    """Round mag * 2^scale to 64n bits, ties to even (exactdot.rs:1316-1392)."""
+    if mag == 0:
+        return Mp(n)
+    p = 64 * n
+    bits = mag.bit_length()
+    shift = bits - p
+    if shift > 0:
+        top = mag >> shift
+        round_bit = (mag >> (shift - 1)) & 1
+        sticky = (mag & ((1 << (shift - 1)) - 1)) != 0
+        if round_bit and (sticky or (top & 1)):
+            top += 1
+            if top >> p:
+                top >>= 1
+                shift += 1
+        mant = top
+    else:
+        mant = mag << (-shift)
+    return Mp(n, negative, mant, scale + shift + p)
+
+
+def from_fraction(n: int, x: Fraction) -> Mp:
+    """Correctly rounded (ties to even) 64n-bit value of a rational."""
+    if x == 0:
+        return Mp(n)
+    neg = x < 0
+    x = abs(x)
+    p = 64 * n
+    num, den = x.numerator, x.denominator
+    # choose s with 2^(p+2) <= num * 2^s / den so the quotient carries guard bits
+    s = p + 2 - (num.bit_length() - den.bit_length()) + 1
+    if s >= 0:
+        q, r = divmod(num << s, den)
+    else:
+        q, r = divmod(num, den << (-s))
+    # q * 2^-s + r / den * 2^-s; fold the remainder into a sticky bit
+    mag = (q << 1) | (1 if r else 0)
+    return from_scaled_integer(n, neg, mag, -s - 1)
+
+
+def exact_dot(n: int, pairs: Sequence[Tuple[Mp, Mp]]) -> Mp:
+    """sum a*b computed exactly and rounded once (the dot_fma contract)."""
+    terms = [(a, b) for a, b in pairs if not a.is_zero() and not b.is_zero()]
+    if not terms:
+        return Mp(n)
+    low = min((a.exp - a.p) + (b.exp - b.p) for a, b in terms)
+    total = 0
+    for a, b in terms:
+        v = (a.mant * b.mant) << ((a.exp - a.p) + (b.exp - b.p) - low)
+        total += -v if (a.neg != b.neg) else v
+    return from_scaled_integer(n, total < 0, abs(total), low)
+
+
+def gemm(n: int, ta: str, tb: str, m: int, ncols: int, k: int, A: List[Mp], lda: int,
+         B: List[Mp], ldb: int) -> List[Mp]:
+    """C = op(A) op(B) with every entry an exact dot rounded once (rns_blas_tests.rs:30-59)."""
+    def at(i, q):
+        return A[i + q * lda] if ta == "N" else A[q + i * lda]
+
+    def bt(q, j):
+        return B[q + j * ldb] if tb == "N" else B[j + q * ldb]
+
+    return [exact_dot(n, [(at(i, q), bt(q, j)) for q in range(k)])
+            for j in range(ncols) for i in range(m)]
+
+
+class Lcg:
+    """The reference's test generator (rns_blas_tests.rs:4-13)."""
+
+    def __init__(self, seed: int):
+        self.s = seed & MASK64
+
+    def next(self) -> float:
+        self.s = (self.s * 6364136223846793005 + 1442695040888963407) & MASK64
+        return (self.s >> 11) / float(1 << 53)
+
+
+def random_values(n: int, rng: Lcg, length: int, spread: int) -> List[Mp]:
+    """rns_blas_tests.rs:15-28: 5% zeros, (2u-1)/(u+1/2) at 64n bits, times 2^shift."""
+    out = []
+    for _ in range(length):
+        if rng.next() < 0.05:
+            out.append(Mp(n))
+            continue
+        num = Fraction(rng.next() * 2.0 - 1.0)
+        den = Fraction(rng.next() + 0.5)
+        shift = int(rng.next() * (2 * spread + 1)) - spread
+        q = from_fraction(n, num / den)
+        if not q.is_zero():
+            q.exp += shift
+        out.append(q)
+    return out
+
+
+def pack_array(vals: Sequence[Mp]) -> bytes:
+    return b"".join(v.pack() for v in vals)
+
+
+def unpack_array(n: int, raw: bytes) -> List[Mp]:
+    size = 8 * n + 8
+    return [Mp.unpack(n, raw[i * size:(i + 1) * size]) for i in range(len(raw) // size)]

@@ -41,11 +41,15 @@ struct sdpxg_ctx {
   std::unique_ptr<HsdSolver> kkt;  // owns the refinement scratch
   DevBuf<double> a, b, c, d, e, f;
   bool uploaded = false;
+  std::shared_ptr<void> rns_ws;  // workspace of the exact (RNS) products, created on first use
 };
 
 namespace sdpxg {
 // The engine of a context with an uploaded problem (nullptr otherwise).
 Engine* ctx_engine(sdpxg_ctx* c) { return (c && c->uploaded) ? c->eng.get() : nullptr; }
+// The engine of any context (no problem needed) and its RNS workspace slot.
+Engine* ctx_engine_any(sdpxg_ctx* c) { return c ? c->eng.get() : nullptr; }
+std::shared_ptr<void>* ctx_rns_slot(sdpxg_ctx* c) { return c ? &c->rns_ws : nullptr; }
 }  // namespace sdpxg
 
 namespace {

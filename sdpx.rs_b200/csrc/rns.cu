@@ -1,0 +1,538 @@
+// Exact products of MpFloat<N> matrices through a residue number system (RNS), on the GPU.
+//
+// Restates the contract of the reference's RNS BLAS (crates/solver/src/algebra/dense/blas/
+// rns_blas.rs:2134-2417 gemm): every entry of C = op(A) op(B) is the exact dot product rounded
+// once to 64N bits, ties to even -- bit-identical to MpFloat::dot_fma (exactdot.rs:53-70).
+//
+// Pipeline (one call):
+//   k_rns_scan      per row of op(A) / column of op(B): lowest set-bit exponent lo and the
+//                   width `bits` of the aligned integers (rns_blas.rs:2164-2183 alignment)
+//   k_rns_residues  every entry as the integer M * 2^(e - 64N - lo) reduced to symmetric
+//                   residues modulo L primes below 2^21 (rns_blas.rs:929-986 panel residues)
+//   k_rns_gemm      one exact FP64 product per prime: symmetric residues keep |r| < 2^20, so
+//                   8192 products sum exactly below 2^53; partial sums are reduced modulo the
+//                   prime every 8192 terms (rns_blas.rs:447-580 per-prime dgemm)
+//   k_rns_crt       Garner's mixed-radix CRT back to the signed integer, then one rounding to
+//                   64N bits, ties to even (rns_blas.rs:1873-2125 CRT and pack,
+//                   exactdot.rs:1316-1392 from_scaled_integer)
+// The number of primes L follows the needed width 2*(64N) + spreads + log2(k) + 2 bits, the
+// same bound as the reference's Plan (rns_blas.rs:2202-2208).
+//
+// Element layout (the reference's in-memory MpFloat<N>, arithmetic/src/lib.rs:333-340):
+//   u64 limbs[N] (least significant first), i32 kind (sign * MPFR kind: 2 zero, 3 regular),
+//   i32 exponent; a regular value is M * 2^(exponent - 64N) with the top bit of M set.
+#include <algorithm>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/sdpx_b200.h"
+#include "engine.cuh"
+
+using namespace sdpxg;
+
+namespace sdpxg {
+extern thread_local std::string g_last_error;
+Engine* ctx_engine_any(sdpxg_ctx* c);
+std::shared_ptr<void>* ctx_rns_slot(sdpxg_ctx* c);
+}  // namespace sdpxg
+
+#define RNS_MAXN 16    // limbs: up to 1024-bit values
+#define RNS_MAXL 160   // primes
+#define RNS_MAXW 56    // 64-bit words of the reconstructed integer
+#define RNS_KC 8192    // exact FP64 terms between two reductions modulo the prime
+#define MP_ZERO 2
+#define MP_REGULAR 3
+#define MP_EXP_MAX ((1 << 30) - 1)
+
+namespace {
+
+__device__ __forceinline__ int elem_kind(const unsigned char* p, int N) {
+  return *reinterpret_cast<const int*>(p + 8 * N);
+}
+__device__ __forceinline__ int elem_exp(const unsigned char* p, int N) {
+  return *reinterpret_cast<const int*>(p + 8 * N + 4);
+}
+
+__device__ __forceinline__ uint32_t pow2mod(long long s, uint32_t p) {
+  unsigned long long r = 1, b = 2 % p;
+  while (s > 0) {
+    if (s & 1) r = r * b % p;
+    b = b * b % p;
+    s >>= 1;
+  }
+  return (uint32_t)r;
+}
+
+}  // namespace
+
+// Scan lines of a matrix view: element (x, y) at index x * sx + y * sy.
+// lo[x] = min over regular entries of (exponent - 64N), bits[x] = max exponent - lo[x].
+extern "C" __global__ void k_rns_scan(const unsigned char* __restrict__ X, int N, int nlines,
+                                      int len, long sx, long sy, int* __restrict__ lo,
+                                      int* __restrict__ bits, int* __restrict__ maxbits,
+                                      uint32_t* __restrict__ status) {
+  const int x = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (x >= nlines) return;
+  const long esz = 8L * N + 8;
+  const int p = 64 * N;
+  int mn = INT_MAX, mx = INT_MIN;
+  bool bad = false;
+  for (int y = lane; y < len; y += 32) {
+    const unsigned char* e = X + (x * sx + y * sy) * esz;
+    int kind = abs(elem_kind(e, N));
+    if (kind == MP_REGULAR) {
+      int ex = elem_exp(e, N);
+      mn = min(mn, ex - p);
+      mx = max(mx, ex);
+    } else if (kind != MP_ZERO) {
+      bad = true;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  bad = __any_sync(0xffffffffu, bad);
+  if (lane == 0) {
+    if (bad) atomicOr(status, SDPXG_ST_NONFINITE);
+    if (mx == INT_MIN) {
+      lo[x] = 0;
+      bits[x] = 0;
+    } else {
+      lo[x] = mn;
+      bits[x] = mx - mn;
+      atomicMax(maxbits, mx - mn);
+    }
+  }
+}
+
+// Symmetric residues of every entry of a view for L primes: out[t * plane + x + y * ldx] when
+// xmajor, else out[t * plane + y + x * ldy].
+extern "C" __global__ void k_rns_residues(const unsigned char* __restrict__ X, int N, int nlines,
+                                          int len, long sx, long sy, const int* __restrict__ lo,
+                                          int L, const uint32_t* __restrict__ primes,
+                                          const uint32_t* __restrict__ W, double* __restrict__ out,
+                                          long plane, int xmajor) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)nlines * len) return;
+  const int x = (int)(idx % nlines), y = (int)(idx / nlines);
+  const long esz = 8L * N + 8;
+  const unsigned char* e = X + (x * sx + y * sy) * esz;
+  const long o = xmajor ? (x + (long)y * nlines) : (y + (long)x * len);
+  const int kind = elem_kind(e, N);
+  if (abs(kind) != MP_REGULAR) {
+    for (int t = 0; t < L; ++t) out[t * plane + o] = 0.0;
+    return;
+  }
+  const bool neg = kind < 0;
+  const long long shift = (long long)elem_exp(e, N) - 64LL * N - lo[x];
+  const unsigned long long* limbs = reinterpret_cast<const unsigned long long*>(e);
+  for (int t = 0; t < L; ++t) {
+    const uint32_t p = primes[t];
+    unsigned long long r = 0;
+    for (int q = 0; q < N; ++q) r = (r + (limbs[q] % p) * W[t * RNS_MAXN + q]) % p;
+    r = r * pow2mod(shift, p) % p;
+    long long s = (long long)r;
+    if (s > (long long)(p / 2)) s -= p;
+    if (neg) s = -s;
+    out[t * plane + o] = (double)s;
+  }
+}
+
+// Per-prime exact products: C_t = A_t B_t (m x n, inner k) with symmetric residues in FP64,
+// reduced modulo p_t every RNS_KC terms.  grid (m/64, n/64, L), 256 threads, 4 x 4 per thread.
+extern "C" __global__ void __launch_bounds__(256)
+k_rns_gemm(const double* __restrict__ RA, const double* __restrict__ RB, double* __restrict__ RC,
+           int m, int n, int k, const uint32_t* __restrict__ primes, long planeA, long planeB,
+           long planeC, int upper_only) {
+  __shared__ double As[32][65];  // [k][row]
+  __shared__ double Bs[32][65];  // [k][col]
+  const int t = blockIdx.z;
+  const int i0 = blockIdx.x * 64, j0 = blockIdx.y * 64;
+  if (upper_only && i0 > j0 + 63) return;
+  const double p = (double)primes[t];
+  const double* A = RA + t * planeA;
+  const double* B = RB + t * planeB;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  int since = 0;
+  for (int k0 = 0; k0 < k; k0 += 32) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < 64 * 32; e += 256) {
+      int r = e % 64, c = e / 64;  // A: row r of the tile, k offset c
+      As[c][r] = (i0 + r < m && k0 + c < k) ? A[(i0 + r) + (long)(k0 + c) * m] : 0.0;
+      int kr = e % 32, cc = e / 32;  // B: k offset kr, column cc of the tile
+      Bs[kr][cc] = (k0 + kr < k && j0 + cc < n) ? B[(k0 + kr) + (long)(j0 + cc) * k] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < 32; ++kk) {
+      double x[4], y[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) x[a] = As[kk][tx + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) y[b] = Bs[kk][ty + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(x[a], y[b], acc[a][b]);
+    }
+    since += 32;
+    if (since >= RNS_KC) {  // keep every partial sum exact: reduce modulo p
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] -= p * rint(acc[a][b] / p);
+      since = 0;
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      int i = i0 + tx + 16 * a, j = j0 + ty + 16 * b;
+      if (i < m && j < n) RC[t * planeC + i + (long)j * m] = acc[a][b] - p * rint(acc[a][b] / p);
+    }
+}
+
+// Garner CRT of the L residues of every output, then one rounding to 64N bits (ties to even).
+extern "C" __global__ void k_rns_crt(const double* __restrict__ RC, long planeC, int m, int n,
+                                     int L, int WW, const uint32_t* __restrict__ primes,
+                                     const uint32_t* __restrict__ inv,
+                                     const uint32_t* __restrict__ pmod,
+                                     const unsigned long long* __restrict__ Mbig,
+                                     const unsigned long long* __restrict__ halfM,
+                                     const int* __restrict__ loA, const int* __restrict__ loB,
+                                     int N, int upper_only, unsigned char* __restrict__ C,
+                                     uint32_t* __restrict__ status) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)m * n) return;
+  const int i = (int)(idx % m), j = (int)(idx / m);
+  unsigned char* out = C + idx * (8L * N + 8);
+  unsigned long long* ol = reinterpret_cast<unsigned long long*>(out);
+  int* okind = reinterpret_cast<int*>(out + 8 * N);
+  int* oexp = okind + 1;
+  auto write_zero = [&]() {
+    for (int q = 0; q < N; ++q) ol[q] = 0;
+    *okind = MP_ZERO;
+    *oexp = 0;
+  };
+  if (upper_only && i > j) {
+    write_zero();
+    return;
+  }
+  uint32_t v[RNS_MAXL];
+  for (int t = 0; t < L; ++t) {
+    const uint32_t p = primes[t];
+    long long r = (long long)RC[t * planeC + idx];
+    r %= (long long)p;
+    if (r < 0) r += p;
+    unsigned long long u = 0;
+    for (int s = 0; s < t; ++s) u = (u + (unsigned long long)v[s] * pmod[s * RNS_MAXL + t]) % p;
+    unsigned long long d = ((unsigned long long)r + p - u) % p;
+    v[t] = (uint32_t)(d * inv[t] % p);
+  }
+  unsigned long long S[RNS_MAXW];
+  for (int w = 0; w < WW; ++w) S[w] = 0;
+  S[0] = v[L - 1];
+  for (int t = L - 2; t >= 0; --t) {  // S = S * p_t + v_t
+    unsigned long long carry = v[t];
+    const unsigned long long p = primes[t];
+    for (int w = 0; w < WW; ++w) {
+      unsigned long long lo = S[w] * p;
+      unsigned long long hi = __umul64hi(S[w], p);
+      unsigned long long sum = lo + carry;
+      hi += (sum < lo);
+      S[w] = sum;
+      carry = hi;
+    }
+  }
+  // sign: S > (M - 1) / 2 means S - M < 0
+  bool neg = false;
+  for (int w = WW - 1; w >= 0; --w) {
+    if (S[w] != halfM[w]) {
+      neg = S[w] > halfM[w];
+      break;
+    }
+  }
+  if (neg) {  // magnitude M - S
+    unsigned long long borrow = 0;
+    for (int w = 0; w < WW; ++w) {
+      unsigned long long a = Mbig[w], b = S[w];
+      unsigned long long d = a - b - borrow;
+      borrow = (a < b) || (a - b < borrow);
+      S[w] = d;
+    }
+  }
+  int top = -1;
+  for (int w = WW - 1; w >= 0; --w)
+    if (S[w]) {
+      top = w;
+      break;
+    }
+  if (top < 0) {
+    write_zero();
+    return;
+  }
+  const int bitlen = top * 64 + 64 - __clzll(S[top]);
+  const int pbits = 64 * N;
+  int shift = bitlen - pbits;
+  auto window = [&](int start) -> unsigned long long {  // bits [start, start + 64) of S
+    int word = (start >= 0) ? start / 64 : -((-start + 63) / 64);
+    int off = start - 64 * word;
+    unsigned long long lo = (word >= 0 && word < WW) ? S[word] : 0ull;
+    unsigned long long hi = (word + 1 >= 0 && word + 1 < WW) ? S[word + 1] : 0ull;
+    return (lo >> off) | (off ? (hi << (64 - off)) : 0ull);
+  };
+  unsigned long long res[RNS_MAXN];
+  for (int q = 0; q < N; ++q) res[q] = window(shift + 64 * q);
+  if (shift > 0) {
+    const int rb = shift - 1;
+    const bool round_bit = (S[rb / 64] >> (rb % 64)) & 1ull;
+    bool sticky = false;
+    for (int w = 0; w < rb / 64; ++w) sticky = sticky || (S[w] != 0);
+    if (rb % 64) sticky = sticky || ((S[rb / 64] & ((1ull << (rb % 64)) - 1)) != 0);
+    if (round_bit && (sticky || (res[0] & 1ull))) {
+      bool carry = true;
+      for (int q = 0; q < N && carry; ++q) {
+        res[q] += 1;
+        carry = (res[q] == 0);
+      }
+      if (carry) {
+        res[N - 1] = 1ull << 63;
+        shift += 1;
+      }
+    }
+  }
+  const long long exponent = (long long)loA[i] + loB[j] + shift + pbits;
+  if (exponent > MP_EXP_MAX || exponent < -MP_EXP_MAX) {
+    atomicOr(status, SDPXG_ST_NONFINITE);
+    write_zero();
+    return;
+  }
+  for (int q = 0; q < N; ++q) ol[q] = res[q];
+  *okind = neg ? -MP_REGULAR : MP_REGULAR;
+  *oexp = (int)exponent;
+}
+
+namespace {
+
+// Host tables of one prime set (largest primes below 2^21, descending).
+struct PrimeTables {
+  int L = 0, WW = 0;
+  std::vector<uint32_t> primes, W, inv, pmod;
+  std::vector<unsigned long long> M, half;
+};
+
+const std::vector<uint32_t>& prime_list() {
+  static std::vector<uint32_t> ps;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    const uint32_t top = 1u << 21;
+    std::vector<bool> comp(top, false);
+    for (uint32_t i = 2; (uint64_t)i * i < top; ++i)
+      if (!comp[i])
+        for (uint32_t j = i * i; j < top; j += i) comp[j] = true;
+    for (uint32_t q = top - 1; q > 2 && ps.size() < RNS_MAXL; --q)
+      if (!comp[q]) ps.push_back(q);
+  });
+  return ps;
+}
+
+uint64_t powmod64(uint64_t b, uint64_t e, uint64_t p) {
+  uint64_t r = 1 % p;
+  b %= p;
+  while (e) {
+    if (e & 1) r = (unsigned __int128)r * b % p;
+    b = (unsigned __int128)b * b % p;
+    e >>= 1;
+  }
+  return r;
+}
+
+PrimeTables make_tables(int L) {
+  PrimeTables T;
+  const auto& ps = prime_list();
+  T.L = L;
+  T.primes.assign(ps.begin(), ps.begin() + L);
+  T.W.assign((size_t)L * RNS_MAXN, 0);
+  for (int t = 0; t < L; ++t)
+    for (int q = 0; q < RNS_MAXN; ++q) T.W[t * RNS_MAXN + q] = (uint32_t)powmod64(2, 64ull * q, T.primes[t]);
+  T.inv.assign(L, 0);
+  T.pmod.assign((size_t)RNS_MAXL * RNS_MAXL, 0);
+  for (int t = 0; t < L; ++t) {
+    uint64_t p = T.primes[t], prod = 1;
+    for (int s = 0; s < t; ++s) {
+      T.pmod[s * RNS_MAXL + t] = (uint32_t)prod;  // prod_{q<s} p_q mod p_t
+      prod = prod * (T.primes[s] % p) % p;
+    }
+    T.inv[t] = (uint32_t)powmod64(prod, p - 2, p);  // (prod_{q<t} p_q)^-1 mod p_t
+  }
+  // M = prod p_t, half = (M - 1) / 2
+  double log2m = 0;
+  for (uint32_t p : T.primes) log2m += std::log2((double)p);
+  T.WW = std::min(RNS_MAXW, (int)(log2m / 64) + 2);
+  T.M.assign(T.WW, 0);
+  T.M[0] = 1;
+  for (uint32_t p : T.primes) {
+    unsigned __int128 carry = 0;
+    for (int w = 0; w < T.WW; ++w) {
+      unsigned __int128 v = (unsigned __int128)T.M[w] * p + carry;
+      T.M[w] = (unsigned long long)v;
+      carry = v >> 64;
+    }
+  }
+  T.half = T.M;
+  T.half[0] -= 1;  // M is odd
+  for (int w = 0; w < T.WW; ++w) {
+    unsigned long long next = (w + 1 < T.WW) ? T.half[w + 1] : 0;
+    T.half[w] = (T.half[w] >> 1) | (next << 63);
+  }
+  return T;
+}
+
+struct RnsWorkspace {
+  DevBuf<unsigned char> a, b, c;
+  DevBuf<int> loA, loB, bitsA, bitsB, maxbits;
+  DevBuf<uint32_t> status, primes, W, inv, pmod;
+  DevBuf<unsigned long long> M, half;
+  DevBuf<double> RA, RB, RC;
+  std::map<int, PrimeTables> tables;
+  int uploaded_L = -1;
+};
+
+template <typename T>
+void grow(DevBuf<T>& b, size_t n) {
+  if (b.n < std::max<size_t>(n, 1)) b.alloc(std::max<size_t>(n, 1));
+}
+
+}  // namespace
+
+extern "C" int32_t sdpxg_rns_gemm(sdpxg_ctx* ctx, uint32_t limbs, char ta, char tb, uint64_t m,
+                                  uint64_t n, uint64_t k, const void* A, uint64_t lda,
+                                  const void* B, uint64_t ldb, uint32_t upper_only, void* C,
+                                  uint32_t* status) {
+  try {
+    Engine* E = ctx_engine_any(ctx);
+    if (!E) throw std::invalid_argument("null context");
+    const int N = (int)limbs;
+    if (N < 1 || N > RNS_MAXN) {
+      g_last_error = "sdpxg_rns_gemm: limbs must be in 1..16";
+      return 2;
+    }
+    if ((ta != 'N' && ta != 'T') || (tb != 'N' && tb != 'T')) throw std::invalid_argument("bad transpose flag");
+    if (m == 0 || n == 0) return 0;
+    if (!A || !B || !C) throw std::invalid_argument("null pointer");
+    if (m > (1u << 30) || n > (1u << 30) || k > (1u << 30)) throw std::invalid_argument("size overflow");
+    const uint64_t ar = (ta == 'N') ? m : k, ac = (ta == 'N') ? k : m;
+    const uint64_t br = (tb == 'N') ? k : n, bc = (tb == 'N') ? n : k;
+    if (lda < std::max<uint64_t>(ar, 1) || ldb < std::max<uint64_t>(br, 1))
+      throw std::invalid_argument("leading dimension too small");
+    const size_t esz = 8 * (size_t)N + 8;
+    const size_t na = ac ? lda * (ac - 1) + ar : 0, nb = bc ? ldb * (bc - 1) + br : 0;
+    auto slot = ctx_rns_slot(ctx);
+    if (!*slot) *slot = std::make_shared<RnsWorkspace>();
+    RnsWorkspace& ws = *static_cast<RnsWorkspace*>(slot->get());
+    cudaStream_t st = E->st;
+    check(cudaSetDevice(E->device), "cudaSetDevice");
+    grow(ws.a, na * esz);
+    grow(ws.b, nb * esz);
+    grow(ws.c, m * n * esz);
+    if (na) ws.a.upload(static_cast<const unsigned char*>(A), na * esz, st);
+    if (nb) ws.b.upload(static_cast<const unsigned char*>(B), nb * esz, st);
+    grow(ws.loA, m); grow(ws.bitsA, m); grow(ws.loB, n); grow(ws.bitsB, n);
+    grow(ws.maxbits, 2); grow(ws.status, 1);
+    check(cudaMemsetAsync(ws.maxbits.p, 0, 2 * sizeof(int), st), "memset");
+    check(cudaMemsetAsync(ws.status.p, 0, sizeof(uint32_t), st), "memset");
+    // op(A) rows: (i, l) -> i*sx + l*sy ; op(B) columns: (j, l) -> j*sx + l*sy
+    const long asx = (ta == 'N') ? 1 : (long)lda, asy = (ta == 'N') ? (long)lda : 1;
+    const long bsx = (tb == 'N') ? (long)ldb : 1, bsy = (tb == 'N') ? 1 : (long)ldb;
+    if (k) {
+      ++g_launches, k_rns_scan<<<(unsigned)((m + 7) / 8), 256, 0, st>>>(ws.a, N, (int)m, (int)k, asx, asy,
+                                                                     ws.loA, ws.bitsA, ws.maxbits,
+                                                                     ws.status);
+      ++g_launches, k_rns_scan<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(ws.b, N, (int)n, (int)k, bsx, bsy,
+                                                                     ws.loB, ws.bitsB, ws.maxbits.p + 1,
+                                                                     ws.status);
+    } else {
+      check(cudaMemsetAsync(ws.loA.p, 0, m * sizeof(int), st), "memset");
+      check(cudaMemsetAsync(ws.loB.p, 0, n * sizeof(int), st), "memset");
+    }
+    int hb[2] = {0, 0};
+    uint32_t hs = 0;
+    check(cudaMemcpyAsync(hb, ws.maxbits.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+    check(cudaMemcpyAsync(&hs, ws.status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "D2H");
+    check(cudaStreamSynchronize(st), "sync");
+    if (hs) {
+      if (status) *status = hs;
+      g_last_error = "sdpxg_rns_gemm: non-finite operands are not supported";
+      return 2;
+    }
+    // width of |sum| < k 2^(bitsA + bitsB); the CRT range must exceed twice that
+    int lg = 0;
+    while ((1ull << lg) < std::max<uint64_t>(k, 1)) ++lg;
+    const double needed = (double)hb[0] + hb[1] + lg + 2;
+    const auto& ps = prime_list();
+    int L = 0;
+    double acc = 0;
+    while (L < RNS_MAXL && acc <= needed) acc += std::log2((double)ps[L++]);
+    if (acc <= needed || (int)(acc / 64) + 2 > RNS_MAXW) {
+      g_last_error = "sdpxg_rns_gemm: exponent spread too wide for the prime set";
+      return 2;
+    }
+    auto it = ws.tables.find(L);
+    if (it == ws.tables.end()) it = ws.tables.emplace(L, make_tables(L)).first;
+    const PrimeTables& T = it->second;
+    if (ws.uploaded_L != L) {
+      grow(ws.primes, L); grow(ws.W, T.W.size()); grow(ws.inv, L); grow(ws.pmod, T.pmod.size());
+      grow(ws.M, T.WW); grow(ws.half, T.WW);
+      ws.primes.upload(T.primes.data(), L, st);
+      ws.W.upload(T.W.data(), T.W.size(), st);
+      ws.inv.upload(T.inv.data(), L, st);
+      ws.pmod.upload(T.pmod.data(), T.pmod.size(), st);
+      ws.M.upload(T.M.data(), T.WW, st);
+      ws.half.upload(T.half.data(), T.WW, st);
+      ws.uploaded_L = L;
+    }
+    const long planeA = (long)(m * std::max<uint64_t>(k, 1)), planeB = (long)(std::max<uint64_t>(k, 1) * n);
+    const long planeC = (long)(m * n);
+    grow(ws.RA, (size_t)L * planeA);
+    grow(ws.RB, (size_t)L * planeB);
+    grow(ws.RC, (size_t)L * planeC);
+    if (k) {
+      ++g_launches, k_rns_residues<<<(unsigned)((m * k + 255) / 256), 256, 0, st>>>(
+          ws.a, N, (int)m, (int)k, asx, asy, ws.loA, L, ws.primes, ws.W, ws.RA, planeA, 1);
+      ++g_launches, k_rns_residues<<<(unsigned)((n * k + 255) / 256), 256, 0, st>>>(
+          ws.b, N, (int)n, (int)k, bsx, bsy, ws.loB, L, ws.primes, ws.W, ws.RB, planeB, 0);
+      dim3 grid((unsigned)((m + 63) / 64), (unsigned)((n + 63) / 64), (unsigned)L);
+      ++g_launches, k_rns_gemm<<<grid, 256, 0, st>>>(ws.RA, ws.RB, ws.RC, (int)m, (int)n, (int)k,
+                                                     ws.primes, planeA, planeB, planeC,
+                                                     upper_only ? 1 : 0);
+    } else {
+      check(cudaMemsetAsync(ws.RC.p, 0, (size_t)L * planeC * sizeof(double), st), "memset");
+    }
+    ++g_launches, k_rns_crt<<<(unsigned)((m * n + 127) / 128), 128, 0, st>>>(
+        ws.RC, planeC, (int)m, (int)n, L, T.WW, ws.primes, ws.inv, ws.pmod, ws.M, ws.half, ws.loA,
+        ws.loB, N, upper_only ? 1 : 0, ws.c, ws.status);
+    check(cudaGetLastError(), "rns launch");
+    check(cudaMemcpyAsync(C, ws.c.p, m * n * esz, cudaMemcpyDeviceToHost, st), "D2H");
+    check(cudaMemcpyAsync(&hs, ws.status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "D2H");
+    check(cudaStreamSynchronize(st), "sync");
+    if (status) *status = hs;
+    return 0;
+  } catch (const std::invalid_argument& e) {
+    g_last_error = e.what();
+    return 1;
+  } catch (const std::exception& e) {
+    g_last_error = std::string("internal error: ") + e.what();
+    return 5;
+  }
+}

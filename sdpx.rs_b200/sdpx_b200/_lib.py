@@ -88,6 +88,8 @@ SIGNATURES = {
     "sdpxg_residual": (i32, [C.c_void_p, PD, PD, PD, PD, PD, PD, PD]),
     "sdpxg_step_length": (i32, [C.c_void_p, PD, PD, f64, u32, PD, PU32]),
     "sdpxg_cone_apply": (i32, [C.c_void_p, u32, PD, PD]),
+    "sdpxg_rns_gemm": (i32, [C.c_void_p, u32, C.c_char, C.c_char, u64, u64, u64, C.c_void_p, u64,
+                             C.c_void_p, u64, u32, C.c_void_p, PU32]),
 }
 
 _lib = None

@@ -305,6 +305,16 @@ class KernelContext:
                   C.byref(a), C.byref(st))
         return a.value, st.value
 
+    def rns_gemm(self, limbs: int, ta: str, tb: str, m: int, n: int, k: int, A: bytes, lda: int,
+                 B: bytes, ldb: int, upper_only: bool = False):
+        """Exact MpFloat<limbs> product (raw element bytes in, raw bytes out)."""
+        esz = 8 * limbs + 8
+        out = C.create_string_buffer(max(m * n * esz, 1))
+        st = C.c_uint32()
+        _lib.call("sdpxg_rns_gemm", self._h, limbs, ta.encode(), tb.encode(), m, n, k,
+                  C.c_char_p(A), lda, C.c_char_p(B), ldb, int(upper_only), out, C.byref(st))
+        return out.raw[:m * n * esz], st.value
+
     def cone_apply(self, op, x):
         x = np.ascontiguousarray(x, dtype=np.float64)
         y = np.empty(self.m)
