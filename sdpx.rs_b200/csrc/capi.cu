@@ -253,6 +253,7 @@ struct sdpx_handle {
   HostProblem equil;  // equilibrated data
   Equilibration eq;
   std::unique_ptr<Engine> eng;
+  std::unique_ptr<HsdSolver> hsd;  // device work vectors, allocated by the first solve
   bool solved = false;
   Info info;
   PhaseTimes times;
@@ -411,13 +412,15 @@ int32_t sdpx_solve(sdpx_handle* h) {
   return boundary([&] {
     operate(h, [](sdpx_handle& hh) {
       hh.solved = false;
-      HsdSolver solver(*hh.eng, hh.equil, hh.eq, hh.settings);
+      if (hh.hsd) hh.hsd->load(hh.equil);
+      else hh.hsd = std::make_unique<HsdSolver>(*hh.eng, hh.equil, hh.eq, hh.settings);
+      HsdSolver& solver = *hh.hsd;
       solver.solve();
       hh.info = solver.info;
       hh.times = solver.times;
-      hh.x = std::move(solver.hx);
-      hh.s = std::move(solver.hs);
-      hh.z = std::move(solver.hz);
+      hh.x = solver.hx;
+      hh.s = solver.hs;
+      hh.z = solver.hz;
       hh.solved = true;
     });
   });

@@ -17,6 +17,7 @@
 #define SDPXG_CONE_THREADS 1024   // one CTA per PSD block: one warp per Jacobi rotation pair
 #define SDPXG_RSQRT2 0.70710678118654752440
 #define SDPXG_SQRT2 1.41421356237309504880
+#define SDPXG_CHOL_SCRATCH (3 * SDPXG_NMAX)  // doubles of shared scratch for cta_cholesky_lower
 
 // Device status bits reported by the kernels (read back by the host after each phase).
 enum SdpxgStatus : uint32_t {
@@ -26,6 +27,7 @@ enum SdpxgStatus : uint32_t {
   SDPXG_ST_NONFINITE = 4u,        // a non-finite value was produced
   SDPXG_ST_PIVOT_FAIL = 8u,       // clearly negative or non-finite Schur pivot
   SDPXG_ST_EIG_FAIL = 16u,        // eigenvalue bisection did not converge
+  SDPXG_ST_SYNC_TIMEOUT = 32u,    // a bounded inter-CTA wait gave up (no progress)
 };
 
 struct BlockDesc {
@@ -147,31 +149,44 @@ __device__ __forceinline__ void cta_gemm(double* C, const double* A, bool ta, co
 
 // In-place lower Cholesky A = L L' (lower triangle of A used).  The update is lagged so
 // one barrier per column suffices: the trailing matrix is updated with the unscaled
-// column divided by the pivot, and columns are scaled at the end.  Returns false (CTA
-// uniform) when a pivot is not positive and finite.  `piv` is n doubles of shared memory.
+// column divided by the pivot, and columns are scaled at the end.  The thread that
+// finishes the next diagonal entry computes its reciprocal once and publishes it for the
+// next step (0 marks a pivot that is not positive and finite: the reciprocal of a finite
+// positive double is never 0).  Returns false (CTA uniform) on such a pivot.
+// `piv` is SDPXG_CHOL_SCRATCH doubles of shared memory: pivots, reciprocals, roots.
 __device__ inline bool cta_cholesky_lower(double* A, int n, double* piv) {
+  double* pinv = piv + SDPXG_NMAX;
+  double* root = pinv + SDPXG_NMAX;
+  if (threadIdx.x == 0 && n > 0) {
+    const double d = SM(A, 0, 0);
+    piv[0] = d;
+    pinv[0] = (d > 0.0 && isfinite(d)) ? 1.0 / d : 0.0;
+  }
   for (int k = 0; k < n; ++k) {
     __syncthreads();
-    double d = SM(A, k, k);
-    if (!(d > 0.0) || !isfinite(d)) {
+    const double dinv = pinv[k];  // written in step k - 1, not touched in step k
+    if (dinv == 0.0) {
       __syncthreads();
       return false;
     }
-    if (threadIdx.x == 0) piv[k] = d;
-    int rem = n - k - 1;
-    double dinv = 1.0 / d;
-    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
-      int i = k + 1 + e % rem, j = k + 1 + e / rem;
-      if (i < j) continue;
-      SM(A, i, j) -= SM(A, i, k) * SM(A, j, k) * dinv;
+    for (int e = threadIdx.x; e < SDPXG_NMAX * SDPXG_NMAX; e += blockDim.x) {
+      const int i = e & (SDPXG_NMAX - 1), j = e / SDPXG_NMAX;
+      if (j <= k || i < j || i >= n) continue;
+      const double v = SM(A, i, j) - SM(A, i, k) * SM(A, j, k) * dinv;
+      SM(A, i, j) = v;
+      if (i == k + 1 && j == k + 1) {  // the next pivot is final now
+        piv[k + 1] = v;
+        pinv[k + 1] = (v > 0.0 && isfinite(v)) ? 1.0 / v : 0.0;
+      }
     }
   }
   __syncthreads();
+  for (int j = threadIdx.x; j < n; j += blockDim.x) root[j] = sqrt(piv[j]);
+  __syncthreads();
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     int i = e % n, j = e / n;
-    double r = sqrt(piv[j]);
-    if (i > j) SM(A, i, j) /= r;
-    else if (i == j) SM(A, i, j) = r;
+    if (i > j) SM(A, i, j) /= root[j];
+    else if (i == j) SM(A, i, j) = root[j];
     else SM(A, i, j) = 0.0;
   }
   __syncthreads();

@@ -18,7 +18,7 @@ constexpr int kMat = SDPXG_LD * SDPXG_NMAX;  // doubles per shared matrix
 // ---------------------------------------------------------------------------------------
 // NT scaling.  L1 = chol(S), L2 = chol(Z), L2'L1 = U diag(lam) V',
 // R = L1 V lam^-1/2, Rinv = lam^1/2 V' L1^-1, Ginv = Rinv' Rinv.
-// Shared memory: 5 matrices + 3n doubles + n ints + 1 int.
+// Shared memory: 5 matrices + Cholesky scratch + 2n doubles + n ints + 1 int.
 // ---------------------------------------------------------------------------------------
 extern "C" __global__ void __launch_bounds__(SDPXG_CONE_THREADS)
 k_nt_scale(const BlockDesc* __restrict__ blocks, const double* __restrict__ s,
@@ -34,7 +34,7 @@ k_nt_scale(const BlockDesc* __restrict__ blocks, const double* __restrict__ s,
   double* V = M + kMat;
   double* X = V + kMat;
   double* piv = X + kMat;
-  double* sig = piv + SDPXG_NMAX;
+  double* sig = piv + SDPXG_CHOL_SCRATCH;
   double* lsort = sig + SDPXG_NMAX;
   int* rank = reinterpret_cast<int*>(lsort + SDPXG_NMAX);
   int* flag = rank + SDPXG_NMAX;
@@ -264,9 +264,9 @@ k_step_length(const BlockDesc* __restrict__ blocks, const double* __restrict__ R
   double* X = B + kMat;
   double* T = X + kMat;
   double* D = T + kMat;
-  double* small = D + kMat;  // piv[n], d[n], e[n], work[2n], red[32]
+  double* small = D + kMat;  // Cholesky scratch, d[n], e[n], work[2n], red[32]
   double* piv = small;
-  double* dd = piv + SDPXG_NMAX;
+  double* dd = piv + SDPXG_CHOL_SCRATCH;
   double* ee = dd + SDPXG_NMAX;
   double* work = ee + SDPXG_NMAX;
   double* red = work + 2 * SDPXG_NMAX;

@@ -34,6 +34,28 @@ extern "C" __global__ void k_shifted_copy(const double* __restrict__ Hs, double*
 }
 
 // ------------------------------------------------------------------------------------
+// Pivot k of the diagonal tile under the dynamic pivot rule (the reference's LDL pivot
+// handling, dense_block.rs): a pivot within eps of zero becomes delta, a clearly negative or
+// non-finite one fails.  Written once by the thread that finished the pivot entry:
+// info = {1/d, sqrt(d), 1/sqrt(d)}, all 0 on failure (sqrt of an accepted pivot is > 0).
+__device__ __forceinline__ void potrf_pivot(double d, double diag, int nb, double eps,
+                                            double delta, int dynamic, double* info) {
+  bool fail = !isfinite(d);
+  if (!fail && dynamic && d <= eps) {
+    if (d < -64.0 * 2.220446049250313e-16 * nb * fabs(diag)) fail = true;
+    else d = delta;
+  }
+  if (!fail && !(d > 0.0)) fail = true;
+  if (fail) {
+    info[0] = info[1] = info[2] = 0.0;
+    return;
+  }
+  const double r = sqrt(d);
+  info[0] = 1.0 / d;
+  info[1] = r;
+  info[2] = 1.0 / r;
+}
+
 // Diagonal tile: lagged upper Cholesky with the dynamic pivot rule, then Dinv = U^-1.
 // Dynamic shared memory: two CH_NB x CH_LD tiles.
 extern "C" __global__ void __launch_bounds__(1024)
@@ -44,12 +66,15 @@ k_potrf_diag(double* __restrict__ H, int m, int kb, double eps, double delta, in
   double* A = pd_sm;
   __shared__ double rowbuf[2][CH_NB];   // row k of the partially eliminated tile
   __shared__ double mrowbuf[2][CH_NB];  // row k of M = L^-1 (unit lower)
-  __shared__ double dmod[CH_NB];
+  __shared__ double pinfo[2][3];        // pivot k: 1/d, sqrt(d), 1/sqrt(d)
+  __shared__ double root[CH_NB];        // sqrt of the accepted pivots
   const int k0 = kb * CH_NB;
   const int nb = min(CH_NB, m - k0);
   // thread (tx, ty) owns rows tx + 32p and columns ty + 32q (p, q < 2) of the tile, in
   // registers: a = upper triangle being eliminated (H = L D L'), mm = lower triangle of
   // M = L^-1, updated with the same elimination multipliers (Gauss elimination applied to I).
+  // The divisions and the square root of a pivot are computed once, by the thread that
+  // finishes the pivot entry, one step ahead of their use.
   const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
   double a[2][2], mm[2][2];
 #pragma unroll
@@ -62,23 +87,18 @@ k_potrf_diag(double* __restrict__ H, int m, int kb, double eps, double delta, in
       if (i == 0 && j < nb) rowbuf[0][j] = a[p][q];
       if (i == 0) mrowbuf[0][j] = (j == 0) ? 1.0 : 0.0;
     }
+  if (threadIdx.x == 0 && nb > 0) {
+    potrf_pivot(a[0][0], diag0[k0], nb, eps, delta, dynamic, pinfo[0]);
+    root[0] = pinfo[0][1];
+  }
   for (int k = 0; k < nb; ++k) {
     __syncthreads();
     const double* row = rowbuf[k & 1];
-    double d = row[k];
-    bool fail = !isfinite(d);
-    if (!fail && dynamic && d <= eps) {
-      // a pivot within rounding of zero becomes delta; a clearly negative one fails
-      if (d < -64.0 * 2.220446049250313e-16 * nb * fabs(diag0[k0 + k])) fail = true;
-      else d = delta;
-    }
-    if (!fail && !(d > 0.0)) fail = true;
-    if (fail) {
+    const double dinv = pinfo[k & 1][0], r = pinfo[k & 1][1], rinv = pinfo[k & 1][2];
+    if (r == 0.0) {
       if (threadIdx.x == 0) atomicOr(status, SDPXG_ST_PIVOT_FAIL);
-      return;  // uniform: every thread read the same pivot
+      return;  // uniform: every thread read the same pivot record
     }
-    const double dinv = 1.0 / d, r = sqrt(d);
-    if (threadIdx.x == 0) dmod[k] = d;
     const double* mrow = mrowbuf[k & 1];
     double* next = rowbuf[(k + 1) & 1];
     double* mnext = mrowbuf[(k + 1) & 1];
@@ -89,10 +109,17 @@ k_potrf_diag(double* __restrict__ H, int m, int kb, double eps, double delta, in
         const int i = tx + 32 * p, j = ty + 32 * q;
         if (i >= nb || j >= nb) continue;
         if (i <= j) {
-          if (i == k) A[k + j * CH_LD] = (j == k) ? r : a[p][q] / r;  // final row k of U
+          if (i == k) A[k + j * CH_LD] = (j == k) ? r : a[p][q] * rinv;  // final row k of U
           if (i > k) {
             a[p][q] -= row[i] * row[j] * dinv;
-            if (i == k + 1) next[j] = a[p][q];
+            if (i == k + 1) {
+              next[j] = a[p][q];
+              if (j == k + 1) {  // pivot k + 1 is final: publish its record for the next step
+                potrf_pivot(a[p][q], diag0[k0 + k + 1], nb, eps, delta, dynamic,
+                            pinfo[(k + 1) & 1]);
+                root[k + 1] = pinfo[(k + 1) & 1][1];
+              }
+            }
           }
         }
         if (i >= j) {  // M entry (i, c = j): row i -= l_ik * row k, for c <= k
@@ -114,7 +141,7 @@ k_potrf_diag(double* __restrict__ H, int m, int kb, double eps, double delta, in
     for (int q = 0; q < 2; ++q) {
       const int i = tx + 32 * p, c = ty + 32 * q;
       const bool live = (i >= c && i < nb);
-      D[c + i * CH_NB] = live ? mm[p][q] / sqrt(dmod[i]) : 0.0;
+      D[c + i * CH_NB] = live ? mm[p][q] / root[i] : 0.0;
     }
 }
 

@@ -53,6 +53,29 @@ struct DevBuf {
   operator T*() const { return p; }
 };
 
+// Page-locked host buffer: scalar device-to-host reads skip the pageable staging copy.
+template <typename T>
+struct PinnedBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  PinnedBuf() = default;
+  PinnedBuf(const PinnedBuf&) = delete;
+  PinnedBuf& operator=(const PinnedBuf&) = delete;
+  ~PinnedBuf() { release(); }
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) check(cudaMallocHost(&p, count * sizeof(T)), "cudaMallocHost");
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+  }
+  T& operator[](size_t i) { return p[i]; }
+  const T& operator[](size_t i) const { return p[i]; }
+};
+
 // Kernel declarations (defined in the *_kernels.cu translation units of this library).
 extern "C" {
 __global__ void k_nt_scale(const BlockDesc*, const double*, const double*, double*, double*,
@@ -85,6 +108,8 @@ __global__ void k_op_adjoint_gather(int, const int*, const int*, const int*, con
 __global__ void k_potrf_diag(double*, int, int, double, double, int, const double*, double*,
                              uint32_t*);
 __global__ void k_trsm_panel(double*, int, int, const double*);
+__global__ void k_chol_dataflow(double*, int, int, const unsigned*, int, int*, double, double, int,
+                                const double*, double*, uint32_t*);
 __global__ void k_syrk_update(double*, int, int);
 __global__ void k_trtri_diag(int, const double*, double*, double*);
 __global__ void k_trinv_level(const double*, double*, double*, double*, int, int, int);
@@ -114,7 +139,7 @@ class Reducer {
   void init() {
     partial_.alloc((size_t)kBlocks * kSlots);
     slots_.alloc(kSlots);
-    host_.resize(kSlots);
+    host_.alloc(kSlots);
   }
   int add(cudaStream_t st, int op, long n, const double* x, const double* y) {
     if (count_ >= kSlots) throw CudaError("reducer slots exhausted");
@@ -131,9 +156,9 @@ class Reducer {
     }
     return s;
   }
-  const std::vector<double>& fetch(cudaStream_t st) {
+  const PinnedBuf<double>& fetch(cudaStream_t st) {
     if (count_) {
-      check(cudaMemcpyAsync(host_.data(), slots_.p, count_ * sizeof(double),
+      check(cudaMemcpyAsync(host_.p, slots_.p, count_ * sizeof(double),
                             cudaMemcpyDeviceToHost, st), "reducer D2H");
     }
     check(cudaStreamSynchronize(st), "reducer sync");
@@ -143,7 +168,7 @@ class Reducer {
 
  private:
   DevBuf<double> partial_, slots_;
-  std::vector<double> host_;
+  PinnedBuf<double> host_;
   int count_ = 0;
   const double id_[4] = {0.0, 0.0, 0.0, 1.0};
 };

@@ -21,15 +21,70 @@
 namespace sdpxg {
 
 constexpr int kMatD = SDPXG_LD * SDPXG_NMAX;
-constexpr size_t kSmemNt = (5 * kMatD + 3 * SDPXG_NMAX) * sizeof(double) + (SDPXG_NMAX + 1) * sizeof(int);
+constexpr size_t kSmemNt =
+    (5 * kMatD + SDPXG_CHOL_SCRATCH + 2 * SDPXG_NMAX) * sizeof(double) + (SDPXG_NMAX + 1) * sizeof(int);
 constexpr size_t kSmemCong = 4 * kMatD * sizeof(double);
 constexpr size_t kSmemCirc = 2 * kMatD * sizeof(double);
-constexpr size_t kSmemStep = (4 * kMatD + 5 * SDPXG_NMAX + 32) * sizeof(double);
+constexpr size_t kSmemStep = (4 * kMatD + SDPXG_CHOL_SCRATCH + 4 * SDPXG_NMAX + 32) * sizeof(double);
 constexpr size_t kSmemMarg = (kMatD + 5 * SDPXG_NMAX + 32) * sizeof(double);
 constexpr size_t kSmemTrans = 3 * kMatD * sizeof(double);
 constexpr size_t kSmemTrsm = 2 * 64 * 65 * sizeof(double);
 constexpr size_t kSmemSyrk = 2 * 64 * 66 * sizeof(double);
 constexpr size_t kSmemTrtri = 2 * 64 * 65 * sizeof(double);
+constexpr size_t kSmemDf = (2 * 64 * 68 + 2 * 8 * 64) * sizeof(double);  // k_chol_dataflow
+constexpr int kDfMaxTiles = 256;  // dataflow schedule up to m = 16384 (nt^3/6 items)
+
+// Work list of the dataflow Cholesky (k_chol_dataflow): POTRF(k), TRSM(k, j), GEMM(k, i, j) of
+// the right-looking tiled algorithm in a topological order with one step of look-ahead: the
+// update of tile row k + 1, POTRF(k + 1) and its TRSM row come before the rest of step k's
+// trailing update.  Encoded type << 30 | k << 20 | i << 10 | j.
+inline std::vector<unsigned> chol_schedule(int nt) {
+  auto code = [](unsigned type, int k, int i, int j) {
+    return (type << 30) | ((unsigned)k << 20) | ((unsigned)i << 10) | (unsigned)j;
+  };
+  std::vector<unsigned> it;
+  if (nt <= 0) return it;
+  it.push_back(code(0u, 0, 0, 0));
+  for (int j = 1; j < nt; ++j) it.push_back(code(1u, 0, 0, j));
+  for (int k = 0; k + 1 < nt; ++k) {
+    for (int j = k + 1; j < nt; ++j) it.push_back(code(2u, k, k + 1, j));
+    it.push_back(code(0u, k + 1, k + 1, k + 1));
+    for (int j = k + 2; j < nt; ++j) it.push_back(code(1u, k + 1, k + 1, j));
+    for (int i = k + 2; i < nt; ++i)
+      for (int j = i; j < nt; ++j) it.push_back(code(2u, k, i, j));
+  }
+  return it;
+}
+
+// Replays a work list in order and checks that every item's inputs are produced by earlier
+// items (the condition under which the ticket order of k_chol_dataflow cannot deadlock) and
+// that every tile ends factored.  Returns false on any violation.
+inline bool chol_schedule_valid(const std::vector<unsigned>& it, int nt) {
+  std::vector<int> upd((size_t)nt * nt, 0), fin((size_t)nt * nt, 0);
+  for (unsigned c : it) {
+    const int type = (int)(c >> 30), k = (int)((c >> 20) & 1023u);
+    const int i = (int)((c >> 10) & 1023u), j = (int)(c & 1023u);
+    if (k >= nt || i >= nt || j >= nt) return false;
+    if (type == 0) {
+      if (i != k || j != k || upd[(size_t)k * nt + k] != k || fin[(size_t)k * nt + k]) return false;
+      fin[(size_t)k * nt + k] = 1;
+    } else if (type == 1) {
+      if (i != k || j <= k || !fin[(size_t)k * nt + k] || upd[(size_t)k * nt + j] != k) return false;
+      fin[(size_t)k * nt + j] = 1;
+    } else if (type == 2) {
+      if (i <= k || j < i || !fin[(size_t)k * nt + i] || !fin[(size_t)k * nt + j] ||
+          upd[(size_t)i * nt + j] != k)
+        return false;
+      upd[(size_t)i * nt + j] = k + 1;
+    } else {
+      return false;
+    }
+  }
+  for (int i = 0; i < nt; ++i)
+    for (int j = i; j < nt; ++j)
+      if (!fin[(size_t)i * nt + j] || upd[(size_t)i * nt + j] != i) return false;
+  return true;
+}
 constexpr int kNB = 64;
 
 // Equilibrated problem in host memory (CSC, int64 indices as in the reference ABI).
@@ -104,8 +159,10 @@ class Engine {
     set_smem(reinterpret_cast<const void*>(k_syrk_update), kSmemSyrk);
     set_smem(reinterpret_cast<const void*>(k_trinv_level), kSmemTrtri);
     set_smem(reinterpret_cast<const void*>(k_potrf_diag), kSmemTrtri);
+    set_smem(reinterpret_cast<const void*>(k_chol_dataflow), kSmemDf);
     red.init();
     status_.alloc(1);
+    hstat_.alloc(1);
     for (auto& e : ev_) check(cudaEventCreate(&e), "event create");
   }
 
@@ -272,7 +329,22 @@ class Engine {
     Uinv_.alloc((size_t)n * n);
     UinvT_.alloc((size_t)n * n);
     Tmp_.alloc((size_t)n * n);
+    df_items_ = 0;
+    if (nchol > 0 && nchol <= kDfMaxTiles) {
+      std::vector<unsigned> items = chol_schedule(nchol);
+      if (!chol_schedule_valid(items, nchol)) throw CudaError("invalid Cholesky work list");
+      df_items_ = (int)items.size();
+      df_list_.alloc(items.size());
+      df_list_.upload(items.data(), items.size(), st);
+      df_sync_.alloc(2 + 2 * (size_t)nchol * nchol);
+      int per_sm = 0, sms = 0;
+      check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chol_dataflow, 256, kSmemDf),
+            "occupancy");
+      check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+      df_grid_ = std::max(1, std::min(std::max(per_sm, 1) * sms, df_items_));
+    }
     step_out_.alloc(2 * std::max(nblk, 1));
+    hblk_.alloc(2 * std::max(nblk, 1));
     marg_out_.alloc(2 * std::max(nblk, 1));
     scal_.alloc(4);
     check(cudaStreamSynchronize(st), "upload sync");
@@ -281,10 +353,9 @@ class Engine {
   // ---- status word ----
   void clear_status() { check(cudaMemsetAsync(status_.p, 0, sizeof(uint32_t), st), "memset"); }
   uint32_t read_status() {
-    uint32_t s = 0;
-    check(cudaMemcpyAsync(&s, status_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "status");
+    check(cudaMemcpyAsync(hstat_.p, status_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "status");
     check(cudaStreamSynchronize(st), "status sync");
-    return s;
+    return hstat_[0];
   }
 
   // ---- cone scaling ----
@@ -350,8 +421,8 @@ class Engine {
                                                                    status_);
     launched("k_step_length");
     tend(KT_STEP);
-    std::vector<double> h(2 * nblk);
-    check(cudaMemcpyAsync(h.data(), step_out_.p, 2 * nblk * sizeof(double),
+    const PinnedBuf<double>& h = hblk_;
+    check(cudaMemcpyAsync(hblk_.p, step_out_.p, 2 * nblk * sizeof(double),
                           cudaMemcpyDeviceToHost, st), "step D2H");
     uint32_t s = read_status();
     for (int j = 0; j < nblk; ++j) {
@@ -368,9 +439,11 @@ class Engine {
     clear_status();
     ++g_launches, k_margins<<<dim3(nblk, 1), SDPXG_CONE_THREADS, kSmemMarg, st>>>(blocks_, v, m, marg_out_, status_);
     launched("k_margins");
-    check(cudaMemcpyAsync(out.data(), marg_out_.p, 2 * nblk * sizeof(double),
+    check(cudaMemcpyAsync(hblk_.p, marg_out_.p, 2 * nblk * sizeof(double),
                           cudaMemcpyDeviceToHost, st), "margins D2H");
-    return read_status() == 0;
+    const bool ok = read_status() == 0;
+    for (int j = 0; j < 2 * nblk; ++j) out[j] = hblk_[j];
+    return ok;
   }
 
   // ---- constraint operator ----
@@ -441,10 +514,9 @@ class Engine {
   double schur_diag_absmax() {
     if (!n) return 0.0;
     ++g_launches, k_diag_absmax<<<1, 1024, 0, st>>>(Hsave_, n, scal_);
-    double v = 0.0;
-    check(cudaMemcpyAsync(&v, scal_.p, sizeof(double), cudaMemcpyDeviceToHost, st), "diag D2H");
+    check(cudaMemcpyAsync(hblk_.p, scal_.p, sizeof(double), cudaMemcpyDeviceToHost, st), "diag D2H");
     check(cudaStreamSynchronize(st), "diag sync");
-    return v;
+    return hblk_[0];
   }
   // F = chol(Hsave + eps I) with the dynamic pivot rule
   bool factor(double eps, bool dynamic, double dyn_eps, double dyn_delta) {
@@ -452,7 +524,14 @@ class Engine {
     clear_status();
     tbegin(KT_FACTOR);
     ++g_launches, k_shifted_copy<<<1184, 256, 0, st>>>(Hsave_, F_, n, eps, diag0_);
-    for (int kb = 0; kb < nchol; ++kb) {
+    if (df_items_ > 0) {  // one persistent launch over the whole tile schedule
+      check(cudaMemsetAsync(df_sync_.p, 0, (2 + 2 * (size_t)nchol * nchol) * sizeof(int), st),
+            "dataflow sync reset");
+      ++g_launches, k_chol_dataflow<<<df_grid_, 256, kSmemDf, st>>>(
+          F_, n, nchol, df_list_, df_items_, df_sync_, dyn_eps, dyn_delta, dynamic ? 1 : 0, diag0_,
+          Dinv_, status_);
+    }
+    for (int kb = 0; df_items_ == 0 && kb < nchol; ++kb) {
       ++g_launches, k_potrf_diag<<<1, 1024, kSmemTrtri, st>>>(F_, n, kb, dyn_eps, dyn_delta, dynamic ? 1 : 0,
                                                 diag0_, Dinv_, status_);
       int rest = nchol - kb - 1;
@@ -463,6 +542,7 @@ class Engine {
     }
     launched("factor");
     uint32_t s = read_status();
+    if (s & SDPXG_ST_SYNC_TIMEOUT) throw CudaError("factorization: a bounded inter-CTA wait gave up");
     factor_ok_ = (s == 0);
     if (factor_ok_) {
       // explicit inverse of the factor: diagonal tiles, then one batched GEMM pair per level
@@ -549,6 +629,11 @@ class Engine {
   DevBuf<double> Hsave_, F_, Dinv_, diag0_, symv_part_, tri_y_, Uinv_, UinvT_, Tmp_;
   DevBuf<double> step_out_, marg_out_, scal_;
   DevBuf<uint32_t> status_;
+  PinnedBuf<uint32_t> hstat_;
+  PinnedBuf<double> hblk_;  // per-block scalars read back (step bounds, margins)
+  DevBuf<unsigned> df_list_;
+  DevBuf<int> df_sync_;
+  int df_items_ = 0, df_grid_ = 0;
   cudaEvent_t ev_[2 * KT_N] = {};
 };
 

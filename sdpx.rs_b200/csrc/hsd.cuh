@@ -80,6 +80,15 @@ class HsdSolver {
                     &prevs_, &prevz_, &bests_, &bestz_, &rhsz_, &rhss_, &cvec_, &workz_, &z1_,
                     &tm_, &ez_, &cz_, &candz_, &ez2_, &wm1_, &wm2_, &wm3_, &b_, &e_, &einv_})
       vm(*b);
+    load(p);
+  }
+
+  // (Re)load the problem vectors; the device work vectors stay allocated across solves, so a
+  // handle that solves repeatedly (sdpx_update, parameter sweeps) allocates nothing per solve.
+  void load(const HostProblem& p) {
+    const int n = n_, m = m_;
+    const Equilibration& eq = eq_;
+    if (p.n != n || p.m != m) throw std::invalid_argument("problem dimensions changed");
     q_.upload(p.q.data(), n, E.st);
     b_.upload(p.b.data(), m, E.st);
     std::vector<double> nq(p.q);
@@ -567,6 +576,7 @@ inline void HsdSolver::solve() {
   auto tstart = clock::now();
   const int n = n_, m = m_;
   info = Info();
+  times = PhaseTimes();
   have_prev_ = false;
   default_start();
   int it = 0;
