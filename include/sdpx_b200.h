@@ -128,6 +128,11 @@ int32_t sdpx_b200_set_kernel_timing(sdpx_handle *handle, int32_t on);
 int32_t sdpx_b200_kernel_times(sdpx_handle *handle, double *ms, uint64_t *counts);
 /* Number of CUDA kernels this library has launched in this process (all handles). */
 uint64_t sdpx_b200_launch_count(void);
+/* Schur forms chosen at prepare: PSD blocks whose every constraint column is rank one
+ * (sigma u u', stored as the factor U and used in the Gram form S = (sigma sigma') o (U' Ginv U)^2,
+ * like the reference's sampled Gram update, sampled/mod.rs:1973-2025) and blocks kept in the
+ * ordinary dense-column form.  Setting SDPX_B200_GRAM=0 before prepare forces the ordinary form. */
+int32_t sdpx_b200_schur_forms(sdpx_handle *handle, uint32_t *gram_blocks, uint32_t *ordinary_blocks);
 
 /* ---- kernel-level ABI (sdpxg_*): one hot-path operation per call ---- */
 typedef struct sdpxg_ctx sdpxg_ctx;

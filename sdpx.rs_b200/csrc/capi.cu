@@ -2,6 +2,7 @@
 // the kernel-level sdpxg_* entry points.  Exceptions never cross the boundary: they become
 // return code 5 (the reference's "panic" code) with the message kept thread-locally, and a
 // handle whose solve threw is poisoned (crates/ffi/src/lib.rs:29-42, 567-584).
+#include <chrono>
 #include <cinttypes>
 #include <cstdio>
 #include <cstdlib>
@@ -11,6 +12,7 @@
 
 #include "../../include/sdpx_b200.h"
 #include "hsd.cuh"
+#include "host_parallel.h"
 
 using namespace sdpxg;
 
@@ -61,7 +63,13 @@ std::vector<double> scalars(const sdpx_scalars& a) {
   std::vector<double> v(a.count);
   if (a.kind == 0) {
     if (a.count && !a.f64) invalid("null pointer");
-    for (uint64_t i = 0; i < a.count; ++i) v[i] = a.f64[i];
+    parallel_for((int64_t)a.count, 1 << 16, [&](int64_t b, int64_t e, int) {
+      for (int64_t i = b; i < e; ++i) {
+        v[i] = a.f64[i];
+        if (!std::isfinite(v[i])) invalid("nonfinite input");
+      }
+    });
+    return v;
   } else if (a.kind == 1) {
     if (a.count && !a.decimal) invalid("null pointer");
     for (uint64_t i = 0; i < a.count; ++i) {
@@ -97,16 +105,18 @@ Csc matrix(const sdpx_csc& a, bool upper) {
   c.colptr.resize(a.cols + 1);
   c.rowval.resize(a.nnz);
   for (uint64_t j = 0; j <= a.cols; ++j) c.colptr[j] = (int64_t)a.colptr[j];
-  for (uint64_t j = 0; j < a.cols; ++j) {
+  for (uint64_t j = 0; j < a.cols; ++j)
     if (a.colptr[j] > a.colptr[j + 1] || a.colptr[j + 1] > a.nnz)
       invalid("invalid CSC column pointers");
-    for (uint64_t p = a.colptr[j]; p < a.colptr[j + 1]; ++p) {
-      uint64_t r = a.rowval[p];
-      if (r >= a.rows || (upper && r > j) || (p > a.colptr[j] && a.rowval[p - 1] >= r))
-        invalid("CSC rows must be sorted unique in range; P upper triangular");
-      c.rowval[p] = (int64_t)r;
-    }
-  }
+  parallel_for((int64_t)a.cols, 8, [&](int64_t j0, int64_t j1, int) {
+    for (int64_t j = j0; j < j1; ++j)
+      for (uint64_t p = a.colptr[j]; p < a.colptr[j + 1]; ++p) {
+        uint64_t r = a.rowval[p];
+        if (r >= a.rows || (upper && r > (uint64_t)j) || (p > a.colptr[j] && a.rowval[p - 1] >= r))
+          invalid("CSC rows must be sorted unique in range; P upper triangular");
+        c.rowval[p] = (int64_t)r;
+      }
+  });
   c.val = scalars(a.values);
   return c;
 }
@@ -167,12 +177,27 @@ void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
           dw[j] = std::max(dw[j], a);
           dw[p.Prow[q]] = std::max(dw[p.Prow[q]], a);
         }
-      for (int j = 0; j < n; ++j)
-        for (int64_t q = p.Acolptr[j]; q < p.Acolptr[j + 1]; ++q) {
-          double a = std::fabs(p.Aval[q]);
-          dw[j] = std::max(dw[j], a);
-          ew[p.Arow[q]] = std::max(ew[p.Arow[q]], a);
-        }
+      {  // column maxima, and row maxima through per-chunk partial arrays
+        const int nt = host_threads();
+        std::vector<std::vector<double>> ewp((size_t)nt);
+        std::vector<char> used((size_t)nt, 0);
+        parallel_for(n, 8, [&](int64_t j0, int64_t j1, int t) {
+          std::vector<double>& er = ewp[(size_t)t];
+          er.assign(m, 0.0);
+          used[(size_t)t] = 1;
+          for (int64_t j = j0; j < j1; ++j)
+            for (int64_t q = p.Acolptr[j]; q < p.Acolptr[j + 1]; ++q) {
+              const double a = std::fabs(p.Aval[q]);
+              dw[j] = std::max(dw[j], a);
+              er[p.Arow[q]] = std::max(er[p.Arow[q]], a);
+            }
+        });
+        parallel_for(m, 1 << 12, [&](int64_t i0, int64_t i1, int) {
+          for (int t = 0; t < nt; ++t)
+            if (used[(size_t)t])
+              for (int64_t i = i0; i < i1; ++i) ew[i] = std::max(ew[i], ewp[(size_t)t][i]);
+        });
+      }
       for (int j = 0; j < n; ++j) {
         double w = dw[j] == 0.0 ? 1.0 : dw[j];
         w = 1.0 / std::sqrt(w);
@@ -183,12 +208,14 @@ void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
         w = 1.0 / std::sqrt(w);
         ew[i] = std::min(std::max(w, smin / eq.e[i]), smax / eq.e[i]);
       }
-      for (int j = 0; j < n; ++j) {
-        for (int64_t q = p.Pcolptr[j]; q < p.Pcolptr[j + 1]; ++q) p.Pval[q] *= dw[p.Prow[q]] * dw[j];
-        for (int64_t q = p.Acolptr[j]; q < p.Acolptr[j + 1]; ++q) p.Aval[q] *= ew[p.Arow[q]] * dw[j];
-        p.q[j] *= dw[j];
-        eq.d[j] *= dw[j];
-      }
+      parallel_for(n, 8, [&](int64_t j0, int64_t j1, int) {
+        for (int64_t j = j0; j < j1; ++j) {
+          for (int64_t q = p.Pcolptr[j]; q < p.Pcolptr[j + 1]; ++q) p.Pval[q] *= dw[p.Prow[q]] * dw[j];
+          for (int64_t q = p.Acolptr[j]; q < p.Acolptr[j + 1]; ++q) p.Aval[q] *= ew[p.Arow[q]] * dw[j];
+          p.q[j] *= dw[j];
+          eq.d[j] *= dw[j];
+        }
+      });
       for (int i = 0; i < m; ++i) {
         p.b[i] *= ew[i];
         eq.e[i] *= ew[i];
@@ -222,8 +249,10 @@ void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
       for (int i = row; i < row + tn; ++i) delta[i] = mean / eq.e[i];
       row += tn;
     }
-    for (int j = 0; j < n; ++j)
-      for (int64_t q = p.Acolptr[j]; q < p.Acolptr[j + 1]; ++q) p.Aval[q] *= delta[p.Arow[q]];
+    parallel_for(n, 8, [&](int64_t j0, int64_t j1, int) {
+      for (int64_t j = j0; j < j1; ++j)
+        for (int64_t q = p.Acolptr[j]; q < p.Acolptr[j + 1]; ++q) p.Aval[q] *= delta[p.Arow[q]];
+    });
     for (int i = 0; i < m; ++i) {
       p.b[i] *= delta[i];
       eq.e[i] *= delta[i];
@@ -233,6 +262,12 @@ void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
   eq.einv.resize(m);
   for (int j = 0; j < n; ++j) eq.dinv[j] = 1.0 / eq.d[j];
   for (int i = 0; i < m; ++i) eq.einv[i] = 1.0 / eq.e[i];
+}
+
+// SDPX_B200_VERBOSE=1 prints the host-side prepare breakdown to stderr.
+bool verbose_from_env() {
+  const char* s = std::getenv("SDPX_B200_VERBOSE");
+  return s && s[0] == '1';
 }
 
 int device_from_env() {
@@ -321,6 +356,7 @@ std::string rust_exp(double x) {
 
 void prepare_impl(const sdpx_csc* P, const sdpx_scalars* q, const sdpx_csc* A, const sdpx_scalars* b,
                   const sdpx_cone* cones, uint64_t nc, const sdpx_settings* s, sdpx_handle** out) {
+  const auto t0 = std::chrono::steady_clock::now();
   if (!out) invalid("null pointer");
   *out = nullptr;
   ref(q); ref(A); ref(b); ref(s);
@@ -360,11 +396,30 @@ void prepare_impl(const sdpx_csc* P, const sdpx_scalars* q, const sdpx_csc* A, c
     rows += c.dim * (c.dim + 1) / 2;
   }
   if (rows != A->rows) invalid("cone dimensions do not match the rows of A");
-  h->equil = h->orig;
+  const auto t1 = std::chrono::steady_clock::now();
+  // the equilibrated copy takes the matrices; the original keeps what sdpx_update and the
+  // info need (dimensions, q, b, cone orders)
+  h->equil = std::move(h->orig);
+  h->orig = HostProblem();
+  h->orig.n = h->equil.n;
+  h->orig.m = h->equil.m;
+  h->orig.q = h->equil.q;
+  h->orig.b = h->equil.b;
+  h->orig.psd = h->equil.psd;
   equilibrate(h->equil, h->settings, h->eq);
+  const auto t2 = std::chrono::steady_clock::now();
   h->eng = std::make_unique<Engine>();
   h->eng->init(device_from_env());
+  const auto t3 = std::chrono::steady_clock::now();
   h->eng->upload(h->equil);
+  const auto t4 = std::chrono::steady_clock::now();
+  if (verbose_from_env()) {
+    auto sec = [](auto a, auto b) { return std::chrono::duration<double>(b - a).count(); };
+    std::fprintf(stderr,
+                 "sdpx_b200 prepare: copy+validate %.3f s, equilibrate %.3f s, device init %.3f s, "
+                 "upload %.3f s (%s)\n",
+                 sec(t0, t1), sec(t1, t2), sec(t2, t3), sec(t3, t4), h->eng->upload_report().c_str());
+  }
   *out = h.release();
 }
 
@@ -543,6 +598,16 @@ int32_t sdpx_b200_kernel_times(sdpx_handle* h, double* ms, uint64_t* counts) {
         ms[k] = hh.eng->kt_ms[k];
         counts[k] = hh.eng->kt_count[k];
       }
+    });
+  });
+}
+
+int32_t sdpx_b200_schur_forms(sdpx_handle* h, uint32_t* gram_blocks, uint32_t* ordinary_blocks) {
+  return boundary([&] {
+    if (!gram_blocks || !ordinary_blocks) invalid("null pointer");
+    operate(h, [&](sdpx_handle& hh) {
+      *gram_blocks = (uint32_t)hh.eng->gram_blocks();
+      *ordinary_blocks = (uint32_t)(hh.eng->nblk - hh.eng->gram_blocks());
     });
   });
 }

@@ -108,6 +108,15 @@ __global__ void k_op_adjoint_gather(int, const int*, const int*, const int*, con
 __global__ void k_potrf_diag(double*, int, int, double, double, int, const double*, double*,
                              uint32_t*);
 __global__ void k_trsm_panel(double*, int, int, const double*);
+__global__ void k_gram_basis(const BlockDesc*, const int*, const int*, const int*, const long*,
+                             const double*, const double*, double*);
+__global__ void k_gram_schur(const BlockDesc*, const int*, const int*, const int*, const long*,
+                             const long*, const double*, const double*, double*);
+__global__ void k_gram_forward(const BlockDesc*, const int*, const int*, const int*, const int*,
+                               const long*, const double*, const double*, const double*, double,
+                               double, double*);
+__global__ void k_gram_adjoint(const BlockDesc*, const int*, const int*, const int*, const int*,
+                               const long*, const double*, const double*, const double*, double*);
 __global__ void k_chol_dataflow(double*, int, int, const unsigned*, int, int*, double, double, int,
                                 const double*, double*, uint32_t*);
 __global__ void k_syrk_update(double*, int, int);

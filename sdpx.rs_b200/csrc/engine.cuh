@@ -13,8 +13,12 @@
 #pragma once
 #include <algorithm>
 #include <cmath>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
+#include <string>
 
 #include "device.cuh"
 
@@ -32,7 +36,52 @@ constexpr size_t kSmemTrsm = 2 * 64 * 65 * sizeof(double);
 constexpr size_t kSmemSyrk = 2 * 64 * 66 * sizeof(double);
 constexpr size_t kSmemTrtri = 2 * 64 * 65 * sizeof(double);
 constexpr size_t kSmemDf = (2 * 64 * 68 + 2 * 8 * 64) * sizeof(double);  // k_chol_dataflow
+constexpr size_t kSmemGram = 3 * kMatD * sizeof(double);                 // k_gram_basis/adjoint
 constexpr int kDfMaxTiles = 256;  // dataflow schedule up to m = 16384 (nt^3/6 items)
+
+// Rank-one test of one PSD column block: svec v (upper, column order, off-diagonal x sqrt2) of
+// an n x n matrix M.  On success M = sigma u u' entrywise to a few ulps (32 eps relative to
+// each entry, exact zeros kept), with u scaled from the column of the largest diagonal.
+inline bool rank_one_column(const double* v, int n, double* u, double* sigma) {
+  int p = 0;
+  double best = -1.0;
+  for (int i = 0; i < n; ++i) {
+    const double a = std::fabs(v[i * (i + 3) / 2]);  // diagonal (i, i) sits at i(i+1)/2 + i
+    if (a > best) {
+      best = a;
+      p = i;
+    }
+  }
+  if (!(best > 0.0)) {  // among rank-one matrices only the zero matrix has a zero diagonal
+    for (int e = 0; e < n * (n + 1) / 2; ++e)
+      if (v[e] != 0.0) return false;
+    for (int i = 0; i < n; ++i) u[i] = 0.0;
+    *sigma = 1.0;
+    return true;
+  }
+  const double mpp = v[p * (p + 3) / 2], sg = mpp > 0.0 ? 1.0 : -1.0;
+  const double r = std::sqrt(std::fabs(mpp));
+  if (!std::isfinite(r)) return false;
+  for (int i = 0; i < n; ++i) {
+    const double mip = (i == p) ? mpp
+                       : (i < p ? v[p * (p + 1) / 2 + i] : v[i * (i + 1) / 2 + p]) * SDPXG_RSQRT2;
+    u[i] = sg * mip / r;
+  }
+  const double tol = 32.0 * 2.220446049250313e-16;
+  const double* e = v;
+  for (int j = 0; j < n; ++j) {
+    const double uj = sg * u[j];
+    for (int i = 0; i < j; ++i, ++e) {  // off-diagonal svec entry sqrt2 M_ij
+      const double g = SDPXG_SQRT2 * (uj * u[i]);
+      if (!(std::fabs(*e - g) <= tol * (std::fabs(*e) + std::fabs(g)))) return false;
+    }
+    const double g = uj * u[j];
+    if (!(std::fabs(*e - g) <= tol * (std::fabs(*e) + std::fabs(g)))) return false;
+    ++e;
+  }
+  *sigma = sg;
+  return true;
+}
 
 // Work list of the dataflow Cholesky (k_chol_dataflow): POTRF(k), TRSM(k, j), GEMM(k, i, j) of
 // the right-looking tiled algorithm in a topological order with one step of look-ahead: the
@@ -121,6 +170,8 @@ class Engine {
   }
   int n = 0, m = 0, nblk = 0;
   int nchol = 0;  // Schur tiles per side
+  bool gram_enabled = true;  // rank-one blocks use the Gram form (SDPX_B200_GRAM=0 disables)
+  int gram_blocks() const { return ngram_; }
   std::vector<BlockDesc> hblocks;
   std::vector<int> hk;  // columns per block
   Reducer red;
@@ -160,13 +211,28 @@ class Engine {
     set_smem(reinterpret_cast<const void*>(k_trinv_level), kSmemTrtri);
     set_smem(reinterpret_cast<const void*>(k_potrf_diag), kSmemTrtri);
     set_smem(reinterpret_cast<const void*>(k_chol_dataflow), kSmemDf);
+    set_smem(reinterpret_cast<const void*>(k_gram_basis), kSmemGram);
+    set_smem(reinterpret_cast<const void*>(k_gram_adjoint), kSmemGram);
+    {
+      const char* g = std::getenv("SDPX_B200_GRAM");  // "0": ordinary Schur form for every block
+      gram_enabled = !(g && g[0] == '0');
+    }
     red.init();
     status_.alloc(1);
     hstat_.alloc(1);
     for (auto& e : ev_) check(cudaEventCreate(&e), "event create");
   }
 
+  // host-side upload breakdown of the last upload (structure, rank-one test, device copies)
+  std::string upload_report() const {
+    char buf[160];
+    std::snprintf(buf, sizeof buf, "structure %.3f s, rank-one test %.3f s, copies %.3f s",
+                  up_t_[0], up_t_[1], up_t_[2]);
+    return buf;
+  }
+
   void upload(const HostProblem& p) {
+    const auto u0 = std::chrono::steady_clock::now();
     n = p.n;
     m = p.m;
     nblk = (int)p.psd.size();
@@ -225,6 +291,46 @@ class Engine {
         }
       }
     }
+    const auto u1 = std::chrono::steady_clock::now();
+    // rank-one (Gram) blocks keep only their factor; the others keep dense columns
+    std::vector<char> gram(nblk, 0);
+    std::vector<long> gu_off(nblk, 0);
+    std::vector<double> gu, gsig(col_ptr[nblk], 1.0);
+    ngram_ = 0;
+    for (int j = 0; j < nblk && gram_enabled; ++j) {
+      const int nj = hblocks[j].n, tn = nj * (nj + 1) / 2;
+      if (hk[j] == 0) continue;
+      std::vector<double> uj((size_t)nj * hk[j]);
+      bool ok = true;
+      for (int t = 0; t < hk[j] && ok; ++t)
+        ok = rank_one_column(&acol[acol_off[j] + (long)t * tn], nj, &uj[(size_t)t * nj],
+                             &gsig[col_ptr[j] + t]);
+      if (!ok) {
+        for (int t = 0; t < hk[j]; ++t) gsig[col_ptr[j] + t] = 1.0;
+        continue;
+      }
+      gram[j] = 1;
+      ngram_++;
+      gu_off[j] = (long)gu.size();
+      gu.insert(gu.end(), uj.begin(), uj.end());
+    }
+    if (ngram_ > 0) {  // repack the dense columns of the ordinary blocks only
+      std::vector<double> packed;
+      long off = 0;
+      for (int j = 0; j < nblk; ++j) {
+        const long len = (long)hblocks[j].n * (hblocks[j].n + 1) / 2 * hk[j];
+        if (gram[j]) {
+          acol_off[j] = 0;
+          continue;
+        }
+        packed.insert(packed.end(), acol.begin() + acol_off[j], acol.begin() + acol_off[j] + len);
+        acol_off[j] = off;
+        off += len;
+      }
+      acol.swap(packed);
+      aoff = off;
+    }
+    const auto u2 = std::chrono::steady_clock::now();
     std::vector<int> c2b_ptr(n + 1, 0), c2b_blk, c2b_loc;
     for (int c = 0; c < n; ++c) {
       for (auto& e : c2b[c]) {
@@ -233,20 +339,41 @@ class Engine {
       }
       c2b_ptr[c + 1] = (int)c2b_blk.size();
     }
-    std::vector<int> wblk, wloc, tiles;
+    std::vector<int> wblk, wloc, tiles, gtiles, gitem_blk, gitem_c0, gblk;
     for (int j = 0; j < nblk; ++j) {
-      for (int t = 0; t < hk[j]; ++t) {
-        wblk.push_back(j);
-        wloc.push_back(t);
+      if (gram[j]) {
+        gblk.push_back(j);
+        for (int c0 = 0; c0 < hk[j]; c0 += 64) {
+          gitem_blk.push_back(j);
+          gitem_c0.push_back(c0);
+        }
+      } else {
+        for (int t = 0; t < hk[j]; ++t) {
+          wblk.push_back(j);
+          wloc.push_back(t);
+        }
       }
+      std::vector<int>& tl = gram[j] ? gtiles : tiles;
       int nt = (hk[j] + 31) / 32;
       for (int tj = 0; tj < nt; ++tj)
         for (int ti = 0; ti < nt; ++ti) {
-          tiles.push_back(j);
-          tiles.push_back(ti);
-          tiles.push_back(tj);
+          tl.push_back(j);
+          tl.push_back(ti);
+          tl.push_back(tj);
         }
     }
+    ncol_ = col_ptr[nblk];
+    ngtiles_ = (int)gtiles.size() / 3;
+    ngitem_ = (int)gitem_blk.size();
+    ngblk_ = (int)gblk.size();
+    gU_.alloc(std::max<size_t>(gu.size(), 1)); gU_.upload(gu.data(), gu.size(), st);
+    gV_.alloc(std::max<size_t>(gu.size(), 1));
+    gsig_.alloc(std::max<size_t>(gsig.size(), 1)); gsig_.upload(gsig.data(), gsig.size(), st);
+    gu_off_.alloc(std::max(nblk, 1)); gu_off_.upload(gu_off.data(), nblk, st);
+    gtiles_.alloc(std::max<size_t>(gtiles.size(), 1)); gtiles_.upload(gtiles.data(), gtiles.size(), st);
+    gitem_blk_.alloc(std::max(ngitem_, 1)); gitem_blk_.upload(gitem_blk.data(), gitem_blk.size(), st);
+    gitem_c0_.alloc(std::max(ngitem_, 1)); gitem_c0_.upload(gitem_c0.data(), gitem_c0.size(), st);
+    gblk_.alloc(std::max(ngblk_, 1)); gblk_.upload(gblk.data(), gblk.size(), st);
     nwork_ = (int)wblk.size();
     ntiles_ = (int)tiles.size() / 3;
     // symmetric P in CSR (both triangles) for the x-row products
@@ -300,6 +427,7 @@ class Engine {
     {  // 64-row tiles of every block for the forward product
       std::vector<int> fb, fr;
       for (int j = 0; j < nblk; ++j) {
+        if (gram[j]) continue;
         int tn = hblocks[j].n * (hblocks[j].n + 1) / 2;
         for (int r0 = 0; r0 < tn; r0 += 64) {
           fb.push_back(j);
@@ -318,7 +446,7 @@ class Engine {
     pup_row_.alloc(std::max<size_t>(pup_row.size(), 1)); pup_row_.upload(pup_row.data(), pup_row.size(), st);
     pup_val_.alloc(std::max<size_t>(pup_val.size(), 1)); pup_val_.upload(pup_val.data(), pup_val.size(), st);
     pup_nnz_ = (int)pup_row.size();
-    adj_part_.alloc(std::max<size_t>((size_t)nwork_ * 2, 1));
+    adj_part_.alloc(std::max<size_t>((size_t)ncol_ * 2, 1));
     nchol = (n + kNB - 1) / kNB;
     Hsave_.alloc((size_t)n * n);
     F_.alloc((size_t)n * n);
@@ -348,6 +476,11 @@ class Engine {
     marg_out_.alloc(2 * std::max(nblk, 1));
     scal_.alloc(4);
     check(cudaStreamSynchronize(st), "upload sync");
+    const auto u3 = std::chrono::steady_clock::now();
+    auto sec = [](auto a, auto b) { return std::chrono::duration<double>(b - a).count(); };
+    up_t_[0] = sec(u0, u1);
+    up_t_[1] = sec(u1, u2);
+    up_t_[2] = sec(u2, u3);
   }
 
   // ---- status word ----
@@ -452,10 +585,17 @@ class Engine {
     need(x, "A_forward x");
     need(y, "A_forward y");
     if (!nblk) return;
-    ++g_launches, k_op_forward<<<dim3(nftile_, 1), 256, 0, st>>>(blocks_, kcount_, col_ptr_, col_idx_,
-                                                              acol_off_, acol_, ftile_blk_, ftile_r0_,
-                                                              x, n, alpha, beta, y, m);
-    launched("k_op_forward");
+    if (nftile_) {
+      ++g_launches, k_op_forward<<<dim3(nftile_, 1), 256, 0, st>>>(
+          blocks_, kcount_, col_ptr_, col_idx_, acol_off_, acol_, ftile_blk_, ftile_r0_, x, n, alpha,
+          beta, y, m);
+      launched("k_op_forward");
+    }
+    if (ngblk_) {
+      ++g_launches, k_gram_forward<<<dim3(ngblk_, SDPXG_NMAX / 8), 256, 0, st>>>(
+          blocks_, gblk_, kcount_, col_ptr_, col_idx_, gu_off_, gsig_, gU_, x, alpha, beta, y);
+      launched("k_gram_forward");
+    }
   }
   // y = alpha * A' z + beta * y   (length n)
   void A_adjoint(const double* z, double alpha, double beta, double* y) {
@@ -464,12 +604,17 @@ class Engine {
     if (nwork_) {
       int wpb = 8;
       ++g_launches, k_op_adjoint_partial<<<dim3((nwork_ + wpb - 1) / wpb, 1), 256, 0, st>>>(
-          blocks_, wblk_, wloc_, col_ptr_, acol_off_, acol_, z, m, adj_part_, nwork_, nwork_);
+          blocks_, wblk_, wloc_, col_ptr_, acol_off_, acol_, z, m, adj_part_, ncol_, nwork_);
       launched("k_op_adjoint_partial");
+    }
+    if (ngitem_) {
+      ++g_launches, k_gram_adjoint<<<ngitem_, 256, kSmemGram, st>>>(
+          blocks_, gitem_blk_, gitem_c0_, kcount_, col_ptr_, gu_off_, gsig_, gU_, z, adj_part_);
+      launched("k_gram_adjoint");
     }
     if (n) {
       ++g_launches, k_op_adjoint_gather<<<dim3((n + 255) / 256, 1), 256, 0, st>>>(
-          n, c2b_ptr_, c2b_blk_, c2b_loc_, col_ptr_, adj_part_, nwork_, alpha, beta, y, n);
+          n, c2b_ptr_, c2b_blk_, c2b_loc_, col_ptr_, adj_part_, ncol_, alpha, beta, y, n);
       launched("k_op_adjoint_gather");
     }
   }
@@ -497,6 +642,14 @@ class Engine {
       ++g_launches, k_schur_block_gemm<<<ntiles_, 256, 0, st>>>(blocks_, tiles_, kcount_, acol_off_, s_off_, acol_,
                                                   tcol_, S_);
       launched("k_schur_block_gemm");
+    }
+    if (ngitem_) {  // rank-one blocks: V = Rinv U, S = (sigma sigma') o (V'V)^2
+      ++g_launches, k_gram_basis<<<ngitem_, 256, kSmemGram, st>>>(blocks_, gitem_blk_, gitem_c0_, kcount_,
+                                                                 gu_off_, Rinv_, gU_, gV_);
+      launched("k_gram_basis");
+      ++g_launches, k_gram_schur<<<ngtiles_, 256, 0, st>>>(blocks_, gtiles_, kcount_, col_ptr_, gu_off_,
+                                                          s_off_, gsig_, gV_, S_);
+      launched("k_gram_schur");
     }
     long tot = (long)n * n;
     if (tot) {
@@ -614,6 +767,7 @@ class Engine {
   }
   void launched(const char* what) { check(cudaGetLastError(), what); }
 
+  double up_t_[3] = {0, 0, 0};
   int matlen_ = 0, veclen_ = 0, nwork_ = 0, ntiles_ = 0, p_nnz_ = 0, pup_nnz_ = 0;
   bool factor_ok_ = false;
   DevBuf<BlockDesc> blocks_;
@@ -623,6 +777,11 @@ class Engine {
   DevBuf<int> kcount_, col_ptr_, col_idx_, c2b_ptr_, c2b_blk_, c2b_loc_, wblk_, wloc_, tiles_;
   DevBuf<int> ftile_blk_, ftile_r0_;
   int nftile_ = 0;
+  // rank-one (Gram) blocks
+  DevBuf<double> gU_, gV_, gsig_;
+  DevBuf<long> gu_off_;
+  DevBuf<int> gtiles_, gitem_blk_, gitem_c0_, gblk_;
+  int ngram_ = 0, ngtiles_ = 0, ngitem_ = 0, ngblk_ = 0, ncol_ = 0;
   DevBuf<int> prp_, pci_, pup_ptr_, pup_row_;
   DevBuf<double> pv_, pup_val_;
   DevBuf<double> adj_part_;

@@ -1,0 +1,194 @@
+// Rank-one (Gram) form of the PSD constraint operator.
+//
+// When every column of A restricted to PSD block j is rank one, svec(sigma_t u_t u_t') with
+// sigma_t = +-1 (the sampled bootstrap SDPs: A_ij = w v v' with v a basis column), the block
+// is stored as its factor U_j = [u_1 .. u_k] (n_j x k_j, column-major) and signs sigma.  Then
+// with V_j = Rinv_j U_j (Ginv_j = Rinv_j' Rinv_j from the NT scaling):
+//   Schur block   S_j[a][b] = < A_a, Ginv A_b Ginv > = sigma_a sigma_b (V_j' V_j)[a][b]^2
+//   forward       (A x)_j   = svec(U_j diag(sigma x) U_j')
+//   adjoint       (A' z)_t += sigma_t u_t' smat(z_j) u_t
+// -- the same entries as the ordinary condensed path (kkt/condensed/psd.rs:1299-1534,
+// scaling.rs:74-81) and as the reference's sampled Gram update for rank-one terms
+// (sampled/mod.rs:1973-2025: H_pq = w_p w_q K_pq^2 with K = V'V, V = Rinv Q), at
+// O(n^2 k + n k^2) work per block instead of O(k n^3 + k^2 n^2), and reading n k instead
+// of k n(n+1)/2 doubles of operator data.
+#include "common.cuh"
+
+#define GR_LD 65
+
+// C (64 x nc, padded) = A (64 x 64, padded) B (64 x nc, padded) on the FP64 tensor cores,
+// one 8 x 8 output tile per warp at a time; K = 64 (zero padding makes the tail exact).
+__device__ __forceinline__ void gr_gemm_nn(double* C, const double* A, const double* B, int nr,
+                                           int nc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int rt = (nr + 7) >> 3, ct = (nc + 7) >> 3;
+  const int r = lane >> 2, q = lane & 3;
+  for (int t = warp; t < rt * ct; t += nwarps) {
+    const int ti = (t % rt) << 3, tj = (t / rt) << 3;
+    double d0 = 0.0, d1 = 0.0;
+#pragma unroll 4
+    for (int ks = 0; ks < 16; ++ks) {
+      const int k = (ks << 2) + q;
+      dmma_m8n8k4(d0, d1, A[(ti + r) + k * GR_LD], B[k + (tj + r) * GR_LD]);
+    }
+    C[(ti + r) + (tj + 2 * q) * GR_LD] = d0;
+    C[(ti + r) + (tj + 2 * q + 1) * GR_LD] = d1;
+  }
+}
+
+// U chunk: rows < n, columns c0 .. c0 + 63 (< k) of a block's factor into padded shared memory.
+__device__ __forceinline__ void gr_load_chunk(double* S, const double* __restrict__ U, int n, int k,
+                                              int c0) {
+  for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+    const int r = e & 63, c = e >> 6;
+    S[r + c * GR_LD] = (r < n && c0 + c < k) ? U[(long)(c0 + c) * n + r] : 0.0;
+  }
+}
+
+// V_j[:, c0 .. c0+63] = Rinv_j U_j[:, c0 .. c0+63]; item (block, column chunk).
+extern "C" __global__ void __launch_bounds__(256)
+k_gram_basis(const BlockDesc* __restrict__ blocks, const int* __restrict__ item_blk,
+             const int* __restrict__ item_c0, const int* __restrict__ kcount,
+             const long* __restrict__ gu_off, const double* __restrict__ Rinv,
+             const double* __restrict__ U, double* __restrict__ V) {
+  extern __shared__ double gsm[];
+  double* Rs = gsm;
+  double* Us = Rs + 64 * GR_LD;
+  double* Cs = Us + 64 * GR_LD;
+  const int j = item_blk[blockIdx.x], c0 = item_c0[blockIdx.x];
+  const BlockDesc bd = blocks[j];
+  const int n = bd.n, k = kcount[j];
+  const int nc = min(64, k - c0);
+  cta_load_mat(Rs, Rinv + bd.mat_off, n);
+  gr_load_chunk(Us, U + gu_off[j], n, k, c0);
+  __syncthreads();
+  gr_gemm_nn(Cs, Rs, Us, n, nc);
+  __syncthreads();
+  double* out = V + gu_off[j] + (long)c0 * n;
+  for (int e = threadIdx.x; e < n * nc; e += blockDim.x) out[e] = Cs[(e % n) + (e / n) * GR_LD];
+}
+
+// S_j tile (32 x 32): S[a][b] = sigma_a sigma_b (sum_r V[r][a] V[r][b])^2.  Both triangles are
+// computed with the same products in the same order, so S_j is exactly symmetric.
+extern "C" __global__ void __launch_bounds__(256)
+k_gram_schur(const BlockDesc* __restrict__ blocks, const int* __restrict__ tiles,
+             const int* __restrict__ kcount, const int* __restrict__ col_ptr,
+             const long* __restrict__ gu_off, const long* __restrict__ s_off,
+             const double* __restrict__ gsig, const double* __restrict__ V,
+             double* __restrict__ S) {
+  __shared__ double Va[64][33];
+  __shared__ double Vb[64][33];
+  const int j = tiles[3 * blockIdx.x], ti = tiles[3 * blockIdx.x + 1], tj = tiles[3 * blockIdx.x + 2];
+  const int n = blocks[j].n, k = kcount[j];
+  const double* Vj = V + gu_off[j];
+  for (int e = threadIdx.x; e < 64 * 32; e += blockDim.x) {
+    const int r = e & 63, c = e >> 6;
+    const int ca = ti * 32 + c, cb = tj * 32 + c;
+    Va[r][c] = (r < n && ca < k) ? Vj[(long)ca * n + r] : 0.0;
+    Vb[r][c] = (r < n && cb < k) ? Vj[(long)cb * n + r] : 0.0;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
+  for (int r = 0; r < n; ++r) {
+    const double x0 = Va[r][2 * tx], x1 = Va[r][2 * tx + 1];
+    const double y0 = Vb[r][2 * ty], y1 = Vb[r][2 * ty + 1];
+    c00 = fma(x0, y0, c00);
+    c01 = fma(x0, y1, c01);
+    c10 = fma(x1, y0, c10);
+    c11 = fma(x1, y1, c11);
+  }
+  const int a0 = ti * 32 + 2 * tx, b0 = tj * 32 + 2 * ty;
+  const double* sg = gsig + col_ptr[j];
+  double* out = S + s_off[j];
+  const double cv[2][2] = {{c00, c01}, {c10, c11}};
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const int a = a0 + u, b = b0 + v;
+      if (a < k && b < k) out[a + (long)b * k] = (sg[a] * sg[b]) * (cv[u][v] * cv[u][v]);
+    }
+}
+
+// y_j = alpha svec(U_j diag(sigma x_cols) U_j') + beta y_j.  Grid (Gram block, 8-row tile R):
+// warp w computes the 8 x 8 output tile (R, w) for w >= R (upper triangle) on the FP64 tensor
+// cores with fragments read straight from the factor (L1/L2 resident), K = k_j in chunks of
+// 256 whose scaled weights d_t = sigma_t x[col_t] are staged in shared memory.
+#define GR_KCH 256
+extern "C" __global__ void __launch_bounds__(256)
+k_gram_forward(const BlockDesc* __restrict__ blocks, const int* __restrict__ gblk,
+               const int* __restrict__ kcount, const int* __restrict__ col_ptr,
+               const int* __restrict__ col_idx, const long* __restrict__ gu_off,
+               const double* __restrict__ gsig, const double* __restrict__ U,
+               const double* __restrict__ x, double alpha, double beta, double* __restrict__ y) {
+  __shared__ double d[GR_KCH];
+  const int j = gblk[blockIdx.x], R = blockIdx.y;
+  const BlockDesc bd = blocks[j];
+  const int n = bd.n, k = kcount[j];
+  if (8 * R >= n) return;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, r = lane >> 2, q = lane & 3;
+  const double* Uj = U + gu_off[j];
+  const int* cols = col_idx + col_ptr[j];
+  const double* sg = gsig + col_ptr[j];
+  const int row = 8 * R + r, col = 8 * w + r;  // fragment rows of the A (rows) and B (cols) sides
+  const bool live = (w >= R) && (8 * w < n);
+  double d0 = 0.0, d1 = 0.0;
+  for (int t0 = 0; t0 < k; t0 += GR_KCH) {
+    const int kc = min(GR_KCH, k - t0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < kc; t += blockDim.x) d[t] = sg[t0 + t] * x[cols[t0 + t]];
+    __syncthreads();
+    if (live) {
+      for (int ks = 0; ks < (kc + 3) / 4; ++ks) {
+        const int t = 4 * ks + q;
+        const bool in = t < kc;
+        const double* ut = Uj + (long)(t0 + t) * n;
+        const double a = (in && row < n) ? d[t] * ut[row] : 0.0;  // (U diag(d))[row][t]
+        const double b = (in && col < n) ? ut[col] : 0.0;          // U'[t][col]
+        dmma_m8n8k4(d0, d1, a, b);
+      }
+    }
+  }
+  if (!live) return;
+  const int orow = 8 * R + r;
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const int ocol = 8 * w + 2 * q + e;
+    if (orow <= ocol && ocol < n) {
+      const double v = (e == 0) ? d0 : d1;
+      const long idx = bd.svec_off + (long)ocol * (ocol + 1) / 2 + orow;
+      const double s = (orow == ocol) ? v : v * SDPXG_SQRT2;
+      y[idx] = alpha * s + ((beta == 0.0) ? 0.0 : beta * y[idx]);
+    }
+  }
+}
+
+// p[col_ptr[j] + t] = sigma_t u_t' smat(z_j) u_t for the columns of one 64-column chunk.
+extern "C" __global__ void __launch_bounds__(256)
+k_gram_adjoint(const BlockDesc* __restrict__ blocks, const int* __restrict__ item_blk,
+               const int* __restrict__ item_c0, const int* __restrict__ kcount,
+               const int* __restrict__ col_ptr, const long* __restrict__ gu_off,
+               const double* __restrict__ gsig, const double* __restrict__ U,
+               const double* __restrict__ z, double* __restrict__ p) {
+  extern __shared__ double gsm[];
+  double* Zs = gsm;
+  double* Us = Zs + 64 * GR_LD;
+  double* Ws = Us + 64 * GR_LD;
+  const int j = item_blk[blockIdx.x], c0 = item_c0[blockIdx.x];
+  const BlockDesc bd = blocks[j];
+  const int n = bd.n, k = kcount[j];
+  const int nc = min(64, k - c0);
+  cta_load_smat(Zs, z + bd.svec_off, n);
+  gr_load_chunk(Us, U + gu_off[j], n, k, c0);
+  __syncthreads();
+  gr_gemm_nn(Ws, Zs, Us, n, nc);  // W = Z U_chunk
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int c = warp; c < nc; c += blockDim.x >> 5) {
+    double acc = 0.0;
+    for (int r = lane; r < n; r += 32) acc = fma(Us[r + c * GR_LD], Ws[r + c * GR_LD], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) p[col_ptr[j] + c0 + c] = gsig[col_ptr[j] + c0 + c] * acc;
+  }
+}

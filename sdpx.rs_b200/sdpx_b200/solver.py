@@ -204,6 +204,12 @@ class DefaultSolver:
         self._b = np.ascontiguousarray(b, dtype=np.float64)
         _lib.call("sdpx_update", self._h, C.byref(_scalars(self._q)), C.byref(_scalars(self._b)))
 
+    def schur_forms(self) -> dict:
+        """PSD blocks in the rank-one Gram form and in the ordinary dense-column form."""
+        g, o = C.c_uint32(), C.c_uint32()
+        _lib.call("sdpx_b200_schur_forms", self._h, C.byref(g), C.byref(o))
+        return {"gram": int(g.value), "ordinary": int(o.value)}
+
     def solver_name(self) -> str:
         need = C.c_uint64()
         _lib.call("sdpx_get_solver_name", self._h, None, 0, C.byref(need))
