@@ -12,7 +12,10 @@
 #include <stdint.h>
 
 #define SDPXG_NMAX 64               // largest PSD block order handled by the CTA kernels
-#define SDPXG_LD (SDPXG_NMAX + 1)   // shared-memory leading dimension (odd: fewer bank conflicts)
+// Shared-memory leading dimension: 68 = 4 (mod 16), so the 16 lanes of a half-warp reading an
+// m8n8k4 f64 fragment (rows r + 4-column k, or 4-row k + columns r) hit 16 distinct 8-byte
+// bank pairs, and a column read is conflict-free.
+#define SDPXG_LD 68
 #define SDPXG_THREADS 256         // dense tile kernels (their thread maps assume 256)
 #define SDPXG_CONE_THREADS 1024   // one CTA per PSD block: one warp per Jacobi rotation pair
 #define SDPXG_RSQRT2 0.70710678118654752440
@@ -115,20 +118,27 @@ __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, do
 }
 
 // C = op(A) op(B) on zero-padded shared matrices, one 8 x 8 output tile per warp at a time,
-// K in steps of 4 up to n rounded up.  C must not alias A or B.
+// K in groups of 16 (four k-steps) up to n rounded up: the fragments of a group are loaded
+// before its four MMAs, so the shared-memory latency overlaps instead of serialising with the
+// accumulation chain (the zero padding makes the rounded-up K exact).  C must not alias A or B.
 template <bool TA, bool TB>
 __device__ __forceinline__ void cta_gemm_mma(double* C, const double* A, const double* B, int n) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int tiles = (n + 7) >> 3, ksteps = (n + 3) >> 2;
+  const int tiles = (n + 7) >> 3, kgroups = (n + 15) >> 4;
   const int r = lane >> 2, q = lane & 3;
   for (int t = warp; t < tiles * tiles; t += nwarps) {
     const int ti = (t % tiles) << 3, tj = (t / tiles) << 3;
     double d0 = 0.0, d1 = 0.0;
-    for (int ks = 0; ks < ksteps; ++ks) {
-      const int k = (ks << 2) + q;
-      const double a = TA ? SM(A, k, ti + r) : SM(A, ti + r, k);
-      const double b = TB ? SM(B, tj + r, k) : SM(B, k, tj + r);
-      dmma_m8n8k4(d0, d1, a, b);
+    for (int kg = 0; kg < kgroups; ++kg) {
+      double a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int k = (kg << 4) + (u << 2) + q;
+        a[u] = TA ? SM(A, k, ti + r) : SM(A, ti + r, k);
+        b[u] = TB ? SM(B, tj + r, k) : SM(B, k, tj + r);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) dmma_m8n8k4(d0, d1, a[u], b[u]);
     }
     SM(C, ti + r, tj + 2 * q) = d0;
     SM(C, ti + r, tj + 2 * q + 1) = d1;

@@ -51,7 +51,7 @@ k_nt_scale(const BlockDesc* __restrict__ blocks, const double* __restrict__ s,
   }
   cta_gemm(M, L2, true, L1, false, n);  // M = L2' L1
   __syncthreads();
-  int sweeps = cta_jacobi_svd(M, V, n, flag);
+  int sweeps = cta_jacobi_svd(M, V, n, flag, piv);  // Cholesky scratch is free now
   if (sweeps < 0) {
     if (threadIdx.x == 0) atomicOr(status, SDPXG_ST_SVD_UNCONVERGED);
     return;

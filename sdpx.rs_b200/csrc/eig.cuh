@@ -17,8 +17,11 @@
 #define SDPXG_BISECT_MAX 256
 
 // Returns the number of sweeps used, or -1 when the sweep bound was hit.
-// `flag` is one int of shared memory.
-__device__ inline int cta_jacobi_svd(double* M, double* V, int n, int* flag) {
+// `flag` is one int of shared memory, `nrm` n doubles of shared memory.  The squared column
+// norms are recomputed at the start of every sweep and carried through the rotations with the
+// exact update a' = a - t g, b' = b + t g, so a rotation needs one warp reduction (g) instead
+// of three.
+__device__ inline int cta_jacobi_svd(double* M, double* V, int n, int* flag, double* nrm) {
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     int i = e % n, j = e / n;
     SM(V, i, j) = (i == j) ? 1.0 : 0.0;
@@ -30,44 +33,65 @@ __device__ inline int cta_jacobi_svd(double* M, double* V, int n, int* flag) {
     return 0;
   }
   for (int sweep = 0; sweep < SDPXG_JACOBI_MAX_SWEEPS; ++sweep) {
+    __syncthreads();  // the previous sweep's last rotations are visible
+    for (int p = warp; p < n; p += nwarps) {
+      double a = 0.0;
+      for (int k = lane; k < n; k += 32) a = fma(SM(M, k, p), SM(M, k, p), a);
+      a = warp_sum(a);
+      if (lane == 0) nrm[p] = a;
+    }
     if (threadIdx.x == 0) *flag = 0;
     __syncthreads();
     for (int r = 0; r < N - 1; ++r) {
       for (int pi = warp; pi < N / 2; pi += nwarps) {
-        int p, q;
+        int p, q;  // round-robin pairing without integer division: r, pi < N - 1
         if (pi == 0) {
           p = N - 1;
           q = r;
         } else {
-          p = (r + pi) % (N - 1);
-          q = (r - pi + N - 1) % (N - 1);
+          p = r + pi;
+          if (p >= N - 1) p -= N - 1;
+          q = r - pi + N - 1;
+          if (q >= N - 1) q -= N - 1;
         }
         if (p >= n || q >= n) continue;
-        double a = 0.0, b = 0.0, g = 0.0;
-        for (int k = lane; k < n; k += 32) {
-          double x = SM(M, k, p), y = SM(M, k, q);
-          a = fma(x, x, a);
-          b = fma(y, y, b);
-          g = fma(x, y, g);
+        const double a = nrm[p], b = nrm[q];
+        double g = 0.0;
+        double x0 = 0.0, y0 = 0.0, x1 = 0.0, y1 = 0.0;  // n <= 64: two entries per lane
+        if (lane < n) {
+          x0 = SM(M, lane, p);
+          y0 = SM(M, lane, q);
         }
-        a = warp_sum(a);
-        b = warp_sum(b);
+        if (lane + 32 < n) {
+          x1 = SM(M, lane + 32, p);
+          y1 = SM(M, lane + 32, q);
+        }
+        g = fma(x1, y1, x0 * y0);
         g = warp_sum(g);
-        if (fabs(g) > SDPXG_JACOBI_TOL * sqrt(a * b)) {
-          double zeta = (b - a) / (2.0 * g);
-          double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
-          double c = rsqrt(fma(t, t, 1.0));
-          double s = c * t;
-          for (int k = lane; k < n; k += 32) {
-            double x = SM(M, k, p), y = SM(M, k, q);
-            SM(M, k, p) = c * x - s * y;
-            SM(M, k, q) = s * x + c * y;
-            x = SM(V, k, p);
-            y = SM(V, k, q);
-            SM(V, k, p) = c * x - s * y;
-            SM(V, k, q) = s * x + c * y;
+        if (g * g > (SDPXG_JACOBI_TOL * SDPXG_JACOBI_TOL) * (a * b)) {  // |g| > tol sqrt(ab)
+          const double zeta = (b - a) / (2.0 * g);
+          const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
+          const double c = rsqrt(fma(t, t, 1.0));
+          const double s = c * t;
+          if (lane < n) {
+            SM(M, lane, p) = c * x0 - s * y0;
+            SM(M, lane, q) = s * x0 + c * y0;
+            const double v0 = SM(V, lane, p), w0 = SM(V, lane, q);
+            SM(V, lane, p) = c * v0 - s * w0;
+            SM(V, lane, q) = s * v0 + c * w0;
           }
-          if (lane == 0) *flag = 1;
+          if (lane + 32 < n) {
+            SM(M, lane + 32, p) = c * x1 - s * y1;
+            SM(M, lane + 32, q) = s * x1 + c * y1;
+            const double v1 = SM(V, lane + 32, p), w1 = SM(V, lane + 32, q);
+            SM(V, lane + 32, p) = c * v1 - s * w1;
+            SM(V, lane + 32, q) = s * v1 + c * w1;
+          }
+          if (lane == 0) {
+            nrm[p] = a - t * g;
+            nrm[q] = b + t * g;
+            *flag = 1;
+          }
         }
       }
       __syncthreads();

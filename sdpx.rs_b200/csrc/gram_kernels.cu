@@ -14,7 +14,7 @@
 // of k n(n+1)/2 doubles of operator data.
 #include "common.cuh"
 
-#define GR_LD 65
+#define GR_LD SDPXG_LD  // the layout of cta_load_mat / cta_load_smat
 
 // C (64 x nc, padded) = A (64 x 64, padded) B (64 x nc, padded) on the FP64 tensor cores,
 // one 8 x 8 output tile per warp at a time; K = 64 (zero padding makes the tail exact).
@@ -26,10 +26,17 @@ __device__ __forceinline__ void gr_gemm_nn(double* C, const double* A, const dou
   for (int t = warp; t < rt * ct; t += nwarps) {
     const int ti = (t % rt) << 3, tj = (t / rt) << 3;
     double d0 = 0.0, d1 = 0.0;
-#pragma unroll 4
-    for (int ks = 0; ks < 16; ++ks) {
-      const int k = (ks << 2) + q;
-      dmma_m8n8k4(d0, d1, A[(ti + r) + k * GR_LD], B[k + (tj + r) * GR_LD]);
+#pragma unroll
+    for (int kg = 0; kg < 4; ++kg) {
+      double a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int k = (kg << 4) + (u << 2) + q;
+        a[u] = A[(ti + r) + k * GR_LD];
+        b[u] = B[k + (tj + r) * GR_LD];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) dmma_m8n8k4(d0, d1, a[u], b[u]);
     }
     C[(ti + r) + (tj + 2 * q) * GR_LD] = d0;
     C[(ti + r) + (tj + 2 * q + 1) * GR_LD] = d1;
