@@ -165,6 +165,9 @@ class Reducer {
     }
     return s;
   }
+  int count() const { return count_; }
+  // Slots queued by a replayed captured segment (its reductions ran inside the graph).
+  void set_count(int c) { count_ = c; }
   const PinnedBuf<double>& fetch(cudaStream_t st) {
     if (count_) {
       check(cudaMemcpyAsync(host_.p, slots_.p, count_ * sizeof(double),

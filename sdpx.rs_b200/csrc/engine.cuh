@@ -19,6 +19,7 @@
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <unordered_map>
 
 #include "device.cuh"
 
@@ -178,8 +179,60 @@ class Engine {
 
   Engine() = default;
   ~Engine() {
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second.exec);
     for (auto& e : ev_) if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
+  }
+
+  // ---- captured segments ----
+  // A segment is a straight run of launches, copies and queued reductions between two host
+  // reads whose shape depends only on the device pointers in its key (fixed scalars).  The
+  // first run captures it into a CUDA graph (stream capture on this engine's stream); later
+  // runs launch the instantiated graph.  The reducer's slot count is restored on replay.
+  // Eager when graphs are off (SDPX_B200_GRAPHS=0) or while phase timing is on (its events
+  // synchronize the host).
+  bool graphs_enabled = true;
+  // Captured graphs hold device pointers by value: drop them whenever buffers they may reference
+  // are (re)allocated (a new upload, a new solver's work vectors).
+  void clear_graphs() {
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second.exec);
+    graphs_.clear();
+  }
+  template <typename F>
+  void segment(int id, std::initializer_list<const void*> ptrs, F&& body) {
+    if (!graphs_enabled || timing || n == 0 || m == 0) {
+      body();
+      return;
+    }
+    if (red.count() != 0) throw CudaError("a captured segment must start with an empty reducer");
+    std::string key(reinterpret_cast<const char*>(&id), sizeof id);
+    for (const void* p : ptrs) key.append(reinterpret_cast<const char*>(&p), sizeof p);
+    auto it = graphs_.find(key);
+    if (it != graphs_.end()) {
+      check(cudaGraphLaunch(it->second.exec, st), "cudaGraphLaunch");
+      red.set_count(it->second.red_count);
+      g_launches += it->second.launches;
+      return;
+    }
+    if (graphs_.size() >= kMaxGraphs) clear_graphs();  // bound the cache
+    const uint64_t l0 = g_launches;
+    check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+      body();
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(st, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    cudaGraph_t g = nullptr;
+    check(cudaStreamEndCapture(st, &g), "end capture");
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    check(e, "cudaGraphInstantiate");
+    graphs_[key] = {ex, red.count(), g_launches - l0};
+    check(cudaGraphLaunch(ex, st), "cudaGraphLaunch");
   }
   void tbegin(int k) {
     if (timing) check(cudaEventRecord(ev_[2 * k], st), "event");
@@ -216,6 +269,8 @@ class Engine {
     {
       const char* g = std::getenv("SDPX_B200_GRAM");  // "0": ordinary Schur form for every block
       gram_enabled = !(g && g[0] == '0');
+      const char* c = std::getenv("SDPX_B200_GRAPHS");  // "0": launch every segment eagerly
+      graphs_enabled = !(c && c[0] == '0');
     }
     red.init();
     status_.alloc(1);
@@ -233,6 +288,7 @@ class Engine {
 
   void upload(const HostProblem& p) {
     const auto u0 = std::chrono::steady_clock::now();
+    clear_graphs();
     n = p.n;
     m = p.m;
     nblk = (int)p.psd.size();
@@ -794,6 +850,13 @@ class Engine {
   DevBuf<int> df_sync_;
   int df_items_ = 0, df_grid_ = 0;
   cudaEvent_t ev_[2 * KT_N] = {};
+  struct GraphEntry {
+    cudaGraphExec_t exec;
+    int red_count;
+    uint64_t launches;
+  };
+  static constexpr size_t kMaxGraphs = 256;
+  std::unordered_map<std::string, GraphEntry> graphs_;
 };
 
 }  // namespace sdpxg

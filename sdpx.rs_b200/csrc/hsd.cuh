@@ -70,6 +70,7 @@ class HsdSolver {
   HsdSolver(Engine& eng, const HostProblem& p, const Equilibration& eq, const Settings& st)
       : E(eng), eq_(eq), st_(st), n_(p.n), m_(p.m) {
     const int n = n_, m = m_;
+    E.clear_graphs();  // segments captured for earlier work vectors must not be replayed
     auto vn = [&](DevBuf<double>& b) { b.alloc(std::max(n, 1)); };
     auto vm = [&](DevBuf<double>& b) { b.alloc(std::max(m, 1)); };
     for (auto* b : {&x_, &px_, &bx_, &rx_, &rxinf_, &Px_, &x2_, &dx_, &ax_, &tx_, &prevx_, &bestx_,
@@ -123,6 +124,10 @@ class HsdSolver {
   // ---------------- KKT system (also driven directly by the kernel-level ABI) ----------------
   bool kkt_update();
   bool reduced_solve(const double* r, double* x);
+  void reduced_first(const double* r, double* x);
+  bool reduced_refine(const double* r, double* x, double normb, double norme);
+  void condense_first(const double* bx, const double* bz, double* x);
+  void recover(const double* bz, const double* x, double* z);
   bool solve_raw(const double* bx, const double* bz, double* x, double* z);
   bool kkt_solve(const double* bx, const double* bz, double* x, double* z);
   void residual_full(const double* bx, const double* bz, const double* x, const double* z,
@@ -197,28 +202,38 @@ inline bool HsdSolver::kkt_update() {
   return ok;
 }
 
-// Stationary refinement of the reduced system against the unshifted Schur complement.
-inline bool HsdSolver::reduced_solve(const double* r, double* x) {
+// Captured segments of the KKT solve (Engine::segment): ids of the straight runs between the
+// host reads of the refinement norms.
+enum : int { SEG_RS_HEAD = 1, SEG_RS_STEP = 2, SEG_RAW_HEAD = 3, SEG_RAW_TAIL = 4,
+             SEG_KKT_HEAD = 5, SEG_KKT_TAIL = 6, SEG_OUT_HEAD = 7, SEG_OUT_TAIL = 8 };
+
+// First pass of the reduced solve: x = F^-1 r and e = r - H x (unshifted Schur).
+// Queues |r|max, |e|max and finite(x).
+inline void HsdSolver::reduced_first(const double* r, double* x) {
   const int n = n_;
   E.trisolve(r, x);
-  if (!st_.ir_enable) return true;
   E.schur_residual(r, x, en_);
-  int s0 = E.red.add(st(), RED_MAXABS, n, r, nullptr);
-  int s1 = E.red.add(st(), RED_MAXABS, n, en_, nullptr);
-  int s2 = E.red.add(st(), RED_FINITE, n, x, nullptr);
-  auto& h = E.red.fetch(st());
-  double normb = h[s0], norme = h[s1];
-  if (h[s2] != 1.0 || !std::isfinite(norme)) return false;
+  E.red.add(st(), RED_MAXABS, n, r, nullptr);
+  E.red.add(st(), RED_MAXABS, n, en_, nullptr);
+  E.red.add(st(), RED_FINITE, n, x, nullptr);
+}
+
+// Stationary refinement of the reduced system against the unshifted Schur complement, from the
+// norms of the first pass (kkt/refinement.rs:118-191 stopping rules).
+inline bool HsdSolver::reduced_refine(const double* r, double* x, double normb, double norme) {
+  const int n = n_;
   const double tol = st_.ir_abstol + st_.ir_reltol * normb;
   bool converged = norme <= tol;
   for (int it = 0; it < st_.ir_max_iter && !converged; ++it) {
     double previous = norme;
     times.inner_refinements++;
-    E.trisolve(en_, dxn_);
-    E.lincomb(n, 1.0, x, 1.0, dxn_, 0.0, nullptr, candn_);
-    E.schur_residual(r, candn_, e2n_);
-    int a = E.red.add(st(), RED_MAXABS, n, e2n_, nullptr);
-    norme = E.red.fetch(st())[a];
+    E.segment(SEG_RS_STEP, {r, x}, [&] {
+      E.trisolve(en_, dxn_);
+      E.lincomb(n, 1.0, x, 1.0, dxn_, 0.0, nullptr, candn_);
+      E.schur_residual(r, candn_, e2n_);
+      E.red.add(st(), RED_MAXABS, n, e2n_, nullptr);
+    });
+    norme = E.red.fetch(st())[0];
     if (!std::isfinite(norme)) return false;
     double ratio = previous / norme;
     if (ratio < st_.ir_stop_ratio) {
@@ -232,15 +247,48 @@ inline bool HsdSolver::reduced_solve(const double* r, double* x) {
   return true;
 }
 
+inline bool HsdSolver::reduced_solve(const double* r, double* x) {
+  if (!st_.ir_enable) {
+    E.trisolve(r, x);
+    return true;
+  }
+  E.segment(SEG_RS_HEAD, {r, x}, [&] { reduced_first(r, x); });
+  auto& h = E.red.fetch(st());
+  const double normb = h[0], norme = h[1];
+  if (h[2] != 1.0 || !std::isfinite(norme)) return false;
+  return reduced_refine(r, x, normb, norme);
+}
+
+// Condense: xhat = bx + A' Hs^-1 bz (kkt/condensed/mod.rs:2416-2507), then the first pass.
+inline void HsdSolver::condense_first(const double* bx, const double* bz, double* x) {
+  E.cone_apply(CM_HINV, bz, tm_);     // Hs^-1 bz
+  E.copy(xhat_, bx, n_);
+  E.A_adjoint(tm_, 1.0, 1.0, xhat_);  // bx + A' Hs^-1 bz
+  reduced_first(xhat_, x);
+}
+
+// Recover z = Hs^-1 (A x - bz) (kkt/condensed/mod.rs:2511-2604).
+inline void HsdSolver::recover(const double* bz, const double* x, double* z) {
+  E.lincomb(m_, -1.0, bz, 0.0, nullptr, 0.0, nullptr, tm_);
+  E.A_forward(x, 1.0, 1.0, tm_);  // A x - bz
+  E.cone_apply(CM_HINV, tm_, z);
+}
+
 // Condense, reduced solve, recover (kkt/condensed/mod.rs:2416-2622).
 inline bool HsdSolver::solve_raw(const double* bx, const double* bz, double* x, double* z) {
-  E.cone_apply(CM_HINV, bz, tm_);             // Hs^-1 bz
-  E.copy(xhat_, bx, n_);
-  E.A_adjoint(tm_, 1.0, 1.0, xhat_);          // bx + A' Hs^-1 bz
-  if (!reduced_solve(xhat_, x)) return false;
-  E.lincomb(m_, -1.0, bz, 0.0, nullptr, 0.0, nullptr, tm_);
-  E.A_forward(x, 1.0, 1.0, tm_);              // A x - bz
-  E.cone_apply(CM_HINV, tm_, z);              // z = Hs^-1 (A x - bz)
+  if (!st_.ir_enable) {
+    E.cone_apply(CM_HINV, bz, tm_);
+    E.copy(xhat_, bx, n_);
+    E.A_adjoint(tm_, 1.0, 1.0, xhat_);
+    E.trisolve(xhat_, x);
+    recover(bz, x, z);
+    return true;
+  }
+  E.segment(SEG_RAW_HEAD, {bx, bz, x}, [&] { condense_first(bx, bz, x); });
+  auto& h = E.red.fetch(st());
+  if (h[2] != 1.0 || !std::isfinite(h[1])) return false;
+  if (!reduced_refine(xhat_, x, h[0], h[1])) return false;
+  E.segment(SEG_RAW_TAIL, {bz, x, z}, [&] { recover(bz, x, z); });
   return true;
 }
 
@@ -256,59 +304,87 @@ inline void HsdSolver::residual_full(const double* bx, const double* bz, const d
 }
 
 // Solve with outer refinement on the original operator (kkt/condensed/kkt.rs:275-318,
-// kkt/refinement.rs:118-191).
+// kkt/refinement.rs:118-191).  The work between two host reads of refinement norms runs as one
+// captured segment: right-hand-side check + condense + first reduced pass; recover + full
+// residual; and the same pair for every outer correction.
 inline bool HsdSolver::kkt_solve(const double* bx, const double* bz, double* x, double* z) {
   auto t0 = clock::now();
   times.kkt_solves++;
   const int n = n_, m = m_;
-  {
+  if (!st_.ir_enable) {
     int a = E.red.add(st(), RED_FINITE, n, bx, nullptr);
     int b = E.red.add(st(), RED_FINITE, m, bz, nullptr);
     auto& h = E.red.fetch(st());
     if (h[a] != 1.0 || h[b] != 1.0) return false;
+    const bool ok = solve_raw(bx, bz, x, z);
+    times.solve += secs(t0);
+    return ok;
   }
-  if (!solve_raw(bx, bz, x, z)) return false;
-  bool ok = true;
-  if (st_.ir_enable) {
-    residual_full(bx, bz, x, z, ex_, ez_);
-    int s0 = E.red.add(st(), RED_MAXABS, n, bx, nullptr);
-    int s1 = E.red.add(st(), RED_MAXABS, m, bz, nullptr);
-    int s2 = E.red.add(st(), RED_MAXABS, n, ex_, nullptr);
-    int s3 = E.red.add(st(), RED_MAXABS, m, ez_, nullptr);
+  E.segment(SEG_KKT_HEAD, {bx, bz, x}, [&] {
+    E.red.add(st(), RED_FINITE, n, bx, nullptr);
+    E.red.add(st(), RED_FINITE, m, bz, nullptr);
+    condense_first(bx, bz, x);
+  });
+  {
     auto& h = E.red.fetch(st());
-    double normb = std::max(h[s0], h[s1]);
-    double norme = std::max(h[s2], h[s3]);
-    if (!std::isfinite(norme)) {
-      ok = false;
-    } else {
-      const double tol = st_.ir_abstol + st_.ir_reltol * normb;
-      bool converged = norme <= tol;
-      for (int it = 0; it < st_.ir_max_iter && !converged; ++it) {
-        double previous = norme;
-        times.outer_refinements++;
-        if (!solve_raw(ex_, ez_, cx_, cz_)) { ok = false; break; }
+    if (h[0] != 1.0 || h[1] != 1.0) return false;  // non-finite right-hand side
+    if (h[4] != 1.0 || !std::isfinite(h[3])) return false;
+    const double normb = h[2], norme = h[3];
+    if (!reduced_refine(xhat_, x, normb, norme)) return false;
+  }
+  E.segment(SEG_KKT_TAIL, {bx, bz, x, z}, [&] {
+    recover(bz, x, z);
+    residual_full(bx, bz, x, z, ex_, ez_);
+    E.red.add(st(), RED_MAXABS, n, bx, nullptr);
+    E.red.add(st(), RED_MAXABS, m, bz, nullptr);
+    E.red.add(st(), RED_MAXABS, n, ex_, nullptr);
+    E.red.add(st(), RED_MAXABS, m, ez_, nullptr);
+  });
+  bool ok = true;
+  auto& h = E.red.fetch(st());
+  const double normb = std::max(h[0], h[1]);
+  double norme = std::max(h[2], h[3]);
+  if (!std::isfinite(norme)) {
+    ok = false;
+  } else {
+    const double tol = st_.ir_abstol + st_.ir_reltol * normb;
+    bool converged = norme <= tol;
+    for (int it = 0; it < st_.ir_max_iter && !converged; ++it) {
+      double previous = norme;
+      times.outer_refinements++;
+      // correction (cx, cz) = K^-1 (ex, ez), same steps as solve_raw
+      E.segment(SEG_OUT_HEAD, {ex_.p, ez_.p, cx_.p}, [&] { condense_first(ex_, ez_, cx_); });
+      {
+        auto& hc = E.red.fetch(st());
+        if (hc[2] != 1.0 || !std::isfinite(hc[1]) || !reduced_refine(xhat_, cx_, hc[0], hc[1])) {
+          ok = false;
+          break;
+        }
+      }
+      E.segment(SEG_OUT_TAIL, {bx, bz, x, z}, [&] {
+        recover(ez_, cx_, cz_);
         E.lincomb(n, 1.0, x, 1.0, cx_, 0.0, nullptr, candx_);
         E.lincomb(m, 1.0, z, 1.0, cz_, 0.0, nullptr, candz_);
         residual_full(bx, bz, candx_, candz_, ex2_, ez2_);
-        int a = E.red.add(st(), RED_MAXABS, n, ex2_, nullptr);
-        int b = E.red.add(st(), RED_MAXABS, m, ez2_, nullptr);
-        auto& hh = E.red.fetch(st());
-        norme = std::max(hh[a], hh[b]);
-        if (!std::isfinite(norme)) { ok = false; break; }
-        double ratio = previous / norme;
-        if (ratio < st_.ir_stop_ratio) {
-          if (ratio > 1.0) {
-            E.copy(x, candx_, n);
-            E.copy(z, candz_, m);
-          }
-          break;
+        E.red.add(st(), RED_MAXABS, n, ex2_, nullptr);
+        E.red.add(st(), RED_MAXABS, m, ez2_, nullptr);
+      });
+      auto& hh = E.red.fetch(st());
+      norme = std::max(hh[0], hh[1]);
+      if (!std::isfinite(norme)) { ok = false; break; }
+      double ratio = previous / norme;
+      if (ratio < st_.ir_stop_ratio) {
+        if (ratio > 1.0) {
+          E.copy(x, candx_, n);
+          E.copy(z, candz_, m);
         }
-        E.copy(x, candx_, n);
-        E.copy(z, candz_, m);
-        E.copy(ex_, ex2_, n);
-        E.copy(ez_, ez2_, m);
-        converged = norme <= tol;
+        break;
       }
+      E.copy(x, candx_, n);
+      E.copy(z, candz_, m);
+      E.copy(ex_, ex2_, n);
+      E.copy(ez_, ez2_, m);
+      converged = norme <= tol;
     }
   }
   times.solve += secs(t0);

@@ -1,0 +1,54 @@
+"""Captured KKT-solve segments (CUDA graphs) against eager launches.
+
+The graphs replay exactly the kernels the eager path launches, in the same order on the same
+stream, so a solve with graphs must be bitwise identical to one with SDPX_B200_GRAPHS=0, and
+repeated solves on one handle (graph replays) must stay bitwise identical too.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from sdpx_b200 import problems as P
+from sdpx_b200.solver import DefaultSettings, DefaultSolver
+
+pytestmark = pytest.mark.gpu
+
+
+def _make(prob, graphs):
+    old = os.environ.get("SDPX_B200_GRAPHS")
+    os.environ["SDPX_B200_GRAPHS"] = "1" if graphs else "0"
+    try:
+        return DefaultSolver(prob.P, prob.q, prob.A, prob.b, prob.cones,
+                             DefaultSettings(kkt_form="condensed"))
+    finally:
+        if old is None:
+            del os.environ["SDPX_B200_GRAPHS"]
+        else:
+            os.environ["SDPX_B200_GRAPHS"] = old
+
+
+@pytest.mark.parametrize("maker", [lambda: P.rank1_sdp(8, 200, seed=4, nmin=6, nmax=24),
+                                   lambda: P.dense_sdp(20, 60, seed=5)])
+def test_graphs_bitwise_equal_eager(maker):
+    prob = maker()
+    eager = _make(prob, False)
+    a = eager.solve()
+    g = _make(prob, True)
+    b = g.solve()
+    c = g.solve()  # second solve replays the cached graphs
+    for s in (b, c):
+        assert s.status == a.status and s.iterations == a.iterations
+        assert np.array_equal(s.x, a.x) and np.array_equal(s.z, a.z) and np.array_equal(s.s, a.s)
+
+
+def test_graphs_survive_update():
+    prob = P.rank1_sdp(6, 120, seed=8, nmin=6, nmax=20)
+    g = _make(prob, True)
+    g.solve()
+    g.update(prob.q * 1.5, prob.b)
+    s1 = g.solve()
+    eager = _make(prob, False)
+    eager.update(prob.q * 1.5, prob.b)
+    s2 = eager.solve()
+    assert s1.iterations == s2.iterations and np.array_equal(s1.x, s2.x)
