@@ -19,6 +19,7 @@ replicas (the solve does not shard): each rank solves the same instance on its o
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -153,8 +154,14 @@ def fp64_gemm_peak():
     return 2.0 * n ** 3 / best / 1e12
 
 
-def schur_model(prob):
-    """Algorithmic work of one iteration's phases (Measurement)."""
+def schur_model(prob, gram=False):
+    """Algorithmic work per launch of the timed phases (flop or bytes).
+
+    factor: m^3/3 (Cholesky of the m x m Schur complement); trinv: m^3/3 (inverse of the
+    triangular factor); assemble: sum_j 4 k_j n_j^3 + k_j^2 n_j (n_j + 1) in the ordinary form,
+    sum_j 8 n_j^3 + 3 k_j^2 in the rank-one Gram form; scale: 20 n_j^3 per block; trisolve and
+    symv: 8 m^2 bytes (two triangles, or the full matrix once).
+    """
     import numpy as np
     n = prob.n
     orders = [d for _, d in prob.cones]
@@ -166,7 +173,10 @@ def schur_model(prob):
         sub = A[r0:r0 + t, :]
         k.append(int(np.count_nonzero(sub.getnnz(axis=0))))
         r0 += t
-    assemble = sum(4.0 * kj * d ** 3 + 2.0 * kj * kj * d * (d + 1) / 2 for kj, d in zip(k, orders))
+    if gram:
+        assemble = sum(8.0 * d ** 3 + 3.0 * kj * kj for kj, d in zip(k, orders))
+    else:
+        assemble = sum(4.0 * kj * d ** 3 + 2.0 * kj * kj * d * (d + 1) / 2 for kj, d in zip(k, orders))
     return {"n": n, "factor_flops": n ** 3 / 3.0, "trisolve_bytes": 8.0 * n * n,
             "symv_bytes": 8.0 * n * n, "assemble_flops": assemble,
             "scale_flops": sum(20.0 * d ** 3 for d in orders)}
@@ -263,9 +273,13 @@ def run_ours(args, world, rank, local):
     # ---- end-to-end through the C ABI with host buffers ----
     e2e_times = []
     h2d = d2h = 0
+    lib = _lib.load()
+    cnt_h2d, cnt_d2h = ctypes.c_uint64(), ctypes.c_uint64()
     for i in range(args.warmup + args.steps):
         barrier(world)
         torch.cuda.synchronize()
+        lib.sdpx_b200_transfer_bytes(ctypes.byref(cnt_h2d), ctypes.byref(cnt_d2h))
+        b0 = (cnt_h2d.value, cnt_d2h.value)
         t0 = time.perf_counter()
         s2 = DefaultSolver(prob.P, prob.q, prob.A, prob.b, prob.cones, settings)
         s2.solve()
@@ -273,21 +287,10 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         if i >= args.warmup:
             e2e_times.append(time.perf_counter() - t0)
+            lib.sdpx_b200_transfer_bytes(ctypes.byref(cnt_h2d), ctypes.byref(cnt_d2h))
+            h2d, d2h = cnt_h2d.value - b0[0], cnt_d2h.value - b0[1]  # bytes the library copied
     e2e = max_over_ranks(world, statistics.mean(e2e_times))
-    # bytes crossing per step: the uploaded problem (dense per-block columns of A, index maps,
-    # q, b) and the result vector
-    model = schur_model(prob)
-    nnz_dense = sum(d * (d + 1) // 2 for _, d in prob.cones)
-    A = prob.A.tocsc()
-    h2d = int(8 * A.nnz + 4 * 3 * A.nnz // max(nnz_dense, 1) + 8 * (prob.n + prob.m))
-    dense_cols = 0
-    r0 = 0
-    for _, d in prob.cones:
-        t = d * (d + 1) // 2
-        dense_cols += t * int(np.count_nonzero(A[r0:r0 + t, :].getnnz(axis=0)))
-        r0 += t
-    h2d = int(8 * dense_cols + 8 * (prob.n + prob.m) + 16 * prob.n * 4)
-    d2h = int(8 * (prob.n + 2 * prob.m + 6))
+    model = schur_model(prob, gram=solver.schur_forms()["ordinary"] == 0)
 
     # ---- roofline of the dominant device phase ----
     hbm, hbm_kind = measured_peaks()
@@ -295,10 +298,10 @@ def run_ours(args, world, rank, local):
     ms, cnt = ktimes[dom]
     per = ms / 1e3 / max(cnt, 1)
     fp64 = None
-    if dom in ("factor", "assemble", "scale", "cone", "step"):
+    if dom in ("factor", "trinv", "assemble", "scale", "cone", "step"):
         fp64 = fp64_gemm_peak()
-        flops = {"factor": model["factor_flops"], "assemble": model["assemble_flops"],
-                 "scale": model["scale_flops"]}.get(dom)
+        flops = {"factor": model["factor_flops"], "trinv": model["factor_flops"],
+                 "assemble": model["assemble_flops"], "scale": model["scale_flops"]}.get(dom)
         if flops is None:
             flops = sum(4.0 * d ** 3 for _, d in prob.cones)
         achieved = flops / per / 1e12

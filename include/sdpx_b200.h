@@ -121,13 +121,17 @@ int32_t sdpx_destroy(sdpx_handle *handle);
 int32_t sdpx_b200_phase_times(sdpx_handle *handle, double *times, uint64_t *counts);
 /* Enable (on != 0) or disable CUDA-event timing of the device phases of later solves and reset
  * the totals.  Events are recorded on the handle's stream around each phase: NT scaling,
- * Schur assembly, factorisation, triangular solves, cone congruences, step lengths and the
- * Schur matvec, in that order (no counterpart in the reference, which has no device). */
+ * Schur assembly, factorisation, triangular solves, cone congruences, step lengths, the
+ * Schur matvec and the inverse of the factor, in that order (no counterpart in the reference, which has no device). */
 int32_t sdpx_b200_set_kernel_timing(sdpx_handle *handle, int32_t on);
-/* Totals since the last reset: ms[7] milliseconds and counts[7] timed regions per phase. */
+/* Totals since the last reset: ms[8] milliseconds and counts[8] timed regions per phase (the
+ * seven above, then the explicit inverse of the factor). */
 int32_t sdpx_b200_kernel_times(sdpx_handle *handle, double *ms, uint64_t *counts);
 /* Number of CUDA kernels this library has launched in this process (all handles). */
 uint64_t sdpx_b200_launch_count(void);
+/* Bytes this library has copied host-to-device and device-to-host in this process (all
+ * handles): the host-device traffic of prepare, solve and result reads. */
+int32_t sdpx_b200_transfer_bytes(uint64_t *h2d, uint64_t *d2h);
 /* Schur forms chosen at prepare: PSD blocks whose every constraint column is rank one
  * (sigma u u', stored as the factor U and used in the Gram form S = (sigma sigma') o (U' Ginv U)^2,
  * like the reference's sampled Gram update, sampled/mod.rs:1973-2025) and blocks kept in the

@@ -581,6 +581,14 @@ int32_t sdpx_destroy(sdpx_handle* h) {
 
 uint64_t sdpx_b200_launch_count(void) { return sdpxg::g_launches; }
 
+int32_t sdpx_b200_transfer_bytes(uint64_t* h2d, uint64_t* d2h) {
+  return boundary([&] {
+    if (!h2d || !d2h) invalid("null pointer");
+    *h2d = sdpxg::g_h2d_bytes;
+    *d2h = sdpxg::g_d2h_bytes;
+  });
+}
+
 int32_t sdpx_b200_set_kernel_timing(sdpx_handle* h, int32_t on) {
   return boundary([&] {
     operate(h, [&](sdpx_handle& hh) {

@@ -19,6 +19,22 @@ inline void check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Bytes this library copied between host and device in this process (all handles): the
+// end-to-end traffic of a solve, read through sdpx_b200_transfer_bytes.
+inline uint64_t g_h2d_bytes = 0, g_d2h_bytes = 0;
+
+inline void copy_h2d(void* d, const void* h, size_t bytes, cudaStream_t st) {
+  if (!bytes) return;
+  check(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st), "H2D");
+  g_h2d_bytes += bytes;
+}
+
+inline void copy_d2h(void* h, const void* d, size_t bytes, cudaStream_t st) {
+  if (!bytes) return;
+  check(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, st), "D2H");
+  g_d2h_bytes += bytes;
+}
+
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
@@ -44,7 +60,7 @@ struct DevBuf {
     n = 0;
   }
   void upload(const T* h, size_t count, cudaStream_t st) {
-    if (count) check(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, st), "H2D");
+    copy_h2d(p, h, count * sizeof(T), st);
   }
   void upload(const std::vector<T>& h, cudaStream_t st) {
     if (h.size() > n) alloc(h.size());
@@ -159,8 +175,7 @@ class Reducer {
       ++g_launches, k_reduce_final<<<1, 32, 0, st>>>(op, kBlocks, partial_.p + (size_t)s * kBlocks, slots_.p + s);
     } else {
       double id = (op == RED_FINITE) ? 1.0 : 0.0;
-      check(cudaMemcpyAsync(slots_.p + s, &id_[op], sizeof(double), cudaMemcpyHostToDevice, st),
-            "reducer identity");
+      copy_h2d(slots_.p + s, &id_[op], sizeof(double), st);
       (void)id;
     }
     return s;
@@ -170,8 +185,7 @@ class Reducer {
   void set_count(int c) { count_ = c; }
   const PinnedBuf<double>& fetch(cudaStream_t st) {
     if (count_) {
-      check(cudaMemcpyAsync(host_.p, slots_.p, count_ * sizeof(double),
-                            cudaMemcpyDeviceToHost, st), "reducer D2H");
+      copy_d2h(host_.p, slots_.p, count_ * sizeof(double), st);
     }
     check(cudaStreamSynchronize(st), "reducer sync");
     count_ = 0;

@@ -158,7 +158,8 @@ inline void need(const void* p, const char* what) {
 }
 
 // Kernel-phase timers: CUDA events recorded on the engine's stream around each phase.
-enum KernelPhase { KT_SCALE = 0, KT_ASSEMBLE, KT_FACTOR, KT_TRISOLVE, KT_CONE, KT_STEP, KT_SYMV, KT_N };
+enum KernelPhase { KT_SCALE = 0, KT_ASSEMBLE, KT_FACTOR, KT_TRISOLVE, KT_CONE, KT_STEP, KT_SYMV, KT_TRINV,
+                   KT_N };
 
 class Engine {
  public:
@@ -542,7 +543,7 @@ class Engine {
   // ---- status word ----
   void clear_status() { check(cudaMemsetAsync(status_.p, 0, sizeof(uint32_t), st), "memset"); }
   uint32_t read_status() {
-    check(cudaMemcpyAsync(hstat_.p, status_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "status");
+    copy_d2h(hstat_.p, status_.p, sizeof(uint32_t), st);
     check(cudaStreamSynchronize(st), "status sync");
     return hstat_[0];
   }
@@ -611,8 +612,7 @@ class Engine {
     launched("k_step_length");
     tend(KT_STEP);
     const PinnedBuf<double>& h = hblk_;
-    check(cudaMemcpyAsync(hblk_.p, step_out_.p, 2 * nblk * sizeof(double),
-                          cudaMemcpyDeviceToHost, st), "step D2H");
+    copy_d2h(hblk_.p, step_out_.p, 2 * nblk * sizeof(double), st);
     uint32_t s = read_status();
     for (int j = 0; j < nblk; ++j) {
       *az = std::min(*az, h[2 * j]);
@@ -628,8 +628,7 @@ class Engine {
     clear_status();
     ++g_launches, k_margins<<<dim3(nblk, 1), SDPXG_CONE_THREADS, kSmemMarg, st>>>(blocks_, v, m, marg_out_, status_);
     launched("k_margins");
-    check(cudaMemcpyAsync(hblk_.p, marg_out_.p, 2 * nblk * sizeof(double),
-                          cudaMemcpyDeviceToHost, st), "margins D2H");
+    copy_d2h(hblk_.p, marg_out_.p, 2 * nblk * sizeof(double), st);
     const bool ok = read_status() == 0;
     for (int j = 0; j < 2 * nblk; ++j) out[j] = hblk_[j];
     return ok;
@@ -723,7 +722,7 @@ class Engine {
   double schur_diag_absmax() {
     if (!n) return 0.0;
     ++g_launches, k_diag_absmax<<<1, 1024, 0, st>>>(Hsave_, n, scal_);
-    check(cudaMemcpyAsync(hblk_.p, scal_.p, sizeof(double), cudaMemcpyDeviceToHost, st), "diag D2H");
+    copy_d2h(hblk_.p, scal_.p, sizeof(double), st);
     check(cudaStreamSynchronize(st), "diag sync");
     return hblk_[0];
   }
@@ -731,11 +730,12 @@ class Engine {
   bool factor(double eps, bool dynamic, double dyn_eps, double dyn_delta) {
     if (!n) return true;
     clear_status();
-    tbegin(KT_FACTOR);
     ++g_launches, k_shifted_copy<<<1184, 256, 0, st>>>(Hsave_, F_, n, eps, diag0_);
-    if (df_items_ > 0) {  // one persistent launch over the whole tile schedule
+    if (df_items_ > 0)
       check(cudaMemsetAsync(df_sync_.p, 0, (2 + 2 * (size_t)nchol * nchol) * sizeof(int), st),
             "dataflow sync reset");
+    tbegin(KT_FACTOR);
+    if (df_items_ > 0) {  // one persistent launch over the whole tile schedule
       ++g_launches, k_chol_dataflow<<<df_grid_, 256, kSmemDf, st>>>(
           F_, n, nchol, df_list_, df_items_, df_sync_, dyn_eps, dyn_delta, dynamic ? 1 : 0, diag0_,
           Dinv_, status_);
@@ -750,10 +750,12 @@ class Engine {
       }
     }
     launched("factor");
+    tend(KT_FACTOR);
     uint32_t s = read_status();
     if (s & SDPXG_ST_SYNC_TIMEOUT) throw CudaError("factorization: a bounded inter-CTA wait gave up");
     factor_ok_ = (s == 0);
     if (factor_ok_) {
+      tbegin(KT_TRINV);
       // explicit inverse of the factor: diagonal tiles, then one batched GEMM pair per level
       ++g_launches, k_trtri_diag<<<nchol, SDPXG_THREADS, 0, st>>>(n, Dinv_, Uinv_, UinvT_);
       for (int level = 1; (1 << (level - 1)) < nchol; ++level) {
@@ -764,8 +766,8 @@ class Engine {
               F_, Uinv_, UinvT_, Tmp_, n, level, phase);
       }
       launched("trinv");
+      tend(KT_TRINV);
     }
-    tend(KT_FACTOR);
     return factor_ok_;
   }
   // x = F^-1 r = U^-1 (U^-T r) through the explicit inverse: two coalesced GEMVs.

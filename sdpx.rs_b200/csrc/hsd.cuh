@@ -845,9 +845,9 @@ inline void HsdSolver::solve() {
   hx.resize(n);
   hs.resize(m);
   hz.resize(m);
-  check(cudaMemcpyAsync(hx.data(), x_.p, n * sizeof(double), cudaMemcpyDeviceToHost, st()), "x D2H");
-  check(cudaMemcpyAsync(hs.data(), s_.p, m * sizeof(double), cudaMemcpyDeviceToHost, st()), "s D2H");
-  check(cudaMemcpyAsync(hz.data(), z_.p, m * sizeof(double), cudaMemcpyDeviceToHost, st()), "z D2H");
+  copy_d2h(hx.data(), x_.p, n * sizeof(double), st());
+  copy_d2h(hs.data(), s_.p, m * sizeof(double), st());
+  copy_d2h(hz.data(), z_.p, m * sizeof(double), st());
   check(cudaStreamSynchronize(st()), "result sync");
   const double tinv = 1.0 / tau_;
   for (int i = 0; i < n; ++i) hx[i] = hx[i] * eq_.d[i] * tinv;

@@ -188,14 +188,14 @@ class DefaultSolver:
                                                "inner_refinements"], counts.tolist())))
         return self.solution
 
-    KERNEL_PHASES = ["scale", "assemble", "factor", "trisolve", "cone", "step", "symv"]
+    KERNEL_PHASES = ["scale", "assemble", "factor", "trisolve", "cone", "step", "symv", "trinv"]
 
     def set_kernel_timing(self, on: bool):
         _lib.call("sdpx_b200_set_kernel_timing", self._h, int(bool(on)))
 
     def kernel_times(self) -> dict:
-        ms = np.zeros(7)
-        cnt = np.zeros(7, dtype=np.uint64)
+        ms = np.zeros(len(self.KERNEL_PHASES))
+        cnt = np.zeros(len(self.KERNEL_PHASES), dtype=np.uint64)
         _lib.call("sdpx_b200_kernel_times", self._h, dptr(ms), cnt.ctypes.data_as(_lib.PU64))
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.KERNEL_PHASES)}
 
