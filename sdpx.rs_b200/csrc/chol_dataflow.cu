@@ -19,7 +19,8 @@
 //  * all tile products run on the FP64 tensor cores (mma.sync m8n8k4 f64) from shared-memory
 //    tiles staged through L2 (the 2000 x 2000 matrix stays L2-resident);
 //  * the diagonal tile is factored in 8 x 8 panels: one warp factors the panel's diagonal
-//    block with the dynamic pivot rule and inverts it in registers (shuffles), the other
+//    block with the dynamic pivot rule and inverts it in registers (each lane redundantly,
+//    so the 64-pivot chain carries no shuffles), the other
 //    warps apply it to the panel row and update the trailing blocks with DMMA; the tile's
 //    inverse U_kk^-1 (used by TRSM and by the explicit inverse of the factor) is formed by
 //    block back-substitution, one warp per block column.
@@ -94,15 +95,16 @@ __device__ __forceinline__ void df_atb(const double* As, const double* Bs, doubl
 }
 
 // Dynamic pivot rule of the reduced KKT factorization: a pivot within eps of zero becomes
-// delta unless it is clearly negative; non-finite or non-positive pivots fail.
-__device__ __forceinline__ double df_pivot(double d, double diag, int nb, double eps, double delta,
-                                           int dynamic, bool& fail) {
+// delta unless it is clearly negative; non-finite or non-positive pivots fail.  The original
+// diagonal (shared memory) is read only on the rare small-pivot branch, off the common path.
+__device__ __forceinline__ double df_pivot(double d, const double* diag, int nb, double eps,
+                                           double delta, int dynamic, bool& fail) {
   if (!isfinite(d)) {
     fail = true;
     return 1.0;
   }
   if (dynamic && d <= eps) {
-    if (d < -64.0 * 2.220446049250313e-16 * nb * fabs(diag)) fail = true;
+    if (d < -64.0 * 2.220446049250313e-16 * nb * fabs(*diag)) fail = true;
     else d = delta;
   }
   if (!(d > 0.0)) {
@@ -115,52 +117,57 @@ __device__ __forceinline__ double df_pivot(double d, double diag, int nb, double
 // Factor the diagonal tile in A (upper triangle valid, lower zero, padded diagonal 1) in
 // place: A <- U.  X <- U^-1 (upper).  Wd: 8 x (8 x 8) inverse diagonal blocks; Sc: 8 x 64
 // scratch.  Returns true when every pivot was accepted (CTA uniform).
-__device__ bool df_potrf_tile(double* A, double* X, double* Wd, double* Sc, int nb, int g0,
-                              const double* __restrict__ diag0, double eps, double delta,
-                              int dynamic, int* s_fail) {
+__device__ bool df_potrf_tile(double* A, double* X, double* Wd, double* Sc, int nb,
+                              const double* sdiag, double eps, double delta, int dynamic,
+                              int* s_fail) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, q = lane & 3, r = lane >> 2;
   for (int p = 0; p < 8; ++p) {
     if (w == 0) {
-      // lane c < 8 owns column c of the 8 x 8 diagonal block (rows 0..c)
+      // Every lane factors the whole 8 x 8 diagonal block in registers (packed upper triangle,
+      // static indices, no shuffles on the pivot chain); lane c < 8 then writes column c of
+      // U_pp and of W = U_pp^-1.  One rsqrt per pivot: 1/sqrt(d) and sqrt(d) = d / sqrt(d).
       const int c = lane & 7;
       const bool own = lane < 8;
-      double a[8], rd[8];
+      double u[36], rd[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) a[i] = (own && i <= c) ? DFS(A, 8 * p + i, 8 * p + c) : 0.0;
+      for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int i = 0; i <= j; ++i) u[j * (j + 1) / 2 + i] = DFS(A, 8 * p + i, 8 * p + j);
       bool fail = false;
 #pragma unroll
       for (int kk = 0; kk < 8; ++kk) {
-        double d = __shfl_sync(0xffffffffu, a[kk], kk);
-        const int row = 8 * p + kk;
-        if (row < nb) d = df_pivot(d, diag0[g0 + row], nb, eps, delta, dynamic, fail);
-        const double rt = sqrt(d), ri = 1.0 / rt;
+        double d = u[kk * (kk + 3) / 2];
+        if (8 * p + kk < nb) d = df_pivot(d, sdiag + 8 * p + kk, nb, eps, delta, dynamic, fail);
+        const double ri = rsqrt(d);
         rd[kk] = ri;
-        if (c == kk) a[kk] = rt;
-        else if (c > kk) a[kk] *= ri;  // U[kk][c]
+        u[kk * (kk + 3) / 2] = d * ri;
 #pragma unroll
-        for (int i = kk + 1; i < 8; ++i) {
-          const double u = __shfl_sync(0xffffffffu, a[kk], i);  // U[kk][i]
-          if (c >= i) a[i] -= u * a[kk];
-        }
+        for (int j = kk + 1; j < 8; ++j) u[j * (j + 1) / 2 + kk] *= ri;  // row kk of U
+#pragma unroll
+        for (int j = kk + 1; j < 8; ++j)
+#pragma unroll
+          for (int i = kk + 1; i <= j; ++i)
+            u[j * (j + 1) / 2 + i] -= u[i * (i + 1) / 2 + kk] * u[j * (j + 1) / 2 + kk];
       }
       if (fail && lane == 0) *s_fail = 1;
-      if (own) {
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-          if (i <= c) DFS(A, 8 * p + i, 8 * p + c) = a[i];
-      }
       // column c of W = U_pp^-1: w_c = 1/U_cc, w_i = -(sum_{l>i} U_il w_l) / U_ii for i < c
       double wv[8];
 #pragma unroll
       for (int l = 0; l < 8; ++l) wv[l] = (l == c) ? rd[l] : 0.0;
 #pragma unroll
       for (int i = 6; i >= 0; --i) {
-        double s = 0.0;
+        double sacc = 0.0;
 #pragma unroll
-        for (int l = i + 1; l < 8; ++l) s += __shfl_sync(0xffffffffu, a[i], l) * wv[l];
-        if (i < c) wv[i] = -s * rd[i];
+        for (int l = i + 1; l < 8; ++l) sacc = fma(u[l * (l + 1) / 2 + i], wv[l], sacc);
+        if (i < c) wv[i] = -sacc * rd[i];
       }
       if (own) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (j == c) {
+#pragma unroll
+            for (int i = 0; i <= j; ++i) DFS(A, 8 * p + i, 8 * p + j) = u[j * (j + 1) / 2 + i];
+          }
 #pragma unroll
         for (int i = 0; i < 8; ++i) Wd[p * 64 + i + 8 * c] = wv[i];  // column-major 8 x 8
       }
@@ -248,6 +255,7 @@ k_chol_dataflow(double* __restrict__ F, int m, int nt, const unsigned* __restric
   double* Wd = Bs + DF_NB * DF_LD;
   double* Sc = Wd + 8 * 64;
   __shared__ int s_item, s_go, s_fail;
+  __shared__ double s_diag[DF_NB];  // original diagonal of the tile being factored
   int* ticket = sync;
   int* err = sync + 1;
   int* upd = sync + 2;
@@ -290,6 +298,7 @@ k_chol_dataflow(double* __restrict__ F, int m, int nt, const unsigned* __restric
       const int nb = min(DF_NB, m - k0);
       // upper triangle of the tile, lower zero, padded diagonal 1
       df_load_tile(As, F + k0 + (long)k0 * m, m, nb, nb, vec2);
+      for (int e = threadIdx.x; e < DF_NB; e += DF_THREADS) s_diag[e] = (e < nb) ? diag0[k0 + e] : 1.0;
       __syncthreads();
       for (int e = threadIdx.x; e < DF_NB * DF_NB; e += DF_THREADS) {
         const int rr = e & 63, cc = e >> 6;
@@ -298,7 +307,7 @@ k_chol_dataflow(double* __restrict__ F, int m, int nt, const unsigned* __restric
         DFS(Bs, rr, cc) = 0.0;
       }
       __syncthreads();
-      const bool ok = df_potrf_tile(As, Bs, Wd, Sc, nb, k0, diag0, eps, delta, dynamic, &s_fail);
+      const bool ok = df_potrf_tile(As, Bs, Wd, Sc, nb, s_diag, eps, delta, dynamic, &s_fail);
       double* D = Dinv + (long)k * DF_NB * DF_NB;
       for (int e = threadIdx.x; e < DF_NB * DF_NB; e += DF_THREADS) {
         const int rr = e & 63, cc = e >> 6;

@@ -16,6 +16,7 @@
 
 #define CH_NB 64
 #define CH_LD (CH_NB + 1)
+#define TI_LD 68  // k_trinv_level tiles (4 mod 16)
 
 // F = Hsave + eps I (copy), diag0 = diag(F).
 extern "C" __global__ void k_shifted_copy(const double* __restrict__ Hs, double* __restrict__ F,
@@ -38,11 +39,11 @@ extern "C" __global__ void k_shifted_copy(const double* __restrict__ Hs, double*
 // handling, dense_block.rs): a pivot within eps of zero becomes delta, a clearly negative or
 // non-finite one fails.  Written once by the thread that finished the pivot entry:
 // info = {1/d, sqrt(d), 1/sqrt(d)}, all 0 on failure (sqrt of an accepted pivot is > 0).
-__device__ __forceinline__ void potrf_pivot(double d, double diag, int nb, double eps,
+__device__ __forceinline__ void potrf_pivot(double d, const double* diag, int nb, double eps,
                                             double delta, int dynamic, double* info) {
   bool fail = !isfinite(d);
   if (!fail && dynamic && d <= eps) {
-    if (d < -64.0 * 2.220446049250313e-16 * nb * fabs(diag)) fail = true;
+    if (d < -64.0 * 2.220446049250313e-16 * nb * fabs(*diag)) fail = true;
     else d = delta;
   }
   if (!fail && !(d > 0.0)) fail = true;
@@ -88,7 +89,7 @@ k_potrf_diag(double* __restrict__ H, int m, int kb, double eps, double delta, in
       if (i == 0) mrowbuf[0][j] = (j == 0) ? 1.0 : 0.0;
     }
   if (threadIdx.x == 0 && nb > 0) {
-    potrf_pivot(a[0][0], diag0[k0], nb, eps, delta, dynamic, pinfo[0]);
+    potrf_pivot(a[0][0], diag0 + k0, nb, eps, delta, dynamic, pinfo[0]);
     root[0] = pinfo[0][1];
   }
   for (int k = 0; k < nb; ++k) {
@@ -115,7 +116,7 @@ k_potrf_diag(double* __restrict__ H, int m, int kb, double eps, double delta, in
             if (i == k + 1) {
               next[j] = a[p][q];
               if (j == k + 1) {  // pivot k + 1 is final: publish its record for the next step
-                potrf_pivot(a[p][q], diag0[k0 + k + 1], nb, eps, delta, dynamic,
+                potrf_pivot(a[p][q], diag0 + k0 + k + 1, nb, eps, delta, dynamic,
                             pinfo[(k + 1) & 1]);
                 root[k + 1] = pinfo[(k + 1) & 1][1];
               }
@@ -266,8 +267,8 @@ extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
 k_trinv_level(const double* __restrict__ F, double* __restrict__ Uinv, double* __restrict__ UinvT,
               double* __restrict__ Tmp, int n, int level, int phase) {
   extern __shared__ double tl_sm[];
-  double* As = tl_sm;               // [r + k * CH_LD]
-  double* Bs = As + CH_NB * CH_LD;  // [k + c * CH_LD]
+  double* As = tl_sm;               // [r + k * TI_LD]
+  double* Bs = As + CH_NB * TI_LD;  // [k + c * TI_LD]
   const int g = 1 << level, h = g >> 1;
   const int L0 = blockIdx.z * g * CH_NB;
   const int R0 = L0 + h * CH_NB;
@@ -288,49 +289,45 @@ k_trinv_level(const double* __restrict__ F, double* __restrict__ Uinv, double* _
   int kbeg = 0, kend = K;
   if (phase == 0) kend = min(K, (tn + 1) * CH_NB);
   else kbeg = tm * CH_NB;
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  double acc[4][4];
+  // FP64 tensor cores: warp w owns the 8-column block w of the 64 x 64 output tile, eight
+  // 8 x 8 accumulators; shared tiles with leading dimension TI_LD (4 mod 16: conflict-free
+  // fragment reads).  Fragments: lane l holds A[l/4][l%4], B[l%4][l/4], C[l/4][2(l%4)+{0,1}].
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, q = lane & 3, rr = lane >> 2;
+  double acc[8][2];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int R = 0; R < 8; ++R) acc[R][0] = acc[R][1] = 0.0;
   for (int k0 = kbeg; k0 < kend; k0 += CH_NB) {
     __syncthreads();
     for (int e = threadIdx.x; e < CH_NB * CH_NB; e += blockDim.x) {
       int r = e % CH_NB, k = e / CH_NB;
       int gr = ar + tm * CH_NB + r, gc = ac + k0 + k;
       bool in = (tm * CH_NB + r < Ln) && (k0 + k < K) && !(phase == 1 && gr > gc);
-      As[r + k * CH_LD] = in ? A[gr + (long)gc * n] : 0.0;
+      As[r + k * TI_LD] = in ? A[gr + (long)gc * n] : 0.0;
       int hr = br + k0 + r, hc = bc + tn * CH_NB + k;
       bool inb = (k0 + r < K) && (tn * CH_NB + k < Rn) && !(phase == 0 && hr > hc);
-      Bs[r + k * CH_LD] = inb ? B[hr + (long)hc * n] : 0.0;
+      Bs[r + k * TI_LD] = inb ? B[hr + (long)hc * n] : 0.0;
     }
     __syncthreads();
 #pragma unroll 4
-    for (int k = 0; k < CH_NB; ++k) {
-      double x[4], y[4];
+    for (int ks = 0; ks < CH_NB / 4; ++ks) {
+      const int kk = ks * 4 + q;
+      const double b = Bs[kk + (8 * w + rr) * TI_LD];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) x[a] = As[(tx + 16 * a) + k * CH_LD];
-#pragma unroll
-      for (int b = 0; b < 4; ++b) y[b] = Bs[k + (ty + 16 * b) * CH_LD];
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(x[a], y[b], acc[a][b]);
+      for (int R = 0; R < 8; ++R) dmma_m8n8k4(acc[R][0], acc[R][1], As[(8 * R + rr) + kk * TI_LD], b);
     }
   }
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int R = 0; R < 8; ++R)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      int r = tm * CH_NB + tx + 16 * a, c = tn * CH_NB + ty + 16 * b;
+    for (int e = 0; e < 2; ++e) {
+      int r = tm * CH_NB + 8 * R + rr, c = tn * CH_NB + 8 * w + 2 * q + e;
       if (r >= Ln || c >= Rn) continue;
       long gr = L0 + r, gc = R0 + c;
       if (phase == 0) {
-        Tmp[gr + gc * n] = acc[a][b];
+        Tmp[gr + gc * n] = acc[R][e];
       } else {
-        Uinv[gr + gc * n] = -acc[a][b];
-        UinvT[gc + gr * n] = -acc[a][b];
+        Uinv[gr + gc * n] = -acc[R][e];
+        UinvT[gc + gr * n] = -acc[R][e];
       }
     }
 }

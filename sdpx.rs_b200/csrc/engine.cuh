@@ -36,6 +36,7 @@ constexpr size_t kSmemTrans = 3 * kMatD * sizeof(double);
 constexpr size_t kSmemTrsm = 2 * 64 * 65 * sizeof(double);
 constexpr size_t kSmemSyrk = 2 * 64 * 66 * sizeof(double);
 constexpr size_t kSmemTrtri = 2 * 64 * 65 * sizeof(double);
+constexpr size_t kSmemTrinv = 2 * 64 * 68 * sizeof(double);  // k_trinv_level (TI_LD 68)
 constexpr size_t kSmemDf = (2 * 64 * 68 + 2 * 8 * 64) * sizeof(double);  // k_chol_dataflow
 constexpr size_t kSmemGram = 3 * kMatD * sizeof(double);                 // k_gram_basis/adjoint
 constexpr int kDfMaxTiles = 256;  // dataflow schedule up to m = 16384 (nt^3/6 items)
@@ -262,7 +263,7 @@ class Engine {
     set_smem(reinterpret_cast<const void*>(k_schur_transform), kSmemTrans);
     set_smem(reinterpret_cast<const void*>(k_trsm_panel), kSmemTrsm);
     set_smem(reinterpret_cast<const void*>(k_syrk_update), kSmemSyrk);
-    set_smem(reinterpret_cast<const void*>(k_trinv_level), kSmemTrtri);
+    set_smem(reinterpret_cast<const void*>(k_trinv_level), kSmemTrinv);
     set_smem(reinterpret_cast<const void*>(k_potrf_diag), kSmemTrtri);
     set_smem(reinterpret_cast<const void*>(k_chol_dataflow), kSmemDf);
     set_smem(reinterpret_cast<const void*>(k_gram_basis), kSmemGram);
@@ -762,7 +763,7 @@ class Engine {
         const int g = 1 << level, h = g >> 1;
         dim3 grid(h, h, (nchol + g - 1) / g);
         for (int phase = 0; phase < 2; ++phase)
-          ++g_launches, k_trinv_level<<<grid, SDPXG_THREADS, kSmemTrtri, st>>>(
+          ++g_launches, k_trinv_level<<<grid, SDPXG_THREADS, kSmemTrinv, st>>>(
               F_, Uinv_, UinvT_, Tmp_, n, level, phase);
       }
       launched("trinv");
