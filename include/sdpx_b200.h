@@ -173,7 +173,7 @@ int32_t sdpxg_solve_many(sdpxg_ctx *ctx, const double *rhs, double *out, uint32_
  * host that owns all device memory through its own pool, or a latency-bound loop where a
  * cudaMalloc could synchronise the device): d_rhs and d_out are DEVICE pointers to n x ncols
  * column-major arrays, and all per-call scratch sits in one static device array of the library
- * (about 0.7 MB on every GPU that loads it).  It calls no cudaMalloc or cudaFree.  n above 4096
+ * (about 0.17 MB on every GPU that loads it).  It calls no cudaMalloc or cudaFree.  n above 4096
  * returns 2.  The first call on a device looks up the array's address: make it before any
  * stream capture.  Calls that overlap on the GPU share the array and race. */
 int32_t sdpxg_solve_noalloc(sdpxg_ctx *ctx, const double *d_rhs, double *d_out, uint32_t ncols);

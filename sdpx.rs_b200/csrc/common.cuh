@@ -75,17 +75,23 @@ __device__ __forceinline__ void cta_zero_mat(double* M) {
   for (int e = threadIdx.x; e < SDPXG_LD * SDPXG_NMAX; e += blockDim.x) M[e] = 0.0;
 }
 
-// M = smat(v): symmetric matrix from an svec (zero padded to 64 x 64).
+// M = smat(v): symmetric matrix from an svec (zero padded to 64 x 64).  Column j of the upper
+// triangle is contiguous in the svec (v[j(j+1)/2 + i], i <= j): one warp per column reads it
+// coalesced and writes both triangles.
 __device__ __forceinline__ void cta_load_smat(double* M, const double* __restrict__ v, int n) {
   for (int e = threadIdx.x; e < SDPXG_NMAX * SDPXG_NMAX; e += blockDim.x) {
-    int i = e % SDPXG_NMAX, j = e / SDPXG_NMAX;
-    double x = 0.0;
-    if (i < n && j < n) {
-      int a = min(i, j), b = max(i, j);
-      x = v[tri_idx(a, b)];
+    const int i = e % SDPXG_NMAX, j = e / SDPXG_NMAX;
+    if (i >= n || j >= n) SM(M, i, j) = 0.0;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int j = warp; j < n; j += nwarps) {
+    const double* col = v + j * (j + 1) / 2;
+    for (int i = lane; i <= j; i += 32) {
+      double x = col[i];
       if (i != j) x *= SDPXG_RSQRT2;
+      SM(M, i, j) = x;
+      SM(M, j, i) = x;
     }
-    SM(M, i, j) = x;
   }
 }
 

@@ -336,41 +336,96 @@ k_trinv_level(const double* __restrict__ F, double* __restrict__ Uinv, double* _
 // (lower), times v.  One warp per column: coalesced column reads.
 extern "C" __global__ void k_tri_colgemv(const double* __restrict__ A, int n, int lower,
                                          const double* __restrict__ v, double* __restrict__ out) {
+  // one warp per column, eight independent partial sums per lane so that each lane keeps eight
+  // loads in flight (the matrix streams from HBM/L2 once per solve)
   const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (c >= n) return;
   const int r0 = lower ? c : 0, r1 = lower ? n : c + 1;
   const double* col = A + (long)c * n;
-  double acc = 0.0;
-  for (int r = r0 + lane; r < r1; r += 32) acc = fma(col[r], v[r], acc);
-  acc = warp_sum(acc);
-  if (lane == 0) out[c] = acc;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int r = r0 + lane;
+  for (; r + 7 * 32 < r1; r += 8 * 32) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc[u] = fma(__ldg(col + r + 32 * u), __ldg(v + r + 32 * u), acc[u]);
+  }
+  for (; r < r1; r += 32) acc[0] = fma(col[r], v[r], acc[0]);
+  double t = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+  t = warp_sum(t);
+  if (lane == 0) out[c] = t;
 }
 
-// Partial sums of e = r - H x over column chunks: part[s][i] for chunk s.
-#define SYMV_SPLIT 16
-extern "C" __global__ void k_symv_partial(const double* __restrict__ Hs, int m,
-                                          const double* __restrict__ x, long ldx,
-                                          double* __restrict__ part, long ldp) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int s = blockIdx.y;
-  const int c = blockIdx.z;
-  if (i >= m) return;
-  const int chunk = (m + SYMV_SPLIT - 1) / SYMV_SPLIT;
-  const int k0 = s * chunk, k1 = min(m, k0 + chunk);
-  const double* xc = x + c * ldx;
-  double acc = 0.0;
-  for (int k = k0; k < k1; ++k) acc = fma(Hs[i + (long)k * m], xc[k], acc);
-  part[(long)c * ldp + (long)s * m + i] = acc;
+// out[c] = rbase[c] + alpha * (column c of A) . v for a dense column-major n x n A restricted to
+// a triangle (tri 0: all rows, 1: rows <= c, 2: rows >= c; other entries are never read).  One
+// warp per (column, 256-row segment), eight loads in flight per lane, so every warp finishes in
+// one memory round trip whatever the column length; the segment sums go to partial[seg][c] and
+// the warp that finishes a column last (a ticket per column, reset for the next use) adds them
+// in increasing segment order -- the result does not depend on the order the warps ran in.
+#define CD_SEG 256
+__device__ __forceinline__ void cd_seg_range(int tri, int c, int n, int& s0, int& s1) {
+  const int nseg = (n + CD_SEG - 1) / CD_SEG;
+  s0 = 0;
+  s1 = nseg;
+  if (tri == 1) s1 = c / CD_SEG + 1;  // rows 0..c
+  if (tri == 2) s0 = c / CD_SEG;      // rows c..n-1
 }
 
-extern "C" __global__ void k_symv_finish(int m, const double* __restrict__ part, long ldp,
-                                         const double* __restrict__ r, long ldr,
-                                         double* __restrict__ e, long lde) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int c = blockIdx.y;
-  if (i >= m) return;
-  double acc = 0.0;
-  for (int s = 0; s < SYMV_SPLIT; ++s) acc += part[(long)c * ldp + (long)s * m + i];
-  e[c * lde + i] = r[c * ldr + i] - acc;
+extern "C" __global__ void __launch_bounds__(256)
+k_coldot_seg(const double* __restrict__ A, int n, int tri, const double* __restrict__ v,
+             const double* __restrict__ rbase, double alpha, double* __restrict__ out,
+             double* __restrict__ partial, unsigned* __restrict__ counters) {
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31, sg = blockIdx.y;
+  if (c >= n) return;
+  int s0, s1;
+  cd_seg_range(tri, c, n, s0, s1);
+  if (sg < s0 || sg >= s1) return;
+  int r0 = sg * CD_SEG, r1 = min(n, r0 + CD_SEG);
+  if (tri == 1) r1 = min(r1, c + 1);
+  if (tri == 2) r0 = max(r0, c);
+  const double* col = A + (long)c * n;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int r = r0 + lane + 32 * u;
+    if (r < r1) acc[u] = __ldg(col + r) * __ldg(v + r);
+  }
+  double t = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+  t = warp_sum(t);
+  unsigned ticket = 0;
+  if (lane == 0) {
+    partial[(long)sg * n + c] = t;
+    __threadfence();
+    ticket = atomicAdd(counters + c, 1u);
+  }
+  ticket = __shfl_sync(0xffffffffu, ticket, 0);
+  if (ticket != (unsigned)(s1 - s0 - 1)) return;
+  if (lane == 0) {
+    __threadfence();
+    double sum = 0.0;
+    for (int k = s0; k < s1; ++k) sum += __ldcg(partial + (long)k * n + c);
+    out[c] = (rbase ? rbase[c] : 0.0) + alpha * sum;
+    counters[c] = 0u;
+  }
+}
+
+// e = r - H x for the symmetric H (both triangles stored): e_i = r_i - (column i of H) . x, one
+// warp per column, coalesced, eight partial sums per lane (one launch, no partial buffer).
+extern "C" __global__ void k_symv_cols(const double* __restrict__ H, int m,
+                                       const double* __restrict__ x, const double* __restrict__ r,
+                                       double* __restrict__ e) {
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (c >= m) return;
+  const double* col = H + (long)c * m;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int k = lane;
+  for (; k + 7 * 32 < m; k += 8 * 32) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc[u] = fma(__ldg(col + k + 32 * u), __ldg(x + k + 32 * u), acc[u]);
+  }
+  for (; k < m; k += 32) acc[0] = fma(col[k], x[k], acc[0]);
+  double t = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+  t = warp_sum(t);
+  if (lane == 0) e[c] = r[c] - t;
 }

@@ -140,12 +140,14 @@ __global__ void k_trtri_diag(int, const double*, double*, double*);
 __global__ void k_trinv_level(const double*, double*, double*, double*, int, int, int);
 __global__ void k_tri_colgemv(const double*, int, int, const double*, double*);
 __global__ void k_shifted_copy(const double*, double*, int, double, double*);
-__global__ void k_symv_partial(const double*, int, const double*, long, double*, long);
-__global__ void k_symv_finish(int, const double*, long, const double*, long, double*, long);
+__global__ void k_symv_cols(const double*, int, const double*, const double*, double*);
+__global__ void k_coldot_seg(const double*, int, int, const double*, const double*, double, double*,
+                             double*, unsigned*);
 __global__ void k_lincomb(long, double, const double*, double, const double*, double,
                           const double*, double*);
 __global__ void k_reduce_partial(int, long, const double*, const double*, double*);
 __global__ void k_reduce_final(int, int, const double*, double*);
+__global__ void k_reduce_fused(int, long, const double*, const double*, double*, unsigned*, double*);
 __global__ void k_diag_absmax(const double*, int, double*);
 __global__ void k_csr_spmv(int, const int*, const int*, const double*, const double*, double,
                            double, double*);
@@ -164,6 +166,8 @@ class Reducer {
   void init() {
     partial_.alloc((size_t)kBlocks * kSlots);
     slots_.alloc(kSlots);
+    counters_.alloc(kSlots);
+    check(cudaMemset(counters_.p, 0, kSlots * sizeof(unsigned)), "reducer counters");
     host_.alloc(kSlots);
   }
   int add(cudaStream_t st, int op, long n, const double* x, const double* y) {
@@ -171,8 +175,8 @@ class Reducer {
     if (n > 0 && !x) throw std::invalid_argument("null device buffer: reduction input");
     int s = count_++;
     if (n > 0) {
-      ++g_launches, k_reduce_partial<<<kBlocks, 256, 0, st>>>(op, n, x, y, partial_.p + (size_t)s * kBlocks);
-      ++g_launches, k_reduce_final<<<1, 32, 0, st>>>(op, kBlocks, partial_.p + (size_t)s * kBlocks, slots_.p + s);
+      ++g_launches, k_reduce_fused<<<kBlocks, 256, 0, st>>>(op, n, x, y, partial_.p + (size_t)s * kBlocks,
+                                                          counters_.p + s, slots_.p + s);
     } else {
       double id = (op == RED_FINITE) ? 1.0 : 0.0;
       copy_h2d(slots_.p + s, &id_[op], sizeof(double), st);
@@ -194,6 +198,7 @@ class Reducer {
 
  private:
   DevBuf<double> partial_, slots_;
+  DevBuf<unsigned> counters_;  // arrival tickets of k_reduce_fused, one per slot (self-resetting)
   PinnedBuf<double> host_;
   int count_ = 0;
   const double id_[4] = {0.0, 0.0, 0.0, 1.0};

@@ -510,8 +510,10 @@ class Engine {
     F_.alloc((size_t)n * n);
     Dinv_.alloc((size_t)std::max(nchol, 1) * kNB * kNB);
     diag0_.alloc(std::max(n, 1));
-    symv_part_.alloc((size_t)16 * std::max(n, 1));
     tri_y_.alloc(std::max(n, 1));
+    gv_part_.alloc((size_t)std::max(n, 1) * ((n + 255) / 256 + 1));
+    gv_cnt_.alloc(std::max(n, 1));
+    check(cudaMemsetAsync(gv_cnt_.p, 0, gv_cnt_.n * sizeof(unsigned), st), "gemv counters");
     Uinv_.alloc((size_t)n * n);
     UinvT_.alloc((size_t)n * n);
     Tmp_.alloc((size_t)n * n);
@@ -776,9 +778,12 @@ class Engine {
     need(r, "trisolve r");
     need(x, "trisolve x");
     tbegin(KT_TRISOLVE);
-    const int grid = (n + 7) / 8;
-    ++g_launches, k_tri_colgemv<<<grid, 256, 0, st>>>(Uinv_, n, 0, r, tri_y_);
-    ++g_launches, k_tri_colgemv<<<grid, 256, 0, st>>>(UinvT_, n, 1, tri_y_, x);
+    // y = X' b: column dots on X (upper); x = X y: column dots on the stored X' (lower)
+    const dim3 grid((n + 7) / 8, (n + 255) / 256);
+    ++g_launches, k_coldot_seg<<<grid, 256, 0, st>>>(Uinv_, n, 1, r, nullptr, 1.0, tri_y_, gv_part_,
+                                                     gv_cnt_);
+    ++g_launches, k_coldot_seg<<<grid, 256, 0, st>>>(UinvT_, n, 2, tri_y_, nullptr, 1.0, x, gv_part_,
+                                                     gv_cnt_);
     launched("trisolve");
     tend(KT_TRISOLVE);
   }
@@ -789,9 +794,8 @@ class Engine {
     need(e, "schur_residual e");
     if (!n) return;
     tbegin(KT_SYMV);
-    ++g_launches, k_symv_partial<<<dim3((n + 127) / 128, 16, 1), 128, 0, st>>>(Hsave_, n, x, n, symv_part_,
-                                                                 (long)16 * n);
-    ++g_launches, k_symv_finish<<<dim3((n + 255) / 256, 1), 256, 0, st>>>(n, symv_part_, (long)16 * n, r, n, e, n);
+    const dim3 grid((n + 7) / 8, (n + 255) / 256);  // H symmetric: column i . x = (H x)_i
+    ++g_launches, k_coldot_seg<<<grid, 256, 0, st>>>(Hsave_, n, 0, x, r, -1.0, e, gv_part_, gv_cnt_);
     launched("schur_residual");
     tend(KT_SYMV);
   }
@@ -844,7 +848,9 @@ class Engine {
   DevBuf<int> prp_, pci_, pup_ptr_, pup_row_;
   DevBuf<double> pv_, pup_val_;
   DevBuf<double> adj_part_;
-  DevBuf<double> Hsave_, F_, Dinv_, diag0_, symv_part_, tri_y_, Uinv_, UinvT_, Tmp_;
+  DevBuf<double> Hsave_, F_, Dinv_, diag0_, tri_y_, Uinv_, UinvT_, Tmp_;
+  DevBuf<double> gv_part_;   // k_coldot_seg segment sums (segments x n)
+  DevBuf<unsigned> gv_cnt_;  // k_coldot_seg column tickets (self-resetting)
   DevBuf<double> step_out_, marg_out_, scal_;
   DevBuf<uint32_t> status_;
   PinnedBuf<uint32_t> hstat_;

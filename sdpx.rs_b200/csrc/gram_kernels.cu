@@ -120,15 +120,17 @@ k_gram_schur(const BlockDesc* __restrict__ blocks, const int* __restrict__ tiles
 
 // y_j = alpha svec(U_j diag(sigma x_cols) U_j') + beta y_j.  Grid (Gram block, 8-row tile R):
 // warp w computes the 8 x 8 output tile (R, w) for w >= R (upper triangle) on the FP64 tensor
-// cores with fragments read straight from the factor (L1/L2 resident), K = k_j in chunks of
-// 256 whose scaled weights d_t = sigma_t x[col_t] are staged in shared memory.
-#define GR_KCH 256
+// cores.  K = k_j runs in chunks of 64 columns of U staged in shared memory (coalesced loads,
+// column t at Us[t * GR_LD + row]: conflict-free fragment reads) with their scaled weights
+// d_t = sigma_t x[col_t].
+#define GR_KCH 64
 extern "C" __global__ void __launch_bounds__(256)
 k_gram_forward(const BlockDesc* __restrict__ blocks, const int* __restrict__ gblk,
                const int* __restrict__ kcount, const int* __restrict__ col_ptr,
                const int* __restrict__ col_idx, const long* __restrict__ gu_off,
                const double* __restrict__ gsig, const double* __restrict__ U,
                const double* __restrict__ x, double alpha, double beta, double* __restrict__ y) {
+  __shared__ __align__(16) double Us[GR_KCH * GR_LD];
   __shared__ double d[GR_KCH];
   const int j = gblk[blockIdx.x], R = blockIdx.y;
   const BlockDesc bd = blocks[j];
@@ -138,21 +140,25 @@ k_gram_forward(const BlockDesc* __restrict__ blocks, const int* __restrict__ gbl
   const double* Uj = U + gu_off[j];
   const int* cols = col_idx + col_ptr[j];
   const double* sg = gsig + col_ptr[j];
-  const int row = 8 * R + r, col = 8 * w + r;  // fragment rows of the A (rows) and B (cols) sides
+  for (int e = threadIdx.x; e < GR_KCH * GR_LD; e += blockDim.x) Us[e] = 0.0;  // rows >= n stay 0
   const bool live = (w >= R) && (8 * w < n);
   double d0 = 0.0, d1 = 0.0;
   for (int t0 = 0; t0 < k; t0 += GR_KCH) {
     const int kc = min(GR_KCH, k - t0);
-    __syncthreads();
-    for (int t = threadIdx.x; t < kc; t += blockDim.x) d[t] = sg[t0 + t] * x[cols[t0 + t]];
+    __syncthreads();  // the zero fill, or the previous chunk's reads, are done
+    for (int e = threadIdx.x; e < n * kc; e += blockDim.x) {
+      const int t = e / n, row = e - t * n;
+      Us[t * GR_LD + row] = Uj[(long)(t0 + t) * n + row];
+    }
+    for (int t = threadIdx.x; t < GR_KCH; t += blockDim.x)
+      d[t] = (t < kc) ? sg[t0 + t] * x[cols[t0 + t]] : 0.0;
     __syncthreads();
     if (live) {
-      for (int ks = 0; ks < (kc + 3) / 4; ++ks) {
+#pragma unroll 4
+      for (int ks = 0; ks < GR_KCH / 4; ++ks) {
         const int t = 4 * ks + q;
-        const bool in = t < kc;
-        const double* ut = Uj + (long)(t0 + t) * n;
-        const double a = (in && row < n) ? d[t] * ut[row] : 0.0;  // (U diag(d))[row][t]
-        const double b = (in && col < n) ? ut[col] : 0.0;          // U'[t][col]
+        const double a = d[t] * Us[t * GR_LD + 8 * R + r];  // (U diag(d))[row][t]
+        const double b = Us[t * GR_LD + 8 * w + r];          // U'[t][col]
         dmma_m8n8k4(d0, d1, a, b);
       }
     }

@@ -6,7 +6,7 @@
 // whole device) is not allowed.  They can still create a context and factor once at set-up,
 // but every later solve must run without allocating.  This entry point takes device pointers
 // for the right-hand sides and the solutions and keeps all of its per-call scratch (the solve
-// intermediate, the refinement vectors, the matvec partial sums and the reduction slots) in
+// intermediate, the refinement vectors and the reduction slots) in
 // one file-scope device array, g_noalloc_scratch, of fixed size.  It calls no cudaMalloc,
 // cudaFree or allocating library routine.
 //
@@ -14,7 +14,7 @@
 //  * n (the Schur dimension of the uploaded problem) must be at most SDPXG_NOALLOC_MAXN;
 //    larger problems are rejected with return code 2 and a message.
 //  * The array lives in every GPU that loads this library until the process exits
-//    (SDPXG_NOALLOC_DOUBLES doubles, about 0.7 MB).
+//    (SDPXG_NOALLOC_DOUBLES doubles, about 0.17 MB).
 //  * Every call shares the array and it keeps the last call's contents.  Nothing in it has to
 //    start at zero: each kernel writes every scratch element before another reads it.  Calls
 //    whose work overlaps on the GPU (two host threads, or contexts on different streams of the
@@ -41,8 +41,8 @@ Engine* ctx_engine(sdpxg_ctx* ctx);
 
 #define SDPXG_NOALLOC_MAXN 4096
 #define SDPXG_NOALLOC_RED_BLOCKS 148
-// tri (n) + e (n) + dx (n) + cand (n) + e2 (n) + matvec partials (16 n) + 3 reduction slots
-#define SDPXG_NOALLOC_DOUBLES (21 * SDPXG_NOALLOC_MAXN + 3 * (SDPXG_NOALLOC_RED_BLOCKS + 1))
+// tri (n) + e (n) + dx (n) + cand (n) + e2 (n) + 3 reduction slots
+#define SDPXG_NOALLOC_DOUBLES (5 * SDPXG_NOALLOC_MAXN + 3 * (SDPXG_NOALLOC_RED_BLOCKS + 1))
 
 static __device__ __align__(256) double g_noalloc_scratch[SDPXG_NOALLOC_DOUBLES];
 
@@ -98,8 +98,7 @@ extern "C" int32_t sdpxg_solve_noalloc(sdpxg_ctx* ctx, const double* d_rhs, doub
     double* dx = en + SDPXG_NOALLOC_MAXN;
     double* cand = dx + SDPXG_NOALLOC_MAXN;
     double* e2 = cand + SDPXG_NOALLOC_MAXN;
-    double* part = e2 + SDPXG_NOALLOC_MAXN;  // 16 n
-    double* red = part + 16 * SDPXG_NOALLOC_MAXN;
+    double* red = e2 + SDPXG_NOALLOC_MAXN;
     double* slots = red + 3 * SDPXG_NOALLOC_RED_BLOCKS;
     cudaStream_t st = E.st;
     const Settings cfg;  // binary64 refinement defaults, as in sdpxg_solve_many
@@ -109,10 +108,7 @@ extern "C" int32_t sdpxg_solve_noalloc(sdpxg_ctx* ctx, const double* d_rhs, doub
       ++g_launches, k_tri_colgemv<<<grid, 256, 0, st>>>(E.uinvT(), n, 1, tri, x);
     };
     auto residual = [&](const double* r, const double* x, double* e) {
-      ++g_launches, k_symv_partial<<<dim3((n + 127) / 128, 16, 1), 128, 0, st>>>(E.Hsave(), n, x, n,
-                                                                                part, (long)16 * n);
-      ++g_launches, k_symv_finish<<<dim3((n + 255) / 256, 1), 256, 0, st>>>(n, part, (long)16 * n, r,
-                                                                          n, e, n);
+      ++g_launches, k_symv_cols<<<(n + 7) / 8, 256, 0, st>>>(E.Hsave(), n, x, r, e);
     };
     auto fetch = [&](int count, double* host) {
       check(cudaMemcpyAsync(host, slots, count * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");

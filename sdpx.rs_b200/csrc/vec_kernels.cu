@@ -57,6 +57,41 @@ k_reduce_partial(int op, long n, const double* __restrict__ x, const double* __r
   }
 }
 
+// One launch per reduction: every block writes its partial, and the block that arrives last
+// (a ticket on counter, reset to 0 for the next use) folds the partials in the fixed order of
+// k_reduce_final and writes out -- the same value as the two-launch form, bit for bit.
+extern "C" __global__ void __launch_bounds__(RED_THREADS)
+k_reduce_fused(int op, long n, const double* __restrict__ x, const double* __restrict__ y,
+               double* __restrict__ partial, unsigned* __restrict__ counter,
+               double* __restrict__ out) {
+  __shared__ double red[RED_THREADS / 32];
+  __shared__ bool last;
+  double acc = red_identity(op);
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    acc = red_combine(op, acc, red_elem(op, x, y, i));
+  for (int o = 16; o > 0; o >>= 1) acc = red_combine(op, acc, __shfl_xor_sync(0xffffffffu, acc, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = red_identity(op);
+    for (int w = 0; w < RED_THREADS / 32; ++w) v = red_combine(op, v, red[w]);
+    partial[blockIdx.x] = v;
+    __threadfence();
+    last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last || threadIdx.x >= 32) return;
+  __threadfence();
+  double v = red_identity(op);
+  for (int p = threadIdx.x; p < (int)gridDim.x; p += 32) v = red_combine(op, v, __ldcg(partial + p));
+  for (int o = 16; o > 0; o >>= 1) v = red_combine(op, v, __shfl_xor_sync(0xffffffffu, v, o));
+  if (threadIdx.x == 0) {
+    *out = v;
+    *counter = 0u;
+  }
+}
+
 // One warp: lane l folds partials l, l+32, ... in order, then a fixed shuffle tree.
 extern "C" __global__ void k_reduce_final(int op, int nparts, const double* __restrict__ partial,
                                           double* __restrict__ out) {
