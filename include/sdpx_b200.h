@@ -132,6 +132,14 @@ uint64_t sdpx_b200_launch_count(void);
 /* Bytes this library has copied host-to-device and device-to-host in this process (all
  * handles): the host-device traffic of prepare, solve and result reads. */
 int32_t sdpx_b200_transfer_bytes(uint64_t *h2d, uint64_t *d2h);
+/* Re-prepare an existing handle with another problem (any dimensions, cones and settings, the
+ * same validation as sdpx_prepare) and keep its device state: buffers are reused and grow only,
+ * so a worker that solves a stream of independent instances allocates and frees nothing per
+ * instance (cudaFree would synchronise the device and stall the other workers' solves).  The
+ * previous result is invalidated.  No counterpart in the reference (it has no batching). */
+int32_t sdpx_b200_reprepare(sdpx_handle *handle, const sdpx_csc *P, const sdpx_scalars *q,
+                            const sdpx_csc *A, const sdpx_scalars *b, const sdpx_cone *cones,
+                            uint64_t cone_count, const sdpx_settings *settings);
 /* Schur forms chosen at prepare: PSD blocks whose every constraint column is rank one
  * (sigma u u', stored as the factor U and used in the Gram form S = (sigma sigma') o (U' Ginv U)^2,
  * like the reference's sampled Gram update, sampled/mod.rs:1973-2025) and blocks kept in the

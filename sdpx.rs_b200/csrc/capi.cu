@@ -22,7 +22,6 @@ thread_local std::string g_last_error;  // shared by both ABI levels
 
 namespace {
 
-std::string& g_error = sdpxg::g_last_error;
 
 struct AbiError {
   int32_t code;
@@ -35,16 +34,16 @@ int32_t boundary(F&& f) {
     f();
     return 0;
   } catch (const AbiError& e) {
-    g_error = e.msg;
+    sdpxg::g_last_error = e.msg;
     return e.code;
   } catch (const std::invalid_argument& e) {
-    g_error = e.what();
+    sdpxg::g_last_error = e.what();
     return 1;
   } catch (const std::exception& e) {
-    g_error = std::string("internal error: ") + e.what();
+    sdpxg::g_last_error = std::string("internal error: ") + e.what();
     return 5;
   } catch (...) {
-    g_error = "internal error at ABI boundary";
+    sdpxg::g_last_error = "internal error at ABI boundary";
     return 5;
   }
 }
@@ -354,11 +353,14 @@ std::string rust_exp(double x) {
   return mant + "e" + std::to_string(ex);
 }
 
-void prepare_impl(const sdpx_csc* P, const sdpx_scalars* q, const sdpx_csc* A, const sdpx_scalars* b,
-                  const sdpx_cone* cones, uint64_t nc, const sdpx_settings* s, sdpx_handle** out) {
+// Validated, equilibrated copy of a problem, without device state (shared by prepare and
+// reprepare).
+std::unique_ptr<sdpx_handle> build_problem(const sdpx_csc* P, const sdpx_scalars* q,
+                                           const sdpx_csc* A, const sdpx_scalars* b,
+                                           const sdpx_cone* cones, uint64_t nc,
+                                           const sdpx_settings* s, double* t_validate,
+                                           double* t_equil) {
   const auto t0 = std::chrono::steady_clock::now();
-  if (!out) invalid("null pointer");
-  *out = nullptr;
   ref(q); ref(A); ref(b); ref(s);
   if (nc && !cones) invalid("null pointer");
   validate_settings(*s);
@@ -408,6 +410,19 @@ void prepare_impl(const sdpx_csc* P, const sdpx_scalars* q, const sdpx_csc* A, c
   h->orig.psd = h->equil.psd;
   equilibrate(h->equil, h->settings, h->eq);
   const auto t2 = std::chrono::steady_clock::now();
+  auto sec = [](auto a, auto b) { return std::chrono::duration<double>(b - a).count(); };
+  *t_validate = sec(t0, t1);
+  *t_equil = sec(t1, t2);
+  return h;
+}
+
+void prepare_impl(const sdpx_csc* P, const sdpx_scalars* q, const sdpx_csc* A, const sdpx_scalars* b,
+                  const sdpx_cone* cones, uint64_t nc, const sdpx_settings* s, sdpx_handle** out) {
+  if (!out) invalid("null pointer");
+  *out = nullptr;
+  double tv = 0, te = 0;
+  auto h = build_problem(P, q, A, b, cones, nc, s, &tv, &te);
+  const auto t2 = std::chrono::steady_clock::now();
   h->eng = std::make_unique<Engine>();
   h->eng->init(device_from_env());
   const auto t3 = std::chrono::steady_clock::now();
@@ -418,7 +433,7 @@ void prepare_impl(const sdpx_csc* P, const sdpx_scalars* q, const sdpx_csc* A, c
     std::fprintf(stderr,
                  "sdpx_b200 prepare: copy+validate %.3f s, equilibrate %.3f s, device init %.3f s, "
                  "upload %.3f s (%s)\n",
-                 sec(t0, t1), sec(t1, t2), sec(t2, t3), sec(t3, t4), h->eng->upload_report().c_str());
+                 tv, te, sec(t2, t3), sec(t3, t4), h->eng->upload_report().c_str());
   }
   *out = h.release();
 }
@@ -460,6 +475,24 @@ int32_t sdpx_prepare_sampled(const sdpx_csc*, const sdpx_scalars*, const sdpx_cs
   return boundary([&] {
     if (out) *out = nullptr;
     unsupported("factor-authoritative sampled blocks are not implemented on the GPU path");
+  });
+}
+
+int32_t sdpx_b200_reprepare(sdpx_handle* h, const sdpx_csc* P, const sdpx_scalars* q,
+                            const sdpx_csc* A, const sdpx_scalars* b, const sdpx_cone* cones,
+                            uint64_t cone_count, const sdpx_settings* settings) {
+  return boundary([&] {
+    double tv = 0, te = 0;
+    auto fresh = build_problem(P, q, A, b, cones, cone_count, settings, &tv, &te);
+    operate(h, [&](sdpx_handle& hh) {
+      hh.solved = false;
+      hh.settings = fresh->settings;
+      hh.orig = std::move(fresh->orig);
+      hh.equil = std::move(fresh->equil);
+      hh.eq = std::move(fresh->eq);
+      hh.eng->upload(hh.equil);  // buffers grow only; cached graphs are dropped
+      if (hh.hsd) hh.hsd->reset(hh.equil, hh.eq, hh.settings);
+    });
   });
 }
 
@@ -558,7 +591,7 @@ int32_t sdpx_result_decimal(sdpx_handle* h, char* out, uint64_t capacity, uint64
 }
 
 uint64_t sdpx_last_error(char* out, uint64_t capacity) {
-  const std::string& e = g_error;
+  const std::string& e = sdpxg::g_last_error;
   uint64_t n = e.size() + 1;
   if (out && capacity > 0) {
     uint64_t k = std::min<uint64_t>(e.size(), capacity - 1);

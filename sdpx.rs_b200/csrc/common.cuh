@@ -123,28 +123,35 @@ __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, do
                : "d"(a), "d"(b));
 }
 
-// C = op(A) op(B) on zero-padded shared matrices, one 8 x 8 output tile per warp at a time,
-// K in groups of 16 (four k-steps) up to n rounded up: the fragments of a group are loaded
-// before its four MMAs, so the shared-memory latency overlaps instead of serialising with the
-// accumulation chain (the zero padding makes the rounded-up K exact).  C must not alias A or B.
+// C = op(A) op(B) on zero-padded shared matrices, one 8 x 8 output tile per warp at a time.
+// K runs to n rounded up to 4, never further: C is written only up to n rounded up to 8, and
+// a later product that reads C as an operand must not reach its unwritten columns (another
+// kernel's leftovers there, NaN included, would enter through 0 x NaN).  Full groups of four
+// k-steps load their fragments before their four MMAs, so the shared-memory latency overlaps
+// the accumulation chain; the remaining k-steps follow one by one.  C must not alias A or B.
 template <bool TA, bool TB>
 __device__ __forceinline__ void cta_gemm_mma(double* C, const double* A, const double* B, int n) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int tiles = (n + 7) >> 3, kgroups = (n + 15) >> 4;
+  const int tiles = (n + 7) >> 3, ksteps = (n + 3) >> 2, kfull = ksteps & ~3;
   const int r = lane >> 2, q = lane & 3;
   for (int t = warp; t < tiles * tiles; t += nwarps) {
     const int ti = (t % tiles) << 3, tj = (t / tiles) << 3;
     double d0 = 0.0, d1 = 0.0;
-    for (int kg = 0; kg < kgroups; ++kg) {
+    for (int ks0 = 0; ks0 < kfull; ks0 += 4) {
       double a[4], b[4];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        const int k = (kg << 4) + (u << 2) + q;
+        const int k = ((ks0 + u) << 2) + q;
         a[u] = TA ? SM(A, k, ti + r) : SM(A, ti + r, k);
         b[u] = TB ? SM(B, tj + r, k) : SM(B, k, tj + r);
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) dmma_m8n8k4(d0, d1, a[u], b[u]);
+    }
+    for (int ks = kfull; ks < ksteps; ++ks) {
+      const int k = (ks << 2) + q;
+      dmma_m8n8k4(d0, d1, TA ? SM(A, k, ti + r) : SM(A, ti + r, k),
+                  TB ? SM(B, tj + r, k) : SM(B, k, tj + r));
     }
     SM(C, ti + r, tj + 2 * q) = d0;
     SM(C, ti + r, tj + 2 * q + 1) = d1;

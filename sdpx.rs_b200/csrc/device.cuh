@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -21,7 +22,7 @@ inline void check(cudaError_t e, const char* what) {
 
 // Bytes this library copied between host and device in this process (all handles): the
 // end-to-end traffic of a solve, read through sdpx_b200_transfer_bytes.
-inline uint64_t g_h2d_bytes = 0, g_d2h_bytes = 0;
+inline std::atomic<uint64_t> g_h2d_bytes{0}, g_d2h_bytes{0};
 
 inline void copy_h2d(void* d, const void* h, size_t bytes, cudaStream_t st) {
   if (!bytes) return;
@@ -35,29 +36,41 @@ inline void copy_d2h(void* h, const void* d, size_t bytes, cudaStream_t st) {
   g_d2h_bytes += bytes;
 }
 
+// Device buffer with grow-only storage: alloc() reuses the allocation when it is large enough,
+// so a handle that is re-prepared with a new problem (batches of instances) allocates only when
+// a buffer grows, and never frees in between (cudaFree synchronises the whole device, which
+// would stall every other instance running on it).  n is the requested element count.
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  size_t cap = 0;
   DevBuf() = default;
   explicit DevBuf(size_t count) { alloc(count); }
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), cap(o.cap) { o.p = nullptr; o.n = o.cap = 0; }
   DevBuf& operator=(DevBuf&& o) noexcept {
-    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    if (this != &o) { release(); p = o.p; n = o.n; cap = o.cap; o.p = nullptr; o.n = o.cap = 0; }
     return *this;
   }
   ~DevBuf() { release(); }
   void alloc(size_t count) {
+    if (count <= cap && p) {
+      n = count;
+      return;
+    }
     release();
     n = count;
-    if (count) check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+    if (count) {
+      check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+      cap = count;
+    }
   }
   void release() {
     if (p) cudaFree(p);
     p = nullptr;
-    n = 0;
+    n = cap = 0;
   }
   void upload(const T* h, size_t count, cudaStream_t st) {
     copy_h2d(p, h, count * sizeof(T), st);
@@ -78,15 +91,23 @@ struct PinnedBuf {
   PinnedBuf(const PinnedBuf&) = delete;
   PinnedBuf& operator=(const PinnedBuf&) = delete;
   ~PinnedBuf() { release(); }
-  void alloc(size_t count) {
+  size_t cap = 0;
+  void alloc(size_t count) {  // grow-only, like DevBuf
+    if (count <= cap && p) {
+      n = count;
+      return;
+    }
     release();
     n = count;
-    if (count) check(cudaMallocHost(&p, count * sizeof(T)), "cudaMallocHost");
+    if (count) {
+      check(cudaMallocHost(&p, count * sizeof(T)), "cudaMallocHost");
+      cap = count;
+    }
   }
   void release() {
     if (p) cudaFreeHost(p);
     p = nullptr;
-    n = 0;
+    n = cap = 0;
   }
   T& operator[](size_t i) { return p[i]; }
   const T& operator[](size_t i) const { return p[i]; }
@@ -154,7 +175,7 @@ __global__ void k_csr_spmv(int, const int*, const int*, const double*, const dou
 }
 
 // Kernel launches issued by this library in this process (every launch site increments it).
-inline uint64_t g_launches = 0;
+inline std::atomic<uint64_t> g_launches{0};  // atomic: handles may run on many host threads
 
 enum RedOp { RED_DOT = 0, RED_SUMSQ = 1, RED_MAXABS = 2, RED_FINITE = 3 };
 

@@ -217,7 +217,6 @@ class Engine {
       return;
     }
     if (graphs_.size() >= kMaxGraphs) clear_graphs();  // bound the cache
-    const uint64_t l0 = g_launches;
     check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
       body();
@@ -229,11 +228,22 @@ class Engine {
     }
     cudaGraph_t g = nullptr;
     check(cudaStreamEndCapture(st, &g), "end capture");
+    // kernel nodes of the segment (the launch counter's increment per replay)
+    size_t nn = 0;
+    uint64_t kernels = 0;
+    check(cudaGraphGetNodes(g, nullptr, &nn), "graph nodes");
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (nn) check(cudaGraphGetNodes(g, nodes.data(), &nn), "graph nodes");
+    for (cudaGraphNode_t nd : nodes) {
+      cudaGraphNodeType ty;
+      check(cudaGraphNodeGetType(nd, &ty), "graph node type");
+      kernels += (ty == cudaGraphNodeTypeKernel);
+    }
     cudaGraphExec_t ex = nullptr;
     const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
     cudaGraphDestroy(g);
     check(e, "cudaGraphInstantiate");
-    graphs_[key] = {ex, red.count(), g_launches - l0};
+    graphs_[key] = {ex, red.count(), kernels};
     check(cudaGraphLaunch(ex, st), "cudaGraphLaunch");
   }
   void tbegin(int k) {

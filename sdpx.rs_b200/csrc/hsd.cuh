@@ -69,6 +69,16 @@ class HsdSolver {
  public:
   HsdSolver(Engine& eng, const HostProblem& p, const Equilibration& eq, const Settings& st)
       : E(eng), eq_(eq), st_(st), n_(p.n), m_(p.m) {
+    reset(p, eq, st);
+  }
+
+  // Take a new problem (other dimensions, equilibration or settings) on the same engine: the
+  // work vectors grow if needed and are otherwise reused.
+  void reset(const HostProblem& p, const Equilibration& eq, const Settings& st) {
+    eq_ = eq;
+    st_ = st;
+    n_ = p.n;
+    m_ = p.m;
     const int n = n_, m = m_;
     E.clear_graphs();  // segments captured for earlier work vectors must not be replayed
     auto vn = [&](DevBuf<double>& b) { b.alloc(std::max(n, 1)); };

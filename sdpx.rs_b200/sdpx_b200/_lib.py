@@ -64,6 +64,8 @@ SIGNATURES = {
                                    C.POINTER(Scalars), C.POINTER(Cone), u64, C.POINTER(Settings),
                                    C.POINTER(SampledBlock), u64, C.POINTER(C.c_void_p)]),
     "sdpx_solve": (i32, [C.c_void_p]),
+    "sdpx_b200_reprepare": (i32, [C.c_void_p, C.POINTER(Csc), C.POINTER(Scalars), C.POINTER(Csc),
+                                  C.POINTER(Scalars), C.POINTER(Cone), u64, C.POINTER(Settings)]),
     "sdpx_update": (i32, [C.c_void_p, C.POINTER(Scalars), C.POINTER(Scalars)]),
     "sdpx_get_info": (i32, [C.c_void_p, C.POINTER(Info)]),
     "sdpx_get_solver_name": (i32, [C.c_void_p, C.c_char_p, u64, PU64]),

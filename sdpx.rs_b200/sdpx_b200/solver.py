@@ -130,6 +130,15 @@ class DefaultSolver:
 
     def __init__(self, P, q, A, b, cones: Sequence[Tuple[str, int]],
                  settings: Optional[DefaultSettings] = None):
+        args = self._c_args(P, q, A, b, cones, settings)
+        h = C.c_void_p()
+        _lib.call("sdpx_prepare", *args, C.byref(h))
+        self._h = h
+        self.solution: Optional[Solution] = None
+        self.info: Optional[SolveInfo] = None
+
+    def _c_args(self, P, q, A, b, cones, settings):
+        """C views of a problem (the numpy buffers are kept alive on self)."""
         settings = settings or DefaultSettings()
         A = sp.csc_matrix(A, dtype=np.float64)
         n = A.shape[1]
@@ -143,14 +152,19 @@ class DefaultSolver:
             cone_arr[i].reserved = 0
             cone_arr[i].dim = int(d)
             cone_arr[i].alpha = _scalars(np.zeros(0))
-        cs, keep = settings.to_c()
-        h = C.c_void_p()
-        _lib.call("sdpx_prepare", C.byref(self._P.c), C.byref(_scalars(self._q)), C.byref(self._A.c),
-                  C.byref(_scalars(self._b)), cone_arr, len(cones), C.byref(cs), C.byref(h))
-        self._h = h
+        cs, self._keep = settings.to_c()
+        self._cones, self._cs = cone_arr, cs
         self.n, self.m = n, A.shape[0]
-        self.solution: Optional[Solution] = None
-        self.info: Optional[SolveInfo] = None
+        return (C.byref(self._P.c), C.byref(_scalars(self._q)), C.byref(self._A.c),
+                C.byref(_scalars(self._b)), cone_arr, len(cones), C.byref(cs))
+
+    def reprepare(self, P, q, A, b, cones: Sequence[Tuple[str, int]],
+                  settings: Optional[DefaultSettings] = None):
+        """Load another problem into this handle, reusing its device buffers and stream."""
+        args = self._c_args(P, q, A, b, cones, settings)
+        _lib.call("sdpx_b200_reprepare", self._h, *args)
+        self.solution = None
+        self.info = None
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -223,6 +237,47 @@ class DefaultSolver:
         buf = C.create_string_buffer(need.value)
         _lib.call("sdpx_result_decimal", self._h, buf, need.value, C.byref(need))
         return [s.decode() for s in buf.raw[:need.value].split(b"\0")[:-1]]
+
+
+class BatchSolver:
+    """Many independent problems on one GPU: ``workers`` host threads each own one handle (its
+    own CUDA stream) and re-prepare it for every instance they take, so instances run
+    concurrently on the device and no device memory is allocated or freed between them.
+    The GIL is released inside every library call."""
+
+    def __init__(self, workers: int = 16, settings: Optional[DefaultSettings] = None):
+        self.workers = max(1, int(workers))
+        self.settings = settings
+        self._solvers: List[Optional[DefaultSolver]] = [None] * self.workers
+
+    def solve(self, problems) -> List[Solution]:
+        import threading
+        from concurrent.futures import ThreadPoolExecutor
+        problems = list(problems)
+        out: List[Optional[Solution]] = [None] * len(problems)
+        lock = threading.Lock()
+        nxt = [0]
+
+        def work(w: int):
+            while True:
+                with lock:
+                    i = nxt[0]
+                    nxt[0] += 1
+                if i >= len(problems):
+                    return
+                p = problems[i]
+                s = self._solvers[w]
+                if s is None:
+                    s = DefaultSolver(p.P, p.q, p.A, p.b, p.cones, self.settings)
+                    self._solvers[w] = s
+                else:
+                    s.reprepare(p.P, p.q, p.A, p.b, p.cones, self.settings)
+                out[i] = s.solve()
+
+        with ThreadPoolExecutor(self.workers) as ex:
+            for f in [ex.submit(work, w) for w in range(self.workers)]:
+                f.result()
+        return out
 
 
 def solve_problem(prob, settings: Optional[DefaultSettings] = None) -> DefaultSolver:

@@ -116,3 +116,36 @@ def test_last_error_truncates(lib):
 def test_null_handle_and_destroy(lib):
     assert lib.sdpx_destroy(None) == 0
     assert lib.sdpx_solve(None) == 1
+
+
+def test_last_error_is_per_thread(lib):
+    """Each host thread reads its own last error (batches call the library from many threads)."""
+    import threading
+
+    problems = []
+
+    def worker(tid):
+        from sdpx_b200.solver import _CscHold, _scalars
+        s = _lib.Settings()
+        lib.sdpx_default_settings_v4(C.byref(s))
+        s.abi_version = 100 + tid  # rejected with a message naming this thread's version
+        a = _CscHold(sp.identity(3, format="csc"))
+        q, b = np.zeros(3), np.ones(3)
+        cone = (_lib.Cone * 1)()
+        cone[0].kind, cone[0].dim = 3, 2
+        h = C.c_void_p()
+        buf = C.create_string_buffer(256)
+        for _ in range(200):
+            rc = lib.sdpx_prepare(None, C.byref(_scalars(q)), C.byref(a.c), C.byref(_scalars(b)),
+                                  cone, 1, C.byref(s), C.byref(h))
+            lib.sdpx_last_error(buf, 256)
+            msg = buf.value.decode()
+            if rc != 1 or f"version {100 + tid};" not in msg:
+                problems.append((tid, rc, msg))
+
+    threads = [threading.Thread(target=worker, args=(t,)) for t in range(8)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not problems, problems[:3]
