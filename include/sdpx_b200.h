@@ -140,6 +140,11 @@ int32_t sdpx_b200_transfer_bytes(uint64_t *h2d, uint64_t *d2h);
 int32_t sdpx_b200_reprepare(sdpx_handle *handle, const sdpx_csc *P, const sdpx_scalars *q,
                             const sdpx_csc *A, const sdpx_scalars *b, const sdpx_cone *cones,
                             uint64_t cone_count, const sdpx_settings *settings);
+/* Capture the KKT solve's straight runs as CUDA graphs and replay them (on != 0, the default
+ * unless SDPX_B200_GRAPHS=0) or launch them eagerly (on == 0); results are bitwise the same.
+ * Capture pays off over the many solves of one problem; a handle re-prepared for every small
+ * instance of a batch is better off eager.  No counterpart in the reference. */
+int32_t sdpx_b200_set_graphs(sdpx_handle *handle, int32_t on);
 /* Schur forms chosen at prepare: PSD blocks whose every constraint column is rank one
  * (sigma u u', stored as the factor U and used in the Gram form S = (sigma sigma') o (U' Ginv U)^2,
  * like the reference's sampled Gram update, sampled/mod.rs:1973-2025) and blocks kept in the

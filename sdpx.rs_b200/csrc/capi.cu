@@ -107,7 +107,7 @@ Csc matrix(const sdpx_csc& a, bool upper) {
   for (uint64_t j = 0; j < a.cols; ++j)
     if (a.colptr[j] > a.colptr[j + 1] || a.colptr[j + 1] > a.nnz)
       invalid("invalid CSC column pointers");
-  parallel_for((int64_t)a.cols, 8, [&](int64_t j0, int64_t j1, int) {
+  parallel_for((int64_t)a.cols, col_grain(a.cols, a.nnz), [&](int64_t j0, int64_t j1, int) {
     for (int64_t j = j0; j < j1; ++j)
       for (uint64_t p = a.colptr[j]; p < a.colptr[j + 1]; ++p) {
         uint64_t r = a.rowval[p];
@@ -180,7 +180,7 @@ void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
         const int nt = host_threads();
         std::vector<std::vector<double>> ewp((size_t)nt);
         std::vector<char> used((size_t)nt, 0);
-        parallel_for(n, 8, [&](int64_t j0, int64_t j1, int t) {
+        parallel_for(n, col_grain(n, p.Aval.size()), [&](int64_t j0, int64_t j1, int t) {
           std::vector<double>& er = ewp[(size_t)t];
           er.assign(m, 0.0);
           used[(size_t)t] = 1;
@@ -191,7 +191,7 @@ void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
               er[p.Arow[q]] = std::max(er[p.Arow[q]], a);
             }
         });
-        parallel_for(m, 1 << 12, [&](int64_t i0, int64_t i1, int) {
+        parallel_for(m, std::max<int64_t>(1 << 12, (int64_t)m * nt / 4), [&](int64_t i0, int64_t i1, int) {
           for (int t = 0; t < nt; ++t)
             if (used[(size_t)t])
               for (int64_t i = i0; i < i1; ++i) ew[i] = std::max(ew[i], ewp[(size_t)t][i]);
@@ -207,7 +207,7 @@ void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
         w = 1.0 / std::sqrt(w);
         ew[i] = std::min(std::max(w, smin / eq.e[i]), smax / eq.e[i]);
       }
-      parallel_for(n, 8, [&](int64_t j0, int64_t j1, int) {
+      parallel_for(n, col_grain(n, p.Aval.size() + p.Pval.size()), [&](int64_t j0, int64_t j1, int) {
         for (int64_t j = j0; j < j1; ++j) {
           for (int64_t q = p.Pcolptr[j]; q < p.Pcolptr[j + 1]; ++q) p.Pval[q] *= dw[p.Prow[q]] * dw[j];
           for (int64_t q = p.Acolptr[j]; q < p.Acolptr[j + 1]; ++q) p.Aval[q] *= ew[p.Arow[q]] * dw[j];
@@ -248,7 +248,7 @@ void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
       for (int i = row; i < row + tn; ++i) delta[i] = mean / eq.e[i];
       row += tn;
     }
-    parallel_for(n, 8, [&](int64_t j0, int64_t j1, int) {
+    parallel_for(n, col_grain(n, p.Aval.size()), [&](int64_t j0, int64_t j1, int) {
       for (int64_t j = j0; j < j1; ++j)
         for (int64_t q = p.Acolptr[j]; q < p.Acolptr[j + 1]; ++q) p.Aval[q] *= delta[p.Arow[q]];
     });
@@ -639,6 +639,15 @@ int32_t sdpx_b200_kernel_times(sdpx_handle* h, double* ms, uint64_t* counts) {
         ms[k] = hh.eng->kt_ms[k];
         counts[k] = hh.eng->kt_count[k];
       }
+    });
+  });
+}
+
+int32_t sdpx_b200_set_graphs(sdpx_handle* h, int32_t on) {
+  return boundary([&] {
+    operate(h, [&](sdpx_handle& hh) {
+      hh.eng->clear_graphs();
+      hh.eng->graphs_enabled = on != 0;
     });
   });
 }

@@ -39,4 +39,13 @@ void parallel_for(int64_t n, int64_t grain, F&& f) {
     if (e) std::rethrow_exception(e);
 }
 
+// Column grain for loops over the columns of a sparse matrix: chunks of at least ~64k stored
+// entries, so small problems (many of them solved concurrently from separate host threads)
+// stay on the calling thread instead of spawning threads for microseconds of work.
+inline int64_t col_grain(uint64_t cols, uint64_t nnz) {
+  if (cols == 0) return 1;
+  const double per_col = std::max(1.0, (double)nnz / (double)cols);
+  return std::max<int64_t>(8, (int64_t)(65536.0 / per_col));
+}
+
 }  // namespace sdpxg

@@ -218,6 +218,10 @@ class DefaultSolver:
         self._b = np.ascontiguousarray(b, dtype=np.float64)
         _lib.call("sdpx_update", self._h, C.byref(_scalars(self._q)), C.byref(_scalars(self._b)))
 
+    def set_graphs(self, on: bool):
+        """Replay the KKT solve's captured CUDA graphs (default) or launch eagerly."""
+        _lib.call("sdpx_b200_set_graphs", self._h, int(bool(on)))
+
     def schur_forms(self) -> dict:
         """PSD blocks in the rank-one Gram form and in the ordinary dense-column form."""
         g, o = C.c_uint32(), C.c_uint32()
@@ -245,9 +249,11 @@ class BatchSolver:
     concurrently on the device and no device memory is allocated or freed between them.
     The GIL is released inside every library call."""
 
-    def __init__(self, workers: int = 16, settings: Optional[DefaultSettings] = None):
+    def __init__(self, workers: int = 16, settings: Optional[DefaultSettings] = None,
+                 graphs: bool = False):
         self.workers = max(1, int(workers))
         self.settings = settings
+        self.graphs = graphs  # graph capture costs more than it saves on one small instance
         self._solvers: List[Optional[DefaultSolver]] = [None] * self.workers
 
     def solve(self, problems) -> List[Solution]:
@@ -269,6 +275,7 @@ class BatchSolver:
                 s = self._solvers[w]
                 if s is None:
                     s = DefaultSolver(p.P, p.q, p.A, p.b, p.cones, self.settings)
+                    s.set_graphs(self.graphs)
                     self._solvers[w] = s
                 else:
                     s.reprepare(p.P, p.q, p.A, p.b, p.cones, self.settings)
