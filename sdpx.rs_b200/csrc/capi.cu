@@ -3,6 +3,7 @@
 // return code 5 (the reference's "panic" code) with the message kept thread-locally, and a
 // handle whose solve threw is poisoned (crates/ffi/src/lib.rs:29-42, 567-584).
 #include <chrono>
+#include <climits>
 #include <cinttypes>
 #include <cstdio>
 #include <cstdlib>
@@ -240,8 +241,15 @@ void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
     // rectify: one scalar per PSD cone, mean(e) (cones/psdtrianglecone.rs:252-255)
     std::vector<double> delta(m, 1.0);
     int row = 0;
-    for (int d : p.psd) {
-      int tn = d * (d + 1) / 2;
+    std::vector<std::pair<int, int>> cl = p.cones;
+    if (cl.empty())
+      for (int d : p.psd) cl.push_back({3, d});
+    for (const auto& c : cl) {
+      if (c.first != 3) {  // orthant rows keep their own scaling
+        row += c.second;
+        continue;
+      }
+      const int d = c.second, tn = d * (d + 1) / 2;
       double mean = 0.0;
       for (int i = row; i < row + tn; ++i) mean += eq.e[i];
       mean /= std::max(tn, 1);
@@ -391,10 +399,18 @@ std::unique_ptr<sdpx_handle> build_problem(const sdpx_csc* P, const sdpx_scalars
     if (c.reserved != 0 && c.kind != 8) invalid("nonzero cone reserved field");
     if (c.dim == 0) invalid("cone dimension must be positive");
     if (c.kind > 8) invalid("invalid cone kind/dimension/parameters");
-    if (c.kind != 3) unsupported("only PSD triangle cones (kind 3) run on the GPU path");
+    if (c.kind != 3 && c.kind != 1)
+      unsupported("only nonnegative (kind 1) and PSD triangle (kind 3) cones run on the GPU path");
     if (c.alpha.count != 0) invalid("unexpected cone alpha");
+    if (c.kind == 1) {
+      if (c.dim > (uint64_t)INT32_MAX) invalid("invalid cone kind/dimension/parameters");
+      p.cones.push_back({1, (int)c.dim});
+      rows += c.dim;
+      continue;
+    }
     if (c.dim > SDPXG_NMAX) unsupported("PSD cone order above 64 is not supported on the GPU path");
     p.psd.push_back((int)c.dim);
+    p.cones.push_back({3, (int)c.dim});
     rows += c.dim * (c.dim + 1) / 2;
   }
   if (rows != A->rows) invalid("cone dimensions do not match the rows of A");
@@ -408,6 +424,7 @@ std::unique_ptr<sdpx_handle> build_problem(const sdpx_csc* P, const sdpx_scalars
   h->orig.q = h->equil.q;
   h->orig.b = h->equil.b;
   h->orig.psd = h->equil.psd;
+  h->orig.cones = h->equil.cones;
   equilibrate(h->equil, h->settings, h->eq);
   const auto t2 = std::chrono::steady_clock::now();
   auto sec = [](auto a, auto b) { return std::chrono::duration<double>(b - a).count(); };

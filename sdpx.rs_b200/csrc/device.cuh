@@ -170,6 +170,19 @@ __global__ void k_reduce_partial(int, long, const double*, const double*, double
 __global__ void k_reduce_final(int, int, const double*, double*);
 __global__ void k_reduce_fused(int, long, const double*, const double*, double*, unsigned*, double*);
 __global__ void k_diag_absmax(const double*, int, double*);
+__global__ void k_nn_scale(int, const int*, const double*, const double*, double*, double*, uint32_t*);
+__global__ void k_nn_identity(int, double*, double*);
+__global__ void k_nn_cone(int, const int*, int, const double*, const double*, double*, long);
+__global__ void k_nn_circ(int, const int*, const double*, const double*, double*);
+__global__ void k_nn_lam_inv(int, const int*, const double*, const double*, double*);
+__global__ void k_nn_affine_ds(int, const int*, const double*, double*);
+__global__ void k_nn_shift(int, const int*, double*, double);
+__global__ void k_nn_step(int, const int*, const double*, const double*, const double*, const double*,
+                          double, int, double*);
+__global__ void k_nn_margins(int, const int*, const double*, double*);
+__global__ void k_nn_forward(int, int, const int*, const double*, const double*, double, double, double*);
+__global__ void k_nn_adjoint(int, int, const int*, const double*, const double*, double, double*);
+__global__ void k_nn_schur(int, int, const double*, const double*, double*);
 __global__ void k_csr_spmv(int, const int*, const int*, const double*, const double*, double,
                            double, double*);
 }
@@ -177,7 +190,7 @@ __global__ void k_csr_spmv(int, const int*, const int*, const double*, const dou
 // Kernel launches issued by this library in this process (every launch site increments it).
 inline std::atomic<uint64_t> g_launches{0};  // atomic: handles may run on many host threads
 
-enum RedOp { RED_DOT = 0, RED_SUMSQ = 1, RED_MAXABS = 2, RED_FINITE = 3 };
+enum RedOp { RED_DOT = 0, RED_SUMSQ = 1, RED_MAXABS = 2, RED_FINITE = 3, RED_NEGMAX = 4 };
 
 // Queues reductions into device scalar slots; fetch() copies them back in one transfer.
 class Reducer {
@@ -222,7 +235,7 @@ class Reducer {
   DevBuf<unsigned> counters_;  // arrival tickets of k_reduce_fused, one per slot (self-resetting)
   PinnedBuf<double> host_;
   int count_ = 0;
-  const double id_[4] = {0.0, 0.0, 0.0, 1.0};
+  const double id_[5] = {0.0, 0.0, 0.0, 1.0, 0.0};
 };
 
 }  // namespace sdpxg

@@ -147,6 +147,9 @@ struct HostProblem {
   std::vector<double> Aval;
   std::vector<double> q, b;
   std::vector<int> psd;  // PSD block orders in cone order
+  // all cones in order: (1, d) nonnegative orthant of dimension d, (3, d) PSD triangle of order d;
+  // empty means every cone is PSD (the orders in psd)
+  std::vector<std::pair<int, int>> cones;
 };
 
 // Cone operator modes of k_congruence.
@@ -175,6 +178,8 @@ class Engine {
   int nchol = 0;  // Schur tiles per side
   bool gram_enabled = true;  // rank-one blocks use the Gram form (SDPX_B200_GRAM=0 disables)
   int gram_blocks() const { return ngram_; }
+  int nn_count() const { return nnn_; }
+  std::vector<int> nn_rows;  // orthant rows of the stacked cone vector (cone order)
   std::vector<BlockDesc> hblocks;
   std::vector<int> hk;  // columns per block
   Reducer red;
@@ -303,19 +308,34 @@ class Engine {
     clear_graphs();
     n = p.n;
     m = p.m;
-    nblk = (int)p.psd.size();
     hblocks.clear();
-    int row = 0, mat = 0, vec = 0;
-    for (int d : p.psd) {
-      if (d > SDPXG_NMAX) throw std::invalid_argument("PSD block order above 64 is not supported");
-      hblocks.push_back({d, row, mat, vec});
-      row += d * (d + 1) / 2;
-      mat += d * d;
-      vec += d;
+    nn_rows.clear();
+    {
+      std::vector<std::pair<int, int>> cl = p.cones;
+      if (cl.empty())
+        for (int d : p.psd) cl.push_back({3, d});
+      int row = 0, mat = 0, vec = 0;
+      for (const auto& c : cl) {
+        if (c.first == 3) {
+          const int d = c.second;
+          if (d > SDPXG_NMAX) throw std::invalid_argument("PSD block order above 64 is not supported");
+          hblocks.push_back({d, row, mat, vec});
+          row += d * (d + 1) / 2;
+          mat += d * d;
+          vec += d;
+        } else if (c.first == 1) {
+          for (int i = 0; i < c.second; ++i) nn_rows.push_back(row + i);
+          row += c.second;
+        } else {
+          throw std::invalid_argument("cone kind not supported on the GPU path");
+        }
+      }
+      if (row != m) throw std::invalid_argument("cone rows do not match A");
+      matlen_ = mat;
+      veclen_ = vec;
     }
-    if (row != m) throw std::invalid_argument("cone rows do not match A");
-    matlen_ = mat;
-    veclen_ = vec;
+    nblk = (int)hblocks.size();
+    nnn_ = (int)nn_rows.size();
     // per-block dense column storage of A
     hk.assign(nblk, 0);
     std::vector<std::vector<int>> bcols(nblk);
@@ -541,9 +561,27 @@ class Engine {
       check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
       df_grid_ = std::max(1, std::min(std::max(per_sm, 1) * sms, df_items_));
     }
-    step_out_.alloc(2 * std::max(nblk, 1));
-    hblk_.alloc(2 * std::max(nblk, 1));
-    marg_out_.alloc(2 * std::max(nblk, 1));
+    step_out_.alloc(2 * (nblk + 1));
+    hblk_.alloc(2 * (nblk + 1));
+    {  // nonnegative-orthant rows: index list and their rows of A, dense (nnn x n)
+      nn_idx_.alloc(std::max(nnn_, 1));
+      nn_idx_.upload(nn_rows.data(), nn_rows.size(), st);
+      nnw_.alloc(std::max(nnn_, 1));
+      nnlam_.alloc(std::max(nnn_, 1));
+      std::vector<double> ann((size_t)nnn_ * n, 0.0);
+      if (nnn_) {
+        std::vector<int> pos(m, -1);
+        for (int i = 0; i < nnn_; ++i) pos[nn_rows[i]] = i;
+        for (int c = 0; c < n; ++c)
+          for (int64_t q = p.Acolptr[c]; q < p.Acolptr[c + 1]; ++q) {
+            const int r = (int)p.Arow[q];
+            if (pos[r] >= 0) ann[(size_t)pos[r] + (size_t)c * nnn_] = p.Aval[q];
+          }
+      }
+      Ann_.alloc(std::max<size_t>(ann.size(), 1));
+      Ann_.upload(ann.data(), ann.size(), st);
+    }
+    marg_out_.alloc(2 * (nblk + 1));
     scal_.alloc(4);
     check(cudaStreamSynchronize(st), "upload sync");
     const auto u3 = std::chrono::steady_clock::now();
@@ -564,6 +602,7 @@ class Engine {
   // ---- cone scaling ----
   void identity_scaling() {
     if (nblk) ++g_launches, k_identity_scaling<<<nblk, 256, 0, st>>>(blocks_, R_, Rinv_, Ginv_, lam_, lisqrt_);
+    if (nnn_) ++g_launches, k_nn_identity<<<(nnn_ + 255) / 256, 256, 0, st>>>(nnn_, nnw_, nnlam_);
   }
   bool nt_scale(const double* s, const double* z) {
     need(s, "nt_scale s");
@@ -573,6 +612,8 @@ class Engine {
     if (nblk)
       ++g_launches, k_nt_scale<<<nblk, SDPXG_CONE_THREADS, kSmemNt, st>>>(blocks_, s, z, R_, Rinv_, Ginv_, lam_,
                                                       lisqrt_, status_);
+    if (nnn_)
+      ++g_launches, k_nn_scale<<<(nnn_ + 255) / 256, 256, 0, st>>>(nnn_, nn_idx_, s, z, nnw_, nnlam_, status_);
     launched("k_nt_scale");
     tend(KT_SCALE);
     return read_status() == 0;
@@ -582,10 +623,14 @@ class Engine {
   void cone_apply(int mode, const double* x, double* y, int ncols = 1, long ld = 0) {
     need(x, "cone_apply x");
     need(y, "cone_apply y");
-    if (!nblk) return;
+    if (!nblk && !nnn_) return;
     tbegin(KT_CONE);
-    ++g_launches, k_congruence<<<dim3(nblk, ncols), SDPXG_CONE_THREADS, kSmemCong, st>>>(blocks_, mode, R_, Rinv_, x,
-                                                                      y, ld ? ld : m);
+    if (nblk)
+      ++g_launches, k_congruence<<<dim3(nblk, ncols), SDPXG_CONE_THREADS, kSmemCong, st>>>(
+          blocks_, mode, R_, Rinv_, x, y, ld ? ld : m);
+    if (nnn_)
+      ++g_launches, k_nn_cone<<<dim3((nnn_ + 255) / 256, ncols), 256, 0, st>>>(nnn_, nn_idx_, mode, nnw_, x,
+                                                                               y, ld ? ld : m);
     launched("k_congruence");
     tend(KT_CONE);
   }
@@ -594,20 +639,24 @@ class Engine {
     need(z, "circ z");
     need(x, "circ x");
     if (nblk) ++g_launches, k_circ_op<<<nblk, SDPXG_CONE_THREADS, kSmemCirc, st>>>(blocks_, y, z, x);
+    if (nnn_) ++g_launches, k_nn_circ<<<(nnn_ + 255) / 256, 256, 0, st>>>(nnn_, nn_idx_, y, z, x);
     launched("k_circ_op");
   }
   void lam_inv_circ(const double* z, double* x) {
     need(z, "lam_inv z");
     need(x, "lam_inv x");
     if (nblk) ++g_launches, k_lam_inv_circ<<<nblk, 256, 0, st>>>(blocks_, lam_, z, x);
+    if (nnn_) ++g_launches, k_nn_lam_inv<<<(nnn_ + 255) / 256, 256, 0, st>>>(nnn_, nn_idx_, nnlam_, z, x);
   }
   void affine_ds(double* ds) {
     need(ds, "affine_ds");
     if (nblk) ++g_launches, k_affine_ds<<<nblk, 256, 0, st>>>(blocks_, lam_, ds);
+    if (nnn_) ++g_launches, k_nn_affine_ds<<<(nnn_ + 255) / 256, 256, 0, st>>>(nnn_, nn_idx_, nnlam_, ds);
   }
   void shift_unit(double* v, double a) {
     need(v, "shift_unit");
     if (nblk) ++g_launches, k_shift_unit<<<nblk, 64, 0, st>>>(blocks_, v, a);
+    if (nnn_) ++g_launches, k_nn_shift<<<(nnn_ + 255) / 256, 256, 0, st>>>(nnn_, nn_idx_, v, a);
   }
   // per-block (dual, primal) bounds; returns false on an eigen failure
   bool step_bounds(const double* dz, const double* ds, double amax, int mode, double* az,
@@ -616,34 +665,43 @@ class Engine {
     need(ds, "step ds");
     *az = amax;
     *as = amax;
-    if (!nblk) return true;
+    if (!nblk && !nnn_) return true;
     clear_status();
     tbegin(KT_STEP);
-    ++g_launches, k_step_length<<<dim3(nblk, 2), SDPXG_CONE_THREADS, kSmemStep, st>>>(blocks_, R_, Rinv_, lisqrt_, dz,
-                                                                   ds, amax, mode, step_out_,
-                                                                   status_);
+    if (nblk)
+      ++g_launches, k_step_length<<<dim3(nblk, 2), SDPXG_CONE_THREADS, kSmemStep, st>>>(
+          blocks_, R_, Rinv_, lisqrt_, dz, ds, amax, mode, step_out_, status_);
+    if (nnn_)
+      ++g_launches, k_nn_step<<<1, 256, 0, st>>>(nnn_, nn_idx_, nnw_, nnlam_, dz, ds, amax, mode,
+                                                 step_out_.p + 2 * nblk);
     launched("k_step_length");
     tend(KT_STEP);
     const PinnedBuf<double>& h = hblk_;
-    copy_d2h(hblk_.p, step_out_.p, 2 * nblk * sizeof(double), st);
+    const int parts = nblk + (nnn_ ? 1 : 0);
+    copy_d2h(hblk_.p, step_out_.p, 2 * parts * sizeof(double), st);
     uint32_t s = read_status();
-    for (int j = 0; j < nblk; ++j) {
+    for (int j = 0; j < parts; ++j) {
       *az = std::min(*az, h[2 * j]);
       *as = std::min(*as, h[2 * j + 1]);
     }
     return s == 0;
   }
-  // (lambda_min, sum of positive eigenvalues) per block of v
+  // (lambda_min, sum of positive eigenvalues) per PSD block of v, then (min, sum of positive
+  // entries) over the orthant rows when there are any
   bool margins(const double* v, std::vector<double>& out) {
     need(v, "margins v");
-    out.assign(2 * nblk, 0.0);
-    if (!nblk) return true;
+    const int parts = nblk + (nnn_ ? 1 : 0);
+    out.assign(2 * parts, 0.0);
+    if (!parts) return true;
     clear_status();
-    ++g_launches, k_margins<<<dim3(nblk, 1), SDPXG_CONE_THREADS, kSmemMarg, st>>>(blocks_, v, m, marg_out_, status_);
+    if (nblk)
+      ++g_launches, k_margins<<<dim3(nblk, 1), SDPXG_CONE_THREADS, kSmemMarg, st>>>(blocks_, v, m, marg_out_,
+                                                                                    status_);
+    if (nnn_) ++g_launches, k_nn_margins<<<1, 256, 0, st>>>(nnn_, nn_idx_, v, marg_out_.p + 2 * nblk);
     launched("k_margins");
-    copy_d2h(hblk_.p, marg_out_.p, 2 * nblk * sizeof(double), st);
+    copy_d2h(hblk_.p, marg_out_.p, 2 * parts * sizeof(double), st);
     const bool ok = read_status() == 0;
-    for (int j = 0; j < 2 * nblk; ++j) out[j] = hblk_[j];
+    for (int j = 0; j < 2 * parts; ++j) out[j] = hblk_[j];
     return ok;
   }
 
@@ -652,6 +710,11 @@ class Engine {
   void A_forward(const double* x, double alpha, double beta, double* y) {
     need(x, "A_forward x");
     need(y, "A_forward y");
+    if (nnn_) {
+      ++g_launches, k_nn_forward<<<(nnn_ + 255) / 256, 256, 0, st>>>(nnn_, n, nn_idx_, Ann_, x, alpha, beta,
+                                                                     y);
+      launched("k_nn_forward");
+    }
     if (!nblk) return;
     if (nftile_) {
       ++g_launches, k_op_forward<<<dim3(nftile_, 1), 256, 0, st>>>(
@@ -684,6 +747,10 @@ class Engine {
       ++g_launches, k_op_adjoint_gather<<<dim3((n + 255) / 256, 1), 256, 0, st>>>(
           n, c2b_ptr_, c2b_blk_, c2b_loc_, col_ptr_, adj_part_, ncol_, alpha, beta, y, n);
       launched("k_op_adjoint_gather");
+    }
+    if (n && nnn_) {
+      ++g_launches, k_nn_adjoint<<<(n + 7) / 8, 256, 0, st>>>(nnn_, n, nn_idx_, Ann_, z, alpha, y);
+      launched("k_nn_adjoint");
     }
   }
   // y = alpha * P x + beta * y  (P symmetric)
@@ -727,6 +794,11 @@ class Engine {
     }
     if (pup_nnz_) {
       ++g_launches, k_add_upper_csc<<<(n + 255) / 256, 256, 0, st>>>(n, pup_ptr_, pup_row_, pup_val_, Hsave_);
+    }
+    if (nnn_ && n) {  // orthant rows: H += A_nn' diag(1 / w^2) A_nn
+      const unsigned t = (n + 31) / 32;
+      ++g_launches, k_nn_schur<<<dim3(t, t), 256, 0, st>>>(nnn_, n, Ann_, nnw_, Hsave_);
+      launched("k_nn_schur");
     }
     tend(KT_ASSEMBLE);
     int s = red.add(st, RED_FINITE, tot, Hsave_, nullptr);
@@ -850,6 +922,10 @@ class Engine {
   DevBuf<int> kcount_, col_ptr_, col_idx_, c2b_ptr_, c2b_blk_, c2b_loc_, wblk_, wloc_, tiles_;
   DevBuf<int> ftile_blk_, ftile_r0_;
   int nftile_ = 0;
+  // nonnegative-orthant rows
+  int nnn_ = 0;
+  DevBuf<int> nn_idx_;
+  DevBuf<double> nnw_, nnlam_, Ann_;
   // rank-one (Gram) blocks
   DevBuf<double> gU_, gV_, gsig_;
   DevBuf<long> gu_off_;

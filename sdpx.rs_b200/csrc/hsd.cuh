@@ -89,7 +89,8 @@ class HsdSolver {
       vn(*b);
     for (auto* b : {&s_, &z_, &ps_, &pz_, &rz_, &rzinf_, &z2_, &ds_, &dz_, &as_, &az_, &ts_, &tz_,
                     &prevs_, &prevz_, &bests_, &bestz_, &rhsz_, &rhss_, &cvec_, &workz_, &z1_,
-                    &tm_, &ez_, &cz_, &candz_, &ez2_, &wm1_, &wm2_, &wm3_, &b_, &e_, &einv_})
+                    &tm_, &ez_, &cz_, &candz_, &ez2_, &wm1_, &wm2_, &wm3_, &b_, &e_, &einv_, &nn_e_,
+                    &nn_einv_})
       vm(*b);
     load(p);
   }
@@ -111,6 +112,16 @@ class HsdSolver {
     einv_.upload(eq.einv.data(), m, E.st);
     degree_ = 0;
     for (int d : p.psd) degree_ += d;
+    degree_ += E.nn_count();  // an orthant of dimension d has degree d
+    {  // original-coordinate scales of the orthant rows (zero on PSD rows: a row mask)
+      std::vector<double> ne(m, 0.0), nei(m, 0.0);
+      for (int r : E.nn_rows) {
+        ne[r] = eq.e[r];
+        nei[r] = eq.einv[r];
+      }
+      nn_e_.upload(ne.data(), m, E.st);
+      nn_einv_.upload(nei.data(), m, E.st);
+    }
     // scaled norms of the data (default/problemdata.rs:444-465)
     normq_ = 0;
     for (int i = 0; i < n; ++i) normq_ = std::max(normq_, std::fabs(p.q[i] * eq.dinv[i]));
@@ -183,7 +194,7 @@ class HsdSolver {
       xhat_, en_, dxn_, candn_, e2n_, ex_, cx_, candx_, ex2_, negq_, q_, d_, dinv_, wn_;
   DevBuf<double> s_, z_, ps_, pz_, rz_, rzinf_, z2_, ds_, dz_, as_, az_, ts_, tz_, prevs_, prevz_,
       bests_, bestz_, rhsz_, rhss_, cvec_, workz_, z1_, tm_, ez_, cz_, candz_, ez2_, wm1_, wm2_, wm3_,
-      b_, e_, einv_;
+      b_, e_, einv_, nn_e_, nn_einv_;
 };
 
 // ------------------------------------------------------------------------------------------
@@ -526,6 +537,14 @@ inline double HsdSolver::original_ratio(bool reduced) {
     prim = std::max(prim, std::max(0.0, -ms[2 * j]) * tinv / ej);
     dual = std::max(dual, std::max(0.0, -mz[2 * j]) * tinv * cinv * ej);
   }
+  if (E.nn_count()) {  // orthant rows, entrywise in original coordinates
+    int ra = E.red.add(st(), RED_NEGMAX, m, wm1_, nn_einv_);
+    int rb = E.red.add(st(), RED_NEGMAX, m, s_, nn_einv_);
+    int rc = E.red.add(st(), RED_NEGMAX, m, z_, nn_e_);
+    auto& hn = E.red.fetch(st());
+    prim = std::max(prim, std::max(hn[ra], hn[rb]) * tinv);
+    dual = std::max(dual, hn[rc] * tinv * cinv);
+  }
   prim /= (1.0 + normb_);
   dual /= (1.0 + normq_);
   double gap_abs = std::fabs(info.cost_primal - info.cost_dual);
@@ -628,9 +647,9 @@ inline bool HsdSolver::default_start() {
       std::vector<double> mg;
       if (!E.margins(v, mg)) return false;
       double mn = std::numeric_limits<double>::max(), pos = 0.0;
-      for (int j = 0; j < E.nblk; ++j) {
-        mn = std::min(mn, mg[2 * j]);
-        pos += mg[2 * j + 1];
+      for (size_t j = 0; j + 1 < mg.size(); j += 2) {  // PSD blocks, then the orthant rows
+        mn = std::min(mn, mg[j]);
+        pos += mg[j + 1];
       }
       double target = std::max(1.0, (pos * 0.1) / std::max(degree_, 1));
       if (mn <= 0) {

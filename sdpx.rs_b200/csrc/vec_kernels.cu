@@ -19,7 +19,8 @@ extern "C" __global__ void k_lincomb(long n, double a, const double* x, double b
 }
 
 // op 0: sum x*y;  op 1: sum (x*y)^2 (scaled 2-norm squared, y = scales or null);
-// op 2: max |x*y|;  op 3: all finite (1.0 / 0.0) of x
+// op 2: max |x*y|;  op 3: all finite (1.0 / 0.0) of x;  op 4: max(0, max -x*y) (y >= 0: a
+// nonnegative scale, or a mask that selects rows)
 __device__ __forceinline__ double red_elem(int op, const double* x, const double* y, long i) {
   double xv = x[i];
   double yv = y ? y[i] : 1.0;
@@ -27,12 +28,13 @@ __device__ __forceinline__ double red_elem(int op, const double* x, const double
     case 0: return xv * yv;
     case 1: { double t = xv * yv; return t * t; }
     case 2: return fabs(xv * yv);
+    case 4: return fmax(0.0, -(xv * yv));
     default: return isfinite(xv) ? 1.0 : 0.0;
   }
 }
 
 __device__ __forceinline__ double red_combine(int op, double a, double b) {
-  if (op == 2) return fmax(a, b);
+  if (op == 2 || op == 4) return fmax(a, b);
   if (op == 3) return fmin(a, b);
   return a + b;
 }

@@ -200,6 +200,31 @@ def batch_sdps(count: int, seed: int = 0, nrange=(8, 64), mrange=(20, 300)) -> L
     return out
 
 
+def conic_qp(seed: int = 0, n: int = 200, n_nn: int = 150, psd: int = 20, rank: int = 50) -> ConicProblem:
+    """Conic QP of the differentiation workload: min 1/2 x'Px + q'x s.t. b - Ax in K.
+
+    x in R^n; P = L L' + 0.1 I with L (n x rank) iid N(0, 1/rank); q ~ N(0, 1); K = the
+    nonnegative orthant of dimension n_nn followed by one PSD triangle cone of order psd;
+    A (n_nn + tri(psd) x n) iid N(0, 1/sqrt(n)); x0 ~ N(0, 1); s0 strictly interior (orthant
+    entries 1, PSD part svec(I)); b = A x0 + s0.  The second argument of N(., .) is the
+    variance for both L and A.  A loss target t ~ N(0, 1)^n is stored in meta["t"].
+    """
+    rng = np.random.default_rng(seed)
+    L = rng.standard_normal((n, rank)) * np.sqrt(1.0 / rank)
+    Pm = L @ L.T + 0.1 * np.eye(n)
+    q = rng.standard_normal(n)
+    rows = n_nn + tri(psd)
+    A = rng.standard_normal((rows, n)) * np.sqrt(1.0 / np.sqrt(n))
+    x0 = rng.standard_normal(n)
+    s0 = np.concatenate([np.ones(n_nn), svec(np.eye(psd))])
+    b = A @ x0 + s0
+    t = rng.standard_normal(n)
+    return ConicProblem(P=sp.csc_matrix(Pm), q=q, A=sp.csc_matrix(A), b=b,
+                        cones=[("nonneg", n_nn), ("psd", psd)],
+                        name=f"conic_qp_n{n}_nn{n_nn}_psd{psd}_s{seed}",
+                        meta={"seed": seed, "t": t, "x0": x0})
+
+
 def basic_projection_sdp() -> ConicProblem:
     """Known-answer projection problem: min 1/2|x|^2 s.t. b - x in PSD(3).
 

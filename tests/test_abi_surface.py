@@ -96,7 +96,7 @@ def test_rejects_nonfinite_and_bad_csc():
         DefaultSolver(P, q, A, b, [("psd", 3)])  # 6 rows expected, 3 given
     assert e.value.code == 1
     with pytest.raises(_lib.SdpxError) as e:
-        DefaultSolver(P, q, A, b, [("nonneg", 3)])
+        DefaultSolver(P, q, A, b, [("soc", 3)])  # second-order cones are not on the GPU path
     assert e.value.code == 2
     with pytest.raises(_lib.SdpxError) as e:
         DefaultSolver(P, q, A, np.ones(2), cones)
