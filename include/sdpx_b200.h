@@ -140,6 +140,15 @@ int32_t sdpx_b200_transfer_bytes(uint64_t *h2d, uint64_t *d2h);
 int32_t sdpx_b200_reprepare(sdpx_handle *handle, const sdpx_csc *P, const sdpx_scalars *q,
                             const sdpx_csc *A, const sdpx_scalars *b, const sdpx_cone *cones,
                             uint64_t cone_count, const sdpx_settings *settings);
+/* Gradients of a loss L(x, z, s) of the solution with respect to the data: given dl_dx (n) and
+ * optionally dl_dz, dl_ds (m; NULL = zero), writes dq (n), db (m) and, when dA is not NULL, dA
+ * (nnz values on the sparsity pattern of the A passed to prepare, in its CSC order).  One solve
+ * of the KKT system [P A'; A -Hs] re-factored at the NT scaling of the solution, on the device
+ * (dq = -u, db = v, dA = -(z u' + v x') with [u; v] = K^-1 [dl_dx; dl_dz - Hs dl_ds]).  Requires
+ * a Solved or AlmostSolved result (else 7).  The reference has no differentiation; this is the
+ * adjoint of its own KKT system. */
+int32_t sdpx_b200_adjoint(sdpx_handle *handle, const double *dl_dx, const double *dl_dz,
+                          const double *dl_ds, double *dq, double *db, double *dA, uint64_t nnz);
 /* Capture the KKT solve's straight runs as CUDA graphs and replay them (on != 0, the default
  * unless SDPX_B200_GRAPHS=0) or launch them eagerly (on == 0); results are bitwise the same.
  * Capture pays off over the many solves of one problem; a handle re-prepared for every small

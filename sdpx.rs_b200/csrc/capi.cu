@@ -660,6 +660,37 @@ int32_t sdpx_b200_kernel_times(sdpx_handle* h, double* ms, uint64_t* counts) {
   });
 }
 
+int32_t sdpx_b200_adjoint(sdpx_handle* h, const double* dl_dx, const double* dl_dz,
+                          const double* dl_ds, double* dq, double* db, double* dA, uint64_t nnz) {
+  return boundary([&] {
+    if (!dl_dx || !dq || !db) invalid("null pointer");
+    operate(h, [&](sdpx_handle& hh) {
+      if (!hh.solved || !hh.hsd) throw AbiError{7, "no result: solve the handle first"};
+      const int st = (int)hh.info.status;
+      if (st != ST_SOLVED && st != ST_ALMOST_SOLVED)
+        throw AbiError{7, "no optimal solution to differentiate (status " + std::to_string(st) + ")"};
+      const int n = hh.orig.n, m = hh.orig.m;
+      const HostProblem& p = hh.equil;  // same sparsity pattern as the input A
+      if (dA && nnz != (uint64_t)p.Aval.size()) invalid("dA needs one value per stored entry of A");
+      std::vector<double> gx(dl_dx, dl_dx + n), gz(m, 0.0), gs(m, 0.0), u, v;
+      if (dl_dz) gz.assign(dl_dz, dl_dz + m);
+      if (dl_ds) gs.assign(dl_ds, dl_ds + m);
+      for (double t : gx)
+        if (!std::isfinite(t)) invalid("nonfinite input");
+      if (!hh.hsd->adjoint(gx, gz, gs, u, v))
+        throw AbiError{5, "adjoint: the KKT system at the solution could not be factored or solved"};
+      for (int j = 0; j < n; ++j) dq[j] = -u[j];
+      for (int i = 0; i < m; ++i) db[i] = v[i];
+      if (dA)
+        for (int j = 0; j < n; ++j)
+          for (int64_t q = p.Acolptr[j]; q < p.Acolptr[j + 1]; ++q) {
+            const int64_t i = p.Arow[q];
+            dA[q] = -(hh.z[i] * u[j] + v[i] * hh.x[j]);
+          }
+    });
+  });
+}
+
 int32_t sdpx_b200_set_graphs(sdpx_handle* h, int32_t on) {
   return boundary([&] {
     operate(h, [&](sdpx_handle& hh) {

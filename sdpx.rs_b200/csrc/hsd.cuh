@@ -141,6 +141,10 @@ class HsdSolver {
   std::vector<double> hx, hs, hz;  // unscaled solution
 
   void solve();
+  // (u, v) = K^-1 [gx; gz - Hs gs] in original coordinates, K = [P A'; A -Hs] re-factored at the
+  // NT scaling of the final point (the solution's sensitivities; see sdpx_b200_adjoint).
+  bool adjoint(const std::vector<double>& gx, const std::vector<double>& gz,
+               const std::vector<double>& gs, std::vector<double>& u, std::vector<double>& v);
 
   // ---------------- KKT system (also driven directly by the kernel-level ABI) ----------------
   bool kkt_update();
@@ -885,6 +889,157 @@ inline void HsdSolver::solve() {
     hz[i] = hz[i] * eq_.e[i] * tinv / eq_.c;
   }
   info.solve_time = secs(tstart);
+}
+
+// Cyclic Jacobi eigen-decomposition of a small symmetric matrix (host, n <= 64, column-major):
+// A = Q diag(w) Q'.  Used once per adjoint call per PSD block.
+inline void host_sym_eig(int n, std::vector<double> A, std::vector<double>& Q, std::vector<double>& w) {
+  Q.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) Q[i + (size_t)i * n] = 1.0;
+  auto a = [&](int i, int j) -> double& { return A[i + (size_t)j * n]; };
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, tot = 0.0;
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        tot += a(i, j) * a(i, j);
+        if (i != j) off += a(i, j) * a(i, j);
+      }
+    if (off <= 1e-30 * tot) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = a(p, q);
+        if (apq == 0.0) continue;
+        const double theta = (a(q, q) - a(p, p)) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+        for (int k = 0; k < n; ++k) {  // A <- J' A J
+          const double akp = a(k, p), akq = a(k, q);
+          a(k, p) = c * akp - sn * akq;
+          a(k, q) = sn * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double apk = a(p, k), aqk = a(q, k);
+          a(p, k) = c * apk - sn * aqk;
+          a(q, k) = sn * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double qkp = Q[k + (size_t)p * n], qkq = Q[k + (size_t)q * n];
+          Q[k + (size_t)p * n] = c * qkp - sn * qkq;
+          Q[k + (size_t)q * n] = sn * qkp + c * qkq;
+        }
+      }
+  }
+  w.resize(n);
+  for (int i = 0; i < n; ++i) w[i] = a(i, i);
+}
+
+// Adjoint of the solution map.  At a strictly complementary solution, perturbing (q, b, A) moves
+// (x, z, s) along
+//   [P A'; A -Hs] [dx; dz] = [-dq - dA' z; db - dA x],  ds = -Hs dz,
+// with Hs the limit of the NT scaling as the iterates approach the solution (the KKT rows plus
+// the linearised complementarity, the system the last iterations solved).  For a loss with
+// gradients (gx, gz, gs) the one solve K [u; v] = [gx; gz - Hs gs] gives dL/dq = -u,
+// dL/db = v, dL/dA = -(z u' + v x').
+// The final iterate's own scaling is too close to that limit to solve with (entries of Hs span
+// ~1e20 at gap 1e-10: the solve loses most digits), so the system is formed at the solution
+// re-centred on the central path at a small relative mu: per PSD block, S - Z = Q diag(l) Q'
+// (complementary ranges), S_c = Q diag(l+ or d |l|) Q', Z_c = Q diag(l- or d |l|) Q' with
+// d = 1e-9 relative to the block scale; per orthant row the smaller of (s, z) becomes d times
+// the larger.  That keeps the O(d) bias of the linearisation and a Schur conditioning of ~1/d.
+// The solve runs on the equilibrated engine: with x = D xb / tau, s = E^-1 sb / tau,
+// z = E zb / (c tau), Kb [ub; vb] = [D gx; E gz / c - Hb (E^-1 gs)] and u = c D ub, v = E vb.
+inline bool HsdSolver::adjoint(const std::vector<double>& gx, const std::vector<double>& gz,
+                               const std::vector<double>& gs, std::vector<double>& u,
+                               std::vector<double>& v) {
+  const int n = n_, m = m_;
+  const double tinv = 1.0 / tau_, rel = 1e-9;
+  std::vector<double> sb(m), zb(m);
+  copy_d2h(sb.data(), s_.p, m * sizeof(double), st());
+  copy_d2h(zb.data(), z_.p, m * sizeof(double), st());
+  check(cudaStreamSynchronize(st()), "adjoint sync");
+  for (int i = 0; i < m; ++i) {
+    sb[i] *= tinv;
+    zb[i] *= tinv;
+  }
+  std::vector<double> sc(sb), zc(zb);
+  for (const BlockDesc& bd : E.hblocks) {  // PSD blocks: re-centre in the eigenbasis of S - Z
+    const int nb = bd.n;
+    std::vector<double> X((size_t)nb * nb), Q, w;
+    auto at = [&](const std::vector<double>& v, int i, int j) {
+      const int a = std::min(i, j), b = std::max(i, j);
+      const double x = v[bd.svec_off + b * (b + 1) / 2 + a];
+      return a == b ? x : x * SDPXG_RSQRT2;
+    };
+    for (int j = 0; j < nb; ++j)
+      for (int i = 0; i < nb; ++i) X[i + (size_t)j * nb] = at(sb, i, j) - at(zb, i, j);
+    host_sym_eig(nb, X, Q, w);
+    double scale = 0.0;
+    for (double l : w) scale = std::max(scale, std::fabs(l));
+    if (!(scale > 0.0)) scale = 1.0;
+    std::vector<double> ls(nb), lz(nb);
+    for (int i = 0; i < nb; ++i) {
+      const double l = std::fabs(w[i]) > rel * scale ? w[i] : (w[i] >= 0 ? rel * scale : -rel * scale);
+      if (l > 0) {
+        ls[i] = l;
+        lz[i] = rel * scale * scale / l;
+      } else {
+        lz[i] = -l;
+        ls[i] = rel * scale * scale / (-l);
+      }
+    }
+    for (int j = 0; j < nb; ++j)
+      for (int i = 0; i <= j; ++i) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < nb; ++k) {
+          const double qq = Q[i + (size_t)k * nb] * Q[j + (size_t)k * nb];
+          a += qq * ls[k];
+          b += qq * lz[k];
+        }
+        const double f = (i == j) ? 1.0 : SDPXG_SQRT2;
+        sc[bd.svec_off + j * (j + 1) / 2 + i] = a * f;
+        zc[bd.svec_off + j * (j + 1) / 2 + i] = b * f;
+      }
+  }
+  for (int r : E.nn_rows) {  // orthant rows: the smaller partner becomes rel x the larger
+    const double big = std::max(std::fabs(sb[r]), std::fabs(zb[r]));
+    if (!(big > 0.0)) return false;
+    if (sb[r] >= zb[r]) {
+      sc[r] = big;
+      zc[r] = rel * big;
+    } else {
+      zc[r] = big;
+      sc[r] = rel * big;
+    }
+  }
+  ts_.upload(sc.data(), m, st());
+  tz_.upload(zc.data(), m, st());
+  if (!E.nt_scale(ts_, tz_)) return false;
+  reg_boost_ = 0;
+  if (!kkt_update()) return false;
+  std::vector<double> bx(n), bz(m), gsi(m);
+  for (int i = 0; i < n; ++i) bx[i] = eq_.d[i] * gx[i];
+  for (int i = 0; i < m; ++i) {
+    bz[i] = eq_.e[i] * gz[i] / eq_.c;
+    gsi[i] = eq_.einv[i] * gs[i];
+  }
+  rhsx_.upload(bx.data(), n, st());
+  rhsz_.upload(bz.data(), m, st());
+  wm1_.upload(gsi.data(), m, st());
+  E.cone_apply(CM_HS, wm1_, wm2_);
+  E.lincomb(m, 1.0, rhsz_, -1.0, wm2_, 0.0, nullptr, rhsz_);
+  if (!kkt_solve(rhsx_, rhsz_, x1_, z1_)) return false;
+  u.resize(n);
+  v.resize(m);
+  copy_d2h(u.data(), x1_.p, n * sizeof(double), st());
+  copy_d2h(v.data(), z1_.p, m * sizeof(double), st());
+  check(cudaStreamSynchronize(st()), "adjoint sync");
+  for (int i = 0; i < n; ++i) u[i] *= eq_.c * eq_.d[i];
+  for (int i = 0; i < m; ++i) v[i] *= eq_.e[i];
+  for (double t : u)
+    if (!std::isfinite(t)) return false;
+  for (double t : v)
+    if (!std::isfinite(t)) return false;
+  return true;
 }
 
 }  // namespace sdpxg

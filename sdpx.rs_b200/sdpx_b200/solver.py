@@ -218,6 +218,21 @@ class DefaultSolver:
         self._b = np.ascontiguousarray(b, dtype=np.float64)
         _lib.call("sdpx_update", self._h, C.byref(_scalars(self._q)), C.byref(_scalars(self._b)))
 
+    def adjoint(self, dl_dx, dl_dz=None, dl_ds=None):
+        """Gradients of a loss of the last solution: returns (dq, db, dA) with dA a CSC matrix on
+        the sparsity pattern of A (sdpx_b200_adjoint)."""
+        gx = np.ascontiguousarray(dl_dx, dtype=np.float64)
+        gz = None if dl_dz is None else np.ascontiguousarray(dl_dz, dtype=np.float64)
+        gs = None if dl_ds is None else np.ascontiguousarray(dl_ds, dtype=np.float64)
+        dq, db = np.empty(self.n), np.empty(self.m)
+        nnz = int(self._A.values.size)
+        dA = np.empty(nnz)
+        _lib.call("sdpx_b200_adjoint", self._h, dptr(gx), dptr(gz), dptr(gs), dptr(dq), dptr(db),
+                  dptr(dA), nnz)
+        A = sp.csc_matrix((dA, self._A.rowval.astype(np.int64), self._A.colptr.astype(np.int64)),
+                          shape=(self.m, self.n))
+        return dq, db, A
+
     def set_graphs(self, on: bool):
         """Replay the KKT solve's captured CUDA graphs (default) or launch eagerly."""
         _lib.call("sdpx_b200_set_graphs", self._h, int(bool(on)))
