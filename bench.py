@@ -356,7 +356,7 @@ def run_batch(args, world, rank, local):
     from sdpx_b200 import problems as Pm
     from sdpx_b200.solver import BatchSolver, DefaultSettings
 
-    count = args.instances
+    count = args.instances or 4096
     probs = Pm.batch_sdps(count, seed=1000 * rank)  # replicas: each rank its own instances
     settings = DefaultSettings(kkt_form="condensed")
     bs = BatchSolver(workers=args.workers, settings=settings)
@@ -374,7 +374,8 @@ def run_batch(args, world, rank, local):
     for s_ in sols:
         statuses[s_.status] = statuses.get(s_.status, 0) + 1
     # accuracy against the oracle on a bounded, evenly spaced sample
-    sample = list(range(0, count, max(1, count // args.oracle_sample)))[: args.oracle_sample]
+    ns = args.oracle_sample or 32
+    sample = list(range(0, count, max(1, count // ns)))[:ns]
     obj_err, x_err = [], []
     t1 = time.perf_counter()
     for i in sample:
@@ -404,6 +405,82 @@ def run_batch(args, world, rank, local):
     return 0
 
 
+ADJOINT_METRIC = ("instances/s, solve to gap 1e-8 plus the adjoint of 1/2|x*-t|^2 w.r.t. q, b, A "
+                  "(Float64), batch of conic QPs")
+
+
+def run_adjoint(args, world, rank, local):
+    """Differentiation workload: conic QPs x in R^200, P = LL' + 0.1 I (L 200 x 50), 150 orthant
+    rows and one 20 x 20 PSD block, loss 1/2 |x* - t|^2.  Each timed step solves the whole batch
+    from host buffers through BatchSolver and, on the same handle after each solve, computes
+    dL/dq, dL/db, dL/dA (the KKT system re-factored at the re-centred solution).  Gradients are
+    checked on an evenly spaced sample against the oracle's dense FP64 KKT solve at the same
+    solution; the CPU baseline is the oracle's solve plus that adjoint."""
+    import numpy as np
+    import torch
+    os.environ["SDPX_B200_DEVICE"] = str(local)
+    torch.cuda.set_device(local)
+    from oracle import adjoint as oracle_adjoint
+    from oracle import ipm
+    from sdpx_b200 import problems as Pm
+    from sdpx_b200.solver import BatchSolver, DefaultSettings
+
+    count = args.instances or 256
+    probs = [Pm.conic_qp(1000 * rank + i) for i in range(count)]
+    settings = DefaultSettings(kkt_form="condensed")
+    bs = BatchSolver(workers=args.workers, settings=settings)
+
+    def grad(i, sol):
+        return sol.x - probs[i].meta["t"]
+
+    for _ in range(args.warmup):
+        bs.solve_adjoint(probs[: min(count, 2 * args.workers)], grad)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sols, grads = bs.solve_adjoint(probs, grad)
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / args.steps
+    wall = max_over_ranks(world, wall)
+    statuses = {}
+    for s_ in sols:
+        statuses[s_.status] = statuses.get(s_.status, 0) + 1
+    ns = args.oracle_sample or 16
+    sample = list(range(0, count, max(1, count // ns)))[:ns]
+    errs, cpu_t = [], 0.0
+    for i in sample:
+        if grads[i] is None:
+            continue
+        g, (dq, db, dA) = sols[i], grads[i]
+        rq, rb, rA = oracle_adjoint.adjoint(probs[i], g.x, g.s, g.z, g.x - probs[i].meta["t"])
+        scale = max(float(np.max(np.abs(rq))), float(np.max(np.abs(rb))), 1.0)
+        errs.append(max(float(np.max(np.abs(dq - rq))), float(np.max(np.abs(db - rb)))) / scale)
+        t1 = time.perf_counter()
+        o = ipm.solve(probs[i])
+        oracle_adjoint.adjoint(probs[i], o.x, o.s, o.z, o.x - probs[i].meta["t"])
+        cpu_t += time.perf_counter() - t1
+    if rank == 0:
+        line = {"metric": ADJOINT_METRIC, "value": world * count / wall, "unit": "instances/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": wall * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"{count} conic QPs n=200, P=LL'+0.1I (L 200x50), 150 orthant "
+                                       "rows + 20x20 PSD, seed+index, gap 1e-8, adjoint of "
+                                       "1/2|x*-t|^2", "workers": args.workers,
+                           "parallelism": f"replicas{world}"},
+                "statuses": statuses,
+                "gradient_vs_oracle": {"sample": len(errs),
+                                       "rel_p50": float(np.percentile(errs, 50)) if errs else None,
+                                       "rel_max": float(np.max(errs)) if errs else None},
+                "cpu_baseline": {"value": len(errs) / cpu_t if cpu_t else None,
+                                 "unit": "instances/s", "cores": os.cpu_count(), "kind": "port",
+                                 "sample": f"oracle solve + dense FP64 KKT adjoint on {len(errs)} "
+                                           "instances of the batch"}}
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -411,13 +488,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--workload", default="rank1", choices=["rank1", "batch"],
+    ap.add_argument("--workload", default="rank1", choices=["rank1", "batch", "adjoint"],
                     help="rank1: the 32-block bootstrap SDP (default line); batch: independent "
-                         "small SDPs, instances/s")
-    ap.add_argument("--instances", type=int, default=4096, help="batch workload: instances")
+                         "small SDPs, instances/s; adjoint: conic QPs solved and differentiated")
+    ap.add_argument("--instances", type=int, default=None,
+                    help="batch workloads: instances (default 4096 for batch, 256 for adjoint)")
     ap.add_argument("--workers", type=int, default=16, help="batch workload: worker handles")
-    ap.add_argument("--oracle-sample", type=int, default=32,
-                    help="batch workload: instances checked against the oracle")
+    ap.add_argument("--oracle-sample", type=int, default=None,
+                    help="batch workloads: instances checked against the oracle (default 32 for "
+                         "batch, 16 for adjoint)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:
@@ -425,6 +504,8 @@ def main():
             rc = run_reference(args, world, rank)
         elif args.workload == "batch":
             rc = run_batch(args, world, rank, local)
+        elif args.workload == "adjoint":
+            rc = run_adjoint(args, world, rank, local)
         else:
             rc = run_ours(args, world, rank, local)
     finally:

@@ -143,8 +143,10 @@ int32_t sdpx_b200_reprepare(sdpx_handle *handle, const sdpx_csc *P, const sdpx_s
 /* Gradients of a loss L(x, z, s) of the solution with respect to the data: given dl_dx (n) and
  * optionally dl_dz, dl_ds (m; NULL = zero), writes dq (n), db (m) and, when dA is not NULL, dA
  * (nnz values on the sparsity pattern of the A passed to prepare, in its CSC order).  One solve
- * of the KKT system [P A'; A -Hs] re-factored at the NT scaling of the solution, on the device
- * (dq = -u, db = v, dA = -(z u' + v x') with [u; v] = K^-1 [dl_dx; dl_dz - Hs dl_ds]).  Requires
+ * of the KKT system [P A'; A -Hs] re-factored on the device at the NT scaling of the solution
+ * moved onto the central path at relative mu 1e-9 in the equilibrated coordinates (per PSD block
+ * in the eigenbasis of S - Z; per orthant row the smaller of s_i, z_i at 1e-9 of the larger):
+ * dq = -u, db = v, dA = -(z u' + v x') with [u; v] = K^-1 [dl_dx; dl_dz - Hs dl_ds].  Requires
  * a Solved or AlmostSolved result (else 7).  The reference has no differentiation; this is the
  * adjoint of its own KKT system. */
 int32_t sdpx_b200_adjoint(sdpx_handle *handle, const double *dl_dx, const double *dl_dz,

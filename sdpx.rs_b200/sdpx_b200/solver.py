@@ -272,10 +272,20 @@ class BatchSolver:
         self._solvers: List[Optional[DefaultSolver]] = [None] * self.workers
 
     def solve(self, problems) -> List[Solution]:
+        return self._run(problems, None)[0]
+
+    def solve_adjoint(self, problems, grad) -> Tuple[List[Solution], list]:
+        """Solve every problem and, on the same handle right after its solve, the adjoint of a
+        loss with dL/dx = grad(index, solution): per instance (dq, db, dA) as
+        ``DefaultSolver.adjoint`` returns them (None where the solve did not succeed)."""
+        return self._run(problems, grad)
+
+    def _run(self, problems, grad):
         import threading
         from concurrent.futures import ThreadPoolExecutor
         problems = list(problems)
         out: List[Optional[Solution]] = [None] * len(problems)
+        grads: list = [None] * len(problems)
         lock = threading.Lock()
         nxt = [0]
 
@@ -294,12 +304,15 @@ class BatchSolver:
                     self._solvers[w] = s
                 else:
                     s.reprepare(p.P, p.q, p.A, p.b, p.cones, self.settings)
-                out[i] = s.solve()
+                sol = s.solve()
+                out[i] = sol
+                if grad is not None and sol.status in ("Solved", "AlmostSolved"):
+                    grads[i] = s.adjoint(grad(i, sol))
 
         with ThreadPoolExecutor(self.workers) as ex:
             for f in [ex.submit(work, w) for w in range(self.workers)]:
                 f.result()
-        return out
+        return out, grads
 
 
 def solve_problem(prob, settings: Optional[DefaultSettings] = None) -> DefaultSolver:

@@ -4,18 +4,19 @@ Checks, on conic QPs of the differentiation workload (orthant rows + one PSD blo
   * against central finite differences of L along random directions in (q, b, A), solving to
     gap 1e-10 with h = 1e-5: relative error of the directional derivative <= 1e-3 (an SDP's x is
     accurate to roughly the square root of the gap tolerance, so the step stays well above that);
-  * against a dense FP64 solve of the reference's KKT system [P A'; A -Hs], with Hs the
-    oracle's NT scaling at the solution re-centred as the library does (eigenbasis of S - Z per
-    PSD block, the smaller partner of each orthant pair at 1e-9 x the larger): dq, db, dA within
-    1e-5 relative;
+  * against the oracle's dense FP64 solve of the reference's KKT system [P A'; A -Hs]
+    (oracle/adjoint.py), Hs the NT scaling at the solution re-centred as the library does
+    (eigenbasis of S - Z per PSD block, the smaller partner of each orthant pair at 1e-9 x the
+    larger, in the equilibrated coordinates): dq, db, dA within 1e-6 relative;
   * through a torch.autograd.Function wrapper (a thin harness that lives in this test only):
-    loss.backward() delivers the library's adjoint unchanged.
+    loss.backward() delivers the library's adjoint unchanged;
+  * through BatchSolver.solve_adjoint: bitwise the single-handle gradients.
 """
 import numpy as np
 import pytest
 import scipy.sparse as sp
 
-from oracle import ipm
+from oracle import adjoint as oracle_adjoint
 from sdpx_b200 import problems as P
 from sdpx_b200.solver import DefaultSettings, DefaultSolver
 
@@ -60,67 +61,18 @@ def test_directional_derivatives_match_finite_differences(seed):
         assert abs(analytic - fd) <= 1e-3 * max(1.0, abs(fd)), (analytic, fd)
 
 
-def _recentre(prob, s, z, rel=1e-9):
-    """The solution moved onto the central path at a small relative mu (the adjoint's point)."""
-    sc, zc, r = s.copy(), z.copy(), 0
-    for kind, d in prob.cones:
-        if kind == "nonneg":
-            for i in range(r, r + d):
-                big = max(abs(s[i]), abs(z[i]))
-                if s[i] >= z[i]:
-                    sc[i], zc[i] = big, rel * big
-                else:
-                    sc[i], zc[i] = rel * big, big
-            r += d
-        else:
-            k = d * (d + 1) // 2
-            w, Q = np.linalg.eigh(P.smat(s[r:r + k], d) - P.smat(z[r:r + k], d))
-            sc_ = np.abs(w).max()
-            ls = np.where(w > 0, w, rel * sc_ * sc_ / np.abs(w))
-            lz = np.where(w > 0, rel * sc_ * sc_ / np.abs(w), -w)
-            sc[r:r + k] = P.svec(Q @ np.diag(ls) @ Q.T)
-            zc[r:r + k] = P.svec(Q @ np.diag(lz) @ Q.T)
-            r += k
-    return sc, zc
-
-
-def _dense_hs(prob, s, z):
-    """Hs of the oracle's NT scaling at (s, z), block diagonal over the cones (svec coordinates)."""
-    cones = ipm.make_cones(prob.cones)
-    blocks, r = [], 0
-    for c in cones:
-        k = c.numel
-        assert c.update_scaling(s[r:r + k], z[r:r + k])
-        blocks.append(np.column_stack([c.mul_Hs(e) for e in np.eye(k)]))
-        r += k
-    out = np.zeros((r, r))
-    o = 0
-    for B in blocks:
-        out[o:o + B.shape[0], o:o + B.shape[0]] = B
-        o += B.shape[0]
-    return out
-
-
 @pytest.mark.parametrize("kw", [dict(n=20, n_nn=15, psd=4, rank=5), dict()])
 def test_adjoint_matches_dense_fp64_kkt_solve(kw):
     prob = P.conic_qp(2, **kw)
     t = prob.meta["t"]
     s, sol = _solve(prob)
     dq, db, dA = s.adjoint(sol.x - t)
-    A = sp.csc_matrix(prob.A).toarray()
-    Pm = sp.csc_matrix(prob.P).toarray()
-    Hs = _dense_hs(prob, *_recentre(prob, sol.s, sol.z))
-    K = np.block([[Pm, A.T], [A, -Hs]])
-    uv = np.linalg.solve(K, np.concatenate([sol.x - t, np.zeros(prob.m)]))
-    u, v = uv[:prob.n], uv[prob.n:]
-    ref_dA = -(np.outer(sol.z, u) + np.outer(v, sol.x))
-    scale = max(np.max(np.abs(u)), np.max(np.abs(v)), 1.0)
-    assert np.max(np.abs(dq + u)) <= 1e-5 * scale
-    assert np.max(np.abs(db - v)) <= 1e-5 * scale
-    got = dA.toarray()
-    mask = sp.csc_matrix(prob.A).toarray() != 0
-    assert np.max(np.abs((got - ref_dA)[mask])) <= 1e-5 * scale * max(1.0, np.max(np.abs(sol.x)),
-                                                                      np.max(np.abs(sol.z)))
+    rq, rb, rA = oracle_adjoint.adjoint(prob, sol.x, sol.s, sol.z, sol.x - t)
+    scale = max(np.max(np.abs(rq)), np.max(np.abs(rb)), 1.0)
+    assert np.max(np.abs(dq - rq)) <= 1e-6 * scale
+    assert np.max(np.abs(db - rb)) <= 1e-6 * scale
+    assert np.max(np.abs(dA.toarray() - rA.toarray())) <= 1e-6 * scale * max(1.0, np.max(np.abs(sol.x)),
+                                                                   np.max(np.abs(sol.z)))
 
 
 def test_torch_autograd_wrapper():
@@ -157,3 +109,19 @@ def test_torch_autograd_wrapper():
     assert np.allclose(q.grad.numpy(), dq, rtol=1e-12, atol=1e-12)
     assert np.allclose(b.grad.numpy(), db, rtol=1e-12, atol=1e-12)
     assert np.allclose(a.grad.numpy(), dA.data, rtol=1e-12, atol=1e-12)
+
+
+def test_batch_adjoint_equals_single_handle():
+    """BatchSolver.solve_adjoint (re-prepared handles, eager launches, concurrent workers) gives
+    bitwise the gradients of a fresh handle per instance."""
+    from sdpx_b200.solver import BatchSolver
+
+    probs = [P.conic_qp(20 + i, n=24, n_nn=16, psd=4, rank=6) for i in range(6)]
+    bs = BatchSolver(workers=3, settings=_settings())
+    sols, grads = bs.solve_adjoint(probs, lambda i, sol: sol.x - probs[i].meta["t"])
+    for p, sol, g in zip(probs, sols, grads):
+        s, ref = _solve(p)
+        assert np.array_equal(sol.x, ref.x)
+        dq, db, dA = s.adjoint(ref.x - p.meta["t"])
+        assert np.array_equal(g[0], dq) and np.array_equal(g[1], db)
+        assert np.array_equal(g[2].data, dA.data)
