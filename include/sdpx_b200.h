@@ -119,6 +119,11 @@ int32_t sdpx_destroy(sdpx_handle *handle);
  * refinement steps).  Counterpart of the reference's SDPX_PROFILE phase receipt
  * (src/receipt.rs:104-160).  times needs 7 doubles, counts 4 uint64. */
 int32_t sdpx_b200_phase_times(sdpx_handle *handle, double *times, uint64_t *counts);
+/* KKT solves of the last solve whose two-level refinement ran on the device (one CUDA graph with
+ * WHILE nodes driven by control kernels, one host read per solve: the default when graphs are on)
+ * and those driven from the host (a host read per refinement step: graphs off, kernel timing on,
+ * or ir_max_iter > 64).  Both run the same kernels in the same order. */
+int32_t sdpx_b200_kkt_paths(sdpx_handle *handle, uint64_t *device_driven, uint64_t *host_driven);
 /* Enable (on != 0) or disable CUDA-event timing of the device phases of later solves and reset
  * the totals.  Events are recorded on the handle's stream around each phase: NT scaling,
  * Schur assembly, factorisation, triangular solves, cone congruences, step lengths, the

@@ -725,4 +725,15 @@ int32_t sdpx_b200_phase_times(sdpx_handle* h, double* times, uint64_t* counts) {
   });
 }
 
+int32_t sdpx_b200_kkt_paths(sdpx_handle* h, uint64_t* device_driven, uint64_t* host_driven) {
+  return boundary([&] {
+    if (!device_driven || !host_driven) invalid("null pointer");
+    operate(h, [&](sdpx_handle& hh) {
+      const PhaseTimes& t = hh.times;
+      *device_driven = (uint64_t)t.device_kkt_solves;
+      *host_driven = (uint64_t)(t.kkt_solves - t.device_kkt_solves);
+    });
+  });
+}
+
 }  // extern "C"

@@ -33,6 +33,24 @@ enum SdpxgStatus : uint32_t {
   SDPXG_ST_SYNC_TIMEOUT = 32u,    // a bounded inter-CTA wait gave up (no progress)
 };
 
+// Device-resident control of one refined KKT solve: the stopping rules of the two-level
+// stationary refinement (kkt/refinement.rs:118-191) evaluated by one-thread control kernels that
+// drive the WHILE nodes of the solve's CUDA graph; the host reads it once per solve.
+struct RefineCtl {
+  double normb, norme, tol;      // reduced-system level (inner)
+  double onormb, onorme, otol;   // original-operator level (outer)
+  int it, oit;                   // accepted steps at each level
+  int ok;                        // cleared by the first failed check
+  int accept, oaccept;           // the last candidate is kept
+  int cont, ocont;               // the loop goes on (its residual is carried over)
+  int inner_steps, outer_steps;  // refinement steps run (trace counters)
+  int guard;                     // loop-body executions: a hard bound on every loop
+};
+struct RefineParams {
+  double abstol, reltol, stop_ratio;
+  int max_iter, guard_max;
+};
+
 struct BlockDesc {
   int n;         // block order
   int svec_off;  // first row of the block in the stacked cone vector

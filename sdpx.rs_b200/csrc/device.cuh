@@ -169,6 +169,15 @@ __global__ void k_lincomb(long, double, const double*, double, const double*, do
 __global__ void k_reduce_partial(int, long, const double*, const double*, double*);
 __global__ void k_reduce_final(int, int, const double*, double*);
 __global__ void k_reduce_fused(int, long, const double*, const double*, double*, unsigned*, double*);
+__global__ void k_refine_head(const double*, const double*, const double*, const double*,
+                              const double*, int, RefineCtl*, RefineParams, cudaGraphConditionalHandle);
+__global__ void k_refine_step(const double*, RefineCtl*, RefineParams, cudaGraphConditionalHandle);
+__global__ void k_refine_outer_init(const double*, const double*, const double*, const double*,
+                                    RefineCtl*, RefineParams, cudaGraphConditionalHandle);
+__global__ void k_refine_outer_step(const double*, const double*, RefineCtl*, RefineParams,
+                                    cudaGraphConditionalHandle);
+__global__ void k_refine_copy(const int*, long, double*, const double*, const int*, long, double*,
+                              const double*);
 __global__ void k_diag_absmax(const double*, int, double*);
 __global__ void k_nn_scale(int, const int*, const double*, const double*, double*, double*, uint32_t*);
 __global__ void k_nn_identity(int, double*, double*);
@@ -219,6 +228,8 @@ class Reducer {
     return s;
   }
   int count() const { return count_; }
+  // Device address of a slot (read by the control kernels of the device-driven solves).
+  const double* slot(int s) const { return slots_.p + s; }
   // Slots queued by a replayed captured segment (its reductions ran inside the graph).
   void set_count(int c) { count_ = c; }
   const PinnedBuf<double>& fetch(cudaStream_t st) {

@@ -187,6 +187,7 @@ class Engine {
   Engine() = default;
   ~Engine() {
     for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second.exec);
+    for (auto& kv : programs_) cudaGraphExecDestroy(kv.second.exec);
     for (auto& e : ev_) if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
   }
@@ -204,6 +205,8 @@ class Engine {
   void clear_graphs() {
     for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second.exec);
     graphs_.clear();
+    for (auto& kv : programs_) cudaGraphExecDestroy(kv.second.exec);
+    programs_.clear();
   }
   template <typename F>
   void segment(int id, std::initializer_list<const void*> ptrs, F&& body) {
@@ -222,6 +225,19 @@ class Engine {
       return;
     }
     if (graphs_.size() >= kMaxGraphs) clear_graphs();  // bound the cache
+    uint64_t kernels = 0;
+    cudaGraph_t g = capture(body, &kernels);
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    check(e, "cudaGraphInstantiate");
+    graphs_[key] = {ex, red.count(), kernels};
+    check(cudaGraphLaunch(ex, st), "cudaGraphLaunch");
+  }
+  // Capture a straight run of launches on this engine's stream into a graph (not instantiated)
+  // and count its kernel nodes.
+  template <typename F>
+  cudaGraph_t capture(F&& body, uint64_t* kernels) {
     check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
       body();
@@ -233,23 +249,33 @@ class Engine {
     }
     cudaGraph_t g = nullptr;
     check(cudaStreamEndCapture(st, &g), "end capture");
-    // kernel nodes of the segment (the launch counter's increment per replay)
     size_t nn = 0;
-    uint64_t kernels = 0;
+    uint64_t k = 0;
     check(cudaGraphGetNodes(g, nullptr, &nn), "graph nodes");
     std::vector<cudaGraphNode_t> nodes(nn);
     if (nn) check(cudaGraphGetNodes(g, nodes.data(), &nn), "graph nodes");
     for (cudaGraphNode_t nd : nodes) {
       cudaGraphNodeType ty;
       check(cudaGraphNodeGetType(nd, &ty), "graph node type");
-      kernels += (ty == cudaGraphNodeTypeKernel);
+      k += (ty == cudaGraphNodeTypeKernel);
     }
-    cudaGraphExec_t ex = nullptr;
-    const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
-    cudaGraphDestroy(g);
-    check(e, "cudaGraphInstantiate");
-    graphs_[key] = {ex, red.count(), kernels};
-    check(cudaGraphLaunch(ex, st), "cudaGraphLaunch");
+    if (kernels) *kernels = k;
+    return g;
+  }
+  // Instantiated graphs with device-side control flow (the refined KKT solve), keyed like the
+  // segments and dropped with them.  Kernel counts: fixed per launch, per inner and per outer
+  // refinement step.
+  struct Program {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t fixed = 0, per_inner = 0, per_outer = 0;
+  };
+  Program* find_program(const std::string& key) {
+    auto it = programs_.find(key);
+    return it == programs_.end() ? nullptr : &it->second;
+  }
+  Program* add_program(const std::string& key, const Program& pg) {
+    if (programs_.size() >= kMaxGraphs) clear_graphs();
+    return &(programs_[key] = pg);
   }
   void tbegin(int k) {
     if (timing) check(cudaEventRecord(ev_[2 * k], st), "event");
@@ -952,6 +978,7 @@ class Engine {
   };
   static constexpr size_t kMaxGraphs = 256;
   std::unordered_map<std::string, GraphEntry> graphs_;
+  std::unordered_map<std::string, Program> programs_;
 };
 
 }  // namespace sdpxg

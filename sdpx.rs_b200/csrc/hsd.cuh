@@ -63,6 +63,7 @@ struct Info {
 struct PhaseTimes {
   double residual = 0, scale = 0, assemble = 0, factor = 0, solve = 0, step = 0, other = 0;
   int factorizations = 0, kkt_solves = 0, outer_refinements = 0, inner_refinements = 0;
+  int device_kkt_solves = 0;  // KKT solves whose refinement ran as one device-driven graph
 };
 
 class HsdSolver {
@@ -81,6 +82,8 @@ class HsdSolver {
     m_ = p.m;
     const int n = n_, m = m_;
     E.clear_graphs();  // segments captured for earlier work vectors must not be replayed
+    ctl_.alloc(1);
+    hctl_.alloc(1);
     auto vn = [&](DevBuf<double>& b) { b.alloc(std::max(n, 1)); };
     auto vm = [&](DevBuf<double>& b) { b.alloc(std::max(m, 1)); };
     for (auto* b : {&x_, &px_, &bx_, &rx_, &rxinf_, &Px_, &x2_, &dx_, &ax_, &tx_, &prevx_, &bestx_,
@@ -155,6 +158,9 @@ class HsdSolver {
   void recover(const double* bz, const double* x, double* z);
   bool solve_raw(const double* bx, const double* bz, double* x, double* z);
   bool kkt_solve(const double* bx, const double* bz, double* x, double* z);
+  // The same refined solve as ONE CUDA graph whose refinement loops run on the device (WHILE
+  // nodes driven by the control kernels of refine_ctl.cu): one host read per solve.
+  bool kkt_solve_graph(const double* bx, const double* bz, double* x, double* z);
   void residual_full(const double* bx, const double* bz, const double* x, const double* z,
                      double* ex, double* ez);
 
@@ -194,6 +200,9 @@ class HsdSolver {
   Info prev_;
   bool have_prev_ = false;
   // device vectors (n-length then m-length groups)
+  DevBuf<RefineCtl> ctl_;
+  PinnedBuf<RefineCtl> hctl_;
+  bool program_failed_ = false;  // building the device-driven solve failed once: host-driven
   DevBuf<double> x_, px_, bx_, rx_, rxinf_, Px_, x2_, dx_, ax_, tx_, prevx_, bestx_, rhsx_, x1_,
       xhat_, en_, dxn_, candn_, e2n_, ex_, cx_, candx_, ex2_, negq_, q_, d_, dinv_, wn_;
   DevBuf<double> s_, z_, ps_, pz_, rz_, rzinf_, z2_, ds_, dz_, as_, az_, ts_, tz_, prevs_, prevz_,
@@ -345,6 +354,12 @@ inline bool HsdSolver::kkt_solve(const double* bx, const double* bz, double* x, 
     times.solve += secs(t0);
     return ok;
   }
+  if (E.graphs_enabled && !E.timing && !program_failed_ && n > 0 && m > 0 &&
+      st_.ir_max_iter >= 0 && st_.ir_max_iter <= 64) {
+    const bool ok = kkt_solve_graph(bx, bz, x, z);
+    times.solve += secs(t0);
+    return ok;
+  }
   E.segment(SEG_KKT_HEAD, {bx, bz, x}, [&] {
     E.red.add(st(), RED_FINITE, n, bx, nullptr);
     E.red.add(st(), RED_FINITE, m, bz, nullptr);
@@ -414,6 +429,222 @@ inline bool HsdSolver::kkt_solve(const double* bx, const double* bz, double* x, 
   }
   times.solve += secs(t0);
   return ok;
+}
+
+// Graph of one refined KKT solve (kkt_solve's steps, in its order):
+//   head run (finite bx, bz; condense; first reduced pass) -> k_refine_head
+//   WHILE inner: [trisolve e, candidate, reduced residual] -> k_refine_step -> keep candidate
+//   tail run (recover; full residual; norms) -> k_refine_outer_init
+//   WHILE outer: [condense (ex, ez); first pass] -> k_refine_head -> WHILE inner (on cx)
+//                -> [recover; candidate (x, z); full residual] -> k_refine_outer_step -> keep
+// Runs are captured once from the same Engine calls as the host-driven path; the graph is cached
+// per (bx, bz, x, z, refinement settings) and replayed.
+inline bool HsdSolver::kkt_solve_graph(const double* bx, const double* bz, double* x, double* z) {
+  const int n = n_, m = m_;
+  RefineParams prm{st_.ir_abstol, st_.ir_reltol, st_.ir_stop_ratio, st_.ir_max_iter, 0};
+  prm.guard_max = (prm.max_iter + 1) * (prm.max_iter + 2) + 2;
+  std::string key("KKT");
+  for (const void* ptr : {(const void*)bx, (const void*)bz, (const void*)x, (const void*)z})
+    key.append(reinterpret_cast<const char*>(&ptr), sizeof ptr);
+  key.append(reinterpret_cast<const char*>(&prm), sizeof prm);
+  Engine::Program* pg = E.find_program(key);
+  if (!pg) {
+    if (E.red.count() != 0) throw CudaError("a captured program must start with an empty reducer");
+    const uint64_t launches0 = g_launches;  // capture counts launches that do not run
+    RefineCtl* c = ctl_.p;
+    const int* accept = &c->accept;
+    const int* cont = &c->cont;
+    const int* oaccept = &c->oaccept;
+    const int* ocont = &c->ocont;
+    cudaGraph_t G = nullptr;
+    std::vector<cudaGraph_t> runs;  // captured runs, destroyed once cloned into G
+    Engine::Program built;
+    try {
+      check(cudaGraphCreate(&G, 0), "graph create");
+      auto child = [&](cudaGraph_t g, std::initializer_list<cudaGraphNode_t> deps,
+                       cudaGraph_t run) {
+        cudaGraphNode_t nd;
+        std::vector<cudaGraphNode_t> d(deps);
+        check(cudaGraphAddChildGraphNode(&nd, g, d.data(), d.size(), run), "child node");
+        return nd;
+      };
+      auto kernel = [&](cudaGraph_t g, cudaGraphNode_t dep, const void* fn, void** args,
+                        unsigned grid) {
+        cudaKernelNodeParams kp{};
+        kp.func = const_cast<void*>(fn);
+        kp.gridDim = dim3(grid);
+        kp.blockDim = dim3(grid > 1 ? 256 : 32);
+        kp.kernelParams = args;
+        cudaGraphNode_t nd;
+        check(cudaGraphAddKernelNode(&nd, g, &dep, 1, &kp), "kernel node");
+        return nd;
+      };
+      auto loop = [&](cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h,
+                      cudaGraph_t* body) {
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t nd;
+        check(cudaGraphAddNode(&nd, g, &dep, 1, &np), "while node");
+        *body = np.conditional.phGraph_out[0];
+        return nd;
+      };
+      auto run = [&](uint64_t* kernels, auto&& f) {
+        E.red.set_count(0);
+        cudaGraph_t g = E.capture(f, kernels);
+        E.red.set_count(0);
+        runs.push_back(g);
+        return g;
+      };
+      const unsigned cgrid = (unsigned)std::min<long>((2L * std::max(n, m) + 255) / 256, 592);
+      // inner refinement loop on (r, xx): body of a WHILE node
+      uint64_t k_step = 0;
+      auto inner = [&](cudaGraph_t body, const double* r, double* xx,
+                       cudaGraphConditionalHandle h) {
+        int se = 0;
+        cudaGraph_t g = run(&k_step, [&] {
+          E.trisolve(en_, dxn_);
+          E.lincomb(n, 1.0, xx, 1.0, dxn_, 0.0, nullptr, candn_);
+          E.schur_residual(r, candn_, e2n_);
+          se = E.red.add(st(), RED_MAXABS, n, e2n_, nullptr);
+        });
+        cudaGraphNode_t a = child(body, {}, g);
+        const double* p_se = E.red.slot(se);
+        void* sa[] = {&p_se, &c, &prm, &h};
+        cudaGraphNode_t b = kernel(body, a, (const void*)k_refine_step, sa, 1);
+        long nn = n;
+        double* d1 = xx;
+        const double* s1 = candn_.p;
+        double* d2 = en_.p;
+        const double* s2 = e2n_.p;
+        void* ca[] = {&accept, &nn, &d1, &s1, &cont, &nn, &d2, &s2};
+        kernel(body, b, (const void*)k_refine_copy, ca, cgrid);
+      };
+      // head
+      int h0 = 0, h1 = 0, hb = 0;
+      uint64_t k_head = 0;
+      cudaGraph_t g_head = run(&k_head, [&] {
+        h0 = E.red.add(st(), RED_FINITE, n, bx, nullptr);
+        h1 = E.red.add(st(), RED_FINITE, m, bz, nullptr);
+        hb = E.red.count();
+        condense_first(bx, bz, x);
+      });
+      cudaGraphNode_t nh = child(G, {}, g_head);
+      cudaGraphConditionalHandle hin;
+      check(cudaGraphConditionalHandleCreate(&hin, G, 0, 0), "conditional handle");
+      {
+        const double *a0 = E.red.slot(h0), *a1 = E.red.slot(h1), *a2 = E.red.slot(hb),
+                     *a3 = E.red.slot(hb + 1), *a4 = E.red.slot(hb + 2);
+        int reset = 1;
+        void* args[] = {&a0, &a1, &a2, &a3, &a4, &reset, &c, &prm, &hin};
+        nh = kernel(G, nh, (const void*)k_refine_head, args, 1);
+      }
+      cudaGraph_t body1;
+      cudaGraphNode_t w1 = loop(G, nh, hin, &body1);
+      inner(body1, xhat_, x, hin);
+      // tail
+      int t0 = 0;
+      uint64_t k_tail = 0;
+      cudaGraph_t g_tail = run(&k_tail, [&] {
+        recover(bz, x, z);
+        residual_full(bx, bz, x, z, ex_, ez_);
+        t0 = E.red.add(st(), RED_MAXABS, n, bx, nullptr);
+        E.red.add(st(), RED_MAXABS, m, bz, nullptr);
+        E.red.add(st(), RED_MAXABS, n, ex_, nullptr);
+        E.red.add(st(), RED_MAXABS, m, ez_, nullptr);
+      });
+      cudaGraphNode_t nt = child(G, {w1}, g_tail);
+      cudaGraphConditionalHandle hout;
+      check(cudaGraphConditionalHandleCreate(&hout, G, 0, 0), "conditional handle");
+      {
+        const double *a0 = E.red.slot(t0), *a1 = E.red.slot(t0 + 1), *a2 = E.red.slot(t0 + 2),
+                     *a3 = E.red.slot(t0 + 3);
+        void* args[] = {&a0, &a1, &a2, &a3, &c, &prm, &hout};
+        nt = kernel(G, nt, (const void*)k_refine_outer_init, args, 1);
+      }
+      cudaGraph_t body2;
+      loop(G, nt, hout, &body2);
+      // outer body: correction (cx, cz) = K^-1 (ex, ez), candidate, full residual
+      int ob = 0;
+      uint64_t k_ohead = 0;
+      cudaGraph_t g_oh = run(&k_ohead, [&] {
+        ob = E.red.count();
+        condense_first(ex_, ez_, cx_);
+      });
+      cudaGraphNode_t no = child(body2, {}, g_oh);
+      cudaGraphConditionalHandle hin2;
+      check(cudaGraphConditionalHandleCreate(&hin2, body2, 0, 0), "conditional handle");
+      {
+        const double* nul = nullptr;
+        const double *a2 = E.red.slot(ob), *a3 = E.red.slot(ob + 1), *a4 = E.red.slot(ob + 2);
+        int reset = 0;
+        void* args[] = {&nul, &nul, &a2, &a3, &a4, &reset, &c, &prm, &hin2};
+        no = kernel(body2, no, (const void*)k_refine_head, args, 1);
+      }
+      cudaGraph_t body3;
+      cudaGraphNode_t w3 = loop(body2, no, hin2, &body3);
+      inner(body3, xhat_, cx_, hin2);
+      int u0 = 0;
+      uint64_t k_otail = 0;
+      cudaGraph_t g_ot = run(&k_otail, [&] {
+        recover(ez_, cx_, cz_);
+        E.lincomb(n, 1.0, x, 1.0, cx_, 0.0, nullptr, candx_);
+        E.lincomb(m, 1.0, z, 1.0, cz_, 0.0, nullptr, candz_);
+        residual_full(bx, bz, candx_, candz_, ex2_, ez2_);
+        u0 = E.red.add(st(), RED_MAXABS, n, ex2_, nullptr);
+        E.red.add(st(), RED_MAXABS, m, ez2_, nullptr);
+      });
+      cudaGraphNode_t nq = child(body2, {w3}, g_ot);
+      {
+        const double *a0 = E.red.slot(u0), *a1 = E.red.slot(u0 + 1);
+        void* args[] = {&a0, &a1, &c, &prm, &hout};
+        nq = kernel(body2, nq, (const void*)k_refine_outer_step, args, 1);
+      }
+      {
+        long nn = n, mm = m;
+        double *d1 = x, *d2 = z;
+        const double *s1 = candx_.p, *s2 = candz_.p;
+        void* args[] = {&oaccept, &nn, &d1, &s1, &oaccept, &mm, &d2, &s2};
+        nq = kernel(body2, nq, (const void*)k_refine_copy, args, cgrid);
+        double *e1 = ex_.p, *e2 = ez_.p;
+        const double *f1 = ex2_.p, *f2 = ez2_.p;
+        void* args2[] = {&ocont, &nn, &e1, &f1, &ocont, &mm, &e2, &f2};
+        kernel(body2, nq, (const void*)k_refine_copy, args2, cgrid);
+      }
+      check(cudaGraphInstantiate(&built.exec, G, 0), "cudaGraphInstantiate");
+      built.fixed = k_head + 1 + k_tail + 1;
+      built.per_inner = k_step + 2;
+      built.per_outer = k_ohead + 1 + k_otail + 1 + 2;
+    } catch (...) {
+      for (cudaGraph_t g : runs) cudaGraphDestroy(g);
+      if (G) cudaGraphDestroy(G);
+      if (built.exec) cudaGraphExecDestroy(built.exec);
+      g_launches = launches0;
+      E.red.set_count(0);
+      cudaGetLastError();
+      program_failed_ = true;  // the host-driven refinement takes over for this handle
+      if (std::getenv("SDPX_B200_VERBOSE"))
+        std::fprintf(stderr, "sdpx_b200: device-driven KKT solve unavailable, host-driven\n");
+      times.kkt_solves--;  // counted again by kkt_solve
+      return kkt_solve(bx, bz, x, z);
+    }
+    for (cudaGraph_t g : runs) cudaGraphDestroy(g);
+    cudaGraphDestroy(G);
+    g_launches = launches0;
+    pg = E.add_program(key, built);
+  }
+  check(cudaGraphLaunch(pg->exec, st()), "cudaGraphLaunch");
+  copy_d2h(hctl_.p, ctl_.p, sizeof(RefineCtl), st());
+  check(cudaStreamSynchronize(st()), "refined solve sync");
+  const RefineCtl& hc = hctl_.p[0];
+  times.device_kkt_solves++;
+  times.inner_refinements += hc.inner_steps;
+  times.outer_refinements += hc.outer_steps;
+  g_launches += pg->fixed + pg->per_inner * (uint64_t)hc.inner_steps +
+                pg->per_outer * (uint64_t)hc.outer_steps;
+  return hc.ok != 0;
 }
 
 // ------------------------------------------------------------------------------------------

@@ -79,6 +79,7 @@ SIGNATURES = {
     "sdpx_b200_launch_count": (u64, []),
     "sdpx_b200_transfer_bytes": (i32, [PU64, PU64]),
     "sdpx_b200_schur_forms": (i32, [C.c_void_p, PU32, PU32]),
+    "sdpx_b200_kkt_paths": (i32, [C.c_void_p, PU64, PU64]),
     "sdpx_b200_set_graphs": (i32, [C.c_void_p, i32]),
     "sdpx_b200_adjoint": (i32, [C.c_void_p, PD, PD, PD, PD, PD, PD, u64]),
     "sdpxg_ctx_create": (i32, [i32, u32, C.POINTER(C.c_void_p)]),

@@ -237,6 +237,12 @@ class DefaultSolver:
         """Replay the KKT solve's captured CUDA graphs (default) or launch eagerly."""
         _lib.call("sdpx_b200_set_graphs", self._h, int(bool(on)))
 
+    def kkt_paths(self) -> dict:
+        """KKT solves of the last solve refined on the device (one graph each) and from the host."""
+        d, h = C.c_uint64(), C.c_uint64()
+        _lib.call("sdpx_b200_kkt_paths", self._h, C.byref(d), C.byref(h))
+        return {"device": int(d.value), "host": int(h.value)}
+
     def schur_forms(self) -> dict:
         """PSD blocks in the rank-one Gram form and in the ordinary dense-column form."""
         g, o = C.c_uint32(), C.c_uint32()

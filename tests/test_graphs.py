@@ -1,8 +1,10 @@
-"""Captured KKT-solve segments (CUDA graphs) against eager launches.
+"""Captured KKT solves (CUDA graphs) against eager launches.
 
-The graphs replay exactly the kernels the eager path launches, in the same order on the same
-stream, so a solve with graphs must be bitwise identical to one with SDPX_B200_GRAPHS=0, and
-repeated solves on one handle (graph replays) must stay bitwise identical too.
+With graphs on, every refined KKT solve is one graph whose two refinement loops are WHILE nodes
+driven on the device; with SDPX_B200_GRAPHS=0 the host drives the loops and launches eagerly.
+Both run the same kernels in the same order on the same stream and apply the same stopping
+rules, so the solves must be bitwise identical, take the same refinement steps, and repeated
+solves on one handle (graph replays) must stay bitwise identical too.
 """
 import os
 
@@ -29,13 +31,18 @@ def _make(prob, graphs):
 
 
 @pytest.mark.parametrize("maker", [lambda: P.rank1_sdp(8, 200, seed=4, nmin=6, nmax=24),
-                                   lambda: P.dense_sdp(20, 60, seed=5)])
+                                   lambda: P.dense_sdp(20, 60, seed=5),
+                                   lambda: P.conic_qp(6, n=40, n_nn=30, psd=6, rank=8)])
 def test_graphs_bitwise_equal_eager(maker):
     prob = maker()
     eager = _make(prob, False)
     a = eager.solve()
+    assert eager.kkt_paths()["device"] == 0
     g = _make(prob, True)
     b = g.solve()
+    paths = g.kkt_paths()
+    assert paths["host"] == 0 and paths["device"] == g.info.counts["kkt_solves"] > 0
+    assert g.info.counts == eager.info.counts  # same refinement steps at both levels
     c = g.solve()  # second solve replays the cached graphs
     for s in (b, c):
         assert s.status == a.status and s.iterations == a.iterations
