@@ -193,45 +193,80 @@ __device__ __forceinline__ void cta_gemm(double* C, const double* A, bool ta, co
 // column divided by the pivot, and columns are scaled at the end.  The thread that
 // finishes the next diagonal entry computes its reciprocal once and publishes it for the
 // next step (0 marks a pivot that is not positive and finite: the reciprocal of a finite
-// positive double is never 0).  Returns false (CTA uniform) on such a pivot.
-// `piv` is SDPXG_CHOL_SCRATCH doubles of shared memory: pivots, reciprocals, roots.
-__device__ inline bool cta_cholesky_lower(double* A, int n, double* piv) {
-  double* pinv = piv + SDPXG_NMAX;
-  double* root = pinv + SDPXG_NMAX;
+// positive double is never 0).  Step k visits only the trailing (n-k-1)^2 square.
+// cta_cholesky_lower2 factors two matrices of the same order at once (one barrier per
+// column for both, the same arithmetic per entry); a failed matrix stops being updated and
+// reports false, the other one carries on.
+// `piv` is SDPXG_CHOL_SCRATCH doubles of shared memory per matrix: pivots, reciprocals, roots.
+__device__ inline void cta_cholesky_lower2(double* A, double* B, int n, double* pivA, double* pivB,
+                                           bool* okA, bool* okB) {
+  double* pinvA = pivA + SDPXG_NMAX;
+  double* pinvB = pivB + SDPXG_NMAX;
+  const bool two = (B != nullptr);
   if (threadIdx.x == 0 && n > 0) {
-    const double d = SM(A, 0, 0);
-    piv[0] = d;
-    pinv[0] = (d > 0.0 && isfinite(d)) ? 1.0 / d : 0.0;
+    const double a = SM(A, 0, 0);
+    pivA[0] = a;
+    pinvA[0] = (a > 0.0 && isfinite(a)) ? 1.0 / a : 0.0;
+    if (two) {
+      const double b = SM(B, 0, 0);
+      pivB[0] = b;
+      pinvB[0] = (b > 0.0 && isfinite(b)) ? 1.0 / b : 0.0;
+    }
   }
+  bool liveA = true, liveB = two;
   for (int k = 0; k < n; ++k) {
     __syncthreads();
-    const double dinv = pinv[k];  // written in step k - 1, not touched in step k
-    if (dinv == 0.0) {
-      __syncthreads();
-      return false;
-    }
-    for (int e = threadIdx.x; e < SDPXG_NMAX * SDPXG_NMAX; e += blockDim.x) {
-      const int i = e & (SDPXG_NMAX - 1), j = e / SDPXG_NMAX;
-      if (j <= k || i < j || i >= n) continue;
-      const double v = SM(A, i, j) - SM(A, i, k) * SM(A, j, k) * dinv;
-      SM(A, i, j) = v;
+    const double dA = pinvA[k];  // written in step k - 1, not touched in step k
+    const double dB = two ? pinvB[k] : 0.0;
+    liveA = liveA && dA != 0.0;
+    liveB = liveB && dB != 0.0;
+    if (!liveA && !liveB) break;
+    const int w = n - k - 1, tot = w * w;
+    const int lim = two ? 2 * tot : tot;
+    for (int e = threadIdx.x; e < lim; e += blockDim.x) {
+      const bool second = e >= tot;
+      const int r = second ? e - tot : e;
+      const int i = k + 1 + r % w, j = k + 1 + r / w;
+      if (i < j || (second ? !liveB : !liveA)) continue;
+      double* X = second ? B : A;
+      const double v = SM(X, i, j) - SM(X, i, k) * SM(X, j, k) * (second ? dB : dA);
+      SM(X, i, j) = v;
       if (i == k + 1 && j == k + 1) {  // the next pivot is final now
-        piv[k + 1] = v;
-        pinv[k + 1] = (v > 0.0 && isfinite(v)) ? 1.0 / v : 0.0;
+        double* pv = second ? pivB : pivA;
+        pv[k + 1] = v;
+        pv[SDPXG_NMAX + k + 1] = (v > 0.0 && isfinite(v)) ? 1.0 / v : 0.0;
       }
     }
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < n; j += blockDim.x) root[j] = sqrt(piv[j]);
-  __syncthreads();
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-    int i = e % n, j = e / n;
-    if (i > j) SM(A, i, j) /= root[j];
-    else if (i == j) SM(A, i, j) = root[j];
-    else SM(A, i, j) = 0.0;
+  *okA = liveA;
+  *okB = liveB;
+  double* rootA = pinvA + SDPXG_NMAX;
+  double* rootB = pinvB + SDPXG_NMAX;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    if (liveA) rootA[j] = sqrt(pivA[j]);
+    if (liveB) rootB[j] = sqrt(pivB[j]);
   }
   __syncthreads();
-  return true;
+  const int lim = two ? 2 * n * n : n * n;
+  for (int e = threadIdx.x; e < lim; e += blockDim.x) {
+    const bool second = e >= n * n;
+    if (second ? !liveB : !liveA) continue;
+    const int r = second ? e - n * n : e;
+    const int i = r % n, j = r / n;
+    double* X = second ? B : A;
+    const double* root = second ? rootB : rootA;
+    if (i > j) SM(X, i, j) /= root[j];
+    else if (i == j) SM(X, i, j) = root[j];
+    else SM(X, i, j) = 0.0;
+  }
+  __syncthreads();
+}
+
+__device__ inline bool cta_cholesky_lower(double* A, int n, double* piv) {
+  bool ok, unused;
+  cta_cholesky_lower2(A, nullptr, n, piv, piv, &ok, &unused);
+  return ok;
 }
 
 // Solve L' X = B in place of B (L lower, n x n), one column per thread.

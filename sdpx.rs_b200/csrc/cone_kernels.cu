@@ -16,9 +16,15 @@ constexpr int kMat = SDPXG_LD * SDPXG_NMAX;  // doubles per shared matrix
 }  // namespace
 
 // ---------------------------------------------------------------------------------------
-// NT scaling.  L1 = chol(S), L2 = chol(Z), L2'L1 = U diag(lam) V',
-// R = L1 V lam^-1/2, Rinv = lam^1/2 V' L1^-1, Ginv = Rinv' Rinv.
-// Shared memory: 5 matrices + Cholesky scratch + 2n doubles + n ints + 1 int.
+// NT scaling.  L1 = chol(S), L2 = chol(Z), L2'L1 = U diag(lam) V' (psdtrianglecone.rs:311-439).
+// The reference forms R = L1 V lam^-1/2 and Rinv = lam^1/2 V' L1^-1.  With M = L2'L1 and
+// M V = U lam, the same matrices are
+//   R = L2^-T U lam^1/2,   Rinv = lam^-1/2 U' L2'
+// (L1 V = L1 M^-1 U lam = L2^-T U lam), which needs only the LEFT singular vectors: the
+// normalised columns that one-sided Jacobi leaves in M, so the rotations are not accumulated
+// into V (half the shared-memory traffic of every Jacobi round).  Both forms have the same
+// normwise accuracy (a triangular solve with L1 or with L2 each).  Ginv = Rinv' Rinv.
+// Shared memory: 5 matrices + 2 Cholesky scratches + 2n doubles + n ints + 1 int.
 // ---------------------------------------------------------------------------------------
 extern "C" __global__ void __launch_bounds__(SDPXG_CONE_THREADS)
 k_nt_scale(const BlockDesc* __restrict__ blocks, const double* __restrict__ s,
@@ -34,7 +40,8 @@ k_nt_scale(const BlockDesc* __restrict__ blocks, const double* __restrict__ s,
   double* V = M + kMat;
   double* X = V + kMat;
   double* piv = X + kMat;
-  double* sig = piv + SDPXG_CHOL_SCRATCH;
+  double* piv2 = piv + SDPXG_CHOL_SCRATCH;
+  double* sig = piv2 + SDPXG_CHOL_SCRATCH;
   double* lsort = sig + SDPXG_NMAX;
   int* rank = reinterpret_cast<int*>(lsort + SDPXG_NMAX);
   int* flag = rank + SDPXG_NMAX;
@@ -43,15 +50,15 @@ k_nt_scale(const BlockDesc* __restrict__ blocks, const double* __restrict__ s,
   cta_zero_mat(X);
   cta_load_smat(L1, s + bd.svec_off, n);
   cta_load_smat(L2, z + bd.svec_off, n);
-  bool ok1 = cta_cholesky_lower(L1, n, piv);
-  bool ok2 = cta_cholesky_lower(L2, n, piv);
+  bool ok1, ok2;
+  cta_cholesky_lower2(L1, L2, n, piv, piv2, &ok1, &ok2);  // chol(S), chol(Z) together
   if (!ok1 || !ok2) {
     if (threadIdx.x == 0) atomicOr(status, SDPXG_ST_CHOL_FAIL);
     return;
   }
-  cta_gemm(M, L2, true, L1, false, n);  // M = L2' L1
+  cta_gemm(M, L2, true, L1, false, n);  // M = L2' L1 (L1 is free from here on)
   __syncthreads();
-  int sweeps = cta_jacobi_svd(M, V, n, flag, piv);  // Cholesky scratch is free now
+  int sweeps = cta_jacobi_svd(M, nullptr, n, flag, piv);  // M -> U diag(lam)
   if (sweeps < 0) {
     if (threadIdx.x == 0) atomicOr(status, SDPXG_ST_SVD_UNCONVERGED);
     return;
@@ -69,43 +76,41 @@ k_nt_scale(const BlockDesc* __restrict__ blocks, const double* __restrict__ s,
     lsort[r] = sig[j];
   }
   __syncthreads();
-  // X = V with columns in descending singular-value order
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-    int i = e % n, j = e / n;
-    SM(X, i, rank[j]) = SM(V, i, j);
-  }
-  __syncthreads();
   bool good = true;
   for (int j = 0; j < n; ++j) good = good && (lsort[j] > 0.0) && isfinite(lsort[j]);
   if (!good) {
     if (threadIdx.x == 0) atomicOr(status, SDPXG_ST_CHOL_FAIL);
     return;
   }
-  // R = L1 X diag(lam^-1/2)
-  cta_gemm(M, L1, false, X, false, n);
+  // X = U with columns in descending singular-value order; V = X as the right-hand side
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    int i = e % n, j = e / n;
+    const double u = SM(M, i, j) / sig[j];
+    SM(X, i, rank[j]) = u;
+    SM(V, i, rank[j]) = u;
+  }
+  __syncthreads();
+  cta_trsm_lower_t(L2, V, n);  // V = L2^-T U
   __syncthreads();
   double* Rg = R + bd.mat_off;
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     int i = e % n, j = e / n;
-    Rg[e] = SM(M, i, j) / sqrt(lsort[j]);
+    Rg[e] = SM(V, i, j) * sqrt(lsort[j]);
   }
-  // V := L1^-T X, then Rinv = diag(lam^1/2) V'
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) SM(V, e % n, e / n) = SM(X, e % n, e / n);
-  __syncthreads();
-  cta_trsm_lower_t(L1, V, n);
+  cta_gemm(L1, X, true, L2, true, n);  // L1 = U' L2'
   __syncthreads();
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     int i = e % n, j = e / n;
-    SM(L2, i, j) = SM(V, j, i) * sqrt(lsort[i]);
+    SM(L1, i, j) /= sqrt(lsort[i]);  // Rinv = lam^-1/2 U' L2'
   }
   __syncthreads();
-  cta_store_mat(Rinv + bd.mat_off, L2, n);
-  cta_gemm(M, L2, true, L2, false, n);  // Ginv = Rinv' Rinv
+  cta_store_mat(Rinv + bd.mat_off, L1, n);
+  cta_gemm(M, L1, true, L1, false, n);  // Ginv = Rinv' Rinv
   __syncthreads();
   cta_store_mat(Ginv + bd.mat_off, M, n);
   bool fin = true;
   for (int e = threadIdx.x; e < n * n; e += blockDim.x)
-    fin = fin && isfinite(SM(M, e % n, e / n)) && isfinite(SM(L2, e % n, e / n));
+    fin = fin && isfinite(SM(M, e % n, e / n)) && isfinite(SM(L1, e % n, e / n));
   if (!fin) atomicOr(status, SDPXG_ST_NONFINITE);
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
     lam[bd.vec_off + j] = lsort[j];

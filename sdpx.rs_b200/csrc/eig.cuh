@@ -16,15 +16,19 @@
 #define SDPXG_JACOBI_TOL 1e-15
 #define SDPXG_BISECT_MAX 256
 
-// Returns the number of sweeps used, or -1 when the sweep bound was hit.
+// Returns the number of sweeps used, or -1 when the sweep bound was hit.  V == nullptr skips
+// the accumulation of the right singular vectors (the left ones are the normalised columns of
+// the result, which is all the NT scaling needs).
 // `flag` is one int of shared memory, `nrm` n doubles of shared memory.  The squared column
 // norms are recomputed at the start of every sweep and carried through the rotations with the
 // exact update a' = a - t g, b' = b + t g, so a rotation needs one warp reduction (g) instead
 // of three.
 __device__ inline int cta_jacobi_svd(double* M, double* V, int n, int* flag, double* nrm) {
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-    int i = e % n, j = e / n;
-    SM(V, i, j) = (i == j) ? 1.0 : 0.0;
+  if (V) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      int i = e % n, j = e / n;
+      SM(V, i, j) = (i == j) ? 1.0 : 0.0;
+    }
   }
   const int N = n + (n & 1);
   const int nwarps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -76,16 +80,22 @@ __device__ inline int cta_jacobi_svd(double* M, double* V, int n, int* flag, dou
           if (lane < n) {
             SM(M, lane, p) = c * x0 - s * y0;
             SM(M, lane, q) = s * x0 + c * y0;
-            const double v0 = SM(V, lane, p), w0 = SM(V, lane, q);
-            SM(V, lane, p) = c * v0 - s * w0;
-            SM(V, lane, q) = s * v0 + c * w0;
           }
           if (lane + 32 < n) {
             SM(M, lane + 32, p) = c * x1 - s * y1;
             SM(M, lane + 32, q) = s * x1 + c * y1;
-            const double v1 = SM(V, lane + 32, p), w1 = SM(V, lane + 32, q);
-            SM(V, lane + 32, p) = c * v1 - s * w1;
-            SM(V, lane + 32, q) = s * v1 + c * w1;
+          }
+          if (V) {
+            if (lane < n) {
+              const double v0 = SM(V, lane, p), w0 = SM(V, lane, q);
+              SM(V, lane, p) = c * v0 - s * w0;
+              SM(V, lane, q) = s * v0 + c * w0;
+            }
+            if (lane + 32 < n) {
+              const double v1 = SM(V, lane + 32, p), w1 = SM(V, lane + 32, q);
+              SM(V, lane + 32, p) = c * v1 - s * w1;
+              SM(V, lane + 32, q) = s * v1 + c * w1;
+            }
           }
           if (lane == 0) {
             nrm[p] = a - t * g;

@@ -27,7 +27,7 @@ namespace sdpxg {
 
 constexpr int kMatD = SDPXG_LD * SDPXG_NMAX;
 constexpr size_t kSmemNt =
-    (5 * kMatD + SDPXG_CHOL_SCRATCH + 2 * SDPXG_NMAX) * sizeof(double) + (SDPXG_NMAX + 1) * sizeof(int);
+    (5 * kMatD + 2 * SDPXG_CHOL_SCRATCH + 2 * SDPXG_NMAX) * sizeof(double) + (SDPXG_NMAX + 1) * sizeof(int);
 constexpr size_t kSmemCong = 4 * kMatD * sizeof(double);
 constexpr size_t kSmemCirc = 2 * kMatD * sizeof(double);
 constexpr size_t kSmemStep = (4 * kMatD + SDPXG_CHOL_SCRATCH + 4 * SDPXG_NMAX + 32) * sizeof(double);
