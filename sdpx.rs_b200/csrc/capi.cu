@@ -87,10 +87,28 @@ std::vector<double> scalars(const sdpx_scalars& a) {
   return v;
 }
 
+// Finite binary64 values of a stored-entry array, copied in parallel (no zero fill first).
+void values_into(const sdpx_scalars& a, F64Vec& v) {
+  if (a.reserved != 0) invalid("nonzero scalar reserved field");
+  if (a.kind != 0) {
+    std::vector<double> t = scalars(a);
+    v.assign(t.begin(), t.end());
+    return;
+  }
+  if (a.count && !a.f64) invalid("null pointer");
+  v.resize(a.count);
+  parallel_for((int64_t)a.count, 1 << 16, [&](int64_t b, int64_t e, int) {
+    for (int64_t i = b; i < e; ++i) {
+      v[i] = a.f64[i];
+      if (!std::isfinite(v[i])) invalid("nonfinite input");
+    }
+  });
+}
+
 struct Csc {
   uint64_t rows = 0, cols = 0;
-  std::vector<int64_t> colptr, rowval;
-  std::vector<double> val;
+  I64Vec colptr, rowval;
+  F64Vec val;
 };
 
 // crates/ffi/src/lib.rs:224-259 validation
@@ -117,7 +135,7 @@ Csc matrix(const sdpx_csc& a, bool upper) {
         c.rowval[p] = (int64_t)r;
       }
   });
-  c.val = scalars(a.values);
+  values_into(a.values, c.val);
   return c;
 }
 
@@ -160,6 +178,12 @@ Settings to_settings(const sdpx_settings& s) {
 // --------------------------------------------------------------------------------------
 // Ruiz equilibration on the host (default/problemdata.rs:639-735), restated on CSC data.
 // --------------------------------------------------------------------------------------
+// Ruiz equilibration (default/problemdata.rs:639-760).  The reference rescales A in place in
+// every pass; here the passes read A against the accumulated scales instead -- the maxima of
+// |e_i a_ij d_j| per column and row of the current iterate -- and A is rescaled once at the end
+// (E A D with the PSD rectification folded in): one read pass over the stored entries per
+// iteration instead of a read and a write pass, the same scalings up to rounding.  P, q, b and
+// the cost scale c are small and are updated in place as in the reference.
 void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
   const int n = p.n, m = p.m;
   eq.d.assign(n, 1.0);
@@ -168,6 +192,9 @@ void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
   if (st.equilibrate_enable) {
     const double smin = st.equilibrate_min_scaling, smax = st.equilibrate_max_scaling;
     std::vector<double> dw(n), ew(m);
+    const int nt = host_threads();
+    std::vector<std::vector<double>> ewp((size_t)nt);
+    std::vector<char> used((size_t)nt, 0);
     for (int it = 0; it < st.equilibrate_max_iter; ++it) {
       std::fill(dw.begin(), dw.end(), 0.0);
       std::fill(ew.begin(), ew.end(), 0.0);
@@ -177,25 +204,32 @@ void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
           dw[j] = std::max(dw[j], a);
           dw[p.Prow[q]] = std::max(dw[p.Prow[q]], a);
         }
-      {  // column maxima, and row maxima through per-chunk partial arrays
-        const int nt = host_threads();
-        std::vector<std::vector<double>> ewp((size_t)nt);
-        std::vector<char> used((size_t)nt, 0);
+      {  // column maxima, and row maxima through per-chunk partial arrays, of E A D
+        const double* e = eq.e.data();
+        const double* d = eq.d.data();
+        std::fill(used.begin(), used.end(), 0);
         parallel_for(n, col_grain(n, p.Aval.size()), [&](int64_t j0, int64_t j1, int t) {
           std::vector<double>& er = ewp[(size_t)t];
           er.assign(m, 0.0);
           used[(size_t)t] = 1;
-          for (int64_t j = j0; j < j1; ++j)
+          for (int64_t j = j0; j < j1; ++j) {
+            const double dj = d[j];
+            double cmax = 0.0;
             for (int64_t q = p.Acolptr[j]; q < p.Acolptr[j + 1]; ++q) {
-              const double a = std::fabs(p.Aval[q]);
-              dw[j] = std::max(dw[j], a);
-              er[p.Arow[q]] = std::max(er[p.Arow[q]], a);
+              const int64_t r = p.Arow[q];
+              const double a = std::fabs(p.Aval[q]) * dj;  // |a_ij| d_j
+              const double v = e[r] * a;                   // |e_i a_ij d_j|
+              cmax = std::max(cmax, v);
+              er[r] = std::max(er[r], a);
             }
+            dw[j] = std::max(dw[j], cmax);
+          }
         });
         parallel_for(m, std::max<int64_t>(1 << 12, (int64_t)m * nt / 4), [&](int64_t i0, int64_t i1, int) {
           for (int t = 0; t < nt; ++t)
             if (used[(size_t)t])
               for (int64_t i = i0; i < i1; ++i) ew[i] = std::max(ew[i], ewp[(size_t)t][i]);
+          for (int64_t i = i0; i < i1; ++i) ew[i] *= e[i];
         });
       }
       for (int j = 0; j < n; ++j) {
@@ -208,14 +242,12 @@ void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
         w = 1.0 / std::sqrt(w);
         ew[i] = std::min(std::max(w, smin / eq.e[i]), smax / eq.e[i]);
       }
-      parallel_for(n, col_grain(n, p.Aval.size() + p.Pval.size()), [&](int64_t j0, int64_t j1, int) {
-        for (int64_t j = j0; j < j1; ++j) {
-          for (int64_t q = p.Pcolptr[j]; q < p.Pcolptr[j + 1]; ++q) p.Pval[q] *= dw[p.Prow[q]] * dw[j];
-          for (int64_t q = p.Acolptr[j]; q < p.Acolptr[j + 1]; ++q) p.Aval[q] *= ew[p.Arow[q]] * dw[j];
-          p.q[j] *= dw[j];
-          eq.d[j] *= dw[j];
-        }
-      });
+      for (int j = 0; j < n; ++j)
+        for (int64_t q = p.Pcolptr[j]; q < p.Pcolptr[j + 1]; ++q) p.Pval[q] *= dw[p.Prow[q]] * dw[j];
+      for (int j = 0; j < n; ++j) {
+        p.q[j] *= dw[j];
+        eq.d[j] *= dw[j];
+      }
       for (int i = 0; i < m; ++i) {
         p.b[i] *= ew[i];
         eq.e[i] *= ew[i];
@@ -239,7 +271,6 @@ void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
       }
     }
     // rectify: one scalar per PSD cone, mean(e) (cones/psdtrianglecone.rs:252-255)
-    std::vector<double> delta(m, 1.0);
     int row = 0;
     std::vector<std::pair<int, int>> cl = p.cones;
     if (cl.empty())
@@ -253,17 +284,20 @@ void equilibrate(HostProblem& p, const Settings& st, Equilibration& eq) {
       double mean = 0.0;
       for (int i = row; i < row + tn; ++i) mean += eq.e[i];
       mean /= std::max(tn, 1);
-      for (int i = row; i < row + tn; ++i) delta[i] = mean / eq.e[i];
+      for (int i = row; i < row + tn; ++i) {
+        p.b[i] *= mean / eq.e[i];
+        eq.e[i] = mean;
+      }
       row += tn;
     }
+    // A := E A D with the final (rectified) scales, one pass
+    const double* e = eq.e.data();
+    const double* d = eq.d.data();
     parallel_for(n, col_grain(n, p.Aval.size()), [&](int64_t j0, int64_t j1, int) {
       for (int64_t j = j0; j < j1; ++j)
-        for (int64_t q = p.Acolptr[j]; q < p.Acolptr[j + 1]; ++q) p.Aval[q] *= delta[p.Arow[q]];
+        for (int64_t q = p.Acolptr[j]; q < p.Acolptr[j + 1]; ++q)
+          p.Aval[q] = e[p.Arow[q]] * p.Aval[q] * d[j];
     });
-    for (int i = 0; i < m; ++i) {
-      p.b[i] *= delta[i];
-      eq.e[i] *= delta[i];
-    }
   }
   eq.dinv.resize(n);
   eq.einv.resize(m);
@@ -385,12 +419,16 @@ std::unique_ptr<sdpx_handle> build_problem(const sdpx_csc* P, const sdpx_scalars
   p.m = (int)A->rows;
   if (P) {
     Csc pm = matrix(*P, true);
-    p.Pcolptr = pm.colptr; p.Prow = pm.rowval; p.Pval = pm.val;
+    p.Pcolptr.assign(pm.colptr.begin(), pm.colptr.end());
+    p.Prow.assign(pm.rowval.begin(), pm.rowval.end());
+    p.Pval.assign(pm.val.begin(), pm.val.end());
   } else {
     p.Pcolptr.assign(n + 1, 0);
   }
   Csc am = matrix(*A, false);
-  p.Acolptr = am.colptr; p.Arow = am.rowval; p.Aval = am.val;
+  p.Acolptr = std::move(am.colptr);
+  p.Arow = std::move(am.rowval);
+  p.Aval = std::move(am.val);
   p.q = scalars(*q);
   p.b = scalars(*b);
   uint64_t rows = 0;
@@ -439,6 +477,8 @@ void prepare_impl(const sdpx_csc* P, const sdpx_scalars* q, const sdpx_csc* A, c
   *out = nullptr;
   double tv = 0, te = 0;
   auto h = build_problem(P, q, A, b, cones, nc, s, &tv, &te);
+  if (verbose_from_env())
+    std::fprintf(stderr, "sdpx_b200 prepare: copy+validate %.3f s, equilibrate %.3f s\n", tv, te);
   const auto t2 = std::chrono::steady_clock::now();
   h->eng = std::make_unique<Engine>();
   h->eng->init(device_from_env());
@@ -448,9 +488,8 @@ void prepare_impl(const sdpx_csc* P, const sdpx_scalars* q, const sdpx_csc* A, c
   if (verbose_from_env()) {
     auto sec = [](auto a, auto b) { return std::chrono::duration<double>(b - a).count(); };
     std::fprintf(stderr,
-                 "sdpx_b200 prepare: copy+validate %.3f s, equilibrate %.3f s, device init %.3f s, "
-                 "upload %.3f s (%s)\n",
-                 tv, te, sec(t2, t3), sec(t3, t4), h->eng->upload_report().c_str());
+                 "sdpx_b200 prepare: device init %.3f s, upload %.3f s (%s)\n", sec(t2, t3),
+                 sec(t3, t4), h->eng->upload_report().c_str());
   }
   *out = h.release();
 }

@@ -198,8 +198,8 @@ __device__ __forceinline__ void cta_gemm(double* C, const double* A, bool ta, co
 // column for both, the same arithmetic per entry); a failed matrix stops being updated and
 // reports false, the other one carries on.
 // `piv` is SDPXG_CHOL_SCRATCH doubles of shared memory per matrix: pivots, reciprocals, roots.
-__device__ inline void cta_cholesky_lower2(double* A, double* B, int n, double* pivA, double* pivB,
-                                           bool* okA, bool* okB) {
+__device__ inline void cta_cholesky_lower2_smem(double* A, double* B, int n, double* pivA,
+                                                double* pivB, bool* okA, bool* okB) {
   double* pinvA = pivA + SDPXG_NMAX;
   double* pinvB = pivB + SDPXG_NMAX;
   const bool two = (B != nullptr);
@@ -261,6 +261,99 @@ __device__ inline void cta_cholesky_lower2(double* A, double* B, int n, double* 
     else SM(X, i, j) = 0.0;
   }
   __syncthreads();
+}
+
+// 1024-thread form: every entry stays in a register of its owner thread for the whole
+// factorisation -- thread t holds rows i = t % 64 of columns j = t / 64 + 16 p (p < 4) of each
+// matrix -- and column k is broadcast through a double-buffered shared row, so a column step is
+// one barrier, two shared reads per entry and no shared writes of the trailing matrix.  The
+// arithmetic per entry is the lagged update of the shared-memory form.
+__device__ inline void cta_cholesky_lower2_reg(double* A, double* B, int n, double* pivA,
+                                               double* pivB, bool* okA, bool* okB) {
+  __shared__ double colA[2][SDPXG_NMAX], colB[2][SDPXG_NMAX];
+  double* pinvA = pivA + SDPXG_NMAX;
+  double* pinvB = pivB + SDPXG_NMAX;
+  const bool two = (B != nullptr);
+  const int t = threadIdx.x, i = t & (SDPXG_NMAX - 1), j0 = t >> 6;
+  double a[4], b[4];
+  __syncthreads();  // the matrices were just written by other threads (loads, copies)
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int j = j0 + 16 * p;
+    const bool in = i < n && j < n;
+    a[p] = in ? SM(A, i, j) : 0.0;
+    b[p] = (in && two) ? SM(B, i, j) : 0.0;
+  }
+  if (t == 0 && n > 0) {
+    const double x = a[0];
+    pivA[0] = x;
+    pinvA[0] = (x > 0.0 && isfinite(x)) ? 1.0 / x : 0.0;
+    if (two) {
+      const double y = b[0];
+      pivB[0] = y;
+      pinvB[0] = (y > 0.0 && isfinite(y)) ? 1.0 / y : 0.0;
+    }
+  }
+  bool liveA = true, liveB = two;
+  for (int k = 0; k < n; ++k) {
+    const int buf = k & 1;
+    if (j0 == (k & 15) && i > k && i < n) {  // the owners of column k publish it (rows > k)
+      const int p = k >> 4;  // select, not a dynamic index: a[] and b[] stay in registers
+      colA[buf][i] = p == 0 ? a[0] : p == 1 ? a[1] : p == 2 ? a[2] : a[3];
+      if (two) colB[buf][i] = p == 0 ? b[0] : p == 1 ? b[1] : p == 2 ? b[2] : b[3];
+    }
+    __syncthreads();  // column k and pivot k (published in step k - 1) are visible
+    const double dA = pinvA[k];
+    const double dB = two ? pinvB[k] : 0.0;
+    liveA = liveA && dA != 0.0;
+    liveB = liveB && dB != 0.0;
+    if (!liveA && !liveB) break;
+    if (i > k && i < n) {
+      const double ciA = colA[buf][i];
+      const double ciB = two ? colB[buf][i] : 0.0;
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        const int j = j0 + 16 * p;
+        if (j <= k || j > i) continue;
+        if (liveA) a[p] = a[p] - ciA * colA[buf][j] * dA;
+        if (liveB) b[p] = b[p] - ciB * colB[buf][j] * dB;
+        if (i == k + 1 && j == k + 1) {  // the next pivot is final now
+          if (liveA) {
+            pivA[k + 1] = a[p];
+            pinvA[k + 1] = (a[p] > 0.0 && isfinite(a[p])) ? 1.0 / a[p] : 0.0;
+          }
+          if (liveB) {
+            pivB[k + 1] = b[p];
+            pinvB[k + 1] = (b[p] > 0.0 && isfinite(b[p])) ? 1.0 / b[p] : 0.0;
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  *okA = liveA;
+  *okB = liveB;
+  double* rootA = pinvA + SDPXG_NMAX;
+  double* rootB = pinvB + SDPXG_NMAX;
+  if (t < n) {
+    if (liveA) rootA[t] = sqrt(pivA[t]);
+    if (liveB) rootB[t] = sqrt(pivB[t]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int j = j0 + 16 * p;
+    if (i >= n || j >= n) continue;
+    if (liveA) SM(A, i, j) = (i > j) ? a[p] / rootA[j] : ((i == j) ? rootA[j] : 0.0);
+    if (liveB) SM(B, i, j) = (i > j) ? b[p] / rootB[j] : ((i == j) ? rootB[j] : 0.0);
+  }
+  __syncthreads();
+}
+
+__device__ inline void cta_cholesky_lower2(double* A, double* B, int n, double* pivA, double* pivB,
+                                           bool* okA, bool* okB) {
+  if (blockDim.x == 1024) cta_cholesky_lower2_reg(A, B, n, pivA, pivB, okA, okB);
+  else cta_cholesky_lower2_smem(A, B, n, pivA, pivB, okA, okB);
 }
 
 __device__ inline bool cta_cholesky_lower(double* A, int n, double* piv) {

@@ -331,11 +331,7 @@ k_margins(const BlockDesc* __restrict__ blocks, const double* __restrict__ v, lo
   cta_load_smat(X, v + (long)blockIdx.y * ld + bd.svec_off, n);
   __syncthreads();
   cta_tridiagonalize(X, n, dd, ee, work, red);
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    bool ok = true;
-    eig[k] = bisect_kth(dd, ee, n, k, &ok);
-    if (!ok) atomicOr(status, SDPXG_ST_EIG_FAIL);
-  }
+  cta_eig_all(dd, ee, n, eig, status);
   __syncthreads();
   if (threadIdx.x == 0) {
     double mn = eig[0], pos = 0.0;

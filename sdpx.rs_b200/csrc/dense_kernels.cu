@@ -259,16 +259,29 @@ extern "C" __global__ void k_trtri_diag(int m, const double* __restrict__ Dinv,
   }
 }
 
+// 8-byte asynchronous global -> shared copy; src_bytes 0 writes zero (masked element).
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool in) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
+               "r"(in ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
 // Level `level` >= 1 of the recursive inverse: groups of 2^level tiles, left half L (2^(level-1)
 // full tiles), right half R (possibly ragged).  phase 0: T = U[L,R] X[R,R] into Tmp[L,R];
 // phase 1: X[L,R] = -X[L,L] T.  X's strictly lower part is never stored: loads mask it to zero.
-// grid = (row tiles of L, column tiles of R, groups).  Dynamic shared memory: two tiles.
+// grid = (row tiles of L, column tiles of R, groups).  The K loop is a two-stage pipeline: the
+// next 64-wide chunk of both operands streams into shared memory (cp.async, zero-filled where
+// masked or out of range) while the tensor cores work on the current one.
+// Dynamic shared memory: two stages of two tiles.
 extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
 k_trinv_level(const double* __restrict__ F, double* __restrict__ Uinv, double* __restrict__ UinvT,
               double* __restrict__ Tmp, int n, int level, int phase) {
   extern __shared__ double tl_sm[];
-  double* As = tl_sm;               // [r + k * TI_LD]
-  double* Bs = As + CH_NB * TI_LD;  // [k + c * TI_LD]
   const int g = 1 << level, h = g >> 1;
   const int L0 = blockIdx.z * g * CH_NB;
   const int R0 = L0 + h * CH_NB;
@@ -289,6 +302,21 @@ k_trinv_level(const double* __restrict__ F, double* __restrict__ Uinv, double* _
   int kbeg = 0, kend = K;
   if (phase == 0) kend = min(K, (tn + 1) * CH_NB);
   else kbeg = tm * CH_NB;
+  // stage s: As = tl_sm + s * 2 * CH_NB * TI_LD ([r + k * TI_LD]), Bs = As + CH_NB * TI_LD
+  auto load = [&](int k0, int s) {
+    double* As = tl_sm + s * 2 * CH_NB * TI_LD;
+    double* Bs = As + CH_NB * TI_LD;
+    for (int e = threadIdx.x; e < CH_NB * CH_NB; e += blockDim.x) {
+      const int r = e % CH_NB, k = e / CH_NB;
+      const int gr = ar + tm * CH_NB + r, gc = ac + k0 + k;
+      const bool in = (tm * CH_NB + r < Ln) && (k0 + k < K) && !(phase == 1 && gr > gc);
+      cp_async8(As + r + k * TI_LD, in ? A + gr + (long)gc * n : A, in);
+      const int hr = br + k0 + r, hc = bc + tn * CH_NB + k;
+      const bool inb = (k0 + r < K) && (tn * CH_NB + k < Rn) && !(phase == 0 && hr > hc);
+      cp_async8(Bs + r + k * TI_LD, inb ? B + hr + (long)hc * n : B, inb);
+    }
+    cp_async_commit();
+  };
   // FP64 tensor cores: warp w owns the 8-column block w of the 64 x 64 output tile, eight
   // 8 x 8 accumulators; shared tiles with leading dimension TI_LD (4 mod 16: conflict-free
   // fragment reads).  Fragments: lane l holds A[l/4][l%4], B[l%4][l/4], C[l/4][2(l%4)+{0,1}].
@@ -296,18 +324,18 @@ k_trinv_level(const double* __restrict__ F, double* __restrict__ Uinv, double* _
   double acc[8][2];
 #pragma unroll
   for (int R = 0; R < 8; ++R) acc[R][0] = acc[R][1] = 0.0;
-  for (int k0 = kbeg; k0 < kend; k0 += CH_NB) {
-    __syncthreads();
-    for (int e = threadIdx.x; e < CH_NB * CH_NB; e += blockDim.x) {
-      int r = e % CH_NB, k = e / CH_NB;
-      int gr = ar + tm * CH_NB + r, gc = ac + k0 + k;
-      bool in = (tm * CH_NB + r < Ln) && (k0 + k < K) && !(phase == 1 && gr > gc);
-      As[r + k * TI_LD] = in ? A[gr + (long)gc * n] : 0.0;
-      int hr = br + k0 + r, hc = bc + tn * CH_NB + k;
-      bool inb = (k0 + r < K) && (tn * CH_NB + k < Rn) && !(phase == 0 && hr > hc);
-      Bs[r + k * TI_LD] = inb ? B[hr + (long)hc * n] : 0.0;
+  int s = 0;
+  if (kbeg < kend) load(kbeg, 0);
+  for (int k0 = kbeg; k0 < kend; k0 += CH_NB, s ^= 1) {
+    if (k0 + CH_NB < kend) {
+      load(k0 + CH_NB, s ^ 1);  // its buffer was released by the barrier that ended step k0-64
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
-    __syncthreads();
+    __syncthreads();  // chunk k0 is in shared memory for every thread
+    const double* As = tl_sm + s * 2 * CH_NB * TI_LD;
+    const double* Bs = As + CH_NB * TI_LD;
 #pragma unroll 4
     for (int ks = 0; ks < CH_NB / 4; ++ks) {
       const int kk = ks * 4 + q;
@@ -315,6 +343,7 @@ k_trinv_level(const double* __restrict__ F, double* __restrict__ Uinv, double* _
 #pragma unroll
       for (int R = 0; R < 8; ++R) dmma_m8n8k4(acc[R][0], acc[R][1], As[(8 * R + rr) + kk * TI_LD], b);
     }
+    __syncthreads();  // every warp is done with stage s before it is refilled
   }
 #pragma unroll
   for (int R = 0; R < 8; ++R)

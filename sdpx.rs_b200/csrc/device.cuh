@@ -4,6 +4,8 @@
 
 #include <atomic>
 #include <cstdint>
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -36,6 +38,52 @@ inline void copy_d2h(void* h, const void* d, size_t bytes, cudaStream_t st) {
   g_d2h_bytes += bytes;
 }
 
+// Device allocations are recycled through a process-wide cache instead of going back to the
+// driver: the next handle (an e2e loop, a new problem) takes the blocks the last one released,
+// without cudaMalloc's mapping cost and cudaFree's unmapping.  A block is released the way
+// cudaFree releases it -- after a device synchronisation, so no queued work can still touch it
+// when it is handed out again.  Best fit among cached blocks of at most twice the request; at
+// most kCacheBytes are kept per device (the largest blocks go back to the driver first).
+class DeviceCache {
+ public:
+  static constexpr size_t kCacheBytes = size_t(8) << 30;
+  static DeviceCache& get() {
+    static DeviceCache c;
+    return c;
+  }
+  // A cached block of at least `bytes` (its true size in *got), or nullptr.
+  void* take(size_t bytes, int dev, size_t* got) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto& f = free_[dev & 15];
+    auto it = f.lower_bound(bytes);
+    if (it == f.end() || it->first > 2 * bytes + (size_t(1) << 20)) return nullptr;
+    void* p = it->second;
+    *got = it->first;
+    held_[dev & 15] -= it->first;
+    f.erase(it);
+    return p;
+  }
+  // bytes: the size the block was allocated with
+  void give(void* p, size_t bytes, int dev) {
+    cudaDeviceSynchronize();  // what cudaFree would wait for
+    std::lock_guard<std::mutex> lk(mu_);
+    auto& f = free_[dev & 15];
+    f.emplace(bytes, p);
+    held_[dev & 15] += bytes;
+    while (held_[dev & 15] > kCacheBytes && !f.empty()) {
+      auto last = std::prev(f.end());
+      cudaFree(last->second);
+      held_[dev & 15] -= last->first;
+      f.erase(last);
+    }
+  }
+
+ private:
+  std::mutex mu_;
+  std::multimap<size_t, void*> free_[16];
+  size_t held_[16] = {};
+};
+
 // Device buffer with grow-only storage: alloc() reuses the allocation when it is large enough,
 // so a handle that is re-prepared with a new problem (batches of instances) allocates only when
 // a buffer grows, and never frees in between (cudaFree synchronises the whole device, which
@@ -44,14 +92,23 @@ template <typename T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
-  size_t cap = 0;
+  size_t cap = 0;    // elements the block holds
+  size_t bytes = 0;  // true size of the block (a cached block may be larger than asked for)
+  int dev = 0;
   DevBuf() = default;
   explicit DevBuf(size_t count) { alloc(count); }
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), cap(o.cap) { o.p = nullptr; o.n = o.cap = 0; }
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), cap(o.cap), bytes(o.bytes), dev(o.dev) {
+    o.p = nullptr;
+    o.n = o.cap = o.bytes = 0;
+  }
   DevBuf& operator=(DevBuf&& o) noexcept {
-    if (this != &o) { release(); p = o.p; n = o.n; cap = o.cap; o.p = nullptr; o.n = o.cap = 0; }
+    if (this != &o) {
+      release();
+      p = o.p; n = o.n; cap = o.cap; bytes = o.bytes; dev = o.dev;
+      o.p = nullptr; o.n = o.cap = o.bytes = 0;
+    }
     return *this;
   }
   ~DevBuf() { release(); }
@@ -63,14 +120,20 @@ struct DevBuf {
     release();
     n = count;
     if (count) {
-      check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
-      cap = count;
+      check(cudaGetDevice(&dev), "cudaGetDevice");
+      const size_t want = count * sizeof(T);
+      size_t got = want;
+      void* q = DeviceCache::get().take(want, dev, &got);
+      if (!q) check(cudaMalloc(&q, want), "cudaMalloc");
+      p = static_cast<T*>(q);
+      bytes = got;
+      cap = got / sizeof(T);
     }
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) DeviceCache::get().give(p, bytes, dev);
     p = nullptr;
-    n = cap = 0;
+    n = cap = bytes = 0;
   }
   void upload(const T* h, size_t count, cudaStream_t st) {
     copy_h2d(p, h, count * sizeof(T), st);
@@ -150,8 +213,8 @@ __global__ void k_gram_basis(const BlockDesc*, const int*, const int*, const int
 __global__ void k_gram_schur(const BlockDesc*, const int*, const int*, const int*, const long*,
                              const long*, const double*, const double*, double*);
 __global__ void k_gram_forward(const BlockDesc*, const int*, const int*, const int*, const int*,
-                               const long*, const double*, const double*, const double*, double,
-                               double, double*);
+                               const int*, const long*, const double*, const double*,
+                               const double*, double, double, double*, double*, unsigned*);
 __global__ void k_gram_adjoint(const BlockDesc*, const int*, const int*, const int*, const int*,
                                const long*, const double*, const double*, const double*, double*);
 __global__ void k_chol_dataflow(double*, int, int, const unsigned*, int, int*, double, double, int,

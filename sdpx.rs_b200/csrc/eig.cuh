@@ -146,11 +146,13 @@ __device__ inline void cta_tridiagonalize(double* A, int n, double* d, double* e
     for (int i = threadIdx.x; i < m; i += blockDim.x)
       v[i] = (i == 0 ? (x0 - alpha) : SM(A, k + 1 + i, k)) * vs;
     __syncthreads();
-    // p = A_sub v
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    // p = A_sub v: one warp per row, reading the row as column i (A_sub stays exactly
+    // symmetric: the rank-2 update below forms both triangles from the same two products)
+    for (int i = warp; i < m; i += nwarps) {
       double acc = 0.0;
-      for (int j = 0; j < m; ++j) acc = fma(SM(A, k + 1 + i, k + 1 + j), v[j], acc);
-      p[i] = acc;
+      for (int j = lane; j < m; j += 32) acc = fma(SM(A, k + 1 + j, k + 1 + i), v[j], acc);
+      acc = warp_sum(acc);
+      if (lane == 0) p[i] = acc;
     }
     __syncthreads();
     part = 0.0;
@@ -165,7 +167,8 @@ __device__ inline void cta_tridiagonalize(double* A, int n, double* d, double* e
     __syncthreads();
     for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
       int i = t % m, j = t / m;
-      SM(A, k + 1 + i, k + 1 + j) -= 2.0 * (v[i] * p[j] + p[i] * v[j]);
+      const double u = __dadd_rn(__dmul_rn(v[i], p[j]), __dmul_rn(p[i], v[j]));  // symmetric in i, j
+      SM(A, k + 1 + i, k + 1 + j) -= 2.0 * u;
     }
     __syncthreads();
   }
@@ -239,6 +242,42 @@ __device__ inline double cta_eig_min(const double* d, const double* e, int n, in
   }
   *ok = false;
   return 0.5 * (lo + hi);
+}
+
+// Every eigenvalue of the tridiagonal (d, e), ascending, into eig[0..n): 16-lane groups, one
+// eigenvalue per group, multisection with 15 Sturm counts per round (the bracket shrinks
+// 16-fold per round), the same convergence test as bisect_kth; no CTA barrier inside.
+// Sets the status bit SDPXG_ST_EIG_FAIL for an eigenvalue whose round bound was hit.
+__device__ inline void cta_eig_all(const double* d, const double* e, int n, double* eig,
+                                   uint32_t* status) {
+  double lo0, hi0, pivmin;
+  gershgorin(d, e, n, &lo0, &hi0, &pivmin);
+  constexpr int P = 16;
+  const int grp = threadIdx.x / P, sl = threadIdx.x % P, base = threadIdx.x & 16;
+  const unsigned gmask = 0xFFFFu << base;
+  for (int k = grp; k < n; k += blockDim.x / P) {
+    double lo = lo0, hi = hi0;
+    bool conv = false;
+    for (int round = 0; round < 64; ++round) {
+      if (!(hi - lo > 2.0 * 2.220446049250313e-16 * fmax(fabs(lo), fabs(hi)) + pivmin)) {
+        conv = true;
+        break;
+      }
+      const double step = (hi - lo) / P;
+      const double x = lo + step * (sl + 1);
+      const bool above = (sl < P - 1) && x > lo && x < hi && sturm_count(d, e, n, x, pivmin) > k;
+      const unsigned bal = (__ballot_sync(gmask, above) >> base) & 0xFFFFu;
+      const int c = bal ? __ffs(bal) - 1 : P - 1;  // eigenvalue k lies in cell c
+      const double nlo = (c == 0) ? lo : lo + step * c;
+      const double nhi = (c == P - 1) ? hi : lo + step * (c + 1);
+      lo = nlo;
+      hi = nhi;
+    }
+    if (sl == 0) {
+      eig[k] = 0.5 * (lo + hi);
+      if (!conv) atomicOr(status, SDPXG_ST_EIG_FAIL);
+    }
+  }
 }
 
 // k-th smallest eigenvalue (k = 0 is the minimum) by bisection; one thread.

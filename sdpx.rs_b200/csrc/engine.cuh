@@ -17,11 +17,14 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <numeric>
+#include <utility>
 #include <string>
 #include <unordered_map>
 
 #include "device.cuh"
+#include "host_parallel.h"
 
 namespace sdpxg {
 
@@ -36,7 +39,7 @@ constexpr size_t kSmemTrans = 3 * kMatD * sizeof(double);
 constexpr size_t kSmemTrsm = 2 * 64 * 65 * sizeof(double);
 constexpr size_t kSmemSyrk = 2 * 64 * 66 * sizeof(double);
 constexpr size_t kSmemTrtri = 2 * 64 * 65 * sizeof(double);
-constexpr size_t kSmemTrinv = 2 * 64 * 68 * sizeof(double);  // k_trinv_level (TI_LD 68)
+constexpr size_t kSmemTrinv = 4 * 64 * 68 * sizeof(double);  // k_trinv_level: 2 stages x 2 tiles
 constexpr size_t kSmemDf = (2 * 64 * 68 + 2 * 8 * 64) * sizeof(double);  // k_chol_dataflow
 constexpr size_t kSmemGram = 3 * kMatD * sizeof(double);                 // k_gram_basis/adjoint
 constexpr int kDfMaxTiles = 256;  // dataflow schedule up to m = 16384 (nt^3/6 items)
@@ -139,12 +142,38 @@ inline bool chol_schedule_valid(const std::vector<unsigned>& it, int nt) {
 constexpr int kNB = 64;
 
 // Equilibrated problem in host memory (CSC, int64 indices as in the reference ABI).
+// std::vector storage whose resize() leaves new elements default-initialised (unset for
+// arithmetic types): the large CSC arrays of a prepare are written right away by parallel loops,
+// so zero-filling them first on one thread -- and taking every first-touch page fault there --
+// is wasted time.
+template <typename T>
+struct UninitAlloc : std::allocator<T> {
+  using value_type = T;
+  template <class U>
+  struct rebind {
+    using other = UninitAlloc<U>;
+  };
+  UninitAlloc() = default;
+  template <class U>
+  UninitAlloc(const UninitAlloc<U>&) noexcept {}
+  template <class U>
+  void construct(U* ptr) noexcept {
+    ::new (static_cast<void*>(ptr)) U;
+  }
+  template <class U, class... Args>
+  void construct(U* ptr, Args&&... args) {
+    ::new (static_cast<void*>(ptr)) U(std::forward<Args>(args)...);
+  }
+};
+using I64Vec = std::vector<int64_t, UninitAlloc<int64_t>>;
+using F64Vec = std::vector<double, UninitAlloc<double>>;
+
 struct HostProblem {
   int n = 0, m = 0;
   std::vector<int64_t> Pcolptr, Prow;
   std::vector<double> Pval;
-  std::vector<int64_t> Acolptr, Arow;
-  std::vector<double> Aval;
+  I64Vec Acolptr, Arow;
+  F64Vec Aval;
   std::vector<double> q, b;
   std::vector<int> psd;  // PSD block orders in cone order
   // all cones in order: (1, d) nonnegative orthant of dimension d, (3, d) PSD triangle of order d;
@@ -362,26 +391,31 @@ class Engine {
     }
     nblk = (int)hblocks.size();
     nnn_ = (int)nn_rows.size();
-    // per-block dense column storage of A
+    // per-block dense column storage of A.  Columns of A are independent: the block memberships,
+    // the dense columns and the rank-one tests run on the host threads (rows within a column are
+    // sorted, so a block's entries are one contiguous range found by binary search).
     hk.assign(nblk, 0);
-    std::vector<std::vector<int>> bcols(nblk);
     std::vector<std::vector<std::pair<int, int>>> c2b(n);  // (block, local)
-    for (int c = 0; c < n; ++c) {
-      int64_t p0 = p.Acolptr[c], p1 = p.Acolptr[c + 1];
-      int64_t q0 = p0;
-      for (int j = 0; j < nblk && q0 < p1; ++j) {
-        int r0 = hblocks[j].svec_off, r1 = r0 + hblocks[j].n * (hblocks[j].n + 1) / 2;
-        while (q0 < p1 && p.Arow[q0] < r0) ++q0;
-        int64_t q1 = q0;
-        while (q1 < p1 && p.Arow[q1] < r1) ++q1;
-        if (q1 > q0) {
-          c2b[c].push_back({j, hk[j]});
-          bcols[j].push_back(c);
-          hk[j]++;
+    parallel_for(n, col_grain(n, p.Aval.size()), [&](int64_t c0, int64_t c1, int) {
+      for (int64_t c = c0; c < c1; ++c) {
+        const int64_t p0 = p.Acolptr[c], p1 = p.Acolptr[c + 1];
+        int64_t q0 = p0;
+        for (int j = 0; j < nblk && q0 < p1; ++j) {
+          const int r0 = hblocks[j].svec_off, r1 = r0 + hblocks[j].n * (hblocks[j].n + 1) / 2;
+          q0 = std::lower_bound(p.Arow.begin() + q0, p.Arow.begin() + p1, (int64_t)r0) - p.Arow.begin();
+          const int64_t q1 =
+              std::lower_bound(p.Arow.begin() + q0, p.Arow.begin() + p1, (int64_t)r1) - p.Arow.begin();
+          if (q1 > q0) c2b[c].push_back({j, 0});
+          q0 = q1;
         }
-        q0 = q1;
       }
-    }
+    });
+    std::vector<std::vector<int>> bcols(nblk);
+    for (int c = 0; c < n; ++c)
+      for (auto& e : c2b[c]) {
+        e.second = hk[e.first]++;
+        bcols[e.first].push_back(c);
+      }
     std::vector<long> acol_off(nblk), s_off(nblk);
     std::vector<int> col_ptr(nblk + 1, 0), col_idx;
     long aoff = 0, soff = 0;
@@ -394,42 +428,60 @@ class Engine {
       col_ptr[j + 1] = col_ptr[j] + hk[j];
       col_idx.insert(col_idx.end(), bcols[j].begin(), bcols[j].end());
     }
-    std::vector<double> acol(aoff, 0.0);
-    for (int j = 0; j < nblk; ++j) {
-      int r0 = hblocks[j].svec_off, tn = hblocks[j].n * (hblocks[j].n + 1) / 2;
-      for (int t = 0; t < hk[j]; ++t) {
-        int c = bcols[j][t];
-        for (int64_t q = p.Acolptr[c]; q < p.Acolptr[c + 1]; ++q) {
-          int64_t r = p.Arow[q];
-          if (r >= r0 && r < r0 + tn) acol[acol_off[j] + (long)t * tn + (r - r0)] = p.Aval[q];
-        }
+    // (block, local column) items in block order: item i is column i - col_ptr[j] of block j
+    const int nitems = col_ptr[nblk];
+    std::vector<int> item_blk(nitems);
+    for (int j = 0; j < nblk; ++j)
+      for (int t = col_ptr[j]; t < col_ptr[j + 1]; ++t) item_blk[t] = j;
+    F64Vec acol(aoff);
+    const int64_t item_grain = std::max<int64_t>(1, nitems * 65536LL / std::max<int64_t>(aoff, 1));
+    parallel_for(nitems, item_grain, [&](int64_t i0, int64_t i1, int) {
+      for (int64_t it = i0; it < i1; ++it) {
+        const int j = item_blk[it], t = (int)(it - col_ptr[j]), c = bcols[j][t];
+        const int r0 = hblocks[j].svec_off, tn = hblocks[j].n * (hblocks[j].n + 1) / 2;
+        double* dst = &acol[acol_off[j] + (long)t * tn];
+        std::fill(dst, dst + tn, 0.0);
+        const int64_t p1 = p.Acolptr[c + 1];
+        int64_t q = std::lower_bound(p.Arow.begin() + p.Acolptr[c], p.Arow.begin() + p1, (int64_t)r0) -
+                    p.Arow.begin();
+        for (; q < p1 && p.Arow[q] < r0 + tn; ++q) dst[p.Arow[q] - r0] = p.Aval[q];
       }
-    }
+    });
     const auto u1 = std::chrono::steady_clock::now();
     // rank-one (Gram) blocks keep only their factor; the others keep dense columns
     std::vector<char> gram(nblk, 0);
     std::vector<long> gu_off(nblk, 0);
     std::vector<double> gu, gsig(col_ptr[nblk], 1.0);
     ngram_ = 0;
-    for (int j = 0; j < nblk && gram_enabled; ++j) {
-      const int nj = hblocks[j].n, tn = nj * (nj + 1) / 2;
-      if (hk[j] == 0) continue;
-      std::vector<double> uj((size_t)nj * hk[j]);
-      bool ok = true;
-      for (int t = 0; t < hk[j] && ok; ++t)
-        ok = rank_one_column(&acol[acol_off[j] + (long)t * tn], nj, &uj[(size_t)t * nj],
-                             &gsig[col_ptr[j] + t]);
-      if (!ok) {
-        for (int t = 0; t < hk[j]; ++t) gsig[col_ptr[j] + t] = 1.0;
-        continue;
+    if (gram_enabled) {
+      std::vector<long> u_off(nblk + 1, 0);
+      for (int j = 0; j < nblk; ++j) u_off[j + 1] = u_off[j] + (long)hblocks[j].n * hk[j];
+      std::vector<double> u_all(u_off[nblk]);
+      std::vector<char> col_ok(nitems, 0);
+      parallel_for(nitems, item_grain, [&](int64_t i0, int64_t i1, int) {
+        for (int64_t it = i0; it < i1; ++it) {
+          const int j = item_blk[it], t = (int)(it - col_ptr[j]);
+          const int nj = hblocks[j].n, tn = nj * (nj + 1) / 2;
+          col_ok[it] = rank_one_column(&acol[acol_off[j] + (long)t * tn], nj,
+                                       &u_all[u_off[j] + (long)t * nj], &gsig[it]);
+        }
+      });
+      for (int j = 0; j < nblk; ++j) {
+        if (hk[j] == 0) continue;
+        bool ok = true;
+        for (int t = col_ptr[j]; t < col_ptr[j + 1] && ok; ++t) ok = col_ok[t] != 0;
+        if (!ok) {
+          for (int t = col_ptr[j]; t < col_ptr[j + 1]; ++t) gsig[t] = 1.0;
+          continue;
+        }
+        gram[j] = 1;
+        ngram_++;
+        gu_off[j] = (long)gu.size();
+        gu.insert(gu.end(), u_all.begin() + u_off[j], u_all.begin() + u_off[j + 1]);
       }
-      gram[j] = 1;
-      ngram_++;
-      gu_off[j] = (long)gu.size();
-      gu.insert(gu.end(), uj.begin(), uj.end());
     }
     if (ngram_ > 0) {  // repack the dense columns of the ordinary blocks only
-      std::vector<double> packed;
+      F64Vec packed;
       long off = 0;
       for (int j = 0; j < nblk; ++j) {
         const long len = (long)hblocks[j].n * (hblocks[j].n + 1) / 2 * hk[j];
@@ -488,6 +540,9 @@ class Engine {
     gitem_blk_.alloc(std::max(ngitem_, 1)); gitem_blk_.upload(gitem_blk.data(), gitem_blk.size(), st);
     gitem_c0_.alloc(std::max(ngitem_, 1)); gitem_c0_.upload(gitem_c0.data(), gitem_c0.size(), st);
     gblk_.alloc(std::max(ngblk_, 1)); gblk_.upload(gblk.data(), gblk.size(), st);
+    gf_part_.alloc((size_t)std::max(ngitem_, 1) * SDPXG_NMAX * SDPXG_NMAX);
+    gf_cnt_.alloc(std::max(nblk, 1));
+    check(cudaMemsetAsync(gf_cnt_.p, 0, std::max(nblk, 1) * sizeof(unsigned), st), "gram tickets");
     nwork_ = (int)wblk.size();
     ntiles_ = (int)tiles.size() / 3;
     // symmetric P in CSR (both triangles) for the x-row products
@@ -749,8 +804,9 @@ class Engine {
       launched("k_op_forward");
     }
     if (ngblk_) {
-      ++g_launches, k_gram_forward<<<dim3(ngblk_, SDPXG_NMAX / 8), 256, 0, st>>>(
-          blocks_, gblk_, kcount_, col_ptr_, col_idx_, gu_off_, gsig_, gU_, x, alpha, beta, y);
+      ++g_launches, k_gram_forward<<<ngitem_, 256, 0, st>>>(
+          blocks_, gitem_blk_, gitem_c0_, kcount_, col_ptr_, col_idx_, gu_off_, gsig_, gU_, x,
+          alpha, beta, y, gf_part_, gf_cnt_);
       launched("k_gram_forward");
     }
   }
@@ -956,6 +1012,8 @@ class Engine {
   DevBuf<double> gU_, gV_, gsig_;
   DevBuf<long> gu_off_;
   DevBuf<int> gtiles_, gitem_blk_, gitem_c0_, gblk_;
+  DevBuf<double> gf_part_;  // k_gram_forward chunk partials (64 x 64 per item)
+  DevBuf<unsigned> gf_cnt_;  // its per-block arrival tickets (self-resetting)
   int ngram_ = 0, ngtiles_ = 0, ngitem_ = 0, ngblk_ = 0, ncol_ = 0;
   DevBuf<int> prp_, pci_, pup_ptr_, pup_row_;
   DevBuf<double> pv_, pup_val_;

@@ -118,62 +118,77 @@ k_gram_schur(const BlockDesc* __restrict__ blocks, const int* __restrict__ tiles
     }
 }
 
-// y_j = alpha svec(U_j diag(sigma x_cols) U_j') + beta y_j.  Grid (Gram block, 8-row tile R):
-// warp w computes the 8 x 8 output tile (R, w) for w >= R (upper triangle) on the FP64 tensor
-// cores.  K = k_j runs in chunks of 64 columns of U staged in shared memory (coalesced loads,
-// column t at Us[t * GR_LD + row]: conflict-free fragment reads) with their scaled weights
-// d_t = sigma_t x[col_t].
+// y_j = alpha svec(U_j diag(sigma x_cols) U_j') + beta y_j, K = k_j split in 64-column chunks.
+// One CTA per (Gram block, chunk) item (the items of a block are consecutive, chunk order):
+// it stages its 64 columns of U (coalesced, column t at Us[t * GR_LD + row], zero padded) and
+// their weights d_t = sigma_t x[col_t], forms the upper 8 x 8 tiles of U_c diag(d) U_c' on the
+// FP64 tensor cores (one warp per tile) into part[item] (64 x 64, column-major), and takes a
+// ticket on cnt[j].  The block's last CTA (the ticket is reset for the next launch) sums the
+// chunk partials in chunk order -- the same result for every arrival order -- and writes y.
 #define GR_KCH 64
 extern "C" __global__ void __launch_bounds__(256)
-k_gram_forward(const BlockDesc* __restrict__ blocks, const int* __restrict__ gblk,
-               const int* __restrict__ kcount, const int* __restrict__ col_ptr,
-               const int* __restrict__ col_idx, const long* __restrict__ gu_off,
-               const double* __restrict__ gsig, const double* __restrict__ U,
-               const double* __restrict__ x, double alpha, double beta, double* __restrict__ y) {
+k_gram_forward(const BlockDesc* __restrict__ blocks, const int* __restrict__ item_blk,
+               const int* __restrict__ item_c0, const int* __restrict__ kcount,
+               const int* __restrict__ col_ptr, const int* __restrict__ col_idx,
+               const long* __restrict__ gu_off, const double* __restrict__ gsig,
+               const double* __restrict__ U, const double* __restrict__ x, double alpha,
+               double beta, double* __restrict__ y, double* __restrict__ part,
+               unsigned* __restrict__ cnt) {
   __shared__ __align__(16) double Us[GR_KCH * GR_LD];
   __shared__ double d[GR_KCH];
-  const int j = gblk[blockIdx.x], R = blockIdx.y;
+  __shared__ bool last;
+  const int it = blockIdx.x, j = item_blk[it], c0 = item_c0[it];
   const BlockDesc bd = blocks[j];
-  const int n = bd.n, k = kcount[j];
-  if (8 * R >= n) return;
+  const int n = bd.n, k = kcount[j], kc = min(GR_KCH, k - c0);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, r = lane >> 2, q = lane & 3;
   const double* Uj = U + gu_off[j];
-  const int* cols = col_idx + col_ptr[j];
-  const double* sg = gsig + col_ptr[j];
-  for (int e = threadIdx.x; e < GR_KCH * GR_LD; e += blockDim.x) Us[e] = 0.0;  // rows >= n stay 0
-  const bool live = (w >= R) && (8 * w < n);
-  double d0 = 0.0, d1 = 0.0;
-  for (int t0 = 0; t0 < k; t0 += GR_KCH) {
-    const int kc = min(GR_KCH, k - t0);
-    __syncthreads();  // the zero fill, or the previous chunk's reads, are done
-    for (int e = threadIdx.x; e < n * kc; e += blockDim.x) {
-      const int t = e / n, row = e - t * n;
-      Us[t * GR_LD + row] = Uj[(long)(t0 + t) * n + row];
-    }
-    for (int t = threadIdx.x; t < GR_KCH; t += blockDim.x)
-      d[t] = (t < kc) ? sg[t0 + t] * x[cols[t0 + t]] : 0.0;
-    __syncthreads();
-    if (live) {
-#pragma unroll 4
-      for (int ks = 0; ks < GR_KCH / 4; ++ks) {
-        const int t = 4 * ks + q;
-        const double a = d[t] * Us[t * GR_LD + 8 * R + r];  // (U diag(d))[row][t]
-        const double b = Us[t * GR_LD + 8 * w + r];          // U'[t][col]
-        dmma_m8n8k4(d0, d1, a, b);
-      }
-    }
+  for (int e = threadIdx.x; e < GR_KCH * GR_LD; e += blockDim.x) {
+    const int t = e / GR_LD, row = e - t * GR_LD;
+    Us[e] = (t < kc && row < n) ? Uj[(long)(c0 + t) * n + row] : 0.0;
   }
-  if (!live) return;
-  const int orow = 8 * R + r;
-#pragma unroll
-  for (int e = 0; e < 2; ++e) {
-    const int ocol = 8 * w + 2 * q + e;
-    if (orow <= ocol && ocol < n) {
-      const double v = (e == 0) ? d0 : d1;
-      const long idx = bd.svec_off + (long)ocol * (ocol + 1) / 2 + orow;
-      const double s = (orow == ocol) ? v : v * SDPXG_SQRT2;
-      y[idx] = alpha * s + ((beta == 0.0) ? 0.0 : beta * y[idx]);
+  for (int t = threadIdx.x; t < GR_KCH; t += blockDim.x)
+    d[t] = (t < kc) ? gsig[col_ptr[j] + c0 + t] * x[col_idx[col_ptr[j] + c0 + t]] : 0.0;
+  __syncthreads();
+  double* P = part + (size_t)it * (SDPXG_NMAX * SDPXG_NMAX);
+  const int T = (n + 7) >> 3, ntile = T * (T + 1) / 2;
+  for (int tile = w; tile < ntile; tile += (int)(blockDim.x >> 5)) {
+    int J = 0, I = tile;  // upper tiles column by column: (0,0), (0,1), (1,1), (0,2), ...
+    while (I > J) {
+      I -= J + 1;
+      ++J;
     }
+    double d0 = 0.0, d1 = 0.0;
+#pragma unroll 4
+    for (int ks = 0; ks < GR_KCH / 4; ++ks) {
+      const int t = 4 * ks + q;
+      const double a = d[t] * Us[t * GR_LD + 8 * I + r];  // (U diag(d))[row][t]
+      const double b = Us[t * GR_LD + 8 * J + r];          // U'[t][col]
+      dmma_m8n8k4(d0, d1, a, b);
+    }
+    P[(8 * J + 2 * q) * SDPXG_NMAX + 8 * I + r] = d0;
+    P[(8 * J + 2 * q + 1) * SDPXG_NMAX + 8 * I + r] = d1;
+  }
+  __threadfence();
+  __syncthreads();
+  const int nch = (k + GR_KCH - 1) / GR_KCH;
+  if (threadIdx.x == 0) {
+    const unsigned tk = atomicAdd(&cnt[j], 1u);
+    last = (tk == (unsigned)(nch - 1));
+    if (last) cnt[j] = 0u;  // ready for the next launch (stream order)
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const double* P0 = part + (size_t)(it - c0 / GR_KCH) * (SDPXG_NMAX * SDPXG_NMAX);
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int row = e % n, col = e / n;
+    if (row > col) continue;
+    double v = 0.0;
+    for (int c = 0; c < nch; ++c)
+      v += __ldcg(P0 + (size_t)c * (SDPXG_NMAX * SDPXG_NMAX) + col * SDPXG_NMAX + row);
+    const long idx = bd.svec_off + (long)col * (col + 1) / 2 + row;
+    const double s2 = (row == col) ? v : v * SDPXG_SQRT2;
+    y[idx] = alpha * s2 + ((beta == 0.0) ? 0.0 : beta * y[idx]);
   }
 }
 

@@ -72,8 +72,8 @@ void to_host(double* h, const DevBuf<double>& buf, size_t n, cudaStream_t st) {
   check(cudaMemcpyAsync(h, buf.p, n * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
   check(cudaStreamSynchronize(st), "sync");
 }
-void csc_into(const sdpx_csc* m, std::vector<int64_t>& cp, std::vector<int64_t>& rv,
-              std::vector<double>& v, uint64_t cols) {
+template <class IC, class IR, class DV>
+void csc_into(const sdpx_csc* m, IC& cp, IR& rv, DV& v, uint64_t cols) {
   cp.assign(cols + 1, 0);
   rv.clear();
   v.clear();

@@ -125,27 +125,20 @@ class _CscHold:
         self.c = c
 
 
-class DefaultSolver:
-    """GPU solve through the reference-compatible C ABI (sdpx_prepare / sdpx_solve)."""
+class CProblem:
+    """A problem in the C ABI's host layout: sdpx_csc / sdpx_scalars / sdpx_cone / sdpx_settings
+    views over numpy buffers this object keeps alive (what a C or Rust caller of sdpx_prepare
+    holds).  Building it converts scipy/numpy inputs once; sdpx_prepare then reads it."""
 
     def __init__(self, P, q, A, b, cones: Sequence[Tuple[str, int]],
-                 settings: Optional[DefaultSettings] = None):
-        args = self._c_args(P, q, A, b, cones, settings)
-        h = C.c_void_p()
-        _lib.call("sdpx_prepare", *args, C.byref(h))
-        self._h = h
-        self.solution: Optional[Solution] = None
-        self.info: Optional[SolveInfo] = None
-
-    def _c_args(self, P, q, A, b, cones, settings):
-        """C views of a problem (the numpy buffers are kept alive on self)."""
+                 settings: Optional["DefaultSettings"] = None):
         settings = settings or DefaultSettings()
         A = sp.csc_matrix(A, dtype=np.float64)
         n = A.shape[1]
         P = sp.csc_matrix((n, n)) if P is None else sp.triu(sp.csc_matrix(P, dtype=np.float64)).tocsc()
-        self._q = np.ascontiguousarray(q, dtype=np.float64)
-        self._b = np.ascontiguousarray(b, dtype=np.float64)
-        self._P, self._A = _CscHold(P), _CscHold(A)
+        self.q = np.ascontiguousarray(q, dtype=np.float64)
+        self.b = np.ascontiguousarray(b, dtype=np.float64)
+        self.P, self.A = _CscHold(P), _CscHold(A)
         cone_arr = (_lib.Cone * max(len(cones), 1))()
         for i, (kind, d) in enumerate(cones):
             cone_arr[i].kind = CONE_KINDS[kind]
@@ -153,16 +146,51 @@ class DefaultSolver:
             cone_arr[i].dim = int(d)
             cone_arr[i].alpha = _scalars(np.zeros(0))
         cs, self._keep = settings.to_c()
-        self._cones, self._cs = cone_arr, cs
+        self.cones, self.cs = cone_arr, cs
         self.n, self.m = n, A.shape[0]
-        return (C.byref(self._P.c), C.byref(_scalars(self._q)), C.byref(self._A.c),
-                C.byref(_scalars(self._b)), cone_arr, len(cones), C.byref(cs))
+        self.args = (C.byref(self.P.c), C.byref(_scalars(self.q)), C.byref(self.A.c),
+                     C.byref(_scalars(self.b)), cone_arr, len(cones), C.byref(cs))
+
+
+class DefaultSolver:
+    """GPU solve through the reference-compatible C ABI (sdpx_prepare / sdpx_solve)."""
+
+    def __init__(self, P, q, A, b, cones: Sequence[Tuple[str, int]],
+                 settings: Optional[DefaultSettings] = None):
+        self._prepare(CProblem(P, q, A, b, cones, settings))
+
+    @classmethod
+    def from_c_problem(cls, cp: CProblem) -> "DefaultSolver":
+        """sdpx_prepare on a problem already in the C ABI's host layout."""
+        self = cls.__new__(cls)
+        self._prepare(cp)
+        return self
+
+    def _prepare(self, cp: CProblem):
+        self._hold(cp)
+        h = C.c_void_p()
+        _lib.call("sdpx_prepare", *cp.args, C.byref(h))
+        self._h = h
+        self.solution: Optional[Solution] = None
+        self.info: Optional[SolveInfo] = None
+
+    def _hold(self, cp: CProblem):
+        self._cp, self._A = cp, cp.A
+        self.n, self.m = cp.n, cp.m
+
+    def close(self):
+        """sdpx_destroy now (otherwise at garbage collection)."""
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _lib.load().sdpx_destroy(h)
+            self._h = None
 
     def reprepare(self, P, q, A, b, cones: Sequence[Tuple[str, int]],
                   settings: Optional[DefaultSettings] = None):
         """Load another problem into this handle, reusing its device buffers and stream."""
-        args = self._c_args(P, q, A, b, cones, settings)
-        _lib.call("sdpx_b200_reprepare", self._h, *args)
+        cp = CProblem(P, q, A, b, cones, settings)
+        self._hold(cp)
+        _lib.call("sdpx_b200_reprepare", self._h, *cp.args)
         self.solution = None
         self.info = None
 
