@@ -114,60 +114,52 @@ __device__ inline int cta_jacobi_svd(double* M, double* V, int n, int* flag, dou
 }
 
 // Householder tridiagonalisation of the symmetric A (destroyed).  d[0..n), e[0..n-1).
-// `work` is 2*n doubles of shared memory, `red` 32 doubles.
+// `work` is 2*n doubles of shared memory, `red` 32 doubles (unused: kept for the callers).
+// Step k reflects column k below the diagonal, x = A[k+1:n, k] (m <= 63 entries): every warp
+// forms |x|^2 and, after the matvec, v'p itself (one warp covers the whole vector, and every
+// warp gets the same value from the same butterfly), v and q = p - (v'p) v are formed inline
+// from column k (which the step does not modify), so a step needs two barriers: after p = A v
+// (one warp per row, reading the row as a column: A stays exactly symmetric) and after the
+// rank-2 update.
 __device__ inline void cta_tridiagonalize(double* A, int n, double* d, double* e, double* work,
-                                   double* red) {
-  double* v = work;
-  double* p = work + n;
+                                          double* red) {
+  (void)red;
+  double* p = work;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (int k = 0; k + 2 < n; ++k) {
     const int m = n - k - 1;  // length of the column below the diagonal
-    // ||x||^2 of x = A[k+1:n, k]
+    const double* x = &SM(A, k + 1, k);
     double part = 0.0;
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
-      double x = SM(A, k + 1 + i, k);
-      part = fma(x, x, part);
-    }
-    part = warp_sum(part);
-    if (lane == 0) red[warp] = part;
-    __syncthreads();
-    double nrm2 = 0.0;
-    for (int w = 0; w < nwarps; ++w) nrm2 += red[w];
-    double x0 = SM(A, k + 1, k);
-    double alpha = -copysign(sqrt(nrm2), x0);
-    double vnorm2 = nrm2 - x0 * x0 + (x0 - alpha) * (x0 - alpha);
+    for (int i = lane; i < m; i += 32) part = fma(x[i], x[i], part);
+    const double nrm2 = warp_sum(part);
+    const double x0 = x[0];
+    const double alpha = -copysign(sqrt(nrm2), x0);
+    const double vnorm2 = nrm2 - x0 * x0 + (x0 - alpha) * (x0 - alpha);
     if (threadIdx.x == 0) {
       d[k] = SM(A, k, k);
       e[k] = (nrm2 == 0.0) ? 0.0 : alpha;
     }
-    __syncthreads();
     if (nrm2 == 0.0 || vnorm2 == 0.0) continue;  // column already reduced (uniform)
-    double vs = rsqrt(vnorm2);
-    for (int i = threadIdx.x; i < m; i += blockDim.x)
-      v[i] = (i == 0 ? (x0 - alpha) : SM(A, k + 1 + i, k)) * vs;
-    __syncthreads();
-    // p = A_sub v: one warp per row, reading the row as column i (A_sub stays exactly
-    // symmetric: the rank-2 update below forms both triangles from the same two products)
+    const double vs = rsqrt(vnorm2);
+    const double v0 = (x0 - alpha) * vs;
+    // p = A_sub v
     for (int i = warp; i < m; i += nwarps) {
       double acc = 0.0;
-      for (int j = lane; j < m; j += 32) acc = fma(SM(A, k + 1 + j, k + 1 + i), v[j], acc);
+      for (int j = lane; j < m; j += 32)
+        acc = fma(SM(A, k + 1 + j, k + 1 + i), (j == 0) ? v0 : x[j] * vs, acc);
       acc = warp_sum(acc);
       if (lane == 0) p[i] = acc;
     }
     __syncthreads();
-    part = 0.0;
-    for (int i = threadIdx.x; i < m; i += blockDim.x) part = fma(v[i], p[i], part);
-    part = warp_sum(part);
-    if (lane == 0) red[warp] = part;
-    __syncthreads();
-    double K = 0.0;
-    for (int w = 0; w < nwarps; ++w) K += red[w];
-    __syncthreads();
-    for (int i = threadIdx.x; i < m; i += blockDim.x) p[i] = p[i] - K * v[i];  // q
-    __syncthreads();
+    double kp = 0.0;
+    for (int i = lane; i < m; i += 32) kp = fma((i == 0) ? v0 : x[i] * vs, p[i], kp);
+    const double K = warp_sum(kp);
+    // A_sub -= 2 (v q' + q v'), q = p - K v (both triangles from the same two products)
     for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
-      int i = t % m, j = t / m;
-      const double u = __dadd_rn(__dmul_rn(v[i], p[j]), __dmul_rn(p[i], v[j]));  // symmetric in i, j
+      const int i = t % m, j = t / m;
+      const double vi = (i == 0) ? v0 : x[i] * vs, vj = (j == 0) ? v0 : x[j] * vs;
+      const double qi = p[i] - K * vi, qj = p[j] - K * vj;
+      const double u = __dadd_rn(__dmul_rn(vi, qj), __dmul_rn(qi, vj));
       SM(A, k + 1 + i, k + 1 + j) -= 2.0 * u;
     }
     __syncthreads();
@@ -214,14 +206,17 @@ __device__ __forceinline__ void gershgorin(const double* d, const double* e, int
   *pivmin = 2.2250738585072014e-308 * fmax(1.0, emax);
 }
 
-// Smallest eigenvalue of the tridiagonal (d, e) by CTA-wide multisection: each round every
-// thread evaluates one Sturm count on an even grid over the current bracket and the bracket
-// shrinks to the first grid cell holding an eigenvalue (about blockDim-fold per round).
+// Smallest eigenvalue of the tridiagonal (d, e) by CTA-wide multisection: each round T threads
+// evaluate one Sturm count each on an even grid over the current bracket and the bracket
+// shrinks to the first grid cell holding an eigenvalue (about T-fold per round).  T = 512: a
+// Sturm count is a chain of n dependent divisions, and with more than 16 warps per SM evaluating
+// them the rounds become bound by FP64 issue rather than by that chain, so 1024 points cost
+// twice as long per round for one more bit.
 // Uniform result; `best` is one int of shared memory.  *ok = false if the round bound is hit.
 __device__ inline double cta_eig_min(const double* d, const double* e, int n, int* best, bool* ok) {
   double lo, hi, pivmin;
   gershgorin(d, e, n, &lo, &hi, &pivmin);
-  const int T = blockDim.x;
+  const int T = min((int)blockDim.x, 512);
   for (int round = 0; round < 16; ++round) {
     if (!(hi - lo > 2.0 * 2.220446049250313e-16 * fmax(fabs(lo), fabs(hi)) + pivmin)) {
       *ok = true;
@@ -231,7 +226,8 @@ __device__ inline double cta_eig_min(const double* d, const double* e, int n, in
     if (threadIdx.x == 0) *best = T;
     __syncthreads();
     const double x = lo + step * (threadIdx.x + 1);
-    if (x > lo && x < hi && sturm_count(d, e, n, x, pivmin) >= 1) atomicMin(best, (int)threadIdx.x);
+    if ((int)threadIdx.x < T && x > lo && x < hi && sturm_count(d, e, n, x, pivmin) >= 1)
+      atomicMin(best, (int)threadIdx.x);
     __syncthreads();
     const int t = *best;
     __syncthreads();
