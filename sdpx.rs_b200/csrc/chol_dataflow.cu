@@ -6,10 +6,12 @@
 // system (m of a few thousand) that chain is latency-bound: every diagonal tile waits for the
 // previous step's trailing update.  Here the whole factorization is ONE launch:
 //
-//  * work items are the tile tasks POTRF(k), TRSM(k, j), GEMM(k, i, j) of the right-looking
-//    algorithm, listed on the host in a topological order with one step of look-ahead
-//    (row k + 1 of step k's update, then POTRF(k + 1) and its TRSM row, then the rest of step
-//    k's update), so the critical path overlaps the bulk of the trailing updates;
+//  * the critical path -- GEMM(k-1, k, k), POTRF(k), TRSM(k, k+1) for every k -- is ONE work
+//    item, the chain (ticket 0): a single CTA keeps the diagonal tile, U_kk^-1 and U(k, k+1) in
+//    shared memory from one step to the next, so the path carries no tile reloads and no hand-
+//    offs between CTAs; it waits only for the other CTAs' trailing updates of its next tiles;
+//  * the remaining tile tasks TRSM(k, j > k+1) and GEMM(k, i, j) are listed on the host step by
+//    step (rows k+1, k+2 first: they feed the chain's next steps);
 //  * each CTA takes the next item with an atomic ticket and waits for the item's inputs on
 //    per-tile progress words in global memory (acquire/release at GPU scope).  The item with
 //    the smallest unfinished ticket always has all inputs ready, and a ticket is only taken by
@@ -32,7 +34,7 @@
 #define DF_SPIN_LIMIT (1 << 22)
 #define DFS(A, i, j) (A)[(i) + (j) * DF_LD]
 
-enum : unsigned { DF_POTRF = 0u, DF_TRSM = 1u, DF_GEMM = 2u };
+enum : unsigned { DF_POTRF = 0u, DF_TRSM = 1u, DF_GEMM = 2u, DF_CHAIN = 3u };
 
 __device__ __forceinline__ int df_ld_acquire(const int* p) {
   int v;
@@ -240,6 +242,105 @@ __device__ bool df_potrf_tile(double* A, double* X, double* Wd, double* Sc, int 
   return *s_fail == 0;
 }
 
+// Thread 0 waits, the CTA learns the outcome: true = go on.
+__device__ __forceinline__ bool df_cta_wait(const int* flag, int target, const int* err,
+                                            uint32_t* status, int* err_w, int* s_go) {
+  if (threadIdx.x == 0) {
+    const int ok = df_wait(flag, target, err);
+    if (ok < 0) {
+      atomicOr(status, SDPXG_ST_SYNC_TIMEOUT);
+      atomicExch(err_w, 1);
+    }
+    *s_go = (ok == 1);
+  }
+  __syncthreads();
+  return *s_go != 0;
+}
+
+// The critical path of the factorization, step k = 0 .. nt-1, in one CTA:
+//   diagonal tile: wait for the updates of steps < k-1 (upd[k][k] = k-1), load it, apply
+//   step k-1's update with U(k-1, k) still in Cs, factor it (POTRF with the dynamic pivot rule)
+//   and publish U_kk and U_kk^-1 (fin[k][k]);  then TRSM(k, k+1): wait for the updates of steps
+//   < k of tile (k, k+1), U(k, k+1) = U_kk^-T H(k, k+1) into Cs, publish it (fin[k][k+1]).
+// False when a wait gave up or a pivot failed (the error word is raised either way).
+__device__ bool df_chain(double* __restrict__ F, int m, int nt, int* upd, int* fin, int* err,
+                         double eps, double delta, int dynamic, const double* __restrict__ diag0,
+                         double* __restrict__ Dinv, uint32_t* __restrict__ status, double* As,
+                         double* Bs, double* Cs, double* Wd, double* Sc, double* s_diag, int* s_go,
+                         int* s_fail, bool vec2) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, q = lane & 3, r = lane >> 2;
+  for (int k = 0; k < nt; ++k) {
+    const int k0 = k * DF_NB, nb = min(DF_NB, m - k0);
+    if (k > 0 && !df_cta_wait(upd + k * nt + k, k - 1, err, status, err, s_go)) return false;
+    // diagonal tile H(k, k) - U(k-1, k)' U(k-1, k), assembled in registers, then into As
+    double acc[8][2];
+#pragma unroll
+    for (int R = 0; R < 8; ++R)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int row = 8 * R + r, col = 8 * w + 2 * q + e;
+        acc[R][e] = (row < nb && col < nb) ? __ldcg(F + (k0 + row) + (long)(k0 + col) * m) : 0.0;
+      }
+    if (k > 0) df_atb(Cs, Cs, acc, -1.0);
+    for (int e = threadIdx.x; e < DF_NB; e += DF_THREADS) s_diag[e] = (e < nb) ? diag0[k0 + e] : 1.0;
+    __syncthreads();  // every warp is done reading Cs
+#pragma unroll
+    for (int R = 0; R < 8; ++R)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int row = 8 * R + r, col = 8 * w + 2 * q + e;
+        DFS(As, row, col) = (row > col) ? 0.0 : ((row == col && row >= nb) ? 1.0 : acc[R][e]);
+      }
+    for (int e = threadIdx.x; e < DF_NB * DF_NB; e += DF_THREADS) DFS(Bs, e & 63, e >> 6) = 0.0;
+    if (threadIdx.x == 0) *s_fail = 0;
+    __syncthreads();
+    const bool ok = df_potrf_tile(As, Bs, Wd, Sc, nb, s_diag, eps, delta, dynamic, s_fail);
+    double* D = Dinv + (long)k * DF_NB * DF_NB;
+    for (int e = threadIdx.x; e < DF_NB * DF_NB; e += DF_THREADS) {
+      const int rr = e & 63, cc = e >> 6;
+      const bool live = rr <= cc && cc < nb;
+      if (live) F[(k0 + rr) + (long)(k0 + cc) * m] = DFS(As, rr, cc);
+      D[e] = live ? DFS(Bs, rr, cc) : 0.0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (ok) {
+        __threadfence();
+        df_st_release(upd + k * nt + k, k);
+        df_st_release(fin + k * nt + k, 1);
+      } else {  // the dependants of this tile leave at their next wait
+        atomicOr(status, SDPXG_ST_PIVOT_FAIL);
+        atomicExch(err, 1);
+      }
+    }
+    if (!ok) return false;
+    if (k + 1 >= nt) break;
+    // TRSM(k, k+1): U(k, k+1) = U_kk^-T H(k, k+1), U_kk^-1 in Bs
+    if (!df_cta_wait(upd + k * nt + k + 1, k, err, status, err, s_go)) return false;
+    const int j0 = (k + 1) * DF_NB, nc = min(DF_NB, m - j0);
+    df_load_tile(Cs, F + k0 + (long)j0 * m, m, DF_NB, nc, vec2);
+    __syncthreads();
+    double t[8][2] = {};
+    df_atb(Bs, Cs, t, 1.0);
+    __syncthreads();  // every warp is done reading Cs before it becomes U(k, k+1)
+#pragma unroll
+    for (int R = 0; R < 8; ++R)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int row = 8 * R + r, col = 8 * w + 2 * q + e;
+        const double v = (col < nc) ? t[R][e] : 0.0;
+        DFS(Cs, row, col) = v;
+        if (col < nc) F[(k0 + row) + (long)(j0 + col) * m] = v;
+      }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      df_st_release(fin + k * nt + k + 1, 1);
+    }
+  }
+  return true;
+}
+
 // items[t] = type << 30 | k << 20 | i << 10 | j (topological order, built on the host).
 // sync = {ticket, error, upd[nt * nt], fin[nt * nt]}, zero at launch:
 //   upd[i * nt + j] = trailing updates applied to tile (i, j) (GEMM(k, i, j) sets k + 1);
@@ -252,7 +353,8 @@ k_chol_dataflow(double* __restrict__ F, int m, int nt, const unsigned* __restric
   extern __shared__ __align__(16) double df_sm[];
   double* As = df_sm;
   double* Bs = As + DF_NB * DF_LD;
-  double* Wd = Bs + DF_NB * DF_LD;
+  double* Cs = Bs + DF_NB * DF_LD;  // the chain's U(k, k+1) (and the tile it comes from)
+  double* Wd = Cs + DF_NB * DF_LD;
   double* Sc = Wd + 8 * 64;
   __shared__ int s_item, s_go, s_fail;
   __shared__ double s_diag[DF_NB];  // original diagonal of the tile being factored
@@ -271,6 +373,12 @@ k_chol_dataflow(double* __restrict__ F, int m, int nt, const unsigned* __restric
     const unsigned code = items[t];
     const int type = (int)(code >> 30), k = (int)((code >> 20) & 1023u);
     const int i = (int)((code >> 10) & 1023u), j = (int)(code & 1023u);
+    if (type == DF_CHAIN) {
+      if (!df_chain(F, m, nt, upd, fin, err, eps, delta, dynamic, diag0, Dinv, status, As, Bs, Cs,
+                    Wd, Sc, s_diag, &s_go, &s_fail, vec2))
+        break;
+      continue;
+    }
     if (threadIdx.x == 0) {
       int ok;
       if (type == DF_POTRF) {

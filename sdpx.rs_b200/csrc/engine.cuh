@@ -40,7 +40,7 @@ constexpr size_t kSmemTrsm = 2 * 64 * 65 * sizeof(double);
 constexpr size_t kSmemSyrk = 2 * 64 * 66 * sizeof(double);
 constexpr size_t kSmemTrtri = 2 * 64 * 65 * sizeof(double);
 constexpr size_t kSmemTrinv = 4 * 64 * 68 * sizeof(double);  // k_trinv_level: 2 stages x 2 tiles
-constexpr size_t kSmemDf = (2 * 64 * 68 + 2 * 8 * 64) * sizeof(double);  // k_chol_dataflow
+constexpr size_t kSmemDf = (3 * 64 * 68 + 2 * 8 * 64) * sizeof(double);  // k_chol_dataflow
 constexpr size_t kSmemGram = 3 * kMatD * sizeof(double);                 // k_gram_basis/adjoint
 constexpr int kDfMaxTiles = 256;  // dataflow schedule up to m = 16384 (nt^3/6 items)
 
@@ -98,45 +98,75 @@ inline std::vector<unsigned> chol_schedule(int nt) {
   };
   std::vector<unsigned> it;
   if (nt <= 0) return it;
-  it.push_back(code(0u, 0, 0, 0));
-  for (int j = 1; j < nt; ++j) it.push_back(code(1u, 0, 0, j));
+  // ticket 0: the critical-path chain (every POTRF(k), TRSM(k, k+1) and GEMM(k, k+1, k+1))
+  it.push_back(code(3u, 0, 0, 0));
+  // then step by step the rest of each step: the TRSM row beyond k + 1, and the trailing
+  // updates row by row (rows k + 1 and k + 2 first feed the chain's next two steps)
   for (int k = 0; k + 1 < nt; ++k) {
-    for (int j = k + 1; j < nt; ++j) it.push_back(code(2u, k, k + 1, j));
-    it.push_back(code(0u, k + 1, k + 1, k + 1));
-    for (int j = k + 2; j < nt; ++j) it.push_back(code(1u, k + 1, k + 1, j));
-    for (int i = k + 2; i < nt; ++i)
-      for (int j = i; j < nt; ++j) it.push_back(code(2u, k, i, j));
+    for (int j = k + 2; j < nt; ++j) it.push_back(code(1u, k, k, j));
+    for (int i = k + 1; i < nt; ++i)
+      for (int j = i; j < nt; ++j)
+        if (!(i == k + 1 && j == k + 1)) it.push_back(code(2u, k, i, j));
   }
   return it;
 }
 
-// Replays a work list in order and checks that every item's inputs are produced by earlier
-// items (the condition under which the ticket order of k_chol_dataflow cannot deadlock) and
-// that every tile ends factored.  Returns false on any violation.
+// Replays a work list in ticket order and checks that every item's inputs come from earlier
+// items or from chain steps whose own inputs come from earlier items -- the condition under
+// which k_chol_dataflow cannot deadlock (the chain, ticket 0, only waits on items that precede
+// every item waiting on it) -- and that every tile ends factored.  False on any violation.
 inline bool chol_schedule_valid(const std::vector<unsigned>& it, int nt) {
   std::vector<int> upd((size_t)nt * nt, 0), fin((size_t)nt * nt, 0);
-  for (unsigned c : it) {
+  auto U = [&](int i, int j) -> int& { return upd[(size_t)i * nt + j]; };
+  auto Fn = [&](int i, int j) -> int& { return fin[(size_t)i * nt + j]; };
+  bool chain = false;
+  int step = 0;          // next chain step
+  bool diag_done = false;  // the chain's POTRF of `step` is done, its TRSM is pending
+  auto advance = [&]() {
+    while (chain && step < nt) {
+      const int s = step;
+      if (!diag_done) {
+        if (s > 0 && (U(s, s) != s - 1 || !Fn(s - 1, s))) return;  // GEMM(s-1, s, s) inputs
+        U(s, s) = s;
+        Fn(s, s) = 1;
+        diag_done = true;
+      }
+      if (s + 1 < nt) {
+        if (U(s, s + 1) != s) return;  // TRSM(s, s+1) input
+        Fn(s, s + 1) = 1;
+      }
+      diag_done = false;
+      ++step;
+    }
+  };
+  for (size_t t = 0; t < it.size(); ++t) {
+    const unsigned c = it[t];
     const int type = (int)(c >> 30), k = (int)((c >> 20) & 1023u);
     const int i = (int)((c >> 10) & 1023u), j = (int)(c & 1023u);
     if (k >= nt || i >= nt || j >= nt) return false;
-    if (type == 0) {
-      if (i != k || j != k || upd[(size_t)k * nt + k] != k || fin[(size_t)k * nt + k]) return false;
-      fin[(size_t)k * nt + k] = 1;
-    } else if (type == 1) {
-      if (i != k || j <= k || !fin[(size_t)k * nt + k] || upd[(size_t)k * nt + j] != k) return false;
-      fin[(size_t)k * nt + j] = 1;
+    if (type == 3) {
+      if (t != 0 || chain) return false;
+      chain = true;
+      advance();
+      continue;
+    }
+    advance();
+    if (type == 1) {
+      if (i != k || j <= k + 1 || !Fn(k, k) || U(k, j) != k) return false;
+      Fn(k, j) = 1;
     } else if (type == 2) {
-      if (i <= k || j < i || !fin[(size_t)k * nt + i] || !fin[(size_t)k * nt + j] ||
-          upd[(size_t)i * nt + j] != k)
+      if (i <= k || j < i || (i == k + 1 && j == k + 1) || !Fn(k, i) || !Fn(k, j) || U(i, j) != k)
         return false;
-      upd[(size_t)i * nt + j] = k + 1;
+      U(i, j) = k + 1;
     } else {
       return false;
     }
   }
+  advance();
+  if (!chain || step != nt) return false;
   for (int i = 0; i < nt; ++i)
     for (int j = i; j < nt; ++j)
-      if (!fin[(size_t)i * nt + j] || upd[(size_t)i * nt + j] != i) return false;
+      if (!Fn(i, j) || U(i, j) != i) return false;
   return true;
 }
 constexpr int kNB = 64;
