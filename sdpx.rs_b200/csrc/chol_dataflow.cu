@@ -119,62 +119,88 @@ __device__ __forceinline__ double df_pivot(double d, const double* diag, int nb,
 // Factor the diagonal tile in A (upper triangle valid, lower zero, padded diagonal 1) in
 // place: A <- U.  X <- U^-1 (upper).  Wd: 8 x (8 x 8) inverse diagonal blocks; Sc: 8 x 64
 // scratch.  Returns true when every pivot was accepted (CTA uniform).
+// Warp 0: factor the 8 x 8 diagonal block of panel p in registers and invert it.  Every lane
+// factors the whole block (packed upper triangle, static indices, no shuffles on the pivot
+// chain); lane c < 8 then writes column c of U_pp and of W = U_pp^-1.  One rsqrt per pivot:
+// 1/sqrt(d) and sqrt(d) = d / sqrt(d).
+__device__ __forceinline__ void df_panel_factor(double* A, double* Wd, int p, int nb,
+                                                const double* sdiag, double eps, double delta,
+                                                int dynamic, int* s_fail) {
+  const int lane = threadIdx.x & 31;
+  const int c = lane & 7;
+  const bool own = lane < 8;
+  double u[36], rd[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int i = 0; i <= j; ++i) u[j * (j + 1) / 2 + i] = DFS(A, 8 * p + i, 8 * p + j);
+  bool fail = false;
+#pragma unroll
+  for (int kk = 0; kk < 8; ++kk) {
+    double d = u[kk * (kk + 3) / 2];
+    if (8 * p + kk < nb) d = df_pivot(d, sdiag + 8 * p + kk, nb, eps, delta, dynamic, fail);
+    const double ri = rsqrt(d);
+    rd[kk] = ri;
+    u[kk * (kk + 3) / 2] = d * ri;
+#pragma unroll
+    for (int j = kk + 1; j < 8; ++j) u[j * (j + 1) / 2 + kk] *= ri;  // row kk of U
+#pragma unroll
+    for (int j = kk + 1; j < 8; ++j)
+#pragma unroll
+      for (int i = kk + 1; i <= j; ++i)
+        u[j * (j + 1) / 2 + i] -= u[i * (i + 1) / 2 + kk] * u[j * (j + 1) / 2 + kk];
+  }
+  if (fail && lane == 0) *s_fail = 1;
+  // column c of W = U_pp^-1: w_c = 1/U_cc, w_i = -(sum_{l>i} U_il w_l) / U_ii for i < c
+  double wv[8];
+#pragma unroll
+  for (int l = 0; l < 8; ++l) wv[l] = (l == c) ? rd[l] : 0.0;
+#pragma unroll
+  for (int i = 6; i >= 0; --i) {
+    double sacc = 0.0;
+#pragma unroll
+    for (int l = i + 1; l < 8; ++l) sacc = fma(u[l * (l + 1) / 2 + i], wv[l], sacc);
+    if (i < c) wv[i] = -sacc * rd[i];
+  }
+  if (own) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (j == c) {
+#pragma unroll
+        for (int i = 0; i <= j; ++i) DFS(A, 8 * p + i, 8 * p + j) = u[j * (j + 1) / 2 + i];
+      }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) Wd[p * 64 + i + 8 * c] = wv[i];  // column-major 8 x 8
+  }
+}
+
+// A[I, J] -= U[P, I]' U[P, J] for one 8 x 8 block (one warp).
+__device__ __forceinline__ void df_block_update(double* A, int p, int I, int J) {
+  const int lane = threadIdx.x & 31, q = lane & 3, r = lane >> 2;
+  double c0 = DFS(A, 8 * I + r, 8 * J + 2 * q), c1 = DFS(A, 8 * I + r, 8 * J + 2 * q + 1);
+#pragma unroll
+  for (int ks = 0; ks < 2; ++ks) {
+    const int kk = ks * 4 + q;
+    dmma_m8n8k4(c0, c1, -DFS(A, 8 * p + kk, 8 * I + r), DFS(A, 8 * p + kk, 8 * J + r));
+  }
+  DFS(A, 8 * I + r, 8 * J + 2 * q) = c0;
+  DFS(A, 8 * I + r, 8 * J + 2 * q + 1) = c1;
+}
+
+// Factor the diagonal tile in A (upper triangle valid, lower zero, padded diagonal 1) in
+// place: A <- U.  X <- U^-1 (upper).  Wd: 8 x (8 x 8) inverse diagonal blocks; Sc: 8 x 64
+// scratch.  Returns true when every pivot was accepted (CTA uniform).
+// Panels of 8 columns with one panel of look-ahead: once panel p's row U[P, J] is formed, warp
+// 0 updates diagonal block p+1 itself and factors panel p+1 while warps 1..7 apply the rest of
+// panel p's trailing update -- two barriers per panel, the register factorisation overlapped
+// with the tensor-core updates.
 __device__ bool df_potrf_tile(double* A, double* X, double* Wd, double* Sc, int nb,
                               const double* sdiag, double eps, double delta, int dynamic,
                               int* s_fail) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, q = lane & 3, r = lane >> 2;
+  if (w == 0) df_panel_factor(A, Wd, 0, nb, sdiag, eps, delta, dynamic, s_fail);
+  __syncthreads();
   for (int p = 0; p < 8; ++p) {
-    if (w == 0) {
-      // Every lane factors the whole 8 x 8 diagonal block in registers (packed upper triangle,
-      // static indices, no shuffles on the pivot chain); lane c < 8 then writes column c of
-      // U_pp and of W = U_pp^-1.  One rsqrt per pivot: 1/sqrt(d) and sqrt(d) = d / sqrt(d).
-      const int c = lane & 7;
-      const bool own = lane < 8;
-      double u[36], rd[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j)
-#pragma unroll
-        for (int i = 0; i <= j; ++i) u[j * (j + 1) / 2 + i] = DFS(A, 8 * p + i, 8 * p + j);
-      bool fail = false;
-#pragma unroll
-      for (int kk = 0; kk < 8; ++kk) {
-        double d = u[kk * (kk + 3) / 2];
-        if (8 * p + kk < nb) d = df_pivot(d, sdiag + 8 * p + kk, nb, eps, delta, dynamic, fail);
-        const double ri = rsqrt(d);
-        rd[kk] = ri;
-        u[kk * (kk + 3) / 2] = d * ri;
-#pragma unroll
-        for (int j = kk + 1; j < 8; ++j) u[j * (j + 1) / 2 + kk] *= ri;  // row kk of U
-#pragma unroll
-        for (int j = kk + 1; j < 8; ++j)
-#pragma unroll
-          for (int i = kk + 1; i <= j; ++i)
-            u[j * (j + 1) / 2 + i] -= u[i * (i + 1) / 2 + kk] * u[j * (j + 1) / 2 + kk];
-      }
-      if (fail && lane == 0) *s_fail = 1;
-      // column c of W = U_pp^-1: w_c = 1/U_cc, w_i = -(sum_{l>i} U_il w_l) / U_ii for i < c
-      double wv[8];
-#pragma unroll
-      for (int l = 0; l < 8; ++l) wv[l] = (l == c) ? rd[l] : 0.0;
-#pragma unroll
-      for (int i = 6; i >= 0; --i) {
-        double sacc = 0.0;
-#pragma unroll
-        for (int l = i + 1; l < 8; ++l) sacc = fma(u[l * (l + 1) / 2 + i], wv[l], sacc);
-        if (i < c) wv[i] = -sacc * rd[i];
-      }
-      if (own) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (j == c) {
-#pragma unroll
-            for (int i = 0; i <= j; ++i) DFS(A, 8 * p + i, 8 * p + j) = u[j * (j + 1) / 2 + i];
-          }
-#pragma unroll
-        for (int i = 0; i < 8; ++i) Wd[p * 64 + i + 8 * c] = wv[i];  // column-major 8 x 8
-      }
-    }
-    __syncthreads();
     // panel row: U[P, J] = W_pp' A[P, J], one block column per warp
     if (w < 7 - p) {
       const int J = p + 1 + w;
@@ -188,23 +214,23 @@ __device__ bool df_potrf_tile(double* A, double* X, double* Wd, double* Sc, int 
       DFS(A, 8 * p + r, 8 * J + 2 * q + 1) = c1;
     }
     __syncthreads();
-    // trailing blocks: A[I, J] -= U[P, I]' U[P, J] for p < I <= J
-    const int nrem = 7 - p, cnt = nrem * (nrem + 1) / 2;
-    for (int t = w; t < cnt; t += DF_THREADS / 32) {
-      int I = p + 1, tt = t;
-      while (tt >= 8 - I) {
-        tt -= 8 - I;
-        ++I;
+    if (p == 7) break;
+    if (w == 0) {
+      // look-ahead: the next diagonal block is final after this update; factor it
+      df_block_update(A, p, p + 1, p + 1);
+      __syncwarp();
+      df_panel_factor(A, Wd, p + 1, nb, sdiag, eps, delta, dynamic, s_fail);
+    } else {
+      // the rest of panel p's trailing update: A[I, J] for p < I <= J, (I, J) != (p+1, p+1)
+      const int nrem = 7 - p, cnt = nrem * (nrem + 1) / 2;
+      for (int t = w; t < cnt; t += DF_THREADS / 32 - 1) {  // t = 0 is (p+1, p+1): warp 0's
+        int I = p + 1, tt = t;
+        while (tt >= 8 - I) {
+          tt -= 8 - I;
+          ++I;
+        }
+        df_block_update(A, p, I, I + tt);
       }
-      const int J = I + tt;
-      double c0 = DFS(A, 8 * I + r, 8 * J + 2 * q), c1 = DFS(A, 8 * I + r, 8 * J + 2 * q + 1);
-#pragma unroll
-      for (int ks = 0; ks < 2; ++ks) {
-        const int kk = ks * 4 + q;
-        dmma_m8n8k4(c0, c1, -DFS(A, 8 * p + kk, 8 * I + r), DFS(A, 8 * p + kk, 8 * J + r));
-      }
-      DFS(A, 8 * I + r, 8 * J + 2 * q) = c0;
-      DFS(A, 8 * I + r, 8 * J + 2 * q + 1) = c1;
     }
     __syncthreads();
   }

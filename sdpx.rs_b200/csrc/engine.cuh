@@ -670,7 +670,10 @@ class Engine {
       check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chol_dataflow, 256, kSmemDf),
             "occupancy");
       check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
-      df_grid_ = std::max(1, std::min(std::max(per_sm, 1) * sms, df_items_));
+      // one CTA per SM: the chain CTA (the critical path) then has its SM to itself; the
+      // trailing updates are far from saturating the others
+      (void)per_sm;
+      df_grid_ = std::max(1, std::min(sms, df_items_));
     }
     step_out_.alloc(2 * (nblk + 1));
     hblk_.alloc(2 * (nblk + 1));
