@@ -49,6 +49,16 @@ def make_problem():
     return problems.rank1_sdp(32, 2000, seed=0)
 
 
+def dist_backend():
+    """NCCL between GPUs; gloo where there is no GPU (the multi-process tests on CPU).
+    SDPX_B200_DIST_BACKEND overrides."""
+    b = os.environ.get("SDPX_B200_DIST_BACKEND")
+    if b:
+        return b
+    import torch
+    return "nccl" if torch.cuda.is_available() else "gloo"
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -58,8 +68,10 @@ def dist_setup():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = dist_backend()
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return world, rank, local
 
 
@@ -70,11 +82,13 @@ def barrier(world):
 
 
 def max_over_ranks(world, value):
+    """The largest of the ranks' values (device timings: the slowest rank sets the job time)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
