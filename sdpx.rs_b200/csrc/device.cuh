@@ -63,19 +63,26 @@ class DeviceCache {
     f.erase(it);
     return p;
   }
-  // bytes: the size the block was allocated with
+  // bytes: the size the block was allocated with; dev: the device it lives on (made current for
+  // the synchronisation and any eviction, the caller's current device restored after)
   void give(void* p, size_t bytes, int dev) {
+    int cur = dev;
+    cudaGetDevice(&cur);
+    if (cur != dev) cudaSetDevice(dev);
     cudaDeviceSynchronize();  // what cudaFree would wait for
-    std::lock_guard<std::mutex> lk(mu_);
-    auto& f = free_[dev & 15];
-    f.emplace(bytes, p);
-    held_[dev & 15] += bytes;
-    while (held_[dev & 15] > kCacheBytes && !f.empty()) {
-      auto last = std::prev(f.end());
-      cudaFree(last->second);
-      held_[dev & 15] -= last->first;
-      f.erase(last);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      auto& f = free_[dev & 15];
+      f.emplace(bytes, p);
+      held_[dev & 15] += bytes;
+      while (held_[dev & 15] > kCacheBytes && !f.empty()) {
+        auto last = std::prev(f.end());
+        cudaFree(last->second);
+        held_[dev & 15] -= last->first;
+        f.erase(last);
+      }
     }
+    if (cur != dev) cudaSetDevice(cur);
   }
 
  private:
