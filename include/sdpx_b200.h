@@ -134,6 +134,10 @@ int32_t sdpx_b200_set_kernel_timing(sdpx_handle *handle, int32_t on);
 int32_t sdpx_b200_kernel_times(sdpx_handle *handle, double *ms, uint64_t *counts);
 /* Number of CUDA kernels this library has launched in this process (all handles). */
 uint64_t sdpx_b200_launch_count(void);
+/* Number of device memory blocks this library has obtained in this process (from its cache of
+ * released blocks or from cudaMalloc; all handles).  A call that allocates nothing leaves it
+ * unchanged.  No counterpart in the reference (it has no device memory). */
+uint64_t sdpx_b200_device_allocations(void);
 /* Bytes this library has copied host-to-device and device-to-host in this process (all
  * handles): the host-device traffic of prepare, solve and result reads. */
 int32_t sdpx_b200_transfer_bytes(uint64_t *h2d, uint64_t *d2h);
@@ -203,8 +207,13 @@ int32_t sdpxg_solve_many(sdpxg_ctx *ctx, const double *rhs, double *out, uint32_
  * cudaMalloc could synchronise the device): d_rhs and d_out are DEVICE pointers to n x ncols
  * column-major arrays, and all per-call scratch sits in one static device array of the library
  * (about 0.17 MB on every GPU that loads it).  It calls no cudaMalloc or cudaFree.  n above 4096
- * returns 2.  The first call on a device looks up the array's address: make it before any
- * stream capture.  Calls that overlap on the GPU share the array and race. */
+ * returns 2; host pointers, or no current factorization (sdpxg_factor not called since the last
+ * upload or assembly), return 1.  The solve runs on the context's own stream, which is not
+ * ordered after the caller's streams: the writes to d_rhs must be complete before the call (for
+ * instance, synchronise the stream that produced them); d_out is complete when the call
+ * returns.  The caller's current device is restored on return.  The first call on a device
+ * looks up the array's address: make it before any stream capture.  Calls that overlap on the
+ * GPU share the array and race. */
 int32_t sdpxg_solve_noalloc(sdpxg_ctx *ctx, const double *d_rhs, double *d_out, uint32_t ncols);
 /* Full condensed KKT solve [P A'; A -Hs][x; z] = [bx; bz] with the outer refinement on the
  * original operator.  Replaces CondensedKKTSolver::solve (kkt/condensed/kkt.rs:275-318). */

@@ -669,6 +669,7 @@ int32_t sdpx_destroy(sdpx_handle* h) {
 }
 
 uint64_t sdpx_b200_launch_count(void) { return sdpxg::g_launches; }
+uint64_t sdpx_b200_device_allocations(void) { return sdpxg::g_dev_allocs; }
 
 int32_t sdpx_b200_transfer_bytes(uint64_t* h2d, uint64_t* d2h) {
   return boundary([&] {

@@ -38,6 +38,11 @@ inline void copy_d2h(void* h, const void* d, size_t bytes, cudaStream_t st) {
   g_d2h_bytes += bytes;
 }
 
+// Device blocks this library has obtained in this process (from the cache below or from
+// cudaMalloc), read through sdpx_b200_device_allocations: a call that must not allocate leaves
+// it unchanged.
+inline std::atomic<uint64_t> g_dev_allocs{0};
+
 // Device allocations are recycled through a process-wide cache instead of going back to the
 // driver: the next handle (an e2e loop, a new problem) takes the blocks the last one released,
 // without cudaMalloc's mapping cost and cudaFree's unmapping.  A block is released the way
@@ -132,6 +137,7 @@ struct DevBuf {
       size_t got = want;
       void* q = DeviceCache::get().take(want, dev, &got);
       if (!q) check(cudaMalloc(&q, want), "cudaMalloc");
+      ++g_dev_allocs;
       p = static_cast<T*>(q);
       bytes = got;
       cap = got / sizeof(T);

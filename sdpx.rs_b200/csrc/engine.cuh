@@ -391,6 +391,7 @@ class Engine {
   void upload(const HostProblem& p) {
     const auto u0 = std::chrono::steady_clock::now();
     clear_graphs();
+    factor_ok_ = false;  // the factor (and its inverse) belong to the previous problem
     n = p.n;
     m = p.m;
     hblocks.clear();
@@ -884,6 +885,7 @@ class Engine {
 
   // ---- Schur complement ----
   bool assemble() {
+    factor_ok_ = false;  // the factor no longer matches the Schur complement being rebuilt
     tbegin(KT_ASSEMBLE);
     if (nwork_) {
       ++g_launches, k_schur_transform<<<nwork_, SDPXG_CONE_THREADS, kSmemTrans, st>>>(blocks_, wblk_, wloc_, acol_off_,
@@ -928,6 +930,7 @@ class Engine {
   }
   // F = chol(Hsave + eps I) with the dynamic pivot rule
   bool factor(double eps, bool dynamic, double dyn_eps, double dyn_delta) {
+    factor_ok_ = false;
     if (!n) return true;
     clear_status();
     ++g_launches, k_shifted_copy<<<1184, 256, 0, st>>>(Hsave_, F_, n, eps, diag0_);

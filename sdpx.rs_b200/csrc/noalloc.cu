@@ -22,6 +22,9 @@
 //  * Host code cannot use the array's name as a device address, so the first call on each
 //    device (with that device current) looks its address up with cudaGetSymbolAddress and
 //    caches it.  Make that first call before any stream capture.
+//  * The solve runs on the context's stream, which is not ordered after the caller's streams:
+//    the caller finishes writing d_rhs (e.g. synchronises its stream) before the call; d_out is
+//    complete when the call returns.  The caller's current device is restored on every exit.
 #include <mutex>
 #include <string>
 
@@ -68,6 +71,27 @@ double* scratch_for_current_device() {
   return g_scratch_ptr[dev];
 }
 
+// Restores the caller's current device when the entry point returns or throws.
+struct DeviceRestore {
+  int saved = -1;
+  DeviceRestore() {
+    if (cudaGetDevice(&saved) != cudaSuccess) saved = -1;
+  }
+  ~DeviceRestore() {
+    if (saved >= 0) cudaSetDevice(saved);
+  }
+};
+
+// True when p is memory the GPU addresses as device (or managed) memory.
+bool is_device_pointer(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // reset the error the failed query recorded
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
 // One reduction into slot `slot` of the scratch reduction area, no host transfer.
 void reduce_into(cudaStream_t st, int op, long n, const double* x, double* partial, double* slot) {
   ++g_launches, k_reduce_partial<<<SDPXG_NOALLOC_RED_BLOCKS, 256, 0, st>>>(op, n, x, nullptr, partial);
@@ -91,7 +115,10 @@ extern "C" int32_t sdpxg_solve_noalloc(sdpxg_ctx* ctx, const double* d_rhs, doub
     }
     if (ncols && (!d_rhs || !d_out)) throw std::invalid_argument("null pointer");
     if (!E.factored()) throw std::invalid_argument("no factorization: call sdpxg_factor first");
+    DeviceRestore restore;
     check(cudaSetDevice(E.device), "cudaSetDevice");
+    if (ncols && (!is_device_pointer(d_rhs) || !is_device_pointer(d_out)))
+      throw std::invalid_argument("d_rhs and d_out must be device pointers");
     double* base = scratch_for_current_device();
     double* tri = base;
     double* en = tri + SDPXG_NOALLOC_MAXN;
@@ -159,6 +186,9 @@ extern "C" int32_t sdpxg_solve_noalloc(sdpxg_ctx* ctx, const double* d_rhs, doub
     return 1;
   } catch (const std::exception& e) {
     sdpxg::g_last_error = std::string("internal error: ") + e.what();
+    return 5;
+  } catch (...) {
+    sdpxg::g_last_error = "internal error";
     return 5;
   }
 }

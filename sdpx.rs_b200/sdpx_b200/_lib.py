@@ -77,6 +77,7 @@ SIGNATURES = {
     "sdpx_b200_set_kernel_timing": (i32, [C.c_void_p, i32]),
     "sdpx_b200_kernel_times": (i32, [C.c_void_p, PD, PU64]),
     "sdpx_b200_launch_count": (u64, []),
+    "sdpx_b200_device_allocations": (u64, []),
     "sdpx_b200_transfer_bytes": (i32, [PU64, PU64]),
     "sdpx_b200_schur_forms": (i32, [C.c_void_p, PU32, PU32]),
     "sdpx_b200_kkt_paths": (i32, [C.c_void_p, PU64, PU64]),
