@@ -19,8 +19,9 @@
  * (the reference's "panic": an exception caught at the boundary), 6 insufficient output
  * capacity, 7 no solved result.  The last error message is thread-local.
  *
- * Supported subset: precision_bits 53 (binary64), PSD triangle cones of order <= 64,
- * kkt_form 0 (auto) or 2 (condensed).  Other inputs return 2 (unsupported) with a message.
+ * Supported subset: precision_bits 53 (binary64), PSD triangle cones of order <= 64 and
+ * nonnegative orthants, sampled blocks with dim = 1, kkt_form 0 (auto) or 2 (condensed).  Other
+ * inputs return 2 (unsupported) with a message.
  */
 #ifndef SDPX_B200_H
 #define SDPX_B200_H
@@ -89,7 +90,9 @@ int32_t sdpx_mpi_world_size(void);
 int32_t sdpx_prepare(const sdpx_csc *P, const sdpx_scalars *q, const sdpx_csc *A,
                      const sdpx_scalars *b, const sdpx_cone *cones, uint64_t cone_count,
                      const sdpx_settings *settings, sdpx_handle **out);
-/* include/sdpx.h:92 (ffi/src/lib.rs:608-621): factor blocks are not supported here (2) */
+/* include/sdpx.h:92 (ffi/src/lib.rs:608-658): factor-authoritative sampled blocks.  Blocks with
+ * dim = 1 (columns weight_k svec(q_k q_k')) run on the GPU's Gram form with the given basis and
+ * weights (scaled by the equilibration); matrix-valued blocks (dim > 1) return 2. */
 int32_t sdpx_prepare_sampled(const sdpx_csc *P, const sdpx_scalars *q, const sdpx_csc *A_linear,
                              const sdpx_scalars *b, const sdpx_cone *cones, uint64_t cone_count,
                              const sdpx_settings *settings, const sdpx_sampled_block *blocks,
@@ -165,6 +168,14 @@ int32_t sdpx_b200_adjoint(sdpx_handle *handle, const double *dl_dx, const double
  * Capture pays off over the many solves of one problem; a handle re-prepared for every small
  * instance of a batch is better off eager.  No counterpart in the reference. */
 int32_t sdpx_b200_set_graphs(sdpx_handle *handle, int32_t on);
+/* Factorisation form of later solves: 0 plain (one FP64 dataflow Cholesky of the Schur
+ * complement and its explicit inverse; the default unless SDPX_B200_FORM=split), 1 split
+ * precision (Schur dimension >= 1024: the two diagonal halves factored and inverted in FP64
+ * with the same pivot rule, the off-diagonal block, the trailing Schur update and the inverse's
+ * off-diagonal block as Ozaki-II products on the INT8 tensor cores; refinement against the
+ * unshifted FP64 Schur complement as before).  Replaces the f64 dgemm/dsyrk trailing updates
+ * of DenseBlockSolver::tiled_potrf (kkt/ldl/dense_block.rs:515-594). */
+int32_t sdpx_b200_set_form(sdpx_handle *handle, uint32_t form);
 /* Schur forms chosen at prepare: PSD blocks whose every constraint column is rank one
  * (sigma u u', stored as the factor U and used in the Gram form S = (sigma sigma') o (U' Ginv U)^2,
  * like the reference's sampled Gram update, sampled/mod.rs:1973-2025) and blocks kept in the
@@ -181,6 +192,19 @@ int32_t sdpxg_ctx_destroy(sdpxg_ctx *ctx);
  * that CondensedKKTSolver::new reads (kkt/condensed/mod.rs:1279-1347). */
 int32_t sdpxg_problem_upload(sdpxg_ctx *ctx, const sdpx_csc *P, const sdpx_csc *A,
                              const uint64_t *psd_orders, uint64_t block_count);
+/* sdpxg_problem_upload with factor-authoritative sampled blocks (dim = 1; the layout of
+ * sdpx_prepare_sampled): their columns are weight_k svec(q_k q_k') materialised into A, and the
+ * Schur complement and operator use the given basis and weights exactly.  Replaces
+ * CondensedKKTSolver::set_sampled_operator (kkt/mod.rs:34-135, solver/sampled/mod.rs:180). */
+int32_t sdpxg_problem_upload_sampled(sdpxg_ctx *ctx, const sdpx_csc *P, const sdpx_csc *A_linear,
+                                     const uint64_t *psd_orders, uint64_t block_count,
+                                     const sdpx_sampled_block *blocks, uint64_t nblocks);
+/* Set the scaling of every PSD block from R and R^-1 (n_j x n_j column-major per block, stacked in
+ * cone order); G^-1 = R^-T R^-1 is formed on the device.  Only the Schur assembly and the cone
+ * operators read it (lambda is not set).  Replaces the condensed KKT's sync of R / R^-1 from the
+ * cones (kkt/condensed/kkt.rs:1077-1180) and SampledSchurWorkspace::update_with_pool's Rinv
+ * (solver/sampled/mod.rs:1836-1867). */
+int32_t sdpxg_set_scaling(sdpxg_ctx *ctx, const double *R, const double *Rinv);
 /* NT scaling of every PSD block at (s, z) (m-length svec vectors).  Writes lambda (sum of
  * orders) when out_lambda is not NULL.  *status: 0 ok, else SDPXG_ST bits.
  * Replaces PSDTriangleCone::update_scaling (cones/psdtrianglecone.rs:311-439). */
@@ -197,6 +221,19 @@ int32_t sdpxg_schur_assemble(sdpxg_ctx *ctx, double *out_schur);
  * factor_with_shift (kkt/ldl/dense_block.rs:95-365, kkt/direct/solver.rs:758-877). */
 int32_t sdpxg_factor(sdpxg_ctx *ctx, double shift, uint32_t dynamic, double eps, double delta,
                      uint32_t *status);
+/* Factorisation form of this context's sdpxg_factor (0 plain, 1 split precision; see
+ * sdpx_b200_set_form).  Same seam: DenseBlockSolver::refactor (kkt/ldl/dense_block.rs:95-365). */
+int32_t sdpxg_set_factor_form(sdpxg_ctx *ctx, uint32_t form);
+/* C = alpha op(A) op(B) + beta C in binary64 through split-precision products on the INT8 tensor
+ * cores (Ozaki scheme II: rows of op(A) and columns of op(B) scaled by powers of two to integers
+ * of b = 55..57 bits, residues modulo 16 coprime moduli <= 256, one tcgen05 kind::i8 GEMM per
+ * modulus, Garner reconstruction in FP64).  DEVICE pointers, column-major, k <= 65536; returns
+ * when C is complete; *status = SDPXG_ST_NONFINITE bit for non-finite inputs.  Replaces the f64
+ * dgemm of the reference's BLAS provider on the dense factorisation's trailing updates
+ * (algebra/dense/blas/traits.rs XgemmScalar, used by kkt/ldl/dense_block.rs:515-594). */
+int32_t sdpxg_split_dgemm_device(sdpxg_ctx *ctx, char ta, char tb, uint64_t m, uint64_t n, uint64_t k,
+                                 double alpha, const double *d_A, uint64_t lda, const double *d_B,
+                                 uint64_t ldb, double beta, double *d_C, uint64_t ldc, uint32_t *status);
 /* Solve the factored reduced system for ncols right-hand sides (n-length columns), refined
  * against the unshifted Schur complement.  Replaces DirectLDLSolver::solve
  * (kkt/ldl/dense_block.rs:795-850 with kkt/direct/solver.rs:1046-1125). */
@@ -234,11 +271,26 @@ int32_t sdpxg_step_length(sdpxg_ctx *ctx, const double *dz, const double *ds, do
  * 64 * limbs bits, ties to even -- bitwise MpFloat::dot_fma.  ta, tb are 'N' or 'T'; upper_only
  * computes the entries i <= j and writes zeros below.  limbs 1..16.  Non-finite operands
  * return 2 with *status = SDPXG_ST_NONFINITE.  Replaces rns_blas::gemm
- * (crates/solver/src/algebra/dense/blas/rns_blas.rs:2134-2417) with residue products modulo
- * primes below 2^21 on the GPU. */
+ * (crates/solver/src/algebra/dense/blas/rns_blas.rs:2134-2417): the residue products run on
+ * the INT8 tensor cores (primes below 2^15 as two signed-byte digits, tcgen05.mma kind::i8)
+ * or, after sdpxg_rns_set_form(ctx, 1), as exact FP64 products modulo primes below 2^21; both
+ * forms give the same bits. */
 int32_t sdpxg_rns_gemm(sdpxg_ctx *ctx, uint32_t limbs, char ta, char tb, uint64_t m, uint64_t n,
                        uint64_t k, const void *A, uint64_t lda, const void *B, uint64_t ldb,
                        uint32_t upper_only, void *C, uint32_t *status);
+/* sdpxg_rns_gemm on DEVICE buffers (A, B and C in device memory, same layouts): no host copies of
+ * the operands or the result, for callers that keep MpFloat matrices resident (a factorisation's
+ * trailing updates).  Runs on the context's stream and returns when C is complete; the operands
+ * must be complete before the call.  Same rns_blas::gemm contract
+ * (crates/solver/src/algebra/dense/blas/rns_blas.rs:2134-2417). */
+int32_t sdpxg_rns_gemm_device(sdpxg_ctx *ctx, uint32_t limbs, char ta, char tb, uint64_t m,
+                              uint64_t n, uint64_t k, const void *d_A, uint64_t lda,
+                              const void *d_B, uint64_t ldb, uint32_t upper_only, void *d_C,
+                              uint32_t *status);
+/* Residue arithmetic of the exact products of this context: 0 = INT8 tensor cores (default),
+ * 1 = FP64 CUDA cores.  The reference computes its per-prime products with FP64 dgemm
+ * (rns_blas.rs:447-580); the result bits do not depend on the form. */
+int32_t sdpxg_rns_set_form(sdpxg_ctx *ctx, uint32_t form);
 /* y = op(x) per PSD block: op 0 W, 1 W', 2 W^-1, 3 W^-T, 4 Hs = W'W, 5 Hs^-1.
  * Replaces mul_W / mul_Winv / PsdBlock::apply (cones/psdtrianglecone.rs:860-917,
  * kkt/condensed/psd.rs:1968-2027). */

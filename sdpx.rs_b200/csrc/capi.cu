@@ -13,6 +13,7 @@
 
 #include "../../include/sdpx_b200.h"
 #include "hsd.cuh"
+#include "sampled.cuh"
 #include "host_parallel.h"
 
 using namespace sdpxg;
@@ -37,6 +38,9 @@ int32_t boundary(F&& f) {
   } catch (const AbiError& e) {
     sdpxg::g_last_error = e.msg;
     return e.code;
+  } catch (const sdpxg::SampledUnsupported& e) {
+    sdpxg::g_last_error = e.what();
+    return 2;
   } catch (const std::invalid_argument& e) {
     sdpxg::g_last_error = e.what();
     return 1;
@@ -494,6 +498,54 @@ void prepare_impl(const sdpx_csc* P, const sdpx_scalars* q, const sdpx_csc* A, c
   *out = h.release();
 }
 
+// Factor-authoritative sampled input (ffi/src/lib.rs:608-658): the columns are materialised
+// into A for validation, equilibration and the residuals (materialize_sampled), and the factors
+// -- basis and weights scaled by the equilibration (one scalar per PSD cone after rectification,
+// times the column scale) -- drive the Schur complement and the operator on the GPU.
+void prepare_sampled_impl(const sdpx_csc* P, const sdpx_scalars* q, const sdpx_csc* A_linear,
+                          const sdpx_scalars* b, const sdpx_cone* cones, uint64_t nc,
+                          const sdpx_settings* s, const sdpx_sampled_block* blocks, uint64_t nb,
+                          sdpx_handle** out) {
+  if (!out) invalid("null pointer");
+  *out = nullptr;
+  ref(A_linear);
+  if (nc && !cones) invalid("null pointer");
+  Csc lin = matrix(*A_linear, false);
+  std::vector<std::pair<uint64_t, uint64_t>> psd_rows;  // (row start, order) of the PSD cones
+  uint64_t row = 0;
+  for (uint64_t i = 0; i < nc; ++i) {
+    const uint64_t d = cones[i].dim;
+    if (cones[i].kind == 3) {
+      psd_rows.push_back({row, d});
+      row += d * (d + 1) / 2;
+    } else {
+      row += d;
+    }
+  }
+  SampledCsc merged = materialize_sampled(A_linear->rows, A_linear->cols, lin.colptr, lin.rowval, lin.val,
+                                          psd_rows, blocks, nb);
+  sdpx_csc A{};
+  A.rows = A_linear->rows;
+  A.cols = A_linear->cols;
+  A.nnz = merged.rowval.size();
+  A.colptr = merged.colptr.data();
+  A.rowval = merged.rowval.data();
+  A.values.kind = 0;
+  A.values.count = merged.val.size();
+  A.values.f64 = merged.val.data();
+  double tv = 0, te = 0;
+  auto h = build_problem(P, q, &A, b, cones, nc, s, &tv, &te);
+  for (auto& r : merged.recs) {  // the factors in the equilibrated coordinates
+    const double e = h->eq.e[(size_t)r.row_start];
+    for (int k = 0; k < r.count; ++k) r.weight[k] = r.weight[k] * h->eq.d[(size_t)(r.col0 + k)] * e;
+  }
+  h->equil.sampled = std::move(merged.recs);
+  h->eng = std::make_unique<Engine>();
+  h->eng->init(device_from_env());
+  h->eng->upload(h->equil);
+  *out = h.release();
+}
+
 }  // namespace
 
 extern "C" {
@@ -524,14 +576,11 @@ int32_t sdpx_prepare(const sdpx_csc* P, const sdpx_scalars* q, const sdpx_csc* A
   return boundary([&] { prepare_impl(P, q, A, b, cones, cone_count, settings, out); });
 }
 
-int32_t sdpx_prepare_sampled(const sdpx_csc*, const sdpx_scalars*, const sdpx_csc*,
-                             const sdpx_scalars*, const sdpx_cone*, uint64_t,
-                             const sdpx_settings*, const sdpx_sampled_block*, uint64_t,
-                             sdpx_handle** out) {
-  return boundary([&] {
-    if (out) *out = nullptr;
-    unsupported("factor-authoritative sampled blocks are not implemented on the GPU path");
-  });
+int32_t sdpx_prepare_sampled(const sdpx_csc* P, const sdpx_scalars* q, const sdpx_csc* A_linear,
+                             const sdpx_scalars* b, const sdpx_cone* cones, uint64_t cone_count,
+                             const sdpx_settings* settings, const sdpx_sampled_block* blocks,
+                             uint64_t block_count, sdpx_handle** out) {
+  return boundary([&] { prepare_sampled_impl(P, q, A_linear, b, cones, cone_count, settings, blocks, block_count, out); });
 }
 
 int32_t sdpx_b200_reprepare(sdpx_handle* h, const sdpx_csc* P, const sdpx_scalars* q,
@@ -737,6 +786,13 @@ int32_t sdpx_b200_set_graphs(sdpx_handle* h, int32_t on) {
       hh.eng->clear_graphs();
       hh.eng->graphs_enabled = on != 0;
     });
+  });
+}
+
+int32_t sdpx_b200_set_form(sdpx_handle* h, uint32_t form) {
+  return boundary([&] {
+    if (form > 1) invalid("form must be 0 (plain) or 1 (split precision)");
+    operate(h, [&](sdpx_handle& hh) { hh.eng->factor_form = (int)form; });
   });
 }
 

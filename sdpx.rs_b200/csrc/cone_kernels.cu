@@ -136,6 +136,22 @@ extern "C" __global__ void k_identity_scaling(const BlockDesc* __restrict__ bloc
   }
 }
 
+// G^-1 = R^-T R^-1 per block from a given R^-1 (column-major n x n): G^-1(a, b) =
+// sum_r R^-1(r, a) R^-1(r, b), summed in r order (exactly symmetric).
+extern "C" __global__ void k_ginv_from_rinv(const BlockDesc* __restrict__ blocks, const double* __restrict__ Rinv,
+                                            double* __restrict__ Ginv) {
+  const BlockDesc bd = blocks[blockIdx.x];
+  const int n = bd.n;
+  const double* X = Rinv + bd.mat_off;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int a = e % n, b = e / n;
+    const int lo = a < b ? a : b, hi = a < b ? b : a;
+    double acc = 0.0;
+    for (int r = 0; r < n; ++r) acc = fma(X[r + lo * n], X[r + hi * n], acc);
+    Ginv[bd.mat_off + e] = acc;
+  }
+}
+
 // ---------------------------------------------------------------------------------------
 // Congruences on svec vectors.  mode:
 //   0  W x     = svec(R' X R)          1  W' x     = svec(R X R')

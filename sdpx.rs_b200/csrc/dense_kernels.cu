@@ -34,6 +34,31 @@ extern "C" __global__ void k_shifted_copy(const double* __restrict__ Hs, double*
   }
 }
 
+// out[i] = H[i * stride] + eps: a strided diagonal (the original diagonal of a trailing block).
+extern "C" __global__ void k_strided_diag(const double* __restrict__ H, long stride, int n, double eps,
+                                          double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = H[(long)i * stride] + eps;
+}
+
+// dst(j, i) = src(i, j) for a rows x cols block (column-major, leading dimensions lds, ldd),
+// through a 32 x 33 shared tile so both sides are coalesced.  block (32, 8), grid (cols/32,
+// rows/32).
+extern "C" __global__ void k_transpose_block(const double* __restrict__ src, long lds, int rows, int cols,
+                                             double* __restrict__ dst, long ldd) {
+  __shared__ double t[32][33];
+  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+  for (int jj = threadIdx.y; jj < 32; jj += 8) {
+    const int i = i0 + threadIdx.x, j = j0 + jj;
+    if (i < rows && j < cols) t[jj][threadIdx.x] = src[i + (long)j * lds];
+  }
+  __syncthreads();
+  for (int ii = threadIdx.y; ii < 32; ii += 8) {
+    const int j = j0 + threadIdx.x, i = i0 + ii;
+    if (i < rows && j < cols) dst[j + (long)i * ldd] = t[threadIdx.x][ii];
+  }
+}
+
 // ------------------------------------------------------------------------------------
 // Pivot k of the diagonal tile under the dynamic pivot rule (the reference's LDL pivot
 // handling, dense_block.rs): a pivot within eps of zero becomes delta, a clearly negative or

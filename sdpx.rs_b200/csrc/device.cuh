@@ -194,6 +194,7 @@ extern "C" {
 __global__ void k_nt_scale(const BlockDesc*, const double*, const double*, double*, double*,
                            double*, double*, double*, uint32_t*);
 __global__ void k_identity_scaling(const BlockDesc*, double*, double*, double*, double*, double*);
+__global__ void k_ginv_from_rinv(const BlockDesc*, const double*, double*);
 __global__ void k_congruence(const BlockDesc*, int, const double*, const double*, const double*,
                              double*, long);
 __global__ void k_circ_op(const BlockDesc*, const double*, const double*, double*);
@@ -237,6 +238,8 @@ __global__ void k_trtri_diag(int, const double*, double*, double*);
 __global__ void k_trinv_level(const double*, double*, double*, double*, int, int, int);
 __global__ void k_tri_colgemv(const double*, int, int, const double*, double*);
 __global__ void k_shifted_copy(const double*, double*, int, double, double*);
+__global__ void k_strided_diag(const double*, long, int, double, double*);
+__global__ void k_transpose_block(const double*, long, int, int, double*, long);
 __global__ void k_symv_cols(const double*, int, const double*, const double*, double*);
 __global__ void k_coldot_seg(const double*, int, int, const double*, const double*, double, double*,
                              double*, unsigned*);

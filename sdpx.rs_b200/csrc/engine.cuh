@@ -25,6 +25,7 @@
 
 #include "device.cuh"
 #include "host_parallel.h"
+#include "ozaki.cuh"
 
 namespace sdpxg {
 
@@ -171,6 +172,16 @@ inline bool chol_schedule_valid(const std::vector<unsigned>& it, int nt) {
 }
 constexpr int kNB = 64;
 
+// Factorisation forms of the Schur complement.
+//   kFormPlain  one FP64 dataflow Cholesky of the whole matrix, then its explicit inverse;
+//   kFormSplit  (m >= kSplitMin) H = [H11 H12; H12' H22] in two halves: FP64 dataflow Cholesky
+//               and inverse of the diagonal blocks (pivots and the dynamic pivot rule stay FP64),
+//               and the four large products -- U12 = X11' H12, S = H22 - U12' U12,
+//               W = X11 U12, X12 = -W X22 -- as split-precision (Ozaki-II) INT8 tensor-core
+//               GEMMs.  The refinement against the unshifted FP64 Schur complement is unchanged.
+enum FactorForm { kFormPlain = 0, kFormSplit = 1 };
+constexpr int kSplitMin = 1024;
+
 // Equilibrated problem in host memory (CSC, int64 indices as in the reference ABI).
 // std::vector storage whose resize() leaves new elements default-initialised (unset for
 // arithmetic types): the large CSC arrays of a prepare are written right away by parallel loops,
@@ -209,6 +220,15 @@ struct HostProblem {
   // all cones in order: (1, d) nonnegative orthant of dimension d, (3, d) PSD triangle of order d;
   // empty means every cone is PSD (the orders in psd)
   std::vector<std::pair<int, int>> cones;
+  // Factor-authoritative sampled blocks (sdpx_prepare_sampled): the PSD block starting at row
+  // `row_start` holds the columns col0 .. col0 + count - 1, column col0 + k being
+  // weight[k] svec(q_k q_k') with q_k column k of `basis` (order x count, column-major).  The
+  // engine uses these factors instead of testing the materialised columns.
+  struct Sampled {
+    int row_start = 0, col0 = 0, count = 0, order = 0;
+    std::vector<double> basis, weight;
+  };
+  std::vector<Sampled> sampled;
 };
 
 // Cone operator modes of k_congruence.
@@ -235,6 +255,9 @@ class Engine {
   }
   int n = 0, m = 0, nblk = 0;
   int nchol = 0;  // Schur tiles per side
+  int factor_form = kFormPlain;  // SDPX_B200_FORM=split or sdpx_b200_set_form
+  OzakiWorkspace oz;             // split-precision GEMM scratch
+  bool split_active() const { return factor_form == kFormSplit && n >= kSplitMin; }
   bool gram_enabled = true;  // rank-one blocks use the Gram form (SDPX_B200_GRAM=0 disables)
   int gram_blocks() const { return ngram_; }
   int nn_count() const { return nnn_; }
@@ -373,6 +396,8 @@ class Engine {
       gram_enabled = !(g && g[0] == '0');
       const char* c = std::getenv("SDPX_B200_GRAPHS");  // "0": launch every segment eagerly
       graphs_enabled = !(c && c[0] == '0');
+      const char* f = std::getenv("SDPX_B200_FORM");  // "split": split-precision factorisation
+      factor_form = (f && std::string(f) == "split") ? kFormSplit : kFormPlain;
     }
     red.init();
     status_.alloc(1);
@@ -484,7 +509,17 @@ class Engine {
     std::vector<long> gu_off(nblk, 0);
     std::vector<double> gu, gsig(col_ptr[nblk], 1.0);
     ngram_ = 0;
-    if (gram_enabled) {
+    std::vector<const HostProblem::Sampled*> sampled_of(nblk, nullptr);
+    for (const auto& sb : p.sampled) {
+      int j = 0;
+      while (j < nblk && hblocks[j].svec_off != sb.row_start) ++j;
+      if (j == nblk || hblocks[j].n != sb.order || hk[j] != sb.count)
+        throw std::invalid_argument("sampled block does not match its PSD cone or columns");
+      for (int t = 0; t < sb.count; ++t)
+        if (bcols[j][t] != sb.col0 + t) throw std::invalid_argument("sampled block columns are not its own");
+      sampled_of[j] = &sb;
+    }
+    if (gram_enabled || !p.sampled.empty()) {
       std::vector<long> u_off(nblk + 1, 0);
       for (int j = 0; j < nblk; ++j) u_off[j + 1] = u_off[j] + (long)hblocks[j].n * hk[j];
       std::vector<double> u_all(u_off[nblk]);
@@ -493,8 +528,15 @@ class Engine {
         for (int64_t it = i0; it < i1; ++it) {
           const int j = item_blk[it], t = (int)(it - col_ptr[j]);
           const int nj = hblocks[j].n, tn = nj * (nj + 1) / 2;
-          col_ok[it] = rank_one_column(&acol[acol_off[j] + (long)t * tn], nj,
-                                       &u_all[u_off[j] + (long)t * nj], &gsig[it]);
+          if (const HostProblem::Sampled* sb = sampled_of[j]) {  // the given factor, exactly
+            std::copy(sb->basis.begin() + (long)t * nj, sb->basis.begin() + (long)(t + 1) * nj,
+                      u_all.begin() + u_off[j] + (long)t * nj);
+            gsig[it] = sb->weight[t];
+            col_ok[it] = 1;
+          } else if (gram_enabled) {
+            col_ok[it] = rank_one_column(&acol[acol_off[j] + (long)t * tn], nj,
+                                         &u_all[u_off[j] + (long)t * nj], &gsig[it]);
+          }
         }
       });
       for (int j = 0; j < nblk; ++j) {
@@ -659,23 +701,8 @@ class Engine {
     Uinv_.alloc((size_t)n * n);
     UinvT_.alloc((size_t)n * n);
     Tmp_.alloc((size_t)n * n);
-    df_items_ = 0;
-    if (nchol > 0 && nchol <= kDfMaxTiles) {
-      std::vector<unsigned> items = chol_schedule(nchol);
-      if (!chol_schedule_valid(items, nchol)) throw CudaError("invalid Cholesky work list");
-      df_items_ = (int)items.size();
-      df_list_.alloc(items.size());
-      df_list_.upload(items.data(), items.size(), st);
-      df_sync_.alloc(2 + 2 * (size_t)nchol * nchol);
-      int per_sm = 0, sms = 0;
-      check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chol_dataflow, 256, kSmemDf),
-            "occupancy");
-      check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
-      // one CTA per SM: the chain CTA (the critical path) then has its SM to itself; the
-      // trailing updates are far from saturating the others
-      (void)per_sm;
-      df_grid_ = std::max(1, std::min(sms, df_items_));
-    }
+    make_schedule(nchol, df_list_, df_sync_, &df_items_, &df_grid_);
+    if (split_active()) prepare_split();
     step_out_.alloc(2 * (nblk + 1));
     hblk_.alloc(2 * (nblk + 1));
     {  // nonnegative-orthant rows: index list and their rows of A, dense (nnn x n)
@@ -732,6 +759,20 @@ class Engine {
     launched("k_nt_scale");
     tend(KT_SCALE);
     return read_status() == 0;
+  }
+
+  // Scaling given by the caller (the condensed KKT's sync from the cones' R and R^-1): per PSD
+  // block the n_j x n_j column-major R and R^-1 stacked in cone order (sum n_j^2 each); G^-1 =
+  // R^-T R^-1 is formed on the device.  lambda is not set (only the Schur assembly and the
+  // operators read this scaling).
+  void set_scaling(const double* hR, const double* hRinv) {
+    if (!nblk) return;
+    if (!hR || !hRinv) throw std::invalid_argument("null pointer");
+    R_.upload(hR, matlen_, st);
+    Rinv_.upload(hRinv, matlen_, st);
+    ++g_launches, k_ginv_from_rinv<<<nblk, 256, 0, st>>>(blocks_, Rinv_, Ginv_);
+    launched("k_ginv_from_rinv");
+    check(cudaStreamSynchronize(st), "scaling sync");
   }
 
   // y = op(x) for cone operator `mode`, ncols columns with stride ld.
@@ -928,50 +969,195 @@ class Engine {
     check(cudaStreamSynchronize(st), "diag sync");
     return hblk_[0];
   }
-  // F = chol(Hsave + eps I) with the dynamic pivot rule
-  bool factor(double eps, bool dynamic, double dyn_eps, double dyn_delta) {
-    factor_ok_ = false;
-    if (!n) return true;
-    clear_status();
-    ++g_launches, k_shifted_copy<<<1184, 256, 0, st>>>(Hsave_, F_, n, eps, diag0_);
-    if (df_items_ > 0)
-      check(cudaMemsetAsync(df_sync_.p, 0, (2 + 2 * (size_t)nchol * nchol) * sizeof(int), st),
+  // Storage of one dense factorisation: source matrix H (contiguous n x n), its shifted copy
+  // that becomes U, the diagonal-tile inverses, the original diagonal, the explicit inverse X
+  // and its transpose, a GEMM scratch, and the dataflow work list.
+  struct FactorBufs {
+    int n = 0, nchol = 0, df_items = 0, df_grid = 0;
+    const double* H = nullptr;
+    double *F = nullptr, *Dinv = nullptr, *diag0 = nullptr, *Uinv = nullptr, *UinvT = nullptr, *Tmp = nullptr;
+    const unsigned* df_list = nullptr;
+    int* df_sync = nullptr;
+  };
+  // A diagonal block of the split form with storage of its own (contiguous, so every dense
+  // kernel runs on it unchanged).
+  struct SubFactor {
+    DevBuf<double> H, F, Dinv, diag0, Uinv, UinvT, Tmp;
+    DevBuf<unsigned> df_list;
+    DevBuf<int> df_sync;
+    FactorBufs b;
+  };
+
+  // The dataflow work list of an nt x nt tile grid (validated before upload) and its grid size.
+  void make_schedule(int nt, DevBuf<unsigned>& list, DevBuf<int>& sync, int* items_out, int* grid_out) {
+    *items_out = 0;
+    *grid_out = 0;
+    if (nt <= 0 || nt > kDfMaxTiles) return;
+    std::vector<unsigned> items = chol_schedule(nt);
+    if (!chol_schedule_valid(items, nt)) throw CudaError("invalid Cholesky work list");
+    list.alloc(items.size());
+    list.upload(items.data(), items.size(), st);
+    sync.alloc(2 + 2 * (size_t)nt * nt);
+    int sms = 0;
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+    // one CTA per SM: the chain CTA (the critical path) then has its SM to itself; the
+    // trailing updates are far from saturating the others
+    *items_out = (int)items.size();
+    *grid_out = std::max(1, std::min(sms, *items_out));
+  }
+
+  FactorBufs full_bufs() {
+    FactorBufs b;
+    b.n = n; b.nchol = nchol; b.df_items = df_items_; b.df_grid = df_grid_;
+    b.H = Hsave_; b.F = F_; b.Dinv = Dinv_; b.diag0 = diag0_; b.Uinv = Uinv_; b.UinvT = UinvT_; b.Tmp = Tmp_;
+    b.df_list = df_list_; b.df_sync = df_sync_;
+    return b;
+  }
+
+  void setup_sub(SubFactor& s, int ns) {
+    const int nt = (ns + kNB - 1) / kNB;
+    s.H.alloc((size_t)ns * ns);
+    s.F.alloc((size_t)ns * ns);
+    s.Dinv.alloc((size_t)nt * kNB * kNB);
+    s.diag0.alloc(ns);
+    s.Uinv.alloc((size_t)ns * ns);
+    s.UinvT.alloc((size_t)ns * ns);
+    s.Tmp.alloc((size_t)ns * ns);
+    s.b = FactorBufs();
+    s.b.n = ns;
+    s.b.nchol = nt;
+    make_schedule(nt, s.df_list, s.df_sync, &s.b.df_items, &s.b.df_grid);
+    s.b.H = s.H; s.b.F = s.F; s.b.Dinv = s.Dinv; s.b.diag0 = s.diag0; s.b.Uinv = s.Uinv;
+    s.b.UinvT = s.UinvT; s.b.Tmp = s.Tmp; s.b.df_list = s.df_list; s.b.df_sync = s.df_sync;
+  }
+  int split_n1() const { return ((n / 2 + kNB - 1) / kNB) * kNB; }
+  void prepare_split() {
+    const int n1 = split_n1(), n2 = n - n1;
+    if (sub1_.b.n != n1) setup_sub(sub1_, n1);
+    if (sub2_.b.n != n2) setup_sub(sub2_, n2);
+  }
+
+  // F = chol(H + eps I) of one factorisation's buffers (dynamic pivot rule); the status word
+  // collects pivot failures.  diag_src (stride diag_stride): when given, the pivot rule's
+  // original diagonal is taken from there (+ eps) instead of from H.
+  void launch_chol(const FactorBufs& b, double eps, bool dynamic, double dyn_eps, double dyn_delta,
+                   const double* diag_src = nullptr, long diag_stride = 0) {
+    ++g_launches, k_shifted_copy<<<1184, 256, 0, st>>>(b.H, b.F, b.n, eps, b.diag0);
+    if (diag_src)
+      ++g_launches, k_strided_diag<<<(b.n + 255) / 256, 256, 0, st>>>(diag_src, diag_stride, b.n, eps, b.diag0);
+    if (b.df_items > 0) {  // one persistent launch over the whole tile schedule
+      check(cudaMemsetAsync(b.df_sync, 0, (2 + 2 * (size_t)b.nchol * b.nchol) * sizeof(int), st),
             "dataflow sync reset");
-    tbegin(KT_FACTOR);
-    if (df_items_ > 0) {  // one persistent launch over the whole tile schedule
-      ++g_launches, k_chol_dataflow<<<df_grid_, 256, kSmemDf, st>>>(
-          F_, n, nchol, df_list_, df_items_, df_sync_, dyn_eps, dyn_delta, dynamic ? 1 : 0, diag0_,
-          Dinv_, status_);
+      ++g_launches, k_chol_dataflow<<<b.df_grid, 256, kSmemDf, st>>>(
+          b.F, b.n, b.nchol, b.df_list, b.df_items, b.df_sync, dyn_eps, dyn_delta, dynamic ? 1 : 0, b.diag0,
+          b.Dinv, status_);
     }
-    for (int kb = 0; df_items_ == 0 && kb < nchol; ++kb) {
-      ++g_launches, k_potrf_diag<<<1, 1024, kSmemTrtri, st>>>(F_, n, kb, dyn_eps, dyn_delta, dynamic ? 1 : 0,
-                                                diag0_, Dinv_, status_);
-      int rest = nchol - kb - 1;
+    for (int kb = 0; b.df_items == 0 && kb < b.nchol; ++kb) {
+      ++g_launches, k_potrf_diag<<<1, 1024, kSmemTrtri, st>>>(b.F, b.n, kb, dyn_eps, dyn_delta, dynamic ? 1 : 0,
+                                                              b.diag0, b.Dinv, status_);
+      int rest = b.nchol - kb - 1;
       if (rest > 0) {
-        ++g_launches, k_trsm_panel<<<rest, SDPXG_THREADS, kSmemTrsm, st>>>(F_, n, kb, Dinv_);
-        ++g_launches, k_syrk_update<<<rest * (rest + 1) / 2, SDPXG_THREADS, kSmemSyrk, st>>>(F_, n, kb);
+        ++g_launches, k_trsm_panel<<<rest, SDPXG_THREADS, kSmemTrsm, st>>>(b.F, b.n, kb, b.Dinv);
+        ++g_launches, k_syrk_update<<<rest * (rest + 1) / 2, SDPXG_THREADS, kSmemSyrk, st>>>(b.F, b.n, kb);
       }
     }
     launched("factor");
+  }
+  // X = U^-1 of one factorisation: diagonal tiles, then one batched GEMM pair per level.
+  void launch_trinv(const FactorBufs& b) {
+    ++g_launches, k_trtri_diag<<<b.nchol, SDPXG_THREADS, 0, st>>>(b.n, b.Dinv, b.Uinv, b.UinvT);
+    for (int level = 1; (1 << (level - 1)) < b.nchol; ++level) {
+      const int g = 1 << level, h = g >> 1;
+      dim3 grid(h, h, (b.nchol + g - 1) / g);
+      for (int phase = 0; phase < 2; ++phase)
+        ++g_launches, k_trinv_level<<<grid, SDPXG_THREADS, kSmemTrinv, st>>>(b.F, b.Uinv, b.UinvT, b.Tmp, b.n,
+                                                                             level, phase);
+    }
+    launched("trinv");
+  }
+  void copy_block(double* dst, long ldd, const double* src, long lds, int rows, int cols) {
+    if (rows <= 0 || cols <= 0) return;
+    check(cudaMemcpy2DAsync(dst, ldd * sizeof(double), src, lds * sizeof(double), rows * sizeof(double), cols,
+                            cudaMemcpyDeviceToDevice, st),
+          "block copy");
+  }
+
+  // F = chol(Hsave + eps I) with the dynamic pivot rule, then X = F^-1 explicitly.
+  bool factor(double eps, bool dynamic, double dyn_eps, double dyn_delta) {
+    factor_ok_ = false;
+    if (!n) return true;
+    if (split_active()) return factor_split(eps, dynamic, dyn_eps, dyn_delta);
+    clear_status();
+    const FactorBufs b = full_bufs();
+    tbegin(KT_FACTOR);
+    launch_chol(b, eps, dynamic, dyn_eps, dyn_delta);
     tend(KT_FACTOR);
     uint32_t s = read_status();
     if (s & SDPXG_ST_SYNC_TIMEOUT) throw CudaError("factorization: a bounded inter-CTA wait gave up");
     factor_ok_ = (s == 0);
     if (factor_ok_) {
       tbegin(KT_TRINV);
-      // explicit inverse of the factor: diagonal tiles, then one batched GEMM pair per level
-      ++g_launches, k_trtri_diag<<<nchol, SDPXG_THREADS, 0, st>>>(n, Dinv_, Uinv_, UinvT_);
-      for (int level = 1; (1 << (level - 1)) < nchol; ++level) {
-        const int g = 1 << level, h = g >> 1;
-        dim3 grid(h, h, (nchol + g - 1) / g);
-        for (int phase = 0; phase < 2; ++phase)
-          ++g_launches, k_trinv_level<<<grid, SDPXG_THREADS, kSmemTrinv, st>>>(
-              F_, Uinv_, UinvT_, Tmp_, n, level, phase);
-      }
-      launched("trinv");
+      launch_trinv(b);
       tend(KT_TRINV);
     }
     return factor_ok_;
+  }
+
+  // The split form (kFormSplit).  With n1 = n/2 rounded up to the tile and n2 = n - n1:
+  //   U11' U11 = H11 + eps I (FP64 dataflow), X11 = U11^-1 (FP64)
+  //   U12 = X11' H12                       split-precision GEMM
+  //   U22' U22 = H22 + eps I - U12' U12      split-precision GEMM, then FP64 dataflow, X22 (FP64)
+  //   X12 = -(X11 U12) X22                  two split-precision GEMMs
+  // so that U = [U11 U12; 0 U22] and X = U^-1 = [X11 X12; 0 X22], with the same pivot rule on
+  // the same original diagonal as the plain form.  Only the upper triangles of X and U and the
+  // lower triangle of X' are assembled (the solves read nothing else).
+  bool factor_split(double eps, bool dynamic, double dyn_eps, double dyn_delta) {
+    prepare_split();
+    const int n1 = split_n1(), n2 = n - n1;
+    const long ldn = n;
+    clear_status();
+    check(cudaMemsetAsync(oz_status_word(), 0, sizeof(uint32_t), st), "memset");
+    tbegin(KT_FACTOR);
+    copy_block(sub1_.H, n1, Hsave_, ldn, n1, n1);
+    copy_block(sub2_.H, n2, Hsave_ + (long)n1 * ldn + n1, ldn, n2, n2);
+    launch_chol(sub1_.b, eps, dynamic, dyn_eps, dyn_delta);
+    launch_trinv(sub1_.b);
+    double* U12 = F_.p + (long)n1 * ldn;  // F[0:n1, n1:n]
+    // U12 = X11' H12: rows of the left operand are the columns of X11, rows of the right
+    // operand the columns of H12
+    ozaki_gemm(oz, st, n1, n2, n1, sub1_.Uinv, n1, 1, Hsave_.p + (long)n1 * ldn, ldn, 1, 1.0, 0.0, U12, ldn, 0);
+    // S = H22 - U12' U12 (full, exactly symmetric: the integer product of an operand with itself)
+    ozaki_gemm(oz, st, n2, n2, n1, U12, ldn, 1, U12, ldn, 1, -1.0, 1.0, sub2_.H, n2, 0);
+    // the pivot rule's original diagonal is that of H22 + eps I, as in the plain form
+    launch_chol(sub2_.b, eps, dynamic, dyn_eps, dyn_delta, Hsave_.p + (long)n1 * ldn + n1, ldn + 1);
+    launch_trinv(sub2_.b);
+    // X12 = -(X11 U12) X22
+    ozaki_gemm(oz, st, n1, n2, n1, sub1_.Uinv, 1, n1, U12, ldn, 1, 1.0, 0.0, Tmp_, n1, 0);
+    ozaki_gemm(oz, st, n1, n2, n2, Tmp_, 1, n1, sub2_.Uinv, n2, 1, -1.0, 0.0, Uinv_.p + (long)n1 * ldn, ldn, 0);
+    // assemble U, X and X'
+    copy_block(F_, ldn, sub1_.F, n1, n1, n1);
+    copy_block(F_.p + (long)n1 * ldn + n1, ldn, sub2_.F, n2, n2, n2);
+    copy_block(Uinv_, ldn, sub1_.Uinv, n1, n1, n1);
+    copy_block(Uinv_.p + (long)n1 * ldn + n1, ldn, sub2_.Uinv, n2, n2, n2);
+    copy_block(UinvT_, ldn, sub1_.UinvT, n1, n1, n1);
+    copy_block(UinvT_.p + (long)n1 * ldn + n1, ldn, sub2_.UinvT, n2, n2, n2);
+    ++g_launches, k_transpose_block<<<dim3((n2 + 31) / 32, (n1 + 31) / 32), dim3(32, 8), 0, st>>>(
+        Uinv_.p + (long)n1 * ldn, ldn, n1, n2, UinvT_.p + n1, ldn);
+    launched("split factor");
+    tend(KT_FACTOR);
+    uint32_t s = read_status();
+    if (s & SDPXG_ST_SYNC_TIMEOUT) throw CudaError("factorization: a bounded inter-CTA wait gave up");
+    uint32_t hs[2] = {0, 0};
+    copy_d2h(&hs[0], oz.status.p, sizeof(uint32_t), st);
+    copy_d2h(&hs[1], oz.err.p, sizeof(uint32_t), st);
+    check(cudaStreamSynchronize(st), "split status");
+    if (hs[1]) throw CudaError("split-precision GEMM: a bounded wait gave up");
+    factor_ok_ = (s == 0 && hs[0] == 0);
+    return factor_ok_;
+  }
+  uint32_t* oz_status_word() {
+    if (!oz.status.p) oz.status.alloc(1);
+    return oz.status.p;
   }
   // x = F^-1 r = U^-1 (U^-T r) through the explicit inverse: two coalesced GEMVs.
   void trisolve(const double* r, double* x) {
@@ -1064,6 +1250,7 @@ class Engine {
   DevBuf<unsigned> df_list_;
   DevBuf<int> df_sync_;
   int df_items_ = 0, df_grid_ = 0;
+  SubFactor sub1_, sub2_;  // diagonal blocks of the split form
   cudaEvent_t ev_[2 * KT_N] = {};
   struct GraphEntry {
     cudaGraphExec_t exec;

@@ -1,0 +1,287 @@
+// Modular INT8 tensor-core GEMM on sm_100a: one CTA per (128-row tile, tile_n-column tile,
+// modulus).  Warp-specialised, non-persistent:
+//   warp 4 (one lane)  TMA producer: K-blocks of 128 bytes of every digit plane of A and B into a
+//                      ring of shared-memory stages (128-byte swizzle), completion counted in
+//                      bytes on the stage's `full` mbarrier;
+//   warp 5 (one lane)  MMA issuer: 4 x tcgen05.mma.kind::i8 (K = 32 bytes each) per digit pair and
+//                      stage into TMEM accumulators (one per digit sum), tcgen05.commit frees the
+//                      stage; a last commit signals the epilogue;
+//   warps 0-3          epilogue: tcgen05.ld of the accumulators (warp w reads TMEM lanes
+//                      32w..32w+31 = output rows), reduction modulo the tile's modulus, coalesced
+//                      stores (consecutive lanes = consecutive rows of a column-major plane).
+// Every wait is bounded; a wait that gives up sets bit 0 of args.err, the other roles stop at
+// their next wait, outstanding TMA copies are drained (bounded) and TMEM is released before exit.
+#include <cuda.h>
+
+#include <mutex>
+#include <stdexcept>
+#include <string>
+
+#include "device.cuh"
+#include "i8_gemm.cuh"
+#include "tc05.cuh"
+
+namespace sdpxg {
+namespace {
+
+constexpr int kBM = 128;     // rows per tile (MMA M)
+constexpr int kKB = 128;     // K bytes per stage (one 128-byte swizzle row)
+constexpr int kThreads = 192;
+
+template <int DIGITS>
+struct Cfg;
+template <>
+struct Cfg<1> {
+  static constexpr int BN = 256, STAGES = 4, NACC = 1, TMEM_COLS = 256;
+};
+template <>
+struct Cfg<2> {
+  static constexpr int BN = 128, STAGES = 3, NACC = 3, TMEM_COLS = 512;
+};
+
+template <int DIGITS>
+constexpr int stage_bytes() {
+  return DIGITS * (kBM * kKB + Cfg<DIGITS>::BN * kKB);
+}
+template <int DIGITS>
+constexpr size_t smem_bytes() {
+  // stages, then 2 * STAGES + 1 mbarriers, the TMEM address, the abort flag and the consumed
+  // count, plus 1024 bytes to align the stage ring to the swizzle atom
+  return (size_t)Cfg<DIGITS>::STAGES * stage_bytes<DIGITS>() + (2 * Cfg<DIGITS>::STAGES + 1) * 8 + 16 + 1024;
+}
+
+__device__ __forceinline__ void give_up(volatile int* abort, int* err) {
+  *abort = 1;
+  if (err) atomicOr(err, 1);
+}
+
+template <int DIGITS>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_i8_mod_gemm(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, I8GemmArgs a) {
+  constexpr int BN = Cfg<DIGITS>::BN, STAGES = Cfg<DIGITS>::STAGES, NACC = Cfg<DIGITS>::NACC;
+  constexpr int TCOLS = Cfg<DIGITS>::TMEM_COLS;
+  constexpr int SB = stage_bytes<DIGITS>();
+  constexpr int A_TILE = kBM * kKB, B_TILE = BN * kKB;
+  const int tm = blockIdx.x, tn = blockIdx.y, l = blockIdx.z;
+  if (a.upper_only && tm * kBM > tn * BN + BN - 1) return;  // every entry of the tile has i > j
+
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)STAGES * SB);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  int* consumed = reinterpret_cast<int*>(tmem_slot + 2);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      tc05::mbar_init(&full[s], 1);
+      tc05::mbar_init(&empty[s], 1);
+    }
+    tc05::mbar_init(done, 1);
+    *abort = 0;
+    *consumed = 0;
+    tc05::fence_barrier_init();
+  }
+  if (warp == 0) {
+    __syncwarp();  // the .sync.aligned allocation needs the whole warp converged
+    tc05::tmem_alloc(tmem_slot, TCOLS);
+    tc05::tmem_relinquish();
+  }
+  tc05::tc_fence_before();
+  __syncthreads();
+  tc05::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int nk = a.Kpad / kKB;
+  int issued = 0;
+
+  if (warp == 4 && lane == 0) {  // ---- TMA producer ----
+    tc05::tma_prefetch_map(&tA);
+    tc05::tma_prefetch_map(&tB);
+    for (int it = 0; it < nk; ++it) {
+      const int s = it % STAGES, r = it / STAGES;
+      if (r > 0 && !tc05::mbar_wait(&empty[s], (r - 1) & 1, abort)) {
+        give_up(abort, a.err);
+        break;
+      }
+      tc05::mbar_arrive_expect_tx(&full[s], SB);
+      uint8_t* st = smem + (size_t)s * SB;
+      const int x = a.k0 + it * kKB;
+#pragma unroll
+      for (int d = 0; d < DIGITS; ++d) {
+        tc05::tma_load_2d(st + d * A_TILE, &tA, &full[s], x, (l * DIGITS + d) * a.Mpad + tm * kBM);
+        tc05::tma_load_2d(st + DIGITS * A_TILE + d * B_TILE, &tB, &full[s], x,
+                          (l * DIGITS + d) * a.Npad + tn * BN);
+      }
+      issued = it + 1;
+    }
+  } else if (warp == 5 && lane == 0) {  // ---- MMA issuer ----
+    constexpr uint32_t idesc = tc05::idesc_i8(kBM, BN);
+    int it = 0;
+    for (; it < nk; ++it) {
+      const int s = it % STAGES, r = it / STAGES;
+      if (!tc05::mbar_wait(&full[s], r & 1, abort)) {
+        give_up(abort, a.err);
+        break;
+      }
+      tc05::tc_fence_after();
+      const uint32_t st = tc05::smem_u32(smem + (size_t)s * SB);
+#pragma unroll
+      for (int kk = 0; kk < kKB / 32; ++kk) {
+        const uint32_t first = (it == 0 && kk == 0) ? 0u : 1u;
+        if (DIGITS == 1) {
+          const uint64_t ad = tc05::sdesc_k_sw128(st) + 2 * kk;
+          const uint64_t bd = tc05::sdesc_k_sw128(st + A_TILE) + 2 * kk;
+          tc05::mma_i8(tmem, ad, bd, idesc, first);
+        } else {
+          const uint64_t a0 = tc05::sdesc_k_sw128(st) + 2 * kk;
+          const uint64_t a1 = tc05::sdesc_k_sw128(st + A_TILE) + 2 * kk;
+          const uint64_t b0 = tc05::sdesc_k_sw128(st + 2 * A_TILE) + 2 * kk;
+          const uint64_t b1 = tc05::sdesc_k_sw128(st + 2 * A_TILE + B_TILE) + 2 * kk;
+          tc05::mma_i8(tmem, a0, b0, idesc, first);               // D0 += lo lo
+          tc05::mma_i8(tmem + BN, a0, b1, idesc, first);          // D1 += lo hi
+          tc05::mma_i8(tmem + BN, a1, b0, idesc, 1u);             // D1 += hi lo
+          tc05::mma_i8(tmem + 2 * BN, a1, b1, idesc, first);      // D2 += hi hi
+        }
+      }
+      tc05::mma_commit(&empty[s]);
+    }
+    *consumed = it;
+    tc05::mma_commit(done);  // completes once every MMA issued above has
+  } else if (warp < 4) {  // ---- epilogue ----
+    const bool waited = tc05::mbar_wait(done, 0, abort);
+    if (!waited) give_up(abort, a.err);
+    // warp-uniform decision: tcgen05.ld is .sync.aligned
+    const bool go = __all_sync(0xffffffffu, waited && !*abort);
+    tc05::tc_fence_after();
+    if (go) {
+      const int row = warp * 32 + lane;
+      const int i = tm * kBM + row;
+      const int p = a.moduli[l];
+      const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+      for (int c0 = 0; c0 < BN; c0 += 32) {
+        uint32_t acc[NACC][32];
+#pragma unroll
+        for (int q = 0; q < NACC; ++q) tc05::tmem_ld32(lane_base + q * BN + c0, acc[q]);
+        tc05::tmem_ld_wait();
+        const int j0 = tn * BN + c0;
+        if (i < a.m) {
+          if (DIGITS == 1) {
+            int8_t* out = static_cast<int8_t*>(a.out) + (long)l * a.plane;
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+              const int j = j0 + q;
+              if (j < a.n) {
+                int r = (int)acc[0][q] % p;  // |r| < p
+                if (r > p / 2) r -= p;
+                if (r < -((p - 1) / 2)) r += p;
+                out[(long)j * a.m + i] = (int8_t)r;
+              }
+            }
+          } else {
+            int* out = static_cast<int*>(a.out) + (long)l * a.plane;
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+              const int j = j0 + q;
+              if (j < a.n) {
+                long long v = (long long)(int)acc[0][q] + ((long long)(int)acc[NACC > 1 ? 1 : 0][q] << 8) +
+                              ((long long)(int)acc[NACC > 2 ? 2 : 0][q] << 16);
+                long long r = v % p;
+                if (r < 0) r += p;
+                if (a.accumulate) {
+                  r += out[(long)j * a.m + i];
+                  if (r >= p) r -= p;
+                }
+                out[(long)j * a.m + i] = (int)r;
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (warp == 4 && lane == 0) {  // copies the MMA issuer never consumed must land before exit
+    for (int it = *consumed; it < issued; ++it) tc05::mbar_wait(&full[it % STAGES], (it / STAGES) & 1, nullptr);
+  }
+  tc05::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc05::tc_fence_after();
+    tc05::tmem_dealloc(tmem, TCOLS);
+  }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  });
+  if (!fn) throw CudaError("cuTensorMapEncodeTiled is not available");
+  return fn;
+}
+
+// Byte matrix of `rows` rows of `kpad` bytes (row stride kpad), boxes of box_rows x 128 bytes,
+// 128-byte swizzle.
+CUtensorMap byte_map(const int8_t* base, long rows, int kpad, int box_rows) {
+  if (reinterpret_cast<uintptr_t>(base) % 16) throw std::invalid_argument("TMA base not 16-byte aligned");
+  if (kpad % kKB) throw std::invalid_argument("K padding must be a multiple of 128");
+  CUtensorMap m;
+  const cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)kpad};
+  const cuuint32_t box[2] = {(cuuint32_t)kKB, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(base), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return m;
+}
+
+template <int DIGITS>
+void launch(const int8_t* A, const int8_t* B, const I8GemmArgs& a, cudaStream_t st) {
+  constexpr int BN = Cfg<DIGITS>::BN;
+  if (a.Mpad <= 0 || a.Npad <= 0 || a.Kpad <= 0 || a.Mpad % kBM || a.Npad % BN || a.Kpad % kKB ||
+      a.Kld % kKB || a.k0 % kKB || a.k0 < 0 || a.k0 + a.Kpad > a.Kld)
+    throw std::invalid_argument("i8 GEMM: padded extents must be multiples of the tile");
+  if (a.m > a.Mpad || a.n > a.Npad || a.L <= 0 || a.L > 65535 || !a.moduli || !a.out)
+    throw std::invalid_argument("i8 GEMM: bad arguments");
+  if (a.Kpad > (1 << 17)) throw std::invalid_argument("i8 GEMM: K above 2^17 per call is not exact");
+  static std::once_flag attr;
+  std::call_once(attr, [] {
+    check(cudaFuncSetAttribute(k_i8_mod_gemm<DIGITS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem_bytes<DIGITS>()),
+          "i8 gemm smem attribute");
+  });
+  const CUtensorMap ta = byte_map(A, (long)a.L * DIGITS * a.Mpad, a.Kld, kBM);
+  const CUtensorMap tb = byte_map(B, (long)a.L * DIGITS * a.Npad, a.Kld, BN);
+  const dim3 grid(a.Mpad / kBM, a.Npad / BN, a.L);
+  ++g_launches;
+  k_i8_mod_gemm<DIGITS><<<grid, kThreads, smem_bytes<DIGITS>(), st>>>(ta, tb, a);
+  check(cudaGetLastError(), "k_i8_mod_gemm launch");
+}
+
+}  // namespace
+
+void launch_i8_gemm(int digits, const int8_t* A, const int8_t* B, const I8GemmArgs& args, cudaStream_t st) {
+  if (digits == 1)
+    launch<1>(A, B, args, st);
+  else if (digits == 2)
+    launch<2>(A, B, args, st);
+  else
+    throw std::invalid_argument("i8 GEMM: digits must be 1 or 2");
+}
+
+}  // namespace sdpxg

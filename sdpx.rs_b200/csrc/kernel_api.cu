@@ -7,6 +7,7 @@
 
 #include "../../include/sdpx_b200.h"
 #include "hsd.cuh"
+#include "sampled.cuh"
 
 using namespace sdpxg;
 
@@ -20,6 +21,9 @@ template <typename F>
 int32_t guard(F&& f) {
   try {
     return f();
+  } catch (const sdpxg::SampledUnsupported& e) {
+    sdpxg::g_last_error = e.what();
+    return 2;
   } catch (const std::invalid_argument& e) {
     sdpxg::g_last_error = e.what();
     return 1;
@@ -136,6 +140,49 @@ int32_t sdpxg_problem_upload(sdpxg_ctx* ctx, const sdpx_csc* P, const sdpx_csc* 
   });
 }
 
+int32_t sdpxg_problem_upload_sampled(sdpxg_ctx* ctx, const sdpx_csc* P, const sdpx_csc* A_linear,
+                                     const uint64_t* psd_orders, uint64_t block_count,
+                                     const sdpx_sampled_block* blocks, uint64_t nblocks) {
+  return guard([&] {
+    if (!ctx || !A_linear) throw std::invalid_argument("null pointer");
+    if (block_count && !psd_orders) throw std::invalid_argument("null pointer");
+    std::vector<int64_t> cp, rv;
+    std::vector<double> v;
+    csc_into(A_linear, cp, rv, v, A_linear->cols);
+    std::vector<std::pair<uint64_t, uint64_t>> psd_rows;
+    uint64_t row = 0;
+    for (uint64_t j = 0; j < block_count; ++j) {
+      psd_rows.push_back({row, psd_orders[j]});
+      row += psd_orders[j] * (psd_orders[j] + 1) / 2;
+    }
+    SampledCsc merged = materialize_sampled(A_linear->rows, A_linear->cols, cp, rv, v, psd_rows, blocks, nblocks);
+    sdpx_csc A{};
+    A.rows = A_linear->rows;
+    A.cols = A_linear->cols;
+    A.nnz = merged.rowval.size();
+    A.colptr = merged.colptr.data();
+    A.rowval = merged.rowval.data();
+    A.values.kind = 0;
+    A.values.count = merged.val.size();
+    A.values.f64 = merged.val.data();
+    const int32_t rc = sdpxg_problem_upload(ctx, P, &A, psd_orders, block_count);
+    if (rc) return rc;
+    // the given factors replace the rank-one test of the materialised columns
+    ctx->prob.sampled = std::move(merged.recs);
+    ctx->eng->upload(ctx->prob);
+    ctx->kkt = std::make_unique<HsdSolver>(*ctx->eng, ctx->prob, ctx->eq, Settings());
+    return 0;
+  });
+}
+
+int32_t sdpxg_set_scaling(sdpxg_ctx* ctx, const double* R, const double* Rinv) {
+  return guard([&] {
+    need(ctx);
+    ctx->eng->set_scaling(R, Rinv);
+    return 0;
+  });
+}
+
 int32_t sdpxg_identity_scaling(sdpxg_ctx* ctx) {
   return guard([&] {
     need(ctx);
@@ -188,6 +235,45 @@ int32_t sdpxg_factor(sdpxg_ctx* ctx, double shift, uint32_t dynamic, double eps,
     need(ctx);
     bool ok = ctx->eng->factor(shift, dynamic != 0, eps, delta);
     if (status) *status = ok ? 0u : (uint32_t)SDPXG_ST_PIVOT_FAIL;
+    return 0;
+  });
+}
+
+int32_t sdpxg_set_factor_form(sdpxg_ctx* ctx, uint32_t form) {
+  return guard([&] {
+    if (!ctx) throw std::invalid_argument("null context");
+    if (form > 1) throw std::invalid_argument("form must be 0 (plain) or 1 (split precision)");
+    ctx->eng->factor_form = (int)form;
+    return 0;
+  });
+}
+
+int32_t sdpxg_split_dgemm_device(sdpxg_ctx* ctx, char ta, char tb, uint64_t m, uint64_t n, uint64_t k,
+                                 double alpha, const double* d_A, uint64_t lda, const double* d_B, uint64_t ldb,
+                                 double beta, double* d_C, uint64_t ldc, uint32_t* status) {
+  return guard([&] {
+    if (!ctx) throw std::invalid_argument("null context");
+    if ((ta != 'N' && ta != 'T') || (tb != 'N' && tb != 'T')) throw std::invalid_argument("bad transpose flag");
+    if (m > (1u << 30) || n > (1u << 30) || k > (1u << 16)) throw std::invalid_argument("size out of range");
+    if (m == 0 || n == 0) return 0;
+    const uint64_t ar = ta == 'N' ? m : k, br = tb == 'N' ? k : n;
+    if (lda < std::max<uint64_t>(ar, 1) || ldb < std::max<uint64_t>(br, 1) || ldc < m)
+      throw std::invalid_argument("leading dimension too small");
+    if (!d_A || !d_B || !d_C) throw std::invalid_argument("null pointer");
+    Engine& E = *ctx->eng;
+    check(cudaSetDevice(E.device), "cudaSetDevice");
+    // the left operand's row i is row i of op(A); the right operand's row j is column j of op(B)
+    const long l_sr = ta == 'N' ? 1 : (long)lda, l_sk = ta == 'N' ? (long)lda : 1;
+    const long r_sr = tb == 'N' ? (long)ldb : 1, r_sk = tb == 'N' ? 1 : (long)ldb;
+    if (!E.oz.status.p) E.oz.status.alloc(1);
+    check(cudaMemsetAsync(E.oz.status.p, 0, sizeof(uint32_t), E.st), "memset");
+    ozaki_gemm(E.oz, E.st, (int)m, (int)n, (int)k, d_A, l_sr, l_sk, d_B, r_sr, r_sk, alpha, beta, d_C, (long)ldc, 0);
+    uint32_t hs[2] = {0, 0};
+    copy_d2h(&hs[0], E.oz.status.p, sizeof(uint32_t), E.st);
+    copy_d2h(&hs[1], E.oz.err.p, sizeof(uint32_t), E.st);
+    check(cudaStreamSynchronize(E.st), "sync");
+    if (hs[1]) throw std::runtime_error("split-precision GEMM: a bounded wait gave up");
+    if (status) *status = hs[0];
     return 0;
   });
 }

@@ -4,19 +4,32 @@
 // rns_blas.rs:2134-2417 gemm): every entry of C = op(A) op(B) is the exact dot product rounded
 // once to 64N bits, ties to even -- bit-identical to MpFloat::dot_fma (exactdot.rs:53-70).
 //
-// Pipeline (one call):
-//   k_rns_scan      per row of op(A) / column of op(B): lowest set-bit exponent lo and the
-//                   width `bits` of the aligned integers (rns_blas.rs:2164-2183 alignment)
-//   k_rns_residues  every entry as the integer M * 2^(e - 64N - lo) reduced to symmetric
-//                   residues modulo L primes below 2^21 (rns_blas.rs:929-986 panel residues)
-//   k_rns_gemm      one exact FP64 product per prime: symmetric residues keep |r| < 2^20, so
-//                   8192 products sum exactly below 2^53; partial sums are reduced modulo the
-//                   prime every 8192 terms (rns_blas.rs:447-580 per-prime dgemm)
-//   k_rns_crt       Garner's mixed-radix CRT back to the signed integer, then one rounding to
-//                   64N bits, ties to even (rns_blas.rs:1873-2125 CRT and pack,
-//                   exactdot.rs:1316-1392 from_scaled_integer)
+// Two forms of the same product, bitwise equal (correct rounding has one answer):
+//
+// INT8 tensor-core form (the default, RNS_FORM_INT8):
+//   k_rns_scan       per row of op(A) / column of op(B): lowest set-bit exponent lo and the
+//                    width `bits` of the aligned integers (rns_blas.rs:2164-2183 alignment)
+//   k_rns_pow2       2^s mod p for every prime and every bit position an entry can reach
+//   k_rns8_residues  every entry as the integer M * 2^(e - 64N - lo) reduced to symmetric
+//                    residues modulo L primes below 2^15, each split into two signed-byte
+//                    digits r = lo + 256 hi, written as K-major byte planes
+//                    (rns_blas.rs:929-986 panel residues)
+//   k_i8_mod_gemm    per prime, the four digit products on tcgen05.mma kind::i8 with INT32
+//                    accumulators in TMEM, recombined and reduced modulo the prime in the
+//                    epilogue; K beyond 2^16 in chunks whose residues are added
+//                    (rns_blas.rs:447-580 per-prime integer products)
+//   k_rns_crt        Garner's mixed-radix CRT back to the signed integer, then one rounding to
+//                    64N bits, ties to even (rns_blas.rs:1873-2125 CRT and pack,
+//                    exactdot.rs:1316-1392 from_scaled_integer)
+// FP64 form (RNS_FORM_FP64, the plain form on CUDA cores):
+//   k_rns_residues   residues modulo primes below 2^21 as doubles
+//   k_rns_gemm       one exact FP64 product per prime: symmetric residues keep |r| < 2^20, so
+//                    8192 products sum exactly below 2^53; partial sums are reduced modulo the
+//                    prime every 8192 terms
+//   k_rns_crt        as above.
 // The number of primes L follows the needed width 2*(64N) + spreads + log2(k) + 2 bits, the
-// same bound as the reference's Plan (rns_blas.rs:2202-2208).
+// same bound as the reference's Plan (rns_blas.rs:2202-2208); the reference's own primes are
+// 18-26 bits wide, the INT8 form uses 15-bit primes so that a residue is two signed bytes.
 //
 // Element layout (the reference's in-memory MpFloat<N>, arithmetic/src/lib.rs:333-340):
 //   u64 limbs[N] (least significant first), i32 kind (sign * MPFR kind: 2 zero, 3 regular),
@@ -30,6 +43,7 @@
 
 #include "../../include/sdpx_b200.h"
 #include "engine.cuh"
+#include "i8_gemm.cuh"
 
 using namespace sdpxg;
 
@@ -40,7 +54,7 @@ std::shared_ptr<void>* ctx_rns_slot(sdpxg_ctx* c);
 }  // namespace sdpxg
 
 #define RNS_MAXN 16    // limbs: up to 1024-bit values
-#define RNS_MAXL 160   // primes
+#define RNS_MAXL 192   // primes (1024-bit values at k = 2^20 need about 150 of 15 bits)
 #define RNS_MAXW 56    // 64-bit words of the reconstructed integer
 #define RNS_KC 8192    // exact FP64 terms between two reductions modulo the prime
 #define MP_ZERO 2
@@ -203,16 +217,81 @@ k_rns_gemm(const double* __restrict__ RA, const double* __restrict__ RB, double*
     }
 }
 
+// 2^s mod p_t for s < S (row t of the table).
+extern "C" __global__ void k_rns_pow2(int L, const int* __restrict__ primes, int S, uint32_t* __restrict__ out) {
+  const int t = blockIdx.y, s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= L || s >= S) return;
+  out[(size_t)t * S + s] = pow2mod(s, (uint32_t)primes[t]);
+}
+
+// INT8 form: symmetric residues modulo L primes below 2^15 of every entry of a view, each split
+// into signed-byte digits r = lo + 256 hi (|hi| <= 64), written to K-major byte planes: digit d
+// of prime t for line x (a row of op(A) or a column of op(B)) and inner index y at
+// out[((2t + d) * Rpad + x) * Kld + y].  Lines >= nlines and y >= len (the padding) get zeros.
+// One thread per (x, y), y fastest: the plane writes are coalesced.  The residue of
+// M * 2^shift is sum_c chunk_c * (2^(16c + shift) mod p) over the 16-bit chunks of the mantissa
+// limbs (each term < 2^31), reduced once.
+extern "C" __global__ void k_rns8_residues(const unsigned char* __restrict__ X, int N, int nlines, int len,
+                                           long sx, long sy, const int* __restrict__ lo, int L,
+                                           const int* __restrict__ primes, const uint32_t* __restrict__ pow2,
+                                           int S, int8_t* __restrict__ out, int Rpad, int Kld) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)Rpad * Kld) return;
+  const int y = (int)(idx % Kld), x = (int)(idx / Kld);
+  const size_t plane = (size_t)Rpad * Kld;
+  int8_t* o = out + (size_t)x * Kld + y;
+  bool live = x < nlines && y < len;
+  bool neg = false;
+  int shift = 0;
+  unsigned long long limbs[RNS_MAXN];
+  if (live) {
+    const unsigned char* e = X + ((long)x * sx + (long)y * sy) * (8L * N + 8);
+    const int kind = elem_kind(e, N);
+    live = abs(kind) == MP_REGULAR;
+    if (live) {
+      neg = kind < 0;
+      shift = elem_exp(e, N) - 64 * N - lo[x];
+      const unsigned long long* lp = reinterpret_cast<const unsigned long long*>(e);
+#pragma unroll
+      for (int q = 0; q < RNS_MAXN; ++q) limbs[q] = q < N ? lp[q] : 0ull;
+    }
+  }
+  for (int t = 0; t < L; ++t) {
+    int dlo = 0, dhi = 0;
+    if (live) {
+      const uint32_t* w = pow2 + (size_t)t * S + shift;
+      unsigned long long acc = 0;
+#pragma unroll
+      for (int q = 0; q < RNS_MAXN; ++q) {
+        if (q < N) {
+          const unsigned long long v = limbs[q];
+          acc += (v & 0xFFFFull) * w[64 * q] + ((v >> 16) & 0xFFFFull) * w[64 * q + 16] +
+                 ((v >> 32) & 0xFFFFull) * w[64 * q + 32] + (v >> 48) * w[64 * q + 48];
+        }
+      }
+      const int p = primes[t];
+      int r = (int)(acc % (unsigned long long)p);
+      if (r > p / 2) r -= p;
+      if (neg) r = -r;
+      dlo = ((r + 128) & 255) - 128;
+      dhi = (r - dlo) >> 8;
+    }
+    o[(size_t)(2 * t) * plane] = (int8_t)dlo;
+    o[(size_t)(2 * t + 1) * plane] = (int8_t)dhi;
+  }
+}
+
 // Garner CRT of the L residues of every output, then one rounding to 64N bits (ties to even).
-extern "C" __global__ void k_rns_crt(const double* __restrict__ RC, long planeC, int m, int n,
-                                     int L, int WW, const uint32_t* __restrict__ primes,
-                                     const uint32_t* __restrict__ inv,
-                                     const uint32_t* __restrict__ pmod,
-                                     const unsigned long long* __restrict__ Mbig,
-                                     const unsigned long long* __restrict__ halfM,
-                                     const int* __restrict__ loA, const int* __restrict__ loB,
-                                     int N, int upper_only, unsigned char* __restrict__ C,
-                                     uint32_t* __restrict__ status) {
+// Residues are read as R (double: the FP64 form's exact integers, possibly negative; int: the
+// INT8 form's residues in [0, p)).  The mixed-radix digits are formed with one reduction per
+// prime: sum_s v_s (prod_{q<s} p_q mod p_t) stays below 2^50 for L <= 192 primes below 2^21.
+template <typename R>
+__global__ void k_rns_crt(const R* __restrict__ RC, long planeC, int m, int n, int L, int WW,
+                          const uint32_t* __restrict__ primes, const uint32_t* __restrict__ inv,
+                          const uint32_t* __restrict__ pmod, const unsigned long long* __restrict__ Mbig,
+                          const unsigned long long* __restrict__ halfM, const int* __restrict__ loA,
+                          const int* __restrict__ loB, int N, int upper_only, unsigned char* __restrict__ C,
+                          uint32_t* __restrict__ status) {
   const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long)m * n) return;
   const int i = (int)(idx % m), j = (int)(idx / m);
@@ -236,7 +315,8 @@ extern "C" __global__ void k_rns_crt(const double* __restrict__ RC, long planeC,
     r %= (long long)p;
     if (r < 0) r += p;
     unsigned long long u = 0;
-    for (int s = 0; s < t; ++s) u = (u + (unsigned long long)v[s] * pmod[s * RNS_MAXL + t]) % p;
+    for (int s = 0; s < t; ++s) u += (unsigned long long)v[s] * pmod[s * RNS_MAXL + t];
+    u %= p;
     unsigned long long d = ((unsigned long long)r + p - u) % p;
     v[t] = (uint32_t)(d * inv[t] % p);
   }
@@ -325,26 +405,32 @@ extern "C" __global__ void k_rns_crt(const double* __restrict__ RC, long planeC,
 
 namespace {
 
-// Host tables of one prime set (largest primes below 2^21, descending).
+// Host tables of one prime set (descending primes below 2^bits).
 struct PrimeTables {
   int L = 0, WW = 0;
   std::vector<uint32_t> primes, W, inv, pmod;
   std::vector<unsigned long long> M, half;
 };
 
-const std::vector<uint32_t>& prime_list() {
-  static std::vector<uint32_t> ps;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    const uint32_t top = 1u << 21;
+// The largest RNS_MAXL primes below 2^bits, descending.
+const std::vector<uint32_t>& prime_list(int bits) {
+  static std::vector<uint32_t> ps21, ps15;
+  static std::once_flag once21, once15;
+  auto make = [](std::vector<uint32_t>& ps, int b) {
+    const uint32_t top = 1u << b;
     std::vector<bool> comp(top, false);
     for (uint32_t i = 2; (uint64_t)i * i < top; ++i)
       if (!comp[i])
         for (uint32_t j = i * i; j < top; j += i) comp[j] = true;
     for (uint32_t q = top - 1; q > 2 && ps.size() < RNS_MAXL; --q)
       if (!comp[q]) ps.push_back(q);
-  });
-  return ps;
+  };
+  if (bits == 15) {
+    std::call_once(once15, [&] { make(ps15, 15); });
+    return ps15;
+  }
+  std::call_once(once21, [&] { make(ps21, 21); });
+  return ps21;
 }
 
 uint64_t powmod64(uint64_t b, uint64_t e, uint64_t p) {
@@ -358,9 +444,8 @@ uint64_t powmod64(uint64_t b, uint64_t e, uint64_t p) {
   return r;
 }
 
-PrimeTables make_tables(int L) {
+PrimeTables make_tables(const std::vector<uint32_t>& ps, int L) {
   PrimeTables T;
-  const auto& ps = prime_list();
   T.L = L;
   T.primes.assign(ps.begin(), ps.begin() + L);
   T.W.assign((size_t)L * RNS_MAXN, 0);
@@ -399,22 +484,208 @@ PrimeTables make_tables(int L) {
   return T;
 }
 
-struct RnsWorkspace {
-  DevBuf<unsigned char> a, b, c;
-  DevBuf<int> loA, loB, bitsA, bitsB, maxbits;
-  DevBuf<uint32_t> status, primes, W, inv, pmod;
-  DevBuf<unsigned long long> M, half;
-  DevBuf<double> RA, RB, RC;
-  std::map<int, PrimeTables> tables;
-  int uploaded_L = -1;
-};
-
 template <typename T>
 void grow(DevBuf<T>& b, size_t n) {
   if (b.n < std::max<size_t>(n, 1)) b.alloc(std::max<size_t>(n, 1));
 }
 
+// Device copies of one prime set's tables (re-uploaded when L changes).
+struct DevTables {
+  DevBuf<uint32_t> primes, W, inv, pmod;
+  DevBuf<int> iprimes;
+  DevBuf<unsigned long long> M, half;
+  int L = -1;
+  std::map<int, PrimeTables> host;
+  const PrimeTables& get(int bits, int L_, cudaStream_t st) {
+    auto it = host.find(L_);
+    if (it == host.end()) it = host.emplace(L_, make_tables(prime_list(bits), L_)).first;
+    const PrimeTables& T = it->second;
+    if (L != L_) {
+      grow(primes, L_); grow(W, T.W.size()); grow(inv, L_); grow(pmod, T.pmod.size());
+      grow(iprimes, L_); grow(M, T.WW); grow(half, T.WW);
+      primes.upload(T.primes.data(), L_, st);
+      W.upload(T.W.data(), T.W.size(), st);
+      inv.upload(T.inv.data(), L_, st);
+      pmod.upload(T.pmod.data(), T.pmod.size(), st);
+      std::vector<int> ip(T.primes.begin(), T.primes.end());
+      iprimes.upload(ip.data(), L_, st);
+      M.upload(T.M.data(), T.WW, st);
+      half.upload(T.half.data(), T.WW, st);
+      L = L_;
+    }
+    return T;
+  }
+};
+
+struct RnsWorkspace {
+  DevBuf<unsigned char> a, b, c;  // staging of the host entry point
+  DevBuf<int> loA, loB, bitsA, bitsB, maxbits, err;
+  DevBuf<uint32_t> status, pow2;
+  DevTables t21, t15;
+  DevBuf<double> RA, RB, RC;  // FP64 form
+  DevBuf<int8_t> PA, PB;      // INT8 form: digit planes
+  DevBuf<int> RC8;            // INT8 form: residues of the product
+  int form = 0;               // 0: INT8 tensor cores, 1: FP64
+};
+
+constexpr int kI8Chunk = 1 << 16;  // K per modular GEMM call (INT32 accumulators stay exact)
+
+// The exact product on device buffers.  Returns 0, or 2 (non-finite operand, exponent spread
+// too wide) with g_last_error set; *hs receives the device status word.
+int32_t rns_product(RnsWorkspace& ws, cudaStream_t st, int form, int N, char ta, char tb, uint64_t m,
+                    uint64_t n, uint64_t k, const unsigned char* dA, uint64_t lda, const unsigned char* dB,
+                    uint64_t ldb, int upper_only, unsigned char* dC, uint32_t* hs_out) {
+  const size_t esz = 8 * (size_t)N + 8;
+  grow(ws.loA, m); grow(ws.bitsA, m); grow(ws.loB, n); grow(ws.bitsB, n);
+  grow(ws.maxbits, 2); grow(ws.status, 1); grow(ws.err, 1);
+  check(cudaMemsetAsync(ws.maxbits.p, 0, 2 * sizeof(int), st), "memset");
+  check(cudaMemsetAsync(ws.status.p, 0, sizeof(uint32_t), st), "memset");
+  // op(A) rows: (i, l) -> i*sx + l*sy ; op(B) columns: (j, l) -> j*sx + l*sy
+  const long asx = (ta == 'N') ? 1 : (long)lda, asy = (ta == 'N') ? (long)lda : 1;
+  const long bsx = (tb == 'N') ? (long)ldb : 1, bsy = (tb == 'N') ? 1 : (long)ldb;
+  if (k) {
+    ++g_launches, k_rns_scan<<<(unsigned)((m + 7) / 8), 256, 0, st>>>(dA, N, (int)m, (int)k, asx, asy, ws.loA,
+                                                                   ws.bitsA, ws.maxbits, ws.status);
+    ++g_launches, k_rns_scan<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(dB, N, (int)n, (int)k, bsx, bsy, ws.loB,
+                                                                   ws.bitsB, ws.maxbits.p + 1, ws.status);
+  } else {
+    check(cudaMemsetAsync(ws.loA.p, 0, m * sizeof(int), st), "memset");
+    check(cudaMemsetAsync(ws.loB.p, 0, n * sizeof(int), st), "memset");
+  }
+  int hb[2] = {0, 0};
+  uint32_t hs = 0;
+  copy_d2h(hb, ws.maxbits.p, 2 * sizeof(int), st);
+  copy_d2h(&hs, ws.status.p, sizeof(uint32_t), st);
+  check(cudaStreamSynchronize(st), "sync");
+  if (hs) {
+    if (hs_out) *hs_out = hs;
+    g_last_error = "sdpxg_rns_gemm: non-finite operands are not supported";
+    return 2;
+  }
+  // width of |sum| < k 2^(bitsA + bitsB); the CRT range must exceed twice that
+  int lg = 0;
+  while ((1ull << lg) < std::max<uint64_t>(k, 1)) ++lg;
+  const double needed = (double)hb[0] + hb[1] + lg + 2;
+  const int bits = form == 0 ? 15 : 21;
+  const auto& ps = prime_list(bits);
+  int L = 0;
+  double acc = 0;
+  while (L < RNS_MAXL && acc <= needed) acc += std::log2((double)ps[L++]);
+  if (acc <= needed || (int)(acc / 64) + 2 > RNS_MAXW) {
+    g_last_error = "sdpxg_rns_gemm: exponent spread too wide for the prime set";
+    return 2;
+  }
+  DevTables& DT = form == 0 ? ws.t15 : ws.t21;
+  const PrimeTables& T = DT.get(bits, L, st);
+  const long planeC = (long)(m * n);
+  if (form == 0) {
+    const int Mpad = (int)((m + 127) / 128 * 128), Npad = (int)((n + 127) / 128 * 128);
+    const int Kld = (int)((std::max<uint64_t>(k, 1) + 127) / 128 * 128);
+    grow(ws.RC8, (size_t)L * planeC);
+    if (k) {
+      const int S = 64 * N + std::max(hb[0], hb[1]) + 1;
+      grow(ws.pow2, (size_t)L * S);
+      ++g_launches, k_rns_pow2<<<dim3((S + 255) / 256, L), 256, 0, st>>>(L, DT.iprimes, S, ws.pow2);
+      grow(ws.PA, (size_t)L * 2 * Mpad * Kld);
+      grow(ws.PB, (size_t)L * 2 * Npad * Kld);
+      ++g_launches, k_rns8_residues<<<(unsigned)(((long)Mpad * Kld + 255) / 256), 256, 0, st>>>(
+          dA, N, (int)m, (int)k, asx, asy, ws.loA, L, DT.iprimes, ws.pow2, S, ws.PA, Mpad, Kld);
+      ++g_launches, k_rns8_residues<<<(unsigned)(((long)Npad * Kld + 255) / 256), 256, 0, st>>>(
+          dB, N, (int)n, (int)k, bsx, bsy, ws.loB, L, DT.iprimes, ws.pow2, S, ws.PB, Npad, Kld);
+      check(cudaMemsetAsync(ws.err.p, 0, sizeof(int), st), "memset");
+      for (int k0 = 0; k0 < Kld; k0 += kI8Chunk) {
+        I8GemmArgs ga;
+        ga.Mpad = Mpad; ga.Npad = Npad; ga.Kld = Kld;
+        ga.k0 = k0; ga.Kpad = std::min(kI8Chunk, Kld - k0);
+        ga.m = (int)m; ga.n = (int)n; ga.L = L; ga.moduli = DT.iprimes;
+        ga.upper_only = upper_only; ga.accumulate = k0 > 0; ga.out = ws.RC8.p; ga.plane = planeC;
+        ga.err = ws.err.p;
+        launch_i8_gemm(2, ws.PA, ws.PB, ga, st);
+      }
+    } else {
+      check(cudaMemsetAsync(ws.RC8.p, 0, (size_t)L * planeC * sizeof(int), st), "memset");
+    }
+    ++g_launches, k_rns_crt<int><<<(unsigned)((m * n + 127) / 128), 128, 0, st>>>(
+        ws.RC8, planeC, (int)m, (int)n, L, T.WW, DT.primes, DT.inv, DT.pmod, DT.M, DT.half, ws.loA, ws.loB, N,
+        upper_only ? 1 : 0, dC, ws.status);
+  } else {
+    const long planeA = (long)(m * std::max<uint64_t>(k, 1)), planeB = (long)(std::max<uint64_t>(k, 1) * n);
+    grow(ws.RA, (size_t)L * planeA);
+    grow(ws.RB, (size_t)L * planeB);
+    grow(ws.RC, (size_t)L * planeC);
+    if (k) {
+      ++g_launches, k_rns_residues<<<(unsigned)((m * k + 255) / 256), 256, 0, st>>>(
+          dA, N, (int)m, (int)k, asx, asy, ws.loA, L, DT.primes, DT.W, ws.RA, planeA, 1);
+      ++g_launches, k_rns_residues<<<(unsigned)((n * k + 255) / 256), 256, 0, st>>>(
+          dB, N, (int)n, (int)k, bsx, bsy, ws.loB, L, DT.primes, DT.W, ws.RB, planeB, 0);
+      dim3 grid((unsigned)((m + 63) / 64), (unsigned)((n + 63) / 64), (unsigned)L);
+      ++g_launches, k_rns_gemm<<<grid, 256, 0, st>>>(ws.RA, ws.RB, ws.RC, (int)m, (int)n, (int)k, DT.primes,
+                                                     planeA, planeB, planeC, upper_only ? 1 : 0);
+    } else {
+      check(cudaMemsetAsync(ws.RC.p, 0, (size_t)L * planeC * sizeof(double), st), "memset");
+    }
+    ++g_launches, k_rns_crt<double><<<(unsigned)((m * n + 127) / 128), 128, 0, st>>>(
+        ws.RC, planeC, (int)m, (int)n, L, T.WW, DT.primes, DT.inv, DT.pmod, DT.M, DT.half, ws.loA, ws.loB, N,
+        upper_only ? 1 : 0, dC, ws.status);
+  }
+  check(cudaGetLastError(), "rns launch");
+  int herr = 0;
+  copy_d2h(&hs, ws.status.p, sizeof(uint32_t), st);
+  if (form == 0 && k) copy_d2h(&herr, ws.err.p, sizeof(int), st);
+  check(cudaStreamSynchronize(st), "sync");
+  if (herr) throw CudaError("modular INT8 GEMM: a bounded wait gave up");
+  if (hs_out) *hs_out = hs;
+  return 0;
+}
+
+RnsWorkspace& workspace(sdpxg_ctx* ctx) {
+  auto slot = ctx_rns_slot(ctx);
+  if (!*slot) *slot = std::make_shared<RnsWorkspace>();
+  return *static_cast<RnsWorkspace*>(slot->get());
+}
+
+// Shared argument checks of both entry points; returns the element counts of A and B.
+void check_args(uint32_t limbs, char ta, char tb, uint64_t m, uint64_t n, uint64_t k, uint64_t lda, uint64_t ldb,
+                size_t* na, size_t* nb) {
+  if ((ta != 'N' && ta != 'T') || (tb != 'N' && tb != 'T')) throw std::invalid_argument("bad transpose flag");
+  if (m > (1u << 30) || n > (1u << 30) || k > (1u << 30)) throw std::invalid_argument("size overflow");
+  const uint64_t ar = (ta == 'N') ? m : k, ac = (ta == 'N') ? k : m;
+  const uint64_t br = (tb == 'N') ? k : n, bc = (tb == 'N') ? n : k;
+  if (lda < std::max<uint64_t>(ar, 1) || ldb < std::max<uint64_t>(br, 1))
+    throw std::invalid_argument("leading dimension too small");
+  *na = ac ? lda * (ac - 1) + ar : 0;
+  *nb = bc ? ldb * (bc - 1) + br : 0;
+  (void)limbs;
+}
+
+bool device_memory(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
 }  // namespace
+
+extern "C" int32_t sdpxg_rns_set_form(sdpxg_ctx* ctx, uint32_t form) {
+  try {
+    if (!ctx_engine_any(ctx)) throw std::invalid_argument("null context");
+    if (form > 1) throw std::invalid_argument("form must be 0 (INT8 tensor cores) or 1 (FP64)");
+    workspace(ctx).form = (int)form;
+    return 0;
+  } catch (const std::invalid_argument& e) {
+    g_last_error = e.what();
+    return 1;
+  } catch (const std::exception& e) {
+    g_last_error = std::string("internal error: ") + e.what();
+    return 5;
+  } catch (...) {
+    g_last_error = "internal error";
+    return 5;
+  }
+}
 
 extern "C" int32_t sdpxg_rns_gemm(sdpxg_ctx* ctx, uint32_t limbs, char ta, char tb, uint64_t m,
                                   uint64_t n, uint64_t k, const void* A, uint64_t lda,
@@ -428,19 +699,12 @@ extern "C" int32_t sdpxg_rns_gemm(sdpxg_ctx* ctx, uint32_t limbs, char ta, char 
       g_last_error = "sdpxg_rns_gemm: limbs must be in 1..16";
       return 2;
     }
-    if ((ta != 'N' && ta != 'T') || (tb != 'N' && tb != 'T')) throw std::invalid_argument("bad transpose flag");
+    size_t na = 0, nb = 0;
+    check_args(limbs, ta, tb, m, n, k, lda, ldb, &na, &nb);
     if (m == 0 || n == 0) return 0;
     if (!A || !B || !C) throw std::invalid_argument("null pointer");
-    if (m > (1u << 30) || n > (1u << 30) || k > (1u << 30)) throw std::invalid_argument("size overflow");
-    const uint64_t ar = (ta == 'N') ? m : k, ac = (ta == 'N') ? k : m;
-    const uint64_t br = (tb == 'N') ? k : n, bc = (tb == 'N') ? n : k;
-    if (lda < std::max<uint64_t>(ar, 1) || ldb < std::max<uint64_t>(br, 1))
-      throw std::invalid_argument("leading dimension too small");
     const size_t esz = 8 * (size_t)N + 8;
-    const size_t na = ac ? lda * (ac - 1) + ar : 0, nb = bc ? ldb * (bc - 1) + br : 0;
-    auto slot = ctx_rns_slot(ctx);
-    if (!*slot) *slot = std::make_shared<RnsWorkspace>();
-    RnsWorkspace& ws = *static_cast<RnsWorkspace*>(slot->get());
+    RnsWorkspace& ws = workspace(ctx);
     cudaStream_t st = E->st;
     check(cudaSetDevice(E->device), "cudaSetDevice");
     grow(ws.a, na * esz);
@@ -448,91 +712,60 @@ extern "C" int32_t sdpxg_rns_gemm(sdpxg_ctx* ctx, uint32_t limbs, char ta, char 
     grow(ws.c, m * n * esz);
     if (na) ws.a.upload(static_cast<const unsigned char*>(A), na * esz, st);
     if (nb) ws.b.upload(static_cast<const unsigned char*>(B), nb * esz, st);
-    grow(ws.loA, m); grow(ws.bitsA, m); grow(ws.loB, n); grow(ws.bitsB, n);
-    grow(ws.maxbits, 2); grow(ws.status, 1);
-    check(cudaMemsetAsync(ws.maxbits.p, 0, 2 * sizeof(int), st), "memset");
-    check(cudaMemsetAsync(ws.status.p, 0, sizeof(uint32_t), st), "memset");
-    // op(A) rows: (i, l) -> i*sx + l*sy ; op(B) columns: (j, l) -> j*sx + l*sy
-    const long asx = (ta == 'N') ? 1 : (long)lda, asy = (ta == 'N') ? (long)lda : 1;
-    const long bsx = (tb == 'N') ? (long)ldb : 1, bsy = (tb == 'N') ? 1 : (long)ldb;
-    if (k) {
-      ++g_launches, k_rns_scan<<<(unsigned)((m + 7) / 8), 256, 0, st>>>(ws.a, N, (int)m, (int)k, asx, asy,
-                                                                     ws.loA, ws.bitsA, ws.maxbits,
-                                                                     ws.status);
-      ++g_launches, k_rns_scan<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(ws.b, N, (int)n, (int)k, bsx, bsy,
-                                                                     ws.loB, ws.bitsB, ws.maxbits.p + 1,
-                                                                     ws.status);
-    } else {
-      check(cudaMemsetAsync(ws.loA.p, 0, m * sizeof(int), st), "memset");
-      check(cudaMemsetAsync(ws.loB.p, 0, n * sizeof(int), st), "memset");
-    }
-    int hb[2] = {0, 0};
     uint32_t hs = 0;
-    check(cudaMemcpyAsync(hb, ws.maxbits.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
-    check(cudaMemcpyAsync(&hs, ws.status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "D2H");
-    check(cudaStreamSynchronize(st), "sync");
-    if (hs) {
-      if (status) *status = hs;
-      g_last_error = "sdpxg_rns_gemm: non-finite operands are not supported";
-      return 2;
-    }
-    // width of |sum| < k 2^(bitsA + bitsB); the CRT range must exceed twice that
-    int lg = 0;
-    while ((1ull << lg) < std::max<uint64_t>(k, 1)) ++lg;
-    const double needed = (double)hb[0] + hb[1] + lg + 2;
-    const auto& ps = prime_list();
-    int L = 0;
-    double acc = 0;
-    while (L < RNS_MAXL && acc <= needed) acc += std::log2((double)ps[L++]);
-    if (acc <= needed || (int)(acc / 64) + 2 > RNS_MAXW) {
-      g_last_error = "sdpxg_rns_gemm: exponent spread too wide for the prime set";
-      return 2;
-    }
-    auto it = ws.tables.find(L);
-    if (it == ws.tables.end()) it = ws.tables.emplace(L, make_tables(L)).first;
-    const PrimeTables& T = it->second;
-    if (ws.uploaded_L != L) {
-      grow(ws.primes, L); grow(ws.W, T.W.size()); grow(ws.inv, L); grow(ws.pmod, T.pmod.size());
-      grow(ws.M, T.WW); grow(ws.half, T.WW);
-      ws.primes.upload(T.primes.data(), L, st);
-      ws.W.upload(T.W.data(), T.W.size(), st);
-      ws.inv.upload(T.inv.data(), L, st);
-      ws.pmod.upload(T.pmod.data(), T.pmod.size(), st);
-      ws.M.upload(T.M.data(), T.WW, st);
-      ws.half.upload(T.half.data(), T.WW, st);
-      ws.uploaded_L = L;
-    }
-    const long planeA = (long)(m * std::max<uint64_t>(k, 1)), planeB = (long)(std::max<uint64_t>(k, 1) * n);
-    const long planeC = (long)(m * n);
-    grow(ws.RA, (size_t)L * planeA);
-    grow(ws.RB, (size_t)L * planeB);
-    grow(ws.RC, (size_t)L * planeC);
-    if (k) {
-      ++g_launches, k_rns_residues<<<(unsigned)((m * k + 255) / 256), 256, 0, st>>>(
-          ws.a, N, (int)m, (int)k, asx, asy, ws.loA, L, ws.primes, ws.W, ws.RA, planeA, 1);
-      ++g_launches, k_rns_residues<<<(unsigned)((n * k + 255) / 256), 256, 0, st>>>(
-          ws.b, N, (int)n, (int)k, bsx, bsy, ws.loB, L, ws.primes, ws.W, ws.RB, planeB, 0);
-      dim3 grid((unsigned)((m + 63) / 64), (unsigned)((n + 63) / 64), (unsigned)L);
-      ++g_launches, k_rns_gemm<<<grid, 256, 0, st>>>(ws.RA, ws.RB, ws.RC, (int)m, (int)n, (int)k,
-                                                     ws.primes, planeA, planeB, planeC,
-                                                     upper_only ? 1 : 0);
-    } else {
-      check(cudaMemsetAsync(ws.RC.p, 0, (size_t)L * planeC * sizeof(double), st), "memset");
-    }
-    ++g_launches, k_rns_crt<<<(unsigned)((m * n + 127) / 128), 128, 0, st>>>(
-        ws.RC, planeC, (int)m, (int)n, L, T.WW, ws.primes, ws.inv, ws.pmod, ws.M, ws.half, ws.loA,
-        ws.loB, N, upper_only ? 1 : 0, ws.c, ws.status);
-    check(cudaGetLastError(), "rns launch");
-    check(cudaMemcpyAsync(C, ws.c.p, m * n * esz, cudaMemcpyDeviceToHost, st), "D2H");
-    check(cudaMemcpyAsync(&hs, ws.status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "D2H");
-    check(cudaStreamSynchronize(st), "sync");
+    const int32_t rc = rns_product(ws, st, ws.form, N, ta, tb, m, n, k, ws.a, lda, ws.b, ldb, upper_only ? 1 : 0,
+                                   ws.c, &hs);
     if (status) *status = hs;
+    if (rc) return rc;
+    copy_d2h(C, ws.c.p, m * n * esz, st);
+    check(cudaStreamSynchronize(st), "sync");
     return 0;
   } catch (const std::invalid_argument& e) {
     g_last_error = e.what();
     return 1;
   } catch (const std::exception& e) {
     g_last_error = std::string("internal error: ") + e.what();
+    return 5;
+  } catch (...) {
+    g_last_error = "internal error";
+    return 5;
+  }
+}
+
+extern "C" int32_t sdpxg_rns_gemm_device(sdpxg_ctx* ctx, uint32_t limbs, char ta, char tb, uint64_t m,
+                                         uint64_t n, uint64_t k, const void* d_A, uint64_t lda,
+                                         const void* d_B, uint64_t ldb, uint32_t upper_only, void* d_C,
+                                         uint32_t* status) {
+  try {
+    Engine* E = ctx_engine_any(ctx);
+    if (!E) throw std::invalid_argument("null context");
+    const int N = (int)limbs;
+    if (N < 1 || N > RNS_MAXN) {
+      g_last_error = "sdpxg_rns_gemm_device: limbs must be in 1..16";
+      return 2;
+    }
+    size_t na = 0, nb = 0;
+    check_args(limbs, ta, tb, m, n, k, lda, ldb, &na, &nb);
+    if (m == 0 || n == 0) return 0;
+    if (!d_A || !d_B || !d_C) throw std::invalid_argument("null pointer");
+    check(cudaSetDevice(E->device), "cudaSetDevice");
+    if ((na && !device_memory(d_A)) || (nb && !device_memory(d_B)) || !device_memory(d_C))
+      throw std::invalid_argument("sdpxg_rns_gemm_device: A, B and C must be device pointers");
+    RnsWorkspace& ws = workspace(ctx);
+    uint32_t hs = 0;
+    const int32_t rc = rns_product(ws, E->st, ws.form, N, ta, tb, m, n, k, static_cast<const unsigned char*>(d_A),
+                                   lda, static_cast<const unsigned char*>(d_B), ldb, upper_only ? 1 : 0,
+                                   static_cast<unsigned char*>(d_C), &hs);
+    if (status) *status = hs;
+    return rc;
+  } catch (const std::invalid_argument& e) {
+    g_last_error = e.what();
+    return 1;
+  } catch (const std::exception& e) {
+    g_last_error = std::string("internal error: ") + e.what();
+    return 5;
+  } catch (...) {
+    g_last_error = "internal error";
     return 5;
   }
 }

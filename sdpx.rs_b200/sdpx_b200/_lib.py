@@ -82,15 +82,22 @@ SIGNATURES = {
     "sdpx_b200_schur_forms": (i32, [C.c_void_p, PU32, PU32]),
     "sdpx_b200_kkt_paths": (i32, [C.c_void_p, PU64, PU64]),
     "sdpx_b200_set_graphs": (i32, [C.c_void_p, i32]),
+    "sdpx_b200_set_form": (i32, [C.c_void_p, u32]),
     "sdpx_b200_adjoint": (i32, [C.c_void_p, PD, PD, PD, PD, PD, PD, u64]),
     "sdpxg_ctx_create": (i32, [i32, u32, C.POINTER(C.c_void_p)]),
     "sdpxg_ctx_destroy": (i32, [C.c_void_p]),
     "sdpxg_problem_upload": (i32, [C.c_void_p, C.POINTER(Csc), C.POINTER(Csc), PU64, u64]),
     "sdpxg_nt_scale": (i32, [C.c_void_p, PD, PD, PD, PU32]),
     "sdpxg_identity_scaling": (i32, [C.c_void_p]),
+    "sdpxg_problem_upload_sampled": (i32, [C.c_void_p, C.POINTER(Csc), C.POINTER(Csc), PU64, u64,
+                                           C.POINTER(SampledBlock), u64]),
+    "sdpxg_set_scaling": (i32, [C.c_void_p, PD, PD]),
     "sdpxg_schur_assemble": (i32, [C.c_void_p, PD]),
     "sdpxg_factor": (i32, [C.c_void_p, f64, u32, f64, f64, PU32]),
     "sdpxg_solve_many": (i32, [C.c_void_p, PD, PD, u32]),
+    "sdpxg_set_factor_form": (i32, [C.c_void_p, u32]),
+    "sdpxg_split_dgemm_device": (i32, [C.c_void_p, C.c_char, C.c_char, u64, u64, u64, f64, C.c_void_p,
+                                       u64, C.c_void_p, u64, f64, C.c_void_p, u64, PU32]),
     "sdpxg_solve_noalloc": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u32]),
     "sdpxg_kkt_solve": (i32, [C.c_void_p, PD, PD, PD, PD]),
     "sdpxg_residual": (i32, [C.c_void_p, PD, PD, PD, PD, PD, PD, PD]),
@@ -98,6 +105,9 @@ SIGNATURES = {
     "sdpxg_cone_apply": (i32, [C.c_void_p, u32, PD, PD]),
     "sdpxg_rns_gemm": (i32, [C.c_void_p, u32, C.c_char, C.c_char, u64, u64, u64, C.c_void_p, u64,
                              C.c_void_p, u64, u32, C.c_void_p, PU32]),
+    "sdpxg_rns_gemm_device": (i32, [C.c_void_p, u32, C.c_char, C.c_char, u64, u64, u64, C.c_void_p,
+                                    u64, C.c_void_p, u64, u32, C.c_void_p, PU32]),
+    "sdpxg_rns_set_form": (i32, [C.c_void_p, u32]),
 }
 
 _lib = None

@@ -160,6 +160,33 @@ class DefaultSolver:
         self._prepare(CProblem(P, q, A, b, cones, settings))
 
     @classmethod
+    def new_sampled(cls, P, q, A_linear, b, cones: Sequence[Tuple[str, int]],
+                    blocks: Sequence[dict], settings: Optional[DefaultSettings] = None) -> "DefaultSolver":
+        """sdpx_prepare_sampled: factor-authoritative sampled PSD blocks (the reference's
+        DefaultSolver::new_sampled).  Each block is a dict with row_start, column_start, dim,
+        basis (basis_rows x basis_cols array) and weights (tri(dim) * basis_cols values)."""
+        self = cls.__new__(cls)
+        cp = CProblem(P, q, A_linear, b, cones, settings)
+        self._hold(cp)
+        arr = (_lib.SampledBlock * max(len(blocks), 1))()
+        keep = []
+        for i, blk in enumerate(blocks):
+            Q = np.asfortranarray(blk["basis"], dtype=np.float64)
+            w = np.ascontiguousarray(blk["weights"], dtype=np.float64)
+            qv = Q.ravel(order="F").copy()
+            keep += [qv, w]
+            arr[i].row_start, arr[i].column_start = int(blk["row_start"]), int(blk["column_start"])
+            arr[i].dim, arr[i].basis_rows, arr[i].basis_cols = int(blk.get("dim", 1)), Q.shape[0], Q.shape[1]
+            arr[i].basis, arr[i].weights = _scalars(qv), _scalars(w)
+        self._sampled_keep = (arr, keep)
+        h = C.c_void_p()
+        _lib.call("sdpx_prepare_sampled", *cp.args, arr, len(blocks), C.byref(h))
+        self._h = h
+        self.solution = None
+        self.info = None
+        return self
+
+    @classmethod
     def from_c_problem(cls, cp: CProblem) -> "DefaultSolver":
         """sdpx_prepare on a problem already in the C ABI's host layout."""
         self = cls.__new__(cls)
@@ -264,6 +291,13 @@ class DefaultSolver:
     def set_graphs(self, on: bool):
         """Replay the KKT solve's captured CUDA graphs (default) or launch eagerly."""
         _lib.call("sdpx_b200_set_graphs", self._h, int(bool(on)))
+
+    FORM_PLAIN, FORM_SPLIT = 0, 1
+
+    def set_form(self, form: int):
+        """Factorisation form of later solves: FORM_PLAIN (FP64) or FORM_SPLIT (split-precision
+        INT8 tensor-core products for the large blocks, FP64 diagonal blocks and refinement)."""
+        _lib.call("sdpx_b200_set_form", self._h, int(form))
 
     def kkt_paths(self) -> dict:
         """KKT solves of the last solve refined on the device (one graph each) and from the host."""
@@ -384,6 +418,33 @@ class KernelContext:
         self.m, self.n = A.shape
         self.nlam = int(orders.sum())
 
+    def upload_sampled(self, A_linear, psd_orders: Sequence[int], blocks: Sequence[dict], P=None):
+        """sdpxg_problem_upload_sampled: blocks as in DefaultSolver.new_sampled (dim 1)."""
+        A_linear = sp.csc_matrix(A_linear, dtype=np.float64)
+        self._A = _CscHold(A_linear)
+        self._P = _CscHold(sp.triu(sp.csc_matrix(P)).tocsc()) if P is not None else None
+        orders = np.ascontiguousarray(psd_orders, dtype=np.uint64)
+        arr = (_lib.SampledBlock * max(len(blocks), 1))()
+        keep = []
+        for i, blk in enumerate(blocks):
+            Q = np.asfortranarray(blk["basis"], dtype=np.float64)
+            w = np.ascontiguousarray(blk["weights"], dtype=np.float64)
+            qv = Q.ravel(order="F").copy()
+            keep += [qv, w]
+            arr[i].row_start, arr[i].column_start = int(blk["row_start"]), int(blk["column_start"])
+            arr[i].dim, arr[i].basis_rows, arr[i].basis_cols = int(blk.get("dim", 1)), Q.shape[0], Q.shape[1]
+            arr[i].basis, arr[i].weights = _scalars(qv), _scalars(w)
+        _lib.call("sdpxg_problem_upload_sampled", self._h, C.byref(self._P.c) if self._P else None,
+                  C.byref(self._A.c), orders.ctypes.data_as(_lib.PU64), orders.size, arr, len(blocks))
+        self.m, self.n = A_linear.shape
+        self.nlam = int(orders.sum())
+
+    def set_scaling(self, R_blocks, Rinv_blocks):
+        """sdpxg_set_scaling: per PSD block R and R^-1 (lists of square arrays, cone order)."""
+        R = np.concatenate([np.asfortranarray(r, dtype=np.float64).ravel(order="F") for r in R_blocks])
+        Ri = np.concatenate([np.asfortranarray(r, dtype=np.float64).ravel(order="F") for r in Rinv_blocks])
+        _lib.call("sdpxg_set_scaling", self._h, dptr(R), dptr(Ri))
+
     def nt_scale(self, s, z):
         s = np.ascontiguousarray(s, dtype=np.float64)
         z = np.ascontiguousarray(z, dtype=np.float64)
@@ -435,15 +496,45 @@ class KernelContext:
                   C.byref(a), C.byref(st))
         return a.value, st.value
 
+    RNS_INT8, RNS_FP64 = 0, 1
+
+    def set_factor_form(self, form: int):
+        """sdpxg_factor form: 0 plain FP64, 1 split precision (see DefaultSolver.set_form)."""
+        _lib.call("sdpxg_set_factor_form", self._h, int(form))
+
+    def split_dgemm_device(self, ta: str, tb: str, m: int, n: int, k: int, alpha: float, d_A: int,
+                           lda: int, d_B: int, ldb: int, beta: float, d_C: int, ldc: int) -> int:
+        """Split-precision (INT8 tensor-core) C = alpha op(A) op(B) + beta C on device buffers."""
+        st = C.c_uint32()
+        _lib.call("sdpxg_split_dgemm_device", self._h, ta.encode(), tb.encode(), m, n, k,
+                  float(alpha), C.c_void_p(d_A), lda, C.c_void_p(d_B), ldb, float(beta),
+                  C.c_void_p(d_C), ldc, C.byref(st))
+        return st.value
+
+    def set_rns_form(self, form: int):
+        """Residue products on INT8 tensor cores (RNS_INT8, the default) or in FP64 (RNS_FP64)."""
+        _lib.call("sdpxg_rns_set_form", self._h, int(form))
+
     def rns_gemm(self, limbs: int, ta: str, tb: str, m: int, n: int, k: int, A: bytes, lda: int,
-                 B: bytes, ldb: int, upper_only: bool = False):
+                 B: bytes, ldb: int, upper_only: bool = False, form: Optional[int] = None):
         """Exact MpFloat<limbs> product (raw element bytes in, raw bytes out)."""
+        if form is not None:
+            self.set_rns_form(form)
         esz = 8 * limbs + 8
         out = C.create_string_buffer(max(m * n * esz, 1))
         st = C.c_uint32()
         _lib.call("sdpxg_rns_gemm", self._h, limbs, ta.encode(), tb.encode(), m, n, k,
                   C.c_char_p(A), lda, C.c_char_p(B), ldb, int(upper_only), out, C.byref(st))
         return out.raw[:m * n * esz], st.value
+
+    def rns_gemm_device(self, limbs: int, ta: str, tb: str, m: int, n: int, k: int, d_A: int,
+                        lda: int, d_B: int, ldb: int, d_C: int, upper_only: bool = False):
+        """Exact product on device buffers (addresses of MpFloat arrays in device memory)."""
+        st = C.c_uint32()
+        _lib.call("sdpxg_rns_gemm_device", self._h, limbs, ta.encode(), tb.encode(), m, n, k,
+                  C.c_void_p(d_A), lda, C.c_void_p(d_B), ldb, int(upper_only), C.c_void_p(d_C),
+                  C.byref(st))
+        return st.value
 
     def cone_apply(self, op, x):
         x = np.ascontiguousarray(x, dtype=np.float64)

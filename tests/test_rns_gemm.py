@@ -3,8 +3,10 @@
 CPU part: the oracle's rounding is checked against mpmath (ties to even at 64N bits).
 GPU part: sdpxg_rns_gemm must be bitwise equal to the exact dot product rounded once, on the
 reference's own test inputs -- its LCG generator, shapes, precisions and exponent spreads
-(crates/solver/src/algebra/dense/blas/rns_blas_tests.rs:4-28, 62-144), all four transposes, and
-the upper-only variant.
+(crates/solver/src/algebra/dense/blas/rns_blas_tests.rs:4-28, 62-144, 225-229), all four
+transposes, and the upper-only variant -- in both residue forms: INT8 tensor cores (primes below
+2^15 as two signed-byte digits, tcgen05.mma kind::i8) and FP64 (primes below 2^21).  The
+device-pointer entry point gives the same bits as the host one.
 """
 from fractions import Fraction
 
@@ -57,11 +59,16 @@ REFERENCE_CASES = [(12, 7, 5, 45, 90, 1), (12, 20, 20, 20, 3, 2), (8, 3, 4, 1, 4
                    (4, 9, 6, 300, 60, 4), (2, 5, 5, 33, 10, 5), (16, 35, 37, 45, 90, 7)]
 
 
+FORMS = [0, 1]  # INT8 tensor cores, FP64
+
+
 @pytest.mark.gpu
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("n,m,ncols,k,spread,seed", REFERENCE_CASES)
-def test_rns_gemm_bitwise_reference_cases(n, m, ncols, k, spread, seed):
+def test_rns_gemm_bitwise_reference_cases(n, m, ncols, k, spread, seed, form):
     from sdpx_b200.solver import KernelContext
     ctx = KernelContext()
+    ctx.set_rns_form(form)
     for ta, tb, A, ar, B, br in _case(n, m, ncols, k, spread, seed):
         expect = X.gemm(n, ta, tb, m, ncols, k, A, ar, B, br)
         raw, st = ctx.rns_gemm(n, ta, tb, m, ncols, k, X.pack_array(A), ar, X.pack_array(B), br)
@@ -79,22 +86,46 @@ def test_rns_gemm_bitwise_reference_cases(n, m, ncols, k, spread, seed):
 
 
 @pytest.mark.gpu
-def test_rns_gemm_long_inner_dimension():
-    """k = 70000 (rns_blas_tests.rs:225-229): several exact FP64 chunks per prime."""
+@pytest.mark.parametrize("form", FORMS)
+def test_rns_gemm_long_inner_dimension(form):
+    """check::<4>(2, 3, 70_000, 4, 6) (rns_blas_tests.rs:225-229), all four transposes: the INT8
+    form splits K into two tensor-core passes (2^16 per pass), the FP64 form reduces every 8192
+    terms."""
     from sdpx_b200.solver import KernelContext
-    n, m, ncols, k = 4, 2, 2, 70000
-    rng = X.Lcg(21)
-    A = X.random_values(n, rng, m * k, 4)
-    B = X.random_values(n, rng, k * ncols, 4)
-    expect = X.gemm(n, "N", "N", m, ncols, k, A, m, B, k)
-    raw, st = KernelContext().rns_gemm(n, "N", "N", m, ncols, k, X.pack_array(A), m,
-                                       X.pack_array(B), k)
-    assert st == 0
-    assert all(g == e for g, e in zip(X.unpack_array(n, raw), expect))
+    n, m, ncols, k = 4, 2, 3, 70000
+    ctx = KernelContext()
+    ctx.set_rns_form(form)
+    for ta, tb, A, ar, B, br in _case(n, m, ncols, k, 4, 6):
+        expect = X.gemm(n, ta, tb, m, ncols, k, A, ar, B, br)
+        raw, st = ctx.rns_gemm(n, ta, tb, m, ncols, k, X.pack_array(A), ar, X.pack_array(B), br)
+        assert st == 0
+        assert all(g == e for g, e in zip(X.unpack_array(n, raw), expect)), (ta, tb)
 
 
 @pytest.mark.gpu
-def test_rns_gemm_cancellation_and_zero():
+def test_rns_gemm_device_entry_matches_host_entry():
+    """sdpxg_rns_gemm_device on device-resident MpFloat arrays gives the host entry's bits."""
+    import numpy as np
+    import torch
+    from sdpx_b200.solver import KernelContext
+    n, m, ncols, k = 4, 35, 37, 45
+    (ta, tb, A, ar, B, br), = _case(n, m, ncols, k, 90, 7)[:1]
+    ctx = KernelContext()
+    host, st = ctx.rns_gemm(n, ta, tb, m, ncols, k, X.pack_array(A), ar, X.pack_array(B), br)
+    esz = 8 * n + 8
+    dA = torch.from_numpy(np.frombuffer(X.pack_array(A), dtype=np.uint8).copy()).cuda()
+    dB = torch.from_numpy(np.frombuffer(X.pack_array(B), dtype=np.uint8).copy()).cuda()
+    dC = torch.zeros(m * ncols * esz, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    st2 = ctx.rns_gemm_device(n, ta, tb, m, ncols, k, dA.data_ptr(), ar, dB.data_ptr(), br,
+                              dC.data_ptr())
+    assert st == st2 == 0
+    assert dC.cpu().numpy().tobytes() == host
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", FORMS)
+def test_rns_gemm_cancellation_and_zero(form):
     """Exact cancellation gives zero; a tiny remainder survives the cancellation exactly."""
     from sdpx_b200.solver import KernelContext
     n = 4
@@ -105,6 +136,7 @@ def test_rns_gemm_cancellation_and_zero():
     A = [big, nbig, tiny]  # 1 x 3
     B = [one, one, one]  # 3 x 1
     ctx = KernelContext()
+    ctx.set_rns_form(form)
     raw, st = ctx.rns_gemm(n, "N", "N", 1, 1, 3, X.pack_array(A), 1, X.pack_array(B), 3)
     got = X.unpack_array(n, raw)[0]
     assert got == tiny
