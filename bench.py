@@ -4,13 +4,21 @@
 Workload: the bootstrap-shaped Float64 SDP -- 32 PSD blocks of order U{10..60} with Chebyshev
 bases, m = 2000 constraints of four rank-one terms each, seed 0 -- solved to the reference's
 default gap 1e-8 with the condensed KKT form.  One "step" is one complete solve to the gap.
+Both factorisation forms solve it in the same process: the plain FP64 form and the
+split-precision form (INT8 tensor-core Ozaki-II products for the large blocks of the Schur
+factorisation and its inverse, FP64 diagonal blocks, pivots and refinement).
 
-  value     time-to-gap (s) with the problem already resident in HBM (sdpx_solve), max over ranks
+  value     time-to-gap (s) of the split-precision form with the problem already resident in HBM
+            (sdpx_solve), max over ranks; `forms` gives both forms and plain / split
+  precision_f64  the same comparison on the 64-block m = 4000 workload at Float64
+  rns_256   exact 256-bit products (2000^3) in both residue forms (INT8 tensor cores, FP64)
   e2e       the same metric through the C ABI with host buffers in the ABI's layout (built before
             the timed region, as a C caller holds them): sdpx_prepare (copy and validation, Ruiz
             equilibration, operator packing, H2D upload) + sdpx_solve + sdpx_result_f64 (D2H) +
             sdpx_destroy
-  roofline  the dominant device phase, timed with CUDA events on the library's stream
+  roofline  the dominant device phase of the split form, timed with CUDA events on the library's
+            stream; int8_gemm: the INT8 tensor-core GEMM's achieved TOP/s against an INT8 GEMM peak
+            measured in the same run
   cpu_baseline  the oracle (reference-algorithm CPU restatement, numpy/OpenBLAS, all host cores)
             solving the same instance to the gap once (measured, not projected)
 
@@ -35,7 +43,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "sdpx.rs_b200"))
 
-METRIC = "time-to-gap 1e-8 (Float64, plain GPU form)"
+METRIC = ("time-to-gap 1e-8 (Float64): split-precision form (INT8 tensor-core Ozaki-II products, "
+          "FP64 pivots and refinement) vs the plain FP64 GPU form")
 WORKLOAD = {"workload": "rank1_sdp: 32 PSD blocks n_j~U{10..60}, Chebyshev bases s_j=2n_j, "
                         "m=2000 constraints x 4 rank-one terms, seed 0, gap 1e-8, kkt_form condensed",
             "blocks": 32, "m": 2000, "seed": 0, "precision_bits": 53,
@@ -261,49 +270,183 @@ def run_reference(args, world, rank):
     return 0
 
 
+def time_solves(solver, steps):
+    """Device-clock seconds per solve (CUDA events around `steps` solves; every solve returns
+    to the host with its result, so the events bracket complete solves), wall seconds per solve
+    and kernel launches."""
+    import torch
+    from sdpx_b200 import _lib
+    lib = _lib.load()
+    launches0 = lib.sdpx_b200_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        solver.solve()
+    ev1.record()
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / steps
+    return ev0.elapsed_time(ev1) / 1e3 / steps, wall, lib.sdpx_b200_launch_count() - launches0
+
+
+def int8_peak():
+    """cuBLASLt INT8 GEMM throughput (torch._int_mm, 8192^3): the INT8 roofline denominator
+    (INT8 is not in MEASURED_PEAKS.json)."""
+    import torch
+    n = 8192
+    a = torch.randint(-128, 127, (n, n), dtype=torch.int8, device="cuda")
+    b = torch.randint(-128, 127, (n, n), dtype=torch.int8, device="cuda")
+    for _ in range(2):
+        torch._int_mm(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(4):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch._int_mm(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def i8_measure(fn):
+    """Run fn with the INT8 GEMM launches timed: (ms, executed ops, algorithmic ops, launches)."""
+    from sdpx_b200 import _lib
+    lib = _lib.load()
+    lib.sdpx_b200_set_i8_timing(1)
+    fn()
+    ms, ops, alg = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    cnt = ctypes.c_uint64()
+    lib.sdpx_b200_i8_times(ctypes.byref(ms), ctypes.byref(ops), ctypes.byref(alg), ctypes.byref(cnt))
+    lib.sdpx_b200_set_i8_timing(0)
+    return ms.value, ops.value, alg.value, cnt.value
+
+
+def precision_f64(args):
+    """The precision workload at Float64 (64 blocks, m = 4000): both forms to the gap."""
+    from sdpx_b200 import problems
+    from sdpx_b200.solver import DefaultSettings, DefaultSolver
+    prob = problems.rank1_sdp(64, 4000, seed=0)
+    out = {"workload": "rank1_sdp: 64 PSD blocks n_j~U{10..60}, m=4000, seed 0, gap 1e-8, Float64"}
+    for name, form in (("plain", 0), ("split", 1)):
+        s = DefaultSolver(prob.P, prob.q, prob.A, prob.b, prob.cones, DefaultSettings(kkt_form="condensed"))
+        s.set_form(form)
+        s.solve()
+        dev, wall, _ = time_solves(s, max(2, args.steps // 2))
+        out[name] = {"s": dev, "status": s.solution.status, "iterations": s.solution.iterations,
+                     "objective": s.solution.obj_val}
+        s.close()
+    out["plain_over_split"] = out["plain"]["s"] / out["split"]["s"]
+    return out
+
+
+def _random_mp(count, limbs, rng, spread=4):
+    """Random MpFloat<limbs> values in the reference's layout (top mantissa bit set, sign in the
+    kind, exponents in [-spread, spread], 5 % zeros) as raw bytes."""
+    import numpy as np
+    dt = np.dtype([("l", "<u8", (limbs,)), ("kind", "<i4"), ("exp", "<i4")])
+    a = np.zeros(count, dtype=dt)
+    a["l"] = rng.integers(0, 2 ** 63, size=(count, limbs), dtype=np.uint64) * np.uint64(2) + np.uint64(1)
+    a["l"][:, limbs - 1] |= np.uint64(1) << np.uint64(63)
+    a["kind"] = np.where(rng.random(count) < 0.5, 3, -3)
+    a["exp"] = rng.integers(-spread, spread + 1, size=count)
+    zero = rng.random(count) < 0.05
+    a["l"][zero] = 0
+    a["kind"][zero] = 2
+    a["exp"][zero] = 0
+    return a.tobytes()
+
+
+def rns_256(args, peak_i8):
+    """Exact 256-bit products (MpFloat<4>) of 2000 x 2000 matrices, both residue forms, on device
+    buffers: the trailing-update shape of the precision workload's factorisation."""
+    import numpy as np
+    import torch
+    from sdpx_b200.solver import KernelContext
+    n, limbs = 2000, 4
+    rng = np.random.default_rng(7)
+    esz = 8 * limbs + 8
+    dA = torch.from_numpy(np.frombuffer(_random_mp(n * n, limbs, rng), dtype=np.uint8).copy()).cuda()
+    dB = torch.from_numpy(np.frombuffer(_random_mp(n * n, limbs, rng), dtype=np.uint8).copy()).cuda()
+    outs, res = {}, {"shape": f"{n} x {n} x {n}, 256-bit (MpFloat<4>), exponent spread 4, device buffers"}
+    ctx = KernelContext()
+    for name, form in (("int8", 0), ("fp64", 1)):
+        ctx.set_rns_form(form)
+        dC = torch.zeros(n * n * esz, dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        ctx.rns_gemm_device(limbs, "N", "N", n, n, n, dA.data_ptr(), n, dB.data_ptr(), n, dC.data_ptr())
+        reps = 2
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            ctx.rns_gemm_device(limbs, "N", "N", n, n, n, dA.data_ptr(), n, dB.data_ptr(), n, dC.data_ptr())
+        dt = (time.perf_counter() - t0) / reps
+        res[name] = {"s": dt, "exact_macs_per_s": n ** 3 / dt}
+        if form == 0:
+            ms, ops, alg, cnt = i8_measure(lambda: ctx.rns_gemm_device(
+                limbs, "N", "N", n, n, n, dA.data_ptr(), n, dB.data_ptr(), n, dC.data_ptr()))
+            res[name]["i8_gemm"] = {"ms": ms, "launches": cnt, "tops_executed": ops / ms / 1e9,
+                                    "tops_algorithmic": alg / ms / 1e9,
+                                    "frac_of_int8_peak": (ops / ms / 1e9) / peak_i8}
+        outs[name] = dC.cpu().numpy().tobytes()
+        del dC
+    res["bitwise_equal_forms"] = outs["int8"] == outs["fp64"]
+    res["fp64_over_int8"] = res["fp64"]["s"] / res["int8"]["s"]
+    return res
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
     os.environ["SDPX_B200_DEVICE"] = str(local)
     torch.cuda.set_device(local)
+    from sdpx_b200 import _lib
     from sdpx_b200.solver import CProblem, DefaultSettings, DefaultSolver
 
     prob = make_problem()
     settings = DefaultSettings(kkt_form="condensed")
-    solver = DefaultSolver(prob.P, prob.q, prob.A, prob.b, prob.cones, settings)
-    for _ in range(args.warmup):
-        solver.solve()
-    iters = solver.solution.iterations
-    status = solver.solution.status
+    arms = {}
+    for name, form in (("plain", DefaultSolver.FORM_PLAIN), ("split", DefaultSolver.FORM_SPLIT)):
+        s = DefaultSolver(prob.P, prob.q, prob.A, prob.b, prob.cones, settings)
+        s.set_form(form)
+        for _ in range(args.warmup):
+            s.solve()
+        arms[name] = s
     clocks = ClockSampler(local)
     barrier(world)
     torch.cuda.synchronize()
     clocks.start()
-    from sdpx_b200 import _lib
-    launches0 = _lib.load().sdpx_b200_launch_count()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        solver.solve()
-    ev1.record()
-    torch.cuda.synchronize()
-    launches = _lib.load().sdpx_b200_launch_count() - launches0
-    wall = (time.perf_counter() - t0) / args.steps
+    timed = {}
+    for name in ("plain", "split"):  # the chosen (split) arm last: the headline value
+        timed[name] = time_solves(arms[name], args.steps)
     barrier(world)
     clk = clocks.stop()
-    dev_s = ev0.elapsed_time(ev1) / 1e3 / args.steps
+    solver = arms["split"]
+    dev_s, wall, launches = timed["split"]
     value = max_over_ranks(world, dev_s)
-    gpu_launches = int(launches)
-    timed_host = {k: round(v, 5) for k, v in solver.info.phase_times.items()}  # graph-mode solve
-    # per-phase device times from one more solve with phase events on (outside the timed
-    # region: the events synchronize the host at every phase boundary)
-    solver.set_kernel_timing(True)
-    solver.solve()
-    ktimes = solver.kernel_times()
-    solver.set_kernel_timing(False)
+    plain_s = max_over_ranks(world, timed["plain"][0])
+    iters, status = solver.solution.iterations, solver.solution.status
+    forms = {name: {"s": max_over_ranks(world, timed[name][0]), "status": arms[name].solution.status,
+                    "iterations": arms[name].solution.iterations,
+                    "objective": arms[name].solution.obj_val,
+                    "gpu_launches_per_solve": timed[name][2] / args.steps} for name in arms}
+    forms["plain_over_split"] = plain_s / value
+    timed_host = {k: round(v, 5) for k, v in solver.info.phase_times.items()}
+    # per-phase device times from one more solve per arm with phase events on (outside the
+    # timed region: the events synchronize the host at every phase boundary)
+    ktimes = {}
+    for name, s in arms.items():
+        s.set_kernel_timing(True)
+        s.solve()
+        ktimes[name] = s.kernel_times()
+        s.set_kernel_timing(False)
+    # INT8 tensor-core GEMM of the split form, timed inside one more solve
+    i8 = i8_measure(lambda: solver.solve())
 
-    # ---- end-to-end through the C ABI with host buffers ----
+    # ---- end-to-end through the C ABI with host buffers (split form) ----
     e2e_times = []
     h2d = d2h = 0
     lib = _lib.load()
@@ -317,6 +460,7 @@ def run_ours(args, world, rank, local):
         b0 = (cnt_h2d.value, cnt_d2h.value)
         t0 = time.perf_counter()
         s2 = DefaultSolver.from_c_problem(cp)  # sdpx_prepare: validate, equilibrate, upload
+        s2.set_form(DefaultSolver.FORM_SPLIT)
         s2.solve()                             # sdpx_solve, sdpx_get_info, sdpx_result_f64
         s2.close()                             # sdpx_destroy
         torch.cuda.synchronize()
@@ -327,34 +471,51 @@ def run_ours(args, world, rank, local):
     e2e = max_over_ranks(world, statistics.mean(e2e_times))
     model = schur_model(prob, gram=solver.schur_forms()["ordinary"] == 0)
 
-    # ---- roofline of the dominant device phase ----
+    # ---- roofline of the dominant device phase of the chosen (split) arm ----
     hbm, hbm_kind = measured_peaks()
-    dom = max(ktimes, key=lambda k: ktimes[k][0])
-    ms, cnt = ktimes[dom]
+    kt = ktimes["split"]
+    dom = max(kt, key=lambda k: kt[k][0])
+    ms, cnt = kt[dom]
     per = ms / 1e3 / max(cnt, 1)
-    fp64 = None
-    if dom in ("factor", "trinv", "assemble", "scale", "cone", "step"):
+    peak_i8 = int8_peak()
+    nh = model["n"] // 2
+    half_flops = ((nh + 63) // 64 * 64) ** 3 / 3.0
+    if dom == "split":
+        achieved = i8[1] / (i8[0] / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak_i8, "unit": "TOP/s",
+                "frac": achieved / peak_i8, "traffic": traffic_from_profile("i8_gemm"),
+                "kernel": "k_i8_mod_gemm", "launch_ms": i8[0] / max(i8[3], 1),
+                "note": "INT8 pipe; peak = cuBLASLt INT8 GEMM 8192^3 (torch._int_mm) measured in this run"}
+    elif dom in ("factor", "trinv", "assemble", "scale", "cone", "step"):
         fp64 = fp64_gemm_peak()
-        flops = {"factor": model["factor_flops"], "trinv": model["factor_flops"],
+        flops = {"factor": half_flops, "trinv": half_flops,
                  "assemble": model["assemble_flops"], "scale": model["scale_flops"]}.get(dom)
         if flops is None:
             flops = sum(4.0 * d ** 3 for _, d in prob.cones)
         achieved = flops / per / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
                 "frac": achieved / fp64, "traffic": traffic_from_profile(dom),
-                "kernel": dom, "launch_ms": per * 1e3,
-                "note": "FP64 pipe; peak = cuBLAS DGEMM 8192^3 measured in this run (FP64 is not "
-                        "in MEASURED_PEAKS.json)"}
+                "kernel": "k_chol_dataflow" if dom == "factor" else dom, "launch_ms": per * 1e3,
+                "note": "FP64 pipe; the split form factors two diagonal halves of order ~m/2 "
+                        "(n^3/3 flop per launch); peak = cuBLAS DGEMM 8192^3 measured in this run "
+                        "(FP64 is not in MEASURED_PEAKS.json)"}
     else:
         nbytes = model["trisolve_bytes"] if dom == "trisolve" else model["symv_bytes"]
         achieved = nbytes / per / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic_from_profile(dom), "kernel": dom,
                 "launch_ms": per * 1e3, "note": f"peak {hbm_kind} (MEASURED_PEAKS.json hbm_gbs)"}
-    phases = {k: {"ms_total": v[0], "launches": v[1]} for k, v in ktimes.items()}
-    host_phases = {k: round(v, 5) for k, v in solver.info.phase_times.items()}
-    host_phases["counts"] = solver.info.counts
+    i8_obj = {"ms_per_solve": i8[0], "launches_per_solve": i8[3],
+              "tops_executed": i8[1] / (i8[0] / 1e3) / 1e12 if i8[0] else None,
+              "tops_algorithmic": i8[2] / (i8[0] / 1e3) / 1e12 if i8[0] else None,
+              "int8_peak_tops": peak_i8}
+    phases = {arm: {k: {"ms_total": v[0], "launches": v[1]} for k, v in kt_.items()}
+              for arm, kt_ in ktimes.items()}
 
+    extra = {}
+    if rank == 0 and not args.quick:
+        extra["precision_f64"] = precision_f64(args)
+        extra["rns_256"] = rns_256(args, peak_i8)
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline(prob)
@@ -365,12 +526,14 @@ def run_ours(args, world, rank, local):
                 "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "config": dict(WORKLOAD, parallelism=f"replicas{world}"),
                 "status": status, "iterations": iters, "wall_s_per_step": wall,
+                "forms": forms,
                 "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
-                "roofline": roof, "phases": phases, "host_phase_s_last_solve": host_phases,
+                "roofline": roof, "int8_gemm": i8_obj, "phases": phases,
                 "host_phase_s_timed_solve": timed_host,
-                "gpu_launches": gpu_launches,
+                "gpu_launches": int(launches),
                 "clocks": clk, "cpu_baseline": cb}
+        line.update(extra)
         print(json.dumps(line))
     return 0
 
@@ -524,6 +687,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--quick", action="store_true",
+                    help="skip the nested precision-workload and 256-bit RNS measurements")
     ap.add_argument("--workload", default="rank1", choices=["rank1", "batch", "adjoint"],
                     help="rank1: the 32-block bootstrap SDP (default line); batch: independent "
                          "small SDPs, instances/s; adjoint: conic QPs solved and differentiated")

@@ -132,8 +132,9 @@ int32_t sdpx_b200_kkt_paths(sdpx_handle *handle, uint64_t *device_driven, uint64
  * Schur assembly, factorisation, triangular solves, cone congruences, step lengths, the
  * Schur matvec and the inverse of the factor, in that order (no counterpart in the reference, which has no device). */
 int32_t sdpx_b200_set_kernel_timing(sdpx_handle *handle, int32_t on);
-/* Totals since the last reset: ms[8] milliseconds and counts[8] timed regions per phase (the
- * seven above, then the explicit inverse of the factor). */
+/* Totals since the last reset: ms[9] milliseconds and counts[9] timed regions per phase (the
+ * seven above, then the explicit inverse of the factor, then the split-precision products and
+ * block assembly of the split form). */
 int32_t sdpx_b200_kernel_times(sdpx_handle *handle, double *ms, uint64_t *counts);
 /* Number of CUDA kernels this library has launched in this process (all handles). */
 uint64_t sdpx_b200_launch_count(void);
@@ -141,6 +142,15 @@ uint64_t sdpx_b200_launch_count(void);
  * released blocks or from cudaMalloc; all handles).  A call that allocates nothing leaves it
  * unchanged.  No counterpart in the reference (it has no device memory). */
 uint64_t sdpx_b200_device_allocations(void);
+/* Measurement of the INT8 tensor-core GEMM (k_i8_mod_gemm, used by the exact RNS products and
+ * the split-precision products): on != 0 times every later launch with CUDA events on its stream
+ * (synchronising the host: measurement runs only) and resets the totals.  No counterpart in the
+ * reference (it has no device). */
+int32_t sdpx_b200_set_i8_timing(int32_t on);
+/* Totals since the last sdpx_b200_set_i8_timing: milliseconds, INT8 operations executed (2 per
+ * multiply-add over the padded tiles), algorithmic INT8 operations (2 m n k per digit pair and
+ * modulus), launches. */
+int32_t sdpx_b200_i8_times(double *ms, double *ops, double *alg_ops, uint64_t *launches);
 /* Bytes this library has copied host-to-device and device-to-host in this process (all
  * handles): the host-device traffic of prepare, solve and result reads. */
 int32_t sdpx_b200_transfer_bytes(uint64_t *h2d, uint64_t *d2h);

@@ -14,6 +14,7 @@
 #include "../../include/sdpx_b200.h"
 #include "hsd.cuh"
 #include "sampled.cuh"
+#include "i8_gemm.cuh"
 #include "host_parallel.h"
 
 using namespace sdpxg;
@@ -719,6 +720,17 @@ int32_t sdpx_destroy(sdpx_handle* h) {
 
 uint64_t sdpx_b200_launch_count(void) { return sdpxg::g_launches; }
 uint64_t sdpx_b200_device_allocations(void) { return sdpxg::g_dev_allocs; }
+
+int32_t sdpx_b200_set_i8_timing(int32_t on) {
+  return boundary([&] { sdpxg::i8_timing(on != 0); });
+}
+
+int32_t sdpx_b200_i8_times(double* ms, double* ops, double* alg_ops, uint64_t* launches) {
+  return boundary([&] {
+    if (!ms || !ops || !alg_ops || !launches) invalid("null pointer");
+    sdpxg::i8_times(ms, ops, alg_ops, launches);
+  });
+}
 
 int32_t sdpx_b200_transfer_bytes(uint64_t* h2d, uint64_t* d2h) {
   return boundary([&] {

@@ -242,7 +242,7 @@ inline void need(const void* p, const char* what) {
 
 // Kernel-phase timers: CUDA events recorded on the engine's stream around each phase.
 enum KernelPhase { KT_SCALE = 0, KT_ASSEMBLE, KT_FACTOR, KT_TRISOLVE, KT_CONE, KT_STEP, KT_SYMV, KT_TRINV,
-                   KT_N };
+                   KT_SPLIT, KT_N };
 
 class Engine {
  public:
@@ -1117,20 +1117,32 @@ class Engine {
     const long ldn = n;
     clear_status();
     check(cudaMemsetAsync(oz_status_word(), 0, sizeof(uint32_t), st), "memset");
-    tbegin(KT_FACTOR);
+    // phase timers: the dataflow launches under KT_FACTOR, the diagonal-block inverses under
+    // KT_TRINV, the split-precision products and the assembly under KT_SPLIT
     copy_block(sub1_.H, n1, Hsave_, ldn, n1, n1);
     copy_block(sub2_.H, n2, Hsave_ + (long)n1 * ldn + n1, ldn, n2, n2);
+    tbegin(KT_FACTOR);
     launch_chol(sub1_.b, eps, dynamic, dyn_eps, dyn_delta);
+    tend(KT_FACTOR);
+    tbegin(KT_TRINV);
     launch_trinv(sub1_.b);
+    tend(KT_TRINV);
     double* U12 = F_.p + (long)n1 * ldn;  // F[0:n1, n1:n]
+    tbegin(KT_SPLIT);
     // U12 = X11' H12: rows of the left operand are the columns of X11, rows of the right
     // operand the columns of H12
     ozaki_gemm(oz, st, n1, n2, n1, sub1_.Uinv, n1, 1, Hsave_.p + (long)n1 * ldn, ldn, 1, 1.0, 0.0, U12, ldn, 0);
     // S = H22 - U12' U12 (full, exactly symmetric: the integer product of an operand with itself)
     ozaki_gemm(oz, st, n2, n2, n1, U12, ldn, 1, U12, ldn, 1, -1.0, 1.0, sub2_.H, n2, 0);
+    tend(KT_SPLIT);
     // the pivot rule's original diagonal is that of H22 + eps I, as in the plain form
+    tbegin(KT_FACTOR);
     launch_chol(sub2_.b, eps, dynamic, dyn_eps, dyn_delta, Hsave_.p + (long)n1 * ldn + n1, ldn + 1);
+    tend(KT_FACTOR);
+    tbegin(KT_TRINV);
     launch_trinv(sub2_.b);
+    tend(KT_TRINV);
+    tbegin(KT_SPLIT);
     // X12 = -(X11 U12) X22
     ozaki_gemm(oz, st, n1, n2, n1, sub1_.Uinv, 1, n1, U12, ldn, 1, 1.0, 0.0, Tmp_, n1, 0);
     ozaki_gemm(oz, st, n1, n2, n2, Tmp_, 1, n1, sub2_.Uinv, n2, 1, -1.0, 0.0, Uinv_.p + (long)n1 * ldn, ldn, 0);
@@ -1144,7 +1156,7 @@ class Engine {
     ++g_launches, k_transpose_block<<<dim3((n2 + 31) / 32, (n1 + 31) / 32), dim3(32, 8), 0, st>>>(
         Uinv_.p + (long)n1 * ldn, ldn, n1, n2, UinvT_.p + n1, ldn);
     launched("split factor");
-    tend(KT_FACTOR);
+    tend(KT_SPLIT);
     uint32_t s = read_status();
     if (s & SDPXG_ST_SYNC_TIMEOUT) throw CudaError("factorization: a bounded inter-CTA wait gave up");
     uint32_t hs[2] = {0, 0};

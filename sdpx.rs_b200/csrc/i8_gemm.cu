@@ -13,6 +13,7 @@
 // their next wait, outstanding TMA copies are drained (bounded) and TMEM is released before exit.
 #include <cuda.h>
 
+#include <atomic>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -250,6 +251,13 @@ CUtensorMap byte_map(const int8_t* base, long rows, int kpad, int box_rows) {
   return m;
 }
 
+// Optional CUDA-event timing of every launch (sdpx_b200_set_i8_timing): events on the launch
+// stream around the kernel, host-synchronised, so only for measurement runs.
+std::atomic<int> g_i8_timing{0};
+std::mutex g_i8_mu;
+double g_i8_ms = 0.0, g_i8_ops = 0.0, g_i8_alg_ops = 0.0;
+uint64_t g_i8_count = 0;
+
 template <int DIGITS>
 void launch(const int8_t* A, const int8_t* B, const I8GemmArgs& a, cudaStream_t st) {
   constexpr int BN = Cfg<DIGITS>::BN;
@@ -268,12 +276,50 @@ void launch(const int8_t* A, const int8_t* B, const I8GemmArgs& a, cudaStream_t 
   const CUtensorMap ta = byte_map(A, (long)a.L * DIGITS * a.Mpad, a.Kld, kBM);
   const CUtensorMap tb = byte_map(B, (long)a.L * DIGITS * a.Npad, a.Kld, BN);
   const dim3 grid(a.Mpad / kBM, a.Npad / BN, a.L);
+  const bool timed = g_i8_timing.load() != 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (timed) {
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+    check(cudaEventRecord(e0, st), "event");
+  }
   ++g_launches;
   k_i8_mod_gemm<DIGITS><<<grid, kThreads, smem_bytes<DIGITS>(), st>>>(ta, tb, a);
   check(cudaGetLastError(), "k_i8_mod_gemm launch");
+  if (timed) {
+    check(cudaEventRecord(e1, st), "event");
+    check(cudaEventSynchronize(e1), "event sync");
+    float ms = 0.f;
+    check(cudaEventElapsedTime(&ms, e0, e1), "event time");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    double tiles = 0;  // tiles actually computed (upper_only skips those below the diagonal)
+    for (int tm = 0; tm < a.Mpad / kBM; ++tm)
+      for (int tn = 0; tn < a.Npad / BN; ++tn)
+        if (!(a.upper_only && tm * kBM > tn * BN + BN - 1)) tiles += 1;
+    std::lock_guard<std::mutex> lk(g_i8_mu);
+    g_i8_ms += ms;
+    g_i8_ops += 2.0 * DIGITS * DIGITS * tiles * kBM * BN * (double)a.Kpad * a.L;
+    g_i8_alg_ops += 2.0 * DIGITS * DIGITS * (double)a.m * a.n * (double)a.Kpad * a.L;
+    ++g_i8_count;
+  }
 }
 
 }  // namespace
+
+void i8_timing(int on) {
+  std::lock_guard<std::mutex> lk(g_i8_mu);
+  g_i8_timing = on;
+  g_i8_ms = g_i8_ops = g_i8_alg_ops = 0.0;
+  g_i8_count = 0;
+}
+void i8_times(double* ms, double* ops, double* alg_ops, uint64_t* count) {
+  std::lock_guard<std::mutex> lk(g_i8_mu);
+  *ms = g_i8_ms;
+  *ops = g_i8_ops;
+  *alg_ops = g_i8_alg_ops;
+  *count = g_i8_count;
+}
 
 void launch_i8_gemm(int digits, const int8_t* A, const int8_t* B, const I8GemmArgs& args, cudaStream_t st) {
   if (digits == 1)

@@ -46,4 +46,10 @@ constexpr int i8_tile_n(int digits) { return digits == 1 ? 256 : 128; }
 void launch_i8_gemm(int digits, const int8_t* A, const int8_t* B, const I8GemmArgs& args,
                     cudaStream_t st);
 
+// Measurement hooks: on != 0 times every later launch with CUDA events (synchronising) and
+// resets the totals; i8_times reads milliseconds, INT8 operations executed (padded tiles),
+// algorithmic INT8 operations (2 m n K per digit pair and modulus) and the launch count.
+void i8_timing(int on);
+void i8_times(double* ms, double* ops, double* alg_ops, uint64_t* count);
+
 }  // namespace sdpxg

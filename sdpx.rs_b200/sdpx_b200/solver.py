@@ -257,7 +257,7 @@ class DefaultSolver:
                                                "inner_refinements"], counts.tolist())))
         return self.solution
 
-    KERNEL_PHASES = ["scale", "assemble", "factor", "trisolve", "cone", "step", "symv", "trinv"]
+    KERNEL_PHASES = ["scale", "assemble", "factor", "trisolve", "cone", "step", "symv", "trinv", "split"]
 
     def set_kernel_timing(self, on: bool):
         _lib.call("sdpx_b200_set_kernel_timing", self._h, int(bool(on)))
