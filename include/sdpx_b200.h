@@ -297,6 +297,16 @@ int32_t sdpxg_rns_gemm_device(sdpxg_ctx *ctx, uint32_t limbs, char ta, char tb, 
                               uint64_t n, uint64_t k, const void *d_A, uint64_t lda,
                               const void *d_B, uint64_t ldb, uint32_t upper_only, void *d_C,
                               uint32_t *status);
+/* Exact congruence C = op(A) X op(A)' of MpFloat<limbs> matrices (op(A) m x k, X k x k, host
+ * buffers in the layout of sdpxg_rns_gemm; C m x m column-major): every entry is the exact sum
+ * over all (a, b) of op(A)(i, a) X(a, b) op(A)(j, b), rounded once to 64 * limbs bits, ties to
+ * even.  Two products per prime on the INT8 tensor cores (T = X op(A)', C = op(A) T) and one
+ * CRT.  upper_only writes zeros below the diagonal.  Replaces rns_blas::congruence
+ * (crates/solver/src/algebra/dense/blas/rns_blas.rs:3563-3736), the exact congruence behind the
+ * MPFR PSD transforms (congruence_exact_sym). */
+int32_t sdpxg_rns_congruence(sdpxg_ctx *ctx, uint32_t limbs, char ta, uint64_t m, uint64_t k,
+                             const void *A, uint64_t lda, const void *X, uint64_t ldx,
+                             uint32_t upper_only, void *C, uint32_t *status);
 /* Residue arithmetic of the exact products of this context: 0 = INT8 tensor cores (default),
  * 1 = FP64 CUDA cores.  The reference computes its per-prime products with FP64 dgemm
  * (rns_blas.rs:447-580); the result bits do not depend on the form. */

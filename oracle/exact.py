@@ -177,3 +177,42 @@ def pack_array(vals: Sequence[Mp]) -> bytes:
 def unpack_array(n: int, raw: bytes) -> List[Mp]:
     size = 8 * n + 8
     return [Mp.unpack(n, raw[i * size:(i + 1) * size]) for i in range(len(raw) // size)]
+
+
+def exact_sum_of_products(n: int, factors: Sequence[Sequence[Mp]]) -> Mp:
+    """sum over terms of the product of each term's factors, exact, rounded once."""
+    terms = [t for t in factors if all(not f.is_zero() for f in t)]
+    if not terms:
+        return Mp(n)
+
+    def scale(t):
+        return sum(f.exp - f.p for f in t)
+    low = min(scale(t) for t in terms)
+    total = 0
+    for t in terms:
+        v = 1
+        neg = False
+        for f in t:
+            v *= f.mant
+            neg ^= f.neg
+        v <<= scale(t) - low
+        total += -v if neg else v
+    return from_scaled_integer(n, total < 0, abs(total), low)
+
+
+def congruence(n: int, ta: str, m: int, k: int, A: List[Mp], lda: int, X: List[Mp], ldx: int,
+               upper_only: bool = False) -> List[Mp]:
+    """C = op(A) X op(A)' with every entry the exact triple sum rounded once
+    (crates/solver/src/algebra/dense/blas/rns_blas.rs:3563-3736 congruence; op(A) is m x k, X is
+    k x k, C column-major m x m; upper_only leaves zeros below the diagonal)."""
+    def at(i, q):
+        return A[i + q * lda] if ta == "N" else A[q + i * lda]
+    out = []
+    for j in range(m):
+        for i in range(m):
+            if upper_only and i > j:
+                out.append(Mp(n))
+                continue
+            out.append(exact_sum_of_products(
+                n, [(at(i, a), X[a + b * ldx], at(j, b)) for a in range(k) for b in range(k)]))
+    return out

@@ -35,6 +35,8 @@
 //   u64 limbs[N] (least significant first), i32 kind (sign * MPFR kind: 2 zero, 3 regular),
 //   i32 exponent; a regular value is M * 2^(exponent - 64N) with the top bit of M set.
 #include <algorithm>
+#include <climits>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -281,6 +283,42 @@ extern "C" __global__ void k_rns8_residues(const unsigned char* __restrict__ X, 
   }
 }
 
+// Residues of an intermediate product (INT8 form, values in [0, p) as written by the modular
+// GEMM: RC[t * plane + j * inner + r]) re-split into signed-byte digit planes for the next
+// product: line j, inner index r at out[((2t + d) * Rpad + j) * Kld + r]; padding zeros.
+extern "C" __global__ void k_rns8_replane(const int* __restrict__ RC, long plane, int lines, int inner, int L,
+                                          const int* __restrict__ primes, int8_t* __restrict__ out, int Rpad,
+                                          int Kld) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)Rpad * Kld) return;
+  const int r = (int)(idx % Kld), j = (int)(idx / Kld);
+  const size_t pl = (size_t)Rpad * Kld;
+  int8_t* o = out + (size_t)j * Kld + r;
+  const bool live = j < lines && r < inner;
+  for (int t = 0; t < L; ++t) {
+    int dlo = 0, dhi = 0;
+    if (live) {
+      const int p = primes[t];
+      int v = RC[t * plane + (long)j * inner + r];
+      if (v > p / 2) v -= p;
+      dlo = ((v + 128) & 255) - 128;
+      dhi = (v - dlo) >> 8;
+    }
+    o[(size_t)(2 * t) * pl] = (int8_t)dlo;
+    o[(size_t)(2 * t + 1) * pl] = (int8_t)dhi;
+  }
+}
+
+// out[i] = a[i] + c (exponent offsets of the congruence's second factor).
+extern "C" __global__ void k_add_const_int(const int* __restrict__ a, int n, int c, int* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a[i] + c;
+}
+extern "C" __global__ void k_fill_int(int* __restrict__ a, int n, int v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+
 // Garner CRT of the L residues of every output, then one rounding to 64N bits (ties to even).
 // Residues are read as R (double: the FP64 form's exact integers, possibly negative; int: the
 // INT8 form's residues in [0, p)).  The mixed-radix digits are formed with one reduction per
@@ -525,6 +563,7 @@ struct RnsWorkspace {
   DevBuf<double> RA, RB, RC;  // FP64 form
   DevBuf<int8_t> PA, PB;      // INT8 form: digit planes
   DevBuf<int> RC8;            // INT8 form: residues of the product
+  DevBuf<int> RT8, loX, bitsX, loB2;  // congruence: intermediate residues, X scan, column offsets
   int form = 0;               // 0: INT8 tensor cores, 1: FP64
 };
 
@@ -632,6 +671,110 @@ int32_t rns_product(RnsWorkspace& ws, cudaStream_t st, int form, int N, char ta,
   int herr = 0;
   copy_d2h(&hs, ws.status.p, sizeof(uint32_t), st);
   if (form == 0 && k) copy_d2h(&herr, ws.err.p, sizeof(int), st);
+  check(cudaStreamSynchronize(st), "sync");
+  if (herr) throw CudaError("modular INT8 GEMM: a bounded wait gave up");
+  if (hs_out) *hs_out = hs;
+  return 0;
+}
+
+// The exact congruence C = op(A) X op(A)' (INT8 form) on device buffers: op(A) m x k aligned per
+// row (lo_i), X k x k aligned as one block (lo_x, so that its scale factors out of the sums),
+// then per prime T = X A~' and C = A~ T on the tensor cores, and the CRT with the exponents
+// lo_i + lo_j + lo_x.  Width: |C| < k^2 2^(2 max bits(A) + bits(X)), so the primes cover
+// 2 bits(A) + bits(X) + 2 log2 k + 2 bits.  Returns 0 or 2 (non-finite, too wide).
+int32_t rns_congruence(RnsWorkspace& ws, cudaStream_t st, int N, char ta, uint64_t m, uint64_t k,
+                       const unsigned char* dA, uint64_t lda, const unsigned char* dX, uint64_t ldx, int upper_only,
+                       unsigned char* dC, uint32_t* hs_out) {
+  grow(ws.loA, m); grow(ws.bitsA, m); grow(ws.loX, k); grow(ws.bitsX, k); grow(ws.loB2, m);
+  grow(ws.maxbits, 2); grow(ws.status, 1); grow(ws.err, 1);
+  check(cudaMemsetAsync(ws.maxbits.p, 0, 2 * sizeof(int), st), "memset");
+  check(cudaMemsetAsync(ws.status.p, 0, sizeof(uint32_t), st), "memset");
+  const long asx = (ta == 'N') ? 1 : (long)lda, asy = (ta == 'N') ? (long)lda : 1;
+  ++g_launches, k_rns_scan<<<(unsigned)((m + 7) / 8), 256, 0, st>>>(dA, N, (int)m, (int)k, asx, asy, ws.loA,
+                                                                 ws.bitsA, ws.maxbits, ws.status);
+  // X by columns (line c: entries (r, c), r < k), combined on the host into one alignment
+  ++g_launches, k_rns_scan<<<(unsigned)((k + 7) / 8), 256, 0, st>>>(dX, N, (int)k, (int)k, (long)ldx, 1, ws.loX,
+                                                                 ws.bitsX, ws.maxbits.p + 1, ws.status);
+  int hb[2] = {0, 0};
+  uint32_t hs = 0;
+  std::vector<int> hlo(k), hbits(k);
+  copy_d2h(hb, ws.maxbits.p, 2 * sizeof(int), st);
+  copy_d2h(&hs, ws.status.p, sizeof(uint32_t), st);
+  copy_d2h(hlo.data(), ws.loX.p, k * sizeof(int), st);
+  copy_d2h(hbits.data(), ws.bitsX.p, k * sizeof(int), st);
+  check(cudaStreamSynchronize(st), "sync");
+  if (hs) {
+    if (hs_out) *hs_out = hs;
+    g_last_error = "sdpxg_rns_congruence: non-finite operands are not supported";
+    return 2;
+  }
+  // one alignment for the whole of X: lowest bit over all regular entries, and its width
+  long long lo_x = LLONG_MAX, top_x = LLONG_MIN;
+  for (uint64_t c = 0; c < k; ++c)
+    if (hbits[c] > 0 || hlo[c] != 0) {  // a column with a regular entry (an all-zero one reports 0, 0)
+      lo_x = std::min<long long>(lo_x, hlo[c]);
+      top_x = std::max<long long>(top_x, (long long)hlo[c] + hbits[c]);
+    }
+  if (lo_x == LLONG_MAX) lo_x = top_x = 0;
+  if (top_x - lo_x > (1 << 20)) {
+    g_last_error = "sdpxg_rns_congruence: exponent spread too wide";
+    return 2;
+  }
+  const int bits_x = (int)(top_x - lo_x);
+  int lg = 0;
+  while ((1ull << lg) < std::max<uint64_t>(k, 1)) ++lg;
+  const double needed = 2.0 * hb[0] + bits_x + 2.0 * lg + 2;
+  const auto& ps = prime_list(15);
+  int L = 0;
+  double acc = 0;
+  while (L < RNS_MAXL && acc <= needed) acc += std::log2((double)ps[L++]);
+  if (acc <= needed || (int)(acc / 64) + 2 > RNS_MAXW) {
+    g_last_error = "sdpxg_rns_congruence: exponent spread too wide for the prime set";
+    return 2;
+  }
+  DevTables& DT = ws.t15;
+  const PrimeTables& T = DT.get(15, L, st);
+  const int Mpad = (int)((m + 127) / 128 * 128), Kpad = (int)((k + 127) / 128 * 128);
+  const long planeT = (long)(k * m), planeC = (long)(m * m);
+  grow(ws.RT8, (size_t)L * planeT);
+  grow(ws.RC8, (size_t)L * planeC);
+  const int S = 64 * N + std::max(hb[0], bits_x) + 1;
+  grow(ws.pow2, (size_t)L * S);
+  ++g_launches, k_rns_pow2<<<dim3((S + 255) / 256, L), 256, 0, st>>>(L, DT.iprimes, S, ws.pow2);
+  grow(ws.PA, (size_t)L * 2 * Mpad * Kpad);  // A~ (rows of op(A)), used by both products
+  grow(ws.PB, (size_t)L * 2 * (size_t)std::max(Kpad, Mpad) * Kpad);
+  ++g_launches, k_rns8_residues<<<(unsigned)(((long)Mpad * Kpad + 255) / 256), 256, 0, st>>>(
+      dA, N, (int)m, (int)k, asx, asy, ws.loA, L, DT.iprimes, ws.pow2, S, ws.PA, Mpad, Kpad);
+  ++g_launches, k_fill_int<<<(unsigned)((k + 255) / 256), 256, 0, st>>>(ws.loX, (int)k, (int)lo_x);
+  // X~ by rows (line r: entries (r, c)): the left operand of T = X~ A~'
+  ++g_launches, k_rns8_residues<<<(unsigned)(((long)Kpad * Kpad + 255) / 256), 256, 0, st>>>(
+      dX, N, (int)k, (int)k, 1, (long)ldx, ws.loX, L, DT.iprimes, ws.pow2, S, ws.PB, Kpad, Kpad);
+  check(cudaMemsetAsync(ws.err.p, 0, sizeof(int), st), "memset");
+  for (int k0 = 0; k0 < Kpad; k0 += kI8Chunk) {  // T (k x m) = X~ A~'
+    I8GemmArgs ga;
+    ga.Mpad = Kpad; ga.Npad = Mpad; ga.Kld = Kpad; ga.k0 = k0; ga.Kpad = std::min(kI8Chunk, Kpad - k0);
+    ga.m = (int)k; ga.n = (int)m; ga.L = L; ga.moduli = DT.iprimes; ga.accumulate = k0 > 0;
+    ga.out = ws.RT8.p; ga.plane = planeT; ga.err = ws.err.p;
+    launch_i8_gemm(2, ws.PB, ws.PA, ga, st);
+  }
+  // columns of T as the right operand of C = A~ T (line j, inner r)
+  ++g_launches, k_rns8_replane<<<(unsigned)(((long)Mpad * Kpad + 255) / 256), 256, 0, st>>>(
+      ws.RT8, planeT, (int)m, (int)k, L, DT.iprimes, ws.PB, Mpad, Kpad);
+  for (int k0 = 0; k0 < Kpad; k0 += kI8Chunk) {  // C (m x m) = A~ T
+    I8GemmArgs ga;
+    ga.Mpad = Mpad; ga.Npad = Mpad; ga.Kld = Kpad; ga.k0 = k0; ga.Kpad = std::min(kI8Chunk, Kpad - k0);
+    ga.m = (int)m; ga.n = (int)m; ga.L = L; ga.moduli = DT.iprimes; ga.upper_only = upper_only;
+    ga.accumulate = k0 > 0; ga.out = ws.RC8.p; ga.plane = planeC; ga.err = ws.err.p;
+    launch_i8_gemm(2, ws.PA, ws.PB, ga, st);
+  }
+  ++g_launches, k_add_const_int<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(ws.loA, (int)m, (int)lo_x, ws.loB2);
+  ++g_launches, k_rns_crt<int><<<(unsigned)((m * m + 127) / 128), 128, 0, st>>>(
+      ws.RC8, planeC, (int)m, (int)m, L, T.WW, DT.primes, DT.inv, DT.pmod, DT.M, DT.half, ws.loA, ws.loB2, N,
+      upper_only ? 1 : 0, dC, ws.status);
+  check(cudaGetLastError(), "congruence launch");
+  int herr = 0;
+  copy_d2h(&hs, ws.status.p, sizeof(uint32_t), st);
+  copy_d2h(&herr, ws.err.p, sizeof(int), st);
   check(cudaStreamSynchronize(st), "sync");
   if (herr) throw CudaError("modular INT8 GEMM: a bounded wait gave up");
   if (hs_out) *hs_out = hs;
@@ -758,6 +901,60 @@ extern "C" int32_t sdpxg_rns_gemm_device(sdpxg_ctx* ctx, uint32_t limbs, char ta
                                    static_cast<unsigned char*>(d_C), &hs);
     if (status) *status = hs;
     return rc;
+  } catch (const std::invalid_argument& e) {
+    g_last_error = e.what();
+    return 1;
+  } catch (const std::exception& e) {
+    g_last_error = std::string("internal error: ") + e.what();
+    return 5;
+  } catch (...) {
+    g_last_error = "internal error";
+    return 5;
+  }
+}
+
+extern "C" int32_t sdpxg_rns_congruence(sdpxg_ctx* ctx, uint32_t limbs, char ta, uint64_t m, uint64_t k,
+                                        const void* A, uint64_t lda, const void* X, uint64_t ldx,
+                                        uint32_t upper_only, void* C, uint32_t* status) {
+  try {
+    Engine* E = ctx_engine_any(ctx);
+    if (!E) throw std::invalid_argument("null context");
+    const int N = (int)limbs;
+    if (N < 1 || N > RNS_MAXN) {
+      g_last_error = "sdpxg_rns_congruence: limbs must be in 1..16";
+      return 2;
+    }
+    if (ta != 'N' && ta != 'T') throw std::invalid_argument("bad transpose flag");
+    if (m > (1u << 20) || k > (1u << 20)) throw std::invalid_argument("size overflow");
+    const uint64_t ar = ta == 'N' ? m : k, ac = ta == 'N' ? k : m;
+    if (lda < std::max<uint64_t>(ar, 1) || ldx < std::max<uint64_t>(k, 1))
+      throw std::invalid_argument("leading dimension too small");
+    if (m == 0) return 0;
+    if (!A || !X || !C) throw std::invalid_argument("null pointer");
+    const size_t esz = 8 * (size_t)N + 8;
+    const size_t na = ac ? lda * (ac - 1) + ar : 0, nx = k ? ldx * (k - 1) + k : 0;
+    RnsWorkspace& ws = workspace(ctx);
+    cudaStream_t st = E->st;
+    check(cudaSetDevice(E->device), "cudaSetDevice");
+    if (k == 0) {  // empty sums: zeros
+      std::vector<unsigned char> z(m * m * esz, 0);
+      for (size_t e = 0; e < m * m; ++e) *reinterpret_cast<int*>(&z[e * esz + 8 * N]) = MP_ZERO;
+      std::memcpy(C, z.data(), z.size());
+      if (status) *status = 0;
+      return 0;
+    }
+    grow(ws.a, na * esz);
+    grow(ws.b, nx * esz);
+    grow(ws.c, m * m * esz);
+    ws.a.upload(static_cast<const unsigned char*>(A), na * esz, st);
+    ws.b.upload(static_cast<const unsigned char*>(X), nx * esz, st);
+    uint32_t hs = 0;
+    const int32_t rc = rns_congruence(ws, st, N, ta, m, k, ws.a, lda, ws.b, ldx, upper_only ? 1 : 0, ws.c, &hs);
+    if (status) *status = hs;
+    if (rc) return rc;
+    copy_d2h(C, ws.c.p, m * m * esz, st);
+    check(cudaStreamSynchronize(st), "sync");
+    return 0;
   } catch (const std::invalid_argument& e) {
     g_last_error = e.what();
     return 1;

@@ -527,6 +527,16 @@ class KernelContext:
                   C.c_char_p(A), lda, C.c_char_p(B), ldb, int(upper_only), out, C.byref(st))
         return out.raw[:m * n * esz], st.value
 
+    def rns_congruence(self, limbs: int, ta: str, m: int, k: int, A: bytes, lda: int, X: bytes,
+                       ldx: int, upper_only: bool = False):
+        """Exact op(A) X op(A)' of MpFloat<limbs> matrices (raw bytes in, raw bytes out)."""
+        esz = 8 * limbs + 8
+        out = C.create_string_buffer(max(m * m * esz, 1))
+        st = C.c_uint32()
+        _lib.call("sdpxg_rns_congruence", self._h, limbs, ta.encode(), m, k, C.c_char_p(A), lda,
+                  C.c_char_p(X), ldx, int(upper_only), out, C.byref(st))
+        return out.raw[:m * m * esz], st.value
+
     def rns_gemm_device(self, limbs: int, ta: str, tb: str, m: int, n: int, k: int, d_A: int,
                         lda: int, d_B: int, ldb: int, d_C: int, upper_only: bool = False):
         """Exact product on device buffers (addresses of MpFloat arrays in device memory)."""

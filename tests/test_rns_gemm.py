@@ -142,3 +142,49 @@ def test_rns_gemm_cancellation_and_zero(form):
     assert got == tiny
     raw, st = ctx.rns_gemm(n, "N", "N", 1, 1, 2, X.pack_array(A[:2]), 1, X.pack_array(B[:2]), 2)
     assert X.unpack_array(n, raw)[0].is_zero()
+
+
+# congruence cases: (limbs, m, k, spread, seed, ta); inputs from the reference's generator
+CONGRUENCE_CASES = [(4, 5, 7, 4, 11, "N"), (2, 6, 9, 60, 12, "T"), (8, 3, 4, 10, 13, "N"),
+                    (4, 12, 20, 30, 14, "T")]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,m,k,spread,seed,ta", CONGRUENCE_CASES)
+def test_rns_congruence_bitwise(n, m, k, spread, seed, ta):
+    """sdpxg_rns_congruence: op(A) X op(A)' with every entry the exact triple sum rounded once
+    (rns_blas.rs:3563-3736), against the oracle's exact restatement; upper-only too."""
+    from sdpx_b200.solver import KernelContext
+    rng = X.Lcg(seed)
+    ar, ac = (m, k) if ta == "N" else (k, m)
+    A = X.random_values(n, rng, ar * ac, spread)
+    Xm = X.random_values(n, rng, k * k, spread)
+    expect = X.congruence(n, ta, m, k, A, ar, Xm, k)
+    ctx = KernelContext()
+    raw, st = ctx.rns_congruence(n, ta, m, k, X.pack_array(A), ar, X.pack_array(Xm), k)
+    assert st == 0
+    got = X.unpack_array(n, raw)
+    bad = [(i, g, e) for i, (g, e) in enumerate(zip(got, expect)) if not g == e]
+    assert not bad, bad[:3]
+    raw_u, _ = ctx.rns_congruence(n, ta, m, k, X.pack_array(A), ar, X.pack_array(Xm), k, upper_only=True)
+    up = X.unpack_array(n, raw_u)
+    for j in range(m):
+        for i in range(m):
+            if i <= j:
+                assert up[i + j * m] == expect[i + j * m]
+            else:
+                assert up[i + j * m].is_zero()
+
+
+def test_oracle_congruence_matches_products():
+    """The oracle's congruence equals the exact rational triple product rounded once."""
+    rng = X.Lcg(3)
+    n, m, k = 2, 3, 4
+    A = X.random_values(n, rng, m * k, 5)
+    Xm = X.random_values(n, rng, k * k, 5)
+    C = X.congruence(n, "N", m, k, A, m, Xm, k)
+    for j in range(m):
+        for i in range(m):
+            exact = sum(A[i + a * m].fraction() * Xm[a + b * k].fraction() * A[j + b * m].fraction()
+                        for a in range(k) for b in range(k))
+            assert C[i + j * m] == X.from_fraction(n, exact)
