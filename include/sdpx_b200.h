@@ -307,6 +307,23 @@ int32_t sdpxg_rns_gemm_device(sdpxg_ctx *ctx, uint32_t limbs, char ta, char tb, 
 int32_t sdpxg_rns_congruence(sdpxg_ctx *ctx, uint32_t limbs, char ta, uint64_t m, uint64_t k,
                              const void *A, uint64_t lda, const void *X, uint64_t ldx,
                              uint32_t upper_only, void *C, uint32_t *status);
+/* The reference's dense MPFR LDL' (ArrowLDLSolver::try_dense -> ldl_rec, kkt/ldl/arrow.rs:2609-2620,
+ * 255-420, with ldl_dots leaves 156-242 and solve_unit_lower_t 430-470) of the n x n MpFloat<limbs>
+ * matrix A (host, column-major, leading dimension lda; its lower triangle is read): L (n x n,
+ * ld n) receives the unit lower factor in its lower triangle (the strict upper triangle holds A's
+ * upper triangle, as the reference leaves it), dinv (n) receives D^-1.  Blocks up to 128 are
+ * factored by exact dots rounded once (left-looking), larger ones are halved with their trailing
+ * update A22 -= W21 L21' as one exact product per entry (INT8 tensor-core RNS) rounded once and
+ * then subtracted; every other operation rounds once (round to nearest, ties to even).  reg:
+ * NULL or two MpFloat values (eps, delta) of the pivot rule (a pivot below eps becomes delta).
+ * limbs 1..8.  A zero pivot sets SDPXG_ST_PIVOT_FAIL in *status (return 0); an exact dot whose
+ * exponent spread exceeds the device accumulator returns 2. */
+int32_t sdpxg_mp_ldl(sdpxg_ctx *ctx, uint32_t limbs, uint64_t n, const void *A, uint64_t lda,
+                     const void *reg, void *L, void *dinv, uint32_t *status);
+/* sdpxg_mp_ldl in place on device memory: d_A (n x n, ld lda) is overwritten with L, d_dinv (n)
+ * receives D^-1, d_reg NULL or (eps, delta) in device memory. */
+int32_t sdpxg_mp_ldl_device(sdpxg_ctx *ctx, uint32_t limbs, uint64_t n, void *d_A, uint64_t lda,
+                            const void *d_reg, void *d_dinv, uint32_t *status);
 /* Residue arithmetic of the exact products of this context: 0 = INT8 tensor cores (default),
  * 1 = FP64 CUDA cores.  The reference computes its per-prime products with FP64 dgemm
  * (rns_blas.rs:447-580); the result bits do not depend on the form. */

@@ -216,3 +216,121 @@ def congruence(n: int, ta: str, m: int, k: int, A: List[Mp], lda: int, X: List[M
             out.append(exact_sum_of_products(
                 n, [(at(i, a), X[a + b * ldx], at(j, b)) for a in range(k) for b in range(k)]))
     return out
+
+
+# ------------------------------------------------------------------------------------------
+# MpFloat arithmetic (each operation exact, then rounded once to 64n bits, ties to even: the
+# MPFR contract of crates/arithmetic/src/lib.rs) and the reference's dense MPFR LDL'
+# (crates/solver/src/solver/kkt/ldl/arrow.rs:156-242 ldl_dots, 255-420 ldl_rec,
+# 430-470 solve_unit_lower_t) for a dense matrix (row envelope all zero, no cut, sign +1).
+# ------------------------------------------------------------------------------------------
+REC_BASE = 128  # arrow.rs:63
+
+
+def mp_sub(n: int, a: Mp, b: Mp) -> Mp:
+    return from_fraction(n, a.fraction() - b.fraction())
+
+
+def mp_mul(n: int, a: Mp, b: Mp) -> Mp:
+    return from_fraction(n, a.fraction() * b.fraction())
+
+
+def mp_recip(n: int, d: Mp) -> Mp:
+    return from_fraction(n, 1 / d.fraction())
+
+
+def mp_from_float(n: int, x: float) -> Mp:
+    return from_fraction(n, Fraction(x))
+
+
+def mp_one(n: int) -> Mp:
+    return Mp(n, False, 1 << (64 * n - 1), 1)
+
+
+def _pivot(d: Mp, reg):
+    """DenseLeaf::pivot (arrow.rs:618-632) with sign +1: below eps becomes delta; zero fails."""
+    if reg is not None:
+        eps, delta = reg
+        if d.fraction() < eps.fraction():
+            d = delta
+    if d.is_zero():
+        raise ArithmeticError("zero_pivot")
+    return d
+
+
+def ldl_dots(n: int, A: List[Mp], lda: int, off: int, size: int, reg=None):
+    """arrow.rs:156-242 on the diagonal block at (off, off) of A (column-major, lower triangle
+    read and overwritten with the unit lower L); returns the block's D^-1.  Every dot is exact
+    and rounded once; differences, products and the reciprocal are rounded once each."""
+    def at(i, j):
+        return A[off + i + (off + j) * lda]
+    r = [[None] * size for _ in range(size)]  # r[i][j] = L(i, j), j < i
+    w = [[None] * size for _ in range(size)]  # w[i][j] = L(i, j) d_j
+    dinv = [None] * size
+    for j in range(size):
+        rj = [(r[j][c], w[j][c]) for c in range(j)]
+        dj = mp_sub(n, at(j, j), exact_dot(n, rj))
+        if dj.is_zero() and rj:  # the exact difference rounded once (arrow.rs:190-197)
+            dj = from_fraction(n, at(j, j).fraction() - sum(x.fraction() * y.fraction() for x, y in rj))
+        dj = _pivot(dj, reg)
+        dinv[j] = mp_recip(n, dj)
+        for i in range(j + 1, size):
+            dot = exact_dot(n, [(r[i][c], w[j][c]) for c in range(j)])
+            v = mp_mul(n, mp_sub(n, at(i, j), dot), dinv[j])
+            r[i][j] = v
+            w[i][j] = mp_mul(n, v, dj)
+    for j in range(size):
+        A[off + j + (off + j) * lda] = mp_one(n)
+        for i in range(j + 1, size):
+            A[off + i + (off + j) * lda] = r[i][j]
+    return dinv
+
+
+def solve_unit_lower_t(n: int, m: int, k: int, L: List[Mp], ldl: int, loff: int, B: List[Mp], ldb: int,
+                       boff_r: int, boff_c: int):
+    """X L' = B (arrow.rs:430-470) for B m x k at (boff_r, boff_c) of B, L unit lower k x k at
+    (loff, loff) of L; X overwrites B."""
+    def lt(i, j):
+        return L[loff + i + (loff + j) * ldl]
+
+    def bt(i, j):
+        return B[boff_r + i + (boff_c + j) * ldb]
+    if k <= REC_BASE:
+        for i in range(m):
+            x = [bt(i, j) for j in range(k)]
+            for j in range(k):
+                x[j] = mp_sub(n, x[j], exact_dot(n, [(x[c], lt(j, c)) for c in range(j)]))
+            for j in range(k):
+                B[boff_r + i + (boff_c + j) * ldb] = x[j]
+        return
+    k1, k2 = k // 2, k - k // 2
+    solve_unit_lower_t(n, m, k1, L, ldl, loff, B, ldb, boff_r, boff_c)
+    # B2 -= B1 L21' with L21 = L(k1:, :k1), each entry exact and rounded once, then subtracted
+    for j in range(k2):
+        for i in range(m):
+            p = exact_dot(n, [(bt(i, c), lt(k1 + j, c)) for c in range(k1)])
+            B[boff_r + i + (boff_c + k1 + j) * ldb] = mp_sub(n, bt(i, k1 + j), p)
+    solve_unit_lower_t(n, m, k2, L, ldl, loff + k1, B, ldb, boff_r, boff_c + k1)
+
+
+def ldl_rec(n: int, A: List[Mp], lda: int, off: int, size: int, reg=None) -> List[Mp]:
+    """arrow.rs:255-420 for a dense block (no envelope cut): halves, W21 = A21 L11^-T,
+    L21 = W21 D1^-1, then A22(b, a) -= (W21 L21')(a, b) for b >= a (one exact product per
+    entry, rounded once, then subtracted), recursion; blocks up to REC_BASE take ldl_dots.
+    Returns D^-1."""
+    if size <= REC_BASE:
+        return ldl_dots(n, A, lda, off, size, reg)
+    n1, n2 = size // 2, size - size // 2
+    d1 = ldl_rec(n, A, lda, off, n1, reg)
+    solve_unit_lower_t(n, n2, n1, A, lda, off, A, lda, off + n1, off)
+    W = [[A[off + n1 + i + (off + j) * lda] for j in range(n1)] for i in range(n2)]
+    for j in range(n1):
+        for i in range(n2):
+            A[off + n1 + i + (off + j) * lda] = mp_mul(n, W[i][j], d1[j])
+    for a in range(n2):
+        for b in range(a, n2):
+            p = exact_dot(n, [(W[a][c], A[off + n1 + b + (off + c) * lda]) for c in range(n1)])
+            idx = off + n1 + b + (off + n1 + a) * lda
+            A[idx] = mp_sub(n, A[idx], p)
+    d2 = ldl_rec(n, A, lda, off + n1, n2, reg)
+    return d1 + d2

@@ -31,6 +31,7 @@ enum SdpxgStatus : uint32_t {
   SDPXG_ST_PIVOT_FAIL = 8u,       // clearly negative or non-finite Schur pivot
   SDPXG_ST_EIG_FAIL = 16u,        // eigenvalue bisection did not converge
   SDPXG_ST_SYNC_TIMEOUT = 32u,    // a bounded inter-CTA wait gave up (no progress)
+  SDPXG_ST_EXACT_SPREAD = 64u,    // an exact dot's terms spread beyond the device accumulator
 };
 
 // Device-resident control of one refined KKT solve: the stopping rules of the two-level

@@ -1,0 +1,169 @@
+// MPFR dense LDL' kernels on MpFloat<N> arrays (see mp_ldl.cuh and mp.cuh).
+#include <stdexcept>
+
+#include "device.cuh"
+#include "mp.cuh"
+#include "mp_ldl.cuh"
+
+namespace sdpxg {
+namespace {
+
+using mpd::Val;
+
+__device__ __forceinline__ unsigned char* el(unsigned char* A, long i, long j, long ld, int N) {
+  return A + (i + j * ld) * (8L * N + 8);
+}
+__device__ __forceinline__ const unsigned char* el(const unsigned char* A, long i, long j, long ld, int N) {
+  return A + (i + j * ld) * (8L * N + 8);
+}
+
+// arrow.rs:156-242 ldl_dots on one block: columns in order; the CTA's thread 0 forms the pivot
+// d_j = a_jj - dot(r_j, w_j) (the exact difference rounded once when that rounds to zero), the
+// pivot rule, D^-1; then every later row i: r_ij = (a_ij - dot(r_i, w_j)) * d_j^-1,
+// w_ij = r_ij d_j.  Dots are exact and rounded once; the other operations round once each.
+__global__ void __launch_bounds__(128) k_mp_ldl_dots(unsigned char* A, long lda, int off, int size, int N,
+                                                     unsigned char* W, unsigned char* dinv,
+                                                     const unsigned char* reg, uint32_t* status) {
+  __shared__ __align__(8) unsigned char sd[8 * mpd::kMaxN + 8];  // d_j
+  __shared__ int s_fail;
+  unsigned char* B = A + ((long)off + (long)off * lda) * (8L * N + 8);
+  if (threadIdx.x == 0) s_fail = 0;
+  __syncthreads();
+  for (int j = 0; j < size; ++j) {
+    if (threadIdx.x == 0) {
+      bool ok = true;
+      const Val a = mpd::mp_load(el(B, j, j, lda, N), N);
+      const Val dot = mpd::mp_dot_sub(nullptr, el(B, j, 0, lda, N), lda, el(W, j, 0, size, N), size, j, N, &ok);
+      Val d = mpd::mp_addsub(a, dot, -1, N);
+      if (d.zero && j > 0) d = mpd::mp_dot_sub(&a, el(B, j, 0, lda, N), lda, el(W, j, 0, size, N), size, j, N, &ok);
+      if (reg) {  // DenseLeaf::pivot (arrow.rs:618-632), sign +1
+        const Val eps = mpd::mp_load(reg, N), delta = mpd::mp_load(reg + 8 * N + 8, N);
+        if (mpd::mp_cmp(d, eps, N) < 0) d = delta;
+      }
+      if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
+      if (d.zero) {
+        atomicOr(status, SDPXG_ST_PIVOT_FAIL);
+        s_fail = 1;
+      } else {
+        mpd::mp_store(sd, N, d, status);
+        mpd::mp_store(dinv + (long)j * (8L * N + 8), N, mpd::mp_recip(d, N), status);
+      }
+    }
+    __syncthreads();
+    if (s_fail) return;
+    const Val d = mpd::mp_load(sd, N);
+    const Val di = mpd::mp_load(dinv + (long)j * (8L * N + 8), N);
+    for (int i = j + 1 + threadIdx.x; i < size; i += blockDim.x) {
+      bool ok = true;
+      const Val a = mpd::mp_load(el(B, i, j, lda, N), N);
+      const Val dot = mpd::mp_dot_sub(nullptr, el(B, i, 0, lda, N), lda, el(W, j, 0, size, N), size, j, N, &ok);
+      if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
+      const Val v = mpd::mp_mul(mpd::mp_addsub(a, dot, -1, N), di, N);
+      mpd::mp_store(el(B, i, j, lda, N), N, v, status);
+      mpd::mp_store(el(W, i, j, size, N), N, mpd::mp_mul(v, d, N), status);
+    }
+    __syncthreads();
+  }
+  for (int j = threadIdx.x; j < size; j += blockDim.x) {  // unit diagonal
+    Val one = mpd::mp_zero();
+    one.zero = false;
+    one.m[N - 1] = 1ull << 63;
+    one.s = 1 - 64LL * N;
+    mpd::mp_store(el(B, j, j, lda, N), N, one, status);
+  }
+}
+
+// arrow.rs:437-447: each row of B solves x L' = b by exact dots, x_j = b_j - dot(x_<j, L(j, <j)).
+__global__ void k_mp_solve_lt(const unsigned char* L, long ldl, int k, unsigned char* B, long ldb, int m, int N,
+                              uint32_t* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  for (int j = 0; j < k; ++j) {
+    bool ok = true;
+    const Val x = mpd::mp_load(el(B, i, j, ldb, N), N);
+    const Val dot = mpd::mp_dot_sub(nullptr, el(B, i, 0, ldb, N), ldb, el(L, j, 0, ldl, N), ldl, j, N, &ok);
+    if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
+    mpd::mp_store(el(B, i, j, ldb, N), N, mpd::mp_addsub(x, dot, -1, N), status);
+  }
+}
+
+__global__ void k_mp_sub_block(unsigned char* B, long ldb, const unsigned char* P, long ldp, int m, int n, int N,
+                               uint32_t* status) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)m * n) return;
+  const int i = (int)(idx % m), j = (int)(idx / m);
+  const Val b = mpd::mp_load(el(B, i, j, ldb, N), N), p = mpd::mp_load(el(P, i, j, ldp, N), N);
+  mpd::mp_store(el(B, i, j, ldb, N), N, mpd::mp_addsub(b, p, -1, N), status);
+}
+
+__global__ void k_mp_copy_scale_cols(unsigned char* A, long lda, unsigned char* W, const unsigned char* d, int m,
+                                     int n, int N, uint32_t* status) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)m * n) return;
+  const int i = (int)(idx % m), j = (int)(idx / m);
+  const long esz = 8L * N + 8;
+  const Val a = mpd::mp_load(el(A, i, j, lda, N), N);
+  unsigned char* w = el(W, i, j, m, N);
+  const unsigned char* src = el(A, i, j, lda, N);
+  for (long b = 0; b < esz; ++b) w[b] = src[b];
+  mpd::mp_store(el(A, i, j, lda, N), N, mpd::mp_mul(a, mpd::mp_load(d + (long)j * esz, N), N), status);
+}
+
+__global__ void k_mp_sub_upper_t(unsigned char* A, long lda, const unsigned char* C, long ldc, int n, int N,
+                                 uint32_t* status) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)n * n) return;
+  const int b = (int)(idx % n), a = (int)(idx / n);  // entry (b, a) of the lower triangle
+  if (b < a) return;
+  const Val x = mpd::mp_load(el(A, b, a, lda, N), N), c = mpd::mp_load(el(C, a, b, ldc, N), N);
+  mpd::mp_store(el(A, b, a, lda, N), N, mpd::mp_addsub(x, c, -1, N), status);
+}
+
+void check_limbs(int N) {
+  if (N < 1 || N > mpd::kMaxN) throw std::invalid_argument("MPFR LDL: limbs must be in 1..8");
+}
+
+}  // namespace
+
+void mp_launch_ldl_dots(unsigned char* A, long lda, int off, int size, int N, unsigned char* W, unsigned char* dinv,
+                        const unsigned char* reg, uint32_t* status, cudaStream_t st) {
+  check_limbs(N);
+  if (size <= 0) return;
+  if (size > kMpRecBase) throw std::invalid_argument("MPFR LDL: leaf above the recursion base");
+  ++g_launches, k_mp_ldl_dots<<<1, 128, 0, st>>>(A, lda, off, size, N, W, dinv, reg, status);
+  check(cudaGetLastError(), "k_mp_ldl_dots");
+}
+
+void mp_launch_solve_lt(const unsigned char* L, long ldl, int k, unsigned char* B, long ldb, int m, int N,
+                        uint32_t* status, cudaStream_t st) {
+  check_limbs(N);
+  if (m <= 0 || k <= 0) return;
+  ++g_launches, k_mp_solve_lt<<<(m + 63) / 64, 64, 0, st>>>(L, ldl, k, B, ldb, m, N, status);
+  check(cudaGetLastError(), "k_mp_solve_lt");
+}
+
+void mp_launch_sub_block(unsigned char* B, long ldb, const unsigned char* P, long ldp, int m, int n, int N,
+                         uint32_t* status, cudaStream_t st) {
+  if (m <= 0 || n <= 0) return;
+  ++g_launches, k_mp_sub_block<<<(unsigned)(((long)m * n + 127) / 128), 128, 0, st>>>(B, ldb, P, ldp, m, n, N,
+                                                                                      status);
+  check(cudaGetLastError(), "k_mp_sub_block");
+}
+
+void mp_launch_copy_scale_cols(unsigned char* A, long lda, unsigned char* W, const unsigned char* d, int m, int n,
+                               int N, uint32_t* status, cudaStream_t st) {
+  if (m <= 0 || n <= 0) return;
+  ++g_launches, k_mp_copy_scale_cols<<<(unsigned)(((long)m * n + 127) / 128), 128, 0, st>>>(A, lda, W, d, m, n, N,
+                                                                                            status);
+  check(cudaGetLastError(), "k_mp_copy_scale_cols");
+}
+
+void mp_launch_sub_upper_t(unsigned char* A, long lda, const unsigned char* C, long ldc, int n, int N,
+                           uint32_t* status, cudaStream_t st) {
+  if (n <= 0) return;
+  ++g_launches, k_mp_sub_upper_t<<<(unsigned)(((long)n * n + 127) / 128), 128, 0, st>>>(A, lda, C, ldc, n, N,
+                                                                                        status);
+  check(cudaGetLastError(), "k_mp_sub_upper_t");
+}
+
+}  // namespace sdpxg

@@ -1,0 +1,34 @@
+// Kernels of the MPFR dense LDL' on the GPU (the reference's ArrowLDLSolver dense leaf,
+// crates/solver/src/solver/kkt/ldl/arrow.rs:156-470), on MpFloat<N> arrays in device memory
+// (column-major, element size 8N + 8).  The recursion that drives them, with its exact products,
+// lives beside the RNS product (rns.cu).
+#pragma once
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace sdpxg {
+
+constexpr int kMpRecBase = 128;  // arrow.rs:63 REC_BASE: blocks up to this order take exact dots
+constexpr int kMpMaxLimbs = 8;   // up to 512-bit values on the device
+
+// Left-looking exact-dot LDL' of the order-`size` diagonal block at (off, off) of A (lower
+// triangle read and overwritten with the unit lower L), D^-1 into dinv[0..size); W is a
+// size x size scratch.  reg: NULL or (eps, delta) as two MpFloat values (the pivot rule).
+void mp_launch_ldl_dots(unsigned char* A, long lda, int off, int size, int N, unsigned char* W,
+                        unsigned char* dinv, const unsigned char* reg, uint32_t* status, cudaStream_t st);
+// X L' = B for the m rows of B (m x k, ld ldb) with L unit lower k x k (ld ldl), k <= 128:
+// each row by exact dots (arrow.rs:437-447).
+void mp_launch_solve_lt(const unsigned char* L, long ldl, int k, unsigned char* B, long ldb, int m, int N,
+                        uint32_t* status, cudaStream_t st);
+// B -= P (m x n blocks, rounded once per entry).
+void mp_launch_sub_block(unsigned char* B, long ldb, const unsigned char* P, long ldp, int m, int n, int N,
+                         uint32_t* status, cudaStream_t st);
+// W = A (m x n block, ld m), then A(:, j) *= d[j] (rounded): L21 = W21 D1^-1.
+void mp_launch_copy_scale_cols(unsigned char* A, long lda, unsigned char* W, const unsigned char* d, int m, int n,
+                               int N, uint32_t* status, cudaStream_t st);
+// A(b, a) -= C(a, b) for b >= a (the Schur update of the lower triangle from the upper product).
+void mp_launch_sub_upper_t(unsigned char* A, long lda, const unsigned char* C, long ldc, int n, int N,
+                           uint32_t* status, cudaStream_t st);
+
+}  // namespace sdpxg

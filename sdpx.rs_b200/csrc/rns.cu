@@ -46,6 +46,7 @@
 #include "../../include/sdpx_b200.h"
 #include "engine.cuh"
 #include "i8_gemm.cuh"
+#include "mp_ldl.cuh"
 
 using namespace sdpxg;
 
@@ -781,6 +782,63 @@ int32_t rns_congruence(RnsWorkspace& ws, cudaStream_t st, int N, char ta, uint64
   return 0;
 }
 
+// The reference's dense MPFR LDL' (ArrowLDLSolver::try_dense -> ldl_rec, arrow.rs:255-470) on
+// device MpFloat<N> arrays: blocks up to 128 by the exact-dot kernel, larger blocks halved with
+// W21 = A21 L11^-T (solve_lt), L21 = W21 D1^-1 and A22 -= W21 L21' as one exact product (INT8
+// tensor-core RNS, every entry rounded once) then subtracted.  Status bits accumulate in *status.
+struct MpLdl {
+  RnsWorkspace& ws;
+  cudaStream_t st;
+  int N;
+  const unsigned char* reg;  // device (eps, delta) or null
+  uint32_t* status;          // device status word
+  size_t esz() const { return 8 * (size_t)N + 8; }
+
+  // the exact product C = op(A) op(B) (m x n, ld m) into C
+  void product(char ta, char tb, int m, int n, int k, const unsigned char* A, long lda, const unsigned char* B,
+               long ldb, int upper, DevBuf<unsigned char>& C) {
+    C.alloc((size_t)m * n * esz());
+    uint32_t hs = 0;
+    if (rns_product(ws, st, 0, N, ta, tb, m, n, k, A, lda, B, ldb, upper, C, &hs) != 0)
+      throw std::runtime_error(g_last_error);
+    if (hs) throw std::runtime_error("MPFR LDL: exact product reported status " + std::to_string(hs));
+  }
+  // X L' = B, L unit lower k x k (ld ldl), B m x k (ld ldb), X over B (arrow.rs:430-470)
+  void solve_lt(const unsigned char* L, long ldl, int k, unsigned char* B, long ldb, int m) {
+    if (m <= 0 || k <= 0) return;
+    if (k <= kMpRecBase) {
+      mp_launch_solve_lt(L, ldl, k, B, ldb, m, N, status, st);
+      return;
+    }
+    const int k1 = k / 2, k2 = k - k1;
+    solve_lt(L, ldl, k1, B, ldb, m);
+    DevBuf<unsigned char> P;
+    product('N', 'T', m, k2, k1, B, ldb, L + (size_t)k1 * esz(), ldl, 0, P);  // B1 L21'
+    mp_launch_sub_block(B + (size_t)k1 * ldb * esz(), ldb, P, m, m, k2, N, status, st);
+    solve_lt(L + ((size_t)k1 + (size_t)k1 * ldl) * esz(), ldl, k2, B + (size_t)k1 * ldb * esz(), ldb, m);
+  }
+  // arrow.rs:255-420 on the diagonal block at (off, off), size `size`; D^-1 into dinv + off
+  void ldl_rec(unsigned char* A, long lda, int off, int size, unsigned char* dinv, DevBuf<unsigned char>& Wleaf) {
+    if (size <= kMpRecBase) {
+      mp_launch_ldl_dots(A, lda, off, size, N, Wleaf, dinv + (size_t)off * esz(), reg, status, st);
+      return;
+    }
+    const int n1 = size / 2, n2 = size - n1;
+    ldl_rec(A, lda, off, n1, dinv, Wleaf);
+    unsigned char* A11 = A + ((size_t)off + (size_t)off * lda) * esz();
+    unsigned char* A21 = A + ((size_t)off + n1 + (size_t)off * lda) * esz();
+    solve_lt(A11, lda, n1, A21, lda, n2);  // W21 = A21 L11^-T in place
+    DevBuf<unsigned char> W, C;
+    W.alloc((size_t)n2 * n1 * esz());
+    mp_launch_copy_scale_cols(A21, lda, W, dinv + (size_t)off * esz(), n2, n1, N, status, st);  // L21 = W21 D1^-1
+    // (W L21')(a, b) for a <= b, subtracted from A22(b, a)
+    product('N', 'T', n2, n2, n1, W, n2, A21, lda, 1, C);
+    unsigned char* A22 = A + ((size_t)off + n1 + ((size_t)off + n1) * lda) * esz();
+    mp_launch_sub_upper_t(A22, lda, C, n2, n2, N, status, st);
+    ldl_rec(A, lda, off + n1, n2, dinv, Wleaf);
+  }
+};
+
 RnsWorkspace& workspace(sdpxg_ctx* ctx) {
   auto slot = ctx_rns_slot(ctx);
   if (!*slot) *slot = std::make_shared<RnsWorkspace>();
@@ -954,6 +1012,86 @@ extern "C" int32_t sdpxg_rns_congruence(sdpxg_ctx* ctx, uint32_t limbs, char ta,
     if (rc) return rc;
     copy_d2h(C, ws.c.p, m * m * esz, st);
     check(cudaStreamSynchronize(st), "sync");
+    return 0;
+  } catch (const std::invalid_argument& e) {
+    g_last_error = e.what();
+    return 1;
+  } catch (const std::exception& e) {
+    g_last_error = std::string("internal error: ") + e.what();
+    return 5;
+  } catch (...) {
+    g_last_error = "internal error";
+    return 5;
+  }
+}
+
+extern "C" int32_t sdpxg_mp_ldl_device(sdpxg_ctx* ctx, uint32_t limbs, uint64_t n, void* d_A, uint64_t lda,
+                                       const void* d_reg, void* d_dinv, uint32_t* status) {
+  try {
+    Engine* E = ctx_engine_any(ctx);
+    if (!E) throw std::invalid_argument("null context");
+    const int N = (int)limbs;
+    if (N < 1 || N > kMpMaxLimbs) {
+      g_last_error = "sdpxg_mp_ldl: limbs must be in 1..8";
+      return 2;
+    }
+    if (n == 0) return 0;
+    if (n > (1u << 20) || lda < n) throw std::invalid_argument("bad size or leading dimension");
+    if (!d_A || !d_dinv) throw std::invalid_argument("null pointer");
+    check(cudaSetDevice(E->device), "cudaSetDevice");
+    if (!device_memory(d_A) || !device_memory(d_dinv) || (d_reg && !device_memory(d_reg)))
+      throw std::invalid_argument("sdpxg_mp_ldl_device: A, reg and dinv must be device pointers");
+    RnsWorkspace& ws = workspace(ctx);
+    DevBuf<uint32_t> stw(1);
+    check(cudaMemsetAsync(stw.p, 0, sizeof(uint32_t), E->st), "memset");
+    MpLdl f{ws, E->st, N, static_cast<const unsigned char*>(d_reg), stw.p};
+    DevBuf<unsigned char> Wleaf((size_t)kMpRecBase * kMpRecBase * f.esz());
+    f.ldl_rec(static_cast<unsigned char*>(d_A), (long)lda, 0, (int)n, static_cast<unsigned char*>(d_dinv), Wleaf);
+    uint32_t hs = 0;
+    copy_d2h(&hs, stw.p, sizeof(uint32_t), E->st);
+    check(cudaStreamSynchronize(E->st), "sync");
+    if (status) *status = hs;
+    if (hs & SDPXG_ST_EXACT_SPREAD) {
+      g_last_error = "sdpxg_mp_ldl: an exact dot's exponent spread exceeds the device accumulator";
+      return 2;
+    }
+    return 0;
+  } catch (const std::invalid_argument& e) {
+    g_last_error = e.what();
+    return 1;
+  } catch (const std::exception& e) {
+    g_last_error = std::string("internal error: ") + e.what();
+    return 5;
+  } catch (...) {
+    g_last_error = "internal error";
+    return 5;
+  }
+}
+
+extern "C" int32_t sdpxg_mp_ldl(sdpxg_ctx* ctx, uint32_t limbs, uint64_t n, const void* A, uint64_t lda,
+                                const void* reg, void* L, void* dinv, uint32_t* status) {
+  try {
+    Engine* E = ctx_engine_any(ctx);
+    if (!E) throw std::invalid_argument("null context");
+    const int N = (int)limbs;
+    if (N < 1 || N > kMpMaxLimbs) {
+      g_last_error = "sdpxg_mp_ldl: limbs must be in 1..8";
+      return 2;
+    }
+    if (n == 0) return 0;
+    if (n > (1u << 20) || lda < n) throw std::invalid_argument("bad size or leading dimension");
+    if (!A || !L || !dinv) throw std::invalid_argument("null pointer");
+    const size_t esz = 8 * (size_t)N + 8;
+    check(cudaSetDevice(E->device), "cudaSetDevice");
+    DevBuf<unsigned char> dA(n * n * esz), dD(n * esz), dR(2 * esz);
+    check(cudaMemcpy2DAsync(dA.p, n * esz, A, lda * esz, n * esz, n, cudaMemcpyHostToDevice, E->st), "H2D");
+    g_h2d_bytes += n * n * esz;
+    if (reg) dR.upload(static_cast<const unsigned char*>(reg), 2 * esz, E->st);
+    const int32_t rc = sdpxg_mp_ldl_device(ctx, limbs, n, dA.p, n, reg ? dR.p : nullptr, dD.p, status);
+    if (rc) return rc;
+    copy_d2h(L, dA.p, n * n * esz, E->st);
+    copy_d2h(dinv, dD.p, n * esz, E->st);
+    check(cudaStreamSynchronize(E->st), "sync");
     return 0;
   } catch (const std::invalid_argument& e) {
     g_last_error = e.what();

@@ -537,6 +537,17 @@ class KernelContext:
                   C.c_char_p(X), ldx, int(upper_only), out, C.byref(st))
         return out.raw[:m * m * esz], st.value
 
+    def mp_ldl(self, limbs: int, n: int, A: bytes, lda: int, reg: Optional[bytes] = None):
+        """The reference's dense MPFR LDL' of an n x n MpFloat<limbs> matrix (raw bytes):
+        returns (L bytes n x n, dinv bytes n, status)."""
+        esz = 8 * limbs + 8
+        L = C.create_string_buffer(max(n * n * esz, 1))
+        D = C.create_string_buffer(max(n * esz, 1))
+        st = C.c_uint32()
+        _lib.call("sdpxg_mp_ldl", self._h, limbs, n, C.c_char_p(A), lda,
+                  C.c_char_p(reg) if reg is not None else None, L, D, C.byref(st))
+        return L.raw[:n * n * esz], D.raw[:n * esz], st.value
+
     def rns_gemm_device(self, limbs: int, ta: str, tb: str, m: int, n: int, k: int, d_A: int,
                         lda: int, d_B: int, ldb: int, d_C: int, upper_only: bool = False):
         """Exact product on device buffers (addresses of MpFloat arrays in device memory)."""
