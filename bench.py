@@ -538,6 +538,72 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+def run_i8(args, world, rank, local):
+    """INT8 tensor-core GEMM microbenchmark: the cuBLASLt INT8 peak (torch._int_mm 8192^3), the
+    split-precision DGEMM (Ozaki-II, 16 INT8 modular products) of --size^3 against cuBLAS DGEMM,
+    and the exact 256-bit RNS product of --size^3 (INT8 form) -- each with the INT8 kernel's own
+    event-timed TOP/s."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    from sdpx_b200.solver import KernelContext
+    n, reps = args.size, args.reps
+    ctx = KernelContext(local)
+    rng = np.random.default_rng(3)
+    A = torch.from_numpy(rng.standard_normal((n, n))).cuda()
+    B = torch.from_numpy(rng.standard_normal((n, n))).cuda()
+    C = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    split = lambda: ctx.split_dgemm_device("N", "N", n, n, n, 1.0, A.data_ptr(), n, B.data_ptr(), n, 0.0,
+                                           C.data_ptr(), n)
+    split()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        split()
+    t_split = (time.perf_counter() - t0) / reps
+    ms, ops, alg, cnt = i8_measure(split)
+    # column-major device buffers: C = A B in BLAS terms is B^T A^T on torch's row-major views
+    ref = (A.T @ B.T).T
+    err = float((C - ref).abs().max() / ref.abs().max())
+    torch.cuda.synchronize()
+    s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s_.record()
+    for _ in range(reps):
+        torch.matmul(A, B)
+    e_.record()
+    torch.cuda.synchronize()
+    t_dgemm = s_.elapsed_time(e_) / 1e3 / reps
+    del A, B, C, ref
+    torch.cuda.empty_cache()
+    peak = int8_peak()
+    limbs, esz = 4, 40
+    dA = torch.from_numpy(np.frombuffer(_random_mp(n * n, limbs, rng), dtype=np.uint8).copy()).cuda()
+    dB = torch.from_numpy(np.frombuffer(_random_mp(n * n, limbs, rng), dtype=np.uint8).copy()).cuda()
+    dC = torch.zeros(n * n * esz, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    rns = lambda: ctx.rns_gemm_device(limbs, "N", "N", n, n, n, dA.data_ptr(), n, dB.data_ptr(), n, dC.data_ptr())
+    rns()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        rns()
+    t_rns = (time.perf_counter() - t0) / reps
+    rms, rops, ralg, rcnt = i8_measure(rns)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "INT8 tensor-core GEMM throughput (tcgen05 kind::i8 modular GEMM)", "value": ops / ms / 1e9,
+            "unit": "TOP/s", "n_gpus": 1, "steps": reps, "warmup": 1, "higher_is_better": True,
+            "data": "synthetic", "int8_peak_tops": peak,
+            "split_dgemm": {"n": n, "s": t_split, "tflops_fp64_equivalent": 2.0 * n ** 3 / t_split / 1e12,
+                            "cublas_dgemm_s": t_dgemm, "dgemm_over_split": t_dgemm / t_split,
+                            "max_rel_err_vs_dgemm": err, "i8_gemm_ms": ms, "i8_launches": cnt,
+                            "i8_tops_executed": ops / ms / 1e9, "i8_tops_algorithmic": alg / ms / 1e9,
+                            "frac_of_int8_peak": ops / ms / 1e9 / peak},
+            "rns_256": {"n": n, "s": t_rns, "i8_gemm_ms": rms, "i8_launches": rcnt,
+                        "i8_tops_executed": rops / rms / 1e9, "i8_tops_algorithmic": ralg / rms / 1e9,
+                        "frac_of_int8_peak": rops / rms / 1e9 / peak}}))
+    return 0
+
+
 BATCH_METRIC = "instances/s to gap 1e-8 (Float64), batch of independent small SDPs"
 
 
@@ -689,7 +755,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--quick", action="store_true",
                     help="skip the nested precision-workload and 256-bit RNS measurements")
-    ap.add_argument("--workload", default="rank1", choices=["rank1", "batch", "adjoint"],
+    ap.add_argument("--size", type=int, default=2048, help="i8 workload: matrix order")
+    ap.add_argument("--reps", type=int, default=3, help="i8 workload: timed repetitions")
+    ap.add_argument("--workload", default="rank1", choices=["rank1", "batch", "adjoint", "i8"],
                     help="rank1: the 32-block bootstrap SDP (default line); batch: independent "
                          "small SDPs, instances/s; adjoint: conic QPs solved and differentiated")
     ap.add_argument("--instances", type=int, default=None,
@@ -703,6 +771,8 @@ def main():
     try:
         if args.impl == "reference":
             rc = run_reference(args, world, rank)
+        elif args.workload == "i8":
+            rc = run_i8(args, world, rank, local)
         elif args.workload == "batch":
             rc = run_batch(args, world, rank, local)
         elif args.workload == "adjoint":

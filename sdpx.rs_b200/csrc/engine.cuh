@@ -1124,6 +1124,10 @@ class Engine {
     tbegin(KT_FACTOR);
     launch_chol(sub1_.b, eps, dynamic, dyn_eps, dyn_delta);
     tend(KT_FACTOR);
+    // the inverse kernels write the upper triangles only; the split-precision products read
+    // X11 and X22 whole, so their lower triangles must be zeros, not a recycled block's contents
+    check(cudaMemsetAsync(sub1_.Uinv.p, 0, (size_t)n1 * n1 * sizeof(double), st), "memset");
+    check(cudaMemsetAsync(sub2_.Uinv.p, 0, (size_t)n2 * n2 * sizeof(double), st), "memset");
     tbegin(KT_TRINV);
     launch_trinv(sub1_.b);
     tend(KT_TRINV);
