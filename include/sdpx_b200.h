@@ -151,6 +151,17 @@ int32_t sdpx_b200_set_i8_timing(int32_t on);
  * multiply-add over the padded tiles), algorithmic INT8 operations (2 m n k per digit pair and
  * modulus), launches. */
 int32_t sdpx_b200_i8_times(double *ms, double *ops, double *alg_ops, uint64_t *launches);
+/* Tile configuration of the INT8 tensor-core GEMM: -1 (default) autotuned -- the first launch of
+ * each shape class (digit count, power-of-two classes of the padded extents, K range and moduli)
+ * times every configuration on the real operands with CUDA events and keeps the fastest; results
+ * do not depend on the choice (exact integer arithmetic) -- or 0 / 1 to force a configuration
+ * (0: 128 x 256 tiles for single-digit and 128 x 128 for two-digit residues, 1: half-width tiles
+ * with a deeper stage ring).  SDPX_B200_AUTOTUNE=0 keeps configuration 0.  No counterpart in the
+ * reference (it tunes CPU tile sizes by constant). */
+int32_t sdpx_b200_i8_config(int32_t variant);
+/* The autotuner's table as text (one line per shape class), in the sdpx_result_decimal style:
+ * required receives the bytes needed including the terminating zero. */
+int32_t sdpx_b200_i8_tuning(char *out, uint64_t capacity, uint64_t *required);
 /* Bytes this library has copied host-to-device and device-to-host in this process (all
  * handles): the host-device traffic of prepare, solve and result reads. */
 int32_t sdpx_b200_transfer_bytes(uint64_t *h2d, uint64_t *d2h);

@@ -725,6 +725,20 @@ int32_t sdpx_b200_set_i8_timing(int32_t on) {
   return boundary([&] { sdpxg::i8_timing(on != 0); });
 }
 
+int32_t sdpx_b200_i8_config(int32_t variant) {
+  return boundary([&] {
+    if (variant < -1 || variant > 1) invalid("variant must be -1 (autotuned), 0 or 1");
+    sdpxg::i8_set_config(variant);
+  });
+}
+
+int32_t sdpx_b200_i8_tuning(char* out, uint64_t capacity, uint64_t* required) {
+  return boundary([&] {
+    const std::string t = sdpxg::i8_tuning_table();
+    output_bytes(t.c_str(), t.size() + 1, 1, out, capacity, required);
+  });
+}
+
 int32_t sdpx_b200_i8_times(double* ms, double* ops, double* alg_ops, uint64_t* launches) {
   return boundary([&] {
     if (!ms || !ops || !alg_ops || !launches) invalid("null pointer");

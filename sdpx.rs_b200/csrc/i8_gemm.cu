@@ -13,9 +13,13 @@
 // their next wait, outstanding TMA copies are drained (bounded) and TMEM is released before exit.
 #include <cuda.h>
 
+#include <array>
 #include <atomic>
+#include <cstdlib>
+#include <map>
 #include <mutex>
 #include <stdexcept>
+#include <cstdio>
 #include <string>
 
 #include "device.cuh"
@@ -29,26 +33,37 @@ constexpr int kBM = 128;     // rows per tile (MMA M)
 constexpr int kKB = 128;     // K bytes per stage (one 128-byte swizzle row)
 constexpr int kThreads = 192;
 
-template <int DIGITS>
+// Tile configurations: variant 0 (the default) and variant 1 (half the tile width, deeper
+// stage ring); the autotuner picks per shape class.  Every variant gives the same bits.
+template <int DIGITS, int VAR>
 struct Cfg;
 template <>
-struct Cfg<1> {
+struct Cfg<1, 0> {
   static constexpr int BN = 256, STAGES = 4, NACC = 1, TMEM_COLS = 256;
 };
 template <>
-struct Cfg<2> {
+struct Cfg<1, 1> {
+  static constexpr int BN = 128, STAGES = 6, NACC = 1, TMEM_COLS = 128;
+};
+template <>
+struct Cfg<2, 0> {
   static constexpr int BN = 128, STAGES = 3, NACC = 3, TMEM_COLS = 512;
 };
+template <>
+struct Cfg<2, 1> {
+  static constexpr int BN = 64, STAGES = 4, NACC = 3, TMEM_COLS = 256;
+};
 
-template <int DIGITS>
+template <int DIGITS, int VAR>
 constexpr int stage_bytes() {
-  return DIGITS * (kBM * kKB + Cfg<DIGITS>::BN * kKB);
+  return DIGITS * (kBM * kKB + Cfg<DIGITS, VAR>::BN * kKB);
 }
-template <int DIGITS>
+template <int DIGITS, int VAR>
 constexpr size_t smem_bytes() {
   // stages, then 2 * STAGES + 1 mbarriers, the TMEM address, the abort flag and the consumed
   // count, plus 1024 bytes to align the stage ring to the swizzle atom
-  return (size_t)Cfg<DIGITS>::STAGES * stage_bytes<DIGITS>() + (2 * Cfg<DIGITS>::STAGES + 1) * 8 + 16 + 1024;
+  return (size_t)Cfg<DIGITS, VAR>::STAGES * stage_bytes<DIGITS, VAR>() + (2 * Cfg<DIGITS, VAR>::STAGES + 1) * 8 + 16 +
+         1024;
 }
 
 __device__ __forceinline__ void give_up(volatile int* abort, int* err) {
@@ -56,12 +71,12 @@ __device__ __forceinline__ void give_up(volatile int* abort, int* err) {
   if (err) atomicOr(err, 1);
 }
 
-template <int DIGITS>
+template <int DIGITS, int VAR>
 __global__ void __launch_bounds__(kThreads, 1)
     k_i8_mod_gemm(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, I8GemmArgs a) {
-  constexpr int BN = Cfg<DIGITS>::BN, STAGES = Cfg<DIGITS>::STAGES, NACC = Cfg<DIGITS>::NACC;
-  constexpr int TCOLS = Cfg<DIGITS>::TMEM_COLS;
-  constexpr int SB = stage_bytes<DIGITS>();
+  constexpr int BN = Cfg<DIGITS, VAR>::BN, STAGES = Cfg<DIGITS, VAR>::STAGES, NACC = Cfg<DIGITS, VAR>::NACC;
+  constexpr int TCOLS = Cfg<DIGITS, VAR>::TMEM_COLS;
+  constexpr int SB = stage_bytes<DIGITS, VAR>();
   constexpr int A_TILE = kBM * kKB, B_TILE = BN * kKB;
   const int tm = blockIdx.x, tn = blockIdx.y, l = blockIdx.z;
   if (a.upper_only && tm * kBM > tn * BN + BN - 1) return;  // every entry of the tile has i > j
@@ -258,25 +273,20 @@ std::mutex g_i8_mu;
 double g_i8_ms = 0.0, g_i8_ops = 0.0, g_i8_alg_ops = 0.0;
 uint64_t g_i8_count = 0;
 
-template <int DIGITS>
-void launch(const int8_t* A, const int8_t* B, const I8GemmArgs& a, cudaStream_t st) {
-  constexpr int BN = Cfg<DIGITS>::BN;
-  if (a.Mpad <= 0 || a.Npad <= 0 || a.Kpad <= 0 || a.Mpad % kBM || a.Npad % BN || a.Kpad % kKB ||
-      a.Kld % kKB || a.k0 % kKB || a.k0 < 0 || a.k0 + a.Kpad > a.Kld)
-    throw std::invalid_argument("i8 GEMM: padded extents must be multiples of the tile");
-  if (a.m > a.Mpad || a.n > a.Npad || a.L <= 0 || a.L > 65535 || !a.moduli || !a.out)
-    throw std::invalid_argument("i8 GEMM: bad arguments");
-  if (a.Kpad > (1 << 17)) throw std::invalid_argument("i8 GEMM: K above 2^17 per call is not exact");
+// One launch of variant VAR (returns after queueing; with timing on, after the event).
+template <int DIGITS, int VAR>
+void launch_variant(const int8_t* A, const int8_t* B, const I8GemmArgs& a, cudaStream_t st, float* ms_out) {
+  constexpr int BN = Cfg<DIGITS, VAR>::BN;
   static std::once_flag attr;
   std::call_once(attr, [] {
-    check(cudaFuncSetAttribute(k_i8_mod_gemm<DIGITS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem_bytes<DIGITS>()),
+    check(cudaFuncSetAttribute(k_i8_mod_gemm<DIGITS, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem_bytes<DIGITS, VAR>()),
           "i8 gemm smem attribute");
   });
   const CUtensorMap ta = byte_map(A, (long)a.L * DIGITS * a.Mpad, a.Kld, kBM);
   const CUtensorMap tb = byte_map(B, (long)a.L * DIGITS * a.Npad, a.Kld, BN);
   const dim3 grid(a.Mpad / kBM, a.Npad / BN, a.L);
-  const bool timed = g_i8_timing.load() != 0;
+  const bool timed = ms_out != nullptr || g_i8_timing.load() != 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (timed) {
     check(cudaEventCreate(&e0), "event");
@@ -284,7 +294,7 @@ void launch(const int8_t* A, const int8_t* B, const I8GemmArgs& a, cudaStream_t 
     check(cudaEventRecord(e0, st), "event");
   }
   ++g_launches;
-  k_i8_mod_gemm<DIGITS><<<grid, kThreads, smem_bytes<DIGITS>(), st>>>(ta, tb, a);
+  k_i8_mod_gemm<DIGITS, VAR><<<grid, kThreads, smem_bytes<DIGITS, VAR>(), st>>>(ta, tb, a);
   check(cudaGetLastError(), "k_i8_mod_gemm launch");
   if (timed) {
     check(cudaEventRecord(e1, st), "event");
@@ -293,16 +303,91 @@ void launch(const int8_t* A, const int8_t* B, const I8GemmArgs& a, cudaStream_t 
     check(cudaEventElapsedTime(&ms, e0, e1), "event time");
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    double tiles = 0;  // tiles actually computed (upper_only skips those below the diagonal)
-    for (int tm = 0; tm < a.Mpad / kBM; ++tm)
-      for (int tn = 0; tn < a.Npad / BN; ++tn)
-        if (!(a.upper_only && tm * kBM > tn * BN + BN - 1)) tiles += 1;
-    std::lock_guard<std::mutex> lk(g_i8_mu);
-    g_i8_ms += ms;
-    g_i8_ops += 2.0 * DIGITS * DIGITS * tiles * kBM * BN * (double)a.Kpad * a.L;
-    g_i8_alg_ops += 2.0 * DIGITS * DIGITS * (double)a.m * a.n * (double)a.Kpad * a.L;
-    ++g_i8_count;
+    if (ms_out) *ms_out = ms;
+    if (g_i8_timing.load()) {
+      double tiles = 0;  // tiles actually computed (upper_only skips those below the diagonal)
+      for (int tm = 0; tm < a.Mpad / kBM; ++tm)
+        for (int tn = 0; tn < a.Npad / BN; ++tn)
+          if (!(a.upper_only && tm * kBM > tn * BN + BN - 1)) tiles += 1;
+      std::lock_guard<std::mutex> lk(g_i8_mu);
+      g_i8_ms += ms;
+      g_i8_ops += 2.0 * DIGITS * DIGITS * tiles * kBM * BN * (double)a.Kpad * a.L;
+      g_i8_alg_ops += 2.0 * DIGITS * DIGITS * (double)a.m * a.n * (double)a.Kpad * a.L;
+      ++g_i8_count;
+    }
   }
+}
+
+// Autotuner of the tile configuration.  A shape class is (digits, ceil log2 of Mpad, Npad and
+// the K range, moduli); the first launch of a class (outside stream capture, not accumulating
+// into an earlier chunk's residues) runs every variant on the real operands, times each with
+// CUDA events on the launch stream and keeps the fastest for the rest of the process.  All
+// variants compute the same exact integers, so the choice never changes a result.
+// SDPX_B200_AUTOTUNE=0 keeps variant 0; sdpx_b200_i8_config forces one.
+struct Tuner {
+  std::mutex mu;
+  std::map<std::array<int, 5>, std::pair<int, std::array<float, 2>>> table;
+  int forced = -1;
+  bool enabled = true;
+  Tuner() {
+    const char* e = std::getenv("SDPX_B200_AUTOTUNE");
+    enabled = !(e && e[0] == '0');
+  }
+};
+Tuner& tuner() {
+  static Tuner t;
+  return t;
+}
+int lg2(long v) {
+  int l = 0;
+  while ((1L << l) < v) ++l;
+  return l;
+}
+
+template <int DIGITS>
+void launch(const int8_t* A, const int8_t* B, const I8GemmArgs& a, cudaStream_t st) {
+  constexpr int BN = Cfg<DIGITS, 0>::BN;  // the padding rule: a multiple of every variant's width
+  static_assert(Cfg<DIGITS, 0>::BN % Cfg<DIGITS, 1>::BN == 0, "variant widths must divide the padding");
+  if (a.Mpad <= 0 || a.Npad <= 0 || a.Kpad <= 0 || a.Mpad % kBM || a.Npad % BN || a.Kpad % kKB ||
+      a.Kld % kKB || a.k0 % kKB || a.k0 < 0 || a.k0 + a.Kpad > a.Kld)
+    throw std::invalid_argument("i8 GEMM: padded extents must be multiples of the tile");
+  if (a.m > a.Mpad || a.n > a.Npad || a.L <= 0 || a.L > 65535 || !a.moduli || !a.out)
+    throw std::invalid_argument("i8 GEMM: bad arguments");
+  if (a.Kpad > (1 << 17)) throw std::invalid_argument("i8 GEMM: K above 2^17 per call is not exact");
+  Tuner& T = tuner();
+  const std::array<int, 5> key = {DIGITS, lg2(a.Mpad), lg2(a.Npad), lg2(a.Kpad), lg2(a.L)};
+  int var = 0;
+  bool tune = false;
+  {
+    std::lock_guard<std::mutex> lk(T.mu);
+    if (T.forced >= 0) {
+      var = T.forced;
+    } else if (T.enabled) {
+      auto it = T.table.find(key);
+      if (it != T.table.end()) {
+        var = it->second.first;
+      } else {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        check(cudaStreamIsCapturing(st, &cs), "capture status");
+        tune = cs == cudaStreamCaptureStatusNone && !a.accumulate;
+      }
+    }
+  }
+  if (!tune) {
+    if (var == 0)
+      launch_variant<DIGITS, 0>(A, B, a, st, nullptr);
+    else
+      launch_variant<DIGITS, 1>(A, B, a, st, nullptr);
+    return;
+  }
+  // warm both, then time both; variant 0 runs last and leaves its (identical) output
+  std::array<float, 2> ms = {0.f, 0.f};
+  launch_variant<DIGITS, 1>(A, B, a, st, &ms[1]);
+  launch_variant<DIGITS, 0>(A, B, a, st, &ms[0]);
+  launch_variant<DIGITS, 1>(A, B, a, st, &ms[1]);
+  launch_variant<DIGITS, 0>(A, B, a, st, &ms[0]);
+  std::lock_guard<std::mutex> lk(T.mu);
+  T.table[key] = {ms[1] < ms[0] ? 1 : 0, ms};
 }
 
 }  // namespace
@@ -319,6 +404,23 @@ void i8_times(double* ms, double* ops, double* alg_ops, uint64_t* count) {
   *ops = g_i8_ops;
   *alg_ops = g_i8_alg_ops;
   *count = g_i8_count;
+}
+
+void i8_set_config(int variant) {
+  std::lock_guard<std::mutex> lk(tuner().mu);
+  tuner().forced = variant;
+}
+std::string i8_tuning_table() {
+  std::lock_guard<std::mutex> lk(tuner().mu);
+  std::string out;
+  for (const auto& kv : tuner().table) {
+    char line[160];
+    std::snprintf(line, sizeof line, "digits %d Mpad<=2^%d Npad<=2^%d K<=2^%d L<=2^%d -> variant %d (%.4f ms, %.4f ms)\n",
+                  kv.first[0], kv.first[1], kv.first[2], kv.first[3], kv.first[4], kv.second.first,
+                  (double)kv.second.second[0], (double)kv.second.second[1]);
+    out += line;
+  }
+  return out;
 }
 
 void launch_i8_gemm(int digits, const int8_t* A, const int8_t* B, const I8GemmArgs& args, cudaStream_t st) {

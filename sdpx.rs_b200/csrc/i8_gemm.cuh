@@ -19,6 +19,7 @@
 // l * plane + j * m + i), only i < m, j < n written.
 #pragma once
 #include <cstdint>
+#include <string>
 
 #include <cuda_runtime.h>
 
@@ -51,5 +52,9 @@ void launch_i8_gemm(int digits, const int8_t* A, const int8_t* B, const I8GemmAr
 // algorithmic INT8 operations (2 m n K per digit pair and modulus) and the launch count.
 void i8_timing(int on);
 void i8_times(double* ms, double* ops, double* alg_ops, uint64_t* count);
+// Tile configuration of later launches: -1 autotuned (default), 0 or 1 a fixed variant; and the
+// autotuner's table (one line per shape class: the chosen variant and both timings).
+void i8_set_config(int variant);
+std::string i8_tuning_table();
 
 }  // namespace sdpxg

@@ -79,6 +79,8 @@ SIGNATURES = {
     "sdpx_b200_launch_count": (u64, []),
     "sdpx_b200_device_allocations": (u64, []),
     "sdpx_b200_set_i8_timing": (i32, [i32]),
+    "sdpx_b200_i8_config": (i32, [i32]),
+    "sdpx_b200_i8_tuning": (i32, [C.c_char_p, u64, PU64]),
     "sdpx_b200_i8_times": (i32, [PD, PD, PD, PU64]),
     "sdpx_b200_transfer_bytes": (i32, [PU64, PU64]),
     "sdpx_b200_schur_forms": (i32, [C.c_void_p, PU32, PU32]),
