@@ -331,6 +331,14 @@ int32_t sdpxg_rns_congruence(sdpxg_ctx *ctx, uint32_t limbs, char ta, uint64_t m
  * exponent spread exceeds the device accumulator returns 2. */
 int32_t sdpxg_mp_ldl(sdpxg_ctx *ctx, uint32_t limbs, uint64_t n, const void *A, uint64_t lda,
                      const void *reg, void *L, void *dinv, uint32_t *status);
+/* The reference's exact Cholesky XpotrfScalar::xpotrf for MpFloat<limbs> (algebra/dense/blas/
+ * mpfr.rs:726-789), in place on the host n x n matrix A (column-major, ld lda), uplo 'L' (lower
+ * triangle stored) or 'U': left-looking, every dot exact and rounded once, the differences, the
+ * square roots and the divisions rounded once (round to nearest, ties to even).  *info = 0, or
+ * j + 1 when pivot j is not positive (A then holds the factor up to it), as LAPACK's potrf.
+ * limbs 1..8. */
+int32_t sdpxg_mp_potrf(sdpxg_ctx *ctx, uint32_t limbs, char uplo, uint64_t n, void *A, uint64_t lda,
+                       int32_t *info, uint32_t *status);
 /* sdpxg_mp_ldl in place on device memory: d_A (n x n, ld lda) is overwritten with L, d_dinv (n)
  * receives D^-1, d_reg NULL or (eps, delta) in device memory. */
 int32_t sdpxg_mp_ldl_device(sdpxg_ctx *ctx, uint32_t limbs, uint64_t n, void *d_A, uint64_t lda,

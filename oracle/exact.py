@@ -334,3 +334,43 @@ def ldl_rec(n: int, A: List[Mp], lda: int, off: int, size: int, reg=None) -> Lis
             A[idx] = mp_sub(n, A[idx], p)
     d2 = ldl_rec(n, A, lda, off + n1, n2, reg)
     return d1 + d2
+
+
+def mp_div(n: int, a: Mp, b: Mp) -> Mp:
+    return from_fraction(n, a.fraction() / b.fraction())
+
+
+def mp_sqrt(n: int, a: Mp) -> Mp:
+    """Correctly rounded square root (ties to even) of a >= 0: the integer square root of the
+    scaled mantissa with the remainder as a sticky bit."""
+    if a.is_zero():
+        return Mp(n)
+    from math import isqrt
+    s = a.exp - a.p  # a = mant 2^s
+    e = 64 * n + 4
+    if (s - e) % 2:
+        e += 1
+    X = a.mant << e
+    y = isqrt(X)
+    sticky = 1 if y * y != X else 0
+    return from_scaled_integer(n, False, (y << 1) | sticky, (s - e) // 2 - 1)
+
+
+def xpotrf(n: int, uplo: str, size: int, A: List[Mp], lda: int) -> int:
+    """XpotrfScalar::xpotrf for MpFloat (algebra/dense/blas/mpfr.rs:726-789), in place; returns
+    info (0, or j + 1 at the first non-positive pivot)."""
+    lower = uplo == "L"
+
+    def at(i, k):
+        return i + k * lda if lower else k + i * lda
+    for j in range(size):
+        d = mp_sub(n, A[j + j * lda], exact_dot(n, [(A[at(j, k)], A[at(j, k)]) for k in range(j)]))
+        if d.is_zero() or d.neg:
+            A[j + j * lda] = d
+            return j + 1
+        d = mp_sqrt(n, d)
+        A[j + j * lda] = d
+        for i in range(j + 1, size):
+            solved = exact_dot(n, [(A[at(i, k)], A[at(j, k)]) for k in range(j)])
+            A[at(i, j)] = mp_div(n, mp_sub(n, A[at(i, j)], solved), d)
+    return 0

@@ -270,6 +270,123 @@ __device__ inline Val mp_recip(const Val& d, int N) {
   return mp_round(S, QW + 1, d.neg, -(long long)K - d.s - 1, N);
 }
 
+// a / b: the quotient of M_a 2^K (K = 64N + 2) by M_b by binary long division, remainder folded
+// into a sticky bit.  b must be nonzero.
+__device__ inline Val mp_div(const Val& a, const Val& b, int N) {
+  if (a.zero) {
+    Val z = mp_zero();
+    z.neg = a.neg != b.neg;
+    return z;
+  }
+  const int K = 64 * N + 2;
+  const int DB = 64 * N + K;  // dividend bits
+  unsigned long long Q[2 * kMaxN + 2] = {}, R[kMaxN + 1] = {};
+  for (int bit = DB - 1; bit >= 0; --bit) {
+    // next dividend bit: bit (bit - K) of M_a, zero below K
+    const int src = bit - K;
+    unsigned long long carry = (src >= 0) ? ((a.m[src >> 6] >> (src & 63)) & 1ull) : 0ull;
+    for (int w = 0; w <= N; ++w) {
+      const unsigned long long nc = R[w] >> 63;
+      R[w] = (R[w] << 1) | carry;
+      carry = nc;
+    }
+    int cmp = R[N] ? 1 : 0;
+    for (int w = N - 1; w >= 0 && !cmp; --w) cmp = R[w] > b.m[w] ? 1 : (R[w] < b.m[w] ? -1 : 0);
+    if (cmp >= 0) {
+      unsigned long long borrow = 0;
+      for (int w = 0; w <= N; ++w) {
+        const unsigned long long dm = w < N ? b.m[w] : 0ull;
+        const unsigned long long t = R[w] - dm;
+        const unsigned long long b1 = R[w] < dm;
+        const unsigned long long t2 = t - borrow;
+        const unsigned long long b2 = t < borrow;
+        R[w] = t2;
+        borrow = b1 + b2;
+      }
+      Q[bit >> 6] |= 1ull << (bit & 63);
+    }
+  }
+  bool sticky = false;
+  for (int w = 0; w <= N; ++w) sticky = sticky || R[w];
+  const int QW = (DB + 63) / 64;
+  unsigned long long S[2 * kMaxN + 3] = {};
+  unsigned long long carry = sticky ? 1ull : 0ull;
+  for (int w = 0; w < QW + 1; ++w) {
+    const unsigned long long q = w < QW ? Q[w] : 0ull;
+    S[w] = (q << 1) | carry;
+    carry = q >> 63;
+  }
+  // a / b = (Q + R/M_b) 2^(s_a - s_b - K)
+  return mp_round(S, QW + 1, a.neg != b.neg, a.s - b.s - K - 1, N);
+}
+
+// sqrt(a), a >= 0: the integer square root of M 2^e (e making the exponent even and the radicand
+// 2(64N + 2) bits wide) by the bit-pair restoring method, remainder folded into a sticky bit.
+__device__ inline Val mp_sqrt(const Val& a, int N) {
+  if (a.zero) return a;
+  const int RB = 64 * N + 2;              // root bits
+  long long e = 2LL * RB - 64LL * N;      // radicand = M 2^e has 2 RB bits (M has 64N)
+  if ((a.s - e) & 1) e += 1;              // a = M 2^s = (M 2^e) 2^(s - e), s - e even
+  const int XB = 64 * N + (int)e;         // radicand bit length bound
+  unsigned long long Y[kMaxN + 2] = {}, R[kMaxN + 3] = {};
+  const int W = N + 2;
+  for (int pair = (XB + 1) / 2 - 1; pair >= 0; --pair) {
+    // R = 4 R + next two radicand bits (bits 2 pair + 1, 2 pair of M 2^e)
+    unsigned long long two = 0;
+    for (int t = 1; t >= 0; --t) {
+      const long long bit = 2LL * pair + t - e;
+      const unsigned long long b = (bit >= 0 && bit < 64LL * N) ? ((a.m[bit >> 6] >> (bit & 63)) & 1ull) : 0ull;
+      two = (two << 1) | b;
+    }
+    unsigned long long carry = two;
+    for (int w = 0; w <= W; ++w) {
+      const unsigned long long nc = R[w] >> 62;
+      R[w] = (R[w] << 2) | carry;
+      carry = nc;
+    }
+    // T = 4 Y + 1; if R >= T: R -= T, Y = 2Y + 1 else Y = 2Y
+    unsigned long long T[kMaxN + 3] = {};
+    carry = 1;
+    for (int w = 0; w <= W; ++w) {
+      const unsigned long long y = w < W ? Y[w] : 0ull;
+      const unsigned long long prev = (w > 0 && w - 1 < W) ? Y[w - 1] : 0ull;
+      T[w] = (y << 2) | (prev >> 62) | carry;
+      carry = 0;
+    }
+    int cmp = 0;
+    for (int w = W; w >= 0 && !cmp; --w) cmp = R[w] > T[w] ? 1 : (R[w] < T[w] ? -1 : 0);
+    const bool take = cmp >= 0;
+    if (take) {
+      unsigned long long borrow = 0;
+      for (int w = 0; w <= W; ++w) {
+        const unsigned long long t1 = R[w] - T[w];
+        const unsigned long long b1 = R[w] < T[w];
+        const unsigned long long t2 = t1 - borrow;
+        const unsigned long long b2 = t1 < borrow;
+        R[w] = t2;
+        borrow = b1 + b2;
+      }
+    }
+    carry = take ? 1ull : 0ull;
+    for (int w = 0; w < W; ++w) {
+      const unsigned long long nc = Y[w] >> 63;
+      Y[w] = (Y[w] << 1) | carry;
+      carry = nc;
+    }
+  }
+  bool sticky = false;
+  for (int w = 0; w <= W; ++w) sticky = sticky || R[w];
+  unsigned long long S[kMaxN + 3] = {};
+  unsigned long long c2 = sticky ? 1ull : 0ull;
+  for (int w = 0; w < W + 1; ++w) {
+    const unsigned long long y = w < W ? Y[w] : 0ull;
+    S[w] = (y << 1) | c2;
+    c2 = y >> 63;
+  }
+  // sqrt(M 2^e 2^(s - e)) = Y' 2^((s - e) / 2), Y' = Y + frac
+  return mp_round(S, W + 1, false, (a.s - e) / 2 - 1, N);
+}
+
 // sign of a - b: -1, 0, 1.
 __device__ inline int mp_cmp(const Val& a, const Val& b, int N) {
   if (a.zero && b.zero) return 0;

@@ -119,6 +119,53 @@ __global__ void k_mp_sub_upper_t(unsigned char* A, long lda, const unsigned char
   mpd::mp_store(el(A, b, a, lda, N), N, mpd::mp_addsub(x, c, -1, N), status);
 }
 
+// XpotrfScalar::xpotrf for MpFloat (algebra/dense/blas/mpfr.rs:726-789): left-looking Cholesky
+// of the stored triangle, entry (i, k), i >= k, at i * si + k * sk (lower: si = 1, sk = ld;
+// upper: si = ld, sk = 1).  Per column j: d = a_jj - dot(l_j, l_j) (the dot exact and rounded
+// once, the difference rounded), failure when d <= 0 (info = j + 1), l_jj = sqrt(d) rounded; then
+// every later row i: l_ij = (a_ij - dot(l_i, l_j)) / l_jj, each operation rounded once.
+__global__ void __launch_bounds__(128) k_mp_potrf(unsigned char* A, long si, long sk, int n, int N, int* info,
+                                                  uint32_t* status) {
+  __shared__ __align__(8) unsigned char sd[8 * mpd::kMaxN + 8];
+  __shared__ int s_fail;
+  const long esz = 8L * N + 8;
+  auto at = [&](long i, long k) { return A + (i * si + k * sk) * esz; };
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    *info = 0;
+  }
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    if (threadIdx.x == 0) {
+      bool ok = true;
+      const Val a = mpd::mp_load(at(j, j), N);
+      const Val dot = mpd::mp_dot_sub(nullptr, at(j, 0), sk, at(j, 0), sk, j, N, &ok);
+      const Val d = mpd::mp_addsub(a, dot, -1, N);
+      if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
+      if (d.zero || d.neg) {
+        mpd::mp_store(at(j, j), N, d, status);
+        *info = j + 1;
+        s_fail = 1;
+      } else {
+        const Val r = mpd::mp_sqrt(d, N);
+        mpd::mp_store(at(j, j), N, r, status);
+        mpd::mp_store(sd, N, r, status);
+      }
+    }
+    __syncthreads();
+    if (s_fail) return;
+    const Val r = mpd::mp_load(sd, N);
+    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
+      bool ok = true;
+      const Val a = mpd::mp_load(at(i, j), N);
+      const Val dot = mpd::mp_dot_sub(nullptr, at(i, 0), sk, at(j, 0), sk, j, N, &ok);
+      if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
+      mpd::mp_store(at(i, j), N, mpd::mp_div(mpd::mp_addsub(a, dot, -1, N), r, N), status);
+    }
+    __syncthreads();
+  }
+}
+
 void check_limbs(int N) {
   if (N < 1 || N > mpd::kMaxN) throw std::invalid_argument("MPFR LDL: limbs must be in 1..8");
 }
@@ -132,6 +179,14 @@ void mp_launch_ldl_dots(unsigned char* A, long lda, int off, int size, int N, un
   if (size > kMpRecBase) throw std::invalid_argument("MPFR LDL: leaf above the recursion base");
   ++g_launches, k_mp_ldl_dots<<<1, 128, 0, st>>>(A, lda, off, size, N, W, dinv, reg, status);
   check(cudaGetLastError(), "k_mp_ldl_dots");
+}
+
+void mp_launch_potrf(unsigned char* A, long lda, int n, bool lower, int N, int* info, uint32_t* status,
+                     cudaStream_t st) {
+  check_limbs(N);
+  if (n <= 0) return;
+  ++g_launches, k_mp_potrf<<<1, 128, 0, st>>>(A, lower ? 1 : lda, lower ? lda : 1, n, N, info, status);
+  check(cudaGetLastError(), "k_mp_potrf");
 }
 
 void mp_launch_solve_lt(const unsigned char* L, long ldl, int k, unsigned char* B, long ldb, int m, int N,

@@ -17,6 +17,11 @@ constexpr int kMpMaxLimbs = 8;   // up to 512-bit values on the device
 // size x size scratch.  reg: NULL or (eps, delta) as two MpFloat values (the pivot rule).
 void mp_launch_ldl_dots(unsigned char* A, long lda, int off, int size, int N, unsigned char* W,
                         unsigned char* dinv, const unsigned char* reg, uint32_t* status, cudaStream_t st);
+// The reference's exact Cholesky xpotrf (mpfr.rs:726-789) of the n x n triangle of A (lower
+// or upper storage, ld lda) in place; *info (device int): 0, or j + 1 when pivot j is not
+// positive.  One CTA, left-looking, exact dots.
+void mp_launch_potrf(unsigned char* A, long lda, int n, bool lower, int N, int* info, uint32_t* status,
+                     cudaStream_t st);
 // X L' = B for the m rows of B (m x k, ld ldb) with L unit lower k x k (ld ldl), k <= 128:
 // each row by exact dots (arrow.rs:437-447).
 void mp_launch_solve_lt(const unsigned char* L, long ldl, int k, unsigned char* B, long ldb, int m, int N,

@@ -1104,3 +1104,52 @@ extern "C" int32_t sdpxg_mp_ldl(sdpxg_ctx* ctx, uint32_t limbs, uint64_t n, cons
     return 5;
   }
 }
+
+extern "C" int32_t sdpxg_mp_potrf(sdpxg_ctx* ctx, uint32_t limbs, char uplo, uint64_t n, void* A, uint64_t lda,
+                                  int32_t* info, uint32_t* status) {
+  try {
+    Engine* E = ctx_engine_any(ctx);
+    if (!E) throw std::invalid_argument("null context");
+    const int N = (int)limbs;
+    if (N < 1 || N > kMpMaxLimbs) {
+      g_last_error = "sdpxg_mp_potrf: limbs must be in 1..8";
+      return 2;
+    }
+    if (uplo != 'L' && uplo != 'U') throw std::invalid_argument("uplo must be 'L' or 'U'");
+    if (n > (1u << 16) || lda < std::max<uint64_t>(n, 1)) throw std::invalid_argument("bad size or leading dimension");
+    if (!info) throw std::invalid_argument("null pointer");
+    *info = 0;
+    if (n == 0) return 0;
+    if (!A) throw std::invalid_argument("null pointer");
+    const size_t esz = 8 * (size_t)N + 8;
+    check(cudaSetDevice(E->device), "cudaSetDevice");
+    DevBuf<unsigned char> dA(n * n * esz);
+    DevBuf<int> dinfo(1);
+    DevBuf<uint32_t> stw(1);
+    check(cudaMemsetAsync(stw.p, 0, sizeof(uint32_t), E->st), "memset");
+    check(cudaMemcpy2DAsync(dA.p, n * esz, A, lda * esz, n * esz, n, cudaMemcpyHostToDevice, E->st), "H2D");
+    g_h2d_bytes += n * n * esz;
+    mp_launch_potrf(dA.p, (long)n, (int)n, uplo == 'L', N, dinfo.p, stw.p, E->st);
+    check(cudaMemcpy2DAsync(A, lda * esz, dA.p, n * esz, n * esz, n, cudaMemcpyDeviceToHost, E->st), "D2H");
+    g_d2h_bytes += n * n * esz;
+    uint32_t hs = 0;
+    copy_d2h(&hs, stw.p, sizeof(uint32_t), E->st);
+    copy_d2h(info, dinfo.p, sizeof(int), E->st);
+    check(cudaStreamSynchronize(E->st), "sync");
+    if (status) *status = hs;
+    if (hs & SDPXG_ST_EXACT_SPREAD) {
+      g_last_error = "sdpxg_mp_potrf: an exact dot's exponent spread exceeds the device accumulator";
+      return 2;
+    }
+    return 0;
+  } catch (const std::invalid_argument& e) {
+    g_last_error = e.what();
+    return 1;
+  } catch (const std::exception& e) {
+    g_last_error = std::string("internal error: ") + e.what();
+    return 5;
+  } catch (...) {
+    g_last_error = "internal error";
+    return 5;
+  }
+}

@@ -115,6 +115,7 @@ SIGNATURES = {
     "sdpxg_mp_ldl": (i32, [C.c_void_p, u32, u64, C.c_void_p, u64, C.c_void_p, C.c_void_p, C.c_void_p,
                            PU32]),
     "sdpxg_mp_ldl_device": (i32, [C.c_void_p, u32, u64, C.c_void_p, u64, C.c_void_p, C.c_void_p, PU32]),
+    "sdpxg_mp_potrf": (i32, [C.c_void_p, u32, C.c_char, u64, C.c_void_p, u64, C.POINTER(i32), PU32]),
     "sdpxg_rns_congruence": (i32, [C.c_void_p, u32, C.c_char, u64, u64, C.c_void_p, u64, C.c_void_p,
                                    u64, u32, C.c_void_p, PU32]),
 }

@@ -548,6 +548,13 @@ class KernelContext:
                   C.c_char_p(reg) if reg is not None else None, L, D, C.byref(st))
         return L.raw[:n * n * esz], D.raw[:n * esz], st.value
 
+    def mp_potrf(self, limbs: int, uplo: str, n: int, A: bytes, lda: int):
+        """The reference's exact MpFloat Cholesky (xpotrf): returns (factor bytes, info, status)."""
+        buf = C.create_string_buffer(bytes(A), len(A))
+        info, st = C.c_int32(), C.c_uint32()
+        _lib.call("sdpxg_mp_potrf", self._h, limbs, uplo.encode(), n, buf, lda, C.byref(info), C.byref(st))
+        return buf.raw[:len(A)], info.value, st.value
+
     def rns_gemm_device(self, limbs: int, ta: str, tb: str, m: int, n: int, k: int, d_A: int,
                         lda: int, d_B: int, ldb: int, d_C: int, upper_only: bool = False):
         """Exact product on device buffers (addresses of MpFloat arrays in device memory)."""
