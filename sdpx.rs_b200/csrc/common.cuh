@@ -59,6 +59,13 @@ struct BlockDesc {
   int vec_off;   // offset of the block's length-n vectors (lambda, Lambda^-1/2)
 };
 
+// A matrix-valued sampled block (dim D > 1): its PSD block j, D, basis rows h, basis columns c,
+// and the offsets of its basis Q (h x c), of V = R^-1 U (n x Dc) and of K = V'V (Dc x Dc).
+struct MsDesc {
+  int j, D, h, c;
+  long q_off, v_off, k_off;
+};
+
 __device__ __forceinline__ int tri_idx(int i, int j) {  // i <= j
   return j * (j + 1) / 2 + i;
 }

@@ -271,6 +271,14 @@ __global__ void k_nn_margins(int, const int*, const double*, double*);
 __global__ void k_nn_forward(int, int, const int*, const double*, const double*, double, double, double*);
 __global__ void k_nn_adjoint(int, int, const int*, const double*, const double*, double, double*);
 __global__ void k_nn_schur(int, int, const double*, const double*, double*);
+__global__ void k_ms_basis(const BlockDesc*, const MsDesc*, const double*, const double*, double*);
+__global__ void k_ms_gram(const BlockDesc*, const MsDesc*, const double*, double*);
+__global__ void k_ms_schur(const MsDesc*, const int*, const int*, const long*, const double*, const int*,
+                           const double*, double*);
+__global__ void k_ms_forward(const BlockDesc*, const MsDesc*, const int*, const int*, const double*,
+                             const double*, const double*, double, double, double*);
+__global__ void k_ms_adjoint(const BlockDesc*, const MsDesc*, const int*, const int*, const double*, const int*,
+                             const double*, const double*, double*);
 __global__ void k_csr_spmv(int, const int*, const int*, const double*, const double*, double,
                            double, double*);
 }

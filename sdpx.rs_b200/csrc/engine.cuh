@@ -225,8 +225,9 @@ struct HostProblem {
   // weight[k] svec(q_k q_k') with q_k column k of `basis` (order x count, column-major).  The
   // engine uses these factors instead of testing the materialised columns.
   struct Sampled {
-    int row_start = 0, col0 = 0, count = 0, order = 0;
-    std::vector<double> basis, weight;
+    int row_start = 0, col0 = 0, count = 0, order = 0;  // count: basis columns; order: dim * basis rows
+    int dim = 1;                                        // matrix blocks per side
+    std::vector<double> basis, weight;                  // basis (order / dim) x count; tri(dim) count weights
   };
   std::vector<Sampled> sampled;
 };
@@ -260,6 +261,7 @@ class Engine {
   bool split_active() const { return factor_form == kFormSplit && n >= kSplitMin; }
   bool gram_enabled = true;  // rank-one blocks use the Gram form (SDPX_B200_GRAM=0 disables)
   int gram_blocks() const { return ngram_; }
+  int sampled_matrix_blocks() const { return nms_; }
   int nn_count() const { return nnn_; }
   std::vector<int> nn_rows;  // orthant rows of the stacked cone vector (cone order)
   std::vector<BlockDesc> hblocks;
@@ -509,15 +511,16 @@ class Engine {
     std::vector<long> gu_off(nblk, 0);
     std::vector<double> gu, gsig(col_ptr[nblk], 1.0);
     ngram_ = 0;
-    std::vector<const HostProblem::Sampled*> sampled_of(nblk, nullptr);
+    std::vector<const HostProblem::Sampled*> sampled_of(nblk, nullptr), ms_of(nblk, nullptr);
     for (const auto& sb : p.sampled) {
       int j = 0;
       while (j < nblk && hblocks[j].svec_off != sb.row_start) ++j;
-      if (j == nblk || hblocks[j].n != sb.order || hk[j] != sb.count)
+      const int prims = sb.dim * (sb.dim + 1) / 2 * sb.count;
+      if (j == nblk || hblocks[j].n != sb.order || hk[j] != prims)
         throw std::invalid_argument("sampled block does not match its PSD cone or columns");
-      for (int t = 0; t < sb.count; ++t)
+      for (int t = 0; t < prims; ++t)
         if (bcols[j][t] != sb.col0 + t) throw std::invalid_argument("sampled block columns are not its own");
-      sampled_of[j] = &sb;
+      (sb.dim == 1 ? sampled_of : ms_of)[j] = &sb;
     }
     if (gram_enabled || !p.sampled.empty()) {
       std::vector<long> u_off(nblk + 1, 0);
@@ -533,7 +536,7 @@ class Engine {
                       u_all.begin() + u_off[j] + (long)t * nj);
             gsig[it] = sb->weight[t];
             col_ok[it] = 1;
-          } else if (gram_enabled) {
+          } else if (gram_enabled && !ms_of[j]) {
             col_ok[it] = rank_one_column(&acol[acol_off[j] + (long)t * tn], nj,
                                          &u_all[u_off[j] + (long)t * nj], &gsig[it]);
           }
@@ -553,7 +556,37 @@ class Engine {
         gu.insert(gu.end(), u_all.begin() + u_off[j], u_all.begin() + u_off[j + 1]);
       }
     }
-    if (ngram_ > 0) {  // repack the dense columns of the ordinary blocks only
+    // matrix-valued sampled blocks (dim > 1) keep their factors in a form of their own
+    nms_ = 0;
+    std::vector<MsDesc> msd;
+    std::vector<double> msq, msw(col_ptr[nblk], 0.0);
+    std::vector<int> mspairs(2 * (size_t)std::max(col_ptr[nblk], 1), 0);
+    long msv = 0, msk = 0;
+    int ms_rmax = 0, ms_kmax = 0, ms_tnmax = 0;
+    for (int j = 0; j < nblk; ++j) {
+      const HostProblem::Sampled* sb = ms_of[j];
+      if (!sb) continue;
+      gram[j] = 2;
+      const int D = sb->dim, h = sb->order / D, c = sb->count, r = D * c;
+      MsDesc d{j, D, h, c, (long)msq.size(), msv, msk};
+      msd.push_back(d);
+      msq.insert(msq.end(), sb->basis.begin(), sb->basis.end());
+      msv += (long)hblocks[j].n * r;
+      msk += (long)r * r;
+      ms_rmax = std::max(ms_rmax, r);
+      ms_kmax = std::max(ms_kmax, hk[j]);
+      ms_tnmax = std::max(ms_tnmax, hblocks[j].n * (hblocks[j].n + 1) / 2);
+      int t = 0;
+      for (int ss = 0; ss < D; ++ss)
+        for (int rr = 0; rr <= ss; ++rr)
+          for (int k = 0; k < c; ++k, ++t) {  // primitive (s, r, k): the pair (r c + k, s c + k)
+            msw[col_ptr[j] + t] = sb->weight[t];
+            mspairs[2 * (col_ptr[j] + t)] = rr * c + k;
+            mspairs[2 * (col_ptr[j] + t) + 1] = ss * c + k;
+          }
+      nms_++;
+    }
+    if (ngram_ > 0 || nms_ > 0) {  // repack the dense columns of the ordinary blocks only
       F64Vec packed;
       long off = 0;
       for (int j = 0; j < nblk; ++j) {
@@ -580,6 +613,7 @@ class Engine {
     }
     std::vector<int> wblk, wloc, tiles, gtiles, gitem_blk, gitem_c0, gblk;
     for (int j = 0; j < nblk; ++j) {
+      if (gram[j] == 2) continue;  // matrix-valued sampled: kernels of their own
       if (gram[j]) {
         gblk.push_back(j);
         for (int c0 = 0; c0 < hk[j]; c0 += 64) {
@@ -613,6 +647,15 @@ class Engine {
     gitem_blk_.alloc(std::max(ngitem_, 1)); gitem_blk_.upload(gitem_blk.data(), gitem_blk.size(), st);
     gitem_c0_.alloc(std::max(ngitem_, 1)); gitem_c0_.upload(gitem_c0.data(), gitem_c0.size(), st);
     gblk_.alloc(std::max(ngblk_, 1)); gblk_.upload(gblk.data(), gblk.size(), st);
+    ms_desc_.alloc(std::max(nms_, 1)); ms_desc_.upload(msd.data(), msd.size(), st);
+    ms_q_.alloc(std::max<size_t>(msq.size(), 1)); ms_q_.upload(msq.data(), msq.size(), st);
+    ms_w_.alloc(std::max<size_t>(msw.size(), 1)); ms_w_.upload(msw.data(), msw.size(), st);
+    ms_pairs_.alloc(mspairs.size()); ms_pairs_.upload(mspairs.data(), mspairs.size(), st);
+    ms_v_.alloc(std::max<long>(msv, 1));
+    ms_k_.alloc(std::max<long>(msk, 1));
+    ms_rmax_ = ms_rmax;
+    ms_kmax_ = ms_kmax;
+    ms_tnmax_ = ms_tnmax;
     gf_part_.alloc((size_t)std::max(ngitem_, 1) * SDPXG_NMAX * SDPXG_NMAX);
     gf_cnt_.alloc(std::max(nblk, 1));
     check(cudaMemsetAsync(gf_cnt_.p, 0, std::max(nblk, 1) * sizeof(unsigned), st), "gram tickets");
@@ -669,7 +712,7 @@ class Engine {
     {  // 64-row tiles of every block for the forward product
       std::vector<int> fb, fr;
       for (int j = 0; j < nblk; ++j) {
-        if (gram[j]) continue;
+        if (gram[j]) continue;  // Gram and matrix-valued sampled blocks have their own operators
         int tn = hblocks[j].n * (hblocks[j].n + 1) / 2;
         for (int r0 = 0; r0 < tn; r0 += 64) {
           fb.push_back(j);
@@ -878,6 +921,11 @@ class Engine {
           beta, y, m);
       launched("k_op_forward");
     }
+    if (nms_) {
+      ++g_launches, k_ms_forward<<<dim3(nms_, (ms_tnmax_ + 255) / 256), 256, 0, st>>>(
+          blocks_, ms_desc_, col_ptr_, col_idx_, ms_w_, ms_q_, x, alpha, beta, y);
+      launched("k_ms_forward");
+    }
     if (ngblk_) {
       ++g_launches, k_gram_forward<<<ngitem_, 256, 0, st>>>(
           blocks_, gitem_blk_, gitem_c0_, kcount_, col_ptr_, col_idx_, gu_off_, gsig_, gU_, x,
@@ -894,6 +942,11 @@ class Engine {
       ++g_launches, k_op_adjoint_partial<<<dim3((nwork_ + wpb - 1) / wpb, 1), 256, 0, st>>>(
           blocks_, wblk_, wloc_, col_ptr_, acol_off_, acol_, z, m, adj_part_, ncol_, nwork_);
       launched("k_op_adjoint_partial");
+    }
+    if (nms_) {
+      ++g_launches, k_ms_adjoint<<<dim3(nms_, (ms_kmax_ + 127) / 128), 128, 0, st>>>(
+          blocks_, ms_desc_, kcount_, col_ptr_, ms_w_, ms_pairs_, ms_q_, z, adj_part_);
+      launched("k_ms_adjoint");
     }
     if (ngitem_) {
       ++g_launches, k_gram_adjoint<<<ngitem_, 256, kSmemGram, st>>>(
@@ -943,6 +996,15 @@ class Engine {
       ++g_launches, k_gram_schur<<<ngtiles_, 256, 0, st>>>(blocks_, gtiles_, kcount_, col_ptr_, gu_off_,
                                                           s_off_, gsig_, gV_, S_);
       launched("k_gram_schur");
+    }
+    if (nms_) {  // matrix-valued sampled blocks: V = Rinv U, K = V'V, S from K
+      ++g_launches, k_ms_basis<<<dim3(nms_, (ms_rmax_ + 7) / 8), 256, 0, st>>>(blocks_, ms_desc_, Rinv_, ms_q_,
+                                                                           ms_v_);
+      ++g_launches, k_ms_gram<<<dim3(nms_, (unsigned)(((long)ms_rmax_ * ms_rmax_ + 255) / 256)), 256, 0, st>>>(
+          blocks_, ms_desc_, ms_v_, ms_k_);
+      ++g_launches, k_ms_schur<<<dim3(nms_, (unsigned)(((long)ms_kmax_ * ms_kmax_ + 255) / 256)), 256, 0, st>>>(
+          ms_desc_, kcount_, col_ptr_, s_off_, ms_w_, ms_pairs_, ms_k_, S_);
+      launched("k_ms_schur");
     }
     long tot = (long)n * n;
     if (tot) {
@@ -1253,6 +1315,11 @@ class Engine {
   DevBuf<double> gf_part_;  // k_gram_forward chunk partials (64 x 64 per item)
   DevBuf<unsigned> gf_cnt_;  // its per-block arrival tickets (self-resetting)
   int ngram_ = 0, ngtiles_ = 0, ngitem_ = 0, ngblk_ = 0, ncol_ = 0;
+  // matrix-valued sampled blocks (dim > 1)
+  int nms_ = 0, ms_rmax_ = 0, ms_kmax_ = 0, ms_tnmax_ = 0;
+  DevBuf<MsDesc> ms_desc_;
+  DevBuf<double> ms_q_, ms_w_, ms_v_, ms_k_;
+  DevBuf<int> ms_pairs_;
   DevBuf<int> prp_, pci_, pup_ptr_, pup_row_;
   DevBuf<double> pv_, pup_val_;
   DevBuf<double> adj_part_;
