@@ -154,9 +154,10 @@ int32_t sdpx_b200_i8_times(double *ms, double *ops, double *alg_ops, uint64_t *l
 /* Tile configuration of the INT8 tensor-core GEMM: -1 (default) autotuned -- the first launch of
  * each shape class (digit count, power-of-two classes of the padded extents, K range and moduli)
  * times every configuration on the real operands with CUDA events and keeps the fastest; results
- * do not depend on the choice (exact integer arithmetic) -- or 0 / 1 to force a configuration
- * (0: 128 x 256 tiles for single-digit and 128 x 128 for two-digit residues, 1: half-width tiles
- * with a deeper stage ring).  SDPX_B200_AUTOTUNE=0 keeps configuration 0.  No counterpart in the
+ * do not depend on the choice (exact integer arithmetic) -- or 0 / 1 / 2 to force a configuration
+ * (0: 128 x 256 tiles for single-digit and 128 x 128 for two-digit residues, one CTA per SM;
+ * 1: half-width tiles with a deeper stage ring; 2: two CTAs per SM with two-stage rings, 128 x 256
+ * and 128 x 64 tiles).  SDPX_B200_AUTOTUNE=0 keeps configuration 0.  No counterpart in the
  * reference (it tunes CPU tile sizes by constant). */
 int32_t sdpx_b200_i8_config(int32_t variant);
 /* The autotuner's table as text (one line per shape class), in the sdpx_result_decimal style:

@@ -536,9 +536,9 @@ void prepare_sampled_impl(const sdpx_csc* P, const sdpx_scalars* q, const sdpx_c
   A.values.f64 = merged.val.data();
   double tv = 0, te = 0;
   auto h = build_problem(P, q, &A, b, cones, nc, s, &tv, &te);
-  for (auto& r : merged.recs) {  // the factors in the equilibrated coordinates
+  for (auto& r : merged.recs) {  // the factors in the equilibrated coordinates: one weight per column
     const double e = h->eq.e[(size_t)r.row_start];
-    for (int k = 0; k < r.count; ++k) r.weight[k] = r.weight[k] * h->eq.d[(size_t)(r.col0 + k)] * e;
+    for (size_t k = 0; k < r.weight.size(); ++k) r.weight[k] = r.weight[k] * h->eq.d[(size_t)r.col0 + k] * e;
   }
   h->equil.sampled = std::move(merged.recs);
   h->eng = std::make_unique<Engine>();
@@ -727,7 +727,7 @@ int32_t sdpx_b200_set_i8_timing(int32_t on) {
 
 int32_t sdpx_b200_i8_config(int32_t variant) {
   return boundary([&] {
-    if (variant < -1 || variant > 1) invalid("variant must be -1 (autotuned), 0 or 1");
+    if (variant < -1 || variant > 2) invalid("variant must be -1 (autotuned), 0, 1 or 2");
     sdpxg::i8_set_config(variant);
   });
 }

@@ -33,25 +33,35 @@ constexpr int kBM = 128;     // rows per tile (MMA M)
 constexpr int kKB = 128;     // K bytes per stage (one 128-byte swizzle row)
 constexpr int kThreads = 192;
 
-// Tile configurations: variant 0 (the default) and variant 1 (half the tile width, deeper
-// stage ring); the autotuner picks per shape class.  Every variant gives the same bits.
+// Tile configurations: variant 0 (the default), variant 1 (half the tile width, deeper stage
+// ring) and variant 2 (two CTAs per SM: a two-stage ring each, so that one CTA's epilogue overlaps
+// the other's main loop); the autotuner picks per shape class.  Every variant gives the same bits.
+constexpr int kVariants = 3;
 template <int DIGITS, int VAR>
 struct Cfg;
 template <>
 struct Cfg<1, 0> {
-  static constexpr int BN = 256, STAGES = 4, NACC = 1, TMEM_COLS = 256;
+  static constexpr int BN = 256, STAGES = 4, NACC = 1, TMEM_COLS = 256, CTAS = 1;
 };
 template <>
 struct Cfg<1, 1> {
-  static constexpr int BN = 128, STAGES = 6, NACC = 1, TMEM_COLS = 128;
+  static constexpr int BN = 128, STAGES = 6, NACC = 1, TMEM_COLS = 128, CTAS = 1;
+};
+template <>
+struct Cfg<1, 2> {
+  static constexpr int BN = 256, STAGES = 2, NACC = 1, TMEM_COLS = 256, CTAS = 2;
 };
 template <>
 struct Cfg<2, 0> {
-  static constexpr int BN = 128, STAGES = 3, NACC = 3, TMEM_COLS = 512;
+  static constexpr int BN = 128, STAGES = 3, NACC = 3, TMEM_COLS = 512, CTAS = 1;
 };
 template <>
 struct Cfg<2, 1> {
-  static constexpr int BN = 64, STAGES = 4, NACC = 3, TMEM_COLS = 256;
+  static constexpr int BN = 64, STAGES = 4, NACC = 3, TMEM_COLS = 256, CTAS = 1;
+};
+template <>
+struct Cfg<2, 2> {
+  static constexpr int BN = 64, STAGES = 2, NACC = 3, TMEM_COLS = 256, CTAS = 2;
 };
 
 template <int DIGITS, int VAR>
@@ -71,8 +81,29 @@ __device__ __forceinline__ void give_up(volatile int* abort, int* err) {
   if (err) atomicOr(err, 1);
 }
 
+// Symmetric residue of v modulo p (|v| < 2^31, 2 <= p <= 256) in [-(p-1)/2, p/2]: the quotient
+// rounded from an FP64 product (v and v/p are exact to far below 1/2 in FP64, so it is the
+// nearest integer to v/p up to a tie), the remainder in 32-bit integers (exact modulo 2^32, and
+// the true remainder is small), then at most one correction each way.
+__device__ __forceinline__ int sym_mod_small(int v, int p, double pinv) {
+  const int q = __double2int_rn((double)v * pinv);
+  int r = v - q * p;
+  if (r > p / 2) r -= p;
+  if (r < -((p - 1) / 2)) r += p;
+  return r;
+}
+// Residue of v modulo p in [0, p) for |v| < 2^50, p < 2^15: FP64 quotient as above (v exact in
+// FP64), remainder in 64-bit integers, one correction.
+__device__ __forceinline__ int mod_wide(long long v, int p, double pinv) {
+  const long long q = __double2ll_rn((double)v * pinv);
+  long long r = v - q * p;
+  if (r < 0) r += p;
+  if (r >= p) r -= p;
+  return (int)r;
+}
+
 template <int DIGITS, int VAR>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, Cfg<DIGITS, VAR>::CTAS)
     k_i8_mod_gemm(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, I8GemmArgs a) {
   constexpr int BN = Cfg<DIGITS, VAR>::BN, STAGES = Cfg<DIGITS, VAR>::STAGES, NACC = Cfg<DIGITS, VAR>::NACC;
   constexpr int TCOLS = Cfg<DIGITS, VAR>::TMEM_COLS;
@@ -176,6 +207,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int row = warp * 32 + lane;
       const int i = tm * kBM + row;
       const int p = a.moduli[l];
+      const double pinv = 1.0 / (double)p;
       const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
       for (int c0 = 0; c0 < BN; c0 += 32) {
@@ -191,10 +223,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int q = 0; q < 32; ++q) {
               const int j = j0 + q;
               if (j < a.n) {
-                int r = (int)acc[0][q] % p;  // |r| < p
-                if (r > p / 2) r -= p;
-                if (r < -((p - 1) / 2)) r += p;
-                out[(long)j * a.m + i] = (int8_t)r;
+                out[(long)j * a.m + i] = (int8_t)sym_mod_small((int)acc[0][q], p, pinv);
               }
             }
           } else {
@@ -205,8 +234,7 @@ __global__ void __launch_bounds__(kThreads, 1)
               if (j < a.n) {
                 long long v = (long long)(int)acc[0][q] + ((long long)(int)acc[NACC > 1 ? 1 : 0][q] << 8) +
                               ((long long)(int)acc[NACC > 2 ? 2 : 0][q] << 16);
-                long long r = v % p;
-                if (r < 0) r += p;
+                long long r = mod_wide(v, p, pinv);
                 if (a.accumulate) {
                   r += out[(long)j * a.m + i];
                   if (r >= p) r -= p;
@@ -326,7 +354,7 @@ void launch_variant(const int8_t* A, const int8_t* B, const I8GemmArgs& a, cudaS
 // SDPX_B200_AUTOTUNE=0 keeps variant 0; sdpx_b200_i8_config forces one.
 struct Tuner {
   std::mutex mu;
-  std::map<std::array<int, 5>, std::pair<int, std::array<float, 2>>> table;
+  std::map<std::array<int, 5>, std::pair<int, std::array<float, kVariants>>> table;
   int forced = -1;
   bool enabled = true;
   Tuner() {
@@ -347,7 +375,8 @@ int lg2(long v) {
 template <int DIGITS>
 void launch(const int8_t* A, const int8_t* B, const I8GemmArgs& a, cudaStream_t st) {
   constexpr int BN = Cfg<DIGITS, 0>::BN;  // the padding rule: a multiple of every variant's width
-  static_assert(Cfg<DIGITS, 0>::BN % Cfg<DIGITS, 1>::BN == 0, "variant widths must divide the padding");
+  static_assert(Cfg<DIGITS, 0>::BN % Cfg<DIGITS, 1>::BN == 0 && Cfg<DIGITS, 0>::BN % Cfg<DIGITS, 2>::BN == 0,
+                "variant widths must divide the padding");
   if (a.Mpad <= 0 || a.Npad <= 0 || a.Kpad <= 0 || a.Mpad % kBM || a.Npad % BN || a.Kpad % kKB ||
       a.Kld % kKB || a.k0 % kKB || a.k0 < 0 || a.k0 + a.Kpad > a.Kld)
     throw std::invalid_argument("i8 GEMM: padded extents must be multiples of the tile");
@@ -373,21 +402,27 @@ void launch(const int8_t* A, const int8_t* B, const I8GemmArgs& a, cudaStream_t 
       }
     }
   }
-  if (!tune) {
-    if (var == 0)
-      launch_variant<DIGITS, 0>(A, B, a, st, nullptr);
+  auto run = [&](int v, float* ms) {
+    if (v == 0)
+      launch_variant<DIGITS, 0>(A, B, a, st, ms);
+    else if (v == 1)
+      launch_variant<DIGITS, 1>(A, B, a, st, ms);
     else
-      launch_variant<DIGITS, 1>(A, B, a, st, nullptr);
+      launch_variant<DIGITS, 2>(A, B, a, st, ms);
+  };
+  if (!tune) {
+    run(var, nullptr);
     return;
   }
-  // warm both, then time both; variant 0 runs last and leaves its (identical) output
-  std::array<float, 2> ms = {0.f, 0.f};
-  launch_variant<DIGITS, 1>(A, B, a, st, &ms[1]);
-  launch_variant<DIGITS, 0>(A, B, a, st, &ms[0]);
-  launch_variant<DIGITS, 1>(A, B, a, st, &ms[1]);
-  launch_variant<DIGITS, 0>(A, B, a, st, &ms[0]);
+  // warm every variant, then time each; variant 0 runs last and leaves its (identical) output
+  std::array<float, kVariants> ms{};
+  for (int pass = 0; pass < 2; ++pass)
+    for (int v = kVariants - 1; v >= 0; --v) run(v, &ms[v]);
+  int best = 0;
+  for (int v = 1; v < kVariants; ++v)
+    if (ms[v] < ms[best]) best = v;
   std::lock_guard<std::mutex> lk(T.mu);
-  T.table[key] = {ms[1] < ms[0] ? 1 : 0, ms};
+  T.table[key] = {best, ms};
 }
 
 }  // namespace
@@ -414,10 +449,11 @@ std::string i8_tuning_table() {
   std::lock_guard<std::mutex> lk(tuner().mu);
   std::string out;
   for (const auto& kv : tuner().table) {
-    char line[160];
-    std::snprintf(line, sizeof line, "digits %d Mpad<=2^%d Npad<=2^%d K<=2^%d L<=2^%d -> variant %d (%.4f ms, %.4f ms)\n",
+    char line[192];
+    std::snprintf(line, sizeof line,
+                  "digits %d Mpad<=2^%d Npad<=2^%d K<=2^%d L<=2^%d -> variant %d (%.4f ms, %.4f ms, %.4f ms)\n",
                   kv.first[0], kv.first[1], kv.first[2], kv.first[3], kv.first[4], kv.second.first,
-                  (double)kv.second.second[0], (double)kv.second.second[1]);
+                  (double)kv.second.second[0], (double)kv.second.second[1], (double)kv.second.second[2]);
     out += line;
   }
   return out;

@@ -52,8 +52,8 @@ void launch_i8_gemm(int digits, const int8_t* A, const int8_t* B, const I8GemmAr
 // algorithmic INT8 operations (2 m n K per digit pair and modulus) and the launch count.
 void i8_timing(int on);
 void i8_times(double* ms, double* ops, double* alg_ops, uint64_t* count);
-// Tile configuration of later launches: -1 autotuned (default), 0 or 1 a fixed variant; and the
-// autotuner's table (one line per shape class: the chosen variant and both timings).
+// Tile configuration of later launches: -1 autotuned (default), 0, 1 or 2 a fixed variant; and
+// the autotuner's table (one line per shape class: the chosen variant and every timing).
 void i8_set_config(int variant);
 std::string i8_tuning_table();
 

@@ -24,7 +24,8 @@ namespace sdpxg {
 constexpr int kOzMod = 16;
 
 struct OzakiWorkspace {
-  DevBuf<int> shiftL, shiftR, moduli, err;
+  DevBuf<unsigned long long> amaxL, amaxR;  // per-line maxima of |operand| (FP64 bits)
+  DevBuf<int> moduli, err;
   DevBuf<int8_t> PL, PR, PC;
   DevBuf<uint32_t> status;
   bool init = false;

@@ -1,7 +1,7 @@
 """The INT8 tensor-core GEMM's tile-configuration autotuner (sdpx_b200_i8_config / _i8_tuning).
 
 Every configuration computes the same exact integers, so the split-precision product and the
-exact RNS product must be bitwise equal whichever configuration runs (forced 0, forced 1,
+exact RNS product must be bitwise equal whichever configuration runs (forced 0, 1 or 2,
 autotuned), and the autotuner must have recorded the shape classes it timed.
 """
 import ctypes as C
@@ -39,7 +39,7 @@ def test_configurations_agree_bitwise():
     Am = X.pack_array(X.random_values(n_mp, lcg, mm * kk, 20))
     Bm = X.pack_array(X.random_values(n_mp, lcg, kk * nn, 20))
     try:
-        for cfg in (0, 1, -1):
+        for cfg in (0, 1, 2, -1):
             assert lib.sdpx_b200_i8_config(cfg) == 0
             Cd = torch.zeros((n, m), dtype=torch.float64, device="cuda")
             torch.cuda.synchronize()
@@ -50,6 +50,6 @@ def test_configurations_agree_bitwise():
             outs.append((Cd.cpu().numpy().tobytes(), raw))
     finally:
         lib.sdpx_b200_i8_config(-1)
-    assert outs[0] == outs[1] == outs[2]
+    assert outs[0] == outs[1] == outs[2] == outs[3]
     table = _tuning_table()
     assert "digits 1" in table and "digits 2" in table, table
