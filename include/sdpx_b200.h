@@ -319,6 +319,37 @@ int32_t sdpxg_rns_gemm_device(sdpxg_ctx *ctx, uint32_t limbs, char ta, char tb, 
 int32_t sdpxg_rns_congruence(sdpxg_ctx *ctx, uint32_t limbs, char ta, uint64_t m, uint64_t k,
                              const void *A, uint64_t lda, const void *X, uint64_t ldx,
                              uint32_t upper_only, void *C, uint32_t *status);
+/* Exact C = A' diag(d) A (m x m) of MpFloat<limbs> arrays: A k x m column-major (leading
+ * dimension lda), d k entries; every entry is the exact sum over r of A(r, i) d(r) A(r, j),
+ * rounded once to 64 * limbs bits, ties to even.  One product per prime on the INT8 tensor cores
+ * (left operand the residues of A's columns, right operand those residues times d's) and one CRT.
+ * upper_only writes zeros below the diagonal.  Replaces rns_blas::diag_congruence
+ * (crates/solver/src/algebra/dense/blas/rns_blas.rs:2990-3194). */
+int32_t sdpxg_rns_diag_congruence(sdpxg_ctx *ctx, uint32_t limbs, uint64_t m, uint64_t k, const void *A,
+                                  uint64_t lda, const void *d, uint32_t upper_only, void *C, uint32_t *status);
+/* Exact weighted quadratic forms v[k] = sum_{i <= j} c_ij x_t Q(i, k) Q(j, k), k < kmax, with x an
+ * svec of order h (t = j (j + 1) / 2 + i), c_ii = 1 and c_ij = sqrt2 (the caller's working-precision
+ * constant, one MpFloat<limbs>), Q h x kmax column-major (abs_q: |Q|); each v[k] the exact sum
+ * rounded once.  Replaces rns_blas::svec_quadratic (rns_blas.rs:4025-4174), the sampled adjoint's
+ * exact form. */
+int32_t sdpxg_rns_svec_quadratic(sdpxg_ctx *ctx, uint32_t limbs, uint64_t h, uint64_t kmax, const void *Q,
+                                 uint32_t abs_q, const void *x, const void *sqrt2, void *out, uint32_t *status);
+/* Exact bilinear forms out[s] = Q(:, a)' X Q(:, b) for the pairs s = (pairs[2s], pairs[2s+1]), X
+ * symmetric of order h packed upper without svec factors (entry (i, j), i <= j, at
+ * j (j + 1) / 2 + i), Q h x columns column-major; each the exact sum rounded once.  Replaces
+ * rns_blas::symmetric_bilinear (rns_blas.rs:4175-4277). */
+int32_t sdpxg_rns_symmetric_bilinear(sdpxg_ctx *ctx, uint32_t limbs, uint64_t h, uint64_t columns, const void *Q,
+                                     const void *X, uint64_t npairs, const uint64_t *pairs, void *out,
+                                     uint32_t *status);
+/* Upper triangle of sum_b Z_b' Y_b (m x m) with Z_b = diag(d_b) Y_b rounded entrywise: block b has
+ * width widths[b] and counts[b] sorted global columns (below m), its factor Y_b widths[b] x counts[b]
+ * column-major; y, d and columns concatenate the blocks in order.  Every entry of the sum over all
+ * blocks and rows is exact and rounded once (zeros below the diagonal).  Replaces
+ * rns_blas::gemm_blocks_upper (rns_blas.rs:2656-2923); the blocks are stacked into dense operands
+ * (sum of widths times m entries at most 2^28). */
+int32_t sdpxg_rns_gemm_blocks_upper(sdpxg_ctx *ctx, uint32_t limbs, uint64_t m, uint64_t nblocks,
+                                    const uint64_t *widths, const uint64_t *counts, const void *y, const void *d,
+                                    const uint64_t *columns, void *C, uint32_t *status);
 /* The reference's dense MPFR LDL' (ArrowLDLSolver::try_dense -> ldl_rec, kkt/ldl/arrow.rs:2609-2620,
  * 255-420, with ldl_dots leaves 156-242 and solve_unit_lower_t 430-470) of the n x n MpFloat<limbs>
  * matrix A (host, column-major, leading dimension lda; its lower triangle is read): L (n x n,

@@ -374,3 +374,78 @@ def xpotrf(n: int, uplo: str, size: int, A: List[Mp], lda: int) -> int:
             solved = exact_dot(n, [(A[at(i, k)], A[at(j, k)]) for k in range(j)])
             A[at(i, j)] = mp_div(n, mp_sub(n, A[at(i, j)], solved), d)
     return 0
+
+
+# ------------------------------------------------------------------------------------------
+# Exact forms of small factors (crates/solver/src/algebra/dense/blas/rns_blas.rs): every output
+# is one exact sum of products, rounded once to 64n bits, ties to even.
+# ------------------------------------------------------------------------------------------
+def mp_abs(a: Mp) -> Mp:
+    return Mp(a.n, False, a.mant, a.exp) if not a.is_zero() else Mp(a.n)
+
+
+def sqrt2(n: int) -> Mp:
+    """The working-precision sqrt 2 (correctly rounded; FloatConst::SQRT_2 of MpFloat<n>)."""
+    return mp_sqrt(n, mp_from_float(n, 2.0))
+
+
+def diag_congruence(n: int, m: int, k: int, A: List[Mp], lda: int, d: List[Mp],
+                    upper_only: bool = False) -> List[Mp]:
+    """C = A' diag(d) A for A k x m column-major (rns_blas.rs:2990-3194 diag_congruence): entry
+    (i, j) is sum_r A(r, i) d(r) A(r, j), exact, rounded once; zeros below the diagonal when
+    upper_only."""
+    out = []
+    for j in range(m):
+        for i in range(m):
+            if upper_only and i > j:
+                out.append(Mp(n))
+                continue
+            out.append(exact_sum_of_products(
+                n, [(A[r + i * lda], d[r], A[r + j * lda]) for r in range(k)]))
+    return out
+
+
+def svec_quadratic(n: int, h: int, kmax: int, Q: List[Mp], x: List[Mp], s2: Mp,
+                   abs_q: bool = False) -> List[Mp]:
+    """v[k] = sum_{i <= j} c_ij x_t q_ik q_jk, t = tri(j) + i, c_ii = 1, c_ij = s2 (the
+    working-precision sqrt 2), each exact and rounded once (rns_blas.rs:4025-4174)."""
+    q = [mp_abs(v) for v in Q] if abs_q else Q
+    out = []
+    for k in range(kmax):
+        terms = []
+        for j in range(h):
+            for i in range(j + 1):
+                t = j * (j + 1) // 2 + i
+                a, b = q[i + k * h], q[j + k * h]
+                terms.append((x[t], a, b) if i == j else (s2, x[t], a, b))
+        out.append(exact_sum_of_products(n, terms))
+    return out
+
+
+def symmetric_bilinear(n: int, h: int, Q: List[Mp], X: List[Mp],
+                       pairs: Sequence[Tuple[int, int]]) -> List[Mp]:
+    """q_a' X q_b for each pair, X symmetric packed upper without svec factors
+    (rns_blas.rs:4175-4277 symmetric_bilinear), exact, rounded once."""
+    def xe(i, j):
+        lo, hi = min(i, j), max(i, j)
+        return X[hi * (hi + 1) // 2 + lo]
+    return [exact_sum_of_products(n, [(Q[i + a * h], xe(i, j), Q[j + b * h])
+                                      for i in range(h) for j in range(h)])
+            for a, b in pairs]
+
+
+def gemm_blocks_upper(n: int, m: int, blocks) -> List[Mp]:
+    """Upper triangle of sum_b Z_b' Y_b, Z_b = diag(d_b) Y_b rounded entrywise, the sum over all
+    blocks and rows exact and rounded once (rns_blas.rs:2656-2923 gemm_blocks_upper); blocks are
+    (y, d, columns, w) with y w x len(columns) column-major.  Zeros below the diagonal."""
+    terms = {}
+    for y, d, cols, w in blocks:
+        for a, ca in enumerate(cols):
+            for b, cb in enumerate(cols):
+                if ca > cb:
+                    continue
+                lst = terms.setdefault((ca, cb), [])
+                for r in range(w):
+                    lst.append((mp_mul(n, d[r], y[r + a * w]), y[r + b * w]))
+    return [exact_dot(n, terms.get((i, j), [])) if i <= j else Mp(n)
+            for j in range(m) for i in range(m)]

@@ -181,6 +181,45 @@ void mp_launch_ldl_dots(unsigned char* A, long lda, int off, int size, int N, un
   check(cudaGetLastError(), "k_mp_ldl_dots");
 }
 
+// The stacked operands of the block product sum (rns_blas.rs:2656-2923 gemm_blocks_upper): block
+// b's w_b x q_b factor y_b (column-major) fills rows [r0_b, r0_b + w_b) of the W x m matrices Y
+// and Z at its global columns cols, Y = y_b and Z = d_b[r] * y_b (each product rounded once); every
+// other entry is zero.  One thread per stacked entry (W x m): the block of a row by binary search
+// over the row offsets, the column by a search of the block's sorted column list.
+__global__ void k_mp_stack_blocks(int nb, const long* __restrict__ r0, const long* __restrict__ yoff,
+                                  const long* __restrict__ coff, const int* __restrict__ qn,
+                                  const unsigned char* __restrict__ y, const unsigned char* __restrict__ d,
+                                  const unsigned long long* __restrict__ cols, long W, int m, int N,
+                                  unsigned char* __restrict__ Z, unsigned char* __restrict__ Y,
+                                  uint32_t* __restrict__ status) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= W * m) return;
+  const long row = e % W;
+  const int col = (int)(e / W);
+  const size_t esz = 8 * (size_t)N + 8;
+  int lo = 0, hi = nb - 1;  // last block with r0 <= row
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (r0[mid] <= row) lo = mid; else hi = mid - 1;
+  }
+  const int b = lo;
+  const long r = row - r0[b], w = r0[b + 1] - r0[b];
+  const unsigned long long* cb = cols + coff[b];
+  int a = 0, z = qn[b] - 1, c = -1;
+  while (a <= z) {
+    const int mid = (a + z) / 2;
+    if (cb[mid] == (unsigned long long)col) { c = mid; break; }
+    if (cb[mid] < (unsigned long long)col) a = mid + 1; else z = mid - 1;
+  }
+  mpd::Val vy = mpd::mp_zero(), vz = mpd::mp_zero();
+  if (c >= 0) {
+    vy = mpd::mp_load(y + (size_t)(yoff[b] + r + (long)c * w) * esz, N);
+    vz = mpd::mp_mul(mpd::mp_load(d + (size_t)(r0[b] + r) * esz, N), vy, N);
+  }
+  mpd::mp_store(Y + (size_t)e * esz, N, vy, status);
+  mpd::mp_store(Z + (size_t)e * esz, N, vz, status);
+}
+
 void mp_launch_potrf(unsigned char* A, long lda, int n, bool lower, int N, int* info, uint32_t* status,
                      cudaStream_t st) {
   check_limbs(N);
@@ -219,6 +258,16 @@ void mp_launch_sub_upper_t(unsigned char* A, long lda, const unsigned char* C, l
   ++g_launches, k_mp_sub_upper_t<<<(unsigned)(((long)n * n + 127) / 128), 128, 0, st>>>(A, lda, C, ldc, n, N,
                                                                                         status);
   check(cudaGetLastError(), "k_mp_sub_upper_t");
+}
+
+void mp_launch_stack_blocks(int nb, const long* r0, const long* yoff, const long* coff, const int* qn,
+                            const unsigned char* y, const unsigned char* d, const unsigned long long* cols, long W,
+                            int m, int N, unsigned char* Z, unsigned char* Y, uint32_t* status, cudaStream_t st) {
+  check_limbs(N);
+  if (W <= 0 || m <= 0) return;
+  ++g_launches, k_mp_stack_blocks<<<(unsigned)((W * m + 127) / 128), 128, 0, st>>>(nb, r0, yoff, coff, qn, y, d,
+                                                                                   cols, W, m, N, Z, Y, status);
+  check(cudaGetLastError(), "k_mp_stack_blocks");
 }
 
 }  // namespace sdpxg

@@ -36,4 +36,12 @@ void mp_launch_copy_scale_cols(unsigned char* A, long lda, unsigned char* W, con
 void mp_launch_sub_upper_t(unsigned char* A, long lda, const unsigned char* C, long ldc, int n, int N,
                            uint32_t* status, cudaStream_t st);
 
+// Stacked operands of the exact block product sum (gemm_blocks_upper): nb blocks, block b with
+// rows [r0[b], r0[b+1]) of the W x m outputs, factor y_b at element yoff[b] of y (w_b x qn[b],
+// column-major), scales d at rows r0[b].., sorted global columns cols[coff[b] ..]; Y = y_b and
+// Z = d_b y_b (rounded) at those columns, zeros elsewhere.  All arrays on the device.
+void mp_launch_stack_blocks(int nb, const long* r0, const long* yoff, const long* coff, const int* qn,
+                            const unsigned char* y, const unsigned char* d, const unsigned long long* cols, long W,
+                            int m, int N, unsigned char* Z, unsigned char* Y, uint32_t* status, cudaStream_t st);
+
 }  // namespace sdpxg

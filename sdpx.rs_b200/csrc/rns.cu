@@ -442,6 +442,116 @@ __global__ void k_rns_crt(const R* __restrict__ RC, long planeC, int m, int n, i
   *oexp = (int)exponent;
 }
 
+// ---- exact forms of small factors (rns_blas.rs:2990-3194 diag_congruence, 4025-4174
+// svec_quadratic, 4175-4277 symmetric_bilinear) ----
+// Residues in [0, p_t) of a flat array of MpFloat<N> aligned at one exponent lo (the class's
+// lowest set bit): entry e is (-1)^s M_e 2^(exp_e - 64N - lo); out[t * count + e].  absval drops
+// the signs.  The residue is sum_c chunk_c (2^(16c + shift) mod p) over the mantissa's 16-bit
+// chunks, as in k_rns8_residues.
+extern "C" __global__ void k_rns_class_residues(const unsigned char* __restrict__ X, int N, int count, int lo,
+                                                int absval, int L, const int* __restrict__ primes,
+                                                const uint32_t* __restrict__ pow2, int S, int* __restrict__ out) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= count) return;
+  const unsigned char* x = X + (size_t)e * (8 * N + 8);
+  const int kind = elem_kind(x, N);
+  if (abs(kind) != MP_REGULAR) {
+    for (int t = 0; t < L; ++t) out[(size_t)t * count + e] = 0;
+    return;
+  }
+  const bool neg = kind < 0 && !absval;
+  const int shift = elem_exp(x, N) - 64 * N - lo;
+  const unsigned long long* lp = reinterpret_cast<const unsigned long long*>(x);
+  for (int t = 0; t < L; ++t) {
+    const uint32_t* w = pow2 + (size_t)t * S + shift;
+    unsigned long long acc = 0;
+    for (int q = 0; q < N; ++q) {
+      const unsigned long long v = lp[q];
+      acc += (v & 0xFFFFull) * w[64 * q] + ((v >> 16) & 0xFFFFull) * w[64 * q + 16] +
+             ((v >> 32) & 0xFFFFull) * w[64 * q + 32] + (v >> 48) * w[64 * q + 48];
+    }
+    const int p = primes[t];
+    int r = (int)(acc % (unsigned long long)p);
+    if (neg && r) r = p - r;
+    out[(size_t)t * count + e] = r;
+  }
+}
+
+// Right operand of the diagonal congruence: digit planes of (r_t(line j, inner r) * d_t(r)) mod
+// p_t, symmetric, from the left operand's digit planes (the same layout as k_rns8_residues) and
+// the residues of d (k entries per prime, in [0, p)).  Padding stays zero.
+extern "C" __global__ void k_rns8_scale_planes(const int8_t* __restrict__ in, const int* __restrict__ dres, int k,
+                                               int L, const int* __restrict__ primes, int8_t* __restrict__ out,
+                                               int Rpad, int Kld) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)Rpad * Kld) return;
+  const int r = (int)(idx % Kld);
+  const size_t pl = (size_t)Rpad * Kld;
+  for (int t = 0; t < L; ++t) {
+    int dlo = 0, dhi = 0;
+    if (r < k) {
+      const int p = primes[t];
+      const long long v = (long long)in[(size_t)(2 * t) * pl + idx] + 256LL * in[(size_t)(2 * t + 1) * pl + idx];
+      long long w = v * dres[(size_t)t * k + r] % p;
+      if (w < 0) w += p;
+      int sv = (int)w;
+      if (sv > p / 2) sv -= p;
+      dlo = ((sv + 128) & 255) - 128;
+      dhi = (sv - dlo) >> 8;
+    }
+    out[(size_t)(2 * t) * pl + idx] = (int8_t)dlo;
+    out[(size_t)(2 * t + 1) * pl + idx] = (int8_t)dhi;
+  }
+}
+
+// svec_quadratic residues: out[t * kmax + k] = sum_{i <= j} c_ij x_tri(j)+i q_ik q_jk mod p_t,
+// c_ii = c[0] (the value 1), c_ij = c[1] (the working-precision sqrt 2).  One thread per (k, t).
+extern "C" __global__ void k_rns_svec_quadratic(int h, int kmax, const int* __restrict__ xr, const int* __restrict__ qr,
+                                                const int* __restrict__ cr, int L, const int* __restrict__ primes,
+                                                int* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x, t = blockIdx.y;
+  if (k >= kmax || t >= L) return;
+  const unsigned long long p = (unsigned)primes[t];
+  const int tri = h * (h + 1) / 2;
+  const int* x = xr + (size_t)t * tri;
+  const int* q = qr + (size_t)t * h * kmax + (size_t)k * h;
+  const unsigned long long c0 = (unsigned)cr[2 * t], c1 = (unsigned)cr[2 * t + 1];
+  unsigned long long acc = 0;  // terms below 2^15 each
+  for (int j = 0; j < h; ++j) {
+    const unsigned long long qj = (unsigned)q[j];
+    unsigned long long row = 0;  // sum_{i < j} x_ij q_i, terms below 2^30
+    for (int i = 0; i < j; ++i) row += (unsigned long long)(unsigned)x[j * (j + 1) / 2 + i] * (unsigned)q[i];
+    row %= p;
+    acc += (row * c1 % p) * qj % p;
+    acc += ((unsigned long long)(unsigned)x[j * (j + 1) / 2 + j] * qj % p) * qj % p * c0 % p;
+  }
+  out[(size_t)t * kmax + k] = (int)(acc % p);
+}
+
+// symmetric_bilinear residues: out[t * np + s] = q_a' X q_b mod p_t for pair s = (a, b), X
+// symmetric from its packed upper triangle (entry (i, j), i <= j, at tri(j) + i).
+extern "C" __global__ void k_rns_bilinear(int h, int cols, const int* __restrict__ xr, const int* __restrict__ qr,
+                                          const unsigned long long* __restrict__ pairs, int np, int L,
+                                          const int* __restrict__ primes, int* __restrict__ out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x, t = blockIdx.y;
+  if (s >= np || t >= L) return;
+  const unsigned long long p = (unsigned)primes[t];
+  const int tri = h * (h + 1) / 2;
+  const int* x = xr + (size_t)t * tri;
+  const int* qa = qr + (size_t)t * h * cols + (size_t)pairs[2 * s] * h;
+  const int* qb = qr + (size_t)t * h * cols + (size_t)pairs[2 * s + 1] * h;
+  unsigned long long acc = 0;
+  for (int j = 0; j < h; ++j) {
+    unsigned long long u = 0;  // (X q_a)_j, terms below 2^30
+    for (int i = 0; i < h; ++i) {
+      const int lo = i < j ? i : j, hi = i < j ? j : i;
+      u += (unsigned long long)(unsigned)x[hi * (hi + 1) / 2 + lo] * (unsigned)qa[i];
+    }
+    acc += (u % p) * (unsigned)qb[j] % p;
+  }
+  out[(size_t)t * np + s] = (int)(acc % p);
+}
+
 namespace {
 
 // Host tables of one prime set (descending primes below 2^bits).
@@ -565,6 +675,11 @@ struct RnsWorkspace {
   DevBuf<int8_t> PA, PB;      // INT8 form: digit planes
   DevBuf<int> RC8;            // INT8 form: residues of the product
   DevBuf<int> RT8, loX, bitsX, loB2;  // congruence: intermediate residues, X scan, column offsets
+  DevBuf<int> cres, clo, cbits, cmax;   // exact forms: class residues, class scans
+  DevBuf<unsigned char> zs, ys, fd;     // block products: stacked operands, staging
+  DevBuf<long> boff;                    // block products: row, factor and column offsets
+  DevBuf<int> bq;
+  DevBuf<unsigned long long> bcols, bpairs;
   int form = 0;               // 0: INT8 tensor cores, 1: FP64
 };
 
@@ -575,7 +690,6 @@ constexpr int kI8Chunk = 1 << 16;  // K per modular GEMM call (INT32 accumulator
 int32_t rns_product(RnsWorkspace& ws, cudaStream_t st, int form, int N, char ta, char tb, uint64_t m,
                     uint64_t n, uint64_t k, const unsigned char* dA, uint64_t lda, const unsigned char* dB,
                     uint64_t ldb, int upper_only, unsigned char* dC, uint32_t* hs_out) {
-  const size_t esz = 8 * (size_t)N + 8;
   grow(ws.loA, m); grow(ws.bitsA, m); grow(ws.loB, n); grow(ws.bitsB, n);
   grow(ws.maxbits, 2); grow(ws.status, 1); grow(ws.err, 1);
   check(cudaMemsetAsync(ws.maxbits.p, 0, 2 * sizeof(int), st), "memset");
@@ -780,6 +894,245 @@ int32_t rns_congruence(RnsWorkspace& ws, cudaStream_t st, int N, char ta, uint64
   if (herr) throw CudaError("modular INT8 GEMM: a bounded wait gave up");
   if (hs_out) *hs_out = hs;
   return 0;
+}
+
+
+// ---- exact forms of small factors: every output is one exact sum of products of MpFloat
+// factors, rounded once.  Each operand is one class aligned at its lowest set bit, so a term's
+// integer is the product of its factors' integers and every term of an output carries the same
+// power of two; per prime the sums run on CUDA cores (the shapes are per-block sized), and the
+// CRT rounds once. ----
+
+// Scans of `n` flat arrays (one line each) into (lo, bits) on the host; returns false (status
+// bits in *hs) when an operand is not finite.
+bool scan_classes(RnsWorkspace& ws, cudaStream_t st, int N, const unsigned char* const* arr, const int* count, int n,
+                  int* lo, int* bits, uint32_t* hs) {
+  grow(ws.clo, n); grow(ws.cbits, n); grow(ws.cmax, n); grow(ws.status, 1);
+  check(cudaMemsetAsync(ws.status.p, 0, sizeof(uint32_t), st), "memset");
+  check(cudaMemsetAsync(ws.cmax.p, 0, n * sizeof(int), st), "memset");
+  for (int c = 0; c < n; ++c)
+    ++g_launches, k_rns_scan<<<1, 32, 0, st>>>(arr[c], N, 1, count[c], 0, 1, ws.clo.p + c, ws.cbits.p + c,
+                                               ws.cmax.p + c, ws.status);
+  copy_d2h(lo, ws.clo.p, n * sizeof(int), st);
+  copy_d2h(bits, ws.cbits.p, n * sizeof(int), st);
+  copy_d2h(hs, ws.status.p, sizeof(uint32_t), st);
+  check(cudaStreamSynchronize(st), "sync");
+  return *hs == 0;
+}
+
+// Primes (15 bits) covering `needed` bits, or 0 when the set is too small.
+int primes_for(double needed) {
+  const auto& ps = prime_list(15);
+  int L = 0;
+  double acc = 0;
+  while (L < RNS_MAXL && acc <= needed) acc += std::log2((double)ps[L++]);
+  if (acc <= needed || (int)(acc / 64) + 2 > RNS_MAXW) return 0;
+  return L;
+}
+
+int ceil_log2(uint64_t v) {
+  int lg = 0;
+  while ((1ull << lg) < std::max<uint64_t>(v, 1)) ++lg;
+  return lg;
+}
+
+// CRT of `count` outputs (residues ws.RC8[t * count + o]) at exponent `lo` into dOut.
+void crt_vector(RnsWorkspace& ws, cudaStream_t st, DevTables& DT, const PrimeTables& T, int N, int L, int count,
+                int lo, unsigned char* dOut) {
+  grow(ws.loA, count); grow(ws.loB, 1);
+  ++g_launches, k_fill_int<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(ws.loA, count, lo);
+  ++g_launches, k_fill_int<<<1, 32, 0, st>>>(ws.loB, 1, 0);
+  ++g_launches, k_rns_crt<int><<<(unsigned)((count + 127) / 128), 128, 0, st>>>(
+      ws.RC8, count, count, 1, L, T.WW, DT.primes, DT.inv, DT.pmod, DT.M, DT.half, ws.loA, ws.loB, N, 0, dOut,
+      ws.status);
+}
+
+// The residue tables of the classes: class c's residues at ws.cres + off[c] * L (count[c] per prime).
+void class_residues(RnsWorkspace& ws, cudaStream_t st, DevTables& DT, int N, int L, const unsigned char* const* arr,
+                    const int* count, const int* lo, const int* absval, int n, int maxbits, size_t* off) {
+  size_t total = 0;
+  for (int c = 0; c < n; ++c) {
+    off[c] = total;
+    total += (size_t)std::max(count[c], 1);
+  }
+  grow(ws.cres, total * L);
+  const int S = 64 * N + maxbits + 1;
+  grow(ws.pow2, (size_t)L * S);
+  ++g_launches, k_rns_pow2<<<dim3((S + 255) / 256, L), 256, 0, st>>>(L, DT.iprimes, S, ws.pow2);
+  for (int c = 0; c < n; ++c)
+    if (count[c])
+      ++g_launches, k_rns_class_residues<<<(unsigned)((count[c] + 127) / 128), 128, 0, st>>>(
+          arr[c], N, count[c], lo[c], absval[c], L, DT.iprimes, ws.pow2, S, ws.cres.p + off[c] * L);
+}
+
+// v[k] = sum_{i <= j} c_ij x_tri(j)+i q_ik q_jk (c_ii = 1, c_ij = sqrt2), k < kmax, each rounded
+// once (rns_blas.rs:4025-4174 svec_quadratic).  dC2 holds the two coefficients (1, sqrt2).
+int32_t rns_svec_quadratic(RnsWorkspace& ws, cudaStream_t st, int N, int h, int kmax, const unsigned char* dQ,
+                           int abs_q, const unsigned char* dX, const unsigned char* dC2, unsigned char* dOut,
+                           uint32_t* hs_out) {
+  const int tri = h * (h + 1) / 2;
+  const unsigned char* arr[3] = {dQ, dX, dC2};
+  const int count[3] = {h * kmax, tri, 2};
+  int lo[3], bits[3];
+  uint32_t hs = 0;
+  if (!scan_classes(ws, st, N, arr, count, 3, lo, bits, &hs)) {
+    if (hs_out) *hs_out = hs;
+    g_last_error = "sdpxg_rns_svec_quadratic: non-finite operands are not supported";
+    return 2;
+  }
+  const int L = primes_for(2.0 * bits[0] + bits[1] + bits[2] + ceil_log2((uint64_t)tri) + 2);
+  if (!L) {
+    g_last_error = "sdpxg_rns_svec_quadratic: exponent spread too wide for the prime set";
+    return 2;
+  }
+  DevTables& DT = ws.t15;
+  const PrimeTables& T = DT.get(15, L, st);
+  size_t off[3];
+  const int absv[3] = {abs_q, 0, 0};
+  class_residues(ws, st, DT, N, L, arr, count, lo, absv, 3, std::max(bits[0], std::max(bits[1], bits[2])), off);
+  grow(ws.RC8, (size_t)L * kmax);
+  ++g_launches, k_rns_svec_quadratic<<<dim3((unsigned)((kmax + 63) / 64), (unsigned)L), 64, 0, st>>>(
+      h, kmax, ws.cres.p + off[1] * L, ws.cres.p + off[0] * L, ws.cres.p + off[2] * L, L, DT.iprimes, ws.RC8);
+  crt_vector(ws, st, DT, T, N, L, kmax, 2 * lo[0] + lo[1] + lo[2], dOut);
+  check(cudaGetLastError(), "svec_quadratic launch");
+  copy_d2h(&hs, ws.status.p, sizeof(uint32_t), st);
+  check(cudaStreamSynchronize(st), "sync");
+  if (hs_out) *hs_out = hs;
+  return 0;
+}
+
+// out[s] = q_a' X q_b for the pairs s = (a, b), each the exact sum rounded once
+// (rns_blas.rs:4175-4277 symmetric_bilinear); X packed upper without svec factors.
+int32_t rns_bilinear(RnsWorkspace& ws, cudaStream_t st, int N, int h, int cols, const unsigned char* dQ,
+                     const unsigned char* dX, const unsigned long long* dPairs, int np, unsigned char* dOut,
+                     uint32_t* hs_out) {
+  const unsigned char* arr[2] = {dQ, dX};
+  const int count[2] = {h * cols, h * (h + 1) / 2};
+  int lo[2], bits[2];
+  uint32_t hs = 0;
+  if (!scan_classes(ws, st, N, arr, count, 2, lo, bits, &hs)) {
+    if (hs_out) *hs_out = hs;
+    g_last_error = "sdpxg_rns_symmetric_bilinear: non-finite operands are not supported";
+    return 2;
+  }
+  const int L = primes_for(2.0 * bits[0] + bits[1] + 2 * ceil_log2((uint64_t)h) + 2);
+  if (!L) {
+    g_last_error = "sdpxg_rns_symmetric_bilinear: exponent spread too wide for the prime set";
+    return 2;
+  }
+  DevTables& DT = ws.t15;
+  const PrimeTables& T = DT.get(15, L, st);
+  size_t off[2];
+  const int absv[2] = {0, 0};
+  class_residues(ws, st, DT, N, L, arr, count, lo, absv, 2, std::max(bits[0], bits[1]), off);
+  grow(ws.RC8, (size_t)L * np);
+  ++g_launches, k_rns_bilinear<<<dim3((unsigned)((np + 63) / 64), (unsigned)L), 64, 0, st>>>(
+      h, cols, ws.cres.p + off[1] * L, ws.cres.p + off[0] * L, dPairs, np, L, DT.iprimes, ws.RC8);
+  crt_vector(ws, st, DT, T, N, L, np, 2 * lo[0] + lo[1], dOut);
+  check(cudaGetLastError(), "symmetric_bilinear launch");
+  copy_d2h(&hs, ws.status.p, sizeof(uint32_t), st);
+  check(cudaStreamSynchronize(st), "sync");
+  if (hs_out) *hs_out = hs;
+  return 0;
+}
+
+// C = A' diag(d) A (m x m) for A k x m (ld lda), every entry the exact sum rounded once
+// (rns_blas.rs:2990-3194 diag_congruence), on the INT8 tensor cores: the columns of A aligned
+// per column (lo_j), d as one class (lo_d); the right operand's residues are the left operand's
+// times d's, and the CRT exponent of (i, j) is lo_i + lo_j + lo_d.
+int32_t rns_diag_congruence(RnsWorkspace& ws, cudaStream_t st, int N, uint64_t m, uint64_t k,
+                            const unsigned char* dA, uint64_t lda, const unsigned char* dD, int upper_only,
+                            unsigned char* dC, uint32_t* hs_out) {
+  grow(ws.loA, m); grow(ws.bitsA, m); grow(ws.loB2, m);
+  grow(ws.maxbits, 2); grow(ws.status, 1); grow(ws.err, 1);
+  const unsigned char* arr[1] = {dD};
+  const int count[1] = {(int)k};
+  int lo_d = 0, bits_d = 0;
+  uint32_t hs = 0;
+  if (!scan_classes(ws, st, N, arr, count, 1, &lo_d, &bits_d, &hs)) {
+    if (hs_out) *hs_out = hs;
+    g_last_error = "sdpxg_rns_diag_congruence: non-finite operands are not supported";
+    return 2;
+  }
+  check(cudaMemsetAsync(ws.maxbits.p, 0, 2 * sizeof(int), st), "memset");
+  ++g_launches, k_rns_scan<<<(unsigned)((m + 7) / 8), 256, 0, st>>>(dA, N, (int)m, (int)k, (long)lda, 1, ws.loA,
+                                                                 ws.bitsA, ws.maxbits, ws.status);
+  int hb[2] = {0, 0};
+  copy_d2h(hb, ws.maxbits.p, 2 * sizeof(int), st);
+  copy_d2h(&hs, ws.status.p, sizeof(uint32_t), st);
+  check(cudaStreamSynchronize(st), "sync");
+  if (hs) {
+    if (hs_out) *hs_out = hs;
+    g_last_error = "sdpxg_rns_diag_congruence: non-finite operands are not supported";
+    return 2;
+  }
+  const int L = primes_for(2.0 * hb[0] + bits_d + ceil_log2(k) + 2);
+  if (!L) {
+    g_last_error = "sdpxg_rns_diag_congruence: exponent spread too wide for the prime set";
+    return 2;
+  }
+  DevTables& DT = ws.t15;
+  const PrimeTables& T = DT.get(15, L, st);
+  const int Mpad = (int)((m + 127) / 128 * 128), Kpad = (int)((k + 127) / 128 * 128);
+  const long planeC = (long)(m * m);
+  grow(ws.RC8, (size_t)L * planeC);
+  size_t off[1];
+  const int absv[1] = {0};
+  class_residues(ws, st, DT, N, L, arr, count, &lo_d, absv, 1, std::max(hb[0], bits_d), off);
+  const int S = 64 * N + std::max(hb[0], bits_d) + 1;  // the table class_residues just built
+  grow(ws.PA, (size_t)L * 2 * Mpad * Kpad);
+  grow(ws.PB, (size_t)L * 2 * Mpad * Kpad);
+  ++g_launches, k_rns8_residues<<<(unsigned)(((long)Mpad * Kpad + 255) / 256), 256, 0, st>>>(
+      dA, N, (int)m, (int)k, (long)lda, 1, ws.loA, L, DT.iprimes, ws.pow2, S, ws.PA, Mpad, Kpad);
+  ++g_launches, k_rns8_scale_planes<<<(unsigned)(((long)Mpad * Kpad + 255) / 256), 256, 0, st>>>(
+      ws.PA, ws.cres.p + off[0] * L, (int)k, L, DT.iprimes, ws.PB, Mpad, Kpad);
+  check(cudaMemsetAsync(ws.err.p, 0, sizeof(int), st), "memset");
+  for (int k0 = 0; k0 < Kpad; k0 += kI8Chunk) {
+    I8GemmArgs ga;
+    ga.Mpad = Mpad; ga.Npad = Mpad; ga.Kld = Kpad; ga.k0 = k0; ga.Kpad = std::min(kI8Chunk, Kpad - k0);
+    ga.m = (int)m; ga.n = (int)m; ga.L = L; ga.moduli = DT.iprimes; ga.upper_only = upper_only;
+    ga.accumulate = k0 > 0; ga.out = ws.RC8.p; ga.plane = planeC; ga.err = ws.err.p;
+    launch_i8_gemm(2, ws.PA, ws.PB, ga, st);
+  }
+  ++g_launches, k_add_const_int<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(ws.loA, (int)m, lo_d, ws.loB2);
+  ++g_launches, k_rns_crt<int><<<(unsigned)((m * m + 127) / 128), 128, 0, st>>>(
+      ws.RC8, planeC, (int)m, (int)m, L, T.WW, DT.primes, DT.inv, DT.pmod, DT.M, DT.half, ws.loA, ws.loB2, N,
+      upper_only ? 1 : 0, dC, ws.status);
+  check(cudaGetLastError(), "diag_congruence launch");
+  int herr = 0;
+  copy_d2h(&hs, ws.status.p, sizeof(uint32_t), st);
+  copy_d2h(&herr, ws.err.p, sizeof(int), st);
+  check(cudaStreamSynchronize(st), "sync");
+  if (herr) throw CudaError("modular INT8 GEMM: a bounded wait gave up");
+  if (hs_out) *hs_out = hs;
+  return 0;
+}
+
+// Upper triangle of sum_b Z_b' Y_b with Z_b = diag(d_b) Y_b rounded entrywise, the exact sum over
+// every block and row rounded once (rns_blas.rs:2656-2923 gemm_blocks_upper): the blocks are
+// stacked into W x m operands (zeros off their columns, Z rounded while stacking) and multiplied
+// by the exact product (W = the blocks' total width).  hr0/hyoff/hcoff/hq: host offsets.
+int32_t rns_blocks_upper(RnsWorkspace& ws, cudaStream_t st, int N, uint64_t m, int nb, const std::vector<long>& hr0,
+                         const std::vector<long>& hyoff, const std::vector<long>& hcoff, const std::vector<int>& hq,
+                         const unsigned char* dY, const unsigned char* dD, const unsigned long long* dCols,
+                         unsigned char* dC, uint32_t* hs_out) {
+  const size_t esz = 8 * (size_t)N + 8;
+  const long W = hr0[nb];
+  grow(ws.boff, 3 * (size_t)nb + 1);
+  grow(ws.bq, nb);
+  std::vector<long> offs(hr0.begin(), hr0.end());
+  offs.insert(offs.end(), hyoff.begin(), hyoff.end());
+  offs.insert(offs.end(), hcoff.begin(), hcoff.end());
+  ws.boff.upload(offs.data(), offs.size(), st);
+  ws.bq.upload(hq.data(), nb, st);
+  grow(ws.zs, (size_t)W * m * esz);
+  grow(ws.ys, (size_t)W * m * esz);
+  grow(ws.status, 1);
+  check(cudaMemsetAsync(ws.status.p, 0, sizeof(uint32_t), st), "memset");
+  mp_launch_stack_blocks(nb, ws.boff.p, ws.boff.p + nb + 1, ws.boff.p + 2 * nb + 1, ws.bq.p, dY, dD, dCols, W,
+                         (int)m, N, ws.zs, ws.ys, ws.status, st);
+  return rns_product(ws, st, ws.form, N, 'T', 'N', m, m, (uint64_t)W, ws.zs, (uint64_t)W, ws.ys, (uint64_t)W, 1, dC,
+                     hs_out);
 }
 
 // The reference's dense MPFR LDL' (ArrowLDLSolver::try_dense -> ldl_rec, arrow.rs:255-470) on
@@ -1152,4 +1505,227 @@ extern "C" int32_t sdpxg_mp_potrf(sdpxg_ctx* ctx, uint32_t limbs, char uplo, uin
     g_last_error = "internal error";
     return 5;
   }
+}
+
+// ---- entry points of the exact forms (host arrays in the reference's MpFloat<N> layout) ----
+namespace {
+template <class F>
+int32_t rns_entry(F&& f) {
+  try {
+    return f();
+  } catch (const std::invalid_argument& e) {
+    g_last_error = e.what();
+    return 1;
+  } catch (const std::exception& e) {
+    g_last_error = std::string("internal error: ") + e.what();
+    return 5;
+  } catch (...) {
+    g_last_error = "internal error";
+    return 5;
+  }
+}
+Engine* entry_engine(sdpxg_ctx* ctx, uint32_t limbs, const char* name, uint32_t max_limbs) {
+  Engine* E = ctx_engine_any(ctx);
+  if (!E) throw std::invalid_argument("null context");
+  if (limbs < 1 || limbs > max_limbs)
+    throw std::invalid_argument(std::string(name) + ": limbs must be in 1.." + std::to_string(max_limbs));
+  check(cudaSetDevice(E->device), "cudaSetDevice");
+  return E;
+}
+void zero_outputs(void* out, size_t count, int N) {
+  const size_t esz = 8 * (size_t)N + 8;
+  unsigned char* o = static_cast<unsigned char*>(out);
+  std::memset(o, 0, count * esz);
+  for (size_t e = 0; e < count; ++e) *reinterpret_cast<int*>(o + e * esz + 8 * N) = MP_ZERO;
+}
+}  // namespace
+
+extern "C" int32_t sdpxg_rns_diag_congruence(sdpxg_ctx* ctx, uint32_t limbs, uint64_t m, uint64_t k, const void* A,
+                                             uint64_t lda, const void* d, uint32_t upper_only, void* C,
+                                             uint32_t* status) {
+  return rns_entry([&]() -> int32_t {
+    Engine* E = entry_engine(ctx, limbs, "sdpxg_rns_diag_congruence", RNS_MAXN);
+    const int N = (int)limbs;
+    if (m > (1u << 20) || k > (1u << 20)) throw std::invalid_argument("size overflow");
+    if (lda < std::max<uint64_t>(k, 1)) throw std::invalid_argument("leading dimension too small");
+    if (status) *status = 0;
+    if (m == 0) return 0;
+    if (!A || !d || !C) throw std::invalid_argument("null pointer");
+    if (k == 0) {
+      zero_outputs(C, m * m, N);
+      return 0;
+    }
+    const size_t esz = 8 * (size_t)N + 8, na = lda * (m - 1) + k;
+    RnsWorkspace& ws = workspace(ctx);
+    cudaStream_t st = E->st;
+    grow(ws.a, na * esz);
+    grow(ws.b, k * esz);
+    grow(ws.c, m * m * esz);
+    ws.a.upload(static_cast<const unsigned char*>(A), na * esz, st);
+    ws.b.upload(static_cast<const unsigned char*>(d), k * esz, st);
+    uint32_t hs = 0;
+    const int32_t rc = rns_diag_congruence(ws, st, N, m, k, ws.a, lda, ws.b, upper_only ? 1 : 0, ws.c, &hs);
+    if (status) *status = hs;
+    if (rc) return rc;
+    copy_d2h(C, ws.c.p, m * m * esz, st);
+    check(cudaStreamSynchronize(st), "sync");
+    return 0;
+  });
+}
+
+extern "C" int32_t sdpxg_rns_svec_quadratic(sdpxg_ctx* ctx, uint32_t limbs, uint64_t h, uint64_t kmax, const void* Q,
+                                            uint32_t abs_q, const void* x, const void* sqrt2, void* out,
+                                            uint32_t* status) {
+  return rns_entry([&]() -> int32_t {
+    Engine* E = entry_engine(ctx, limbs, "sdpxg_rns_svec_quadratic", RNS_MAXN);
+    const int N = (int)limbs;
+    if (h > 4096 || kmax > (1u << 20)) throw std::invalid_argument("size overflow");
+    if (status) *status = 0;
+    if (kmax == 0) return 0;
+    if (!Q || !x || !sqrt2 || !out) throw std::invalid_argument("null pointer");
+    if (h == 0) {
+      zero_outputs(out, kmax, N);
+      return 0;
+    }
+    const size_t esz = 8 * (size_t)N + 8, tri = h * (h + 1) / 2;
+    RnsWorkspace& ws = workspace(ctx);
+    cudaStream_t st = E->st;
+    grow(ws.a, h * kmax * esz);
+    grow(ws.b, tri * esz);
+    grow(ws.fd, 2 * esz);
+    grow(ws.c, kmax * esz);
+    std::vector<unsigned char> c2(2 * esz, 0);  // (1, sqrt2): 1 = 2^63 in the top limb, exponent 1
+    reinterpret_cast<unsigned long long*>(c2.data())[N - 1] = 1ull << 63;
+    *reinterpret_cast<int*>(&c2[8 * N]) = MP_REGULAR;
+    *reinterpret_cast<int*>(&c2[8 * N + 4]) = 1;
+    std::memcpy(&c2[esz], sqrt2, esz);
+    ws.a.upload(static_cast<const unsigned char*>(Q), h * kmax * esz, st);
+    ws.b.upload(static_cast<const unsigned char*>(x), tri * esz, st);
+    ws.fd.upload(c2.data(), 2 * esz, st);
+    uint32_t hs = 0;
+    const int32_t rc = rns_svec_quadratic(ws, st, N, (int)h, (int)kmax, ws.a, abs_q ? 1 : 0, ws.b, ws.fd, ws.c, &hs);
+    if (status) *status = hs;
+    if (rc) return rc;
+    copy_d2h(out, ws.c.p, kmax * esz, st);
+    check(cudaStreamSynchronize(st), "sync");
+    return 0;
+  });
+}
+
+extern "C" int32_t sdpxg_rns_symmetric_bilinear(sdpxg_ctx* ctx, uint32_t limbs, uint64_t h, uint64_t columns,
+                                                const void* Q, const void* X, uint64_t npairs, const uint64_t* pairs,
+                                                void* out, uint32_t* status) {
+  return rns_entry([&]() -> int32_t {
+    Engine* E = entry_engine(ctx, limbs, "sdpxg_rns_symmetric_bilinear", RNS_MAXN);
+    const int N = (int)limbs;
+    if (h > 4096 || columns > (1u << 20) || npairs > (1u << 24)) throw std::invalid_argument("size overflow");
+    if (status) *status = 0;
+    if (npairs == 0) return 0;
+    if (!Q || !X || !pairs || !out) throw std::invalid_argument("null pointer");
+    for (uint64_t s = 0; s < 2 * npairs; ++s)
+      if (pairs[s] >= columns) throw std::invalid_argument("pair column out of range");
+    if (h == 0) {
+      zero_outputs(out, npairs, N);
+      return 0;
+    }
+    const size_t esz = 8 * (size_t)N + 8, tri = h * (h + 1) / 2;
+    RnsWorkspace& ws = workspace(ctx);
+    cudaStream_t st = E->st;
+    grow(ws.a, h * columns * esz);
+    grow(ws.b, tri * esz);
+    grow(ws.c, npairs * esz);
+    grow(ws.bpairs, 2 * npairs);
+    ws.a.upload(static_cast<const unsigned char*>(Q), h * columns * esz, st);
+    ws.b.upload(static_cast<const unsigned char*>(X), tri * esz, st);
+    ws.bpairs.upload(reinterpret_cast<const unsigned long long*>(pairs), 2 * npairs, st);
+    uint32_t hs = 0;
+    const int32_t rc = rns_bilinear(ws, st, N, (int)h, (int)columns, ws.a, ws.b, ws.bpairs, (int)npairs, ws.c, &hs);
+    if (status) *status = hs;
+    if (rc) return rc;
+    copy_d2h(out, ws.c.p, npairs * esz, st);
+    check(cudaStreamSynchronize(st), "sync");
+    return 0;
+  });
+}
+
+extern "C" int32_t sdpxg_rns_gemm_blocks_upper(sdpxg_ctx* ctx, uint32_t limbs, uint64_t m, uint64_t nblocks,
+                                               const uint64_t* widths, const uint64_t* counts, const void* y,
+                                               const void* d, const uint64_t* columns, void* C, uint32_t* status) {
+  return rns_entry([&]() -> int32_t {
+    Engine* E = entry_engine(ctx, limbs, "sdpxg_rns_gemm_blocks_upper", kMpMaxLimbs);
+    const int N = (int)limbs;
+    if (m > (1u << 16) || nblocks > (1u << 20)) throw std::invalid_argument("size overflow");
+    if (status) *status = 0;
+    if (m == 0) return 0;
+    if (!C || (nblocks && (!widths || !counts))) throw std::invalid_argument("null pointer");
+    std::vector<long> r0(1, 0), yoff, coff;
+    std::vector<int> q;
+    long ytot = 0, ctot = 0;
+    for (uint64_t b = 0; b < nblocks; ++b) {
+      if (widths[b] > (1u << 20) || counts[b] > m) throw std::invalid_argument("block extent out of range");
+      if (widths[b] == 0 || counts[b] == 0) continue;  // an empty block adds nothing
+      yoff.push_back(ytot);
+      coff.push_back(ctot);
+      q.push_back((int)counts[b]);
+      r0.push_back(r0.back() + (long)widths[b]);
+      ytot += (long)(widths[b] * counts[b]);
+      ctot += (long)counts[b];
+    }
+    // columns of every (nonempty or not) block, in order: validate sorted and in range
+    uint64_t cpos = 0;
+    std::vector<unsigned long long> cols;
+    for (uint64_t b = 0; b < nblocks; ++b) {
+      for (uint64_t c = 0; c < counts[b]; ++c) {
+        const uint64_t v = columns[cpos + c];
+        if (v >= m || (c && v <= columns[cpos + c - 1]))
+          throw std::invalid_argument("block columns must be increasing and below m");
+        if (widths[b]) cols.push_back(v);
+      }
+      cpos += counts[b];
+    }
+    const int nb = (int)q.size();
+    if (nb == 0 || r0.back() * (long)m > (1L << 28)) {
+      if (nb == 0) {
+        zero_outputs(C, m * m, N);
+        return 0;
+      }
+      throw std::invalid_argument("stacked block operands too large");
+    }
+    if (!y || !d || !columns) throw std::invalid_argument("null pointer");
+    // the inputs of the nonempty blocks, packed in order
+    const size_t esz = 8 * (size_t)N + 8;
+    std::vector<unsigned char> hy((size_t)ytot * esz), hd((size_t)r0.back() * esz);
+    {
+      const unsigned char* ys = static_cast<const unsigned char*>(y);
+      const unsigned char* ds = static_cast<const unsigned char*>(d);
+      size_t yi = 0, di = 0, yo = 0, dO = 0;
+      for (uint64_t b = 0; b < nblocks; ++b) {
+        const size_t ny = widths[b] * counts[b], nd = widths[b];
+        if (widths[b] && counts[b]) {
+          std::memcpy(&hy[yo * esz], ys + yi * esz, ny * esz);
+          std::memcpy(&hd[dO * esz], ds + di * esz, nd * esz);
+          yo += ny;
+          dO += nd;
+        }
+        yi += ny;
+        di += nd;
+      }
+    }
+    RnsWorkspace& ws = workspace(ctx);
+    cudaStream_t st = E->st;
+    grow(ws.a, hy.size());
+    grow(ws.b, hd.size());
+    grow(ws.c, m * m * esz);
+    grow(ws.bcols, cols.size());
+    ws.a.upload(hy.data(), hy.size(), st);
+    ws.b.upload(hd.data(), hd.size(), st);
+    ws.bcols.upload(cols.data(), cols.size(), st);
+    uint32_t hs = 0;
+    const int32_t rc = rns_blocks_upper(ws, st, N, m, nb, r0, yoff, coff, q, ws.a, ws.b, ws.bcols, ws.c, &hs);
+    if (status) *status = hs;
+    if (rc) return rc;
+    copy_d2h(C, ws.c.p, m * m * esz, st);
+    check(cudaStreamSynchronize(st), "sync");
+    return 0;
+  });
 }

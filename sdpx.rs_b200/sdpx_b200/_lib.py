@@ -118,6 +118,14 @@ SIGNATURES = {
     "sdpxg_mp_potrf": (i32, [C.c_void_p, u32, C.c_char, u64, C.c_void_p, u64, C.POINTER(i32), PU32]),
     "sdpxg_rns_congruence": (i32, [C.c_void_p, u32, C.c_char, u64, u64, C.c_void_p, u64, C.c_void_p,
                                    u64, u32, C.c_void_p, PU32]),
+    "sdpxg_rns_diag_congruence": (i32, [C.c_void_p, u32, u64, u64, C.c_void_p, u64, C.c_void_p, u32,
+                                        C.c_void_p, PU32]),
+    "sdpxg_rns_svec_quadratic": (i32, [C.c_void_p, u32, u64, u64, C.c_void_p, u32, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, PU32]),
+    "sdpxg_rns_symmetric_bilinear": (i32, [C.c_void_p, u32, u64, u64, C.c_void_p, C.c_void_p, u64,
+                                           C.POINTER(u64), C.c_void_p, PU32]),
+    "sdpxg_rns_gemm_blocks_upper": (i32, [C.c_void_p, u32, u64, u64, C.POINTER(u64), C.POINTER(u64),
+                                          C.c_void_p, C.c_void_p, C.POINTER(u64), C.c_void_p, PU32]),
 }
 
 _lib = None

@@ -537,6 +537,53 @@ class KernelContext:
                   C.c_char_p(X), ldx, int(upper_only), out, C.byref(st))
         return out.raw[:m * m * esz], st.value
 
+    def rns_diag_congruence(self, limbs: int, m: int, k: int, A: bytes, lda: int, d: bytes,
+                            upper_only: bool = False):
+        """Exact A' diag(d) A (A k x m) of MpFloat<limbs> arrays: (raw bytes m x m, status)."""
+        esz = 8 * limbs + 8
+        out = C.create_string_buffer(max(m * m * esz, 1))
+        st = C.c_uint32()
+        _lib.call("sdpxg_rns_diag_congruence", self._h, limbs, m, k, C.c_char_p(A), lda, C.c_char_p(d),
+                  int(upper_only), out, C.byref(st))
+        return out.raw[:m * m * esz], st.value
+
+    def rns_svec_quadratic(self, limbs: int, h: int, kmax: int, Q: bytes, x: bytes, sqrt2: bytes,
+                           abs_q: bool = False):
+        """Exact svec quadratic forms (one MpFloat<limbs> per basis column): (raw bytes, status)."""
+        esz = 8 * limbs + 8
+        out = C.create_string_buffer(max(kmax * esz, 1))
+        st = C.c_uint32()
+        _lib.call("sdpxg_rns_svec_quadratic", self._h, limbs, h, kmax, C.c_char_p(Q), int(abs_q),
+                  C.c_char_p(x), C.c_char_p(sqrt2), out, C.byref(st))
+        return out.raw[:kmax * esz], st.value
+
+    def rns_symmetric_bilinear(self, limbs: int, h: int, columns: int, Q: bytes, X: bytes, pairs):
+        """Exact q_a' X q_b for the given (a, b) pairs: (raw bytes, status)."""
+        esz = 8 * limbs + 8
+        flat = [int(v) for ab in pairs for v in ab]
+        arr = (C.c_uint64 * max(len(flat), 1))(*flat)
+        out = C.create_string_buffer(max(len(pairs) * esz, 1))
+        st = C.c_uint32()
+        _lib.call("sdpxg_rns_symmetric_bilinear", self._h, limbs, h, columns, C.c_char_p(Q), C.c_char_p(X),
+                  len(pairs), arr, out, C.byref(st))
+        return out.raw[:len(pairs) * esz], st.value
+
+    def rns_gemm_blocks_upper(self, limbs: int, m: int, blocks):
+        """Upper triangle of sum_b (diag(d_b) Y_b)' Y_b over blocks (y bytes, d bytes, columns,
+        width): (raw bytes m x m, status)."""
+        esz = 8 * limbs + 8
+        widths = (C.c_uint64 * max(len(blocks), 1))(*[b[3] for b in blocks])
+        counts = (C.c_uint64 * max(len(blocks), 1))(*[len(b[2]) for b in blocks])
+        cols = [int(c) for b in blocks for c in b[2]]
+        carr = (C.c_uint64 * max(len(cols), 1))(*cols)
+        y = b"".join(b[0] for b in blocks)
+        d = b"".join(b[1] for b in blocks)
+        out = C.create_string_buffer(max(m * m * esz, 1))
+        st = C.c_uint32()
+        _lib.call("sdpxg_rns_gemm_blocks_upper", self._h, limbs, m, len(blocks), widths, counts,
+                  C.c_char_p(y) if y else None, C.c_char_p(d) if d else None, carr, out, C.byref(st))
+        return out.raw[:m * m * esz], st.value
+
     def mp_ldl(self, limbs: int, n: int, A: bytes, lda: int, reg: Optional[bytes] = None):
         """The reference's dense MPFR LDL' of an n x n MpFloat<limbs> matrix (raw bytes):
         returns (L bytes n x n, dinv bytes n, status)."""
