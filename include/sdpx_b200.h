@@ -350,6 +350,19 @@ int32_t sdpxg_rns_symmetric_bilinear(sdpxg_ctx *ctx, uint32_t limbs, uint64_t h,
 int32_t sdpxg_rns_gemm_blocks_upper(sdpxg_ctx *ctx, uint32_t limbs, uint64_t m, uint64_t nblocks,
                                     const uint64_t *widths, const uint64_t *counts, const void *y, const void *d,
                                     const uint64_t *columns, void *C, uint32_t *status);
+/* NT scaling of PSD blocks at MPFR width: the reference's PSDTriangleCone::update_scaling
+ * (crates/solver/src/solver/cones/psdtrianglecone.rs:311-439) for MpFloat<limbs> (1..8), blocks of
+ * order orders[b] <= 64 with their svec s and z concatenated (tri(n_b) entries each).  Per block:
+ * L1 = chol(mat(s)), L2 = chol(mat(z)) (exact-dot Cholesky), the right singular vectors V of
+ * L2' L1 by one-sided Jacobi in MpFloat arithmetic (singular values descending), and lambda (n_b),
+ * Lambda^-1/2 (n_b), R = L1 V Lambda^-1/2, Rinv = Lambda^1/2 V' L1^-1 and G = R R' (upper, zeros
+ * below) as n_b x n_b column-major, concatenated.  block_status[b]: 0, 1 (s or z not interior) or
+ * 2 (Jacobi sweeps exhausted).  Replaces the MPFR right SVD (algebra/dense/blas/mpfr_svd.rs,
+ * mpfr_dqds.rs) behind update_scaling: V may differ in column signs, lambda, G and the
+ * congruences agree. */
+int32_t sdpxg_mp_nt_scale(sdpxg_ctx *ctx, uint32_t limbs, uint64_t nblocks, const uint64_t *orders,
+                          const void *s, const void *z, void *lambda, void *lisqrt, void *R, void *Rinv,
+                          void *G, int32_t *block_status, uint32_t *status);
 /* The reference's dense MPFR LDL' (ArrowLDLSolver::try_dense -> ldl_rec, kkt/ldl/arrow.rs:2609-2620,
  * 255-420, with ldl_dots leaves 156-242 and solve_unit_lower_t 430-470) of the n x n MpFloat<limbs>
  * matrix A (host, column-major, leading dimension lda; its lower triangle is read): L (n x n,

@@ -44,4 +44,17 @@ void mp_launch_stack_blocks(int nb, const long* r0, const long* yoff, const long
                             const unsigned char* y, const unsigned char* d, const unsigned long long* cols, long W,
                             int m, int N, unsigned char* Z, unsigned char* Y, uint32_t* status, cudaStream_t st);
 
+// MPFR NT scaling of PSD blocks (mp_nt.cu): block b of order n (<= 64) reads its svec at element
+// `svec` of s and z, writes R, Rinv and G (upper) as n x n column-major at element `mat`, lambda and
+// Lambda^-1/2 at element `vec`; work holds 5 * sum n^2 elements, wvec 2 * sum n; frac (one
+// element) receives the working-precision 1/sqrt 2.  bstatus[b]: 0, SDPXG_ST_CHOL_FAIL or SDPXG_ST_SVD_UNCONVERGED.
+struct MpNtBlock {
+  int n;
+  long svec, mat, vec;
+};
+void mp_launch_nt_scale(const MpNtBlock* blocks, int nblk, int N, const unsigned char* s, const unsigned char* z,
+                        unsigned char* frac, unsigned char* work, unsigned char* wvec, unsigned char* lam,
+                        unsigned char* lisqrt, unsigned char* R, unsigned char* Rinv, unsigned char* G, int* bstatus,
+                        uint32_t* status, cudaStream_t st);
+
 }  // namespace sdpxg

@@ -57,8 +57,8 @@ std::shared_ptr<void>* ctx_rns_slot(sdpxg_ctx* c);
 }  // namespace sdpxg
 
 #define RNS_MAXN 16    // limbs: up to 1024-bit values
-#define RNS_MAXL 192   // primes (1024-bit values at k = 2^20 need about 150 of 15 bits)
-#define RNS_MAXW 56    // 64-bit words of the reconstructed integer
+#define RNS_MAXL 256   // primes (products of four 768-bit factors need about 220 of 15 bits)
+#define RNS_MAXW 64    // 64-bit words of the reconstructed integer
 #define RNS_KC 8192    // exact FP64 terms between two reductions modulo the prime
 #define MP_ZERO 2
 #define MP_REGULAR 3
@@ -323,7 +323,7 @@ extern "C" __global__ void k_fill_int(int* __restrict__ a, int n, int v) {
 // Garner CRT of the L residues of every output, then one rounding to 64N bits (ties to even).
 // Residues are read as R (double: the FP64 form's exact integers, possibly negative; int: the
 // INT8 form's residues in [0, p)).  The mixed-radix digits are formed with one reduction per
-// prime: sum_s v_s (prod_{q<s} p_q mod p_t) stays below 2^50 for L <= 192 primes below 2^21.
+// prime: sum_s v_s (prod_{q<s} p_q mod p_t) stays below 2^50 for L <= 256 primes below 2^21.
 template <typename R>
 __global__ void k_rns_crt(const R* __restrict__ RC, long planeC, int m, int n, int L, int WW,
                           const uint32_t* __restrict__ primes, const uint32_t* __restrict__ inv,
@@ -1726,6 +1726,67 @@ extern "C" int32_t sdpxg_rns_gemm_blocks_upper(sdpxg_ctx* ctx, uint32_t limbs, u
     if (rc) return rc;
     copy_d2h(C, ws.c.p, m * m * esz, st);
     check(cudaStreamSynchronize(st), "sync");
+    return 0;
+  });
+}
+
+extern "C" int32_t sdpxg_mp_nt_scale(sdpxg_ctx* ctx, uint32_t limbs, uint64_t nblocks, const uint64_t* orders,
+                                     const void* s, const void* z, void* lambda, void* lisqrt, void* R, void* Rinv,
+                                     void* G, int32_t* block_status, uint32_t* status) {
+  return rns_entry([&]() -> int32_t {
+    Engine* E = entry_engine(ctx, limbs, "sdpxg_mp_nt_scale", kMpMaxLimbs);
+    const int N = (int)limbs;
+    if (status) *status = 0;
+    if (nblocks == 0) return 0;
+    if (nblocks > (1u << 20)) throw std::invalid_argument("size overflow");
+    if (!orders || !s || !z || !lambda || !lisqrt || !R || !Rinv || !G || !block_status)
+      throw std::invalid_argument("null pointer");
+    std::vector<MpNtBlock> desc;
+    std::vector<int> slot;  // block index of each nonempty descriptor
+    long tri = 0, sq = 0, lin = 0;
+    for (uint64_t b = 0; b < nblocks; ++b) {
+      if (orders[b] > 64) throw std::invalid_argument("sdpxg_mp_nt_scale: block orders must be at most 64");
+      block_status[b] = 0;
+      const long n = (long)orders[b];
+      if (n) {
+        desc.push_back({(int)n, tri, sq, lin});
+        slot.push_back((int)b);
+      }
+      tri += n * (n + 1) / 2;
+      sq += n * n;
+      lin += n;
+    }
+    const size_t esz = 8 * (size_t)N + 8;
+    cudaStream_t st = E->st;
+    DevBuf<MpNtBlock> dd(std::max<size_t>(desc.size(), 1));
+    DevBuf<unsigned char> ds(tri * esz + esz), dz(tri * esz + esz), dwork(5 * sq * esz + esz), dwv(2 * lin * esz + esz);
+    DevBuf<unsigned char> dlam(lin * esz + esz), dlis(lin * esz + esz), dR(sq * esz + esz), dRi(sq * esz + esz),
+        dG(sq * esz + esz), dfrac(esz);
+    DevBuf<int> dbs(std::max<size_t>(desc.size(), 1));
+    DevBuf<uint32_t> stw(1);
+    check(cudaMemsetAsync(stw.p, 0, sizeof(uint32_t), st), "memset");
+    if (!desc.empty()) dd.upload(desc.data(), desc.size(), st);
+    ds.upload(static_cast<const unsigned char*>(s), tri * esz, st);
+    dz.upload(static_cast<const unsigned char*>(z), tri * esz, st);
+    // blocks of order 0 keep zero-filled outputs
+    check(cudaMemsetAsync(dR.p, 0, sq * esz + esz, st), "memset");
+    mp_launch_nt_scale(dd, (int)desc.size(), N, ds, dz, dfrac, dwork, dwv, dlam, dlis, dR, dRi, dG, dbs, stw, st);
+    std::vector<int> hbs(desc.size());
+    uint32_t hs = 0;
+    copy_d2h(lambda, dlam.p, lin * esz, st);
+    copy_d2h(lisqrt, dlis.p, lin * esz, st);
+    copy_d2h(R, dR.p, sq * esz, st);
+    copy_d2h(Rinv, dRi.p, sq * esz, st);
+    copy_d2h(G, dG.p, sq * esz, st);
+    if (!desc.empty()) copy_d2h(hbs.data(), dbs.p, desc.size() * sizeof(int), st);
+    copy_d2h(&hs, stw.p, sizeof(uint32_t), st);
+    check(cudaStreamSynchronize(st), "sync");
+    for (size_t i = 0; i < desc.size(); ++i) block_status[slot[i]] = hbs[i];
+    if (status) *status = hs;
+    if (hs & SDPXG_ST_EXACT_SPREAD) {
+      g_last_error = "sdpxg_mp_nt_scale: an exact dot's exponent spread exceeds the device accumulator";
+      return 2;
+    }
     return 0;
   });
 }

@@ -584,6 +584,26 @@ class KernelContext:
                   C.c_char_p(y) if y else None, C.c_char_p(d) if d else None, carr, out, C.byref(st))
         return out.raw[:m * m * esz], st.value
 
+    def mp_nt_scale(self, limbs: int, orders, s: bytes, z: bytes):
+        """MPFR NT scaling of PSD blocks (svec s, z as raw MpFloat bytes, concatenated): returns
+        (lambda, lisqrt, R, Rinv, G raw bytes concatenated per block, block status list, status)."""
+        esz = 8 * limbs + 8
+        nb = len(orders)
+        lin = sum(orders)
+        sq = sum(n * n for n in orders)
+        arr = (C.c_uint64 * max(nb, 1))(*orders)
+        lam = C.create_string_buffer(max(lin * esz, 1))
+        lis = C.create_string_buffer(max(lin * esz, 1))
+        R = C.create_string_buffer(max(sq * esz, 1))
+        Ri = C.create_string_buffer(max(sq * esz, 1))
+        G = C.create_string_buffer(max(sq * esz, 1))
+        bst = (C.c_int32 * max(nb, 1))()
+        st = C.c_uint32()
+        _lib.call("sdpxg_mp_nt_scale", self._h, limbs, nb, arr, C.c_char_p(s), C.c_char_p(z), lam, lis, R, Ri,
+                  G, bst, C.byref(st))
+        return (lam.raw[:lin * esz], lis.raw[:lin * esz], R.raw[:sq * esz], Ri.raw[:sq * esz],
+                G.raw[:sq * esz], list(bst)[:nb], st.value)
+
     def mp_ldl(self, limbs: int, n: int, A: bytes, lda: int, reg: Optional[bytes] = None):
         """The reference's dense MPFR LDL' of an n x n MpFloat<limbs> matrix (raw bytes):
         returns (L bytes n x n, dinv bytes n, status)."""
