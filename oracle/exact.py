@@ -449,3 +449,65 @@ def gemm_blocks_upper(n: int, m: int, blocks) -> List[Mp]:
                     lst.append((mp_mul(n, d[r], y[r + a * w]), y[r + b * w]))
     return [exact_dot(n, terms.get((i, j), [])) if i <= j else Mp(n)
             for j in range(m) for i in range(m)]
+
+
+# ------------------------------------------------------------------------------------------
+# NT scaling of one PSD block at MPFR width (crates/solver/src/solver/cones/
+# psdtrianglecone.rs:311-439 update_scaling, svec_to_mat algebra/dense/matrix_math.rs:156-180):
+# exact-dot Cholesky of both sides, M = L2' L1 with every entry an exact dot rounded once, its
+# right singular vectors (here from mpmath's SVD at twice the width, standing in for the
+# reference's MPFR right SVD), then lambda, Lambda^-1/2, R = L1 V Lambda^-1/2,
+# Rinv = Lambda^1/2 (L1^-T V)' and G = R R' (upper) with MpFloat operations rounded once.
+# ------------------------------------------------------------------------------------------
+def _mpf_fraction(x) -> Fraction:
+    sign, man, exp, _ = x._mpf_
+    v = Fraction(int(man)) * (Fraction(2) ** int(exp))
+    return -v if sign else v
+
+
+def frac_1_sqrt2(n: int) -> Mp:
+    return mp_sqrt(n, from_fraction(n, Fraction(1, 2)))
+
+
+def nt_scale(n: int, order: int, s: List[Mp], z: List[Mp]):
+    """Returns (lam, lisqrt, R, Rinv, G) as lists (matrices column-major order x order), or
+    None when s or z is not interior (a Cholesky fails)."""
+    import mpmath
+    k = order
+    f = frac_1_sqrt2(n)
+    S = [Mp(n)] * (k * k)
+    Z = [Mp(n)] * (k * k)
+    for j in range(k):
+        for i in range(j, k):
+            t = i * (i + 1) // 2 + j
+            S[i + j * k] = s[t] if i == j else mp_mul(n, s[t], f)
+            Z[i + j * k] = z[t] if i == j else mp_mul(n, z[t], f)
+    if xpotrf(n, "L", k, S, k) or xpotrf(n, "L", k, Z, k):
+        return None
+    L1, L2 = S, Z
+    M = [exact_dot(n, [(L2[q + i * k], L1[q + j * k]) for q in range(max(i, j), k)])
+         for j in range(k) for i in range(k)]
+    with mpmath.workprec(128 * n + 64):  # twice the working width: small values keep their digits
+        Mm = mpmath.matrix(k, k)
+        for j in range(k):
+            for i in range(k):
+                Mm[i, j] = mpmath.mpf(M[i + j * k].fraction().numerator) / M[i + j * k].fraction().denominator
+        _, sv, Vt = mpmath.svd_r(Mm, compute_uv=True)
+        order_idx = sorted(range(k), key=lambda r: -sv[r])
+        V = [from_fraction(n, _mpf_fraction(mpmath.mpf(Vt[order_idx[r], i])))
+             for r in range(k) for i in range(k)]  # column r of V, row i
+        sig = [from_fraction(n, _mpf_fraction(mpmath.mpf(sv[order_idx[r]]))) for r in range(k)]
+    lam = sig
+    root = [mp_sqrt(n, v) for v in lam]
+    lis = [mp_recip(n, v) for v in root]
+    R = [mp_mul(n, exact_dot(n, [(L1[i + q * k], V[q + r * k]) for q in range(i + 1)]), lis[r])
+         for r in range(k) for i in range(k)]
+    X = [Mp(n)] * (k * k)  # L1' X = V by back substitution (xtrsm_lower, transposed)
+    for r in range(k):
+        for i in range(k - 1, -1, -1):
+            d = mp_sub(n, V[i + r * k], exact_dot(n, [(L1[q + i * k], X[q + r * k]) for q in range(i + 1, k)]))
+            X[i + r * k] = mp_div(n, d, L1[i + i * k])
+    Rinv = [mp_mul(n, X[j + r * k], root[r]) for j in range(k) for r in range(k)]
+    G = [exact_dot(n, [(R[i + q * k], R[j + q * k]) for q in range(k)]) if i <= j else Mp(n)
+         for j in range(k) for i in range(k)]
+    return lam, lis, R, Rinv, G

@@ -13,7 +13,7 @@
 //                                      pairs run in parallel, one warp per pair; singular values
 //                                      are the final column norms, sorted descending
 //   lambda = sigma, Lambda^-1/2 = 1 / sqrt(sigma)
-//   R = L1 V Lambda^-1/2,  Rinv = Lambda^1/2 (L1^-1 V)',  G = R R' (upper)
+//   R = L1 V Lambda^-1/2,  Rinv = Lambda^1/2 (L1^-T V)',  G = R R' (upper)
 // V is unique up to the signs of its columns (and rotations within clusters of equal singular
 // values); R, Rinv change with it as the reference's do, G, lambda and the congruences they define
 // do not.  Per-block status: 0, or SDPXG_ST_CHOL_FAIL (s or z not interior), or
@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(kNtThreads) k_mp_nt_scale(const MpNtBlock* __r
     mpd::mp_store(el(lisqrt, B.vec + r), N, mpd::mp_recip(rt, N), status);
   }
   __syncthreads();
-  // R = L1 V Lambda^-1/2 (row i of L1 has entries k <= i); X = L1^-1 V (forward substitution)
+  // R = L1 V Lambda^-1/2 (row i of L1 has entries k <= i); X = L1^-T V (back substitution)
   for (int e = tid; e < nn; e += kNtThreads) {
     const int i = e % n, r = e / n;
     bool ok = true;
@@ -333,10 +333,11 @@ __global__ void __launch_bounds__(kNtThreads) k_mp_nt_scale(const MpNtBlock* __r
     mpd::mp_store(el(R, B.mat + e), N, mul(d, mpd::mp_load(el(lisqrt, B.vec + r), N), N), status);
   }
   for (int r = tid; r < n; r += kNtThreads) {
-    for (int i = 0; i < n; ++i) {
+    for (int i = n - 1; i >= 0; --i) {
       bool ok = true;
       const Val b = mpd::mp_load(el(V, i + (long)perm[r] * n), N);
-      const Val d = mpd::mp_dot_sub(&b, el(L1, i), n, el(X, (long)r * n), 1, i, N, &ok);
+      const Val d = mpd::mp_dot_sub(&b, el(L1, i + 1 + (long)i * n), 1, el(X, i + 1 + (long)r * n), 1, n - 1 - i, N,
+                                    &ok);
       if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
       mpd::mp_store(el(X, i + (long)r * n), N, mpd::mp_div(d, mpd::mp_load(el(L1, i + (long)i * n), N), N), status);
     }
