@@ -357,12 +357,26 @@ int32_t sdpxg_rns_gemm_blocks_upper(sdpxg_ctx *ctx, uint32_t limbs, uint64_t m, 
  * L2' L1 by one-sided Jacobi in MpFloat arithmetic (singular values descending), and lambda (n_b),
  * Lambda^-1/2 (n_b), R = L1 V Lambda^-1/2, Rinv = Lambda^1/2 V' L1^-1 and G = R R' (upper, zeros
  * below) as n_b x n_b column-major, concatenated.  block_status[b]: 0, 1 (s or z not interior) or
- * 2 (Jacobi sweeps exhausted).  Replaces the MPFR right SVD (algebra/dense/blas/mpfr_svd.rs,
+ * 2 (Jacobi sweeps exhausted); a failed block's outputs are zeros.  Replaces the MPFR right SVD (algebra/dense/blas/mpfr_svd.rs,
  * mpfr_dqds.rs) behind update_scaling: V may differ in column signs, lambda, G and the
  * congruences agree. */
 int32_t sdpxg_mp_nt_scale(sdpxg_ctx *ctx, uint32_t limbs, uint64_t nblocks, const uint64_t *orders,
                           const void *s, const void *z, void *lambda, void *lisqrt, void *R, void *Rinv,
                           void *G, int32_t *block_status, uint32_t *status);
+/* Step-length bounds of PSD blocks at MPFR width: the reference's step_component /
+ * step_length_psd_component for precisions above 64 bits (crates/solver/src/solver/cones/
+ * psdtrianglecone.rs:1041-1072, 1180-1390) for MpFloat<limbs> (1..8).  Per block of order
+ * orders[b] <= 64: the direction's svec d (concatenated), the scaling matrix Rx (R for a dual
+ * direction, primal = 0; Rinv for a primal one, primal = 1; n_b x n_b column-major, concatenated)
+ * and Lambda^-1/2 (concatenated).  Delta = Lambda^-1/2 W-congruence(mat(d)) Lambda^-1/2 with the
+ * congruence exact (rounded once per entry); gamma = lambda_min(Delta) from its binary64 copy
+ * (the reference's Householder/Sturm bisection, bitwise) under the a priori bound or an exact
+ * Cholesky certificate of I + alpha_c Delta, else from an MpFloat Jacobi eigensolver; alpha[b] =
+ * min(-1/gamma, alpha_max) for gamma < 0, else alpha_max (one MpFloat each).  path[b]: 0 a priori
+ * bound, 1 certified, 2 MpFloat eigensolver, 3 eigensolver not converged (alpha 0). */
+int32_t sdpxg_mp_step_length(sdpxg_ctx *ctx, uint32_t limbs, uint64_t nblocks, const uint64_t *orders,
+                             uint32_t primal, const void *d, const void *Rx, const void *lisqrt,
+                             const void *alpha_max, void *alpha, int32_t *path, uint32_t *status);
 /* The reference's dense MPFR LDL' (ArrowLDLSolver::try_dense -> ldl_rec, kkt/ldl/arrow.rs:2609-2620,
  * 255-420, with ldl_dots leaves 156-242 and solve_unit_lower_t 430-470) of the n x n MpFloat<limbs>
  * matrix A (host, column-major, leading dimension lda; its lower triangle is read): L (n x n,

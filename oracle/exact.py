@@ -18,6 +18,7 @@ cross-checks the rounding against mpmath.
 """
 from __future__ import annotations
 
+import math
 import struct
 from fractions import Fraction
 from typing import List, Sequence, Tuple
@@ -511,3 +512,154 @@ def nt_scale(n: int, order: int, s: List[Mp], z: List[Mp]):
     G = [exact_dot(n, [(R[i + q * k], R[j + q * k]) for q in range(k)]) if i <= j else Mp(n)
          for j in range(k) for i in range(k)]
     return lam, lis, R, Rinv, G
+
+
+# ------------------------------------------------------------------------------------------
+# Step-length bound of one PSD block at MPFR width (psdtrianglecone.rs:1041-1072
+# step_component_inner, 1180-1231 step_length_psd_component, 1233-1285 eigval_min_f64,
+# 1287-1390 min_eigenvalue_f64, 1168-1178 admits, 1391-1406 lrscale_symmetric).
+# ------------------------------------------------------------------------------------------
+def mp_add(n: int, a: Mp, b: Mp) -> Mp:
+    return from_fraction(n, a.fraction() + b.fraction())
+
+
+def min_eigenvalue_f64(a: List[float], n: int):
+    """The reference's binary64 Householder tridiagonalisation and Sturm bisection, in its
+    operation order (Python floats round each operation, as Rust does)."""
+    a = list(a)
+
+    def at(i, j):
+        return i + j * n
+    d = [0.0] * n
+    e = [0.0] * n
+    for i in range(n - 1, 0, -1):
+        l = i - 1
+        h = 0.0
+        if l > 0:
+            scale = -0.0
+            for k in range(l + 1):
+                scale += abs(a[at(i, k)])
+            if scale == 0.0:
+                e[i] = a[at(i, l)]
+            else:
+                for k in range(l + 1):
+                    a[at(i, k)] /= scale
+                    h += a[at(i, k)] * a[at(i, k)]
+                f = a[at(i, l)]
+                g = -math.sqrt(h) if f >= 0.0 else math.sqrt(h)
+                e[i] = scale * g
+                h -= f * g
+                a[at(i, l)] = f - g
+                f = 0.0
+                for j in range(l + 1):
+                    g = 0.0
+                    for k in range(j + 1):
+                        g += a[at(j, k)] * a[at(i, k)]
+                    for k in range(j + 1, l + 1):
+                        g += a[at(k, j)] * a[at(i, k)]
+                    e[j] = g / h
+                    f += e[j] * a[at(i, j)]
+                hh = f / (h + h)
+                for j in range(l + 1):
+                    f = a[at(i, j)]
+                    g = e[j] - hh * f
+                    e[j] = g
+                    for k in range(j + 1):
+                        a[at(j, k)] -= f * e[k] + g * a[at(i, k)]
+        else:
+            e[i] = a[at(i, l)]
+        d[i] = h
+    e[0] = 0.0
+    for i in range(n):
+        d[i] = a[at(i, i)]
+    eps = 2.0 ** -52
+    tiny = 2.0 ** -1022 / eps
+
+    def below(x):
+        count = 0
+        q = d[0] - x
+        for i in range(n):
+            if i > 0:
+                q = d[i] - x - e[i] * e[i] / q
+            if q == 0.0:
+                q = -tiny
+            if q < 0.0:
+                count += 1
+        return count
+    lo, hi = math.inf, -math.inf
+    for i in range(n):
+        r = abs(e[i]) + (abs(e[i + 1]) if i + 1 < n else 0.0)
+        lo = min(lo, d[i] - r)
+        hi = max(hi, d[i] + r)
+    if not (math.isfinite(lo) and math.isfinite(hi)):
+        return None
+    width = max(hi - lo, max(abs(hi), abs(lo)) * eps)
+    lo -= width * eps
+    hi += width * eps
+    for _ in range(128):
+        mid = 0.5 * (lo + hi)
+        if mid <= lo or mid >= hi:
+            break
+        if below(mid) >= 1:
+            hi = mid
+        else:
+            lo = mid
+    return 0.5 * (lo + hi)
+
+
+def step_component(n: int, k: int, d: List[Mp], Rx: List[Mp], lis: List[Mp], primal: bool, amax: Mp):
+    """Returns (alpha, path): path 0 a priori binary64 bound, 1 certified by the exact Cholesky of
+    I + alpha_c Delta, 2 the full-precision eigensolver (here mpmath at 64 extra bits)."""
+    import mpmath
+    f = frac_1_sqrt2(n)
+    Xm = [Mp(n)] * (k * k)
+    for c in range(k):
+        for r in range(k):
+            lo, hi = min(r, c), max(r, c)
+            v = d[hi * (hi + 1) // 2 + lo]
+            Xm[r + c * k] = v if r == c else mp_mul(n, v, f)
+    Y = congruence(n, "N" if primal else "T", k, k, Rx, k, Xm, k)
+    D = [Mp(n)] * (k * k)
+    for c in range(k):
+        for r in range(c + 1):
+            v = Y[r + c * k]
+            if r != c:
+                two = v if v.is_zero() else Mp(n, v.neg, v.mant, v.exp + 1)
+                v = mp_mul(n, mp_mul(n, two, f), f)
+            v = mp_mul(n, v, mp_mul(n, lis[r], lis[c]))
+            D[r + c * k] = D[c + r * k] = v
+
+    def finish(gamma: Mp, path: int):
+        if not gamma.is_zero() and gamma.neg:
+            a = mp_recip(n, gamma)
+            a = Mp(n, not a.neg, a.mant, a.exp)
+            return (a if a.fraction() < amax.fraction() else amax), path
+        return amax, path
+    if k > 3:
+        amx = float(amax.fraction())
+        vals = [float(v.fraction()) for v in D]
+        if all(math.isfinite(v) and abs(v) <= 1e150 for v in vals) and math.isfinite(amx):
+            sumsq = 0.0
+            for v in vals:
+                sumsq += v * v
+            gamma = min_eigenvalue_f64(vals, k)
+            if gamma is not None:
+                bound = 2.0 * float((k + 1) ** 2) * 2.0 ** -52 * math.sqrt(sumsq)
+                floor = 1.0 / amx if (amx > 0.0 and math.isfinite(amx)) else 0.0
+                if bound <= 1e-10 * max(abs(gamma), floor):
+                    return finish(mp_from_float(n, gamma), 0)
+                alc = mp_from_float(n, -(1.0 - 1e-10) / gamma) if (gamma < 0.0 and -1.0 / gamma < amx) else amax
+                C = [mp_mul(n, v, alc) for v in D]
+                for i in range(k):
+                    C[i + i * k] = mp_add(n, C[i + i * k], mp_one(n))
+                if xpotrf(n, "L", k, C, k) == 0:
+                    return finish(mp_from_float(n, gamma), 1)
+    with mpmath.workprec(64 * n + 64):
+        Mm = mpmath.matrix(k, k)
+        for c in range(k):
+            for r in range(k):
+                fr = D[r + c * k].fraction()
+                Mm[r, c] = mpmath.mpf(fr.numerator) / fr.denominator
+        ev = mpmath.eigsy(Mm, eigvals_only=True)
+        lam = min(ev[i] for i in range(k))
+        return finish(from_fraction(n, _mpf_fraction(lam)), 2)

@@ -461,4 +461,53 @@ __device__ inline Val mp_dot_sub(const Val* a, const unsigned char* x, long xs, 
   return mp_round(acc, W, neg, lo, N);
 }
 
+// A value as (double in [0.5, 1), binary exponent): v = f 2^e.
+__device__ __forceinline__ double frac_exp(const Val& v, int N, long long* e) {
+  const double top = (double)(v.m[N - 1] >> 11) * 0x1p-53;  // the top 53 bits, in [0.5, 1)
+  *e = v.s + 64LL * N;
+  return v.neg ? -top : top;
+}
+
+// f 2^e as a Val (f a finite nonzero double).
+__device__ inline Val from_double(double f, long long e, int N) {
+  Val v = mp_zero();
+  if (f == 0.0) return v;
+  int fe = 0;
+  const double m = frexp(fabs(f), &fe);  // m in [0.5, 1)
+  v.zero = false;
+  v.neg = f < 0;
+  v.m[N - 1] = (unsigned long long)(m * 0x1p64);  // exact: 53 significant bits
+  v.s = e + fe - 64LL * N;
+  return v;
+}
+
+// 1 / x and 1 / sqrt(x) by Newton's iteration from an FP64 seed (quadratic convergence: four
+// steps carry 53 bits past 512): accurate to a few units in the last place, not correctly
+// rounded -- used only for the Jacobi rotation parameters, whose orthogonality they bound.
+__device__ inline Val mp_recip_approx(const Val& x, int N) {
+  long long e;
+  const double f = frac_exp(x, N, &e);
+  Val y = from_double(1.0 / f, -e, N);
+  const Val two = from_double(0.5, 2, N);
+  const int steps = N <= 2 ? 2 : (N <= 4 ? 3 : 4);
+  for (int k = 0; k < steps; ++k) y = mp_mul(y, mp_addsub(two, mp_mul(x, y, N), -1, N), N);
+  return y;
+}
+__device__ inline Val mp_rsqrt_approx(const Val& x, int N) {  // x > 0
+  long long e;
+  const double f = frac_exp(x, N, &e);
+  // x = f 2^e: 1/sqrt(x) = (1/sqrt(f 2^(e mod 2))) 2^(-(e - e mod 2) / 2)
+  const long long odd = e & 1;
+  Val y = from_double(1.0 / sqrt(f * (odd ? 2.0 : 1.0)), -((e - odd) / 2), N);
+  const Val three = from_double(0.75, 2, N);
+  const int steps = N <= 2 ? 2 : (N <= 4 ? 3 : 4);
+  for (int k = 0; k < steps; ++k) {
+    Val t = mp_addsub(three, mp_mul(x, mp_mul(y, y, N), N), -1, N);
+    t.s -= 1;  // / 2
+    y = mp_mul(y, t, N);
+  }
+  return y;
+}
+
+
 }  // namespace mpd

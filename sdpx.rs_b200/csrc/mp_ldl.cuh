@@ -57,4 +57,22 @@ void mp_launch_nt_scale(const MpNtBlock* blocks, int nblk, int N, const unsigned
                         unsigned char* lisqrt, unsigned char* R, unsigned char* Rinv, unsigned char* G, int* bstatus,
                         uint32_t* status, cudaStream_t st);
 
+// MPFR step-length bound of PSD blocks (mp_step.cu): block b of order n reads the exact
+// congruence Y of its direction (n x n at element `mat`) and Lambda^-1/2 (at element `vec`); consts
+// holds two elements: [0] the working-precision 1/sqrt 2 (mp_launch_step_smat), [1] alpha_max.  work:
+// 2 sum n^2 elements, fwork: sum (n^2 + 2n) doubles.  alpha[b] (one element each) and path[b]
+// (0 a priori FP64 bound, 1 certified by the exact Cholesky, 2 MpFloat eigensolver, 3 that did not
+// converge: alpha 0).
+struct MpStepBlock {
+  int n;
+  long svec, mat, vec;
+};
+// X_b = mat(d_b) (d's svec at element `svec`, X at element `mat`, full symmetric) after computing
+// consts[0] = the working-precision 1/sqrt 2.
+void mp_launch_step_smat(const MpStepBlock* blocks, int nblk, int N, const unsigned char* d, unsigned char* consts,
+                         unsigned char* X, uint32_t* status, cudaStream_t st);
+void mp_launch_step_bound(const MpStepBlock* blocks, int nblk, int N, const unsigned char* Y,
+                          const unsigned char* lisqrt, unsigned char* consts, unsigned char* work, double* fwork,
+                          unsigned char* alpha, int* path, uint32_t* status, cudaStream_t st);
+
 }  // namespace sdpxg

@@ -17,7 +17,7 @@
 // V is unique up to the signs of its columns (and rotations within clusters of equal singular
 // values); R, Rinv change with it as the reference's do, G, lambda and the congruences they define
 // do not.  Per-block status: 0, or SDPXG_ST_CHOL_FAIL (s or z not interior), or
-// SDPXG_ST_SVD_UNCONVERGED; SDPXG_ST_EXACT_SPREAD in the shared status word when an exact dot
+// SDPXG_ST_SVD_UNCONVERGED, and then the block's outputs are zeros; SDPXG_ST_EXACT_SPREAD in the shared status word when an exact dot
 // exceeds the accumulator.
 #include <stdexcept>
 
@@ -42,54 +42,6 @@ __device__ __forceinline__ void named_sync(int id, int count) {
 __device__ __forceinline__ Val add(const Val& a, const Val& b, int N) { return mpd::mp_addsub(a, b, 1, N); }
 __device__ __forceinline__ Val sub(const Val& a, const Val& b, int N) { return mpd::mp_addsub(a, b, -1, N); }
 __device__ __forceinline__ Val mul(const Val& a, const Val& b, int N) { return mpd::mp_mul(a, b, N); }
-
-// A value as (double in [0.5, 1), binary exponent): v = f 2^e.
-__device__ __forceinline__ double frac_exp(const Val& v, int N, long long* e) {
-  const double top = (double)(v.m[N - 1] >> 11) * 0x1p-53;  // the top 53 bits, in [0.5, 1)
-  *e = v.s + 64LL * N;
-  return v.neg ? -top : top;
-}
-
-// f 2^e as a Val (f a finite nonzero double).
-__device__ inline Val from_double(double f, long long e, int N) {
-  Val v = mpd::mp_zero();
-  if (f == 0.0) return v;
-  int fe = 0;
-  const double m = frexp(fabs(f), &fe);  // m in [0.5, 1)
-  v.zero = false;
-  v.neg = f < 0;
-  v.m[N - 1] = (unsigned long long)(m * 0x1p64);  // exact: 53 significant bits
-  v.s = e + fe - 64LL * N;
-  return v;
-}
-
-// 1 / x and 1 / sqrt(x) by Newton's iteration from an FP64 seed (quadratic convergence: four
-// steps carry 53 bits past 512): accurate to a few units in the last place, not correctly
-// rounded -- used only for the Jacobi rotation parameters, whose orthogonality they bound.
-__device__ inline Val recip_newton(const Val& x, int N) {
-  long long e;
-  const double f = frac_exp(x, N, &e);
-  Val y = from_double(1.0 / f, -e, N);
-  const Val two = from_double(0.5, 2, N);
-  const int steps = N <= 2 ? 2 : (N <= 4 ? 3 : 4);
-  for (int k = 0; k < steps; ++k) y = mul(y, sub(two, mul(x, y, N), N), N);
-  return y;
-}
-__device__ inline Val rsqrt_newton(const Val& x, int N) {  // x > 0
-  long long e;
-  const double f = frac_exp(x, N, &e);
-  // x = f 2^e: 1/sqrt(x) = (1/sqrt(f 2^(e mod 2))) 2^(-(e - e mod 2) / 2)
-  const long long odd = e & 1;
-  Val y = from_double(1.0 / sqrt(f * (odd ? 2.0 : 1.0)), -((e - odd) / 2), N);
-  const Val three = from_double(0.75, 2, N);
-  const int steps = N <= 2 ? 2 : (N <= 4 ? 3 : 4);
-  for (int k = 0; k < steps; ++k) {
-    Val t = sub(three, mul(x, mul(y, y, N), N), N);
-    t.s -= 1;  // / 2
-    y = mul(y, t, N);
-  }
-  return y;
-}
 
 __device__ __forceinline__ Val shfl_down(const Val& v, int d) {
   Val r;
@@ -208,8 +160,21 @@ __global__ void __launch_bounds__(kNtThreads) k_mp_nt_scale(const MpNtBlock* __r
   else
     chol_group(L2, n, N, tid - kNtThreads / 2, kNtThreads / 2, 2, sd[1], &fail[1], status);
   __syncthreads();
+  // a failed block's outputs are zeros
+  auto zero_outputs = [&]() {
+    for (int e = tid; e < nn; e += kNtThreads) {
+      mpd::mp_store(el(R, B.mat + e), N, mpd::mp_zero(), status);
+      mpd::mp_store(el(Rinv, B.mat + e), N, mpd::mp_zero(), status);
+      mpd::mp_store(el(G, B.mat + e), N, mpd::mp_zero(), status);
+    }
+    for (int r = tid; r < n; r += kNtThreads) {
+      mpd::mp_store(el(lam, B.vec + r), N, mpd::mp_zero(), status);
+      mpd::mp_store(el(lisqrt, B.vec + r), N, mpd::mp_zero(), status);
+    }
+  };
   if (fail[0] || fail[1]) {
     if (tid == 0) bstatus[blockIdx.x] = SDPXG_ST_CHOL_FAIL;
+    zero_outputs();
     return;
   }
   // A = M = L2' L1 (entry (i, j): rows k >= max(i, j)), V = I
@@ -259,23 +224,23 @@ __global__ void __launch_bounds__(kNtThreads) k_mp_nt_scale(const MpNtBlock* __r
         // zeta = (b - a) / (2 g), t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), c = 1/sqrt(1+t^2)
         Val g2 = gg;
         g2.s += 1;
-        Val zeta = mul(sub(bb, aa, N), recip_newton(g2, N), N);
+        Val zeta = mul(sub(bb, aa, N), mpd::mp_recip_approx(g2, N), N);
         Val t;
         if (zeta.zero) {
           t = one;
         } else if (zeta.s + 64LL * N > 32LL * N + 8) {  // |zeta| > 2^(32N+8): t = 1 / (2 zeta)
           Val z2 = zeta;
           z2.s += 1;
-          t = recip_newton(z2, N);
+          t = mpd::mp_recip_approx(z2, N);
         } else {
           Val az = zeta;
           az.neg = false;
           const Val w = add(one, mul(zeta, zeta, N), N);
-          const Val sq = mul(w, rsqrt_newton(w, N), N);
-          t = recip_newton(add(az, sq, N), N);
+          const Val sq = mul(w, mpd::mp_rsqrt_approx(w, N), N);
+          t = mpd::mp_recip_approx(add(az, sq, N), N);
           t.neg = zeta.neg;
         }
-        const Val c = rsqrt_newton(add(one, mul(t, t, N), N), N);
+        const Val c = mpd::mp_rsqrt_approx(add(one, mul(t, t, N), N), N);
         const Val sn = mul(c, t, N);
         for (int i = lane; i < n; i += 32) {
           unsigned char* M2[2] = {A, V};
@@ -295,6 +260,7 @@ __global__ void __launch_bounds__(kNtThreads) k_mp_nt_scale(const MpNtBlock* __r
   }
   if (!converged) {
     if (tid == 0) bstatus[blockIdx.x] = SDPXG_ST_SVD_UNCONVERGED;
+    zero_outputs();
     return;
   }
   // singular values: column norms (exact sums of squares, correctly rounded roots), descending

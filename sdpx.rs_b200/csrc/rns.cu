@@ -1790,3 +1790,82 @@ extern "C" int32_t sdpxg_mp_nt_scale(sdpxg_ctx* ctx, uint32_t limbs, uint64_t nb
     return 0;
   });
 }
+
+extern "C" int32_t sdpxg_mp_step_length(sdpxg_ctx* ctx, uint32_t limbs, uint64_t nblocks, const uint64_t* orders,
+                                        uint32_t primal, const void* d, const void* Rx, const void* lisqrt,
+                                        const void* alpha_max, void* alpha, int32_t* path, uint32_t* status) {
+  return rns_entry([&]() -> int32_t {
+    Engine* E = entry_engine(ctx, limbs, "sdpxg_mp_step_length", kMpMaxLimbs);
+    const int N = (int)limbs;
+    if (status) *status = 0;
+    if (nblocks == 0) return 0;
+    if (nblocks > (1u << 20)) throw std::invalid_argument("size overflow");
+    if (!orders || !d || !Rx || !lisqrt || !alpha_max || !alpha || !path) throw std::invalid_argument("null pointer");
+    std::vector<MpStepBlock> desc;
+    std::vector<int> slot;
+    long tri = 0, sq = 0, lin = 0, fw = 0;
+    for (uint64_t b = 0; b < nblocks; ++b) {
+      if (orders[b] > 64) throw std::invalid_argument("sdpxg_mp_step_length: block orders must be at most 64");
+      const long n = (long)orders[b];
+      if (n) {
+        desc.push_back({(int)n, tri, sq, lin});
+        slot.push_back((int)b);
+      }
+      tri += n * (n + 1) / 2;
+      sq += n * n;
+      lin += n;
+      fw += n * n + 2 * n;
+    }
+    const size_t esz = 8 * (size_t)N + 8;
+    cudaStream_t st = E->st;
+    RnsWorkspace& ws = workspace(ctx);
+    DevBuf<MpStepBlock> dd(std::max<size_t>(desc.size(), 1));
+    DevBuf<unsigned char> dD(tri * esz + esz), dR(sq * esz + esz), dL(lin * esz + esz), dX(sq * esz + esz),
+        dY(sq * esz + esz), dwork(2 * sq * esz + esz), dconst(2 * esz), dal(std::max<size_t>(desc.size(), 1) * esz);
+    DevBuf<double> dfw(fw + 1);
+    DevBuf<int> dpath(std::max<size_t>(desc.size(), 1));
+    DevBuf<uint32_t> stw(1);
+    check(cudaMemsetAsync(stw.p, 0, sizeof(uint32_t), st), "memset");
+    if (!desc.empty()) dd.upload(desc.data(), desc.size(), st);
+    dD.upload(static_cast<const unsigned char*>(d), tri * esz, st);
+    dR.upload(static_cast<const unsigned char*>(Rx), sq * esz, st);
+    dL.upload(static_cast<const unsigned char*>(lisqrt), lin * esz, st);
+    check(cudaMemcpyAsync(dconst.p + esz, alpha_max, esz, cudaMemcpyHostToDevice, st), "H2D");
+    g_h2d_bytes += esz;
+    mp_launch_step_smat(dd, (int)desc.size(), N, dD, dconst, dX, stw, st);
+    // Y_b: the exact W-congruence of the direction (mul_Wx_scratch, psdtrianglecone.rs:860-917):
+    // primal (ds) Rinv X Rinv', dual (dz) R' X R
+    for (const MpStepBlock& b : desc) {
+      uint32_t hs = 0;
+      const int32_t rc = rns_congruence(ws, st, N, primal ? 'N' : 'T', (uint64_t)b.n, (uint64_t)b.n,
+                                        dR.p + b.mat * esz, (uint64_t)b.n, dX.p + b.mat * esz, (uint64_t)b.n, 0,
+                                        dY.p + b.mat * esz, &hs);
+      if (rc) return rc;
+    }
+    mp_launch_step_bound(dd, (int)desc.size(), N, dY, dL, dconst, dwork, dfw, dal, dpath, stw, st);
+    std::vector<unsigned char> hal(desc.size() * esz);
+    std::vector<int> hpath(desc.size());
+    uint32_t hs = 0;
+    if (!desc.empty()) {
+      copy_d2h(hal.data(), dal.p, desc.size() * esz, st);
+      copy_d2h(hpath.data(), dpath.p, desc.size() * sizeof(int), st);
+    }
+    copy_d2h(&hs, stw.p, sizeof(uint32_t), st);
+    check(cudaStreamSynchronize(st), "sync");
+    unsigned char* out = static_cast<unsigned char*>(alpha);
+    for (uint64_t b = 0; b < nblocks; ++b) {  // an empty block bounds nothing: alpha_max
+      std::memcpy(out + b * esz, alpha_max, esz);
+      path[b] = 0;
+    }
+    for (size_t i = 0; i < desc.size(); ++i) {
+      std::memcpy(out + (size_t)slot[i] * esz, &hal[i * esz], esz);
+      path[slot[i]] = hpath[i];
+    }
+    if (status) *status = hs;
+    if (hs & SDPXG_ST_EXACT_SPREAD) {
+      g_last_error = "sdpxg_mp_step_length: an exact dot's exponent spread exceeds the device accumulator";
+      return 2;
+    }
+    return 0;
+  });
+}

@@ -124,6 +124,8 @@ SIGNATURES = {
                                        C.c_void_p, C.c_void_p, PU32]),
     "sdpxg_rns_symmetric_bilinear": (i32, [C.c_void_p, u32, u64, u64, C.c_void_p, C.c_void_p, u64,
                                            C.POINTER(u64), C.c_void_p, PU32]),
+    "sdpxg_mp_step_length": (i32, [C.c_void_p, u32, u64, C.POINTER(u64), u32, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(i32), PU32]),
     "sdpxg_mp_nt_scale": (i32, [C.c_void_p, u32, u64, C.POINTER(u64), C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(i32), PU32]),
     "sdpxg_rns_gemm_blocks_upper": (i32, [C.c_void_p, u32, u64, u64, C.POINTER(u64), C.POINTER(u64),

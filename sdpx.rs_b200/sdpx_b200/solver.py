@@ -604,6 +604,20 @@ class KernelContext:
         return (lam.raw[:lin * esz], lis.raw[:lin * esz], R.raw[:sq * esz], Ri.raw[:sq * esz],
                 G.raw[:sq * esz], list(bst)[:nb], st.value)
 
+    def mp_step_length(self, limbs: int, orders, primal: bool, d: bytes, Rx: bytes, lisqrt: bytes,
+                       alpha_max: bytes):
+        """MPFR step-length bounds per PSD block: returns (alpha raw bytes per block, path list,
+        status)."""
+        esz = 8 * limbs + 8
+        nb = len(orders)
+        arr = (C.c_uint64 * max(nb, 1))(*orders)
+        al = C.create_string_buffer(max(nb * esz, 1))
+        pth = (C.c_int32 * max(nb, 1))()
+        st = C.c_uint32()
+        _lib.call("sdpxg_mp_step_length", self._h, limbs, nb, arr, int(primal), C.c_char_p(d), C.c_char_p(Rx),
+                  C.c_char_p(lisqrt), C.c_char_p(alpha_max), al, pth, C.byref(st))
+        return al.raw[:nb * esz], list(pth)[:nb], st.value
+
     def mp_ldl(self, limbs: int, n: int, A: bytes, lda: int, reg: Optional[bytes] = None):
         """The reference's dense MPFR LDL' of an n x n MpFloat<limbs> matrix (raw bytes):
         returns (L bytes n x n, dinv bytes n, status)."""

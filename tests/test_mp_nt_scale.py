@@ -11,7 +11,8 @@ signs.  The bars are on what the scaling defines, at working precision 2^-64N:
     Rinv S Rinv' = diag(lambda), evaluated in 64N + 64-bit arithmetic, to 2^-(64N-24) relative to
     lambda's scale, including a block whose eigenvalues spread over 2^-100;
   * Lambda^-1/2 = 1 / sqrt(lambda) to 2^-(64N-4);
-  * a block with z outside the cone reports status 1 and leaves the others intact.
+  * a block with z outside the cone reports status 1 with zero outputs and leaves the others
+    intact.
 """
 from fractions import Fraction
 
@@ -152,6 +153,7 @@ def test_mp_nt_scale_reports_a_block_outside_the_cone():
     lam_b, _, _, _, _, bst, st = KernelContext().mp_nt_scale(n, orders, X.pack_array(s), X.pack_array(z))
     assert bst == [0, 1, 0] and st == 0
     lam = X.unpack_array(n, lam_b)
+    assert all(v.is_zero() for v in lam[3:8])
     olam = X.nt_scale(n, 4, *mats[2])[0]
     tol = Fraction(1, 2 ** (64 * n - 24))
     for a, b in zip(lam[8:12], olam):
