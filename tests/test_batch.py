@@ -42,3 +42,7 @@ def test_batch_reprepare_grows_and_shrinks():
     for p, b in zip(probs, batch):
         f = solve_problem(p, st).solution
         assert b.iterations == f.iterations and np.array_equal(b.x, f.x)
+        o = ipm.solve(p)  # every size here has m <= tri(n): independent constraints
+        assert b.status_code == o.status
+        assert abs(b.iterations - o.iterations) <= 1
+        assert abs(b.obj_val - o.objective) <= 1e-8 * max(1.0, abs(o.objective))

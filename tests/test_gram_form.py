@@ -116,6 +116,20 @@ def test_gram_schur_matches_ordinary():
         H[gram] = ctx.schur()
     assert np.array_equal(H[True], H[True].T)
     assert np.max(np.abs(H[True] - H[False])) <= 1e-12 * np.max(np.abs(H[False]))
+    # both against the oracle's Schur complement (per PSD block, condensed/psd.rs:1299-1570)
+    A = sp.csc_matrix(prob.A)
+    Ho = np.zeros((prob.n, prob.n))
+    r0 = 0
+    for _, d in prob.cones:
+        t = d * (d + 1) // 2
+        cone = ipm.PsdCone(d)
+        assert cone.update_scaling(s[r0:r0 + t], z[r0:r0 + t])
+        sub = A[r0:r0 + t, :]
+        cols = np.flatnonzero(sub.getnnz(axis=0))
+        Ho[np.ix_(cols, cols)] += cone.schur_block(sub[:, cols].toarray())
+        r0 += t
+    for form in (True, False):
+        assert np.max(np.abs(H[form] - Ho)) <= 1e-11 * np.max(np.abs(Ho))
 
 
 @pytest.mark.parametrize("maker", [lambda: P.rank1_sdp(8, 200, seed=1, nmin=6, nmax=24),
