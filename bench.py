@@ -398,6 +398,92 @@ def rns_256(args, peak_i8):
     return res
 
 
+def _mp_from_f64(vals, limbs):
+    """Binary64 values as MpFloat<limbs> bytes (exact: the 53-bit mantissa in the top limb)."""
+    import numpy as np
+    v = np.asarray(vals, dtype=np.float64)
+    f, e = np.frexp(v)
+    dt = np.dtype([("l", "<u8", (limbs,)), ("kind", "<i4"), ("exp", "<i4")])
+    a = np.zeros(v.size, dtype=dt)
+    a["l"][:, limbs - 1] = (np.abs(f) * 2.0 ** 64).astype(np.uint64)
+    a["kind"] = np.where(v == 0, 2, np.where(f < 0, -3, 3))
+    a["exp"] = np.where(v == 0, 0, e)
+    return a.tobytes()
+
+
+def mp_chain_256(args, m_ldl):
+    """The per-iteration MPFR kernels of the 256-bit precision workload (64 PSD blocks of the
+    bootstrap generator's orders, Schur dimension m_ldl): NT scaling of every block, the step
+    bounds of both sides, and the dense LDL' of an m_ldl x m_ldl 256-bit matrix in both residue
+    forms (the trailing products on the INT8 tensor cores or in FP64).  Host-built interior
+    points, directions and a diagonally dominant Schur stand-in, all device work timed by
+    wall clock around the synchronous entry points."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    from sdpx_b200 import _lib
+    from sdpx_b200.solver import KernelContext
+    limbs, esz = 4, 40
+    rng = np.random.default_rng(11)
+    orders = [d for _, d in problems.rank1_sdp(64, 4000, seed=0).cones]
+
+    def svec_spd(k):
+        A = rng.standard_normal((k, k))
+        S = A @ A.T / k + 0.3 * np.eye(k)
+        return [S[i, j] if i == j else S[i, j] * np.sqrt(2.0) for j in range(k) for i in range(j + 1)]
+
+    def svec_sym(k):
+        A = rng.standard_normal((k, k))
+        S = (A + A.T) / 2
+        return [S[i, j] if i == j else S[i, j] * np.sqrt(2.0) for j in range(k) for i in range(j + 1)]
+    s = _mp_from_f64(np.concatenate([svec_spd(k) for k in orders]), limbs)
+    z = _mp_from_f64(np.concatenate([svec_spd(k) for k in orders]), limbs)
+    ctx = KernelContext()
+    res = {"workload": f"64 PSD blocks (orders of rank1_sdp(64, 4000, seed 0), n {min(orders)}..{max(orders)}), "
+                       f"256-bit (MpFloat<4>); LDL' of a {m_ldl} x {m_ldl} diagonally dominant matrix"}
+    t0 = time.perf_counter()
+    lam, lis, R, Rinv, G, bst, st = ctx.mp_nt_scale(limbs, orders, s, z)
+    res["nt_scale_s"] = time.perf_counter() - t0
+    res["nt_scale_status"] = sorted(set(bst))
+    d = _mp_from_f64(np.concatenate([svec_sym(k) for k in orders]), limbs)
+    amax = _mp_from_f64([1.0], limbs)
+    t0 = time.perf_counter()
+    _, pz, _ = ctx.mp_step_length(limbs, orders, False, d, R, lis, amax)
+    _, ps, _ = ctx.mp_step_length(limbs, orders, True, d, Rinv, lis, amax)
+    res["step_bounds_s"] = time.perf_counter() - t0
+    res["step_paths"] = {str(p): (pz + ps).count(p) for p in sorted(set(pz + ps))}
+    m = m_ldl
+    off = rng.standard_normal((m, m))
+    H = (off + off.T) / 2
+    H[np.diag_indices(m)] = 4.0 * m
+    src = torch.from_numpy(np.frombuffer(_mp_from_f64(H.T.ravel(), limbs), dtype=np.uint8).copy()).cuda()
+    A = torch.empty_like(src)
+    dinv = torch.zeros(m * esz, dtype=torch.uint8, device="cuda")
+    lib = _lib.load()
+    outs = {}
+    for name, form in (("int8", 0), ("fp64", 1)):
+        ctx.set_rns_form(form)
+        A.copy_(src)
+        torch.cuda.synchronize()
+        stw = C.c_uint32()
+        t0 = time.perf_counter()
+        rc = lib.sdpxg_mp_ldl_device(ctx._h, limbs, m, C.c_void_p(A.data_ptr()), m, None,
+                                     C.c_void_p(dinv.data_ptr()), C.byref(stw))
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if rc != 0:
+            raise RuntimeError(_lib.last_error())
+        res[f"ldl_{name}_s"] = dt
+        outs[name] = dinv.cpu().numpy().tobytes()
+    ctx.set_rns_form(0)
+    res["ldl_bitwise_equal_forms"] = outs["int8"] == outs["fp64"]
+    res["ldl_exact_macs"] = m ** 3 / 6
+    res["per_iteration_int8_s"] = res["nt_scale_s"] + res["step_bounds_s"] + res["ldl_int8_s"]
+    res["per_iteration_fp64_s"] = res["nt_scale_s"] + res["step_bounds_s"] + res["ldl_fp64_s"]
+    res["fp64_over_int8"] = res["per_iteration_fp64_s"] / res["per_iteration_int8_s"]
+    return res
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -600,7 +686,8 @@ def run_i8(args, world, rank, local):
                             "frac_of_int8_peak": ops / ms / 1e9 / peak},
             "rns_256": {"n": n, "s": t_rns, "i8_gemm_ms": rms, "i8_launches": rcnt,
                         "i8_tops_executed": rops / rms / 1e9, "i8_tops_algorithmic": ralg / rms / 1e9,
-                        "frac_of_int8_peak": rops / rms / 1e9 / peak}}))
+                        "frac_of_int8_peak": rops / rms / 1e9 / peak},
+            "autotuner": ctx.i8_tuning().strip().splitlines()}))
     return 0
 
 
@@ -757,9 +844,11 @@ def main():
                     help="skip the nested precision-workload and 256-bit RNS measurements")
     ap.add_argument("--size", type=int, default=2048, help="i8 workload: matrix order")
     ap.add_argument("--reps", type=int, default=3, help="i8 workload: timed repetitions")
-    ap.add_argument("--workload", default="rank1", choices=["rank1", "batch", "adjoint", "i8"],
+    ap.add_argument("--workload", default="rank1", choices=["rank1", "batch", "adjoint", "i8", "mp256"],
                     help="rank1: the 32-block bootstrap SDP (default line); batch: independent "
-                         "small SDPs, instances/s; adjoint: conic QPs solved and differentiated")
+                         "small SDPs, instances/s; adjoint: conic QPs solved and differentiated; "
+                         "i8: the INT8 GEMM; mp256: the 256-bit per-iteration kernels (--size: "
+                         "the LDL' order)")
     ap.add_argument("--instances", type=int, default=None,
                     help="batch workloads: instances (default 4096 for batch, 256 for adjoint)")
     ap.add_argument("--workers", type=int, default=16, help="batch workload: worker handles")
@@ -773,6 +862,13 @@ def main():
             rc = run_reference(args, world, rank)
         elif args.workload == "i8":
             rc = run_i8(args, world, rank, local)
+        elif args.workload == "mp256":
+            import torch
+            torch.cuda.set_device(local)
+            if rank == 0:
+                print(json.dumps({"metric": "256-bit per-iteration MPFR kernels (s)", "n_gpus": 1,
+                                  "data": "synthetic", **mp_chain_256(args, args.size)}))
+            rc = 0
         elif args.workload == "batch":
             rc = run_batch(args, world, rank, local)
         elif args.workload == "adjoint":

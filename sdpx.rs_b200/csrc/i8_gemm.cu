@@ -351,7 +351,7 @@ void launch_variant(const int8_t* A, const int8_t* B, const I8GemmArgs& a, cudaS
 // into an earlier chunk's residues) runs every variant on the real operands, times each with
 // CUDA events on the launch stream and keeps the fastest for the rest of the process.  All
 // variants compute the same exact integers, so the choice never changes a result.
-// SDPX_B200_AUTOTUNE=0 keeps variant 0; sdpx_b200_i8_config forces one.
+// SDPX_B200_AUTOTUNE=0 keeps variant 0; SDPX_B200_I8_CONFIG=v or sdpx_b200_i8_config forces one.
 struct Tuner {
   std::mutex mu;
   std::map<std::array<int, 5>, std::pair<int, std::array<float, kVariants>>> table;
@@ -360,6 +360,8 @@ struct Tuner {
   Tuner() {
     const char* e = std::getenv("SDPX_B200_AUTOTUNE");
     enabled = !(e && e[0] == '0');
+    const char* f = std::getenv("SDPX_B200_I8_CONFIG");  // a fixed configuration, e.g. for a profile
+    if (f && f[0] >= '0' && f[0] < '0' + kVariants && f[1] == 0) forced = f[0] - '0';
   }
 };
 Tuner& tuner() {

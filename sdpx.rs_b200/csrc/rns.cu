@@ -320,15 +320,19 @@ extern "C" __global__ void k_fill_int(int* __restrict__ a, int n, int v) {
   if (i < n) a[i] = v;
 }
 
-// Garner CRT of the L residues of every output, then one rounding to 64N bits (ties to even).
+// CRT of the L residues of every output, then one rounding to 64N bits (ties to even).
 // Residues are read as R (double: the FP64 form's exact integers, possibly negative; int: the
-// INT8 form's residues in [0, p)).  The mixed-radix digits are formed with one reduction per
-// prime: sum_s v_s (prod_{q<s} p_q mod p_t) stays below 2^50 for L <= 256 primes below 2^21.
+// INT8 form's residues in [0, p)).  With M = prod p_t, M_t = M / p_t and w_t = M_t^-1 mod p_t:
+// c_t = r_t w_t mod p_t, S = sum_t c_t M_t (exact, WW words), f = sum_t c_t / p_t in FP64, and
+// the signed integer is X = S - rint(f) M.  The prime set covers more than twice the largest |X|
+// plus a margin (|X| < M / 4), so S / M = f sits within 1/4 of an integer and FP64's error
+// (below L^2 2^-53) cannot move rint(f); X is then exact.  L products of a table row with one
+// small factor per output, instead of Garner's L^2 / 2 modular steps.
 template <typename R>
 __global__ void k_rns_crt(const R* __restrict__ RC, long planeC, int m, int n, int L, int WW,
-                          const uint32_t* __restrict__ primes, const uint32_t* __restrict__ inv,
-                          const uint32_t* __restrict__ pmod, const unsigned long long* __restrict__ Mbig,
-                          const unsigned long long* __restrict__ halfM, const int* __restrict__ loA,
+                          const uint32_t* __restrict__ primes, const uint32_t* __restrict__ wt,
+                          const double* __restrict__ pinv, const unsigned long long* __restrict__ MT,
+                          const unsigned long long* __restrict__ Mbig, const int* __restrict__ loA,
                           const int* __restrict__ loB, int N, int upper_only, unsigned char* __restrict__ C,
                           uint32_t* __restrict__ status) {
   const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -347,48 +351,50 @@ __global__ void k_rns_crt(const R* __restrict__ RC, long planeC, int m, int n, i
     write_zero();
     return;
   }
-  uint32_t v[RNS_MAXL];
+  unsigned long long S[RNS_MAXW];
+  for (int w = 0; w < WW; ++w) S[w] = 0;
+  double f = 0.0;
   for (int t = 0; t < L; ++t) {
     const uint32_t p = primes[t];
     long long r = (long long)RC[t * planeC + idx];
     r %= (long long)p;
     if (r < 0) r += p;
-    unsigned long long u = 0;
-    for (int s = 0; s < t; ++s) u += (unsigned long long)v[s] * pmod[s * RNS_MAXL + t];
-    u %= p;
-    unsigned long long d = ((unsigned long long)r + p - u) % p;
-    v[t] = (uint32_t)(d * inv[t] % p);
-  }
-  unsigned long long S[RNS_MAXW];
-  for (int w = 0; w < WW; ++w) S[w] = 0;
-  S[0] = v[L - 1];
-  for (int t = L - 2; t >= 0; --t) {  // S = S * p_t + v_t
-    unsigned long long carry = v[t];
-    const unsigned long long p = primes[t];
-    for (int w = 0; w < WW; ++w) {
-      unsigned long long lo = S[w] * p;
-      unsigned long long hi = __umul64hi(S[w], p);
-      unsigned long long sum = lo + carry;
-      hi += (sum < lo);
-      S[w] = sum;
-      carry = hi;
+    const unsigned long long c = (unsigned long long)r * wt[t] % p;
+    f += (double)c * pinv[t];
+    const unsigned long long* row = MT + (size_t)t * WW;
+    unsigned long long carry = 0;
+    for (int w = 0; w < WW; ++w) {  // S += c * M_t
+      const unsigned long long lo = row[w] * c, hi = __umul64hi(row[w], c);
+      const unsigned long long s1 = S[w] + lo;
+      const unsigned long long c1 = s1 < lo;
+      const unsigned long long s2 = s1 + carry;
+      const unsigned long long c2 = s2 < s1;
+      S[w] = s2;
+      carry = hi + c1 + c2;
     }
   }
-  // sign: S > (M - 1) / 2 means S - M < 0
-  bool neg = false;
-  for (int w = WW - 1; w >= 0; --w) {
-    if (S[w] != halfM[w]) {
-      neg = S[w] > halfM[w];
-      break;
+  // S -= k M (two's complement over WW words; |X| < M / 4 fits with room for the sign)
+  const unsigned long long k = (unsigned long long)rint(f);
+  {
+    unsigned long long carry = 0, borrow = 0;
+    for (int w = 0; w < WW; ++w) {
+      const unsigned long long lo = Mbig[w] * k, hi = __umul64hi(Mbig[w], k);
+      const unsigned long long km = lo + carry;
+      carry = hi + (km < lo);
+      const unsigned long long d1 = S[w] - km;
+      const unsigned long long b1 = S[w] < km;
+      const unsigned long long d2 = d1 - borrow;
+      const unsigned long long b2 = d1 < borrow;
+      S[w] = d2;
+      borrow = b1 + b2;
     }
   }
-  if (neg) {  // magnitude M - S
-    unsigned long long borrow = 0;
+  const bool neg = (S[WW - 1] >> 63) != 0;
+  if (neg) {  // magnitude
+    unsigned long long cy = 1;
     for (int w = 0; w < WW; ++w) {
-      unsigned long long a = Mbig[w], b = S[w];
-      unsigned long long d = a - b - borrow;
-      borrow = (a < b) || (a - b < borrow);
-      S[w] = d;
+      S[w] = ~S[w] + cy;
+      cy = (cy && S[w] == 0) ? 1ull : 0ull;
     }
   }
   int top = -1;
@@ -557,8 +563,9 @@ namespace {
 // Host tables of one prime set (descending primes below 2^bits).
 struct PrimeTables {
   int L = 0, WW = 0;
-  std::vector<uint32_t> primes, W, inv, pmod;
-  std::vector<unsigned long long> M, half;
+  std::vector<uint32_t> primes, W, wt;
+  std::vector<double> pinv;
+  std::vector<unsigned long long> M, MT;  // M = prod p_t; MT row t = M / p_t (WW words each)
 };
 
 // The largest RNS_MAXL primes below 2^bits, descending.
@@ -600,35 +607,37 @@ PrimeTables make_tables(const std::vector<uint32_t>& ps, int L) {
   T.W.assign((size_t)L * RNS_MAXN, 0);
   for (int t = 0; t < L; ++t)
     for (int q = 0; q < RNS_MAXN; ++q) T.W[t * RNS_MAXN + q] = (uint32_t)powmod64(2, 64ull * q, T.primes[t]);
-  T.inv.assign(L, 0);
-  T.pmod.assign((size_t)RNS_MAXL * RNS_MAXL, 0);
-  for (int t = 0; t < L; ++t) {
-    uint64_t p = T.primes[t], prod = 1;
-    for (int s = 0; s < t; ++s) {
-      T.pmod[s * RNS_MAXL + t] = (uint32_t)prod;  // prod_{q<s} p_q mod p_t
-      prod = prod * (T.primes[s] % p) % p;
-    }
-    T.inv[t] = (uint32_t)powmod64(prod, p - 2, p);  // (prod_{q<t} p_q)^-1 mod p_t
-  }
-  // M = prod p_t, half = (M - 1) / 2
+  // M = prod p_t (WW words with room above it), M_t = M / p_t, w_t = M_t^-1 mod p_t
   double log2m = 0;
   for (uint32_t p : T.primes) log2m += std::log2((double)p);
   T.WW = std::min(RNS_MAXW, (int)(log2m / 64) + 2);
-  T.M.assign(T.WW, 0);
-  T.M[0] = 1;
-  for (uint32_t p : T.primes) {
+  auto mul_small = [&](std::vector<unsigned long long>& x, uint64_t p) {
     unsigned __int128 carry = 0;
     for (int w = 0; w < T.WW; ++w) {
-      unsigned __int128 v = (unsigned __int128)T.M[w] * p + carry;
-      T.M[w] = (unsigned long long)v;
+      unsigned __int128 v = (unsigned __int128)x[w] * p + carry;
+      x[w] = (unsigned long long)v;
       carry = v >> 64;
     }
-  }
-  T.half = T.M;
-  T.half[0] -= 1;  // M is odd
-  for (int w = 0; w < T.WW; ++w) {
-    unsigned long long next = (w + 1 < T.WW) ? T.half[w + 1] : 0;
-    T.half[w] = (T.half[w] >> 1) | (next << 63);
+  };
+  T.M.assign(T.WW, 0);
+  T.M[0] = 1;
+  for (uint32_t p : T.primes) mul_small(T.M, p);
+  T.MT.assign((size_t)L * T.WW, 0);
+  T.wt.assign(L, 0);
+  T.pinv.assign(L, 0.0);
+  for (int t = 0; t < L; ++t) {
+    std::vector<unsigned long long> x(T.WW, 0);
+    x[0] = 1;
+    uint64_t rem = 1;  // M_t mod p_t
+    const uint64_t p = T.primes[t];
+    for (int s2 = 0; s2 < L; ++s2)
+      if (s2 != t) {
+        mul_small(x, T.primes[s2]);
+        rem = rem * (T.primes[s2] % p) % p;
+      }
+    for (int w = 0; w < T.WW; ++w) T.MT[(size_t)t * T.WW + w] = x[w];
+    T.wt[t] = (uint32_t)powmod64(rem, p - 2, p);
+    T.pinv[t] = 1.0 / (double)p;
   }
   return T;
 }
@@ -640,9 +649,10 @@ void grow(DevBuf<T>& b, size_t n) {
 
 // Device copies of one prime set's tables (re-uploaded when L changes).
 struct DevTables {
-  DevBuf<uint32_t> primes, W, inv, pmod;
+  DevBuf<uint32_t> primes, W, wt;
+  DevBuf<double> pinv;
   DevBuf<int> iprimes;
-  DevBuf<unsigned long long> M, half;
+  DevBuf<unsigned long long> M, MT;
   int L = -1;
   std::map<int, PrimeTables> host;
   const PrimeTables& get(int bits, int L_, cudaStream_t st) {
@@ -650,16 +660,16 @@ struct DevTables {
     if (it == host.end()) it = host.emplace(L_, make_tables(prime_list(bits), L_)).first;
     const PrimeTables& T = it->second;
     if (L != L_) {
-      grow(primes, L_); grow(W, T.W.size()); grow(inv, L_); grow(pmod, T.pmod.size());
-      grow(iprimes, L_); grow(M, T.WW); grow(half, T.WW);
+      grow(primes, L_); grow(W, T.W.size()); grow(wt, L_); grow(pinv, L_);
+      grow(iprimes, L_); grow(M, T.WW); grow(MT, T.MT.size());
       primes.upload(T.primes.data(), L_, st);
       W.upload(T.W.data(), T.W.size(), st);
-      inv.upload(T.inv.data(), L_, st);
-      pmod.upload(T.pmod.data(), T.pmod.size(), st);
+      wt.upload(T.wt.data(), L_, st);
+      pinv.upload(T.pinv.data(), L_, st);
       std::vector<int> ip(T.primes.begin(), T.primes.end());
       iprimes.upload(ip.data(), L_, st);
       M.upload(T.M.data(), T.WW, st);
-      half.upload(T.half.data(), T.WW, st);
+      MT.upload(T.MT.data(), T.MT.size(), st);
       L = L_;
     }
     return T;
@@ -760,7 +770,7 @@ int32_t rns_product(RnsWorkspace& ws, cudaStream_t st, int form, int N, char ta,
       check(cudaMemsetAsync(ws.RC8.p, 0, (size_t)L * planeC * sizeof(int), st), "memset");
     }
     ++g_launches, k_rns_crt<int><<<(unsigned)((m * n + 127) / 128), 128, 0, st>>>(
-        ws.RC8, planeC, (int)m, (int)n, L, T.WW, DT.primes, DT.inv, DT.pmod, DT.M, DT.half, ws.loA, ws.loB, N,
+        ws.RC8, planeC, (int)m, (int)n, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB, N,
         upper_only ? 1 : 0, dC, ws.status);
   } else {
     const long planeA = (long)(m * std::max<uint64_t>(k, 1)), planeB = (long)(std::max<uint64_t>(k, 1) * n);
@@ -779,7 +789,7 @@ int32_t rns_product(RnsWorkspace& ws, cudaStream_t st, int form, int N, char ta,
       check(cudaMemsetAsync(ws.RC.p, 0, (size_t)L * planeC * sizeof(double), st), "memset");
     }
     ++g_launches, k_rns_crt<double><<<(unsigned)((m * n + 127) / 128), 128, 0, st>>>(
-        ws.RC, planeC, (int)m, (int)n, L, T.WW, DT.primes, DT.inv, DT.pmod, DT.M, DT.half, ws.loA, ws.loB, N,
+        ws.RC, planeC, (int)m, (int)n, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB, N,
         upper_only ? 1 : 0, dC, ws.status);
   }
   check(cudaGetLastError(), "rns launch");
@@ -884,7 +894,7 @@ int32_t rns_congruence(RnsWorkspace& ws, cudaStream_t st, int N, char ta, uint64
   }
   ++g_launches, k_add_const_int<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(ws.loA, (int)m, (int)lo_x, ws.loB2);
   ++g_launches, k_rns_crt<int><<<(unsigned)((m * m + 127) / 128), 128, 0, st>>>(
-      ws.RC8, planeC, (int)m, (int)m, L, T.WW, DT.primes, DT.inv, DT.pmod, DT.M, DT.half, ws.loA, ws.loB2, N,
+      ws.RC8, planeC, (int)m, (int)m, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB2, N,
       upper_only ? 1 : 0, dC, ws.status);
   check(cudaGetLastError(), "congruence launch");
   int herr = 0;
@@ -943,7 +953,7 @@ void crt_vector(RnsWorkspace& ws, cudaStream_t st, DevTables& DT, const PrimeTab
   ++g_launches, k_fill_int<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(ws.loA, count, lo);
   ++g_launches, k_fill_int<<<1, 32, 0, st>>>(ws.loB, 1, 0);
   ++g_launches, k_rns_crt<int><<<(unsigned)((count + 127) / 128), 128, 0, st>>>(
-      ws.RC8, count, count, 1, L, T.WW, DT.primes, DT.inv, DT.pmod, DT.M, DT.half, ws.loA, ws.loB, N, 0, dOut,
+      ws.RC8, count, count, 1, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB, N, 0, dOut,
       ws.status);
 }
 
@@ -1096,7 +1106,7 @@ int32_t rns_diag_congruence(RnsWorkspace& ws, cudaStream_t st, int N, uint64_t m
   }
   ++g_launches, k_add_const_int<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(ws.loA, (int)m, lo_d, ws.loB2);
   ++g_launches, k_rns_crt<int><<<(unsigned)((m * m + 127) / 128), 128, 0, st>>>(
-      ws.RC8, planeC, (int)m, (int)m, L, T.WW, DT.primes, DT.inv, DT.pmod, DT.M, DT.half, ws.loA, ws.loB2, N,
+      ws.RC8, planeC, (int)m, (int)m, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB2, N,
       upper_only ? 1 : 0, dC, ws.status);
   check(cudaGetLastError(), "diag_congruence launch");
   int herr = 0;

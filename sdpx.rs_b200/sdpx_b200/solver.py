@@ -511,6 +511,17 @@ class KernelContext:
                   C.c_void_p(d_C), ldc, C.byref(st))
         return st.value
 
+    @staticmethod
+    def i8_tuning() -> str:
+        """The INT8 GEMM autotuner's table (one line per shape class: chosen configuration and the
+        time of each)."""
+        lib = _lib.load()
+        req = C.c_uint64()
+        lib.sdpx_b200_i8_tuning(None, 0, C.byref(req))
+        buf = C.create_string_buffer(max(req.value, 1))
+        _lib.call("sdpx_b200_i8_tuning", buf, req.value, C.byref(req))
+        return buf.value.decode()
+
     def set_rns_form(self, form: int):
         """Residue products on INT8 tensor cores (RNS_INT8, the default) or in FP64 (RNS_FP64)."""
         _lib.call("sdpxg_rns_set_form", self._h, int(form))
