@@ -73,6 +73,15 @@ __device__ __forceinline__ int elem_exp(const unsigned char* p, int N) {
   return *reinterpret_cast<const int*>(p + 8 * N + 4);
 }
 
+// x mod p for 0 <= x < 2^53 by an FP64 quotient (exact to within one, then corrected).
+__device__ __forceinline__ uint32_t mod53(unsigned long long x, uint32_t p, double pinv) {
+  const unsigned long long q = (unsigned long long)((double)x * pinv);
+  long long r = (long long)(x - q * p);
+  if (r < 0) r += p;
+  if (r >= (long long)p) r -= p;
+  return (uint32_t)r;
+}
+
 __device__ __forceinline__ uint32_t pow2mod(long long s, uint32_t p) {
   unsigned long long r = 1, b = 2 % p;
   while (s > 0) {
@@ -236,8 +245,9 @@ extern "C" __global__ void k_rns_pow2(int L, const int* __restrict__ primes, int
 // limbs (each term < 2^31), reduced once.
 extern "C" __global__ void k_rns8_residues(const unsigned char* __restrict__ X, int N, int nlines, int len,
                                            long sx, long sy, const int* __restrict__ lo, int L,
-                                           const int* __restrict__ primes, const uint32_t* __restrict__ pow2,
-                                           int S, int8_t* __restrict__ out, int Rpad, int Kld) {
+                                           const int* __restrict__ primes, const double* __restrict__ pinv,
+                                           const uint32_t* __restrict__ pow2, int S, int8_t* __restrict__ out,
+                                           int Rpad, int Kld) {
   const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long)Rpad * Kld) return;
   const int y = (int)(idx % Kld), x = (int)(idx / Kld);
@@ -273,7 +283,7 @@ extern "C" __global__ void k_rns8_residues(const unsigned char* __restrict__ X, 
         }
       }
       const int p = primes[t];
-      int r = (int)(acc % (unsigned long long)p);
+      int r = (int)mod53(acc, (uint32_t)p, pinv[t]);  // acc < N 2^33
       if (r > p / 2) r -= p;
       if (neg) r = -r;
       dlo = ((r + 128) & 255) - 128;
@@ -356,11 +366,13 @@ __global__ void k_rns_crt(const R* __restrict__ RC, long planeC, int m, int n, i
   double f = 0.0;
   for (int t = 0; t < L; ++t) {
     const uint32_t p = primes[t];
-    long long r = (long long)RC[t * planeC + idx];
-    r %= (long long)p;
+    const double pi = pinv[t];
+    long long r = (long long)RC[t * planeC + idx];  // |r| < 2^53
+    r -= (long long)floor((double)r * pi) * (long long)p;  // within one multiple of p
     if (r < 0) r += p;
-    const unsigned long long c = (unsigned long long)r * wt[t] % p;
-    f += (double)c * pinv[t];
+    if (r >= (long long)p) r -= p;
+    const unsigned long long c = mod53((unsigned long long)r * wt[t], p, pi);  // < 2^42
+    f += (double)c * pi;
     const unsigned long long* row = MT + (size_t)t * WW;
     unsigned long long carry = 0;
     for (int w = 0; w < WW; ++w) {  // S += c * M_t
@@ -456,6 +468,7 @@ __global__ void k_rns_crt(const R* __restrict__ RC, long planeC, int m, int n, i
 // chunks, as in k_rns8_residues.
 extern "C" __global__ void k_rns_class_residues(const unsigned char* __restrict__ X, int N, int count, int lo,
                                                 int absval, int L, const int* __restrict__ primes,
+                                                const double* __restrict__ pinv,
                                                 const uint32_t* __restrict__ pow2, int S, int* __restrict__ out) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
@@ -477,7 +490,7 @@ extern "C" __global__ void k_rns_class_residues(const unsigned char* __restrict_
              ((v >> 32) & 0xFFFFull) * w[64 * q + 32] + (v >> 48) * w[64 * q + 48];
     }
     const int p = primes[t];
-    int r = (int)(acc % (unsigned long long)p);
+    int r = (int)mod53(acc, (uint32_t)p, pinv[t]);
     if (neg && r) r = p - r;
     out[(size_t)t * count + e] = r;
   }
@@ -753,9 +766,9 @@ int32_t rns_product(RnsWorkspace& ws, cudaStream_t st, int form, int N, char ta,
       grow(ws.PA, (size_t)L * 2 * Mpad * Kld);
       grow(ws.PB, (size_t)L * 2 * Npad * Kld);
       ++g_launches, k_rns8_residues<<<(unsigned)(((long)Mpad * Kld + 255) / 256), 256, 0, st>>>(
-          dA, N, (int)m, (int)k, asx, asy, ws.loA, L, DT.iprimes, ws.pow2, S, ws.PA, Mpad, Kld);
+          dA, N, (int)m, (int)k, asx, asy, ws.loA, L, DT.iprimes, DT.pinv, ws.pow2, S, ws.PA, Mpad, Kld);
       ++g_launches, k_rns8_residues<<<(unsigned)(((long)Npad * Kld + 255) / 256), 256, 0, st>>>(
-          dB, N, (int)n, (int)k, bsx, bsy, ws.loB, L, DT.iprimes, ws.pow2, S, ws.PB, Npad, Kld);
+          dB, N, (int)n, (int)k, bsx, bsy, ws.loB, L, DT.iprimes, DT.pinv, ws.pow2, S, ws.PB, Npad, Kld);
       check(cudaMemsetAsync(ws.err.p, 0, sizeof(int), st), "memset");
       for (int k0 = 0; k0 < Kld; k0 += kI8Chunk) {
         I8GemmArgs ga;
@@ -869,11 +882,11 @@ int32_t rns_congruence(RnsWorkspace& ws, cudaStream_t st, int N, char ta, uint64
   grow(ws.PA, (size_t)L * 2 * Mpad * Kpad);  // A~ (rows of op(A)), used by both products
   grow(ws.PB, (size_t)L * 2 * (size_t)std::max(Kpad, Mpad) * Kpad);
   ++g_launches, k_rns8_residues<<<(unsigned)(((long)Mpad * Kpad + 255) / 256), 256, 0, st>>>(
-      dA, N, (int)m, (int)k, asx, asy, ws.loA, L, DT.iprimes, ws.pow2, S, ws.PA, Mpad, Kpad);
+      dA, N, (int)m, (int)k, asx, asy, ws.loA, L, DT.iprimes, DT.pinv, ws.pow2, S, ws.PA, Mpad, Kpad);
   ++g_launches, k_fill_int<<<(unsigned)((k + 255) / 256), 256, 0, st>>>(ws.loX, (int)k, (int)lo_x);
   // X~ by rows (line r: entries (r, c)): the left operand of T = X~ A~'
   ++g_launches, k_rns8_residues<<<(unsigned)(((long)Kpad * Kpad + 255) / 256), 256, 0, st>>>(
-      dX, N, (int)k, (int)k, 1, (long)ldx, ws.loX, L, DT.iprimes, ws.pow2, S, ws.PB, Kpad, Kpad);
+      dX, N, (int)k, (int)k, 1, (long)ldx, ws.loX, L, DT.iprimes, DT.pinv, ws.pow2, S, ws.PB, Kpad, Kpad);
   check(cudaMemsetAsync(ws.err.p, 0, sizeof(int), st), "memset");
   for (int k0 = 0; k0 < Kpad; k0 += kI8Chunk) {  // T (k x m) = X~ A~'
     I8GemmArgs ga;
@@ -972,7 +985,7 @@ void class_residues(RnsWorkspace& ws, cudaStream_t st, DevTables& DT, int N, int
   for (int c = 0; c < n; ++c)
     if (count[c])
       ++g_launches, k_rns_class_residues<<<(unsigned)((count[c] + 127) / 128), 128, 0, st>>>(
-          arr[c], N, count[c], lo[c], absval[c], L, DT.iprimes, ws.pow2, S, ws.cres.p + off[c] * L);
+          arr[c], N, count[c], lo[c], absval[c], L, DT.iprimes, DT.pinv, ws.pow2, S, ws.cres.p + off[c] * L);
 }
 
 // v[k] = sum_{i <= j} c_ij x_tri(j)+i q_ik q_jk (c_ii = 1, c_ij = sqrt2), k < kmax, each rounded
@@ -1093,7 +1106,7 @@ int32_t rns_diag_congruence(RnsWorkspace& ws, cudaStream_t st, int N, uint64_t m
   grow(ws.PA, (size_t)L * 2 * Mpad * Kpad);
   grow(ws.PB, (size_t)L * 2 * Mpad * Kpad);
   ++g_launches, k_rns8_residues<<<(unsigned)(((long)Mpad * Kpad + 255) / 256), 256, 0, st>>>(
-      dA, N, (int)m, (int)k, (long)lda, 1, ws.loA, L, DT.iprimes, ws.pow2, S, ws.PA, Mpad, Kpad);
+      dA, N, (int)m, (int)k, (long)lda, 1, ws.loA, L, DT.iprimes, DT.pinv, ws.pow2, S, ws.PA, Mpad, Kpad);
   ++g_launches, k_rns8_scale_planes<<<(unsigned)(((long)Mpad * Kpad + 255) / 256), 256, 0, st>>>(
       ws.PA, ws.cres.p + off[0] * L, (int)k, L, DT.iprimes, ws.PB, Mpad, Kpad);
   check(cudaMemsetAsync(ws.err.p, 0, sizeof(int), st), "memset");
