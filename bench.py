@@ -602,6 +602,7 @@ def run_ours(args, world, rank, local):
     if rank == 0 and not args.quick:
         extra["precision_f64"] = precision_f64(args)
         extra["rns_256"] = rns_256(args, peak_i8)
+        extra["mp_256_iteration"] = mp_chain_256(args, 4000)
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline(prob)
