@@ -21,21 +21,35 @@ __device__ __forceinline__ const unsigned char* el(const unsigned char* A, long 
 // d_j = a_jj - dot(r_j, w_j) (the exact difference rounded once when that rounds to zero), the
 // pivot rule, D^-1; then every later row i: r_ij = (a_ij - dot(r_i, w_j)) * d_j^-1,
 // w_ij = r_ij d_j.  Dots are exact and rounded once; the other operations round once each.
+// Row j of R and of W (strided in memory) is staged in shared memory once per column: the pivot's
+// dot runs from there, and every row's dot reads w_j there (a broadcast) and its own row of R
+// from global memory, coalesced across the warp.
 __global__ void __launch_bounds__(128) k_mp_ldl_dots(unsigned char* A, long lda, int off, int size, int N,
                                                      unsigned char* W, unsigned char* dinv,
                                                      const unsigned char* reg, uint32_t* status) {
   __shared__ __align__(8) unsigned char sd[8 * mpd::kMaxN + 8];  // d_j
+  __shared__ __align__(8) unsigned char srow[kMpRecBase * (8 * mpd::kMaxN + 8)];  // r_j (columns < j)
+  __shared__ __align__(8) unsigned char swrow[kMpRecBase * (8 * mpd::kMaxN + 8)];  // w_j
   __shared__ int s_fail;
   unsigned char* B = A + ((long)off + (long)off * lda) * (8L * N + 8);
   if (threadIdx.x == 0) s_fail = 0;
   __syncthreads();
+  const long esz = 8L * N + 8;
   for (int j = 0; j < size; ++j) {
+    for (long wd = threadIdx.x; wd < (long)j * esz / 8; wd += blockDim.x) {  // stage r_j, w_j by words
+      const long b = 8 * wd, c = b / esz, o = b % esz;
+      *reinterpret_cast<unsigned long long*>(srow + b) =
+          *reinterpret_cast<const unsigned long long*>(el(B, j, (int)c, lda, N) + o);
+      *reinterpret_cast<unsigned long long*>(swrow + b) =
+          *reinterpret_cast<const unsigned long long*>(el(W, j, (int)c, size, N) + o);
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
       bool ok = true;
       const Val a = mpd::mp_load(el(B, j, j, lda, N), N);
-      const Val dot = mpd::mp_dot_sub(nullptr, el(B, j, 0, lda, N), lda, el(W, j, 0, size, N), size, j, N, &ok);
+      const Val dot = mpd::mp_dot_sub(nullptr, srow, 1, swrow, 1, j, N, &ok);
       Val d = mpd::mp_addsub(a, dot, -1, N);
-      if (d.zero && j > 0) d = mpd::mp_dot_sub(&a, el(B, j, 0, lda, N), lda, el(W, j, 0, size, N), size, j, N, &ok);
+      if (d.zero && j > 0) d = mpd::mp_dot_sub(&a, srow, 1, swrow, 1, j, N, &ok);
       if (reg) {  // DenseLeaf::pivot (arrow.rs:618-632), sign +1
         const Val eps = mpd::mp_load(reg, N), delta = mpd::mp_load(reg + 8 * N + 8, N);
         if (mpd::mp_cmp(d, eps, N) < 0) d = delta;
@@ -56,7 +70,7 @@ __global__ void __launch_bounds__(128) k_mp_ldl_dots(unsigned char* A, long lda,
     for (int i = j + 1 + threadIdx.x; i < size; i += blockDim.x) {
       bool ok = true;
       const Val a = mpd::mp_load(el(B, i, j, lda, N), N);
-      const Val dot = mpd::mp_dot_sub(nullptr, el(B, i, 0, lda, N), lda, el(W, j, 0, size, N), size, j, N, &ok);
+      const Val dot = mpd::mp_dot_sub(nullptr, el(B, i, 0, lda, N), lda, swrow, 1, j, N, &ok);
       if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
       const Val v = mpd::mp_mul(mpd::mp_addsub(a, dot, -1, N), di, N);
       mpd::mp_store(el(B, i, j, lda, N), N, v, status);
