@@ -236,13 +236,31 @@ extern "C" __global__ void k_rns_pow2(int L, const int* __restrict__ primes, int
   out[(size_t)t * S + s] = pow2mod(s, (uint32_t)primes[t]);
 }
 
+// (M 2^shift) mod p for the mantissa M = sum_q limbs[q] 2^(64q): Horner over the limbs with
+// 2^32 and 2^64 mod p from the power table's row (row[s] = 2^s mod p, s < S, S > 64), each
+// step one FP64-quotient reduction of a value below 2^53, then one product with row[shift].
+__device__ __forceinline__ uint32_t residue_of(const unsigned long long* limbs, int N, const uint32_t* row,
+                                               int shift, uint32_t p, double pinv) {
+  const unsigned long long c32 = row[32], c64 = row[64];
+  unsigned long long r = 0;
+#pragma unroll
+  for (int q = RNS_MAXN - 1; q >= 0; --q) {
+    if (q < N) {
+      const unsigned long long v = limbs[q];
+      const unsigned long long lm = mod53((v >> 32) * c32 + (v & 0xFFFFFFFFull), p, pinv);  // < 2^48
+      r = mod53(r * c64 + lm, p, pinv);                                                      // < 2^37
+    }
+  }
+  return mod53(r * row[shift], p, pinv);
+}
+
 // INT8 form: symmetric residues modulo L primes below 2^15 of every entry of a view, each split
 // into signed-byte digits r = lo + 256 hi (|hi| <= 64), written to K-major byte planes: digit d
 // of prime t for line x (a row of op(A) or a column of op(B)) and inner index y at
 // out[((2t + d) * Rpad + x) * Kld + y].  Lines >= nlines and y >= len (the padding) get zeros.
 // One thread per (x, y), y fastest: the plane writes are coalesced.  The residue of
-// M * 2^shift is sum_c chunk_c * (2^(16c + shift) mod p) over the 16-bit chunks of the mantissa
-// limbs (each term < 2^31), reduced once.
+// M * 2^shift is (M mod p)(2^shift mod p) mod p, M mod p by Horner over the 64-bit limbs
+// (residue_of: three power-table reads per prime).
 extern "C" __global__ void k_rns8_residues(const unsigned char* __restrict__ X, int N, int nlines, int len,
                                            long sx, long sy, const int* __restrict__ lo, int L,
                                            const int* __restrict__ primes, const double* __restrict__ pinv,
@@ -272,18 +290,8 @@ extern "C" __global__ void k_rns8_residues(const unsigned char* __restrict__ X, 
   for (int t = 0; t < L; ++t) {
     int dlo = 0, dhi = 0;
     if (live) {
-      const uint32_t* w = pow2 + (size_t)t * S + shift;
-      unsigned long long acc = 0;
-#pragma unroll
-      for (int q = 0; q < RNS_MAXN; ++q) {
-        if (q < N) {
-          const unsigned long long v = limbs[q];
-          acc += (v & 0xFFFFull) * w[64 * q] + ((v >> 16) & 0xFFFFull) * w[64 * q + 16] +
-                 ((v >> 32) & 0xFFFFull) * w[64 * q + 32] + (v >> 48) * w[64 * q + 48];
-        }
-      }
       const int p = primes[t];
-      int r = (int)mod53(acc, (uint32_t)p, pinv[t]);  // acc < N 2^33
+      int r = (int)residue_of(limbs, N, pow2 + (size_t)t * S, shift, (uint32_t)p, pinv[t]);
       if (r > p / 2) r -= p;
       if (neg) r = -r;
       dlo = ((r + 128) & 255) - 128;
@@ -330,6 +338,15 @@ extern "C" __global__ void k_fill_int(int* __restrict__ a, int n, int v) {
   if (i < n) a[i] = v;
 }
 
+// Word w of S (WM words kept in registers: an unrolled select instead of a dynamic index).
+template <int WM>
+__device__ __forceinline__ unsigned long long word_at(const unsigned long long (&S)[WM], int w) {
+  unsigned long long v = 0ull;
+#pragma unroll
+  for (int k = 0; k < WM; ++k) v = (k == w) ? S[k] : v;
+  return v;
+}
+
 // CRT of the L residues of every output, then one rounding to 64N bits (ties to even).
 // Residues are read as R (double: the FP64 form's exact integers, possibly negative; int: the
 // INT8 form's residues in [0, p)).  With M = prod p_t, M_t = M / p_t and w_t = M_t^-1 mod p_t:
@@ -337,14 +354,17 @@ extern "C" __global__ void k_fill_int(int* __restrict__ a, int n, int v) {
 // the signed integer is X = S - rint(f) M.  The prime set covers more than twice the largest |X|
 // plus a margin (|X| < M / 4), so S / M = f sits within 1/4 of an integer and FP64's error
 // (below L^2 2^-53) cannot move rint(f); X is then exact.  L products of a table row with one
-// small factor per output, instead of Garner's L^2 / 2 modular steps.
-template <typename R>
-__global__ void k_rns_crt(const R* __restrict__ RC, long planeC, int m, int n, int L, int WW,
-                          const uint32_t* __restrict__ primes, const uint32_t* __restrict__ wt,
-                          const double* __restrict__ pinv, const unsigned long long* __restrict__ MT,
-                          const unsigned long long* __restrict__ Mbig, const int* __restrict__ loA,
-                          const int* __restrict__ loB, int N, int upper_only, unsigned char* __restrict__ C,
-                          uint32_t* __restrict__ status) {
+// small factor per output, instead of Garner's L^2 / 2 modular steps.  S lives in registers: the
+// kernel is instantiated for the smallest word count WM >= WW (launch_crt).
+template <typename R, int WM>
+__global__ void __launch_bounds__(128) k_rns_crt(const R* __restrict__ RC, long planeC, int m, int n, int L, int WW,
+                                                 const uint32_t* __restrict__ primes,
+                                                 const uint32_t* __restrict__ wt, const double* __restrict__ pinv,
+                                                 const unsigned long long* __restrict__ MT,
+                                                 const unsigned long long* __restrict__ Mbig,
+                                                 const int* __restrict__ loA, const int* __restrict__ loB, int N,
+                                                 int upper_only, unsigned char* __restrict__ C,
+                                                 uint32_t* __restrict__ status) {
   const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long)m * n) return;
   const int i = (int)(idx % m), j = (int)(idx / m);
@@ -361,8 +381,9 @@ __global__ void k_rns_crt(const R* __restrict__ RC, long planeC, int m, int n, i
     write_zero();
     return;
   }
-  unsigned long long S[RNS_MAXW];
-  for (int w = 0; w < WW; ++w) S[w] = 0;
+  unsigned long long S[WM];
+#pragma unroll
+  for (int w = 0; w < WM; ++w) S[w] = 0ull;
   double f = 0.0;
   for (int t = 0; t < L; ++t) {
     const uint32_t p = primes[t];
@@ -375,76 +396,90 @@ __global__ void k_rns_crt(const R* __restrict__ RC, long planeC, int m, int n, i
     f += (double)c * pi;
     const unsigned long long* row = MT + (size_t)t * WW;
     unsigned long long carry = 0;
-    for (int w = 0; w < WW; ++w) {  // S += c * M_t
-      const unsigned long long lo = row[w] * c, hi = __umul64hi(row[w], c);
-      const unsigned long long s1 = S[w] + lo;
-      const unsigned long long c1 = s1 < lo;
-      const unsigned long long s2 = s1 + carry;
-      const unsigned long long c2 = s2 < s1;
-      S[w] = s2;
-      carry = hi + c1 + c2;
+#pragma unroll
+    for (int w = 0; w < WM; ++w) {  // S += c * M_t
+      if (w < WW) {
+        const unsigned long long mw = row[w];
+        const unsigned long long lo = mw * c, hi = __umul64hi(mw, c);
+        const unsigned long long s1 = S[w] + lo;
+        const unsigned long long c1 = s1 < lo;
+        const unsigned long long s2 = s1 + carry;
+        const unsigned long long c2 = s2 < s1;
+        S[w] = s2;
+        carry = hi + c1 + c2;
+      }
     }
   }
   // S -= k M (two's complement over WW words; |X| < M / 4 fits with room for the sign)
   const unsigned long long k = (unsigned long long)rint(f);
   {
     unsigned long long carry = 0, borrow = 0;
-    for (int w = 0; w < WW; ++w) {
-      const unsigned long long lo = Mbig[w] * k, hi = __umul64hi(Mbig[w], k);
-      const unsigned long long km = lo + carry;
-      carry = hi + (km < lo);
-      const unsigned long long d1 = S[w] - km;
-      const unsigned long long b1 = S[w] < km;
-      const unsigned long long d2 = d1 - borrow;
-      const unsigned long long b2 = d1 < borrow;
-      S[w] = d2;
-      borrow = b1 + b2;
+#pragma unroll
+    for (int w = 0; w < WM; ++w) {
+      if (w < WW) {
+        const unsigned long long lo = Mbig[w] * k, hi = __umul64hi(Mbig[w], k);
+        const unsigned long long km = lo + carry;
+        carry = hi + (km < lo);
+        const unsigned long long d1 = S[w] - km;
+        const unsigned long long b1 = S[w] < km;
+        const unsigned long long d2 = d1 - borrow;
+        const unsigned long long b2 = d1 < borrow;
+        S[w] = d2;
+        borrow = b1 + b2;
+      }
     }
   }
-  const bool neg = (S[WW - 1] >> 63) != 0;
+  const bool neg = (word_at(S, WW - 1) >> 63) != 0;
   if (neg) {  // magnitude
     unsigned long long cy = 1;
-    for (int w = 0; w < WW; ++w) {
-      S[w] = ~S[w] + cy;
-      cy = (cy && S[w] == 0) ? 1ull : 0ull;
+#pragma unroll
+    for (int w = 0; w < WM; ++w) {
+      if (w < WW) {
+        S[w] = ~S[w] + cy;
+        cy = (cy && S[w] == 0) ? 1ull : 0ull;
+      }
     }
   }
   int top = -1;
-  for (int w = WW - 1; w >= 0; --w)
-    if (S[w]) {
-      top = w;
-      break;
-    }
+#pragma unroll
+  for (int w = WM - 1; w >= 0; --w)
+    if (top < 0 && w < WW && S[w]) top = w;
   if (top < 0) {
     write_zero();
     return;
   }
-  const int bitlen = top * 64 + 64 - __clzll(S[top]);
+  const int bitlen = top * 64 + 64 - __clzll(word_at(S, top));
   const int pbits = 64 * N;
   int shift = bitlen - pbits;
   auto window = [&](int start) -> unsigned long long {  // bits [start, start + 64) of S
-    int word = (start >= 0) ? start / 64 : -((-start + 63) / 64);
-    int off = start - 64 * word;
-    unsigned long long lo = (word >= 0 && word < WW) ? S[word] : 0ull;
-    unsigned long long hi = (word + 1 >= 0 && word + 1 < WW) ? S[word + 1] : 0ull;
+    const int word = (start >= 0) ? start / 64 : -((-start + 63) / 64);
+    const int off = start - 64 * word;
+    const unsigned long long lo = word_at(S, word), hi = word_at(S, word + 1);
     return (lo >> off) | (off ? (hi << (64 - off)) : 0ull);
   };
   unsigned long long res[RNS_MAXN];
-  for (int q = 0; q < N; ++q) res[q] = window(shift + 64 * q);
+#pragma unroll
+  for (int q = 0; q < RNS_MAXN; ++q) res[q] = q < N ? window(shift + 64 * q) : 0ull;
   if (shift > 0) {
     const int rb = shift - 1;
-    const bool round_bit = (S[rb / 64] >> (rb % 64)) & 1ull;
+    const bool round_bit = (word_at(S, rb / 64) >> (rb % 64)) & 1ull;
     bool sticky = false;
-    for (int w = 0; w < rb / 64; ++w) sticky = sticky || (S[w] != 0);
-    if (rb % 64) sticky = sticky || ((S[rb / 64] & ((1ull << (rb % 64)) - 1)) != 0);
+#pragma unroll
+    for (int w = 0; w < WM; ++w) sticky = sticky || (w < rb / 64 && S[w] != 0);
+    if (rb % 64) sticky = sticky || ((word_at(S, rb / 64) & ((1ull << (rb % 64)) - 1)) != 0);
     if (round_bit && (sticky || (res[0] & 1ull))) {
       bool carry = true;
-      for (int q = 0; q < N && carry; ++q) {
-        res[q] += 1;
-        carry = (res[q] == 0);
+#pragma unroll
+      for (int q = 0; q < RNS_MAXN; ++q) {
+        if (q < N && carry) {
+          res[q] += 1;
+          carry = (res[q] == 0);
+        }
       }
       if (carry) {
-        res[N - 1] = 1ull << 63;
+#pragma unroll
+        for (int q = 0; q < RNS_MAXN; ++q)
+          if (q == N - 1) res[q] = 1ull << 63;
         shift += 1;
       }
     }
@@ -455,17 +490,38 @@ __global__ void k_rns_crt(const R* __restrict__ RC, long planeC, int m, int n, i
     write_zero();
     return;
   }
-  for (int q = 0; q < N; ++q) ol[q] = res[q];
+#pragma unroll
+  for (int q = 0; q < RNS_MAXN; ++q)
+    if (q < N) ol[q] = res[q];
   *okind = neg ? -MP_REGULAR : MP_REGULAR;
   *oexp = (int)exponent;
+}
+
+// The CRT kernel for WW words, instantiated with the smallest register width that holds them.
+template <typename R>
+void launch_crt(unsigned blocks, cudaStream_t st, const R* RC, long planeC, int m, int n, int L, int WW,
+                const uint32_t* primes, const uint32_t* wt, const double* pinv, const unsigned long long* MT,
+                const unsigned long long* Mbig, const int* loA, const int* loB, int N, int upper_only,
+                unsigned char* C, uint32_t* status) {
+  if (WW <= 8)
+    k_rns_crt<R, 8><<<blocks, 128, 0, st>>>(RC, planeC, m, n, L, WW, primes, wt, pinv, MT, Mbig, loA, loB, N,
+                                            upper_only, C, status);
+  else if (WW <= 16)
+    k_rns_crt<R, 16><<<blocks, 128, 0, st>>>(RC, planeC, m, n, L, WW, primes, wt, pinv, MT, Mbig, loA, loB, N,
+                                             upper_only, C, status);
+  else if (WW <= 32)
+    k_rns_crt<R, 32><<<blocks, 128, 0, st>>>(RC, planeC, m, n, L, WW, primes, wt, pinv, MT, Mbig, loA, loB, N,
+                                             upper_only, C, status);
+  else
+    k_rns_crt<R, RNS_MAXW><<<blocks, 128, 0, st>>>(RC, planeC, m, n, L, WW, primes, wt, pinv, MT, Mbig, loA, loB,
+                                                   N, upper_only, C, status);
 }
 
 // ---- exact forms of small factors (rns_blas.rs:2990-3194 diag_congruence, 4025-4174
 // svec_quadratic, 4175-4277 symmetric_bilinear) ----
 // Residues in [0, p_t) of a flat array of MpFloat<N> aligned at one exponent lo (the class's
 // lowest set bit): entry e is (-1)^s M_e 2^(exp_e - 64N - lo); out[t * count + e].  absval drops
-// the signs.  The residue is sum_c chunk_c (2^(16c + shift) mod p) over the mantissa's 16-bit
-// chunks, as in k_rns8_residues.
+// the signs.  The residue is computed as in k_rns8_residues (residue_of).
 extern "C" __global__ void k_rns_class_residues(const unsigned char* __restrict__ X, int N, int count, int lo,
                                                 int absval, int L, const int* __restrict__ primes,
                                                 const double* __restrict__ pinv,
@@ -481,16 +537,12 @@ extern "C" __global__ void k_rns_class_residues(const unsigned char* __restrict_
   const bool neg = kind < 0 && !absval;
   const int shift = elem_exp(x, N) - 64 * N - lo;
   const unsigned long long* lp = reinterpret_cast<const unsigned long long*>(x);
+  unsigned long long limbs[RNS_MAXN];
+#pragma unroll
+  for (int q = 0; q < RNS_MAXN; ++q) limbs[q] = q < N ? lp[q] : 0ull;
   for (int t = 0; t < L; ++t) {
-    const uint32_t* w = pow2 + (size_t)t * S + shift;
-    unsigned long long acc = 0;
-    for (int q = 0; q < N; ++q) {
-      const unsigned long long v = lp[q];
-      acc += (v & 0xFFFFull) * w[64 * q] + ((v >> 16) & 0xFFFFull) * w[64 * q + 16] +
-             ((v >> 32) & 0xFFFFull) * w[64 * q + 32] + (v >> 48) * w[64 * q + 48];
-    }
     const int p = primes[t];
-    int r = (int)mod53(acc, (uint32_t)p, pinv[t]);
+    int r = (int)residue_of(limbs, N, pow2 + (size_t)t * S, shift, (uint32_t)p, pinv[t]);
     if (neg && r) r = p - r;
     out[(size_t)t * count + e] = r;
   }
@@ -782,7 +834,7 @@ int32_t rns_product(RnsWorkspace& ws, cudaStream_t st, int form, int N, char ta,
     } else {
       check(cudaMemsetAsync(ws.RC8.p, 0, (size_t)L * planeC * sizeof(int), st), "memset");
     }
-    ++g_launches, k_rns_crt<int><<<(unsigned)((m * n + 127) / 128), 128, 0, st>>>(
+    ++g_launches, launch_crt<int>((unsigned)((m * n + 127) / 128), st, 
         ws.RC8, planeC, (int)m, (int)n, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB, N,
         upper_only ? 1 : 0, dC, ws.status);
   } else {
@@ -801,7 +853,7 @@ int32_t rns_product(RnsWorkspace& ws, cudaStream_t st, int form, int N, char ta,
     } else {
       check(cudaMemsetAsync(ws.RC.p, 0, (size_t)L * planeC * sizeof(double), st), "memset");
     }
-    ++g_launches, k_rns_crt<double><<<(unsigned)((m * n + 127) / 128), 128, 0, st>>>(
+    ++g_launches, launch_crt<double>((unsigned)((m * n + 127) / 128), st, 
         ws.RC, planeC, (int)m, (int)n, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB, N,
         upper_only ? 1 : 0, dC, ws.status);
   }
@@ -906,7 +958,7 @@ int32_t rns_congruence(RnsWorkspace& ws, cudaStream_t st, int N, char ta, uint64
     launch_i8_gemm(2, ws.PA, ws.PB, ga, st);
   }
   ++g_launches, k_add_const_int<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(ws.loA, (int)m, (int)lo_x, ws.loB2);
-  ++g_launches, k_rns_crt<int><<<(unsigned)((m * m + 127) / 128), 128, 0, st>>>(
+  ++g_launches, launch_crt<int>((unsigned)((m * m + 127) / 128), st, 
       ws.RC8, planeC, (int)m, (int)m, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB2, N,
       upper_only ? 1 : 0, dC, ws.status);
   check(cudaGetLastError(), "congruence launch");
@@ -965,7 +1017,7 @@ void crt_vector(RnsWorkspace& ws, cudaStream_t st, DevTables& DT, const PrimeTab
   grow(ws.loA, count); grow(ws.loB, 1);
   ++g_launches, k_fill_int<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(ws.loA, count, lo);
   ++g_launches, k_fill_int<<<1, 32, 0, st>>>(ws.loB, 1, 0);
-  ++g_launches, k_rns_crt<int><<<(unsigned)((count + 127) / 128), 128, 0, st>>>(
+  ++g_launches, launch_crt<int>((unsigned)((count + 127) / 128), st, 
       ws.RC8, count, count, 1, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB, N, 0, dOut,
       ws.status);
 }
@@ -1118,7 +1170,7 @@ int32_t rns_diag_congruence(RnsWorkspace& ws, cudaStream_t st, int N, uint64_t m
     launch_i8_gemm(2, ws.PA, ws.PB, ga, st);
   }
   ++g_launches, k_add_const_int<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(ws.loA, (int)m, lo_d, ws.loB2);
-  ++g_launches, k_rns_crt<int><<<(unsigned)((m * m + 127) / 128), 128, 0, st>>>(
+  ++g_launches, launch_crt<int>((unsigned)((m * m + 127) / 128), st, 
       ws.RC8, planeC, (int)m, (int)m, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB2, N,
       upper_only ? 1 : 0, dC, ws.status);
   check(cudaGetLastError(), "diag_congruence launch");
