@@ -381,9 +381,11 @@ __global__ void __launch_bounds__(128) k_rns_crt(const R* __restrict__ RC, long 
     write_zero();
     return;
   }
-  unsigned long long S[WM];
+  // S accumulates in 32-bit digits, one 64-bit accumulator each (c < 2^21 times a 32-bit digit
+  // is below 2^53, so up to 2^11 primes sum without overflow), carried once after the loop
+  unsigned long long acc[2 * WM];
 #pragma unroll
-  for (int w = 0; w < WM; ++w) S[w] = 0ull;
+  for (int w = 0; w < 2 * WM; ++w) acc[w] = 0ull;
   double f = 0.0;
   for (int t = 0; t < L; ++t) {
     const uint32_t p = primes[t];
@@ -394,19 +396,22 @@ __global__ void __launch_bounds__(128) k_rns_crt(const R* __restrict__ RC, long 
     if (r >= (long long)p) r -= p;
     const unsigned long long c = mod53((unsigned long long)r * wt[t], p, pi);  // < 2^42
     f += (double)c * pi;
-    const unsigned long long* row = MT + (size_t)t * WW;
+    const uint32_t* row = reinterpret_cast<const uint32_t*>(MT + (size_t)t * WW);  // 32-bit digits of M_t
+#pragma unroll
+    for (int w = 0; w < 2 * WM; ++w)  // S += c * M_t
+      if (w < 2 * WW) acc[w] += c * (unsigned long long)row[w];
+  }
+  unsigned long long S[WM];
+  {
     unsigned long long carry = 0;
 #pragma unroll
-    for (int w = 0; w < WM; ++w) {  // S += c * M_t
+    for (int w = 0; w < WM; ++w) {
+      S[w] = 0ull;
       if (w < WW) {
-        const unsigned long long mw = row[w];
-        const unsigned long long lo = mw * c, hi = __umul64hi(mw, c);
-        const unsigned long long s1 = S[w] + lo;
-        const unsigned long long c1 = s1 < lo;
-        const unsigned long long s2 = s1 + carry;
-        const unsigned long long c2 = s2 < s1;
-        S[w] = s2;
-        carry = hi + c1 + c2;
+        const unsigned long long lo = acc[2 * w] + carry;
+        const unsigned long long hi = acc[2 * w + 1] + (lo >> 32);
+        carry = hi >> 32;
+        S[w] = (hi << 32) | (lo & 0xFFFFFFFFull);
       }
     }
   }
