@@ -30,7 +30,7 @@ namespace {
 
 using mpd::Val;
 
-constexpr int kNtThreads = 256;
+constexpr int kNtThreads = 512;  // 16 warps: up to 16 rotations of a round at once
 constexpr int kNtWarps = kNtThreads / 32;
 constexpr int kNtMaxSweeps = 80;
 
