@@ -481,6 +481,102 @@ __device__ inline Val from_double(double f, long long e, int N) {
   return v;
 }
 
+// mp_dot_sub computed by a whole warp (every lane calls it with the same arguments; every lane
+// gets the result): the lanes take the terms c = lane, lane + 32, ..., each accumulates its
+// terms exactly in the same fixed-point frame (the warp-wide lowest scale), the partial
+// accumulators are added exactly by a shuffle tree, and lane 0 rounds once -- the bits of
+// mp_dot_sub, about thirty times faster for long dots.
+__device__ inline Val mp_dot_sub_warp(const Val* a, const unsigned char* x, long xs, const unsigned char* y, long ys,
+                                      int count, int N, bool* ok) {
+  const long esz = 8L * N + 8;
+  const int lane = threadIdx.x & 31;
+  long long lo = LLONG_MAX, hi = LLONG_MIN;
+  for (int c = lane; c < count; c += 32) {
+    const Val xv = mp_load(x + c * xs * esz, N), yv = mp_load(y + c * ys * esz, N);
+    if (xv.zero || yv.zero) continue;
+    const long long s = xv.s + yv.s;
+    lo = s < lo ? s : lo;
+    hi = s > hi ? s : hi;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const long long l2 = __shfl_xor_sync(0xffffffffu, lo, o), h2 = __shfl_xor_sync(0xffffffffu, hi, o);
+    lo = l2 < lo ? l2 : lo;
+    hi = h2 > hi ? h2 : hi;
+  }
+  if (a && !a->zero) {
+    lo = a->s < lo ? a->s : lo;
+    hi = (a->s - 64LL * N) > hi ? (a->s - 64LL * N) : hi;
+  }
+  if (lo == LLONG_MAX) return mp_zero();
+  const long long span = hi - lo + 128LL * N + 72;
+  const int W = (int)((span + 63) / 64) + 1;
+  if (W > kAccWords) {
+    *ok = false;
+    return mp_zero();
+  }
+  unsigned long long acc[kAccWords];
+  for (int w = 0; w < W; ++w) acc[w] = 0ull;
+  if (lane == 0 && a && !a->zero) {
+    if (a->neg)
+      sub_shifted(acc, W, a->m, N, a->s - lo);
+    else
+      add_shifted(acc, W, a->m, N, a->s - lo);
+  }
+  for (int c = lane; c < count; c += 32) {
+    const Val xv = mp_load(x + c * xs * esz, N), yv = mp_load(y + c * ys * esz, N);
+    if (xv.zero || yv.zero) continue;
+    unsigned long long P[2 * kMaxN] = {};
+    for (int i = 0; i < N; ++i) {
+      unsigned long long carry = 0;
+      for (int j = 0; j < N; ++j) {
+        const unsigned long long plo = xv.m[i] * yv.m[j], phi = __umul64hi(xv.m[i], yv.m[j]);
+        const unsigned long long t = P[i + j] + plo;
+        const unsigned long long c1 = t < plo;
+        const unsigned long long t2 = t + carry;
+        const unsigned long long c2 = t2 < t;
+        P[i + j] = t2;
+        carry = phi + c1 + c2;
+      }
+      P[i + N] += carry;
+    }
+    const bool term_neg = (xv.neg != yv.neg) != (a != nullptr);
+    if (term_neg)
+      sub_shifted(acc, W, P, 2 * N, xv.s + yv.s - lo);
+    else
+      add_shifted(acc, W, P, 2 * N, xv.s + yv.s - lo);
+  }
+  for (int o = 16; o > 0; o >>= 1) {  // exact two's-complement sum of the partial accumulators
+    unsigned long long carry = 0;
+    for (int w = 0; w < W; ++w) {
+      const unsigned long long b = __shfl_down_sync(0xffffffffu, acc[w], o);
+      const unsigned long long t = acc[w] + b;
+      const unsigned long long c1 = t < b;
+      const unsigned long long t2 = t + carry;
+      const unsigned long long c2 = t2 < t;
+      acc[w] = t2;
+      carry = c1 + c2;
+    }
+  }
+  Val r = mp_zero();
+  if (lane == 0) {
+    const bool neg = (acc[W - 1] >> 63) != 0;
+    if (neg) {
+      unsigned long long carry = 1;
+      for (int w = 0; w < W; ++w) {
+        acc[w] = ~acc[w] + carry;
+        carry = (carry && acc[w] == 0) ? 1ull : 0ull;
+      }
+    }
+    r = mp_round(acc, W, neg, lo, N);
+  }
+#pragma unroll
+  for (int q = 0; q < kMaxN; ++q) r.m[q] = __shfl_sync(0xffffffffu, r.m[q], 0);
+  r.s = __shfl_sync(0xffffffffu, r.s, 0);
+  r.neg = __shfl_sync(0xffffffffu, (int)r.neg, 0) != 0;
+  r.zero = __shfl_sync(0xffffffffu, (int)r.zero, 0) != 0;
+  return r;
+}
+
 // 1 / x and 1 / sqrt(x) by Newton's iteration from an FP64 seed (quadratic convergence: four
 // steps carry 53 bits past 512): accurate to a few units in the last place, not correctly
 // rounded -- used only for the Jacobi rotation parameters, whose orthogonality they bound.

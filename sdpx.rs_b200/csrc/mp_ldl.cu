@@ -44,23 +44,25 @@ __global__ void __launch_bounds__(128) k_mp_ldl_dots(unsigned char* A, long lda,
           *reinterpret_cast<const unsigned long long*>(el(W, j, (int)c, size, N) + o);
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {  // warp 0 forms the pivot's dot, its lane 0 the rest
       bool ok = true;
       const Val a = mpd::mp_load(el(B, j, j, lda, N), N);
-      const Val dot = mpd::mp_dot_sub(nullptr, srow, 1, swrow, 1, j, N, &ok);
+      const Val dot = mpd::mp_dot_sub_warp(nullptr, srow, 1, swrow, 1, j, N, &ok);
       Val d = mpd::mp_addsub(a, dot, -1, N);
-      if (d.zero && j > 0) d = mpd::mp_dot_sub(&a, srow, 1, swrow, 1, j, N, &ok);
-      if (reg) {  // DenseLeaf::pivot (arrow.rs:618-632), sign +1
-        const Val eps = mpd::mp_load(reg, N), delta = mpd::mp_load(reg + 8 * N + 8, N);
-        if (mpd::mp_cmp(d, eps, N) < 0) d = delta;
-      }
-      if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
-      if (d.zero) {
-        atomicOr(status, SDPXG_ST_PIVOT_FAIL);
-        s_fail = 1;
-      } else {
-        mpd::mp_store(sd, N, d, status);
-        mpd::mp_store(dinv + (long)j * (8L * N + 8), N, mpd::mp_recip(d, N), status);
+      if (d.zero && j > 0) d = mpd::mp_dot_sub_warp(&a, srow, 1, swrow, 1, j, N, &ok);
+      if (threadIdx.x == 0) {
+        if (reg) {  // DenseLeaf::pivot (arrow.rs:618-632), sign +1
+          const Val eps = mpd::mp_load(reg, N), delta = mpd::mp_load(reg + 8 * N + 8, N);
+          if (mpd::mp_cmp(d, eps, N) < 0) d = delta;
+        }
+        if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
+        if (d.zero) {
+          atomicOr(status, SDPXG_ST_PIVOT_FAIL);
+          s_fail = 1;
+        } else {
+          mpd::mp_store(sd, N, d, status);
+          mpd::mp_store(dinv + (long)j * (8L * N + 8), N, mpd::mp_recip(d, N), status);
+        }
       }
     }
     __syncthreads();
@@ -88,16 +90,20 @@ __global__ void __launch_bounds__(128) k_mp_ldl_dots(unsigned char* A, long lda,
 }
 
 // arrow.rs:437-447: each row of B solves x L' = b by exact dots, x_j = b_j - dot(x_<j, L(j, <j)).
-__global__ void k_mp_solve_lt(const unsigned char* L, long ldl, int k, unsigned char* B, long ldb, int m, int N,
-                              uint32_t* status) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
+// One warp per row (the dots split over the lanes, mp_dot_sub_warp), four rows per CTA.
+__global__ void __launch_bounds__(128) k_mp_solve_lt(const unsigned char* L, long ldl, int k, unsigned char* B,
+                                                     long ldb, int m, int N, uint32_t* status) {
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (i >= m) return;  // warp-uniform
   for (int j = 0; j < k; ++j) {
     bool ok = true;
     const Val x = mpd::mp_load(el(B, i, j, ldb, N), N);
-    const Val dot = mpd::mp_dot_sub(nullptr, el(B, i, 0, ldb, N), ldb, el(L, j, 0, ldl, N), ldl, j, N, &ok);
-    if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
-    mpd::mp_store(el(B, i, j, ldb, N), N, mpd::mp_addsub(x, dot, -1, N), status);
+    const Val dot = mpd::mp_dot_sub_warp(nullptr, el(B, i, 0, ldb, N), ldb, el(L, j, 0, ldl, N), ldl, j, N, &ok);
+    if (lane == 0) {
+      if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
+      mpd::mp_store(el(B, i, j, ldb, N), N, mpd::mp_addsub(x, dot, -1, N), status);
+    }
+    __syncwarp();  // x_j visible to the lanes' next dot
   }
 }
 
@@ -246,7 +252,7 @@ void mp_launch_solve_lt(const unsigned char* L, long ldl, int k, unsigned char* 
                         uint32_t* status, cudaStream_t st) {
   check_limbs(N);
   if (m <= 0 || k <= 0) return;
-  ++g_launches, k_mp_solve_lt<<<(m + 63) / 64, 64, 0, st>>>(L, ldl, k, B, ldb, m, N, status);
+  ++g_launches, k_mp_solve_lt<<<(m + 3) / 4, 128, 0, st>>>(L, ldl, k, B, ldb, m, N, status);
   check(cudaGetLastError(), "k_mp_solve_lt");
 }
 
