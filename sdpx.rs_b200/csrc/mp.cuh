@@ -10,8 +10,10 @@
 //   mp_addsub           aligned exact sum (operands more than 64N + 64 bits apart: the smaller
 //                       one lies below a 2^-64 fraction of an ulp and leaves the larger unchanged)
 //   mp_mul              2N-limb product
-//   mp_recip            binary long division of 2^(128N + 2) by the mantissa, the remainder
-//                       folded into a sticky bit
+//   mp_recip, mp_div,   the integer quotient floor(2^(128N + 2) / M), floor(M_a 2^(64N + 2) / M_b)
+//   mp_sqrt             or root floor(sqrt(M 2^e)) with its remainder folded into a sticky bit;
+//                       the quotient or root from a Newton estimate corrected exactly by its
+//                       multiword remainder (the same integers a long division would give)
 //   mp_dot_sub          a - sum x_c y_c (or sum x_c y_c) exact in a two's-complement fixed-point
 //                       accumulator of up to kAccWords words, rounded once -- the exact dot of
 //                       exactdot.rs:53-70; terms spread beyond the accumulator report failure.
@@ -227,164 +229,6 @@ __device__ inline Val mp_mul(const Val& a, const Val& b, int N) {
     P[i + N] += carry;
   }
   return mp_round(P, 2 * N, a.neg != b.neg, a.s + b.s, N);
-}
-
-// 1 / d: the quotient of 2^K (K = 128N + 2) by the mantissa by binary long division, the
-// remainder folded into a sticky low bit.
-__device__ inline Val mp_recip(const Val& d, int N) {
-  const int K = 128 * N + 2;
-  const int QW = 2 * N + 2;
-  unsigned long long Q[2 * kMaxN + 2] = {}, R[kMaxN + 1] = {};
-  for (int bit = K; bit >= 0; --bit) {
-    unsigned long long carry = (bit == K) ? 1ull : 0ull;  // R = 2 R + (bit == K)
-    for (int w = 0; w <= N; ++w) {
-      const unsigned long long nc = R[w] >> 63;
-      R[w] = (R[w] << 1) | carry;
-      carry = nc;
-    }
-    int cmp = R[N] ? 1 : 0;
-    for (int w = N - 1; w >= 0 && !cmp; --w) cmp = R[w] > d.m[w] ? 1 : (R[w] < d.m[w] ? -1 : 0);
-    if (cmp >= 0) {
-      unsigned long long borrow = 0;
-      for (int w = 0; w <= N; ++w) {
-        const unsigned long long dm = w < N ? d.m[w] : 0ull;
-        const unsigned long long t = R[w] - dm;
-        const unsigned long long b1 = R[w] < dm;
-        const unsigned long long t2 = t - borrow;
-        const unsigned long long b2 = t < borrow;
-        R[w] = t2;
-        borrow = b1 + b2;
-      }
-      Q[bit >> 6] |= 1ull << (bit & 63);
-    }
-  }
-  bool sticky = false;
-  for (int w = 0; w <= N; ++w) sticky = sticky || R[w];
-  unsigned long long S[2 * kMaxN + 3] = {};  // S = 2 Q + sticky at scale -(K + s) - 1
-  unsigned long long carry = sticky ? 1ull : 0ull;
-  for (int w = 0; w < QW + 1; ++w) {
-    const unsigned long long q = w < QW ? Q[w] : 0ull;
-    S[w] = (q << 1) | carry;
-    carry = q >> 63;
-  }
-  return mp_round(S, QW + 1, d.neg, -(long long)K - d.s - 1, N);
-}
-
-// a / b: the quotient of M_a 2^K (K = 64N + 2) by M_b by binary long division, remainder folded
-// into a sticky bit.  b must be nonzero.
-__device__ inline Val mp_div(const Val& a, const Val& b, int N) {
-  if (a.zero) {
-    Val z = mp_zero();
-    z.neg = a.neg != b.neg;
-    return z;
-  }
-  const int K = 64 * N + 2;
-  const int DB = 64 * N + K;  // dividend bits
-  unsigned long long Q[2 * kMaxN + 2] = {}, R[kMaxN + 1] = {};
-  for (int bit = DB - 1; bit >= 0; --bit) {
-    // next dividend bit: bit (bit - K) of M_a, zero below K
-    const int src = bit - K;
-    unsigned long long carry = (src >= 0) ? ((a.m[src >> 6] >> (src & 63)) & 1ull) : 0ull;
-    for (int w = 0; w <= N; ++w) {
-      const unsigned long long nc = R[w] >> 63;
-      R[w] = (R[w] << 1) | carry;
-      carry = nc;
-    }
-    int cmp = R[N] ? 1 : 0;
-    for (int w = N - 1; w >= 0 && !cmp; --w) cmp = R[w] > b.m[w] ? 1 : (R[w] < b.m[w] ? -1 : 0);
-    if (cmp >= 0) {
-      unsigned long long borrow = 0;
-      for (int w = 0; w <= N; ++w) {
-        const unsigned long long dm = w < N ? b.m[w] : 0ull;
-        const unsigned long long t = R[w] - dm;
-        const unsigned long long b1 = R[w] < dm;
-        const unsigned long long t2 = t - borrow;
-        const unsigned long long b2 = t < borrow;
-        R[w] = t2;
-        borrow = b1 + b2;
-      }
-      Q[bit >> 6] |= 1ull << (bit & 63);
-    }
-  }
-  bool sticky = false;
-  for (int w = 0; w <= N; ++w) sticky = sticky || R[w];
-  const int QW = (DB + 63) / 64;
-  unsigned long long S[2 * kMaxN + 3] = {};
-  unsigned long long carry = sticky ? 1ull : 0ull;
-  for (int w = 0; w < QW + 1; ++w) {
-    const unsigned long long q = w < QW ? Q[w] : 0ull;
-    S[w] = (q << 1) | carry;
-    carry = q >> 63;
-  }
-  // a / b = (Q + R/M_b) 2^(s_a - s_b - K)
-  return mp_round(S, QW + 1, a.neg != b.neg, a.s - b.s - K - 1, N);
-}
-
-// sqrt(a), a >= 0: the integer square root of M 2^e (e making the exponent even and the radicand
-// 2(64N + 2) bits wide) by the bit-pair restoring method, remainder folded into a sticky bit.
-__device__ inline Val mp_sqrt(const Val& a, int N) {
-  if (a.zero) return a;
-  const int RB = 64 * N + 2;              // root bits
-  long long e = 2LL * RB - 64LL * N;      // radicand = M 2^e has 2 RB bits (M has 64N)
-  if ((a.s - e) & 1) e += 1;              // a = M 2^s = (M 2^e) 2^(s - e), s - e even
-  const int XB = 64 * N + (int)e;         // radicand bit length bound
-  unsigned long long Y[kMaxN + 2] = {}, R[kMaxN + 3] = {};
-  const int W = N + 2;
-  for (int pair = (XB + 1) / 2 - 1; pair >= 0; --pair) {
-    // R = 4 R + next two radicand bits (bits 2 pair + 1, 2 pair of M 2^e)
-    unsigned long long two = 0;
-    for (int t = 1; t >= 0; --t) {
-      const long long bit = 2LL * pair + t - e;
-      const unsigned long long b = (bit >= 0 && bit < 64LL * N) ? ((a.m[bit >> 6] >> (bit & 63)) & 1ull) : 0ull;
-      two = (two << 1) | b;
-    }
-    unsigned long long carry = two;
-    for (int w = 0; w <= W; ++w) {
-      const unsigned long long nc = R[w] >> 62;
-      R[w] = (R[w] << 2) | carry;
-      carry = nc;
-    }
-    // T = 4 Y + 1; if R >= T: R -= T, Y = 2Y + 1 else Y = 2Y
-    unsigned long long T[kMaxN + 3] = {};
-    carry = 1;
-    for (int w = 0; w <= W; ++w) {
-      const unsigned long long y = w < W ? Y[w] : 0ull;
-      const unsigned long long prev = (w > 0 && w - 1 < W) ? Y[w - 1] : 0ull;
-      T[w] = (y << 2) | (prev >> 62) | carry;
-      carry = 0;
-    }
-    int cmp = 0;
-    for (int w = W; w >= 0 && !cmp; --w) cmp = R[w] > T[w] ? 1 : (R[w] < T[w] ? -1 : 0);
-    const bool take = cmp >= 0;
-    if (take) {
-      unsigned long long borrow = 0;
-      for (int w = 0; w <= W; ++w) {
-        const unsigned long long t1 = R[w] - T[w];
-        const unsigned long long b1 = R[w] < T[w];
-        const unsigned long long t2 = t1 - borrow;
-        const unsigned long long b2 = t1 < borrow;
-        R[w] = t2;
-        borrow = b1 + b2;
-      }
-    }
-    carry = take ? 1ull : 0ull;
-    for (int w = 0; w < W; ++w) {
-      const unsigned long long nc = Y[w] >> 63;
-      Y[w] = (Y[w] << 1) | carry;
-      carry = nc;
-    }
-  }
-  bool sticky = false;
-  for (int w = 0; w <= W; ++w) sticky = sticky || R[w];
-  unsigned long long S[kMaxN + 3] = {};
-  unsigned long long c2 = sticky ? 1ull : 0ull;
-  for (int w = 0; w < W + 1; ++w) {
-    const unsigned long long y = w < W ? Y[w] : 0ull;
-    S[w] = (y << 1) | c2;
-    c2 = y >> 63;
-  }
-  // sqrt(M 2^e 2^(s - e)) = Y' 2^((s - e) / 2), Y' = Y + frac
-  return mp_round(S, W + 1, false, (a.s - e) / 2 - 1, N);
 }
 
 // sign of a - b: -1, 0, 1.
@@ -605,5 +449,207 @@ __device__ inline Val mp_rsqrt_approx(const Val& x, int N) {  // x > 0
   return y;
 }
 
+
+// ---- correctly rounded reciprocal, quotient and square root ----
+// Each forms the exact integer quotient (or root) and remainder that a binary long division (or
+// digit-by-digit root) would give, from a Newton estimate in MpFloat arithmetic corrected exactly:
+// the remainder of the estimate is computed in multiword integers and the estimate stepped by
+// one until 0 <= remainder < divisor (a few steps: the estimate is within a few units); the
+// remainder then becomes the sticky bit of one rounding to 64N bits, ties to even.
+constexpr int kQW = kMaxN + 2;      // quotient / root words (N + 1 used)
+constexpr int kRW = 2 * kMaxN + 4;  // remainder words, two's complement
+
+// P = A (na words) * B (nb words), na + nb words.
+__device__ inline void mul_words(const unsigned long long* A, int na, const unsigned long long* B, int nb,
+                                 unsigned long long* P) {
+  for (int i = 0; i < na + nb; ++i) P[i] = 0ull;
+  for (int i = 0; i < na; ++i) {
+    unsigned long long carry = 0;
+    for (int j = 0; j < nb; ++j) {
+      const unsigned long long lo = A[i] * B[j], hi = __umul64hi(A[i], B[j]);
+      const unsigned long long t = P[i + j] + lo;
+      const unsigned long long c1 = t < lo;
+      const unsigned long long t2 = t + carry;
+      const unsigned long long c2 = t2 < t;
+      P[i + j] = t2;
+      carry = hi + c1 + c2;
+    }
+    P[i + nb] = carry;
+  }
+}
+// R += M (M n words, zero-extended; R W words, two's complement); R -= M.
+__device__ inline void addw(unsigned long long* R, int W, const unsigned long long* M, int n) {
+  unsigned long long carry = 0;
+  for (int w = 0; w < W; ++w) {
+    const unsigned long long m = w < n ? M[w] : 0ull;
+    const unsigned long long t = R[w] + m;
+    const unsigned long long c1 = t < m;
+    const unsigned long long t2 = t + carry;
+    carry = c1 + (t2 < t);
+    R[w] = t2;
+  }
+}
+__device__ inline void subw(unsigned long long* R, int W, const unsigned long long* M, int n) {
+  unsigned long long borrow = 0;
+  for (int w = 0; w < W; ++w) {
+    const unsigned long long m = w < n ? M[w] : 0ull;
+    const unsigned long long t = R[w] - m;
+    const unsigned long long b1 = R[w] < m;
+    const unsigned long long t2 = t - borrow;
+    borrow = b1 + (t < borrow);
+    R[w] = t2;
+  }
+}
+// Non-negative R (W words) against M (n words): -1, 0, 1.
+__device__ inline int cmpw(const unsigned long long* R, int W, const unsigned long long* M, int n) {
+  for (int w = W - 1; w >= 0; --w) {
+    const unsigned long long m = w < n ? M[w] : 0ull;
+    if (R[w] != m) return R[w] > m ? 1 : -1;
+  }
+  return 0;
+}
+__device__ inline void incw(unsigned long long* Q, int W) {
+  for (int w = 0; w < W; ++w)
+    if (++Q[w] != 0ull) break;
+}
+__device__ inline void decw(unsigned long long* Q, int W) {
+  for (int w = 0; w < W; ++w)
+    if (Q[w]-- != 0ull) break;
+}
+// floor(mantissa(v) 2^(s_v + sh)) into Q (QW words); v > 0.
+__device__ inline void to_int_words(const Val& v, int N, long long sh, unsigned long long* Q, int QW) {
+  for (int w = 0; w < QW; ++w) Q[w] = 0ull;
+  const long long t = v.s + sh;  // Q = M_v 2^t
+  if (t >= 0) {
+    const int q = (int)(t >> 6), r = (int)(t & 63);
+    for (int i = 0; i <= N; ++i) {
+      const unsigned long long lo = i < N ? v.m[i] : 0ull, prev = i > 0 ? v.m[i - 1] : 0ull;
+      if (q + i < QW) Q[q + i] = r ? ((lo << r) | (prev >> (64 - r))) : lo;
+    }
+  } else {
+    const long long u = -t;
+    const int q = (int)(u >> 6), r = (int)(u & 63);
+    for (int w = 0; w < QW; ++w) {
+      const int i = w + q;
+      const unsigned long long lo = i < N ? v.m[i] : 0ull, hi = (i + 1) < N ? v.m[i + 1] : 0ull;
+      Q[w] = r ? ((lo >> r) | (hi << (64 - r))) : lo;
+    }
+  }
+}
+// Step Q until R = X - Q D lies in [0, D) (D n words; R kRW words, two's complement).
+__device__ inline void fix_quotient(unsigned long long* Q, int QW, unsigned long long* R, const unsigned long long* D,
+                                    int n) {
+  for (int it = 0; it < 4096 && (R[kRW - 1] >> 63); ++it) {
+    decw(Q, QW);
+    addw(R, kRW, D, n);
+  }
+  for (int it = 0; it < 4096 && cmpw(R, kRW, D, n) >= 0; ++it) {
+    incw(Q, QW);
+    subw(R, kRW, D, n);
+  }
+}
+__device__ inline Val round_with_sticky(const unsigned long long* Q, int QW, const unsigned long long* R, bool neg,
+                                        long long scale, int N) {
+  bool sticky = false;
+  for (int w = 0; w < kRW; ++w) sticky = sticky || R[w];
+  unsigned long long S[kQW + 1];
+  unsigned long long carry = sticky ? 1ull : 0ull;
+  for (int w = 0; w <= QW; ++w) {  // S = 2 Q + sticky
+    const unsigned long long q = w < QW ? Q[w] : 0ull;
+    S[w] = (q << 1) | carry;
+    carry = q >> 63;
+  }
+  return mp_round(S, QW + 1, neg, scale, N);
+}
+
+// 1 / d: Q = floor(2^K / M_d), K = 128N + 2, remainder sticky.
+__device__ inline Val mp_recip(const Val& d, int N) {
+  const int K = 128 * N + 2, QW = N + 1;
+  Val m = d;  // M_d 2^-64N in [1/2, 1)
+  m.neg = false;
+  m.s = -64LL * N;
+  const Val y = mp_recip_approx(m, N);  // ~ 2^64N / M_d
+  unsigned long long Q[kQW], R[kRW], P[kRW];
+  to_int_words(y, N, K - 64LL * N, Q, QW);  // ~ 2^K / M_d
+  mul_words(Q, QW, d.m, N, P);               // QW + N words
+  for (int w = 0; w < kRW; ++w) R[w] = 0ull;
+  R[K >> 6] = 1ull << (K & 63);
+  subw(R, kRW, P, QW + N);
+  fix_quotient(Q, QW, R, d.m, N);
+  return round_with_sticky(Q, QW, R, d.neg, -(long long)K - d.s - 1, N);
+}
+
+// a / b: Q = floor(M_a 2^K / M_b), K = 64N + 2, remainder sticky.  b must be nonzero.
+__device__ inline Val mp_div(const Val& a, const Val& b, int N) {
+  if (a.zero) {
+    Val z = mp_zero();
+    z.neg = a.neg != b.neg;
+    return z;
+  }
+  const int K = 64 * N + 2, QW = N + 1;
+  Val an = a, bn = b;
+  an.neg = bn.neg = false;
+  an.s = bn.s = -64LL * N;
+  const Val q = mp_mul(an, mp_recip_approx(bn, N), N);  // ~ M_a / M_b
+  unsigned long long Q[kQW], R[kRW], P[kRW];
+  to_int_words(q, N, K, Q, QW);
+  mul_words(Q, QW, b.m, N, P);
+  for (int w = 0; w < kRW; ++w) R[w] = 0ull;
+  for (int w = 0; w < N; ++w) {  // M_a 2^K: K = 64 N + 2
+    R[w + N] |= a.m[w] << 2;
+    R[w + N + 1] |= a.m[w] >> 62;
+  }
+  subw(R, kRW, P, QW + N);
+  fix_quotient(Q, QW, R, b.m, N);
+  return round_with_sticky(Q, QW, R, a.neg != b.neg, a.s - b.s - K - 1, N);
+}
+
+// sqrt(a), a >= 0: Y = floor(sqrt(M 2^e)), the radicand 2 (64N + 2) bits wide (e even with s - e),
+// remainder sticky.
+__device__ inline Val mp_sqrt(const Val& a, int N) {
+  if (a.zero) return a;
+  const int RB = 64 * N + 2, QW = N + 1;
+  long long e = 2LL * RB - 64LL * N;
+  if ((a.s - e) & 1) e += 1;
+  Val x = a;  // M 2^e
+  x.neg = false;
+  x.s = e;
+  const Val y = mp_mul(x, mp_rsqrt_approx(x, N), N);  // ~ sqrt(M 2^e)
+  unsigned long long Y[kQW], R[kRW], P[kRW], T[kQW + 1];
+  to_int_words(y, N, 0, Y, QW);
+  mul_words(Y, QW, Y, QW, P);  // Y^2, 2 QW words
+  for (int w = 0; w < kRW; ++w) R[w] = 0ull;
+  {
+    const int q = (int)(e >> 6), r = (int)(e & 63);  // X = M 2^e
+    for (int i = 0; i <= N; ++i) {
+      const unsigned long long lo = i < N ? a.m[i] : 0ull, prev = i > 0 ? a.m[i - 1] : 0ull;
+      R[q + i] |= r ? ((lo << r) | (prev >> (64 - r))) : lo;
+    }
+  }
+  subw(R, kRW, P, 2 * QW);
+  // 0 <= R = X - Y^2 <= 2Y: while negative Y -= 1, R += 2Y + 1 (new Y); while R > 2Y, R -= 2Y + 1, Y += 1
+  for (int it = 0; it < 4096 && (R[kRW - 1] >> 63); ++it) {
+    decw(Y, QW);
+    unsigned long long c = 1;
+    for (int w = 0; w <= QW; ++w) {  // T = 2Y + 1
+      const unsigned long long v = w < QW ? Y[w] : 0ull, pv = w > 0 ? Y[w - 1] : 0ull;
+      T[w] = (v << 1) | (pv >> 63) | c;
+      c = 0;
+    }
+    addw(R, kRW, T, QW + 1);
+  }
+  for (int it = 0; it < 4096; ++it) {
+    unsigned long long c = 1;
+    for (int w = 0; w <= QW; ++w) {  // T = 2Y + 1
+      const unsigned long long v = w < QW ? Y[w] : 0ull, pv = w > 0 ? Y[w - 1] : 0ull;
+      T[w] = (v << 1) | (pv >> 63) | c;
+      c = 0;
+    }
+    if (cmpw(R, kRW, T, QW + 1) < 0) break;
+    subw(R, kRW, T, QW + 1);
+    incw(Y, QW);
+  }
+  return round_with_sticky(Y, QW, R, false, (a.s - e) / 2 - 1, N);
+}
 
 }  // namespace mpd
