@@ -156,20 +156,22 @@ __global__ void __launch_bounds__(128) k_mp_potrf(unsigned char* A, long si, lon
   }
   __syncthreads();
   for (int j = 0; j < n; ++j) {
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {  // warp 0 forms the pivot's dot, its lane 0 the rest
       bool ok = true;
-      const Val a = mpd::mp_load(at(j, j), N);
-      const Val dot = mpd::mp_dot_sub(nullptr, at(j, 0), sk, at(j, 0), sk, j, N, &ok);
-      const Val d = mpd::mp_addsub(a, dot, -1, N);
-      if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
-      if (d.zero || d.neg) {
-        mpd::mp_store(at(j, j), N, d, status);
-        *info = j + 1;
-        s_fail = 1;
-      } else {
-        const Val r = mpd::mp_sqrt(d, N);
-        mpd::mp_store(at(j, j), N, r, status);
-        mpd::mp_store(sd, N, r, status);
+      const Val dot = mpd::mp_dot_sub_warp(nullptr, at(j, 0), sk, at(j, 0), sk, j, N, &ok);
+      if (threadIdx.x == 0) {
+        const Val a = mpd::mp_load(at(j, j), N);
+        const Val d = mpd::mp_addsub(a, dot, -1, N);
+        if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
+        if (d.zero || d.neg) {
+          mpd::mp_store(at(j, j), N, d, status);
+          *info = j + 1;
+          s_fail = 1;
+        } else {
+          const Val r = mpd::mp_sqrt(d, N);
+          mpd::mp_store(at(j, j), N, r, status);
+          mpd::mp_store(sd, N, r, status);
+        }
       }
     }
     __syncthreads();

@@ -72,23 +72,26 @@ __device__ inline Val warp_sum(Val v, int N) {
 
 
 // Exact-dot Cholesky (lower, in place, column-major ld n) by a group of `nt` threads that
-// synchronise on named barrier `bar`: thread 0 forms each pivot, the group the column below it.
+// synchronise on named barrier `bar`: the group's first warp forms each pivot (its dot split over
+// the lanes), the group the column below it.
 __device__ void chol_group(unsigned char* L, int n, int N, int t, int nt, int bar, unsigned char* sd,
                            volatile int* fail, uint32_t* status) {
   const long esz = 8L * N + 8;
   auto at = [&](int i, int k) { return L + ((long)i + (long)k * n) * esz; };
   for (int j = 0; j < n; ++j) {
-    if (t == 0) {
+    if (t < 32) {  // the group's first warp forms the pivot's dot, its lane 0 the rest
       bool ok = true;
-      const Val dot = mpd::mp_dot_sub(nullptr, at(j, 0), n, at(j, 0), n, j, N, &ok);
-      const Val d = sub(mpd::mp_load(at(j, j), N), dot, N);
-      if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
-      if (d.zero || d.neg) {
-        *fail = 1;
-      } else {
-        const Val r = mpd::mp_sqrt(d, N);
-        mpd::mp_store(at(j, j), N, r, status);
-        mpd::mp_store(sd, N, r, status);
+      const Val dot = mpd::mp_dot_sub_warp(nullptr, at(j, 0), n, at(j, 0), n, j, N, &ok);
+      if (t == 0) {
+        const Val d = sub(mpd::mp_load(at(j, j), N), dot, N);
+        if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
+        if (d.zero || d.neg) {
+          *fail = 1;
+        } else {
+          const Val r = mpd::mp_sqrt(d, N);
+          mpd::mp_store(at(j, j), N, r, status);
+          mpd::mp_store(sd, N, r, status);
+        }
       }
     }
     named_sync(bar, nt);

@@ -291,17 +291,19 @@ __global__ void __launch_bounds__(kStThreads) k_mp_step_bound(const MpStepBlock*
     }
     __syncthreads();
     for (int j = 0; j < n; ++j) {
-      if (tid == 0) {
+      if (tid < 32) {  // warp 0 forms the pivot's dot, its lane 0 the rest
         bool ok = true;
-        const Val dot = mpd::mp_dot_sub(nullptr, el(C, j), n, el(C, j), n, j, N, &ok);
-        const Val d = sub(mpd::mp_load(el(C, j + (long)j * n), N), dot, N);
-        if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
-        if (d.zero || d.neg) {
-          s_fail = 1;
-        } else {
-          const Val r = mpd::mp_sqrt(d, N);
-          mpd::mp_store(el(C, j + (long)j * n), N, r, status);
-          mpd::mp_store(s_piv, N, r, status);
+        const Val dot = mpd::mp_dot_sub_warp(nullptr, el(C, j), n, el(C, j), n, j, N, &ok);
+        if (tid == 0) {
+          const Val d = sub(mpd::mp_load(el(C, j + (long)j * n), N), dot, N);
+          if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
+          if (d.zero || d.neg) {
+            s_fail = 1;
+          } else {
+            const Val r = mpd::mp_sqrt(d, N);
+            mpd::mp_store(el(C, j + (long)j * n), N, r, status);
+            mpd::mp_store(s_piv, N, r, status);
+          }
         }
       }
       __syncthreads();
