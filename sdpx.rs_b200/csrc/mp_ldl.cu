@@ -17,40 +17,43 @@ __device__ __forceinline__ const unsigned char* el(const unsigned char* A, long 
   return A + (i + j * ld) * (8L * N + 8);
 }
 
-// arrow.rs:156-242 ldl_dots on one block: columns in order; the CTA's thread 0 forms the pivot
+// arrow.rs:156-242 ldl_dots on one block: columns in order; the pivot
 // d_j = a_jj - dot(r_j, w_j) (the exact difference rounded once when that rounds to zero), the
 // pivot rule, D^-1; then every later row i: r_ij = (a_ij - dot(r_i, w_j)) * d_j^-1,
 // w_ij = r_ij d_j.  Dots are exact and rounded once; the other operations round once each.
-// Row j of R and of W (strided in memory) is staged in shared memory once per column: the pivot's
-// dot runs from there, and every row's dot reads w_j there (a broadcast) and its own row of R
-// from global memory, coalesced across the warp.
-__global__ void __launch_bounds__(128) k_mp_ldl_dots(unsigned char* A, long lda, int off, int size, int N,
-                                                     unsigned char* W, unsigned char* dinv,
-                                                     const unsigned char* reg, uint32_t* status) {
+// The block's lower triangle is copied into a row-major scratch R (and W is kept row-major) so
+// that every dot reads two contiguous rows; each dot runs on one warp (mp_dot_sub_warp), warp 0
+// for the pivot, the CTA's 16 warps over the later rows; R is written back at the end.
+// Scratch: 2 size^2 elements (W, then R).
+constexpr int kLeafThreads = 512;
+__global__ void __launch_bounds__(kLeafThreads) k_mp_ldl_dots(unsigned char* A, long lda, int off, int size, int N,
+                                                              unsigned char* Wsc, unsigned char* dinv,
+                                                              const unsigned char* reg, uint32_t* status) {
   __shared__ __align__(8) unsigned char sd[8 * mpd::kMaxN + 8];  // d_j
-  __shared__ __align__(8) unsigned char srow[kMpRecBase * (8 * mpd::kMaxN + 8)];  // r_j (columns < j)
-  __shared__ __align__(8) unsigned char swrow[kMpRecBase * (8 * mpd::kMaxN + 8)];  // w_j
   __shared__ int s_fail;
-  unsigned char* B = A + ((long)off + (long)off * lda) * (8L * N + 8);
-  if (threadIdx.x == 0) s_fail = 0;
-  __syncthreads();
   const long esz = 8L * N + 8;
+  unsigned char* B = A + ((long)off + (long)off * lda) * esz;
+  unsigned char* W = Wsc;                            // row-major: (i, c) at i * size + c
+  unsigned char* R = Wsc + (long)size * size * esz;  // row-major copy of the lower triangle
+  auto rm = [&](unsigned char* M, int i, int c) { return M + ((long)i * size + c) * esz; };
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  if (threadIdx.x == 0) s_fail = 0;
+  for (long wd = threadIdx.x; wd < (long)size * size * esz / 8; wd += blockDim.x) {  // R(i, c) = B(i, c)
+    const long e = wd * 8 / esz, o = wd * 8 % esz;
+    const int i = (int)(e / size), c = (int)(e % size);
+    if (c <= i)
+      *reinterpret_cast<unsigned long long*>(rm(R, i, c) + o) =
+          *reinterpret_cast<const unsigned long long*>(el(B, i, c, lda, N) + o);
+  }
+  __syncthreads();
   for (int j = 0; j < size; ++j) {
-    for (long wd = threadIdx.x; wd < (long)j * esz / 8; wd += blockDim.x) {  // stage r_j, w_j by words
-      const long b = 8 * wd, c = b / esz, o = b % esz;
-      *reinterpret_cast<unsigned long long*>(srow + b) =
-          *reinterpret_cast<const unsigned long long*>(el(B, j, (int)c, lda, N) + o);
-      *reinterpret_cast<unsigned long long*>(swrow + b) =
-          *reinterpret_cast<const unsigned long long*>(el(W, j, (int)c, size, N) + o);
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {  // warp 0 forms the pivot's dot, its lane 0 the rest
+    if (warp == 0) {  // the pivot: the dot over the lanes, the rest on lane 0
       bool ok = true;
-      const Val a = mpd::mp_load(el(B, j, j, lda, N), N);
-      const Val dot = mpd::mp_dot_sub_warp(nullptr, srow, 1, swrow, 1, j, N, &ok);
+      const Val a = mpd::mp_load(rm(R, j, j), N);
+      const Val dot = mpd::mp_dot_sub_warp(nullptr, rm(R, j, 0), 1, rm(W, j, 0), 1, j, N, &ok);
       Val d = mpd::mp_addsub(a, dot, -1, N);
-      if (d.zero && j > 0) d = mpd::mp_dot_sub_warp(&a, srow, 1, swrow, 1, j, N, &ok);
-      if (threadIdx.x == 0) {
+      if (d.zero && j > 0) d = mpd::mp_dot_sub_warp(&a, rm(R, j, 0), 1, rm(W, j, 0), 1, j, N, &ok);
+      if (lane == 0) {
         if (reg) {  // DenseLeaf::pivot (arrow.rs:618-632), sign +1
           const Val eps = mpd::mp_load(reg, N), delta = mpd::mp_load(reg + 8 * N + 8, N);
           if (mpd::mp_cmp(d, eps, N) < 0) d = delta;
@@ -61,24 +64,32 @@ __global__ void __launch_bounds__(128) k_mp_ldl_dots(unsigned char* A, long lda,
           s_fail = 1;
         } else {
           mpd::mp_store(sd, N, d, status);
-          mpd::mp_store(dinv + (long)j * (8L * N + 8), N, mpd::mp_recip(d, N), status);
+          mpd::mp_store(dinv + (long)j * esz, N, mpd::mp_recip(d, N), status);
         }
       }
     }
     __syncthreads();
     if (s_fail) return;
     const Val d = mpd::mp_load(sd, N);
-    const Val di = mpd::mp_load(dinv + (long)j * (8L * N + 8), N);
-    for (int i = j + 1 + threadIdx.x; i < size; i += blockDim.x) {
+    const Val di = mpd::mp_load(dinv + (long)j * esz, N);
+    for (int i = j + 1 + warp; i < size; i += nwarps) {  // warp-uniform
       bool ok = true;
-      const Val a = mpd::mp_load(el(B, i, j, lda, N), N);
-      const Val dot = mpd::mp_dot_sub(nullptr, el(B, i, 0, lda, N), lda, swrow, 1, j, N, &ok);
-      if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
-      const Val v = mpd::mp_mul(mpd::mp_addsub(a, dot, -1, N), di, N);
-      mpd::mp_store(el(B, i, j, lda, N), N, v, status);
-      mpd::mp_store(el(W, i, j, size, N), N, mpd::mp_mul(v, d, N), status);
+      const Val dot = mpd::mp_dot_sub_warp(nullptr, rm(R, i, 0), 1, rm(W, j, 0), 1, j, N, &ok);
+      if (lane == 0) {
+        if (!ok) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
+        const Val v = mpd::mp_mul(mpd::mp_addsub(mpd::mp_load(rm(R, i, j), N), dot, -1, N), di, N);
+        mpd::mp_store(rm(R, i, j), N, v, status);
+        mpd::mp_store(rm(W, i, j), N, mpd::mp_mul(v, d, N), status);
+      }
     }
     __syncthreads();
+  }
+  for (long wd = threadIdx.x; wd < (long)size * size * esz / 8; wd += blockDim.x) {  // B(i, c) = R(i, c), c < i
+    const long e = wd * 8 / esz, o = wd * 8 % esz;
+    const int i = (int)(e / size), c = (int)(e % size);
+    if (c < i)
+      *reinterpret_cast<unsigned long long*>(el(B, i, c, lda, N) + o) =
+          *reinterpret_cast<const unsigned long long*>(rm(R, i, c) + o);
   }
   for (int j = threadIdx.x; j < size; j += blockDim.x) {  // unit diagonal
     Val one = mpd::mp_zero();
@@ -199,7 +210,7 @@ void mp_launch_ldl_dots(unsigned char* A, long lda, int off, int size, int N, un
   check_limbs(N);
   if (size <= 0) return;
   if (size > kMpRecBase) throw std::invalid_argument("MPFR LDL: leaf above the recursion base");
-  ++g_launches, k_mp_ldl_dots<<<1, 128, 0, st>>>(A, lda, off, size, N, W, dinv, reg, status);
+  ++g_launches, k_mp_ldl_dots<<<1, kLeafThreads, 0, st>>>(A, lda, off, size, N, W, dinv, reg, status);
   check(cudaGetLastError(), "k_mp_ldl_dots");
 }
 

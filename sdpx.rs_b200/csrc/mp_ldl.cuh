@@ -14,7 +14,7 @@ constexpr int kMpMaxLimbs = 8;   // up to 512-bit values on the device
 
 // Left-looking exact-dot LDL' of the order-`size` diagonal block at (off, off) of A (lower
 // triangle read and overwritten with the unit lower L), D^-1 into dinv[0..size); W is a
-// size x size scratch.  reg: NULL or (eps, delta) as two MpFloat values (the pivot rule).
+// 2 size^2 scratch (row-major W and a row-major copy of the block).  reg: NULL or (eps, delta) as two MpFloat values (the pivot rule).
 void mp_launch_ldl_dots(unsigned char* A, long lda, int off, int size, int N, unsigned char* W,
                         unsigned char* dinv, const unsigned char* reg, uint32_t* status, cudaStream_t st);
 // The reference's exact Cholesky xpotrf (mpfr.rs:726-789) of the n x n triangle of A (lower

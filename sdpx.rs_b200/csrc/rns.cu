@@ -1478,7 +1478,7 @@ extern "C" int32_t sdpxg_mp_ldl_device(sdpxg_ctx* ctx, uint32_t limbs, uint64_t 
     DevBuf<uint32_t> stw(1);
     check(cudaMemsetAsync(stw.p, 0, sizeof(uint32_t), E->st), "memset");
     MpLdl f{ws, E->st, N, static_cast<const unsigned char*>(d_reg), stw.p};
-    DevBuf<unsigned char> Wleaf((size_t)kMpRecBase * kMpRecBase * f.esz());
+    DevBuf<unsigned char> Wleaf(2 * (size_t)kMpRecBase * kMpRecBase * f.esz());  // the leaves' W and R
     f.ldl_rec(static_cast<unsigned char*>(d_A), (long)lda, 0, (int)n, static_cast<unsigned char*>(d_dinv), Wleaf);
     uint32_t hs = 0;
     copy_d2h(&hs, stw.p, sizeof(uint32_t), E->st);
