@@ -307,10 +307,8 @@ class Reducer {
     if (n > 0) {
       ++g_launches, k_reduce_fused<<<kBlocks, 256, 0, st>>>(op, n, x, y, partial_.p + (size_t)s * kBlocks,
                                                           counters_.p + s, slots_.p + s);
-    } else {
-      double id = (op == RED_FINITE) ? 1.0 : 0.0;
+    } else {  // an empty input: the operation's identity (1 for the finite test, 0 otherwise)
       copy_h2d(slots_.p + s, &id_[op], sizeof(double), st);
-      (void)id;
     }
     return s;
   }

@@ -10,7 +10,8 @@
 //                                      MpFloat arithmetic: the reference's MPFR right SVD
 //                                      (mpfr_svd.rs, Golub-Kahan + dqds + inverse iteration) is
 //                                      replaced by a method whose rotations of disjoint column
-//                                      pairs run in parallel, one warp per pair; singular values
+//                                      pairs run in parallel, one warp per pair (its column sums
+//                                      exact dots over the lanes); singular values
 //                                      are the final column norms, sorted descending
 //   lambda = sigma, Lambda^-1/2 = 1 / sqrt(sigma)
 //   R = L1 V Lambda^-1/2,  Rinv = Lambda^1/2 (L1^-T V)',  G = R R' (upper)
@@ -42,34 +43,6 @@ __device__ __forceinline__ void named_sync(int id, int count) {
 __device__ __forceinline__ Val add(const Val& a, const Val& b, int N) { return mpd::mp_addsub(a, b, 1, N); }
 __device__ __forceinline__ Val sub(const Val& a, const Val& b, int N) { return mpd::mp_addsub(a, b, -1, N); }
 __device__ __forceinline__ Val mul(const Val& a, const Val& b, int N) { return mpd::mp_mul(a, b, N); }
-
-__device__ __forceinline__ Val shfl_down(const Val& v, int d) {
-  Val r;
-#pragma unroll
-  for (int q = 0; q < mpd::kMaxN; ++q) r.m[q] = __shfl_down_sync(0xffffffffu, v.m[q], d);
-  r.s = __shfl_down_sync(0xffffffffu, v.s, d);
-  r.neg = __shfl_down_sync(0xffffffffu, (int)v.neg, d) != 0;
-  r.zero = __shfl_down_sync(0xffffffffu, (int)v.zero, d) != 0;
-  return r;
-}
-__device__ __forceinline__ Val shfl_bcast(const Val& v) {
-  Val r;
-#pragma unroll
-  for (int q = 0; q < mpd::kMaxN; ++q) r.m[q] = __shfl_sync(0xffffffffu, v.m[q], 0);
-  r.s = __shfl_sync(0xffffffffu, v.s, 0);
-  r.neg = __shfl_sync(0xffffffffu, (int)v.neg, 0) != 0;
-  r.zero = __shfl_sync(0xffffffffu, (int)v.zero, 0) != 0;
-  return r;
-}
-// Sum over the warp (a fixed tree, lane 0's result broadcast: every lane gets the same bits).
-__device__ inline Val warp_sum(Val v, int N) {
-  for (int d = 16; d > 0; d >>= 1) {
-    const Val o = shfl_down(v, d);
-    v = add(v, o, N);
-  }
-  return shfl_bcast(v);
-}
-
 
 // Exact-dot Cholesky (lower, in place, column-major ld n) by a group of `nt` threads that
 // synchronise on named barrier `bar`: the group's first warp forms each pivot (its dot split over
@@ -207,16 +180,12 @@ __global__ void __launch_bounds__(kNtThreads) k_mp_nt_scale(const MpNtBlock* __r
         const int p = pa == 0 ? 0 : 1 + (pa - 1 + r) % (mm - 1);
         const int q = pb == 0 ? 0 : 1 + (pb - 1 + r) % (mm - 1);
         if (p >= n || q >= n) continue;
-        Val aa = mpd::mp_zero(), bb = mpd::mp_zero(), gg = mpd::mp_zero();
-        for (int i = lane; i < n; i += 32) {
-          const Val ap = mpd::mp_load(el(A, i + (long)p * n), N), aq = mpd::mp_load(el(A, i + (long)q * n), N);
-          aa = add(aa, mul(ap, ap, N), N);
-          bb = add(bb, mul(aq, aq, N), N);
-          gg = add(gg, mul(ap, aq, N), N);
-        }
-        aa = warp_sum(aa, N);
-        bb = warp_sum(bb, N);
-        gg = warp_sum(gg, N);
+        // the three column sums as exact dots over the warp (every lane gets the same bits)
+        bool okd = true;
+        const Val aa = mpd::mp_dot_sub_warp(nullptr, el(A, (long)p * n), 1, el(A, (long)p * n), 1, n, N, &okd);
+        const Val bb = mpd::mp_dot_sub_warp(nullptr, el(A, (long)q * n), 1, el(A, (long)q * n), 1, n, N, &okd);
+        const Val gg = mpd::mp_dot_sub_warp(nullptr, el(A, (long)p * n), 1, el(A, (long)q * n), 1, n, N, &okd);
+        if (!okd && lane == 0) atomicOr(status, SDPXG_ST_EXACT_SPREAD);
         bool rot = !gg.zero && !aa.zero && !bb.zero;
         if (rot) {
           Val ab = mul(aa, bb, N);
