@@ -42,8 +42,11 @@ k_schur_transform(const BlockDesc* __restrict__ blocks, const int* __restrict__ 
   cta_store_svec(Tcol + off, X, n);
 }
 
-// Grouped GEMM S_j = Acol_j' * Tcol_j (k_j x k_j, inner tri(n_j)).  Tile list entries
-// (block, tile row, tile col) of 32 x 32 output tiles.
+// Grouped GEMM S_j = Acol_j' * Tcol_j (k_j x k_j, inner tri(n_j)) on the FP64 tensor cores.
+// Tile list entries (block, tile row, tile col) of 32 x 32 output tiles; a 32-row K chunk of both
+// operands is staged in shared memory, and each of the 8 warps owns two 8 x 8 output subtiles
+// accumulated by mma.sync m8n8k4 (lane (r, q): A fragment A'(row r, k q), B fragment T(k q,
+// column r); results C(r, 2q) and C(r, 2q + 1)).
 #define SCHUR_TILE 32
 #define SCHUR_KC 32
 extern "C" __global__ void __launch_bounds__(SDPXG_THREADS)
@@ -60,34 +63,34 @@ k_schur_block_gemm(const BlockDesc* __restrict__ blocks, const int* __restrict__
   const int k = kcount[j];
   const double* A = Acol + acol_off[j];
   const double* T = Tcol + acol_off[j];
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  const int a0 = ti * SCHUR_TILE + 2 * tx, b0 = tj * SCHUR_TILE + 2 * ty;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, r = lane >> 2, q = lane & 3;
+  // subtiles w and w + 8 of the 4 x 4 grid of 8 x 8 subtiles
+  const int I0 = w >> 2, J0 = w & 3, I1 = (w + 8) >> 2, J1 = (w + 8) & 3;
   double c00 = 0, c01 = 0, c10 = 0, c11 = 0;
   for (int r0 = 0; r0 < tn; r0 += SCHUR_KC) {
     for (int e = threadIdx.x; e < SCHUR_KC * SCHUR_TILE; e += blockDim.x) {
       int rr = e % SCHUR_KC, cc = e / SCHUR_KC;
-      int r = r0 + rr;
+      int rw = r0 + rr;
       int ca = ti * SCHUR_TILE + cc, cb = tj * SCHUR_TILE + cc;
-      As[rr][cc] = (r < tn && ca < k) ? A[(long)ca * tn + r] : 0.0;
-      Ts[rr][cc] = (r < tn && cb < k) ? T[(long)cb * tn + r] : 0.0;
+      As[rr][cc] = (rw < tn && ca < k) ? A[(long)ca * tn + rw] : 0.0;
+      Ts[rr][cc] = (rw < tn && cb < k) ? T[(long)cb * tn + rw] : 0.0;
     }
     __syncthreads();
-#pragma unroll 8
-    for (int rr = 0; rr < SCHUR_KC; ++rr) {
-      double x0 = As[rr][2 * tx], x1 = As[rr][2 * tx + 1];
-      double y0 = Ts[rr][2 * ty], y1 = Ts[rr][2 * ty + 1];
-      c00 = fma(x0, y0, c00);
-      c01 = fma(x0, y1, c01);
-      c10 = fma(x1, y0, c10);
-      c11 = fma(x1, y1, c11);
+#pragma unroll
+    for (int ks = 0; ks < SCHUR_KC / 4; ++ks) {
+      const int kk = 4 * ks + q;
+      dmma_m8n8k4(c00, c01, As[kk][8 * I0 + r], Ts[kk][8 * J0 + r]);
+      dmma_m8n8k4(c10, c11, As[kk][8 * I1 + r], Ts[kk][8 * J1 + r]);
     }
     __syncthreads();
   }
   double* out = S + s_off[j];
+  const int a0 = ti * SCHUR_TILE + 8 * I0 + r, b0 = tj * SCHUR_TILE + 8 * J0 + 2 * q;
+  const int a1 = ti * SCHUR_TILE + 8 * I1 + r, b1 = tj * SCHUR_TILE + 8 * J1 + 2 * q;
   if (a0 < k && b0 < k) out[a0 + (long)b0 * k] = c00;
   if (a0 < k && b0 + 1 < k) out[a0 + (long)(b0 + 1) * k] = c01;
-  if (a0 + 1 < k && b0 < k) out[a0 + 1 + (long)b0 * k] = c10;
-  if (a0 + 1 < k && b0 + 1 < k) out[a0 + 1 + (long)(b0 + 1) * k] = c11;
+  if (a1 < k && b1 < k) out[a1 + (long)b1 * k] = c10;
+  if (a1 < k && b1 + 1 < k) out[a1 + (long)(b1 + 1) * k] = c11;
 }
 
 // H (m x m, full, column-major) = sum over shared blocks of S_j[la, lb], in cone order.
