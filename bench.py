@@ -344,6 +344,22 @@ def precision_f64(args):
     return out
 
 
+def dense_c0(args):
+    """The plain Float64 dense SDP (one PSD block n = 50, m = 200 dense constraints, ordinary Schur
+    form on the FP64 tensor cores): time to the gap per solve, problem resident."""
+    from sdpx_b200 import problems
+    from sdpx_b200.solver import DefaultSettings, DefaultSolver
+    prob = problems.dense_sdp(50, 200, seed=0)
+    s = DefaultSolver(prob.P, prob.q, prob.A, prob.b, prob.cones, DefaultSettings(kkt_form="condensed"))
+    s.solve()
+    dev, wall, _ = time_solves(s, max(3, args.steps))
+    out = {"workload": "dense_sdp: one PSD block n=50, m=200 dense constraints, seed 0, gap 1e-8, Float64",
+           "s": dev, "status": s.solution.status, "iterations": s.solution.iterations,
+           "objective": s.solution.obj_val, "iterations_per_s": s.solution.iterations / dev}
+    s.close()
+    return out
+
+
 def _random_mp(count, limbs, rng, spread=4):
     """Random MpFloat<limbs> values in the reference's layout (top mantissa bit set, sign in the
     kind, exponents in [-spread, spread], 5 % zeros) as raw bytes."""
@@ -602,6 +618,7 @@ def run_ours(args, world, rank, local):
     extra = {}
     if rank == 0 and not args.quick:
         extra["precision_f64"] = precision_f64(args)
+        extra["dense_c0"] = dense_c0(args)
         extra["rns_256"] = rns_256(args, peak_i8)
         try:  # a supplementary measurement: its failure is reported, the headline line still prints
             extra["mp_256_iteration"] = mp_chain_256(args, 4000)
