@@ -41,6 +41,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/sdpx_b200.h"
@@ -73,12 +74,13 @@ __device__ __forceinline__ int elem_exp(const unsigned char* p, int N) {
   return *reinterpret_cast<const int*>(p + 8 * N + 4);
 }
 
-// x mod p for 0 <= x < 2^53 by an FP64 quotient (exact to within one, then corrected).
-__device__ __forceinline__ uint32_t mod53(unsigned long long x, uint32_t p, double pinv) {
-  const unsigned long long q = (unsigned long long)((double)x * pinv);
-  long long r = (long long)(x - q * p);
-  if (r < 0) r += p;
-  if (r >= (long long)p) r -= p;
+// x mod p by Barrett reduction, mu = floor((2^64 - 1) / p): the quotient estimate umulhi(x, mu)
+// is at most two below floor(x / p), so two conditional subtractions finish; integer operations
+// only (no conversions to and from FP64).
+__device__ __forceinline__ uint32_t modb(unsigned long long x, uint32_t p, unsigned long long mu) {
+  unsigned long long r = x - __umul64hi(x, mu) * p;
+  if (r >= p) r -= p;
+  if (r >= p) r -= p;
   return (uint32_t)r;
 }
 
@@ -238,20 +240,20 @@ extern "C" __global__ void k_rns_pow2(int L, const int* __restrict__ primes, int
 
 // (M 2^shift) mod p for the mantissa M = sum_q limbs[q] 2^(64q): Horner over the limbs with
 // 2^32 and 2^64 mod p from the power table's row (row[s] = 2^s mod p, s < S, S > 64), each
-// step one FP64-quotient reduction of a value below 2^53, then one product with row[shift].
+// step one Barrett reduction, then one product with row[shift].
 __device__ __forceinline__ uint32_t residue_of(const unsigned long long* limbs, int N, const uint32_t* row,
-                                               int shift, uint32_t p, double pinv) {
+                                               int shift, uint32_t p, unsigned long long mu) {
   const unsigned long long c32 = row[32], c64 = row[64];
   unsigned long long r = 0;
 #pragma unroll
   for (int q = RNS_MAXN - 1; q >= 0; --q) {
     if (q < N) {
       const unsigned long long v = limbs[q];
-      const unsigned long long lm = mod53((v >> 32) * c32 + (v & 0xFFFFFFFFull), p, pinv);  // < 2^48
-      r = mod53(r * c64 + lm, p, pinv);                                                      // < 2^37
+      const unsigned long long lm = modb((v >> 32) * c32 + (v & 0xFFFFFFFFull), p, mu);
+      r = modb(r * c64 + lm, p, mu);
     }
   }
-  return mod53(r * row[shift], p, pinv);
+  return modb(r * row[shift], p, mu);
 }
 
 // INT8 form: symmetric residues modulo L primes below 2^15 of every entry of a view, each split
@@ -263,7 +265,7 @@ __device__ __forceinline__ uint32_t residue_of(const unsigned long long* limbs, 
 // (residue_of: three power-table reads per prime).
 extern "C" __global__ void k_rns8_residues(const unsigned char* __restrict__ X, int N, int nlines, int len,
                                            long sx, long sy, const int* __restrict__ lo, int L,
-                                           const int* __restrict__ primes, const double* __restrict__ pinv,
+                                           const int* __restrict__ primes, const unsigned long long* __restrict__ mu,
                                            const uint32_t* __restrict__ pow2, int S, int8_t* __restrict__ out,
                                            int Rpad, int Kld) {
   const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -291,7 +293,7 @@ extern "C" __global__ void k_rns8_residues(const unsigned char* __restrict__ X, 
     int dlo = 0, dhi = 0;
     if (live) {
       const int p = primes[t];
-      int r = (int)residue_of(limbs, N, pow2 + (size_t)t * S, shift, (uint32_t)p, pinv[t]);
+      int r = (int)residue_of(limbs, N, pow2 + (size_t)t * S, shift, (uint32_t)p, mu[t]);
       if (r > p / 2) r -= p;
       if (neg) r = -r;
       dlo = ((r + 128) & 255) - 128;
@@ -360,6 +362,7 @@ template <typename R, int WM>
 __global__ void __launch_bounds__(128) k_rns_crt(const R* __restrict__ RC, long planeC, int m, int n, int L, int WW,
                                                  const uint32_t* __restrict__ primes,
                                                  const uint32_t* __restrict__ wt, const double* __restrict__ pinv,
+                                                 const unsigned long long* __restrict__ mu,
                                                  const unsigned long long* __restrict__ MT,
                                                  const unsigned long long* __restrict__ Mbig,
                                                  const int* __restrict__ loA, const int* __restrict__ loB, int N,
@@ -390,11 +393,13 @@ __global__ void __launch_bounds__(128) k_rns_crt(const R* __restrict__ RC, long 
   for (int t = 0; t < L; ++t) {
     const uint32_t p = primes[t];
     const double pi = pinv[t];
-    long long r = (long long)RC[t * planeC + idx];  // |r| < 2^53
-    r -= (long long)floor((double)r * pi) * (long long)p;  // within one multiple of p
-    if (r < 0) r += p;
-    if (r >= (long long)p) r -= p;
-    const unsigned long long c = mod53((unsigned long long)r * wt[t], p, pi);  // < 2^42
+    long long r = (long long)RC[t * planeC + idx];
+    if (!std::is_same<R, int>::value) {  // the FP64 form's exact integers (|r| < 2^53, any sign)
+      r -= (long long)floor((double)r * pi) * (long long)p;  // within one multiple of p
+      if (r < 0) r += p;
+      if (r >= (long long)p) r -= p;
+    }  // the INT8 form's residues are in [0, p) already
+    const unsigned long long c = modb((unsigned long long)r * wt[t], p, mu[t]);
     f += (double)c * pi;
     const uint32_t* row = reinterpret_cast<const uint32_t*>(MT + (size_t)t * WW);  // 32-bit digits of M_t
 #pragma unroll
@@ -505,20 +510,21 @@ __global__ void __launch_bounds__(128) k_rns_crt(const R* __restrict__ RC, long 
 // The CRT kernel for WW words, instantiated with the smallest register width that holds them.
 template <typename R>
 void launch_crt(unsigned blocks, cudaStream_t st, const R* RC, long planeC, int m, int n, int L, int WW,
-                const uint32_t* primes, const uint32_t* wt, const double* pinv, const unsigned long long* MT,
+                const uint32_t* primes, const uint32_t* wt, const double* pinv, const unsigned long long* mu,
+                const unsigned long long* MT,
                 const unsigned long long* Mbig, const int* loA, const int* loB, int N, int upper_only,
                 unsigned char* C, uint32_t* status) {
   if (WW <= 8)
-    k_rns_crt<R, 8><<<blocks, 128, 0, st>>>(RC, planeC, m, n, L, WW, primes, wt, pinv, MT, Mbig, loA, loB, N,
+    k_rns_crt<R, 8><<<blocks, 128, 0, st>>>(RC, planeC, m, n, L, WW, primes, wt, pinv, mu, MT, Mbig, loA, loB, N,
                                             upper_only, C, status);
   else if (WW <= 16)
-    k_rns_crt<R, 16><<<blocks, 128, 0, st>>>(RC, planeC, m, n, L, WW, primes, wt, pinv, MT, Mbig, loA, loB, N,
+    k_rns_crt<R, 16><<<blocks, 128, 0, st>>>(RC, planeC, m, n, L, WW, primes, wt, pinv, mu, MT, Mbig, loA, loB, N,
                                              upper_only, C, status);
   else if (WW <= 32)
-    k_rns_crt<R, 32><<<blocks, 128, 0, st>>>(RC, planeC, m, n, L, WW, primes, wt, pinv, MT, Mbig, loA, loB, N,
+    k_rns_crt<R, 32><<<blocks, 128, 0, st>>>(RC, planeC, m, n, L, WW, primes, wt, pinv, mu, MT, Mbig, loA, loB, N,
                                              upper_only, C, status);
   else
-    k_rns_crt<R, RNS_MAXW><<<blocks, 128, 0, st>>>(RC, planeC, m, n, L, WW, primes, wt, pinv, MT, Mbig, loA, loB,
+    k_rns_crt<R, RNS_MAXW><<<blocks, 128, 0, st>>>(RC, planeC, m, n, L, WW, primes, wt, pinv, mu, MT, Mbig, loA, loB,
                                                    N, upper_only, C, status);
 }
 
@@ -529,7 +535,7 @@ void launch_crt(unsigned blocks, cudaStream_t st, const R* RC, long planeC, int 
 // the signs.  The residue is computed as in k_rns8_residues (residue_of).
 extern "C" __global__ void k_rns_class_residues(const unsigned char* __restrict__ X, int N, int count, int lo,
                                                 int absval, int L, const int* __restrict__ primes,
-                                                const double* __restrict__ pinv,
+                                                const unsigned long long* __restrict__ mu,
                                                 const uint32_t* __restrict__ pow2, int S, int* __restrict__ out) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
@@ -547,7 +553,7 @@ extern "C" __global__ void k_rns_class_residues(const unsigned char* __restrict_
   for (int q = 0; q < RNS_MAXN; ++q) limbs[q] = q < N ? lp[q] : 0ull;
   for (int t = 0; t < L; ++t) {
     const int p = primes[t];
-    int r = (int)residue_of(limbs, N, pow2 + (size_t)t * S, shift, (uint32_t)p, pinv[t]);
+    int r = (int)residue_of(limbs, N, pow2 + (size_t)t * S, shift, (uint32_t)p, mu[t]);
     if (neg && r) r = p - r;
     out[(size_t)t * count + e] = r;
   }
@@ -635,6 +641,7 @@ struct PrimeTables {
   int L = 0, WW = 0;
   std::vector<uint32_t> primes, W, wt;
   std::vector<double> pinv;
+  std::vector<unsigned long long> mu;  // floor((2^64 - 1) / p_t), the Barrett constants
   std::vector<unsigned long long> M, MT;  // M = prod p_t; MT row t = M / p_t (WW words each)
 };
 
@@ -695,6 +702,7 @@ PrimeTables make_tables(const std::vector<uint32_t>& ps, int L) {
   T.MT.assign((size_t)L * T.WW, 0);
   T.wt.assign(L, 0);
   T.pinv.assign(L, 0.0);
+  T.mu.assign(L, 0ull);
   for (int t = 0; t < L; ++t) {
     std::vector<unsigned long long> x(T.WW, 0);
     x[0] = 1;
@@ -708,6 +716,7 @@ PrimeTables make_tables(const std::vector<uint32_t>& ps, int L) {
     for (int w = 0; w < T.WW; ++w) T.MT[(size_t)t * T.WW + w] = x[w];
     T.wt[t] = (uint32_t)powmod64(rem, p - 2, p);
     T.pinv[t] = 1.0 / (double)p;
+    T.mu[t] = ~0ull / p;
   }
   return T;
 }
@@ -721,6 +730,7 @@ void grow(DevBuf<T>& b, size_t n) {
 struct DevTables {
   DevBuf<uint32_t> primes, W, wt;
   DevBuf<double> pinv;
+  DevBuf<unsigned long long> mu;
   DevBuf<int> iprimes;
   DevBuf<unsigned long long> M, MT;
   int L = -1;
@@ -730,12 +740,13 @@ struct DevTables {
     if (it == host.end()) it = host.emplace(L_, make_tables(prime_list(bits), L_)).first;
     const PrimeTables& T = it->second;
     if (L != L_) {
-      grow(primes, L_); grow(W, T.W.size()); grow(wt, L_); grow(pinv, L_);
+      grow(primes, L_); grow(W, T.W.size()); grow(wt, L_); grow(pinv, L_); grow(mu, L_);
       grow(iprimes, L_); grow(M, T.WW); grow(MT, T.MT.size());
       primes.upload(T.primes.data(), L_, st);
       W.upload(T.W.data(), T.W.size(), st);
       wt.upload(T.wt.data(), L_, st);
       pinv.upload(T.pinv.data(), L_, st);
+      mu.upload(T.mu.data(), L_, st);
       std::vector<int> ip(T.primes.begin(), T.primes.end());
       iprimes.upload(ip.data(), L_, st);
       M.upload(T.M.data(), T.WW, st);
@@ -823,9 +834,9 @@ int32_t rns_product(RnsWorkspace& ws, cudaStream_t st, int form, int N, char ta,
       grow(ws.PA, (size_t)L * 2 * Mpad * Kld);
       grow(ws.PB, (size_t)L * 2 * Npad * Kld);
       ++g_launches, k_rns8_residues<<<(unsigned)(((long)Mpad * Kld + 255) / 256), 256, 0, st>>>(
-          dA, N, (int)m, (int)k, asx, asy, ws.loA, L, DT.iprimes, DT.pinv, ws.pow2, S, ws.PA, Mpad, Kld);
+          dA, N, (int)m, (int)k, asx, asy, ws.loA, L, DT.iprimes, DT.mu, ws.pow2, S, ws.PA, Mpad, Kld);
       ++g_launches, k_rns8_residues<<<(unsigned)(((long)Npad * Kld + 255) / 256), 256, 0, st>>>(
-          dB, N, (int)n, (int)k, bsx, bsy, ws.loB, L, DT.iprimes, DT.pinv, ws.pow2, S, ws.PB, Npad, Kld);
+          dB, N, (int)n, (int)k, bsx, bsy, ws.loB, L, DT.iprimes, DT.mu, ws.pow2, S, ws.PB, Npad, Kld);
       check(cudaMemsetAsync(ws.err.p, 0, sizeof(int), st), "memset");
       for (int k0 = 0; k0 < Kld; k0 += kI8Chunk) {
         I8GemmArgs ga;
@@ -840,7 +851,7 @@ int32_t rns_product(RnsWorkspace& ws, cudaStream_t st, int form, int N, char ta,
       check(cudaMemsetAsync(ws.RC8.p, 0, (size_t)L * planeC * sizeof(int), st), "memset");
     }
     ++g_launches, launch_crt<int>((unsigned)((m * n + 127) / 128), st, 
-        ws.RC8, planeC, (int)m, (int)n, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB, N,
+        ws.RC8, planeC, (int)m, (int)n, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.mu, DT.MT, DT.M, ws.loA, ws.loB, N,
         upper_only ? 1 : 0, dC, ws.status);
   } else {
     const long planeA = (long)(m * std::max<uint64_t>(k, 1)), planeB = (long)(std::max<uint64_t>(k, 1) * n);
@@ -859,7 +870,7 @@ int32_t rns_product(RnsWorkspace& ws, cudaStream_t st, int form, int N, char ta,
       check(cudaMemsetAsync(ws.RC.p, 0, (size_t)L * planeC * sizeof(double), st), "memset");
     }
     ++g_launches, launch_crt<double>((unsigned)((m * n + 127) / 128), st, 
-        ws.RC, planeC, (int)m, (int)n, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB, N,
+        ws.RC, planeC, (int)m, (int)n, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.mu, DT.MT, DT.M, ws.loA, ws.loB, N,
         upper_only ? 1 : 0, dC, ws.status);
   }
   check(cudaGetLastError(), "rns launch");
@@ -939,11 +950,11 @@ int32_t rns_congruence(RnsWorkspace& ws, cudaStream_t st, int N, char ta, uint64
   grow(ws.PA, (size_t)L * 2 * Mpad * Kpad);  // A~ (rows of op(A)), used by both products
   grow(ws.PB, (size_t)L * 2 * (size_t)std::max(Kpad, Mpad) * Kpad);
   ++g_launches, k_rns8_residues<<<(unsigned)(((long)Mpad * Kpad + 255) / 256), 256, 0, st>>>(
-      dA, N, (int)m, (int)k, asx, asy, ws.loA, L, DT.iprimes, DT.pinv, ws.pow2, S, ws.PA, Mpad, Kpad);
+      dA, N, (int)m, (int)k, asx, asy, ws.loA, L, DT.iprimes, DT.mu, ws.pow2, S, ws.PA, Mpad, Kpad);
   ++g_launches, k_fill_int<<<(unsigned)((k + 255) / 256), 256, 0, st>>>(ws.loX, (int)k, (int)lo_x);
   // X~ by rows (line r: entries (r, c)): the left operand of T = X~ A~'
   ++g_launches, k_rns8_residues<<<(unsigned)(((long)Kpad * Kpad + 255) / 256), 256, 0, st>>>(
-      dX, N, (int)k, (int)k, 1, (long)ldx, ws.loX, L, DT.iprimes, DT.pinv, ws.pow2, S, ws.PB, Kpad, Kpad);
+      dX, N, (int)k, (int)k, 1, (long)ldx, ws.loX, L, DT.iprimes, DT.mu, ws.pow2, S, ws.PB, Kpad, Kpad);
   check(cudaMemsetAsync(ws.err.p, 0, sizeof(int), st), "memset");
   for (int k0 = 0; k0 < Kpad; k0 += kI8Chunk) {  // T (k x m) = X~ A~'
     I8GemmArgs ga;
@@ -964,7 +975,7 @@ int32_t rns_congruence(RnsWorkspace& ws, cudaStream_t st, int N, char ta, uint64
   }
   ++g_launches, k_add_const_int<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(ws.loA, (int)m, (int)lo_x, ws.loB2);
   ++g_launches, launch_crt<int>((unsigned)((m * m + 127) / 128), st, 
-      ws.RC8, planeC, (int)m, (int)m, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB2, N,
+      ws.RC8, planeC, (int)m, (int)m, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.mu, DT.MT, DT.M, ws.loA, ws.loB2, N,
       upper_only ? 1 : 0, dC, ws.status);
   check(cudaGetLastError(), "congruence launch");
   int herr = 0;
@@ -1023,7 +1034,7 @@ void crt_vector(RnsWorkspace& ws, cudaStream_t st, DevTables& DT, const PrimeTab
   ++g_launches, k_fill_int<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(ws.loA, count, lo);
   ++g_launches, k_fill_int<<<1, 32, 0, st>>>(ws.loB, 1, 0);
   ++g_launches, launch_crt<int>((unsigned)((count + 127) / 128), st, 
-      ws.RC8, count, count, 1, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB, N, 0, dOut,
+      ws.RC8, count, count, 1, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.mu, DT.MT, DT.M, ws.loA, ws.loB, N, 0, dOut,
       ws.status);
 }
 
@@ -1042,7 +1053,7 @@ void class_residues(RnsWorkspace& ws, cudaStream_t st, DevTables& DT, int N, int
   for (int c = 0; c < n; ++c)
     if (count[c])
       ++g_launches, k_rns_class_residues<<<(unsigned)((count[c] + 127) / 128), 128, 0, st>>>(
-          arr[c], N, count[c], lo[c], absval[c], L, DT.iprimes, DT.pinv, ws.pow2, S, ws.cres.p + off[c] * L);
+          arr[c], N, count[c], lo[c], absval[c], L, DT.iprimes, DT.mu, ws.pow2, S, ws.cres.p + off[c] * L);
 }
 
 // v[k] = sum_{i <= j} c_ij x_tri(j)+i q_ik q_jk (c_ii = 1, c_ij = sqrt2), k < kmax, each rounded
@@ -1163,7 +1174,7 @@ int32_t rns_diag_congruence(RnsWorkspace& ws, cudaStream_t st, int N, uint64_t m
   grow(ws.PA, (size_t)L * 2 * Mpad * Kpad);
   grow(ws.PB, (size_t)L * 2 * Mpad * Kpad);
   ++g_launches, k_rns8_residues<<<(unsigned)(((long)Mpad * Kpad + 255) / 256), 256, 0, st>>>(
-      dA, N, (int)m, (int)k, (long)lda, 1, ws.loA, L, DT.iprimes, DT.pinv, ws.pow2, S, ws.PA, Mpad, Kpad);
+      dA, N, (int)m, (int)k, (long)lda, 1, ws.loA, L, DT.iprimes, DT.mu, ws.pow2, S, ws.PA, Mpad, Kpad);
   ++g_launches, k_rns8_scale_planes<<<(unsigned)(((long)Mpad * Kpad + 255) / 256), 256, 0, st>>>(
       ws.PA, ws.cres.p + off[0] * L, (int)k, L, DT.iprimes, ws.PB, Mpad, Kpad);
   check(cudaMemsetAsync(ws.err.p, 0, sizeof(int), st), "memset");
@@ -1176,7 +1187,7 @@ int32_t rns_diag_congruence(RnsWorkspace& ws, cudaStream_t st, int N, uint64_t m
   }
   ++g_launches, k_add_const_int<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(ws.loA, (int)m, lo_d, ws.loB2);
   ++g_launches, launch_crt<int>((unsigned)((m * m + 127) / 128), st, 
-      ws.RC8, planeC, (int)m, (int)m, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.MT, DT.M, ws.loA, ws.loB2, N,
+      ws.RC8, planeC, (int)m, (int)m, L, T.WW, DT.primes, DT.wt, DT.pinv, DT.mu, DT.MT, DT.M, ws.loA, ws.loB2, N,
       upper_only ? 1 : 0, dC, ws.status);
   check(cudaGetLastError(), "diag_congruence launch");
   int herr = 0;
