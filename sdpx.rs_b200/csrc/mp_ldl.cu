@@ -23,9 +23,9 @@ __device__ __forceinline__ const unsigned char* el(const unsigned char* A, long 
 // w_ij = r_ij d_j.  Dots are exact and rounded once; the other operations round once each.
 // The block's lower triangle is copied into a row-major scratch R (and W is kept row-major) so
 // that every dot reads two contiguous rows; each dot runs on one warp (mp_dot_sub_warp), warp 0
-// for the pivot, the CTA's 16 warps over the later rows; R is written back at the end.
+// for the pivot, the CTA's 32 warps over the later rows; R is written back at the end.
 // Scratch: 2 size^2 elements (W, then R).
-constexpr int kLeafThreads = 512;
+constexpr int kLeafThreads = 1024;
 __global__ void __launch_bounds__(kLeafThreads) k_mp_ldl_dots(unsigned char* A, long lda, int off, int size, int N,
                                                               unsigned char* Wsc, unsigned char* dinv,
                                                               const unsigned char* reg, uint32_t* status) {
