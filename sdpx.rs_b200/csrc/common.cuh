@@ -17,7 +17,8 @@
 // bank pairs, and a column read is conflict-free.
 #define SDPXG_LD 68
 #define SDPXG_THREADS 256         // dense tile kernels (their thread maps assume 256)
-#define SDPXG_CONE_THREADS 1024   // one CTA per PSD block: one warp per Jacobi rotation pair
+#define SDPXG_CONE_THREADS 1024   // one CTA per PSD block
+#define SDPXG_NT_SVD_THREADS 512  // the NT scaling's Jacobi launch (8 warps iterate, 128 registers)
 #define SDPXG_RSQRT2 0.70710678118654752440
 #define SDPXG_SQRT2 1.41421356237309504880
 #define SDPXG_CHOL_SCRATCH (3 * SDPXG_NMAX)  // doubles of shared scratch for cta_cholesky_lower

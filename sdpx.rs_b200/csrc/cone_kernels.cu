@@ -22,32 +22,29 @@ constexpr int kMat = SDPXG_LD * SDPXG_NMAX;  // doubles per shared matrix
 //   R = L2^-T U lam^1/2,   Rinv = lam^-1/2 U' L2'
 // (L1 V = L1 M^-1 U lam = L2^-T U lam), which needs only the LEFT singular vectors: the
 // normalised columns that one-sided Jacobi leaves in M, so the rotations are not accumulated
-// into V (half the shared-memory traffic of every Jacobi round).  Both forms have the same
+// into V.  Both forms have the same
 // normwise accuracy (a triangular solve with L1 or with L2 each).  Ginv = Rinv' Rinv.
-// Shared memory: 5 matrices + 2 Cholesky scratches + 2n doubles + n ints + 1 int.
+// Two launches: k_nt_factor (1024 threads: both Cholesky factors in the register-resident CTA
+// form, M = L2'L1) leaves M in R's slot and L2 in Rinv's slot of each block; k_nt_svd (512
+// threads, room for the register-resident Jacobi) reads them back and writes R, Rinv, Ginv,
+// lam and lam^-1/2.  A failed factorisation sets SDPXG_ST_CHOL_FAIL, which the second launch
+// reads to leave every block alone (the scaling is rejected as a whole).
+// Shared memory of k_nt_factor: 3 matrices + 2 Cholesky scratches; of k_nt_svd: 5 matrices +
+// 2n doubles + n ints + 1 int.
 // ---------------------------------------------------------------------------------------
 extern "C" __global__ void __launch_bounds__(SDPXG_CONE_THREADS)
-k_nt_scale(const BlockDesc* __restrict__ blocks, const double* __restrict__ s,
-           const double* __restrict__ z, double* __restrict__ R, double* __restrict__ Rinv,
-           double* __restrict__ Ginv, double* __restrict__ lam, double* __restrict__ lisqrt,
-           uint32_t* __restrict__ status) {
+k_nt_factor(const BlockDesc* __restrict__ blocks, const double* __restrict__ s,
+            const double* __restrict__ z, double* __restrict__ R, double* __restrict__ Rinv,
+            uint32_t* __restrict__ status) {
   extern __shared__ double smem[];
   const BlockDesc bd = blocks[blockIdx.x];
   const int n = bd.n;
   double* L1 = smem;
   double* L2 = L1 + kMat;
   double* M = L2 + kMat;
-  double* V = M + kMat;
-  double* X = V + kMat;
-  double* piv = X + kMat;
+  double* piv = M + kMat;
   double* piv2 = piv + SDPXG_CHOL_SCRATCH;
-  double* sig = piv2 + SDPXG_CHOL_SCRATCH;
-  double* lsort = sig + SDPXG_NMAX;
-  int* rank = reinterpret_cast<int*>(lsort + SDPXG_NMAX);
-  int* flag = rank + SDPXG_NMAX;
-
-  cta_zero_mat(V);  // V and X are written n x n only: keep their padding zero for the MMAs
-  cta_zero_mat(X);
+  cta_zero_mat(M);
   cta_load_smat(L1, s + bd.svec_off, n);
   cta_load_smat(L2, z + bd.svec_off, n);
   bool ok1, ok2;
@@ -56,9 +53,36 @@ k_nt_scale(const BlockDesc* __restrict__ blocks, const double* __restrict__ s,
     if (threadIdx.x == 0) atomicOr(status, SDPXG_ST_CHOL_FAIL);
     return;
   }
-  cta_gemm(M, L2, true, L1, false, n);  // M = L2' L1 (L1 is free from here on)
+  cta_gemm(M, L2, true, L1, false, n);  // M = L2' L1
   __syncthreads();
-  int sweeps = cta_jacobi_svd(M, nullptr, n, flag, piv);  // M -> U diag(lam)
+  cta_store_mat(R + bd.mat_off, M, n);
+  cta_store_mat(Rinv + bd.mat_off, L2, n);
+}
+
+extern "C" __global__ void __launch_bounds__(SDPXG_NT_SVD_THREADS)
+k_nt_svd(const BlockDesc* __restrict__ blocks, double* __restrict__ R, double* __restrict__ Rinv,
+         double* __restrict__ Ginv, double* __restrict__ lam, double* __restrict__ lisqrt,
+         uint32_t* __restrict__ status) {
+  extern __shared__ double smem[];
+  if (*status & SDPXG_ST_CHOL_FAIL) return;
+  const BlockDesc bd = blocks[blockIdx.x];
+  const int n = bd.n;
+  double* L1 = smem;
+  double* L2 = L1 + kMat;
+  double* M = L2 + kMat;
+  double* V = M + kMat;
+  double* X = V + kMat;
+  double* sig = X + kMat;
+  double* lsort = sig + SDPXG_NMAX;
+  int* rank = reinterpret_cast<int*>(lsort + SDPXG_NMAX);
+  int* flag = rank + SDPXG_NMAX;
+
+  cta_zero_mat(V);  // V and X are written n x n only: keep their padding zero for the MMAs
+  cta_zero_mat(X);
+  cta_load_mat(M, R + bd.mat_off, n);
+  cta_load_mat(L2, Rinv + bd.mat_off, n);
+  __syncthreads();
+  int sweeps = cta_jacobi_left(M, n, L1, flag);  // M -> U diag(lam); L1 as scratch
   if (sweeps < 0) {
     if (threadIdx.x == 0) atomicOr(status, SDPXG_ST_SVD_UNCONVERGED);
     return;

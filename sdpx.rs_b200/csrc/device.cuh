@@ -191,8 +191,9 @@ struct PinnedBuf {
 
 // Kernel declarations (defined in the *_kernels.cu translation units of this library).
 extern "C" {
-__global__ void k_nt_scale(const BlockDesc*, const double*, const double*, double*, double*,
-                           double*, double*, double*, uint32_t*);
+__global__ void k_nt_factor(const BlockDesc*, const double*, const double*, double*, double*,
+                            uint32_t*);
+__global__ void k_nt_svd(const BlockDesc*, double*, double*, double*, double*, double*, uint32_t*);
 __global__ void k_identity_scaling(const BlockDesc*, double*, double*, double*, double*, double*);
 __global__ void k_ginv_from_rinv(const BlockDesc*, const double*, double*);
 __global__ void k_congruence(const BlockDesc*, int, const double*, const double*, const double*,

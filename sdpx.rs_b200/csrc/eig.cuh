@@ -1,8 +1,7 @@
 // CTA-level dense eigen / singular-value routines for PSD blocks of order <= SDPXG_NMAX.
 //
-//  * cta_jacobi_svd: one-sided (Hestenes) Jacobi with the parallel round-robin ordering.
-//    It orthogonalises the columns of M in place and accumulates the right singular
-//    vectors V.  Relative accuracy of the small singular values is what the NT scaling
+//  * cta_jacobi_left: one-sided (Hestenes) Jacobi with the parallel round-robin ordering,
+//    register-resident.  It orthogonalises the columns of M in place.  Relative accuracy of the small singular values is what the NT scaling
 //    needs (the reference takes the SVD of L2'L1 directly instead of an eigensolve of the
 //    squared matrix, cones/psdtrianglecone.rs:378-386).
 //  * cta_tridiagonalize: Householder reduction of a symmetric matrix to tridiagonal form.
@@ -13,104 +12,123 @@
 #include "common.cuh"
 
 #define SDPXG_JACOBI_MAX_SWEEPS 60
-#define SDPXG_JACOBI_TOL 1e-15
 #define SDPXG_BISECT_MAX 256
 
-// Returns the number of sweeps used, or -1 when the sweep bound was hit.  V == nullptr skips
-// the accumulation of the right singular vectors (the left ones are the normalised columns of
-// the result, which is all the NT scaling needs).
-// `flag` is one int of shared memory, `nrm` n doubles of shared memory.  The squared column
-// norms are recomputed at the start of every sweep and carried through the rotations with the
-// exact update a' = a - t g, b' = b + t g, so a rotation needs one warp reduction (g) instead
-// of three.
-__device__ inline int cta_jacobi_svd(double* M, double* V, int n, int* flag, double* nrm) {
-  if (V) {
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-      int i = e % n, j = e / n;
-      SM(V, i, j) = (i == j) ? 1.0 : 0.0;
+// One-sided (Hestenes) Jacobi on the columns of M (n x n, n <= 64, column-major shared memory
+// with leading dimension SDPXG_LD): on return M holds M V = U diag(sigma), columns in their
+// original order; V itself is not formed.  Returns the number of sweeps, or -1 when the sweep
+// bound was hit.  Every thread of the CTA calls it (blockDim.x >= 256).
+//
+// The matrix stays in registers for the whole iteration.  Warps 0..7 take part: warp w holds
+// rows [8w, 8w + 8) of the two columns of every pair, lane j the pair of slot j of the
+// round-robin (circle) ordering, which pairs positions j and N-1-j (N = n rounded up to even;
+// an odd n gets a zero column that never rotates).  After each round the columns move to their
+// next positions with two shuffles per row (tops one slot up, bottoms one slot down, slot 0's
+// top fixed), so no column goes back to shared memory inside the sweeps.  A pair's inner
+// products ||x||^2, ||y||^2, x'y are the sums of the eight warps' row partials taken in warp
+// order, so every warp holds the same bits and takes the same rotation decisions without a
+// broadcast; one named barrier per round (the partials are double-buffered in `part`, 1536
+// doubles of shared memory).  A pair rotates while |x'y| > 1e-15 sqrt(||x||^2 ||y||^2); the
+// angle comes from the half-angle formulas  cos 2t = |h| / r, sin 2t = sign(h) 2 x'y / r,
+// r = sqrt(h^2 + 4 (x'y)^2), h = ||y||^2 - ||x||^2,  c = sqrt((1 + cos 2t) / 2),
+// s = sin 2t / (2c)  (|t| <= pi/4, so c >= 1/sqrt 2 and nothing cancels; c^2 + s^2 = 1 to
+// rounding whatever the accuracy of the angle).  The sweeps stop after one without a rotation,
+// or after one in which every pair's cosine was below 1e-10 (the rotations of that sweep leave
+// cosines of order 1e-20: one-sided Jacobi converges quadratically).
+__device__ inline int cta_jacobi_left(double* M, int n, double* part, int* out) {
+  constexpr double kTol2 = 1e-30, kBig2 = 1e-20;
+  constexpr unsigned kFull = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, j = threadIdx.x & 31;
+  if (warp < 8) {
+    const int N = n + (n & 1), H = N / 2;
+    int itop = j < H ? j : -1, ibot = j < H ? N - 1 - j : -1;
+    double x[8], y[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int row = 8 * warp + k;
+      x[k] = (row < n && itop >= 0 && itop < n) ? SM(M, row, itop) : 0.0;
+      y[k] = (row < n && ibot >= 0 && ibot < n) ? SM(M, row, ibot) : 0.0;
     }
-  }
-  const int N = n + (n & 1);
-  const int nwarps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (n < 2) {
-    __syncthreads();
-    return 0;
-  }
-  for (int sweep = 0; sweep < SDPXG_JACOBI_MAX_SWEEPS; ++sweep) {
-    __syncthreads();  // the previous sweep's last rotations are visible
-    for (int p = warp; p < n; p += nwarps) {
-      double a = 0.0;
-      for (int k = lane; k < n; k += 32) a = fma(SM(M, k, p), SM(M, k, p), a);
-      a = warp_sum(a);
-      if (lane == 0) nrm[p] = a;
-    }
-    if (threadIdx.x == 0) *flag = 0;
-    __syncthreads();
-    for (int r = 0; r < N - 1; ++r) {
-      for (int pi = warp; pi < N / 2; pi += nwarps) {
-        int p, q;  // round-robin pairing without integer division: r, pi < N - 1
-        if (pi == 0) {
-          p = N - 1;
-          q = r;
-        } else {
-          p = r + pi;
-          if (p >= N - 1) p -= N - 1;
-          q = r - pi + N - 1;
-          if (q >= N - 1) q -= N - 1;
+    int sweeps = (n < 2) ? 0 : -1;
+    for (int sweep = 0; n >= 2 && sweep < SDPXG_JACOBI_MAX_SWEEPS; ++sweep) {
+      bool any_rot = false, any_big = false;
+      for (int r = 0; r < N - 1; ++r) {
+        double pa = 0.0, pb = 0.0, pg = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          pa = fma(x[k], x[k], pa);
+          pb = fma(y[k], y[k], pb);
+          pg = fma(x[k], y[k], pg);
         }
-        if (p >= n || q >= n) continue;
-        const double a = nrm[p], b = nrm[q];
-        double g = 0.0;
-        double x0 = 0.0, y0 = 0.0, x1 = 0.0, y1 = 0.0;  // n <= 64: two entries per lane
-        if (lane < n) {
-          x0 = SM(M, lane, p);
-          y0 = SM(M, lane, q);
+        double* buf = part + ((sweep * (N - 1) + r) & 1) * 768;
+        buf[warp * 32 + j] = pa;
+        buf[256 + warp * 32 + j] = pb;
+        buf[512 + warp * 32 + j] = pg;
+        asm volatile("bar.sync 1, 256;" ::: "memory");
+        double a = buf[j], b = buf[256 + j], g = buf[512 + j];
+#pragma unroll
+        for (int v = 1; v < 8; ++v) {
+          a += buf[v * 32 + j];
+          b += buf[256 + v * 32 + j];
+          g += buf[512 + v * 32 + j];
         }
-        if (lane + 32 < n) {
-          x1 = SM(M, lane + 32, p);
-          y1 = SM(M, lane + 32, q);
+        const double gg = g * g, ab = a * b;
+        const bool rot = j < H && gg > kTol2 * ab;
+        const bool big = j < H && gg > kBig2 * ab;
+        if (rot) {
+          const double h = b - a;
+          const double ir = rsqrt(fma(h, h, 4.0 * gg));
+          const double c2 = fabs(h) * ir, s2 = (h < 0.0 ? -2.0 * g : 2.0 * g) * ir;
+          const double cc = fma(0.5, c2, 0.5);
+          const double ic = rsqrt(cc);
+          const double c = cc * ic, s = 0.5 * s2 * ic;
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const double xk = x[k], yk = y[k];
+            x[k] = fma(c, xk, -s * yk);
+            y[k] = fma(s, xk, c * yk);
+          }
         }
-        g = fma(x1, y1, x0 * y0);
-        g = warp_sum(g);
-        if (g * g > (SDPXG_JACOBI_TOL * SDPXG_JACOBI_TOL) * (a * b)) {  // |g| > tol sqrt(ab)
-          const double zeta = (b - a) / (2.0 * g);
-          const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
-          const double c = rsqrt(fma(t, t, 1.0));
-          const double s = c * t;
-          if (lane < n) {
-            SM(M, lane, p) = c * x0 - s * y0;
-            SM(M, lane, q) = s * x0 + c * y0;
-          }
-          if (lane + 32 < n) {
-            SM(M, lane + 32, p) = c * x1 - s * y1;
-            SM(M, lane + 32, q) = s * x1 + c * y1;
-          }
-          if (V) {
-            if (lane < n) {
-              const double v0 = SM(V, lane, p), w0 = SM(V, lane, q);
-              SM(V, lane, p) = c * v0 - s * w0;
-              SM(V, lane, q) = s * v0 + c * w0;
-            }
-            if (lane + 32 < n) {
-              const double v1 = SM(V, lane + 32, p), w1 = SM(V, lane + 32, q);
-              SM(V, lane + 32, p) = c * v1 - s * w1;
-              SM(V, lane + 32, q) = s * v1 + c * w1;
-            }
-          }
-          if (lane == 0) {
-            nrm[p] = a - t * g;
-            nrm[q] = b + t * g;
-            *flag = 1;
-          }
+        any_rot |= __any_sync(kFull, rot);
+        any_big |= __any_sync(kFull, big);
+        // next positions: slot j's top from slot j-1 (slot 1's from slot 0's bottom, slot 0's
+        // top stays), slot j's bottom from slot j+1 (the last slot's from its own top; with a
+        // single slot nothing moves)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const double up = __shfl_up_sync(kFull, j == 0 ? y[k] : x[k], 1);
+          const double dn = __shfl_down_sync(kFull, y[k], 1);
+          const double nx = (j == 0) ? x[k] : up;
+          y[k] = (j == H - 1) ? (H == 1 ? y[k] : x[k]) : dn;
+          x[k] = nx;
+        }
+        const int up = __shfl_up_sync(kFull, j == 0 ? ibot : itop, 1);
+        const int dn = __shfl_down_sync(kFull, ibot, 1);
+        if (j < H) {
+          const int nt = (j == 0) ? itop : up;
+          ibot = (j == H - 1) ? (H == 1 ? ibot : itop) : dn;
+          itop = nt;
         }
       }
-      __syncthreads();
+      if (!any_rot || !any_big) {
+        sweeps = sweep + 1;
+        break;
+      }
     }
-    int more = *flag;
-    __syncthreads();
-    if (!more) return sweep + 1;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int row = 8 * warp + k;
+      if (row < n && j < H) {
+        if (itop < n) SM(M, row, itop) = x[k];
+        if (ibot < n) SM(M, row, ibot) = y[k];
+      }
+    }
+    if (threadIdx.x == 0) *out = sweeps;
   }
-  return -1;
+  __syncthreads();
+  const int res = *out;
+  __syncthreads();
+  return res;
 }
 
 // Householder tridiagonalisation of the symmetric A (destroyed).  d[0..n), e[0..n-1).

@@ -30,8 +30,8 @@
 namespace sdpxg {
 
 constexpr int kMatD = SDPXG_LD * SDPXG_NMAX;
-constexpr size_t kSmemNt =
-    (5 * kMatD + 2 * SDPXG_CHOL_SCRATCH + 2 * SDPXG_NMAX) * sizeof(double) + (SDPXG_NMAX + 1) * sizeof(int);
+constexpr size_t kSmemNtFactor = (3 * kMatD + 2 * SDPXG_CHOL_SCRATCH) * sizeof(double);
+constexpr size_t kSmemNt = (5 * kMatD + 2 * SDPXG_NMAX) * sizeof(double) + (SDPXG_NMAX + 1) * sizeof(int);
 constexpr size_t kSmemCong = 4 * kMatD * sizeof(double);
 constexpr size_t kSmemCirc = 2 * kMatD * sizeof(double);
 constexpr size_t kSmemStep = (4 * kMatD + SDPXG_CHOL_SCRATCH + 4 * SDPXG_NMAX + 32) * sizeof(double);
@@ -380,7 +380,8 @@ class Engine {
     device = dev;
     check(cudaSetDevice(device), "cudaSetDevice");
     check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
-    set_smem(reinterpret_cast<const void*>(k_nt_scale), kSmemNt);
+    set_smem(reinterpret_cast<const void*>(k_nt_factor), kSmemNtFactor);
+    set_smem(reinterpret_cast<const void*>(k_nt_svd), kSmemNt);
     set_smem(reinterpret_cast<const void*>(k_congruence), kSmemCong);
     set_smem(reinterpret_cast<const void*>(k_circ_op), kSmemCirc);
     set_smem(reinterpret_cast<const void*>(k_step_length), kSmemStep);
@@ -794,12 +795,15 @@ class Engine {
     need(z, "nt_scale z");
     clear_status();
     tbegin(KT_SCALE);
-    if (nblk)
-      ++g_launches, k_nt_scale<<<nblk, SDPXG_CONE_THREADS, kSmemNt, st>>>(blocks_, s, z, R_, Rinv_, Ginv_, lam_,
-                                                      lisqrt_, status_);
+    if (nblk) {
+      ++g_launches, k_nt_factor<<<nblk, SDPXG_CONE_THREADS, kSmemNtFactor, st>>>(blocks_, s, z, R_, Rinv_,
+                                                                                  status_);
+      ++g_launches, k_nt_svd<<<nblk, SDPXG_NT_SVD_THREADS, kSmemNt, st>>>(blocks_, R_, Rinv_, Ginv_, lam_,
+                                                                           lisqrt_, status_);
+    }
     if (nnn_)
       ++g_launches, k_nn_scale<<<(nnn_ + 255) / 256, 256, 0, st>>>(nnn_, nn_idx_, s, z, nnw_, nnlam_, status_);
-    launched("k_nt_scale");
+    launched("k_nt_factor, k_nt_svd");
     tend(KT_SCALE);
     return read_status() == 0;
   }
