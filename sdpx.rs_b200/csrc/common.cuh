@@ -197,8 +197,8 @@ __device__ __forceinline__ void cta_gemm(double* C, const double* A, bool ta, co
   }
 }
 
-// In-place lower Cholesky A = L L' (lower triangle of A used).  The update is lagged so
-// one barrier per column suffices: the trailing matrix is updated with the unscaled
+// In-place lower Cholesky A = L L' (lower triangle of A used), the shared-memory form for CTAs of
+// fewer than 256 threads.  The update is lagged so one barrier per column suffices: the trailing matrix is updated with the unscaled
 // column divided by the pivot, and columns are scaled at the end.  The thread that
 // finishes the next diagonal entry computes its reciprocal once and publishes it for the
 // next step (0 marks a pivot that is not positive and finite: the reciprocal of a finite
@@ -272,96 +272,118 @@ __device__ inline void cta_cholesky_lower2_smem(double* A, double* B, int n, dou
   __syncthreads();
 }
 
-// 1024-thread form: every entry stays in a register of its owner thread for the whole
-// factorisation -- thread t holds rows i = t % 64 of columns j = t / 64 + 16 p (p < 4) of each
-// matrix -- and column k is broadcast through a double-buffered shared row, so a column step is
-// one barrier, two shared reads per entry and no shared writes of the trailing matrix.  The
-// arithmetic per entry is the lagged update of the shared-memory form.
-__device__ inline void cta_cholesky_lower2_reg(double* A, double* B, int n, double* pivA,
-                                               double* pivB, bool* okA, bool* okB) {
-  __shared__ double colA[2][SDPXG_NMAX], colB[2][SDPXG_NMAX];
-  double* pinvA = pivA + SDPXG_NMAX;
-  double* pinvB = pivB + SDPXG_NMAX;
+// 1/v for a positive v: the hardware approximation refined by two Newton-Raphson steps
+// y <- y + y (1 - v y) (each doubles the correct bits; the result is within a few units in the
+// last place of 1/v).  Outside [2^-1000, 2^1000], where the approximation flushes, the IEEE
+// division.  Used on the critical path of the blocked CTA Cholesky factorisation.
+__device__ __forceinline__ double recip_newton(double v) {
+  if (!(v >= 0x1p-1000 && v <= 0x1p1000)) return 1.0 / v;
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(v));
+  double e = fma(-v, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-v, y, 1.0);
+  return fma(y, e, y);
+}
+
+// Blocked right-looking form (blockDim.x >= 256): panels of 8 columns.  Warp 0 factors A's
+// panel and warp 1 B's, in registers (lane l holds panel rows kb + l and kb + 32 + l; the pivot
+// and the entries of the updating rows come by shuffles; L(r,c) = a(r,c) / sqrt(pivot), the
+// reciprocal by recip_newton); then every warp takes 8 x 8 tiles of the trailing lower triangle
+// of both matrices, A22 -= L21 L21' on the FP64 tensor cores (two m8n8k4 steps).  Two barriers
+// per panel instead of one per column.  A pivot that is not positive and finite stops that
+// matrix (false); the other carries on.  Entries above the diagonal end as zeros.
+__device__ inline void cta_cholesky_lower2_panel(double* A, double* B, int n, bool* okA, bool* okB) {
+  __shared__ int live[2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   const bool two = (B != nullptr);
-  const int t = threadIdx.x, i = t & (SDPXG_NMAX - 1), j0 = t >> 6;
-  double a[4], b[4];
-  __syncthreads();  // the matrices were just written by other threads (loads, copies)
-#pragma unroll
-  for (int p = 0; p < 4; ++p) {
-    const int j = j0 + 16 * p;
-    const bool in = i < n && j < n;
-    a[p] = in ? SM(A, i, j) : 0.0;
-    b[p] = (in && two) ? SM(B, i, j) : 0.0;
+  if (threadIdx.x == 0) {
+    live[0] = 1;
+    live[1] = two ? 1 : 0;
   }
-  if (t == 0 && n > 0) {
-    const double x = a[0];
-    pivA[0] = x;
-    pinvA[0] = (x > 0.0 && isfinite(x)) ? 1.0 / x : 0.0;
-    if (two) {
-      const double y = b[0];
-      pivB[0] = y;
-      pinvB[0] = (y > 0.0 && isfinite(y)) ? 1.0 / y : 0.0;
-    }
-  }
-  bool liveA = true, liveB = two;
-  for (int k = 0; k < n; ++k) {
-    const int buf = k & 1;
-    if (j0 == (k & 15) && i > k && i < n) {  // the owners of column k publish it (rows > k)
-      const int p = k >> 4;  // select, not a dynamic index: a[] and b[] stay in registers
-      colA[buf][i] = p == 0 ? a[0] : p == 1 ? a[1] : p == 2 ? a[2] : a[3];
-      if (two) colB[buf][i] = p == 0 ? b[0] : p == 1 ? b[1] : p == 2 ? b[2] : b[3];
-    }
-    __syncthreads();  // column k and pivot k (published in step k - 1) are visible
-    const double dA = pinvA[k];
-    const double dB = two ? pinvB[k] : 0.0;
-    liveA = liveA && dA != 0.0;
-    liveB = liveB && dB != 0.0;
-    if (!liveA && !liveB) break;
-    if (i > k && i < n) {
-      const double ciA = colA[buf][i];
-      const double ciB = two ? colB[buf][i] : 0.0;
+  __syncthreads();
+  for (int kb = 0; kb < n; kb += 8) {
+    const int w = min(8, n - kb);
+    if (warp < 2 && live[warp]) {  // panel of one matrix in one warp
+      double* X = warp == 0 ? A : B;
+      const int r0 = kb + lane, r1 = kb + 32 + lane;
+      double P0[8], P1[8];
 #pragma unroll
-      for (int p = 0; p < 4; ++p) {
-        const int j = j0 + 16 * p;
-        if (j <= k || j > i) continue;
-        if (liveA) a[p] = a[p] - ciA * colA[buf][j] * dA;
-        if (liveB) b[p] = b[p] - ciB * colB[buf][j] * dB;
-        if (i == k + 1 && j == k + 1) {  // the next pivot is final now
-          if (liveA) {
-            pivA[k + 1] = a[p];
-            pinvA[k + 1] = (a[p] > 0.0 && isfinite(a[p])) ? 1.0 / a[p] : 0.0;
-          }
-          if (liveB) {
-            pivB[k + 1] = b[p];
-            pinvB[k + 1] = (b[p] > 0.0 && isfinite(b[p])) ? 1.0 / b[p] : 0.0;
+      for (int c = 0; c < 8; ++c) {
+        P0[c] = (c < w && r0 < n) ? SM(X, r0, kb + c) : 0.0;
+        P1[c] = (c < w && r1 < n) ? SM(X, r1, kb + c) : 0.0;
+      }
+      bool ok = true;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (c < w && ok) {
+          const double piv = __shfl_sync(0xffffffffu, P0[c], c);
+          ok = piv > 0.0 && isfinite(piv);
+          if (ok) {
+            const double d = sqrt(piv), rd = recip_newton(d);
+            P0[c] = lane < c ? 0.0 : (lane == c ? d : P0[c] * rd);
+            P1[c] *= rd;
+#pragma unroll
+            for (int c2 = c + 1; c2 < 8; ++c2) {
+              const double l = __shfl_sync(0xffffffffu, P0[c], c2);  // L(kb + c2, kb + c)
+              P0[c2] = fma(-P0[c], l, P0[c2]);
+              P1[c2] = fma(-P1[c], l, P1[c2]);
+            }
           }
         }
       }
-    }
-  }
-  __syncthreads();
-  *okA = liveA;
-  *okB = liveB;
-  double* rootA = pinvA + SDPXG_NMAX;
-  double* rootB = pinvB + SDPXG_NMAX;
-  if (t < n) {
-    if (liveA) rootA[t] = sqrt(pivA[t]);
-    if (liveB) rootB[t] = sqrt(pivB[t]);
-  }
-  __syncthreads();
+      if (ok) {
 #pragma unroll
-  for (int p = 0; p < 4; ++p) {
-    const int j = j0 + 16 * p;
-    if (i >= n || j >= n) continue;
-    if (liveA) SM(A, i, j) = (i > j) ? a[p] / rootA[j] : ((i == j) ? rootA[j] : 0.0);
-    if (liveB) SM(B, i, j) = (i > j) ? b[p] / rootB[j] : ((i == j) ? rootB[j] : 0.0);
+        for (int c = 0; c < 8; ++c) {
+          if (c < w && r0 < n) SM(X, r0, kb + c) = P0[c];
+          if (c < w && r1 < n) SM(X, r1, kb + c) = P1[c];
+        }
+      } else if (lane == 0) {
+        live[warp] = 0;
+      }
+    }
+    __syncthreads();
+    const int t0 = kb + 8;
+    if (t0 < n) {  // trailing update of the lower tiles on DMMA
+      const int nt = (n - t0 + 7) >> 3, per = nt * (nt + 1) / 2;
+      const int r = lane >> 2, q = lane & 3;
+      for (int e = warp; e < 2 * per; e += nwarps) {
+        const int mtx = e >= per ? 1 : 0;
+        if (!live[mtx]) continue;
+        double* X = mtx ? B : A;
+        int u = mtx ? e - per : e, ti = 0;
+        while (u > ti) {  // u -> (ti, tj), tj <= ti
+          u -= ti + 1;
+          ++ti;
+        }
+        const int row = t0 + 8 * ti, col = t0 + 8 * u;
+        double d0 = SM(X, row + r, col + 2 * q), d1 = SM(X, row + r, col + 2 * q + 1);
+#pragma unroll
+        for (int k4 = 0; k4 < 8; k4 += 4) {
+          const double a = -SM(X, row + r, kb + k4 + q), b = SM(X, col + r, kb + k4 + q);
+          dmma_m8n8k4(d0, d1, a, b);
+        }
+        SM(X, row + r, col + 2 * q) = d0;
+        SM(X, row + r, col + 2 * q + 1) = d1;
+      }
+    }
+    __syncthreads();
+  }
+  *okA = live[0] != 0;
+  *okB = two && live[1] != 0;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int i = e % n, j = e / n;
+    if (i < j) {
+      if (*okA) SM(A, i, j) = 0.0;
+      if (two && *okB) SM(B, i, j) = 0.0;
+    }
   }
   __syncthreads();
 }
 
 __device__ inline void cta_cholesky_lower2(double* A, double* B, int n, double* pivA, double* pivB,
                                            bool* okA, bool* okB) {
-  if (blockDim.x == 1024) cta_cholesky_lower2_reg(A, B, n, pivA, pivB, okA, okB);
+  if (blockDim.x >= 256) cta_cholesky_lower2_panel(A, B, n, okA, okB);
   else cta_cholesky_lower2_smem(A, B, n, pivA, pivB, okA, okB);
 }
 
@@ -372,6 +394,28 @@ __device__ inline bool cta_cholesky_lower(double* A, int n, double* piv) {
 }
 
 // Solve L' X = B in place of B (L lower, n x n), one column per thread.
+// B := L^-T B for the lower triangular L (n x n): back substitution by rows, one barrier per row.
+// Step i scales row i by 1 / L(i,i) (the reciprocals formed first, in parallel) and subtracts
+// L(i,k) x_i from rows k < i: thread t owns row k = t % 64 of the columns j = t / 64 + s b
+// (b = blockDim.x / 64), so a warp reads consecutive rows and one broadcast x_i.  x_i = B(i,j) /
+// L(i,i) is formed by each thread that needs it from the same operands (the same bits in every
+// copy).  blockDim.x is a multiple of 64; `rd` is n doubles of shared memory.
+__device__ __forceinline__ void cta_trsm_lower_t_rows(const double* L, double* B, int n, double* rd) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) rd[i] = 1.0 / SM(L, i, i);
+  __syncthreads();
+  const int k = threadIdx.x & (SDPXG_NMAX - 1), j0 = threadIdx.x >> 6, stride = blockDim.x >> 6;
+  for (int i = n - 1; i >= 0; --i) {
+    const double r = rd[i];
+    if (k < i) {
+      const double lik = SM(L, i, k);
+      for (int j = j0; j < n; j += stride) SM(B, k, j) = fma(-lik, SM(B, i, j) * r, SM(B, k, j));
+    }
+    __syncthreads();  // row i is read by no later step: scale it while step i-1 runs
+    for (int j = threadIdx.x; j < n; j += blockDim.x) SM(B, i, j) *= r;
+  }
+  __syncthreads();
+}
+
 __device__ __forceinline__ void cta_trsm_lower_t(const double* L, double* B, int n) {
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
     for (int i = n - 1; i >= 0; --i) {

@@ -114,8 +114,7 @@ k_nt_svd(const BlockDesc* __restrict__ blocks, double* __restrict__ R, double* _
     SM(V, i, rank[j]) = u;
   }
   __syncthreads();
-  cta_trsm_lower_t(L2, V, n);  // V = L2^-T U
-  __syncthreads();
+  cta_trsm_lower_t_rows(L2, V, n, sig);  // V = L2^-T U (sig is free: lsort holds lambda)
   double* Rg = R + bd.mat_off;
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     int i = e % n, j = e / n;

@@ -1,7 +1,8 @@
 // CTA-level dense eigen / singular-value routines for PSD blocks of order <= SDPXG_NMAX.
 //
-//  * cta_jacobi_left: one-sided (Hestenes) Jacobi with the parallel round-robin ordering,
-//    register-resident.  It orthogonalises the columns of M in place.  Relative accuracy of the small singular values is what the NT scaling
+//  * cta_jacobi_left: one-sided (Hestenes) Jacobi with the parallel odd-even ordering,
+//    register-resident.  It orthogonalises the columns of M in place.  Relative accuracy of
+//    the small singular values is what the NT scaling
 //    needs (the reference takes the SVD of L2'L1 directly instead of an eigensolve of the
 //    squared matrix, cones/psdtrianglecone.rs:378-386).
 //  * cta_tridiagonalize: Householder reduction of a symmetric matrix to tridiagonal form.
@@ -14,103 +15,158 @@
 #define SDPXG_JACOBI_MAX_SWEEPS 60
 #define SDPXG_BISECT_MAX 256
 
+namespace jacobi_detail {
+
+// x'y over the eight rows a lane holds, as a tree (depth 4).
+__device__ __forceinline__ double dot8(const double* x, const double* y) {
+  const double p0 = fma(x[1], y[1], x[0] * y[0]), p1 = fma(x[3], y[3], x[2] * y[2]);
+  const double p2 = fma(x[5], y[5], x[4] * y[4]), p3 = fma(x[7], y[7], x[6] * y[6]);
+  return (p0 + p1) + (p2 + p3);
+}
+
+// Sum of the eight warps' partials b[0], b[32], ..., b[224] as a tree (the same bits in every
+// warp that reads them).
+__device__ __forceinline__ double sum8(const double* b) {
+  return ((b[0] + b[32]) + (b[64] + b[96])) + ((b[128] + b[160]) + (b[192] + b[224]));
+}
+
+// Rotation x' = c x - s y, y' = s x + c y with x'y' = 0 for a pair with ||x||^2 = a, ||y||^2 = b,
+// x'y = g, by the half-angle formulas (|theta| <= pi/4):
+//   cos 2t = |h| / r, sin 2t = sign(h) 2g / r, r = sqrt(h^2 + 4g^2), h = b - a,
+//   c = sqrt((1 + cos 2t) / 2), s = sin 2t / (2c);
+// c >= 1/sqrt 2, so nothing cancels, and c^2 + s^2 = 1 to rounding.  tg = (s / c) g, with which
+// ||x'||^2 = a - tg and ||y'||^2 = b + tg.
+__device__ __forceinline__ void rotation(double a, double b, double g, double& c, double& s, double& tg) {
+  const double h = b - a;
+  const double ir = rsqrt(fma(h, h, 4.0 * g * g));
+  const double c2 = fabs(h) * ir, s2 = (h < 0.0 ? -2.0 * g : 2.0 * g) * ir;
+  const double cc = fma(0.5, c2, 0.5);
+  const double ic = rsqrt(cc);
+  c = cc * ic;
+  s = 0.5 * s2 * ic;
+  tg = s * ic * g;
+}
+
+}  // namespace jacobi_detail
+
 // One-sided (Hestenes) Jacobi on the columns of M (n x n, n <= 64, column-major shared memory
 // with leading dimension SDPXG_LD): on return M holds M V = U diag(sigma), columns in their
 // original order; V itself is not formed.  Returns the number of sweeps, or -1 when the sweep
 // bound was hit.  Every thread of the CTA calls it (blockDim.x >= 256).
 //
 // The matrix stays in registers for the whole iteration.  Warps 0..7 take part: warp w holds
-// rows [8w, 8w + 8) of the two columns of every pair, lane j the pair of slot j of the
-// round-robin (circle) ordering, which pairs positions j and N-1-j (N = n rounded up to even;
-// an odd n gets a zero column that never rotates).  After each round the columns move to their
-// next positions with two shuffles per row (tops one slot up, bottoms one slot down, slot 0's
-// top fixed), so no column goes back to shared memory inside the sweeps.  A pair's inner
-// products ||x||^2, ||y||^2, x'y are the sums of the eight warps' row partials taken in warp
-// order, so every warp holds the same bits and takes the same rotation decisions without a
-// broadcast; one named barrier per round (the partials are double-buffered in `part`, 1536
-// doubles of shared memory).  A pair rotates while |x'y| > 1e-15 sqrt(||x||^2 ||y||^2); the
-// angle comes from the half-angle formulas  cos 2t = |h| / r, sin 2t = sign(h) 2 x'y / r,
-// r = sqrt(h^2 + 4 (x'y)^2), h = ||y||^2 - ||x||^2,  c = sqrt((1 + cos 2t) / 2),
-// s = sin 2t / (2c)  (|t| <= pi/4, so c >= 1/sqrt 2 and nothing cancels; c^2 + s^2 = 1 to
-// rounding whatever the accuracy of the angle).  The sweeps stop after one without a rotation,
-// or after one in which every pair's cosine was below 1e-10 (the rotations of that sweep leave
-// cosines of order 1e-20: one-sided Jacobi converges quadratically).
+// rows [8w, 8w + 8), lane j the columns at positions 2j (A) and 2j+1 (B) of a line of
+// N = n rounded up to even positions (an odd n gets a zero column that never rotates).  The
+// pairs follow the odd-even ordering of Luk and Park: rounds alternate between the pairs
+// (2j, 2j+1), which a lane holds itself, and (2j+1, 2j+2), whose second column comes from lane
+// j+1 by a warp shuffle; after every rotation the two columns trade places, so in N rounds
+// every pair meets once (the moves are those of odd-even transposition sort on a reversed
+// line).  Only the across-lane rounds move data (two shuffles per row), and the lane that
+// computes a pair's rotation hands (c, s) to its right neighbour.  A pair's inner product is
+// the sum of the eight warps' row partials, taken in a fixed tree order, so every warp holds
+// the same bits and takes the same decisions without a broadcast; one named barrier per round
+// (the partials are double-buffered in `part`, 1536 doubles of shared memory).  Squared column
+// norms are summed exactly at the start of every sweep and carried through its rotations
+// (a - tg, b + tg).  A pair rotates while |x'y| > 1e-15 sqrt(||x||^2 ||y||^2); the sweeps stop
+// after one without a rotation, or after one in which every cosine was below 1e-10 (the
+// rotations of that sweep leave cosines of order 1e-20: one-sided Jacobi converges
+// quadratically).
 __device__ inline int cta_jacobi_left(double* M, int n, double* part, int* out) {
+  using namespace jacobi_detail;
   constexpr double kTol2 = 1e-30, kBig2 = 1e-20;
   constexpr unsigned kFull = 0xffffffffu;
   const int warp = threadIdx.x >> 5, j = threadIdx.x & 31;
   if (warp < 8) {
     const int N = n + (n & 1), H = N / 2;
-    int itop = j < H ? j : -1, ibot = j < H ? N - 1 - j : -1;
-    double x[8], y[8];
+    int iA = j < H ? 2 * j : -1, iB = j < H ? 2 * j + 1 : -1;
+    double A[8], B[8], nA = 0.0, nB = 0.0;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int row = 8 * warp + k;
-      x[k] = (row < n && itop >= 0 && itop < n) ? SM(M, row, itop) : 0.0;
-      y[k] = (row < n && ibot >= 0 && ibot < n) ? SM(M, row, ibot) : 0.0;
+      A[k] = (row < n && iA >= 0 && iA < n) ? SM(M, row, iA) : 0.0;
+      B[k] = (row < n && iB >= 0 && iB < n) ? SM(M, row, iB) : 0.0;
     }
     int sweeps = (n < 2) ? 0 : -1;
+    int phase = 0;
     for (int sweep = 0; n >= 2 && sweep < SDPXG_JACOBI_MAX_SWEEPS; ++sweep) {
-      bool any_rot = false, any_big = false;
-      for (int r = 0; r < N - 1; ++r) {
-        double pa = 0.0, pb = 0.0, pg = 0.0;
+      bool rotated = false, big = false;
+      for (int r = 0; r < N; r += 2) {
+        {  // pairs (2j, 2j+1): both columns in this lane
+          double* buf = part + phase * 768;
+          phase ^= 1;
+          buf[warp * 32 + j] = dot8(A, B);
+          if (r == 0) {
+            buf[256 + warp * 32 + j] = dot8(A, A);
+            buf[512 + warp * 32 + j] = dot8(B, B);
+          }
+          asm volatile("bar.sync 1, 256;" ::: "memory");
+          const double g = sum8(buf + j);
+          if (r == 0) {
+            nA = sum8(buf + 256 + j);
+            nB = sum8(buf + 512 + j);
+          }
+          const double a = nA, b = nB, gg = g * g, ab = a * b;
+          const bool rot = j < H && gg > kTol2 * ab;
+          rotated |= rot;
+          big |= j < H && gg > kBig2 * ab;
+          double c = 1.0, s = 0.0, tg = 0.0;
+          if (rot) rotation(a, b, g, c, s, tg);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          pa = fma(x[k], x[k], pa);
-          pb = fma(y[k], y[k], pb);
-          pg = fma(x[k], y[k], pg);
+          for (int k = 0; k < 8; ++k) {  // rotate and trade places: A <- y', B <- x'
+            const double x = A[k], y = B[k];
+            A[k] = fma(s, x, c * y);
+            B[k] = fma(c, x, -s * y);
+          }
+          nA = b + tg;
+          nB = a - tg;
+          const int t = iA;
+          iA = iB;
+          iB = t;
         }
-        double* buf = part + ((sweep * (N - 1) + r) & 1) * 768;
-        buf[warp * 32 + j] = pa;
-        buf[256 + warp * 32 + j] = pb;
-        buf[512 + warp * 32 + j] = pg;
-        asm volatile("bar.sync 1, 256;" ::: "memory");
-        double a = buf[j], b = buf[256 + j], g = buf[512 + j];
-#pragma unroll
-        for (int v = 1; v < 8; ++v) {
-          a += buf[v * 32 + j];
-          b += buf[256 + v * 32 + j];
-          g += buf[512 + v * 32 + j];
-        }
-        const double gg = g * g, ab = a * b;
-        const bool rot = j < H && gg > kTol2 * ab;
-        const bool big = j < H && gg > kBig2 * ab;
-        if (rot) {
-          const double h = b - a;
-          const double ir = rsqrt(fma(h, h, 4.0 * gg));
-          const double c2 = fabs(h) * ir, s2 = (h < 0.0 ? -2.0 * g : 2.0 * g) * ir;
-          const double cc = fma(0.5, c2, 0.5);
-          const double ic = rsqrt(cc);
-          const double c = cc * ic, s = 0.5 * s2 * ic;
+        {  // pairs (2j+1, 2j+2): this lane's B and lane j+1's A
+          double An[8], Bp[8];
 #pragma unroll
           for (int k = 0; k < 8; ++k) {
-            const double xk = x[k], yk = y[k];
-            x[k] = fma(c, xk, -s * yk);
-            y[k] = fma(s, xk, c * yk);
+            An[k] = __shfl_down_sync(kFull, A[k], 1);
+            Bp[k] = __shfl_up_sync(kFull, B[k], 1);
+          }
+          const double nAn = __shfl_down_sync(kFull, nA, 1);
+          const int iAn = __shfl_down_sync(kFull, iA, 1), iBp = __shfl_up_sync(kFull, iB, 1);
+          double* buf = part + phase * 768;
+          phase ^= 1;
+          buf[warp * 32 + j] = dot8(B, An);
+          asm volatile("bar.sync 1, 256;" ::: "memory");
+          const double g = sum8(buf + j);
+          const bool ex = j + 1 < H;  // pair (2j+1, 2j+2) exists
+          const double a = nB, b = nAn, gg = g * g, ab = a * b;
+          const bool rot = ex && gg > kTol2 * ab;
+          rotated |= rot;
+          big |= ex && gg > kBig2 * ab;
+          double c = ex ? 1.0 : 0.0, s = ex ? 0.0 : 1.0, tg = 0.0;  // no pair: B stays
+          if (rot) rotation(a, b, g, c, s, tg);
+          double cl = __shfl_up_sync(kFull, c, 1), sl = __shfl_up_sync(kFull, s, 1);
+          const double nAl = __shfl_up_sync(kFull, a - tg, 1);
+          const bool recv = j >= 1 && j < H;  // lane j's A is the right column of pair j-1
+          if (!recv) {
+            cl = 0.0;
+            sl = -1.0;
+          }
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            B[k] = fma(s, B[k], c * An[k]);   // y' of pair j
+            A[k] = fma(cl, Bp[k], -sl * A[k]);  // x' of pair j-1
+          }
+          if (ex) {
+            nB = b + tg;
+            iB = iAn;
+          }
+          if (recv) {
+            nA = nAl;
+            iA = iBp;
           }
         }
-        any_rot |= __any_sync(kFull, rot);
-        any_big |= __any_sync(kFull, big);
-        // next positions: slot j's top from slot j-1 (slot 1's from slot 0's bottom, slot 0's
-        // top stays), slot j's bottom from slot j+1 (the last slot's from its own top; with a
-        // single slot nothing moves)
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const double up = __shfl_up_sync(kFull, j == 0 ? y[k] : x[k], 1);
-          const double dn = __shfl_down_sync(kFull, y[k], 1);
-          const double nx = (j == 0) ? x[k] : up;
-          y[k] = (j == H - 1) ? (H == 1 ? y[k] : x[k]) : dn;
-          x[k] = nx;
-        }
-        const int up = __shfl_up_sync(kFull, j == 0 ? ibot : itop, 1);
-        const int dn = __shfl_down_sync(kFull, ibot, 1);
-        if (j < H) {
-          const int nt = (j == 0) ? itop : up;
-          ibot = (j == H - 1) ? (H == 1 ? ibot : itop) : dn;
-          itop = nt;
-        }
       }
-      if (!any_rot || !any_big) {
+      if (!__any_sync(kFull, rotated) || !__any_sync(kFull, big)) {
         sweeps = sweep + 1;
         break;
       }
@@ -119,8 +175,8 @@ __device__ inline int cta_jacobi_left(double* M, int n, double* part, int* out) 
     for (int k = 0; k < 8; ++k) {
       const int row = 8 * warp + k;
       if (row < n && j < H) {
-        if (itop < n) SM(M, row, itop) = x[k];
-        if (ibot < n) SM(M, row, ibot) = y[k];
+        if (iA < n) SM(M, row, iA) = A[k];
+        if (iB < n) SM(M, row, iB) = B[k];
       }
     }
     if (threadIdx.x == 0) *out = sweeps;
