@@ -53,6 +53,33 @@ struct RefineParams {
   int max_iter, guard_max;
 };
 
+// One reduction of a batched launch (k_reduce_batch): op over x (and y) of length n.
+struct RedReq {
+  int op;
+  long n;
+  const double* x;
+  const double* y;
+};
+constexpr int kRedBatchMax = 12;
+struct RedBatch {
+  RedReq r[kRedBatchMax];
+};
+
+// One vector update of a batched launch (k_lincomb_batch): out = a x + b y + c w over n entries
+// (a null operand is left out), with the arithmetic of k_lincomb.
+struct LinReq {
+  long n;
+  double a, b, c;
+  const double* x;
+  const double* y;
+  const double* w;
+  double* out;
+};
+constexpr int kLinBatchMax = 6;
+struct LinBatch {
+  LinReq r[kLinBatchMax];
+};
+
 struct BlockDesc {
   int n;         // block order
   int svec_off;  // first row of the block in the stacked cone vector
@@ -394,26 +421,38 @@ __device__ inline bool cta_cholesky_lower(double* A, int n, double* piv) {
 }
 
 // Solve L' X = B in place of B (L lower, n x n), one column per thread.
-// B := L^-T B for the lower triangular L (n x n): back substitution by rows, one barrier per row.
-// Step i scales row i by 1 / L(i,i) (the reciprocals formed first, in parallel) and subtracts
-// L(i,k) x_i from rows k < i: thread t owns row k = t % 64 of the columns j = t / 64 + s b
-// (b = blockDim.x / 64), so a warp reads consecutive rows and one broadcast x_i.  x_i = B(i,j) /
-// L(i,i) is formed by each thread that needs it from the same operands (the same bits in every
-// copy).  blockDim.x is a multiple of 64; `rd` is n doubles of shared memory.
-__device__ __forceinline__ void cta_trsm_lower_t_rows(const double* L, double* B, int n, double* rd) {
+// B := L^-T B for the lower triangular L (n x n, n <= 64): blocked back substitution, 8 rows at
+// a time from the bottom.  Each block of rows is solved against its 8 x 8 diagonal block, one
+// thread per column of B (x_i = (b_i - sum_k L(k,i) x_k) / L(i,i), the reciprocals formed first,
+// in parallel); the rows above then take B(0:ib, :) -= L(ib:ib+8, 0:ib)' X on the FP64 tensor
+// cores, one warp per 8 x 8 tile (two m8n8k4 steps).  Two barriers per block of rows.
+// blockDim.x >= 64; `rd` is n doubles of shared memory.
+__device__ __forceinline__ void cta_trsm_lower_t_blocked(const double* L, double* B, int n, double* rd) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) rd[i] = 1.0 / SM(L, i, i);
   __syncthreads();
-  const int k = threadIdx.x & (SDPXG_NMAX - 1), j0 = threadIdx.x >> 6, stride = blockDim.x >> 6;
-  for (int i = n - 1; i >= 0; --i) {
-    const double r = rd[i];
-    if (k < i) {
-      const double lik = SM(L, i, k);
-      for (int j = j0; j < n; j += stride) SM(B, k, j) = fma(-lik, SM(B, i, j) * r, SM(B, k, j));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int r = lane >> 2, q = lane & 3, nt = (n + 7) >> 3;
+  for (int ib = (nt - 1) * 8; ib >= 0; ib -= 8) {
+    const int ie = min(ib + 8, n);
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+      for (int i = ie - 1; i >= ib; --i) {
+        double acc = SM(B, i, j);
+        for (int k = i + 1; k < ie; ++k) acc = fma(-SM(L, k, i), SM(B, k, j), acc);
+        SM(B, i, j) = acc * rd[i];
+      }
     }
-    __syncthreads();  // row i is read by no later step: scale it while step i-1 runs
-    for (int j = threadIdx.x; j < n; j += blockDim.x) SM(B, i, j) *= r;
+    __syncthreads();
+    for (int t = warp; t < (ib >> 3) * nt; t += nwarps) {  // tiles above the block
+      const int ti = (t % (ib >> 3)) << 3, tj = (t / (ib >> 3)) << 3;
+      double d0 = SM(B, ti + r, tj + 2 * q), d1 = SM(B, ti + r, tj + 2 * q + 1);
+#pragma unroll
+      for (int k4 = 0; k4 < 8; k4 += 4)
+        dmma_m8n8k4(d0, d1, -SM(L, ib + k4 + q, ti + r), SM(B, ib + k4 + q, tj + r));
+      SM(B, ti + r, tj + 2 * q) = d0;
+      SM(B, ti + r, tj + 2 * q + 1) = d1;
+    }
+    __syncthreads();
   }
-  __syncthreads();
 }
 
 __device__ __forceinline__ void cta_trsm_lower_t(const double* L, double* B, int n) {

@@ -114,7 +114,7 @@ k_nt_svd(const BlockDesc* __restrict__ blocks, double* __restrict__ R, double* _
     SM(V, i, rank[j]) = u;
   }
   __syncthreads();
-  cta_trsm_lower_t_rows(L2, V, n, sig);  // V = L2^-T U (sig is free: lsort holds lambda)
+  cta_trsm_lower_t_blocked(L2, V, n, sig);  // V = L2^-T U (sig is free: lsort holds lambda)
   double* Rg = R + bd.mat_off;
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     int i = e % n, j = e / n;
@@ -354,9 +354,13 @@ k_step_length(const BlockDesc* __restrict__ blocks, const double* __restrict__ R
 // Eigenvalue summary of smat(v) per block: out[2b] = lambda_min, out[2b+1] = sum of positive
 // eigenvalues.  (margins, psdtrianglecone.rs; also the cone distance of the original-
 // coordinate acceptance test, default/original_check.rs:306-340.)
+// min_only != 0 (the acceptance test, which reads only max(0, -lambda_min)): out[2b] =
+// min(lambda_min, 0) and out[2b+1] = 0.  A block whose Cholesky factorisation succeeds is
+// positive definite to working accuracy and gives 0 without an eigensolve; the others take the
+// tridiagonal reduction and the multisection for lambda_min alone.
 extern "C" __global__ void __launch_bounds__(SDPXG_CONE_THREADS)
 k_margins(const BlockDesc* __restrict__ blocks, const double* __restrict__ v, long ld,
-          double* __restrict__ out, uint32_t* __restrict__ status) {
+          double* __restrict__ out, uint32_t* __restrict__ status, int min_only) {
   extern __shared__ double smem[];
   const int b = blockIdx.x;
   const BlockDesc bd = blocks[b];
@@ -367,8 +371,27 @@ k_margins(const BlockDesc* __restrict__ blocks, const double* __restrict__ v, lo
   double* work = ee + SDPXG_NMAX;
   double* red = work + 2 * SDPXG_NMAX;
   double* eig = red + 32;
-  cta_load_smat(X, v + (long)blockIdx.y * ld + bd.svec_off, n);
+  const double* vb = v + (long)blockIdx.y * ld + bd.svec_off;
+  const long o = 2L * ((long)blockIdx.y * gridDim.x + b);
+  cta_load_smat(X, vb, n);
   __syncthreads();
+  if (min_only) {
+    if (cta_cholesky_lower(X, n, dd)) {
+      if (threadIdx.x == 0) out[o] = out[o + 1] = 0.0;
+      return;
+    }
+    cta_load_smat(X, vb, n);
+    __syncthreads();
+    cta_tridiagonalize(X, n, dd, ee, work, red);
+    bool ok = true;
+    const double g = cta_eig_min(dd, ee, n, reinterpret_cast<int*>(red), &ok);
+    if (threadIdx.x == 0) {
+      if (!ok || !isfinite(g)) atomicOr(status, SDPXG_ST_EIG_FAIL);
+      out[o] = fmin(g, 0.0);
+      out[o + 1] = 0.0;
+    }
+    return;
+  }
   cta_tridiagonalize(X, n, dd, ee, work, red);
   cta_eig_all(dd, ee, n, eig, status);
   __syncthreads();
@@ -378,7 +401,6 @@ k_margins(const BlockDesc* __restrict__ blocks, const double* __restrict__ v, lo
       mn = fmin(mn, eig[k]);
       pos += fmax(eig[k], 0.0);
     }
-    long o = 2L * ((long)blockIdx.y * gridDim.x + b);
     out[o] = mn;
     out[o + 1] = pos;
   }

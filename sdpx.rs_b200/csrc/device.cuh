@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <initializer_list>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -204,7 +205,7 @@ __global__ void k_affine_ds(const BlockDesc*, const double*, double*);
 __global__ void k_shift_unit(const BlockDesc*, double*, double);
 __global__ void k_step_length(const BlockDesc*, const double*, const double*, const double*,
                               const double*, const double*, double, int, double*, uint32_t*);
-__global__ void k_margins(const BlockDesc*, const double*, long, double*, uint32_t*);
+__global__ void k_margins(const BlockDesc*, const double*, long, double*, uint32_t*, int);
 __global__ void k_schur_transform(const BlockDesc*, const int*, const int*, const long*,
                                   const double*, const double*, double*);
 __global__ void k_schur_block_gemm(const BlockDesc*, const int*, const int*, const long*,
@@ -249,6 +250,8 @@ __global__ void k_lincomb(long, double, const double*, double, const double*, do
 __global__ void k_reduce_partial(int, long, const double*, const double*, double*);
 __global__ void k_reduce_final(int, int, const double*, double*);
 __global__ void k_reduce_fused(int, long, const double*, const double*, double*, unsigned*, double*);
+__global__ void k_reduce_batch(RedBatch, double*, unsigned*, double*, int);
+__global__ void k_lincomb_batch(LinBatch);
 __global__ void k_refine_head(const double*, const double*, const double*, const double*,
                               const double*, int, RefineCtl*, RefineParams, cudaGraphConditionalHandle);
 __global__ void k_refine_step(const double*, RefineCtl*, RefineParams, cudaGraphConditionalHandle);
@@ -312,6 +315,23 @@ class Reducer {
       copy_h2d(slots_.p + s, &id_[op], sizeof(double), st);
     }
     return s;
+  }
+  // Consecutive reductions in one launch (slots first, first + 1, ...; the same values as the
+  // same adds one by one).  Returns the first slot.
+  int add_batch(cudaStream_t st, std::initializer_list<RedReq> reqs) {
+    const int k = (int)reqs.size();
+    if (k == 0 || k > kRedBatchMax) throw std::invalid_argument("reduction batch size");
+    if (count_ + k > kSlots) throw CudaError("reducer slots exhausted");
+    RedBatch b{};
+    int i = 0;
+    for (const RedReq& q : reqs) {
+      if (q.n > 0 && !q.x) throw std::invalid_argument("null device buffer: reduction input");
+      b.r[i++] = q;
+    }
+    const int first = count_;
+    count_ += k;
+    ++g_launches, k_reduce_batch<<<dim3(kBlocks, k), 256, 0, st>>>(b, partial_.p, counters_.p, slots_.p, first);
+    return first;
   }
   int count() const { return count_; }
   // Device address of a slot (read by the control kernels of the device-driven solves).

@@ -891,7 +891,9 @@ class Engine {
   }
   // (lambda_min, sum of positive eigenvalues) per PSD block of v, then (min, sum of positive
   // entries) over the orthant rows when there are any
-  bool margins(const double* v, std::vector<double>& out) {
+  // min_only: per PSD block min(lambda_min, 0) and 0 (the original-coordinate acceptance
+  // test); otherwise lambda_min and the sum of the positive eigenvalues.
+  bool margins(const double* v, std::vector<double>& out, bool min_only = false) {
     need(v, "margins v");
     const int parts = nblk + (nnn_ ? 1 : 0);
     out.assign(2 * parts, 0.0);
@@ -899,7 +901,7 @@ class Engine {
     clear_status();
     if (nblk)
       ++g_launches, k_margins<<<dim3(nblk, 1), SDPXG_CONE_THREADS, kSmemMarg, st>>>(blocks_, v, m, marg_out_,
-                                                                                    status_);
+                                                                                    status_, min_only ? 1 : 0);
     if (nnn_) ++g_launches, k_nn_margins<<<1, 256, 0, st>>>(nnn_, nn_idx_, v, marg_out_.p + 2 * nblk);
     launched("k_margins");
     copy_d2h(hblk_.p, marg_out_.p, 2 * parts * sizeof(double), st);
@@ -1274,6 +1276,27 @@ class Engine {
     need(out, "lincomb out");
     int grid = (int)std::min<long>((len + 255) / 256, 1184);
     ++g_launches, k_lincomb<<<grid, 256, 0, st>>>(len, a, x, b, y, c, w, out);
+  }
+  // Independent updates out = a x + b y + c w in one launch (the same values as one lincomb
+  // each).  A copy is {len, 1.0, 0.0, 0.0, src, nullptr, nullptr, dst}.  The outputs must not
+  // be read by another request of the same batch.
+  void lincomb_batch(std::initializer_list<LinReq> reqs) {
+    const int k = (int)reqs.size();
+    if (k == 0 || k > kLinBatchMax) throw std::invalid_argument("update batch size");
+    LinBatch b{};
+    long mx = 0;
+    int i = 0;
+    for (const LinReq& q : reqs) {
+      if (q.n > 0) need(q.out, "lincomb out");
+      b.r[i++] = q;
+      mx = std::max(mx, q.n);
+    }
+    if (mx <= 0) return;
+    const int grid = (int)std::min<long>((mx + 255) / 256, 1184);
+    ++g_launches, k_lincomb_batch<<<dim3(grid, k), 256, 0, st>>>(b);
+  }
+  static LinReq cp(double* dst, const double* src, long len) {
+    return LinReq{len, 1.0, 0.0, 0.0, src, nullptr, nullptr, dst};
   }
   void copy(double* dst, const double* src, long len) {
     if (len > 0) {

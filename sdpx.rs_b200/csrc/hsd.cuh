@@ -247,9 +247,7 @@ inline void HsdSolver::reduced_first(const double* r, double* x) {
   const int n = n_;
   E.trisolve(r, x);
   E.schur_residual(r, x, en_);
-  E.red.add(st(), RED_MAXABS, n, r, nullptr);
-  E.red.add(st(), RED_MAXABS, n, en_, nullptr);
-  E.red.add(st(), RED_FINITE, n, x, nullptr);
+  E.red.add_batch(st(), {{RED_MAXABS, n, r, nullptr}, {RED_MAXABS, n, en_, nullptr}, {RED_FINITE, n, x, nullptr}});
 }
 
 // Stationary refinement of the reduced system against the unshifted Schur complement, from the
@@ -346,10 +344,9 @@ inline bool HsdSolver::kkt_solve(const double* bx, const double* bz, double* x, 
   times.kkt_solves++;
   const int n = n_, m = m_;
   if (!st_.ir_enable) {
-    int a = E.red.add(st(), RED_FINITE, n, bx, nullptr);
-    int b = E.red.add(st(), RED_FINITE, m, bz, nullptr);
+    const int a = E.red.add_batch(st(), {{RED_FINITE, n, bx, nullptr}, {RED_FINITE, m, bz, nullptr}});
     auto& h = E.red.fetch(st());
-    if (h[a] != 1.0 || h[b] != 1.0) return false;
+    if (h[a] != 1.0 || h[a + 1] != 1.0) return false;
     const bool ok = solve_raw(bx, bz, x, z);
     times.solve += secs(t0);
     return ok;
@@ -361,8 +358,7 @@ inline bool HsdSolver::kkt_solve(const double* bx, const double* bz, double* x, 
     return ok;
   }
   E.segment(SEG_KKT_HEAD, {bx, bz, x}, [&] {
-    E.red.add(st(), RED_FINITE, n, bx, nullptr);
-    E.red.add(st(), RED_FINITE, m, bz, nullptr);
+    E.red.add_batch(st(), {{RED_FINITE, n, bx, nullptr}, {RED_FINITE, m, bz, nullptr}});
     condense_first(bx, bz, x);
   });
   {
@@ -375,10 +371,8 @@ inline bool HsdSolver::kkt_solve(const double* bx, const double* bz, double* x, 
   E.segment(SEG_KKT_TAIL, {bx, bz, x, z}, [&] {
     recover(bz, x, z);
     residual_full(bx, bz, x, z, ex_, ez_);
-    E.red.add(st(), RED_MAXABS, n, bx, nullptr);
-    E.red.add(st(), RED_MAXABS, m, bz, nullptr);
-    E.red.add(st(), RED_MAXABS, n, ex_, nullptr);
-    E.red.add(st(), RED_MAXABS, m, ez_, nullptr);
+    E.red.add_batch(st(), {{RED_MAXABS, n, bx, nullptr}, {RED_MAXABS, m, bz, nullptr},
+                           {RED_MAXABS, n, ex_, nullptr}, {RED_MAXABS, m, ez_, nullptr}});
   });
   bool ok = true;
   auto& h = E.red.fetch(st());
@@ -403,11 +397,10 @@ inline bool HsdSolver::kkt_solve(const double* bx, const double* bz, double* x, 
       }
       E.segment(SEG_OUT_TAIL, {bx, bz, x, z}, [&] {
         recover(ez_, cx_, cz_);
-        E.lincomb(n, 1.0, x, 1.0, cx_, 0.0, nullptr, candx_);
-        E.lincomb(m, 1.0, z, 1.0, cz_, 0.0, nullptr, candz_);
+        E.lincomb_batch({LinReq{n, 1.0, 1.0, 0.0, x, cx_, nullptr, candx_},
+                         LinReq{m, 1.0, 1.0, 0.0, z, cz_, nullptr, candz_}});
         residual_full(bx, bz, candx_, candz_, ex2_, ez2_);
-        E.red.add(st(), RED_MAXABS, n, ex2_, nullptr);
-        E.red.add(st(), RED_MAXABS, m, ez2_, nullptr);
+        E.red.add_batch(st(), {{RED_MAXABS, n, ex2_, nullptr}, {RED_MAXABS, m, ez2_, nullptr}});
       });
       auto& hh = E.red.fetch(st());
       norme = std::max(hh[0], hh[1]);
@@ -526,8 +519,8 @@ inline bool HsdSolver::kkt_solve_graph(const double* bx, const double* bz, doubl
       int h0 = 0, h1 = 0, hb = 0;
       uint64_t k_head = 0;
       cudaGraph_t g_head = run(&k_head, [&] {
-        h0 = E.red.add(st(), RED_FINITE, n, bx, nullptr);
-        h1 = E.red.add(st(), RED_FINITE, m, bz, nullptr);
+        h0 = E.red.add_batch(st(), {{RED_FINITE, n, bx, nullptr}, {RED_FINITE, m, bz, nullptr}});
+        h1 = h0 + 1;
         hb = E.red.count();
         condense_first(bx, bz, x);
       });
@@ -550,10 +543,8 @@ inline bool HsdSolver::kkt_solve_graph(const double* bx, const double* bz, doubl
       cudaGraph_t g_tail = run(&k_tail, [&] {
         recover(bz, x, z);
         residual_full(bx, bz, x, z, ex_, ez_);
-        t0 = E.red.add(st(), RED_MAXABS, n, bx, nullptr);
-        E.red.add(st(), RED_MAXABS, m, bz, nullptr);
-        E.red.add(st(), RED_MAXABS, n, ex_, nullptr);
-        E.red.add(st(), RED_MAXABS, m, ez_, nullptr);
+        t0 = E.red.add_batch(st(), {{RED_MAXABS, n, bx, nullptr}, {RED_MAXABS, m, bz, nullptr},
+                                    {RED_MAXABS, n, ex_, nullptr}, {RED_MAXABS, m, ez_, nullptr}});
       });
       cudaGraphNode_t nt = child(G, {w1}, g_tail);
       cudaGraphConditionalHandle hout;
@@ -590,11 +581,10 @@ inline bool HsdSolver::kkt_solve_graph(const double* bx, const double* bz, doubl
       uint64_t k_otail = 0;
       cudaGraph_t g_ot = run(&k_otail, [&] {
         recover(ez_, cx_, cz_);
-        E.lincomb(n, 1.0, x, 1.0, cx_, 0.0, nullptr, candx_);
-        E.lincomb(m, 1.0, z, 1.0, cz_, 0.0, nullptr, candz_);
+        E.lincomb_batch({LinReq{n, 1.0, 1.0, 0.0, x, cx_, nullptr, candx_},
+                         LinReq{m, 1.0, 1.0, 0.0, z, cz_, nullptr, candz_}});
         residual_full(bx, bz, candx_, candz_, ex2_, ez2_);
-        u0 = E.red.add(st(), RED_MAXABS, n, ex2_, nullptr);
-        E.red.add(st(), RED_MAXABS, m, ez2_, nullptr);
+        u0 = E.red.add_batch(st(), {{RED_MAXABS, n, ex2_, nullptr}, {RED_MAXABS, m, ez2_, nullptr}});
       });
       cudaGraphNode_t nq = child(body2, {w3}, g_ot);
       {
@@ -659,19 +649,21 @@ inline HsdSolver::Resid HsdSolver::residuals() {
   E.A_forward(x_, 1.0, 1.0, rzinf_);
   E.lincomb(n, -1.0, Px_, -tau_, q_, 1.0, rxinf_, rx_);
   E.lincomb(m, 1.0, rzinf_, -tau_, b_, 0.0, nullptr, rz_);
-  int sq = E.red.add(st(), RED_DOT, n, q_, x_);
-  int sb = E.red.add(st(), RED_DOT, m, b_, z_);
-  int ss = E.red.add(st(), RED_DOT, m, s_, z_);
-  int sp = E.red.add(st(), RED_DOT, n, x_, Px_);
+  const int sq = E.red.add_batch(st(), {{RED_DOT, n, q_, x_},
+                                        {RED_DOT, m, b_, z_},
+                                        {RED_DOT, m, s_, z_},
+                                        {RED_DOT, n, x_, Px_},
+                                        {RED_SUMSQ, n, x_, d_},
+                                        {RED_SUMSQ, m, z_, e_},
+                                        {RED_SUMSQ, m, s_, einv_},
+                                        {RED_SUMSQ, n, rxinf_, dinv_},
+                                        {RED_SUMSQ, n, Px_, dinv_},
+                                        {RED_SUMSQ, m, rzinf_, einv_},
+                                        {RED_SUMSQ, m, rz_, einv_},
+                                        {RED_SUMSQ, n, rx_, dinv_}});
+  const int sb = sq + 1, ss = sq + 2, sp = sq + 3;
   int nr[8];
-  nr[0] = E.red.add(st(), RED_SUMSQ, n, x_, d_);
-  nr[1] = E.red.add(st(), RED_SUMSQ, m, z_, e_);
-  nr[2] = E.red.add(st(), RED_SUMSQ, m, s_, einv_);
-  nr[3] = E.red.add(st(), RED_SUMSQ, n, rxinf_, dinv_);
-  nr[4] = E.red.add(st(), RED_SUMSQ, n, Px_, dinv_);
-  nr[5] = E.red.add(st(), RED_SUMSQ, m, rzinf_, einv_);
-  nr[6] = E.red.add(st(), RED_SUMSQ, m, rz_, einv_);
-  nr[7] = E.red.add(st(), RED_SUMSQ, n, rx_, dinv_);
+  for (int k = 0; k < 8; ++k) nr[k] = sq + 4 + k;
   auto& h = E.red.fetch(st());
   Resid r;
   r.qx = h[sq];
@@ -756,16 +748,15 @@ inline double HsdSolver::original_ratio(bool reduced) {
   if (!(st_.tol_original > 0)) return -1.0;
   const int n = n_, m = m_;
   const double tinv = 1.0 / tau_, cinv = 1.0 / eq_.c;
-  int a = E.red.add(st(), RED_MAXABS, m, rz_, einv_);
-  int b = E.red.add(st(), RED_MAXABS, n, rx_, dinv_);
+  const int a = E.red.add_batch(st(), {{RED_MAXABS, m, rz_, einv_}, {RED_MAXABS, n, rx_, dinv_}});
   auto& h = E.red.fetch(st());
-  double prim = h[a] * tinv, dual = h[b] * tinv * cinv;
+  double prim = h[a] * tinv, dual = h[a + 1] * tinv * cinv;
   E.lincomb(m, tau_, b_, 0.0, nullptr, 0.0, nullptr, wm1_);
   E.A_forward(x_, -1.0, 1.0, wm1_);  // b tau - A x
   std::vector<double> mr, ms, mz;
-  E.margins(wm1_, mr);
-  E.margins(s_, ms);
-  E.margins(z_, mz);
+  E.margins(wm1_, mr, true);
+  E.margins(s_, ms, true);
+  E.margins(z_, mz, true);
   for (int j = 0; j < E.nblk; ++j) {
     double ej = eq_.e[E.hblocks[j].svec_off];
     prim = std::max(prim, std::max(0.0, -mr[2 * j]) * tinv / ej);
@@ -773,9 +764,9 @@ inline double HsdSolver::original_ratio(bool reduced) {
     dual = std::max(dual, std::max(0.0, -mz[2 * j]) * tinv * cinv * ej);
   }
   if (E.nn_count()) {  // orthant rows, entrywise in original coordinates
-    int ra = E.red.add(st(), RED_NEGMAX, m, wm1_, nn_einv_);
-    int rb = E.red.add(st(), RED_NEGMAX, m, s_, nn_einv_);
-    int rc = E.red.add(st(), RED_NEGMAX, m, z_, nn_e_);
+    const int ra = E.red.add_batch(st(), {{RED_NEGMAX, m, wm1_, nn_einv_}, {RED_NEGMAX, m, s_, nn_einv_},
+                                          {RED_NEGMAX, m, z_, nn_e_}});
+    const int rb = ra + 1, rc = ra + 2;
     auto& hn = E.red.fetch(st());
     prim = std::max(prim, std::max(hn[ra], hn[rb]) * tinv);
     dual = std::max(dual, hn[rc] * tinv * cinv);
@@ -802,10 +793,9 @@ inline bool HsdSolver::hsd_direction(const double* rhs_x, const double* workz, d
                                      const double* z1, double* dtau, double* dkappa) {
   (void)rhs_x; (void)workz;
   const int n = n_, m = m_;
-  int a = E.red.add(st(), RED_DOT, n, q_, x1);
-  int b = E.red.add(st(), RED_DOT, m, b_, z1);
-  int c = E.red.add(st(), RED_DOT, n, q_, x2_);
-  int d = E.red.add(st(), RED_DOT, m, b_, z2_);
+  const int a = E.red.add_batch(st(), {{RED_DOT, n, q_, x1}, {RED_DOT, m, b_, z1},
+                                       {RED_DOT, n, q_, x2_}, {RED_DOT, m, b_, z2_}});
+  const int b = a + 1, c = a + 2, d = a + 3;
   int f1 = -1, f2 = -1, f3 = -1;
   if (E.has_P()) {
     // xi = x / tau; quad1 = xi' P x1; delta = (xi - x2)' P (xi - x2); quad2 = x2' P x2
@@ -826,9 +816,8 @@ inline bool HsdSolver::hsd_direction(const double* rhs_x, const double* workz, d
   den += delta - quad2;
   double dt = num / den;
   if (!std::isfinite(dt)) return false;
-  E.lincomb(n, 1.0, x1, dt, x2_, 0.0, nullptr, dx_);
-  E.lincomb(m, 1.0, z1, dt, z2_, 0.0, nullptr, dz_);
-  E.lincomb(m, -1.0, rhs_z, dt, b_, 0.0, nullptr, ds_);
+  E.lincomb_batch({LinReq{n, 1.0, dt, 0.0, x1, x2_, nullptr, dx_}, LinReq{m, 1.0, dt, 0.0, z1, z2_, nullptr, dz_},
+                   LinReq{m, -1.0, dt, 0.0, rhs_z, b_, nullptr, ds_}});
   E.A_forward(dx_, -1.0, 1.0, ds_);
   *dtau = dt;
   *dkappa = -(rhs_kappa + kappa_ * dt) / tau_;
@@ -871,8 +860,8 @@ inline bool HsdSolver::default_start() {
     }
   }
   if (ok) {
-    int a = E.red.add(st(), RED_MAXABS, n, x_, nullptr);
-    int b = E.red.add(st(), RED_MAXABS, m, z_, nullptr);
+    const int a = E.red.add_batch(st(), {{RED_MAXABS, n, x_, nullptr}, {RED_MAXABS, m, z_, nullptr}});
+    const int b = a + 1;
     auto& h = E.red.fetch(st());
     double bound = 1e12 * data_scale_;
     if (!(h[a] <= bound && h[b] <= bound)) ok = false;
@@ -994,19 +983,17 @@ inline void HsdSolver::solve() {
       break;
     }
     // keep the raw affine direction for the curve search
-    E.copy(ax_, dx_, n);
-    E.copy(as_, ds_, m);
-    E.copy(az_, dz_, m);
+    E.lincomb_batch({E.cp(ax_, dx_, n), E.cp(as_, ds_, m), E.cp(az_, dz_, m)});
     double adtau = dtau, adkappa = dkappa;
     alpha = step_bounds(dz_, ds_, dtau, dkappa, 0, 1.0);
     sigma = std::max(std::pow(1.0 - alpha, 3), 0.0);
     const double mfac = (it == 1) ? alpha : 1.0;
     // ---------------- combined rhs ----------------
     auto tc = clock::now();
-    E.lincomb(n, 1.0 - sigma, rx_, 0.0, nullptr, 0.0, nullptr, rhsx_);
+    E.lincomb_batch({LinReq{n, 1.0 - sigma, 0.0, 0.0, rx_, nullptr, nullptr, rhsx_},
+                     LinReq{m, mfac, 0.0, 0.0, dz_, nullptr, nullptr, wm1_}});
     double rhs_tau = (1.0 - sigma) * r.rtau;
     double rhs_kappa = -sigma * mu + mfac * dtau * dkappa + tau_ * kappa_;
-    E.lincomb(m, mfac, dz_, 0.0, nullptr, 0.0, nullptr, wm1_);
     E.cone_apply(CM_W, wm1_, wm2_);       // W dz
     E.cone_apply(CM_WINVT, ds_, wm3_);    // W^-T ds
     E.circ_op(wm3_, wm2_, wm1_);
@@ -1031,9 +1018,9 @@ inline void HsdSolver::solve() {
       for (double frac : {0.5, 0.25}) {
         double t = alpha + (1.0 - alpha) * frac;
         if (t * (1.0 - sigma * t) <= 1.01 * alpha * (1.0 - sigma)) continue;
-        E.lincomb(n, 1.0 - t, ax_, t, dx_, 0.0, nullptr, tx_);
-        E.lincomb(m, 1.0 - t, as_, t, ds_, 0.0, nullptr, ts_);
-        E.lincomb(m, 1.0 - t, az_, t, dz_, 0.0, nullptr, tz_);
+        E.lincomb_batch({LinReq{n, 1.0 - t, t, 0.0, ax_, dx_, nullptr, tx_},
+                         LinReq{m, 1.0 - t, t, 0.0, as_, ds_, nullptr, ts_},
+                         LinReq{m, 1.0 - t, t, 0.0, az_, dz_, nullptr, tz_}});
         double ttau = (1.0 - t) * adtau + t * dtau, tkap = (1.0 - t) * adkappa + t * dkappa;
         double a = t / st_.max_step_fraction;
         bool admitted = a <= 1.0 && tau_ + a * ttau >= 0 && kappa_ + a * tkap >= 0;
@@ -1045,9 +1032,7 @@ inline void HsdSolver::solve() {
           admitted = eok && az >= a && as >= a;
         }
         if (admitted) {
-          E.copy(dx_, tx_, n);
-          E.copy(ds_, ts_, m);
-          E.copy(dz_, tz_, m);
+          E.lincomb_batch({E.cp(dx_, tx_, n), E.cp(ds_, ts_, m), E.cp(dz_, tz_, m)});
           dtau = ttau;
           dkappa = tkap;
           alpha = t;
@@ -1065,20 +1050,17 @@ inline void HsdSolver::solve() {
     if (!have_best || tm < best_tm) {
       have_best = true;
       best_tm = tm;
-      E.copy(bestx_, x_, n);
-      E.copy(bests_, s_, m);
-      E.copy(bestz_, z_, m);
+      E.lincomb_batch({E.cp(bestx_, x_, n), E.cp(bests_, s_, m), E.cp(bestz_, z_, m),
+                       E.cp(prevx_, x_, n), E.cp(prevs_, s_, m), E.cp(prevz_, z_, m)});
       best_tau_ = tau_;
       best_kappa_ = kappa_;
+    } else {
+      E.lincomb_batch({E.cp(prevx_, x_, n), E.cp(prevs_, s_, m), E.cp(prevz_, z_, m)});
     }
-    E.copy(prevx_, x_, n);
-    E.copy(prevs_, s_, m);
-    E.copy(prevz_, z_, m);
     prev_tau = tau_;
     prev_kappa = kappa_;
-    E.lincomb(n, 1.0, x_, alpha, dx_, 0.0, nullptr, x_);
-    E.lincomb(m, 1.0, s_, alpha, ds_, 0.0, nullptr, s_);
-    E.lincomb(m, 1.0, z_, alpha, dz_, 0.0, nullptr, z_);
+    E.lincomb_batch({LinReq{n, 1.0, alpha, 0.0, x_, dx_, nullptr, x_}, LinReq{m, 1.0, alpha, 0.0, s_, ds_, nullptr, s_},
+                     LinReq{m, 1.0, alpha, 0.0, z_, dz_, nullptr, z_}});
     tau_ += alpha * dtau;
     kappa_ += alpha * dkappa;
   }

@@ -18,6 +18,20 @@ extern "C" __global__ void k_lincomb(long n, double a, const double* x, double b
   }
 }
 
+// Several independent updates in one launch: grid row r applies request r (the arithmetic of
+// k_lincomb, so the same bits as the single launches).
+extern "C" __global__ void k_lincomb_batch(LinBatch bt) {
+  const LinReq q = bt.r[blockIdx.y];
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < q.n;
+       i += (long)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    if (q.x) v = q.a * q.x[i];
+    if (q.y) v = fma(q.b, q.y[i], v);
+    if (q.w) v = fma(q.c, q.w[i], v);
+    q.out[i] = v;
+  }
+}
+
 // op 0: sum x*y;  op 1: sum (x*y)^2 (scaled 2-norm squared, y = scales or null);
 // op 2: max |x*y|;  op 3: all finite (1.0 / 0.0) of x;  op 4: max(0, max -x*y) (y >= 0: a
 // nonnegative scale, or a mask that selects rows)
@@ -59,13 +73,13 @@ k_reduce_partial(int op, long n, const double* __restrict__ x, const double* __r
   }
 }
 
-// One launch per reduction: every block writes its partial, and the block that arrives last
+// One reduction per grid row: every block writes its partial, and the block that arrives last
 // (a ticket on counter, reset to 0 for the next use) folds the partials in the fixed order of
-// k_reduce_final and writes out -- the same value as the two-launch form, bit for bit.
-extern "C" __global__ void __launch_bounds__(RED_THREADS)
-k_reduce_fused(int op, long n, const double* __restrict__ x, const double* __restrict__ y,
-               double* __restrict__ partial, unsigned* __restrict__ counter,
-               double* __restrict__ out) {
+// k_reduce_final and writes out -- the same value as the two-launch form, bit for bit.  An
+// empty input (n = 0, x unread) gives the operation's identity.
+__device__ __forceinline__ void reduce_fused_row(int op, long n, const double* __restrict__ x,
+                                                 const double* __restrict__ y, double* __restrict__ partial,
+                                                 unsigned* __restrict__ counter, double* __restrict__ out) {
   __shared__ double red[RED_THREADS / 32];
   __shared__ bool last;
   double acc = red_identity(op);
@@ -92,6 +106,23 @@ k_reduce_fused(int op, long n, const double* __restrict__ x, const double* __res
     *out = v;
     *counter = 0u;
   }
+}
+
+extern "C" __global__ void __launch_bounds__(RED_THREADS)
+k_reduce_fused(int op, long n, const double* __restrict__ x, const double* __restrict__ y,
+               double* __restrict__ partial, unsigned* __restrict__ counter,
+               double* __restrict__ out) {
+  reduce_fused_row(op, n, x, y, partial, counter, out);
+}
+
+// Several independent reductions in one launch: grid row r computes request r into slot
+// first + r exactly as k_reduce_fused would (the same blocks per reduction, the same folding).
+extern "C" __global__ void __launch_bounds__(RED_THREADS)
+k_reduce_batch(RedBatch b, double* __restrict__ partial, unsigned* __restrict__ counters,
+               double* __restrict__ slots, int first) {
+  const RedReq q = b.r[blockIdx.y];
+  const int s = first + blockIdx.y;
+  reduce_fused_row(q.op, q.n, q.x, q.y, partial + (size_t)s * gridDim.x, counters + s, slots + s);
 }
 
 // One warp: lane l folds partials l, l+32, ... in order, then a fixed shuffle tree.
