@@ -188,53 +188,68 @@ __device__ inline int cta_jacobi_left(double* M, int n, double* part, int* out) 
 }
 
 // Householder tridiagonalisation of the symmetric A (destroyed).  d[0..n), e[0..n-1).
-// `work` is 2*n doubles of shared memory, `red` 32 doubles (unused: kept for the callers).
-// Step k reflects column k below the diagonal, x = A[k+1:n, k] (m <= 63 entries): every warp
-// forms |x|^2 and, after the matvec, v'p itself (one warp covers the whole vector, and every
-// warp gets the same value from the same butterfly), v and q = p - (v'p) v are formed inline
-// from column k (which the step does not modify), so a step needs two barriers: after p = A v
-// (one warp per row, reading the row as a column: A stays exactly symmetric) and after the
-// rank-2 update.
+// `work` is 2*n doubles of shared memory, `red` 32 doubles.  blockDim.x is a multiple of 64.
+// Step k reflects column k below the diagonal, x = A[k+1:n, k] (m <= 63 entries): warp 0 forms
+// |x|^2, the reflector's scale and v = (x - alpha e1) / |x - alpha e1| into shared memory (one
+// barrier); p = A v, one warp per row reading the row as a column (A stays exactly symmetric;
+// a barrier); warp 0 forms K = v'p (a barrier); then the rank-2 update A -= 2 (v q' + q v'),
+// q = p - K v, thread t on row t % 64 of the columns t / 64 + 16 s (a barrier).
 __device__ inline void cta_tridiagonalize(double* A, int n, double* d, double* e, double* work,
                                           double* red) {
-  (void)red;
   double* p = work;
+  double* v = work + n;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (int k = 0; k + 2 < n; ++k) {
     const int m = n - k - 1;  // length of the column below the diagonal
     const double* x = &SM(A, k + 1, k);
-    double part = 0.0;
-    for (int i = lane; i < m; i += 32) part = fma(x[i], x[i], part);
-    const double nrm2 = warp_sum(part);
-    const double x0 = x[0];
-    const double alpha = -copysign(sqrt(nrm2), x0);
-    const double vnorm2 = nrm2 - x0 * x0 + (x0 - alpha) * (x0 - alpha);
-    if (threadIdx.x == 0) {
-      d[k] = SM(A, k, k);
-      e[k] = (nrm2 == 0.0) ? 0.0 : alpha;
+    if (warp == 0) {
+      double part = 0.0;
+      for (int i = lane; i < m; i += 32) part = fma(x[i], x[i], part);
+      const double nrm2 = warp_sum(part);
+      const double x0 = x[0];
+      const double alpha = -copysign(sqrt(nrm2), x0);
+      const double vnorm2 = nrm2 - x0 * x0 + (x0 - alpha) * (x0 - alpha);
+      const bool skip = (nrm2 == 0.0 || vnorm2 == 0.0);  // column already reduced
+      const double vs = skip ? 0.0 : rsqrt(vnorm2);
+      for (int i = lane; i < m; i += 32) v[i] = (i == 0) ? (x0 - alpha) * vs : x[i] * vs;
+      if (lane == 0) {
+        d[k] = SM(A, k, k);
+        e[k] = (nrm2 == 0.0) ? 0.0 : alpha;
+        red[0] = skip ? 0.0 : 1.0;
+      }
     }
-    if (nrm2 == 0.0 || vnorm2 == 0.0) continue;  // column already reduced (uniform)
-    const double vs = rsqrt(vnorm2);
-    const double v0 = (x0 - alpha) * vs;
+    __syncthreads();
+    if (red[0] == 0.0) {
+      __syncthreads();  // red[0] is read by every thread before warp 0 rewrites it
+      continue;
+    }
     // p = A_sub v
     for (int i = warp; i < m; i += nwarps) {
       double acc = 0.0;
-      for (int j = lane; j < m; j += 32)
-        acc = fma(SM(A, k + 1 + j, k + 1 + i), (j == 0) ? v0 : x[j] * vs, acc);
+      for (int j = lane; j < m; j += 32) acc = fma(SM(A, k + 1 + j, k + 1 + i), v[j], acc);
       acc = warp_sum(acc);
       if (lane == 0) p[i] = acc;
     }
     __syncthreads();
-    double kp = 0.0;
-    for (int i = lane; i < m; i += 32) kp = fma((i == 0) ? v0 : x[i] * vs, p[i], kp);
-    const double K = warp_sum(kp);
+    if (warp == 0) {
+      double kp = 0.0;
+      for (int i = lane; i < m; i += 32) kp = fma(v[i], p[i], kp);
+      kp = warp_sum(kp);
+      if (lane == 0) red[1] = kp;
+    }
+    __syncthreads();
+    const double K = red[1];
     // A_sub -= 2 (v q' + q v'), q = p - K v (both triangles from the same two products)
-    for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
-      const int i = t % m, j = t / m;
-      const double vi = (i == 0) ? v0 : x[i] * vs, vj = (j == 0) ? v0 : x[j] * vs;
-      const double qi = p[i] - K * vi, qj = p[j] - K * vj;
-      const double u = __dadd_rn(__dmul_rn(vi, qj), __dmul_rn(qi, vj));
-      SM(A, k + 1 + i, k + 1 + j) -= 2.0 * u;
+    const int ri = threadIdx.x & 63, cstride = blockDim.x >> 6;
+    if (ri < m) {
+      const double vi = v[ri];
+      const double qi = p[ri] - K * vi;
+      for (int j = threadIdx.x >> 6; j < m; j += cstride) {
+        const double vj = v[j];
+        const double qj = p[j] - K * vj;
+        const double u = __dadd_rn(__dmul_rn(vi, qj), __dmul_rn(qi, vj));
+        SM(A, k + 1 + ri, k + 1 + j) -= 2.0 * u;
+      }
     }
     __syncthreads();
   }
@@ -250,7 +265,9 @@ __device__ inline void cta_tridiagonalize(double* A, int n, double* d, double* e
   __syncthreads();
 }
 
-// Number of eigenvalues of the tridiagonal (d, e) strictly below x.
+// Number of eigenvalues of the tridiagonal (d, e) strictly below x.  The quotient of each step
+// takes the Newton-refined reciprocal (recip_newton: a few units in the last place), which
+// keeps the count that of a matrix within a few ulps of (d, e); |q| >= pivmin throughout.
 __device__ __forceinline__ int sturm_count(const double* d, const double* e, int n, double x,
                                            double pivmin) {
   int cnt = 0;
@@ -258,7 +275,7 @@ __device__ __forceinline__ int sturm_count(const double* d, const double* e, int
   if (fabs(q) < pivmin) q = -pivmin;
   cnt += (q < 0.0);
   for (int i = 1; i < n; ++i) {
-    q = (d[i] - x) - e[i - 1] * e[i - 1] / q;
+    q = (d[i] - x) - e[i - 1] * e[i - 1] * copysign(recip_newton(fabs(q)), q);
     if (fabs(q) < pivmin) q = -pivmin;
     cnt += (q < 0.0);
   }
