@@ -81,39 +81,39 @@ typedef struct {
   double solve_time, objective, dual_objective, primal_residual, dual_residual, gap_abs, gap_rel;
 } sdpx_info;
 
-/* include/sdpx.h:84 (ffi/src/lib.rs:586-593) */
+/* include/sdpx.h:82 (ffi/src/lib.rs:586-593) */
 int32_t sdpx_default_settings_v4(sdpx_settings *out);
 #define sdpx_default_settings sdpx_default_settings_v4
-/* include/sdpx.h:88 (ffi/src/lib.rs:720-723): always 1, one GPU per handle */
+/* include/sdpx.h:86 (ffi/src/lib.rs:720-723): always 1, one GPU per handle */
 int32_t sdpx_mpi_world_size(void);
-/* include/sdpx.h:89 (ffi/src/lib.rs:594-607) */
+/* include/sdpx.h:87 (ffi/src/lib.rs:594-607) */
 int32_t sdpx_prepare(const sdpx_csc *P, const sdpx_scalars *q, const sdpx_csc *A,
                      const sdpx_scalars *b, const sdpx_cone *cones, uint64_t cone_count,
                      const sdpx_settings *settings, sdpx_handle **out);
-/* include/sdpx.h:92 (ffi/src/lib.rs:608-658): factor-authoritative sampled blocks.  Blocks with
+/* include/sdpx.h:90 (ffi/src/lib.rs:608-658): factor-authoritative sampled blocks.  Blocks with
  * dim = 1 (columns weight_k svec(q_k q_k')) run on the GPU's Gram form with the given basis and
  * weights (scaled by the equilibration); matrix-valued blocks (dim > 1) return 2. */
 int32_t sdpx_prepare_sampled(const sdpx_csc *P, const sdpx_scalars *q, const sdpx_csc *A_linear,
                              const sdpx_scalars *b, const sdpx_cone *cones, uint64_t cone_count,
                              const sdpx_settings *settings, const sdpx_sampled_block *blocks,
                              uint64_t block_count, sdpx_handle **out);
-/* include/sdpx.h:93 (ffi/src/lib.rs:660-663) */
+/* include/sdpx.h:91 (ffi/src/lib.rs:660-663) */
 int32_t sdpx_solve(sdpx_handle *handle);
-/* include/sdpx.h:100 (ffi/src/lib.rs:664-670) */
+/* include/sdpx.h:97 (ffi/src/lib.rs:664-670) */
 int32_t sdpx_update(sdpx_handle *handle, const sdpx_scalars *q, const sdpx_scalars *b);
-/* include/sdpx.h:101 (ffi/src/lib.rs:671-680) */
+/* include/sdpx.h:98 (ffi/src/lib.rs:671-680) */
 int32_t sdpx_get_info(sdpx_handle *handle, sdpx_info *out);
-/* include/sdpx.h:106 (ffi/src/lib.rs:689-703) */
+/* include/sdpx.h:103 (ffi/src/lib.rs:689-703) */
 int32_t sdpx_get_solver_name(sdpx_handle *handle, char *out, uint64_t capacity,
                              uint64_t *required);
-/* include/sdpx.h:113 (ffi/src/lib.rs:722-735): x[n], z[m], s[m], 6 summary scalars */
+/* include/sdpx.h:109 (ffi/src/lib.rs:722-735): x[n], z[m], s[m], 6 summary scalars */
 int32_t sdpx_result_f64(sdpx_handle *handle, double *out, uint64_t capacity, uint64_t *required);
-/* include/sdpx.h:114 (ffi/src/lib.rs:736-752) */
+/* include/sdpx.h:110 (ffi/src/lib.rs:736-752) */
 int32_t sdpx_result_decimal(sdpx_handle *handle, char *out, uint64_t capacity,
                             uint64_t *required);
-/* include/sdpx.h:117 (ffi/src/lib.rs:753-768) */
+/* include/sdpx.h:113 (ffi/src/lib.rs:753-768) */
 uint64_t sdpx_last_error(char *out, uint64_t capacity);
-/* include/sdpx.h:118 (ffi/src/lib.rs:769-786) */
+/* include/sdpx.h:114 (ffi/src/lib.rs:769-786) */
 int32_t sdpx_destroy(sdpx_handle *handle);
 
 /* ---- B200 extensions of the solver ABI ---- */
