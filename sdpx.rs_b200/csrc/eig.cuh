@@ -192,8 +192,8 @@ __device__ inline int cta_jacobi_left(double* M, int n, double* part, int* out) 
 // Step k reflects column k below the diagonal, x = A[k+1:n, k] (m <= 63 entries): warp 0 forms
 // |x|^2, the reflector's scale and v = (x - alpha e1) / |x - alpha e1| into shared memory (one
 // barrier); p = A v, one warp per row reading the row as a column (A stays exactly symmetric;
-// a barrier); warp 0 forms K = v'p (a barrier); then the rank-2 update A -= 2 (v q' + q v'),
-// q = p - K v, thread t on row t % 64 of the columns t / 64 + 16 s (a barrier).
+// a barrier); warp 0 forms K = v'p and q = p - K v in place of p (a barrier); then the rank-2
+// update A -= 2 (v q' + q v'), thread t on row t % 64 of the columns t / 64 + 16 s (a barrier).
 __device__ inline void cta_tridiagonalize(double* A, int n, double* d, double* e, double* work,
                                           double* red) {
   double* p = work;
@@ -231,22 +231,19 @@ __device__ inline void cta_tridiagonalize(double* A, int n, double* d, double* e
       if (lane == 0) p[i] = acc;
     }
     __syncthreads();
-    if (warp == 0) {
+    if (warp == 0) {  // K = v'p, then p <- q = p - K v in place
       double kp = 0.0;
       for (int i = lane; i < m; i += 32) kp = fma(v[i], p[i], kp);
-      kp = warp_sum(kp);
-      if (lane == 0) red[1] = kp;
+      const double K = warp_sum(kp);
+      for (int i = lane; i < m; i += 32) p[i] = p[i] - K * v[i];
     }
     __syncthreads();
-    const double K = red[1];
-    // A_sub -= 2 (v q' + q v'), q = p - K v (both triangles from the same two products)
+    // A_sub -= 2 (v q' + q v') (both triangles from the same two products)
     const int ri = threadIdx.x & 63, cstride = blockDim.x >> 6;
     if (ri < m) {
-      const double vi = v[ri];
-      const double qi = p[ri] - K * vi;
+      const double vi = v[ri], qi = p[ri];
       for (int j = threadIdx.x >> 6; j < m; j += cstride) {
-        const double vj = v[j];
-        const double qj = p[j] - K * vj;
+        const double vj = v[j], qj = p[j];
         const double u = __dadd_rn(__dmul_rn(vi, qj), __dmul_rn(qi, vj));
         SM(A, k + 1 + ri, k + 1 + j) -= 2.0 * u;
       }
