@@ -239,3 +239,40 @@ def test_kkt_solve_residual(kctx_prob):
     x, zz = ctx.kkt_solve(bx, bz)
     ex, ez, nrm = ctx.residual(bx, bz, x, zz)
     assert nrm <= 1e-9 * max(np.max(np.abs(bx)), np.max(np.abs(bz)))
+
+
+@pytest.mark.parametrize("orders", [[1, 2, 3, 4, 5, 7, 8, 9], [16, 33, 63, 64]])
+def test_nt_scale_edge_orders_match_oracle(orders):
+    """The register-resident Jacobi at the orders that exercise its layout: one pair slot (1, 2),
+    odd orders (a zero column that never rotates), and 63 / 64 (every lane and row in use);
+    lambda to 1e-12 and the scaling through Hs, W^-1 W = I and W^-T s = diag(lambda)."""
+    tri = [d * (d + 1) // 2 for d in orders]
+    m = sum(tri)
+    A = sp.random(m, 7, density=0.3, random_state=np.random.default_rng(11), format="csc")
+    ctx = KernelContext()
+    ctx.upload(A, orders)
+    rng = np.random.default_rng(13)
+    s, z, rows = [], [], []
+    r0 = 0
+    for d, t in zip(orders, tri):
+        for out in (s, z):
+            B = rng.standard_normal((d, d))
+            out.append(P.svec(B @ B.T / d + 0.1 * np.eye(d)))
+        rows.append(slice(r0, r0 + t))
+        r0 += t
+    s, z = np.concatenate(s), np.concatenate(z)
+    lam, status = ctx.nt_scale(s, z)
+    assert status == 0
+    cones = [ipm.PsdCone(d) for d in orders]
+    for c, r in zip(cones, rows):
+        assert c.update_scaling(s[r], z[r])
+    assert np.allclose(lam, np.concatenate([c.lam for c in cones]), rtol=1e-12, atol=0)
+    x = np.random.default_rng(17).standard_normal(m)
+    y = ctx.cone_apply(4, x)
+    yo = np.concatenate([c.mul_Hs(x[r]) for c, r in zip(cones, rows)])
+    assert np.max(np.abs(y - yo)) <= 1e-11 * max(1.0, np.max(np.abs(yo)))
+    assert np.max(np.abs(ctx.cone_apply(2, ctx.cone_apply(0, x)) - x)) <= 1e-10
+    y = ctx.cone_apply(3, s)
+    for c, r in zip(cones, rows):
+        M = ipm.svec_to_mat(y[r], c.n)
+        assert np.allclose(M, np.diag(c.lam), atol=1e-10 * c.lam.max())
